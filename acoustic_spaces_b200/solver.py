@@ -1,0 +1,203 @@
+"""The wave solver's time steps on a B200, behind the reference's own stepping interface.
+
+:class:`B200WaveSolver` is a drop-in for ``acoustic_spaces.engine.gpu.GpuWaveSolver``
+(src/acoustic_spaces/engine/gpu.py:445-612 of naelolaiz/acoustic-spaces): it takes a grid that the
+C++ solver (``acoustic_spaces._native.WaveSolver``) has laid out, reads its ``layout()`` once, and
+:meth:`B200WaveSolver.run` does what the solver's ``run`` does — it advances one step per sample
+of the drive and returns each probe's pressure before each step, probes x steps in float64 — from
+the GPU's own state, which persists across calls. Stepping is done by hand-written sm_100a
+kernels through the C ABI of ``include/fdtd_b200.h``; there is no other path, and a missing
+library or device raises.
+
+:func:`gpu_name`, :func:`hardware_gpu` and :func:`use_gpu` mirror the module functions of
+engine/gpu.py:302-346 for this device.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from collections.abc import Mapping
+from typing import Literal
+
+import numpy as np
+
+from acoustic_spaces_b200 import _abi
+
+Device = Literal["cpu", "gpu", "auto"]
+Precision = Literal["fp32", "fp64"]
+
+
+def _error(lib, handle=None) -> str:
+    raw = lib.fdtd_last_error(handle) if handle else lib.fdtd_global_error()
+    return (raw or b"").decode("utf-8", "replace")
+
+
+def _raise(lib, status: int, handle=None) -> None:
+    message = _error(lib, handle)
+    if status == _abi.FDTD_EINVAL:
+        raise ValueError(message)
+    if status == _abi.FDTD_ENOMEM:
+        raise MemoryError(message)
+    raise RuntimeError(message or f"the B200 wave stepper failed ({status})")
+
+
+def gpu_name(device: int = 0) -> str | None:
+    """The GPU the wave solver would run on, as ``"<name> (CUDA sm_100, <memory> GiB)"``, or
+    None without one (engine/gpu.py:302-311)."""
+    try:
+        lib = _abi.load_library()
+    except (RuntimeError, OSError):
+        return None
+    if lib.fdtd_device_count() <= device:
+        return None
+    buf = ctypes.create_string_buffer(256)
+    if lib.fdtd_device_name(device, buf, len(buf)) != _abi.FDTD_OK:
+        return None
+    return buf.value.decode()
+
+
+def hardware_gpu() -> bool:
+    """Whether a B200 is there to step on (engine/gpu.py:314-317)."""
+    return gpu_name() is not None
+
+
+def use_gpu(device: Device, steps: int | None = None) -> bool:
+    """Whether the wave solver runs on the GPU for the setting ``device`` (engine/gpu.py:318-346):
+    ``cpu`` never, ``gpu`` always (a ValueError without a B200), ``auto`` when there is one."""
+    del steps  # a B200 steps any grid the wave stage makes faster than the host
+    if device == "cpu":
+        return False
+    if device == "gpu":
+        if not hardware_gpu():
+            raise ValueError(
+                "simulation.wave.device is gpu, but no B200 (CUDA sm_100) is visible: set it to "
+                "cpu or auto"
+            )
+        return True
+    if device == "auto":
+        return hardware_gpu()
+    raise ValueError(f"the wave solver's device must be cpu, gpu or auto, not {device!r}")
+
+
+class B200WaveSolver:
+    """Steps the grid of ``solver`` (a fresh or reset ``acoustic_spaces._native.WaveSolver``, or
+    a layout dict with the names of its ``layout()``) on the GPU: :meth:`run` does what the
+    solver's ``run`` does, from the GPU's own state.
+
+    ``precision`` ``"fp32"`` is the reference's arithmetic, bit for bit; ``"fp64"`` steps the same
+    layout in double."""
+
+    def __init__(self, solver, *, precision: Precision = "fp32", device: int = 0) -> None:
+        self._lib = lib = _abi.load_library()
+        layout = solver if isinstance(solver, Mapping) else solver.layout()
+        if precision not in ("fp32", "fp64"):
+            raise ValueError("precision is fp32 or fp64")
+        self.precision = precision
+        packed, self._arrays = _abi.pack_layout(layout)
+        handle = ctypes.c_void_p()
+        status = lib.fdtd_create(
+            ctypes.byref(packed),
+            _abi.FDTD_FP64 if precision == "fp64" else _abi.FDTD_FP32,
+            int(device),
+            ctypes.byref(handle),
+        )
+        self._arrays = None  # borrowed only during fdtd_create
+        if status != _abi.FDTD_OK:
+            _raise(lib, status)
+        self._handle = handle
+        info = self.info()
+        self._probes = int(info.probes)
+        self.shape = tuple(int(v) for v in np.asarray(layout["shape"]).reshape(-1))
+
+    @property
+    def probes(self) -> int:
+        return self._probes
+
+    def info(self) -> _abi.FdtdInfo:
+        """The solver's counts (air cells, special rows, branch states, layer cells, ...)."""
+        info = _abi.FdtdInfo()
+        status = self._lib.fdtd_get_info(self._handle, ctypes.byref(info))
+        if status != _abi.FDTD_OK:
+            _raise(self._lib, status, self._handle)
+        return info
+
+    @property
+    def air_cells(self) -> int:
+        return int(self.info().air_cells)
+
+    def run(self, signal: np.ndarray) -> np.ndarray:
+        """Advances one step per sample of ``signal`` (added at the source) and returns the
+        pressure at every probe before each step (probes, steps). A run that does not stay finite
+        returns its non-finite values, as the reference's does; the wave stage refuses it."""
+        signal = np.ascontiguousarray(signal, dtype=np.float32).reshape(-1)
+        steps = len(signal)
+        out = np.empty((self._probes, steps), np.float64)
+        if steps == 0:
+            return out
+        status = self._lib.fdtd_run(
+            self._handle,
+            signal.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+            steps,
+            out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+        )
+        if status not in (_abi.FDTD_OK, _abi.FDTD_ENONFINITE):
+            _raise(self._lib, status, self._handle)
+        return out
+
+    def run_device(self, signal_ptr: int, steps: int, out_ptr: int, out_stride: int) -> None:
+        """Queues ``steps`` steps on device buffers (addresses): the drive at ``signal_ptr``
+        (float32) and the probes' records at ``out_ptr`` (float64, probe p's step k at
+        ``p * out_stride + k``). Asynchronous; :meth:`synchronize` waits."""
+        status = self._lib.fdtd_run_device(self._handle, signal_ptr, steps, out_ptr, out_stride)
+        if status != _abi.FDTD_OK:
+            _raise(self._lib, status, self._handle)
+
+    def synchronize(self) -> None:
+        status = self._lib.fdtd_synchronize(self._handle)
+        if status != _abi.FDTD_OK:
+            _raise(self._lib, status, self._handle)
+
+    def reset(self) -> None:
+        """Silences the grid (WaveSolver::reset, fdtd.hpp:906-915)."""
+        status = self._lib.fdtd_reset(self._handle)
+        if status != _abi.FDTD_OK:
+            _raise(self._lib, status, self._handle)
+
+    def state(self) -> dict[str, np.ndarray]:
+        """The whole state on the host: ``current`` and ``previous`` pressures (cells), the
+        ``branch_current`` and ``branch_previous`` velocities, and ``layer`` (layer cells, 9)."""
+        info = self.info()
+        dtype = np.float64 if self.precision == "fp64" else np.float32
+        arrays = {
+            "current": np.empty(int(info.cells), dtype),
+            "previous": np.empty(int(info.cells), dtype),
+            "branch_current": np.empty(int(info.branch_states), dtype),
+            "branch_previous": np.empty(int(info.branch_states), dtype),
+            "layer": np.empty((int(info.layer_cells), 9), dtype),
+        }
+        status = self._lib.fdtd_read_state(
+            self._handle, *(a.ctypes.data_as(ctypes.c_void_p) for a in arrays.values())
+        )
+        if status != _abi.FDTD_OK:
+            _raise(self._lib, status, self._handle)
+        return arrays
+
+    def close(self) -> None:
+        handle, self._handle = getattr(self, "_handle", None), None
+        if handle:
+            self._lib.fdtd_destroy(handle)
+
+    def __del__(self) -> None:
+        try:
+            self.close()
+        except Exception:  # interpreter shutdown
+            pass
+
+    def __enter__(self) -> B200WaveSolver:
+        return self
+
+    def __exit__(self, *exc) -> None:
+        self.close()
+
+
+__all__ = ["B200WaveSolver", "Device", "gpu_name", "hardware_gpu", "use_gpu"]

@@ -1,0 +1,185 @@
+/*
+ * fdtd_b200.h — C ABI of the B200 (sm_100a) stepper for acoustic-spaces' low-frequency wave
+ * solver.
+ *
+ * The library steps a grid that the reference's C++ solver laid out: the arrays of
+ * WaveSolver::layout() (cpp/include/acoustic_spaces/fdtd.hpp:727-782 of naelolaiz/acoustic-spaces),
+ * borrowed for the duration of fdtd_create() and copied to the GPU. Each step does what
+ * WaveSolver::run() does (fdtd.hpp:786-904): it records every probe's pressure before the step
+ * (summed in double, fdtd.hpp:3525-3533), updates the interior air (fdtd.hpp:242-288), the special
+ * (boundary and source) cells with their branch velocities (fdtd.hpp:860-881) and the matched
+ * layer (fdtd.hpp:2242-2264), then swaps the two pressure levels and the two branch-velocity sets.
+ * In FDTD_FP32 the arithmetic is the reference's, operation for operation, in single precision
+ * with no fused multiply-adds and with subnormal results flushed to zero, as the reference's
+ * -ffp-contract=off build with its MXCSR flush does: the probes' time series equal the
+ * reference's bit for bit. FDTD_FP64 steps the same layout in double (each stored coefficient
+ * promoted), the GPU counterpart of the FP64 oracle.
+ *
+ * Every entry point returns FDTD_OK (0) or a negative status and never aborts; the message of the
+ * last failure is fdtd_last_error(handle), or fdtd_global_error() where no handle exists (a failed
+ * fdtd_create). Argument errors carry the reference's own wording where the reference refuses
+ * the same thing (fdtd.hpp:371-411, engine/gpu.py:495-504).
+ *
+ * Calls on one handle must not overlap; different handles are independent. Each handle owns one
+ * CUDA stream on the device it was created on.
+ */
+#ifndef FDTD_B200_H
+#define FDTD_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FDTD_B200_ABI_VERSION 1
+
+/* Status codes. */
+#define FDTD_OK 0
+#define FDTD_EINVAL (-1)  /* a refused argument: the reference's std::invalid_argument / ValueError */
+#define FDTD_ECUDA (-2)   /* a CUDA runtime error (message from the runtime) */
+#define FDTD_ENOMEM (-3)  /* device or host memory exhausted */
+#define FDTD_ENODEV (-4)  /* no CUDA device of compute capability 10.0 */
+#define FDTD_ENONFINITE (-5) /* fdtd_run: the pressure stopped being finite (wave.py:1220-1224) */
+
+/* Arithmetic of the fields. */
+#define FDTD_FP32 0
+#define FDTD_FP64 1
+
+/*
+ * The grid's layout, named after WaveSolver::layout()'s arrays (fdtd.hpp:727-782). Counts are
+ * given explicitly; the arrays are borrowed only during fdtd_create(). Moving-air arrays
+ * (flow_x, flow_y, flow_mask, wind_*, loop_*) have no place here: the reference steps moving
+ * air on the CPU only (engine/wave.py:1158-1160), and so does this library — a layout with
+ * flow_count > 0 is refused.
+ */
+typedef struct fdtd_layout {
+    uint64_t nx, ny, nz;          /* "shape": x fastest, sy = nx, sz = nx * ny */
+    uint32_t stencil;             /* "stencil": 7 or 19 */
+    uint32_t weight_count;        /* length of "weights": 6 or 18 */
+    const float *weights;         /* "weights": the update's link weights per direction */
+    float centre;                 /* "centre" */
+    float total;                  /* "total": the update's weights summed */
+    uint32_t scaled;              /* "scaled": 1 with a speed of sound per cell */
+    const float *scale;           /* "scale": nx*ny*nz when scaled, else NULL */
+    const float *layer_scale;     /* "layer_scale": layer_count when scaled, else NULL */
+    const uint8_t *types;         /* "types": nx*ny*nz of 0 solid, 1 interior, 2 special, 3 layer */
+    uint64_t special_count;
+    const int64_t *special;       /* "special": each special cell's index */
+    const uint64_t *link_start;   /* "link_start": special_count + 1 */
+    uint64_t link_count;
+    const uint8_t *link_direction; /* "link_direction": 0..17, fdtd.hpp:924-927's order */
+    const float *link_weight;     /* "link_weight" */
+    const float *coef_a;          /* "coef_a", "coef_b", "coef_inv", "source": special_count each */
+    const float *coef_b;
+    const float *coef_inv;
+    const float *source;
+    const uint64_t *state_start;  /* "state_start": special_count + 1 */
+    uint64_t state_count;
+    const int32_t *state_branch;  /* "state_branch": each branch state's branch */
+    const float *state_weight;    /* "state_weight" */
+    uint64_t branch_count;
+    const float *branch_now;      /* "branch_now", "branch_before", "branch_gain": branch_count */
+    const float *branch_before;
+    const float *branch_gain;
+    uint64_t layer_count;
+    const int64_t *layer_cells;   /* "layer_cells" */
+    /* "keep_x", "keep_face_x", "keep_y", "keep_face_y", "keep_z", "keep_face_z" and the same of
+       "push_*": each nx+1, ny+1 or nz+1 long when layer_count > 0, else NULL. */
+    const float *keep[6];
+    const float *push[6];
+    uint64_t probe_count;
+    const uint64_t *probe_start;  /* "probe_start": probe_count + 1 */
+    const uint64_t *probe_cells;  /* "probe_cells" */
+    const double *probe_weights;  /* "probe_weights" */
+    uint64_t flow_count;          /* length of "flow_mask": must be 0 */
+} fdtd_layout;
+
+typedef struct fdtd_solver fdtd_solver;
+
+/* Counts of a created solver, for reports (wave.py:1225-1259's info) and memory planning. */
+typedef struct fdtd_info {
+    uint64_t cells;          /* nx * ny * nz */
+    uint64_t air_cells;      /* interior + special + layer cells (the reference's air_cells) */
+    uint64_t interior_cells; /* cells the bulk sweep updates */
+    uint64_t special_cells;
+    uint64_t links;
+    uint64_t branch_states;
+    uint64_t layer_cells;
+    uint64_t probes;
+    uint64_t steps_done;     /* steps since creation or the last reset */
+    uint64_t device_bytes;   /* device memory the handle holds */
+    int32_t precision;       /* FDTD_FP32 or FDTD_FP64 */
+    int32_t device;          /* CUDA ordinal */
+} fdtd_info;
+
+/*
+ * Replaces engine/gpu.py:GpuWaveSolver.__init__ (engine/gpu.py:449-540), which packs
+ * solver.layout() into WebGPU buffers: copies `layout` to device `device` and creates a solver at
+ * rest (both pressure levels, branch velocities and matched-layer state zero).
+ * precision: FDTD_FP32 or FDTD_FP64. On failure *out is NULL and fdtd_global_error() says why.
+ */
+int fdtd_create(const fdtd_layout *layout, int precision, int device, fdtd_solver **out);
+
+/*
+ * Replaces GpuWaveSolver.run (engine/gpu.py:546-557) and WaveSolver::run (fdtd.hpp:786-904):
+ * advances `steps` steps, adding signal[k] at the source on step k, and writes each probe's
+ * pressure before each step to out[p * steps + k] (probes x steps, row-major). `signal` and `out`
+ * are host buffers (pageable or pinned). The state persists across calls: runs of any lengths
+ * concatenate to one run. Synchronous. Returns FDTD_ENONFINITE (after writing `out`) when a
+ * probe's pressure is not finite, as wave.py:1220-1224 refuses such a run.
+ */
+int fdtd_run(fdtd_solver *solver, const float *signal, uint64_t steps, double *out);
+
+/*
+ * The same as fdtd_run with device buffers, asynchronous on the handle's stream: d_signal holds
+ * `steps` floats, probe p's pressure before step k goes to d_out[p * out_stride + k]
+ * (out_stride >= steps). Nothing is checked for finiteness. fdtd_synchronize waits for it.
+ */
+int fdtd_run_device(fdtd_solver *solver, const float *d_signal, uint64_t steps, double *d_out,
+                    uint64_t out_stride);
+int fdtd_synchronize(fdtd_solver *solver);
+
+/* Replaces WaveSolver::reset (fdtd.hpp:906-915): silences the grid. */
+int fdtd_reset(fdtd_solver *solver);
+
+/* Frees the handle and its device memory; NULL is accepted. */
+int fdtd_destroy(fdtd_solver *solver);
+
+/* Counts of the solver. */
+int fdtd_get_info(const fdtd_solver *solver, fdtd_info *info);
+
+/*
+ * Copies the state to host buffers, each optional (NULL skips it): the current pressure and the
+ * one a step before (nx*ny*nz elements of float in FDTD_FP32, double in FDTD_FP64), the current
+ * and the previous branch velocities (state_count each) and the matched layer's state
+ * (9 * layer_count, the reference's per-cell order p_x, p_y, p_z, u-_x, u+_x, u-_y, u+_y, u-_z,
+ * u+_z, fdtd.hpp:2245). For parity checks of the whole field, not only the probes.
+ */
+int fdtd_read_state(const fdtd_solver *solver, void *current, void *previous, void *branch_current,
+                    void *branch_previous, void *layer_state);
+
+/* The message of the handle's last failure ("" if none). */
+const char *fdtd_last_error(const fdtd_solver *solver);
+
+/* The message of the calling thread's last failure without a handle (fdtd_create, queries). */
+const char *fdtd_global_error(void);
+
+/*
+ * Replaces engine/gpu.py:gpu_name (engine/gpu.py:302-311): the device's name as
+ * "<name> (CUDA sm_<major><minor>, <memory> GiB)" into buf. FDTD_ENODEV without a device.
+ */
+int fdtd_device_name(int device, char *buf, size_t size);
+
+/* CUDA devices of compute capability 10.x visible to the process (0 when none). */
+int fdtd_device_count(void);
+
+/* FDTD_B200_ABI_VERSION of the library. */
+int fdtd_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FDTD_B200_H */
