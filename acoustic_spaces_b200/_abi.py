@@ -222,6 +222,7 @@ SIGNATURES = {
         [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_uint64],
     ),
     "fdtd_synchronize": (ctypes.c_int, [ctypes.c_void_p]),
+    "fdtd_stream": (ctypes.c_void_p, [ctypes.c_void_p]),
     "fdtd_reset": (ctypes.c_int, [ctypes.c_void_p]),
     "fdtd_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "fdtd_get_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(FdtdInfo)]),

@@ -1,20 +1,13 @@
 // B200 (sm_100a) stepper for acoustic-spaces' low-frequency wave solver: the C ABI of
-// include/fdtd_b200.h over hand-written CUDA kernels.
+// include/fdtd_b200.h over the kernels of fdtd_kernels.cuh.
 //
-// One time step of WaveSolver::run (cpp/include/acoustic_spaces/fdtd.hpp:786-904 of
-// naelolaiz/acoustic-spaces) reads the current pressure b and the branch velocities wb, and writes
-// the next pressure over the previous one in a, the branch velocities over wa, and the matched
-// layer's state in place. Every cell's new value depends only on b, wb, its own a, wa and layer
-// state, so the four kinds of work of a step (probe records, interior air, special rows, matched
-// layer cells) write disjoint memory and run as one launch: its blocks are split by kind.
-// Consecutive steps are ordered by the launches on the handle's stream.
-//
-// Arithmetic: the library is built with --fmad=false and -ftz=true. Every expression keeps the
-// reference's operands in the reference's order, so with T = float each operation rounds as the
-// reference's -ffp-contract=off build does, subnormal results flushed to zero as its MXCSR flush
-// does (fdtd.hpp:316-336): the probes' series equal the reference's bit for bit. T = double steps
-// the same layout with every stored coefficient promoted.
+// fdtd_create validates a layout (WaveSolver::layout(), cpp/include/acoustic_spaces/
+// fdtd.hpp:727-782 of naelolaiz/acoustic-spaces) on the host, copies it to the device in a pitched
+// layout, and builds the TMA tensor maps of the bulk sweep. A time step (fdtd.hpp:838-886) is four
+// launches on the handle's stream: the interior air (TMA-pipelined, bulk_kernel), the special rows,
+// the matched layer and the probe records; the levels swap between steps by the launches' pointers.
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -27,12 +20,11 @@
 #include <vector>
 
 #include "fdtd_b200.h"
+#include "fdtd_kernels.cuh"
+
+using namespace fdtd;
 
 namespace {
-
-// ---------------------------------------------------------------------------------------------
-// Errors
-// ---------------------------------------------------------------------------------------------
 
 thread_local std::string g_error;
 
@@ -47,224 +39,25 @@ constexpr int kSteps[18][3] = {
     {-1, -1, 0}, {1, -1, 0}, {-1, 1, 0}, {1, 1, 0},   {-1, 0, -1}, {1, 0, -1},
     {-1, 0, 1},  {1, 0, 1},  {0, -1, -1}, {0, 1, -1}, {0, -1, 1},  {0, 1, 1}};
 
-constexpr int kBlock = 256;   // threads per block of every kind
-constexpr int kTileX = 32;    // bulk tile: 32 cells along x (one warp) ...
-constexpr int kTileY = 8;     // ... by 8 rows along y, marching along z
-constexpr int kSolid = 0, kInterior = 1, kSpecial = 2, kLayer = 3;
+constexpr uint64_t kPitchCells = 16;  // rows padded to a multiple of 16 cells
 
-// ---------------------------------------------------------------------------------------------
-// Device-side description of a grid (passed by value to every launch)
-// ---------------------------------------------------------------------------------------------
-
-struct Grid {
-    uint32_t nx, ny, nz, sy, sz;
-    // The bulk sweep's box: the bounding box of the interior cells, half open, and its tiling.
-    uint32_t x0, y0, z0, x1, y1, z1;
-    uint32_t tiles_x, tiles_y, z_chunk;
-    uint32_t bulk_blocks, special_blocks, layer_blocks, probe_blocks;
-    float axial, diagonal, centre, total;
-    const uint8_t *types;
-    const float *scale;
-    // Special rows (fdtd.hpp:860-881), as structure of arrays.
-    uint32_t specials;
-    const uint32_t *special, *link_start, *state_start;
-    const uint8_t *link_direction;
-    const float *link_weight, *coef_a, *coef_b, *coef_inv, *source;
-    const float *state_weight, *state_now, *state_before, *state_gain;
-    int32_t offset[18];
-    // Matched layer (fdtd.hpp:2242-2264): cells, per-axis coefficient tables (centre keep, face
-    // keep, centre push, face push per axis), and with a speed field each cell's scale.
-    uint32_t layers;
-    const uint32_t *layer_cells;
-    const float *layer_scale;
-    const float *keep_centre[3], *keep_face[3], *push_centre[3], *push_face[3];
-    // Probes (fdtd.hpp:3525-3533).
-    uint32_t probes;
-    const uint32_t *probe_start, *probe_cells;
-    const double *probe_weights;
-};
-
-template <typename T>
-struct Fields {
-    T *a;              // the pressure a step before, overwritten with the next
-    const T *b;        // the current pressure
-    T *wa;             // branch velocities a step before, overwritten with the next
-    const T *wb;       // current branch velocities
-    T *layer_state;    // 9 arrays of `layers`: p_x, p_y, p_z, u-_x, u+_x, u-_y, u+_y, u-_z, u+_z
-    const float *signal;  // the step's drive at signal[0]
-    double *out;       // probe p's record at out[p * out_stride]
-    uint64_t out_stride;
-};
-
-// ---------------------------------------------------------------------------------------------
-// Kernels
-// ---------------------------------------------------------------------------------------------
-
-// Interior air (fdtd.hpp:242-288): one warp-wide row of 32 cells per thread row, eight rows a
-// block, marching along z through a chunk of planes with the z neighbours kept in registers.
-// The reference's sums in its order: x-1, x+1, y-1, y+1, z-1, z+1, then the twelve edges.
-template <typename T, bool WIDE, bool SCALED>
-__device__ __forceinline__ void bulk_tile(const Grid &g, const Fields<T> &f, uint32_t tile) {
-    const uint32_t bx = tile % g.tiles_x;
-    const uint32_t rest = tile / g.tiles_x;
-    const uint32_t by = rest % g.tiles_y;
-    const uint32_t bz = rest / g.tiles_y;
-    const uint32_t x = g.x0 + bx * kTileX + (threadIdx.x % kTileX);
-    const uint32_t y = g.y0 + by * kTileY + (threadIdx.x / kTileX);
-    uint32_t z = g.z0 + bz * g.z_chunk;
-    if (x >= g.x1 || y >= g.y1 || z >= g.z1) return;
-    const uint32_t z_end = min(z + g.z_chunk, g.z1);
-    const uint32_t sy = g.sy, sz = g.sz;
-    const T *__restrict__ b = f.b;
-    T *__restrict__ a = f.a;
-    uint32_t i = x + y * sy + z * sz;
-    T below = b[i - sz], here = b[i];
-    const T axial = (T)g.axial, centre = (T)g.centre, diagonal = (T)g.diagonal, total = (T)g.total;
-    for (; z < z_end; ++z, i += sz) {
-        const T above = b[i + sz];
-        if (g.types[i] == kInterior) {
-            const T sum = b[i - 1] + b[i + 1] + b[i - sy] + b[i + sy] + below + above;
-            T next;
-            if (WIDE) {
-                const T edges = b[i - 1 - sy] + b[i + 1 - sy] + b[i - 1 + sy] + b[i + 1 + sy] +
-                                b[i - 1 - sz] + b[i + 1 - sz] + b[i - 1 + sz] + b[i + 1 + sz] +
-                                b[i - sy - sz] + b[i + sy - sz] + b[i - sy + sz] + b[i + sy + sz];
-                if (SCALED) {
-                    const T s = (T)g.scale[i];
-                    next = ((T)2 - total * s) * here + (s * axial) * sum + (s * diagonal) * edges - a[i];
-                } else {
-                    next = centre * here + axial * sum + diagonal * edges - a[i];
-                }
-            } else {
-                if (SCALED) {
-                    const T s = (T)g.scale[i];
-                    next = ((T)2 - total * s) * here + (s * axial) * sum - a[i];
-                } else {
-                    next = centre * here + axial * sum - a[i];
-                }
-            }
-            a[i] = next;
-        }
-        below = here;
-        here = above;
-    }
-}
-
-// Special row k (fdtd.hpp:860-881): its links, its branch states' flow, the update, then the
-// branch velocities. A state's term now * wb - before * wa is worked out again for the
-// velocities' update rather than kept: wa has not changed in between, so it is the same value.
-template <typename T>
-__device__ __forceinline__ void special_row(const Grid &g, const Fields<T> &f, uint32_t k) {
-    if (k >= g.specials) return;
-    const uint32_t i = g.special[k];
-    const T *__restrict__ b = f.b;
-    T sum = 0;
-    for (uint32_t l = g.link_start[k], e = g.link_start[k + 1]; l < e; ++l) {
-        const uint32_t j = (uint32_t)((int64_t)i + g.offset[g.link_direction[l]]);
-        sum += (T)g.link_weight[l] * b[j];
-    }
-    const uint32_t s0 = g.state_start[k], s1 = g.state_start[k + 1];
-    T flow = 0;
-    for (uint32_t j = s0; j < s1; ++j) {
-        const T own = (T)g.state_now[j] * f.wb[j] - (T)g.state_before[j] * f.wa[j];
-        flow += (T)g.state_weight[j] * own;
-    }
-    const T previous = f.a[i];
-    const T next = ((T)g.coef_a[k] * b[i] + sum - (T)g.coef_b[k] * previous - flow +
-                    (T)g.source[k] * (T)f.signal[0]) * (T)g.coef_inv[k];
-    f.a[i] = next;
-    for (uint32_t j = s0; j < s1; ++j) {
-        const T own = (T)g.state_now[j] * f.wb[j] - (T)g.state_before[j] * f.wa[j];
-        f.wa[j] = f.wa[j] + ((next - previous) * (T)g.state_gain[j] + own);
-    }
-}
-
-// Matched-layer cell c (fdtd.hpp:2242-2264): per axis its two face velocities, then its pressure
-// part; the cell's pressure is the parts' sum.
-template <typename T, bool SCALED>
-__device__ __forceinline__ void layer_cell(const Grid &g, const Fields<T> &f, uint32_t c) {
-    if (c >= g.layers) return;
-    const uint32_t L = g.layers;
-    const uint32_t i = g.layer_cells[c];
-    const uint32_t at[3] = {i % g.nx, (i / g.nx) % g.ny, i / g.sz};
-    const uint32_t strides[3] = {1u, g.sy, g.sz};
-    const T *__restrict__ b = f.b;
-    T *st = f.layer_state;
-    const T here = b[i];
-    T total = 0;
-#pragma unroll
-    for (int axis = 0; axis < 3; ++axis) {
-        const uint32_t stride = strides[axis], x = at[axis];
-        T below = st[(3 + 2 * axis) * L + c], above = st[(4 + 2 * axis) * L + c];
-        below = (T)g.keep_face[axis][x] * below - (T)g.push_face[axis][x] * (here - b[i - stride]);
-        above = (T)g.keep_face[axis][x + 1] * above - (T)g.push_face[axis][x + 1] * (b[i + stride] - here);
-        st[(3 + 2 * axis) * L + c] = below;
-        st[(4 + 2 * axis) * L + c] = above;
-        T part = st[axis * L + c];
-        if (SCALED) {
-            part = (T)g.keep_centre[axis][x] * part -
-                   ((T)g.push_centre[axis][x] * (T)g.layer_scale[c]) * (above - below);
-        } else {
-            part = (T)g.keep_centre[axis][x] * part - (T)g.push_centre[axis][x] * (above - below);
-        }
-        st[axis * L + c] = part;
-        total += part;
-    }
-    f.a[i] = total;
-}
-
-// Probe p's pressure before the step (fdtd.hpp:3525-3533): its cells' weighted sum in double, in
-// the layout's order.
-template <typename T>
-__device__ __forceinline__ void probe_record(const Grid &g, const Fields<T> &f, uint32_t p) {
-    if (p >= g.probes) return;
-    double value = 0.0;
-    for (uint32_t k = g.probe_start[p], e = g.probe_start[p + 1]; k < e; ++k) {
-        value += g.probe_weights[k] * (double)f.b[g.probe_cells[k]];
-    }
-    f.out[(uint64_t)p * f.out_stride] = value;
-}
-
-template <typename T, bool WIDE, bool SCALED>
-__global__ void __launch_bounds__(kBlock) step_kernel(const Grid g, const Fields<T> f) {
-    uint32_t block = blockIdx.x;
-    if (block < g.bulk_blocks) {
-        bulk_tile<T, WIDE, SCALED>(g, f, block);
-        return;
-    }
-    block -= g.bulk_blocks;
-    if (block < g.special_blocks) {
-        special_row<T>(g, f, block * kBlock + threadIdx.x);
-        return;
-    }
-    block -= g.special_blocks;
-    if (block < g.layer_blocks) {
-        layer_cell<T, SCALED>(g, f, block * kBlock + threadIdx.x);
-        return;
-    }
-    block -= g.layer_blocks;
-    probe_record<T>(g, f, block * kBlock + threadIdx.x);
-}
-
-// ---------------------------------------------------------------------------------------------
-// Host side
-// ---------------------------------------------------------------------------------------------
-
-struct DeviceBuffer {
-    void *ptr = nullptr;
-    size_t bytes = 0;
-};
+using EncodeTiled = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                 const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
 }  // namespace
 
 struct fdtd_solver {
     int device = 0;
+    int sms = 148;  // multiprocessors of the device
     int precision = FDTD_FP32;
     bool wide = false, scaled = false;
     cudaStream_t stream = nullptr;
     std::string error;
-    Grid grid{};
-    uint64_t nx = 0, ny = 0, nz = 0, n = 0;
+    Tables tables{};
+    BulkArgs bulk{};
+    uint32_t bulk_blocks = 0;
+    uint64_t nx = 0, ny = 0, nz = 0, n = 0, pitch = 0, n_device = 0;
     uint64_t air = 0, interior = 0, links = 0, states = 0, layers = 0, probes = 0, specials = 0;
     uint64_t steps_done = 0;
     std::vector<void *> allocations;  // every device allocation the handle owns
@@ -274,6 +67,10 @@ struct fdtd_solver {
     void *u[2] = {nullptr, nullptr};
     void *w[2] = {nullptr, nullptr};
     void *layer_state = nullptr;
+    unsigned int *d_error = nullptr;  // set by a kernel whose wait gave up
+    // Tensor maps of the bulk sweep: each level as the pressure tile (with halos) and as the
+    // previous-pressure tile, the cell types and the scales.
+    CUtensorMap map_b[2], map_a[2], map_t, map_s;
     // Staging for fdtd_run's host buffers, grown on demand.
     float *stage_signal = nullptr;
     double *stage_out = nullptr;
@@ -294,9 +91,9 @@ int cuda_fail(fdtd_solver *s, cudaError_t e, const char *what) {
     return e == cudaErrorMemoryAllocation ? FDTD_ENOMEM : FDTD_ECUDA;
 }
 
-#define CUDA_TRY(s, call)                                  \
-    do {                                                   \
-        cudaError_t e_ = (call);                           \
+#define CUDA_TRY(s, call)                                      \
+    do {                                                       \
+        cudaError_t e_ = (call);                               \
         if (e_ != cudaSuccess) return cuda_fail(s, e_, #call); \
     } while (0)
 
@@ -324,9 +121,6 @@ int zeros(fdtd_solver *s, size_t bytes, void **out) {
     return FDTD_OK;
 }
 
-// Host-side checks of every index the kernels will follow, so that no launch reads or writes
-// outside its buffers whatever layout it is given. Messages follow the reference's wording where
-// it refuses the same thing.
 int validate(const fdtd_layout *L, std::string &why) {
     auto refuse = [&](const std::string &m) {
         why = m;
@@ -421,6 +215,41 @@ int validate(const fdtd_layout *L, std::string &why) {
     return FDTD_OK;
 }
 
+// A layout index (x fastest, rows of nx) as the device's pitched index.
+inline uint32_t pitched(const fdtd_solver *s, uint64_t i) {
+    const uint64_t x = i % s->nx, y = (i / s->nx) % s->ny, z = i / (s->nx * s->ny);
+    return (uint32_t)(x + s->pitch * (y + s->ny * z));
+}
+
+EncodeTiled encoder() {
+    static EncodeTiled fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiled>(p);
+    }
+    return fn;
+}
+
+// A tensor map of the pitched 3-D array at `base` (pitch x ny x nz of `type`) read in boxes of
+// box_x x box_y x 1; zero fill outside it.
+int tensor_map(fdtd_solver *s, CUtensorMap *map, void *base, CUtensorMapDataType type, uint32_t bytes,
+               uint32_t box_x, uint32_t box_y) {
+    EncodeTiled encode = encoder();
+    if (!encode) return fail(s, FDTD_ECUDA, "the CUDA driver has no cuTensorMapEncodeTiled");
+    const cuuint64_t dims[3] = {s->pitch, s->ny, s->nz};
+    const cuuint64_t strides[2] = {s->pitch * bytes, s->pitch * s->ny * bytes};
+    const cuuint32_t box[3] = {box_x, box_y, 1};
+    const cuuint32_t unit[3] = {1, 1, 1};
+    const CUresult r = encode(map, type, 3, base, dims, strides, box, unit, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(s, FDTD_ECUDA, "cuTensorMapEncodeTiled refused a tensor map");
+    return FDTD_OK;
+}
+
 template <typename T>
 Fields<T> fields_for(const fdtd_solver *s, bool flip) {
     // flip = false: b is u[1] (current), a is u[0]; flip = true after an odd number of steps.
@@ -435,32 +264,73 @@ Fields<T> fields_for(const fdtd_solver *s, bool flip) {
 }
 
 template <typename T, bool WIDE, bool SCALED>
+int set_up_kernels(fdtd_solver *s) {
+    CUDA_TRY(s, cudaFuncSetAttribute(bulk_kernel<T, WIDE, SCALED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)Stage<T, SCALED>::smem));
+    return FDTD_OK;
+}
+
+template <typename T, bool WIDE, bool SCALED>
 int launch_steps(fdtd_solver *s, const float *d_signal, uint64_t steps, double *d_out, uint64_t stride) {
-    const Grid &g = s->grid;
-    const uint32_t blocks = g.bulk_blocks + g.special_blocks + g.layer_blocks + g.probe_blocks;
-    if (blocks == 0) return FDTD_OK;
+    const Tables &g = s->tables;
+    const uint32_t special_blocks = (uint32_t)((s->specials + kBlock - 1) / kBlock);
+    const uint32_t layer_blocks = (uint32_t)((s->layers + kBlock - 1) / kBlock);
+    const uint32_t probe_blocks = (uint32_t)((s->probes + kBlock - 1) / kBlock);
+    const uint32_t smem = Stage<T, SCALED>::smem;
     for (uint64_t k = 0; k < steps; ++k) {
-        Fields<T> f = fields_for<T>(s, (k & 1) != 0);
+        const bool flip = (k & 1) != 0;
+        Fields<T> f = fields_for<T>(s, flip);
         f.signal = d_signal + k;
         f.out = d_out + k;
         f.out_stride = stride;
-        step_kernel<T, WIDE, SCALED><<<blocks, kBlock, 0, s->stream>>>(g, f);
+        if (s->bulk_blocks) {
+            BulkArgs args = s->bulk;
+            args.a = f.a;
+            const int cur = flip ? 0 : 1, prev = flip ? 1 : 0;
+            bulk_kernel<T, WIDE, SCALED><<<s->bulk_blocks, kBlock, smem, s->stream>>>(s->map_b[cur], s->map_a[prev],
+                                                                                    s->map_t, s->map_s, args);
+        }
+        if (special_blocks) special_kernel<T><<<special_blocks, kBlock, 0, s->stream>>>(g, f);
+        if (layer_blocks) layer_kernel<T, SCALED><<<layer_blocks, kBlock, 0, s->stream>>>(g, f);
+        if (probe_blocks) probe_kernel<T><<<probe_blocks, kBlock, 0, s->stream>>>(g, f);
     }
     CUDA_TRY(s, cudaGetLastError());
     return FDTD_OK;
 }
 
+template <typename T, bool W, bool S>
+int dispatch_run(fdtd_solver *s, const float *d_signal, uint64_t steps, double *d_out, uint64_t stride) {
+    return launch_steps<T, W, S>(s, d_signal, steps, d_out, stride);
+}
+
 int dispatch(fdtd_solver *s, const float *d_signal, uint64_t steps, double *d_out, uint64_t stride) {
-    const bool fp64 = s->precision == FDTD_FP64;
-#define CASE(T, W, S)                                                    \
-    if (s->wide == W && s->scaled == S) return launch_steps<T, W, S>(s, d_signal, steps, d_out, stride);
-    if (fp64) {
-        CASE(double, false, false) CASE(double, false, true) CASE(double, true, false) CASE(double, true, true)
-    } else {
-        CASE(float, false, false) CASE(float, false, true) CASE(float, true, false) CASE(float, true, true)
+#define RUN_CALL(T, W, S) dispatch_run<T, W, S>(s, d_signal, steps, d_out, stride)
+    if (s->precision == FDTD_FP64) {
+        if (!s->wide && !s->scaled) return RUN_CALL(double, false, false);
+        if (!s->wide && s->scaled) return RUN_CALL(double, false, true);
+        if (s->wide && !s->scaled) return RUN_CALL(double, true, false);
+        return RUN_CALL(double, true, true);
     }
-#undef CASE
-    return fail(s, FDTD_EINVAL, "no kernel for this layout");
+    if (!s->wide && !s->scaled) return RUN_CALL(float, false, false);
+    if (!s->wide && s->scaled) return RUN_CALL(float, false, true);
+    if (s->wide && !s->scaled) return RUN_CALL(float, true, false);
+    return RUN_CALL(float, true, true);
+#undef RUN_CALL
+}
+
+int set_up(fdtd_solver *s) {
+#define SET_CALL(T, W, S) set_up_kernels<T, W, S>(s)
+    if (s->precision == FDTD_FP64) {
+        if (!s->wide && !s->scaled) return SET_CALL(double, false, false);
+        if (!s->wide && s->scaled) return SET_CALL(double, false, true);
+        if (s->wide && !s->scaled) return SET_CALL(double, true, false);
+        return SET_CALL(double, true, true);
+    }
+    if (!s->wide && !s->scaled) return SET_CALL(float, false, false);
+    if (!s->wide && s->scaled) return SET_CALL(float, false, true);
+    if (s->wide && !s->scaled) return SET_CALL(float, true, false);
+    return SET_CALL(float, true, true);
+#undef SET_CALL
 }
 
 // After `steps` steps the parity swap of fdtd.hpp:900-903: u[1] stays the current level.
@@ -468,72 +338,121 @@ void settle(fdtd_solver *s, uint64_t steps) {
     if (steps % 2 == 1) {
         std::swap(s->u[0], s->u[1]);
         std::swap(s->w[0], s->w[1]);
+        std::swap(s->map_b[0], s->map_b[1]);
+        std::swap(s->map_a[0], s->map_a[1]);
     }
     s->steps_done += steps;
+}
+
+// Whether a kernel's wait gave up since the last check (then clears the flag).
+int check_device_error(fdtd_solver *s) {
+    unsigned int flag = 0;
+    CUDA_TRY(s, cudaMemcpyAsync(&flag, s->d_error, sizeof flag, cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+    if (flag) {
+        CUDA_TRY(s, cudaMemsetAsync(s->d_error, 0, sizeof flag, s->stream));
+        return fail(s, FDTD_ECUDA, "a pipeline wait of the interior sweep gave up; the step's results are not valid");
+    }
+    return FDTD_OK;
 }
 
 int build(fdtd_solver *s, const fdtd_layout *L) {
     const uint64_t nx = L->nx, ny = L->ny, nz = L->nz, n = nx * ny * nz;
     s->nx = nx, s->ny = ny, s->nz = nz, s->n = n;
+    s->pitch = (nx + kPitchCells - 1) / kPitchCells * kPitchCells;
+    s->n_device = s->pitch * ny * nz;
+    if (s->n_device >= (1ull << 32)) return fail(s, FDTD_EINVAL, "the wave grid is too large for the GPU's 32-bit indices");
     s->wide = L->stencil == 19;
     s->scaled = L->scaled != 0;
-    Grid &g = s->grid;
-    g.nx = (uint32_t)nx, g.ny = (uint32_t)ny, g.nz = (uint32_t)nz;
-    g.sy = (uint32_t)nx, g.sz = (uint32_t)(nx * ny);
-    g.axial = L->weights[0];
-    g.diagonal = s->wide ? L->weights[6] : 0.0f;
-    g.centre = L->centre;
-    g.total = L->total;
+    const size_t e = s->precision == FDTD_FP64 ? 8 : 4;
+    Tables &g = s->tables;
+    g.pitch = (uint32_t)s->pitch;
+    g.ny = (uint32_t)ny;
+    g.nz = (uint32_t)nz;
+    g.sz = (uint32_t)(s->pitch * ny);
     for (int k = 0; k < 18; ++k)
-        g.offset[k] = (int32_t)(kSteps[k][0] + kSteps[k][1] * (int64_t)nx + kSteps[k][2] * (int64_t)(nx * ny));
+        g.offset[k] = (int32_t)(kSteps[k][0] + kSteps[k][1] * (int64_t)s->pitch + kSteps[k][2] * (int64_t)(s->pitch * ny));
 
-    // The interior cells' bounding box and the air count.
+    // Cell types and scales, pitched; the interior cells' bounding box and the air count.
+    std::vector<uint8_t> types(s->n_device, (uint8_t)kSolid);
+    std::vector<float> scale(s->scaled ? s->n_device : 0, 0.0f);
     uint64_t x0 = nx, y0 = ny, z0 = nz, x1 = 0, y1 = 0, z1 = 0, interior = 0, air = 0;
-    for (uint64_t i = 0; i < n; ++i) {
-        const uint8_t t = L->types[i];
-        if (t != kSolid) ++air;
-        if (t != kInterior) continue;
-        ++interior;
-        const uint64_t x = i % nx, y = (i / nx) % ny, z = i / (nx * ny);
-        x0 = std::min(x0, x), x1 = std::max(x1, x + 1);
-        y0 = std::min(y0, y), y1 = std::max(y1, y + 1);
-        z0 = std::min(z0, z), z1 = std::max(z1, z + 1);
-    }
+    for (uint64_t z = 0; z < nz; ++z)
+        for (uint64_t y = 0; y < ny; ++y) {
+            const uint64_t row = nx * (y + ny * z), drow = s->pitch * (y + ny * z);
+            std::memcpy(&types[drow], &L->types[row], nx);
+            if (s->scaled) std::memcpy(&scale[drow], &L->scale[row], nx * sizeof(float));
+            for (uint64_t x = 0; x < nx; ++x) {
+                const uint8_t t = L->types[row + x];
+                if (t != kSolid) ++air;
+                if (t != kInterior) continue;
+                ++interior;
+                x0 = std::min(x0, x), x1 = std::max(x1, x + 1);
+                y0 = std::min(y0, y), y1 = std::max(y1, y + 1);
+                z0 = std::min(z0, z), z1 = std::max(z1, z + 1);
+            }
+        }
     s->interior = interior, s->air = air;
-    if (interior == 0) x0 = y0 = z0 = x1 = y1 = z1 = 1;
-    g.x0 = (uint32_t)x0, g.y0 = (uint32_t)y0, g.z0 = (uint32_t)z0;
-    g.x1 = (uint32_t)x1, g.y1 = (uint32_t)y1, g.z1 = (uint32_t)z1;
-    g.tiles_x = (uint32_t)((x1 - x0 + kTileX - 1) / kTileX);
-    g.tiles_y = (uint32_t)((y1 - y0 + kTileY - 1) / kTileY);
-    // Planes per block: enough blocks for every SM several times over, long enough marches.
-    const uint64_t columns = (uint64_t)g.tiles_x * g.tiles_y;
-    const uint64_t depth = z1 - z0;
-    uint64_t chunk = depth;
-    while (chunk > 8 && columns * ((depth + chunk - 1) / chunk) < 148ull * 16) chunk = (chunk + 1) / 2;
-    g.z_chunk = (uint32_t)std::max<uint64_t>(chunk, 1);
-    const uint64_t tiles_z = interior ? (depth + g.z_chunk - 1) / g.z_chunk : 0;
-    const uint64_t bulk = interior ? columns * tiles_z : 0;
-    if (bulk >= (1ull << 31)) return fail(s, FDTD_EINVAL, "the wave grid is too large for one launch");
-    g.bulk_blocks = (uint32_t)bulk;
 
     int rc;
-    const uint8_t *types;
-    if ((rc = upload(s, L->types, n, &types))) return rc;
-    g.types = types;
-    if (s->scaled) {
-        const float *scale;
-        if ((rc = upload(s, L->scale, n, &scale))) return rc;
-        g.scale = scale;
+    const uint8_t *d_types;
+    if ((rc = upload(s, types.data(), types.size(), &d_types))) return rc;
+    const float *d_scale = nullptr;
+    if (s->scaled && (rc = upload(s, scale.data(), scale.size(), &d_scale))) return rc;
+
+    // The state, at rest; the error flag.
+    for (int k = 0; k < 2; ++k) {
+        if ((rc = zeros(s, e * s->n_device, &s->u[k]))) return rc;
+        if ((rc = zeros(s, e * L->state_count, &s->w[k]))) return rc;
+    }
+    if ((rc = zeros(s, e * 9 * L->layer_count, &s->layer_state))) return rc;
+    void *flag;
+    if ((rc = zeros(s, sizeof(unsigned int), &flag))) return rc;
+    s->d_error = static_cast<unsigned int *>(flag);
+
+    // The bulk sweep: tiles of kTX x kTY over the box, x from a 16-aligned start; chunks of planes
+    // enough for every multiprocessor several times over.
+    BulkArgs &bk = s->bulk;
+    bk.pitch = (uint32_t)s->pitch;
+    bk.ny = (uint32_t)ny;
+    bk.axial = L->weights[0];
+    bk.diagonal = s->wide ? L->weights[6] : 0.0f;
+    bk.centre = L->centre;
+    bk.total = L->total;
+    bk.error = s->d_error;
+    if (interior) {
+        bk.xa = (uint32_t)(x0 / 16 * 16);
+        bk.y0 = (uint32_t)y0, bk.z0 = (uint32_t)z0;
+        bk.x1 = (uint32_t)x1, bk.y1 = (uint32_t)y1, bk.z1 = (uint32_t)z1;
+        bk.tiles_x = (uint32_t)((x1 - bk.xa + kTX - 1) / kTX);
+        bk.tiles_y = (uint32_t)((y1 - y0 + kTY - 1) / kTY);
+        const uint64_t columns = (uint64_t)bk.tiles_x * bk.tiles_y, depth = z1 - z0;
+        uint64_t chunk = depth;
+        while (chunk > 8 && columns * ((depth + chunk - 1) / chunk) < (uint64_t)s->sms * 8) chunk = (chunk + 1) / 2;
+        bk.chunk = (uint32_t)std::max<uint64_t>(chunk, 1);
+        const uint64_t blocks = columns * ((depth + bk.chunk - 1) / bk.chunk);
+        if (blocks >= (1ull << 31)) return fail(s, FDTD_EINVAL, "the wave grid is too large for one launch");
+        s->bulk_blocks = (uint32_t)blocks;
+        const CUtensorMapDataType ft = s->precision == FDTD_FP64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+        for (int k = 0; k < 2; ++k) {
+            if ((rc = tensor_map(s, &s->map_b[k], s->u[k], ft, (uint32_t)e, kBX, kBY))) return rc;
+            if ((rc = tensor_map(s, &s->map_a[k], s->u[k], ft, (uint32_t)e, kTX, kTY))) return rc;
+        }
+        if ((rc = tensor_map(s, &s->map_t, const_cast<uint8_t *>(d_types), CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, kTX, kTY)))
+            return rc;
+        if ((rc = tensor_map(s, &s->map_s, s->scaled ? const_cast<float *>(d_scale) : s->u[0],
+                             CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, kTX, kTY)))
+            return rc;
+        if ((rc = set_up(s))) return rc;
     }
 
-    // Special rows with 32-bit indices.
+    // Special rows with 32-bit pitched indices.
     const uint64_t K = L->special_count;
     s->specials = K, s->links = L->link_count, s->states = L->state_count;
     g.specials = (uint32_t)K;
-    g.special_blocks = (uint32_t)((K + kBlock - 1) / kBlock);
     {
         std::vector<uint32_t> special(K), link_start(K + 1), state_start(K + 1);
-        for (uint64_t k = 0; k < K; ++k) special[k] = (uint32_t)L->special[k];
+        for (uint64_t k = 0; k < K; ++k) special[k] = pitched(s, (uint64_t)L->special[k]);
         for (uint64_t k = 0; k <= K; ++k) {
             link_start[k] = (uint32_t)L->link_start[k];
             state_start[k] = (uint32_t)L->state_start[k];
@@ -583,23 +502,21 @@ int build(fdtd_solver *s, const fdtd_layout *L) {
     const uint64_t Lc = L->layer_count;
     s->layers = Lc;
     g.layers = (uint32_t)Lc;
-    g.layer_blocks = (uint32_t)((Lc + kBlock - 1) / kBlock);
     if (Lc) {
         std::vector<uint32_t> cells(Lc);
-        for (uint64_t c = 0; c < Lc; ++c) cells[c] = (uint32_t)L->layer_cells[c];
+        for (uint64_t c = 0; c < Lc; ++c) cells[c] = pitched(s, (uint64_t)L->layer_cells[c]);
         const uint32_t *p;
         if ((rc = upload(s, cells.data(), Lc, &p))) return rc;
         g.layer_cells = p;
         const uint64_t len[3] = {nx + 1, ny + 1, nz + 1};
         for (int axis = 0; axis < 3; ++axis) {
-            if ((rc = upload(s, L->keep[2 * axis], len[axis], &fp))) return rc;
-            g.keep_centre[axis] = fp;
-            if ((rc = upload(s, L->keep[2 * axis + 1], len[axis], &fp))) return rc;
-            g.keep_face[axis] = fp;
-            if ((rc = upload(s, L->push[2 * axis], len[axis], &fp))) return rc;
-            g.push_centre[axis] = fp;
-            if ((rc = upload(s, L->push[2 * axis + 1], len[axis], &fp))) return rc;
-            g.push_face[axis] = fp;
+            std::vector<float4> packed(len[axis]);
+            for (uint64_t x = 0; x < len[axis]; ++x)
+                packed[x] = make_float4(L->keep[2 * axis][x], L->push[2 * axis][x], L->keep[2 * axis + 1][x],
+                                        L->push[2 * axis + 1][x]);
+            const float4 *p4;
+            if ((rc = upload(s, packed.data(), len[axis], &p4))) return rc;
+            g.layer_coef[axis] = p4;
         }
         if (s->scaled) {
             if ((rc = upload(s, L->layer_scale, Lc, &fp))) return rc;
@@ -611,11 +528,10 @@ int build(fdtd_solver *s, const fdtd_layout *L) {
     const uint64_t P = L->probe_count, pc = L->probe_start[P];
     s->probes = P;
     g.probes = (uint32_t)P;
-    g.probe_blocks = (uint32_t)((P + kBlock - 1) / kBlock);
     {
         std::vector<uint32_t> start(P + 1), cells(pc);
         for (uint64_t p = 0; p <= P; ++p) start[p] = (uint32_t)L->probe_start[p];
-        for (uint64_t k = 0; k < pc; ++k) cells[k] = (uint32_t)L->probe_cells[k];
+        for (uint64_t k = 0; k < pc; ++k) cells[k] = pitched(s, L->probe_cells[k]);
         const uint32_t *p32;
         if ((rc = upload(s, start.data(), P + 1, &p32))) return rc;
         g.probe_start = p32;
@@ -625,14 +541,6 @@ int build(fdtd_solver *s, const fdtd_layout *L) {
         if ((rc = upload(s, L->probe_weights, pc, &pd))) return rc;
         g.probe_weights = pd;
     }
-
-    // The state, at rest.
-    const size_t e = s->precision == FDTD_FP64 ? 8 : 4;
-    for (int k = 0; k < 2; ++k) {
-        if ((rc = zeros(s, e * n, &s->u[k]))) return rc;
-        if ((rc = zeros(s, e * L->state_count, &s->w[k]))) return rc;
-    }
-    if ((rc = zeros(s, e * 9 * Lc, &s->layer_state))) return rc;
     return FDTD_OK;
 }
 
@@ -721,6 +629,7 @@ int fdtd_create(const fdtd_layout *layout, int precision, int device, fdtd_solve
     fdtd_solver *s = new (std::nothrow) fdtd_solver();
     if (!s) return set_global(FDTD_ENOMEM, "out of host memory");
     s->device = device;
+    s->sms = prop.multiProcessorCount;
     s->precision = precision;
     cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
@@ -751,11 +660,13 @@ int fdtd_run_device(fdtd_solver *s, const float *d_signal, uint64_t steps, doubl
     return FDTD_OK;
 }
 
+void *fdtd_stream(const fdtd_solver *s) { return s ? static_cast<void *>(s->stream) : nullptr; }
+
 int fdtd_synchronize(fdtd_solver *s) {
     if (!s) return set_global(FDTD_EINVAL, "no solver");
     DeviceGuard guard(s->device);
     CUDA_TRY(s, cudaStreamSynchronize(s->stream));
-    return FDTD_OK;
+    return check_device_error(s);
 }
 
 int fdtd_run(fdtd_solver *s, const float *signal, uint64_t steps, double *out) {
@@ -804,6 +715,7 @@ int fdtd_run(fdtd_solver *s, const float *signal, uint64_t steps, double *out) {
     cudaFreeAsync(d_out, s->stream);
     if (rc != FDTD_OK) return rc;
     CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+    if ((rc = check_device_error(s)) != FDTD_OK) return rc;
     for (uint64_t k = 0; k < s->probes * steps; ++k) {
         if (!std::isfinite(out[k])) return fail(s, FDTD_ENONFINITE, "the wave solver's run did not stay finite");
     }
@@ -815,7 +727,7 @@ int fdtd_reset(fdtd_solver *s) {
     DeviceGuard guard(s->device);
     const size_t e = s->precision == FDTD_FP64 ? 8 : 4;
     for (int k = 0; k < 2; ++k) {
-        CUDA_TRY(s, cudaMemsetAsync(s->u[k], 0, e * s->n, s->stream));
+        CUDA_TRY(s, cudaMemsetAsync(s->u[k], 0, e * s->n_device, s->stream));
         if (s->states) CUDA_TRY(s, cudaMemsetAsync(s->w[k], 0, e * s->states, s->stream));
     }
     if (s->layers) CUDA_TRY(s, cudaMemsetAsync(s->layer_state, 0, e * 9 * s->layers, s->stream));
@@ -855,8 +767,15 @@ int fdtd_read_state(const fdtd_solver *cs, void *current, void *previous, void *
     DeviceGuard guard(s->device);
     const size_t e = s->precision == FDTD_FP64 ? 8 : 4;
     CUDA_TRY(s, cudaStreamSynchronize(s->stream));
-    if (current) CUDA_TRY(s, cudaMemcpy(current, s->u[1], e * s->n, cudaMemcpyDeviceToHost));
-    if (previous) CUDA_TRY(s, cudaMemcpy(previous, s->u[0], e * s->n, cudaMemcpyDeviceToHost));
+    // The levels are pitched on the device: their rows of nx cells are copied out one plane of
+    // rows at a time.
+    void *levels[2] = {current, previous};
+    const void *sources[2] = {s->u[1], s->u[0]};
+    for (int k = 0; k < 2; ++k) {
+        if (!levels[k]) continue;
+        CUDA_TRY(s, cudaMemcpy2D(levels[k], e * s->nx, sources[k], e * s->pitch, e * s->nx, s->ny * s->nz,
+                                 cudaMemcpyDeviceToHost));
+    }
     if (branch_current && s->states) CUDA_TRY(s, cudaMemcpy(branch_current, s->w[1], e * s->states, cudaMemcpyDeviceToHost));
     if (branch_previous && s->states) CUDA_TRY(s, cudaMemcpy(branch_previous, s->w[0], e * s->states, cudaMemcpyDeviceToHost));
     if (layer_state && s->layers) {

@@ -1,0 +1,657 @@
+"""Grid layouts of synthetic rooms, built on the host with the reference's rules.
+
+The reference lays out a grid in its ``WaveSolver`` constructor (cpp/include/acoustic_spaces/
+fdtd.hpp:360-690 of naelolaiz/acoustic-spaces) from a triangle mesh, by casting rays along every
+link near a face. For rooms whose walls are planes — convex polyhedra, boxes — the same layout
+follows from the planes directly, and this module builds it with NumPy for grids of tens of
+millions of cells, with the reference's rules for walls on cell faces and the 7-point stencil:
+
+- a link between two cell centres is cut when its segment leaves the room through a wall (the
+  face it crosses nearest the cell: for a convex room, the plane it exits through), not through
+  an open face (fdtd.hpp:452-497);
+- the air is what the source reaches (fdtd.hpp:499-519): the room's inside, and with an open face
+  every cell but the grid's edge;
+- air cells within ``layer`` cells of the grid's edge form the matched layer (fdtd.hpp:521-542),
+  with the coefficients of layer_coefficients (fdtd.hpp:2219-2238);
+- an air cell with a cut link, or one to the grid's edge, is a boundary row (fdtd.hpp:544-625):
+  links 1/3 where open, the cut links' boundary weight 1/(2 L) · 1/3 times each wall's admittance
+  beta and its branches' 1/(2 a), one set of branch states per material met, coefficients as
+  add_special (fdtd.hpp:3499-3517), with a speed field's s and r;
+- the source and the probes read the 4 x 4 x 4 cells round them with cubic weights
+  (reading_cells, fdtd.hpp:2361-2472, away from surfaces), the source's cells made special
+  (fdtd.hpp:627-638).
+
+Every array has the name and dtype of ``WaveSolver.layout()`` (fdtd.hpp:727-782), and the tests
+check that a room built here equals the reference's own layout of it, array for array.
+"""
+
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+#: fdtd.hpp:920: the stability margin each link weight is lowered by.
+MARGIN = 1.0 / 262144.0
+AXIAL = 1.0 / 3.0
+COURANT = 1.0 / math.sqrt(3.0)
+#: The boundary weight of one cut axial link of the 7-point stencil: g / (2 L).
+BOUNDARY = AXIAL / (2.0 * math.sqrt(AXIAL))
+#: The axial steps in the reference's order of directions (fdtd.hpp:924-925).
+AXIAL_STEPS = ((-1, 0, 0), (1, 0, 0), (0, -1, 0), (0, 1, 0), (0, 0, -1), (0, 0, 1))
+LAYER_CELLS = 8
+LAYER_DAMPING = 0.5
+
+
+def down(w: np.ndarray | float) -> np.ndarray:
+    """The largest float32 not above each double w (fdtd.hpp:2127-2131)."""
+    w = np.asarray(w, np.float64)
+    f = w.astype(np.float32)
+    over = f.astype(np.float64) > w
+    return np.where(over, np.nextafter(f, np.float32(0)), f).astype(np.float32)
+
+
+def lowered(w) -> np.ndarray:
+    """A link's weight as the update takes it (fdtd.hpp:2133-2135)."""
+    return down(np.asarray(w, np.float64) * (1.0 - MARGIN))
+
+
+@dataclass
+class Material:
+    """A wall's specific admittance: ``beta`` and mass-resistance-stiffness branches (m, r, q),
+    each as the solver takes it (mass over the time step, resistance, stiffness times the time
+    step; engine/impedance.py:199-211)."""
+
+    beta: float
+    branches: np.ndarray = field(default_factory=lambda: np.zeros((0, 3)))
+
+
+def resonant_branch(conductance: float, quality: float, frequency_hz: float, rate: float) -> np.ndarray:
+    """One resonant branch (m, r, q) of admittance ``conductance`` at resonance, quality
+    ``quality`` and resonance ``frequency_hz`` at ``rate`` steps a second: M = Q R / w0,
+    S = Q R w0, R = 1 / conductance (engine/impedance.py:199-211)."""
+    t = 1.0 / rate
+    r = 1.0 / conductance
+    w0 = 2.0 * math.pi * frequency_hz
+    return np.array([[quality * r / (w0 * t), r, quality * r * w0 * t]])
+
+
+@dataclass
+class Grid:
+    """``shape`` cells of ``cell`` metres, cell 0's corner at ``origin``, x fastest."""
+
+    origin: np.ndarray
+    cell: float
+    shape: tuple[int, int, int]
+
+    @property
+    def n(self) -> int:
+        return int(np.prod(self.shape))
+
+    def centres(self, axis: int) -> np.ndarray:
+        return self.origin[axis] + (np.arange(self.shape[axis]) + 0.5) * self.cell
+
+
+@dataclass
+class Room:
+    """A convex room: the cells with n_f . x < d_f for every plane f. ``materials[f]`` is plane
+    f's wall, or None for an open face (no wall: the air goes through)."""
+
+    normals: np.ndarray  # (F, 3), unit
+    offsets: np.ndarray  # (F,)
+    materials: list[Material | None]
+
+    @property
+    def open(self) -> bool:
+        return any(m is None for m in self.materials)
+
+
+@dataclass
+class Built:
+    """A layout and what was set up with it."""
+
+    layout: dict[str, np.ndarray]
+    grid: Grid
+    air_cells: int
+    boundary_cells: int
+    source_cells: int
+    rate: float
+
+
+def _signed(room: Room, grid: Grid, f: int, zs: slice | None = None) -> np.ndarray:
+    """n_f . centre - d_f of every cell (nz, ny, nx), or of the planes zs."""
+    nrm, d = room.normals[f], room.offsets[f]
+    x = nrm[0] * grid.centres(0)
+    y = nrm[1] * grid.centres(1)
+    z = nrm[2] * grid.centres(2)
+    if zs is not None:
+        z = z[zs]
+    return (z[:, None, None] + y[None, :, None]) + x[None, None, :] - d
+
+
+def _inside(room: Room, grid: Grid) -> tuple[np.ndarray, np.ndarray]:
+    """Each cell's centre inside the room, and within a cell's reach of it (every plane's
+    signed distance below one cell), as (nz, ny, nx) masks."""
+    nx, ny, nz = grid.shape
+    inside = np.ones((nz, ny, nx), bool)
+    near = np.ones((nz, ny, nx), bool)
+    for f in range(len(room.offsets)):
+        for z0 in range(0, nz, 64):
+            zs = slice(z0, min(nz, z0 + 64))
+            signed = _signed(room, grid, f, zs)
+            inside[zs] &= signed < 0.0
+            near[zs] &= signed < 1.01 * grid.cell
+    return inside, near
+
+
+def _first_wall(room: Room, grid: Grid, start: np.ndarray, end: np.ndarray) -> np.ndarray:
+    """For the links from cells ``start`` to cells ``end`` (flat indices), the wall each crosses
+    nearest its start, or -1 where it crosses none. The segment's part inside the (convex) room
+    is clipped by every plane: it enters through the plane of the largest entry parameter and
+    leaves through that of the smallest exit one; a cut is either where it is a wall (not an
+    open face), the entry first."""
+    nx, ny, _ = grid.shape
+
+    def centres(i):
+        return np.stack(
+            [grid.centres(0)[i % nx], grid.centres(1)[(i // nx) % ny], grid.centres(2)[i // (nx * ny)]], 1
+        )
+
+    ca, cb = centres(start), centres(end)
+    m = len(start)
+    t_in, t_out = np.zeros(m), np.ones(m)
+    enter, leave = np.full(m, -1, np.int64), np.full(m, -1, np.int64)
+    empty = np.zeros(m, bool)
+    for f in range(len(room.offsets)):
+        sa = ca @ room.normals[f] - room.offsets[f]
+        sb = cb @ room.normals[f] - room.offsets[f]
+        empty |= (sa >= 0.0) & (sb >= 0.0)
+        outgoing = (sa < 0.0) & (sb >= 0.0)
+        incoming = (sa >= 0.0) & (sb < 0.0)
+        denom = np.where(outgoing | incoming, sa - sb, 1.0)
+        t = sa / denom
+        later_in = incoming & (t > t_in)
+        t_in = np.where(later_in, t, t_in)
+        enter = np.where(later_in, f, enter)
+        sooner_out = outgoing & (t < t_out)
+        t_out = np.where(sooner_out, t, t_out)
+        leave = np.where(sooner_out, f, leave)
+    crosses = ~empty & (t_in < t_out)
+    walls = np.array([mat is not None for mat in room.materials] + [False])
+    enter_wall = crosses & (enter >= 0) & walls[enter]
+    leave_wall = crosses & (leave >= 0) & walls[leave]
+    return np.where(enter_wall, enter, np.where(leave_wall, leave, -1))
+
+
+def cubic_cells(grid: Grid, point) -> list[tuple[int, float]]:
+    """The 4 x 4 x 4 cells round ``point`` and their cubic weights, z then y then x
+    (reading_cells, fdtd.hpp:2361-2472, for a point away from every surface)."""
+    nx, ny, _ = grid.shape
+    q = (np.asarray(point, float) - grid.origin) / grid.cell - 0.5
+    start, weight = [], []
+    for a in range(3):
+        below = math.floor(q[a])
+        if not (q[a] >= 1.0 and q[a] < grid.shape[a] - 3.0 and below >= 1):
+            raise ValueError("the point is too near the grid's edge for its cubic stencil")
+        s = below - 1
+        x = q[a] - s
+        ws = []
+        for j in range(4):
+            w = 1.0
+            for m in range(4):
+                if m != j:
+                    w *= (x - m) / float(j - m)
+            ws.append(w)
+        start.append(s)
+        weight.append(ws)
+    out = []
+    for z in range(4):
+        for y in range(4):
+            for x in range(4):
+                w = weight[0][x] * weight[1][y] * weight[2][z]
+                if w != 0.0:
+                    out.append((int(start[0] + x + (start[1] + y) * nx + (start[2] + z) * nx * ny), w))
+    return out
+
+
+def _layer_tables(size: int, layer: int, damping: float, courant: float):
+    """keep and push of the centres and the faces along an axis (fdtd.hpp:2219-2238)."""
+
+    def damp(from_edge: float) -> float:
+        into = max(0.0, layer + 0.5 - from_edge) / layer
+        return damping * into * into
+
+    ck, cp, fk, fp = [], [], [], []
+    last = float(size - 1)
+    for x in range(size + 1):
+        c = float(x)
+        dc = damp(min(c, last - c))
+        df = damp(min(c - 0.5, last - c + 0.5))
+        ck.append((1.0 - dc) / (1.0 + dc))
+        cp.append(courant / (1.0 + dc))
+        fk.append((1.0 - df) / (1.0 + df))
+        fp.append(courant / (1.0 + df))
+    f32 = lambda v: np.array(v, np.float64).astype(np.float32)  # noqa: E731
+    return f32(ck), f32(cp), f32(fk), f32(fp)
+
+
+def cell_face_layout(
+    room: Room,
+    grid: Grid,
+    source,
+    probes,
+    *,
+    layer: int = 0,
+    layer_damping: float = 0.0,
+    edge_admittance: float = 1.0,
+    speed: float | None = None,
+    rate: float | None = None,
+) -> Built:
+    """The reference's layout of ``room`` on ``grid`` with walls on cell faces, the 7-point
+    stencil, a uniform speed ratio ``speed`` (None: the grid's), the source at ``source`` and
+    the probes at ``probes`` (each at least two cells from every wall and from the layer)."""
+    nx, ny, nz = grid.shape
+    n = grid.n
+    sy, sz = nx, nx * ny
+    inside, near = _inside(room, grid)
+    inside, near = inside.reshape(-1), near.reshape(-1)
+    # The grid's edge, and each cell's depth into it.
+    ix = np.arange(nx)
+    dx = np.minimum(ix, nx - 1 - ix)
+    dy = np.minimum(np.arange(ny), ny - 1 - np.arange(ny))
+    dz = np.minimum(np.arange(nz), nz - 1 - np.arange(nz))
+    depth = np.minimum(np.minimum(dz[:, None, None], dy[None, :, None]), dx[None, None, :]).reshape(-1)
+    edge = depth == 0
+
+    # Air: the inside, and with an open face all but the edge (fdtd.hpp:499-519).
+    air = (~edge) if room.open else (inside & ~edge)
+    types = np.where(air, 1, 0).astype(np.uint8)
+    layer_cells = np.zeros(0, np.int64)
+    if layer > 0:
+        in_layer = air & (depth <= layer)
+        types[in_layer] = 3
+        layer_cells = np.flatnonzero(in_layer).astype(np.int64)
+
+    # Cut links: between inside and outside cells, leaving through a wall (not the open face).
+    offsets = [s[0] + s[1] * sy + s[2] * sz for s in AXIAL_STEPS]
+    blocked = np.zeros((6, n), bool)
+    material = np.full((6, n), -1, np.int64)
+    candidates = np.flatnonzero(air & (types == 1))
+    for k, off in enumerate(offsets):
+        j = candidates + off
+        edge_link = edge[j]
+        blocked[k, candidates[edge_link]] = True
+        material[k, candidates[edge_link]] = -2  # the grid's edge
+        # Links that may meet a wall: an end inside and one out, or both within a cell's reach
+        # of the room (a link can clip an edge or corner of it).
+        maybe = ~edge_link & near[candidates] & near[j] & ~(inside[candidates] & inside[j])
+        if not np.any(maybe):
+            continue
+        c, jj = candidates[maybe], j[maybe]
+        face = _first_wall(room, grid, c, jj)
+        walled = face >= 0
+        blocked[k, c[walled]] = True
+        material[k, c[walled]] = face[walled]
+    boundary = np.flatnonzero(blocked.any(axis=0) & (types == 1))
+    # The matched layer's air must meet no face (fdtd.hpp:521-528).
+    for off in offsets:
+        j = layer_cells + off
+        maybe = near[layer_cells] & near[j] & ~edge[j]
+        if np.any(_first_wall(room, grid, layer_cells[maybe], j[maybe]) >= 0):
+            raise ValueError("the model reaches into the matched layer")
+
+    # Materials: beta and branches.
+    mats = room.materials
+    betas = np.array([0.0 if m is None else m.beta for m in mats])
+    branch_rows, branch_owner = [], []
+    for f, m in enumerate(mats):
+        if m is None:
+            continue
+        for row in np.asarray(m.branches, float).reshape(-1, 3):
+            branch_rows.append(row)
+            branch_owner.append(f)
+    branch_rows = np.array(branch_rows).reshape(-1, 3)
+    branch_owner = np.array(branch_owner, np.int64)
+    a_of = branch_rows[:, 0] + 0.5 * branch_rows[:, 1] + 0.5 * branch_rows[:, 2]
+    if len(a_of) and not np.all((branch_rows >= 0) & (a_of[:, None] > 0)):
+        raise ValueError("a branch needs mass, resistance and stiffness >= 0")
+    branch_now = (2.0 * branch_rows[:, 0] / a_of).astype(np.float32)
+    branch_before = ((2.0 * branch_rows[:, 0] + branch_rows[:, 2]) / a_of).astype(np.float32)
+    branch_gain = (0.5 / a_of).astype(np.float32)
+
+    s = 1.0 if speed is None else float(np.float32(speed * speed))
+    r = math.sqrt(s)
+
+    # Boundary rows (fdtd.hpp:560-623), vectorised over the rows, in the reference's order of
+    # directions and materials.
+    B = len(boundary)
+    blk = blocked[:, boundary]  # (6, B)
+    mat = material[:, boundary]
+    open_link = ~blk
+    beta_sum = np.zeros(B)
+    for k in range(6):
+        term = np.where(mat[k] == -2, BOUNDARY * edge_admittance, BOUNDARY * betas[np.maximum(mat[k], 0)])
+        beta_sum = beta_sum + np.where(blk[k], term, 0.0)
+    # The materials met, in order of first meeting, and the weight of each one's cut links.
+    kinds = np.full((6, B), -1, np.int64)
+    kind_weight = np.zeros((6, B))
+    count = np.zeros(B, np.int64)
+    for k in range(6):
+        m = np.where(blk[k] & (mat[k] >= 0), mat[k], -1)
+        seen = np.zeros(B, bool)
+        for slot in range(6):
+            hit = (kinds[slot] == m) & (m >= 0)
+            kind_weight[slot] = np.where(hit, kind_weight[slot] + BOUNDARY, kind_weight[slot])
+            seen |= hit
+        new = (m >= 0) & ~seen
+        rows = np.flatnonzero(new)
+        kinds[count[rows], rows] = m[rows]
+        kind_weight[count[rows], rows] = BOUNDARY
+        count[rows] += 1
+    g = beta_sum.copy()
+    state_rows, state_branch, state_weight = [], [], []
+    by_material = {f: np.flatnonzero(branch_owner == f) for f in range(len(mats))}
+    for slot in range(6):
+        has = kinds[slot] >= 0
+        if not np.any(has):
+            break
+        for f in np.unique(kinds[slot][has]):
+            rows = np.flatnonzero(kinds[slot] == f)
+            for j in by_material[int(f)]:
+                g[rows] = g[rows] + kind_weight[slot, rows] * (0.5 / a_of[j])
+                state_rows.append(np.repeat(rows, 1))
+                state_branch.append(np.full(len(rows), j, np.int32))
+                state_weight.append((r * kind_weight[slot, rows]).astype(np.float32))
+    # Each row's states in slot order then branch order: sort by (row, insertion order).
+    if state_rows:
+        rows_all = np.concatenate(state_rows)
+        order = np.argsort(rows_all, kind="stable")
+        rows_all = rows_all[order]
+        st_branch = np.concatenate(state_branch)[order]
+        st_weight = np.concatenate(state_weight)[order]
+    else:
+        rows_all = np.zeros(0, np.int64)
+        st_branch = np.zeros(0, np.int32)
+        st_weight = np.zeros(0, np.float32)
+    states_per_row = np.bincount(rows_all, minlength=B)
+
+    link_w = lowered(s * AXIAL)
+    total = np.zeros(B)
+    for k in range(6):
+        total = total + np.where(open_link[k], AXIAL, 0.0)
+    coef_a = (2.0 - s * total * (1.0 - MARGIN)).astype(np.float32)
+    coef_b = (1.0 - r * g).astype(np.float32)
+    coef_inv = (1.0 / (1.0 + r * g)).astype(np.float32)
+    links_per_row = open_link.sum(axis=0)
+    link_direction = np.tile(np.arange(6, dtype=np.uint8), (B, 1))[open_link.T]
+    types[boundary] = 2
+
+    special = list(boundary.astype(np.int64))
+    link_start = np.concatenate([[0], np.cumsum(links_per_row)]).astype(np.uint64)
+    state_start = np.concatenate([[0], np.cumsum(states_per_row)]).astype(np.uint64)
+    source_values = np.zeros(B, np.float32)
+
+    # The source's cells (fdtd.hpp:627-638): made special with the stencil's own weights, each
+    # source term summed in float as the reference's source_[k] += float(s w).
+    extra_link_dir: list[np.ndarray] = []
+    accumulated: dict[int, np.float32] = {}
+    made: dict[int, int] = {}
+    for ci, w in cubic_cells(grid, source):
+        t = types[ci]
+        if t == 3:
+            raise ValueError("the source is in the matched layer")
+        if t == 0:
+            raise ValueError("the source sees no cell of the wave grid")
+        if t == 2:
+            k = made.get(ci)
+            if k is None:
+                k = int(np.searchsorted(boundary, ci))
+                if k >= B or boundary[k] != ci:
+                    raise ValueError("a source cell is special but not a boundary row")
+        else:
+            types[ci] = 2
+            k = len(special)
+            special.append(ci)
+            made[ci] = k
+            extra_link_dir.append(np.arange(6, dtype=np.uint8))
+        accumulated[k] = np.float32(accumulated.get(k, np.float32(0.0)) + np.float32(s * w))
+    E = len(made)
+    extra_source = np.zeros(E, np.float32)
+    for k, value in accumulated.items():
+        if k < B:
+            source_values[k] = value
+        else:
+            extra_source[k - B] = value
+    exact_total = 0.0
+    for _ in range(6):
+        exact_total += AXIAL
+    extra_coef_a = np.full(E, np.float32(2.0 - s * exact_total * (1.0 - MARGIN)), np.float32)
+
+    layout: dict[str, np.ndarray] = {}
+    weights = np.full(6, lowered(AXIAL), np.float32)
+    tot = 0.0
+    for w in weights:
+        tot += float(w)
+    layout["shape"] = np.array(grid.shape, np.uint64)
+    layout["stencil"] = np.array([7], np.uint64)
+    layout["weights"] = weights
+    layout["centre"] = np.array([2.0 - tot], np.float32)
+    layout["total"] = np.array([tot], np.float32)
+    layout["scaled"] = np.array([0 if speed is None else 1], np.uint64)
+    layout["scale"] = np.full(n, np.float32(s), np.float32) if speed is not None else np.zeros(0, np.float32)
+    layout["layer_scale"] = (
+        np.full(len(layer_cells), np.float32(s), np.float32) if speed is not None else np.zeros(0, np.float32)
+    )
+    layout["types"] = types
+    layout["special"] = np.array(special, np.int64)
+    layout["link_start"] = np.concatenate([link_start, link_start[-1] + 6 * np.arange(1, E + 1, dtype=np.uint64)])
+    layout["link_direction"] = np.concatenate([link_direction] + extra_link_dir).astype(np.uint8)
+    layout["link_weight"] = np.full(len(layout["link_direction"]), link_w, np.float32)
+    layout["coef_a"] = np.concatenate([coef_a, extra_coef_a])
+    layout["coef_b"] = np.concatenate([coef_b, np.ones(E, np.float32)])
+    layout["coef_inv"] = np.concatenate([coef_inv, np.ones(E, np.float32)])
+    layout["source"] = np.concatenate([source_values, extra_source])
+    layout["state_start"] = np.concatenate([state_start, np.full(E, state_start[-1], np.uint64)])
+    layout["state_branch"] = st_branch.astype(np.int32)
+    layout["state_weight"] = st_weight.astype(np.float32)
+    layout["branch_now"] = branch_now
+    layout["branch_before"] = branch_before
+    layout["branch_gain"] = branch_gain
+    layout["layer_cells"] = layer_cells
+    courant = math.sqrt(float(weights[0]))
+    for a, name in enumerate("xyz"):
+        if len(layer_cells):
+            ck, cp, fk, fp = _layer_tables(grid.shape[a], layer, layer_damping, courant)
+        else:
+            ck = cp = fk = fp = np.zeros(0, np.float32)
+        layout[f"keep_{name}"], layout[f"push_{name}"] = ck, cp
+        layout[f"keep_face_{name}"], layout[f"push_face_{name}"] = fk, fp
+    starts, cells, pweights = [0], [], []
+    for p in np.asarray(probes, float).reshape(-1, 3):
+        if np.linalg.norm(p - np.asarray(source, float)) < (3.0 - 1e-9) * grid.cell:
+            # the reference reads such a probe from the eight cells round it (fdtd.hpp:645-646)
+            raise ValueError("a probe lies within three cells of the source")
+        for ci, w in cubic_cells(grid, p):
+            if types[ci] not in (1, 2):
+                raise ValueError("a probe reads a cell outside the air")
+            cells.append(ci)
+            pweights.append(w)
+        starts.append(len(cells))
+    layout["probe_start"] = np.array(starts, np.uint64)
+    layout["probe_cells"] = np.array(cells, np.uint64)
+    layout["probe_weights"] = np.array(pweights, np.float64)
+    layout["flow_mask"] = np.zeros(0, np.uint8)
+    air_cells = int(np.count_nonzero(types))
+    return Built(layout, grid, air_cells, B, E, rate or 0.0)
+
+
+
+# ---- seeded synthetic rooms ------------------------------------------------------------------
+
+OFFSET = np.array([0.0137, 0.0219, 0.0291])  # cell centres off round numbers
+
+
+def convex_room(
+    rng: np.random.Generator,
+    box,
+    *,
+    faces: int,
+    margin: float,
+    open_face: int | None,
+    material,
+) -> Room:
+    """A seeded convex room with ``faces`` planes inside the box [0, box] shrunk by ``margin``
+    on every side: the shrunk box's six faces (-x, +x, -y, +y, -z, +z) and ``faces - 6`` planes
+    tangent to the ellipsoid inscribed in it at random points, each cutting off part of the box.
+    ``material(rng)`` gives each wall's Material; plane ``open_face`` (an index of the six box
+    faces) is open."""
+    box = np.asarray(box, float)
+    low, high = np.full(3, margin), box - margin
+    normals, offsets = [], []
+    for a in range(3):
+        for sign in (-1.0, 1.0):
+            nrm = np.zeros(3)
+            nrm[a] = sign
+            normals.append(nrm)
+            offsets.append(sign * (high[a] if sign > 0 else low[a]))
+    centre, semi = 0.5 * (low + high), 0.5 * (high - low)
+    for _ in range(max(0, faces - 6)):
+        u = rng.normal(size=3)
+        u /= np.linalg.norm(u)
+        point = centre + semi * u
+        nrm = u / semi
+        nrm /= np.linalg.norm(nrm)
+        normals.append(nrm)
+        offsets.append(float(nrm @ point))
+    mats = [material(rng) for _ in normals]
+    if open_face is not None:
+        mats[open_face] = None
+    return Room(np.array(normals), np.array(offsets), mats)
+
+
+def inside_points(
+    rng: np.random.Generator, room: Room, box, count: int, clearance: float, apart: float = 0.0
+) -> np.ndarray:
+    """``count`` seeded points inside ``room`` at least ``clearance`` from each of its planes,
+    the others at least ``apart`` from the first (a source and its receivers)."""
+    box = np.asarray(box, float)
+    out: list[np.ndarray] = []
+    while len(out) < count:
+        p = rng.uniform(0.0, box)
+        if not np.all(room.normals @ p - room.offsets < -clearance):
+            continue
+        if out and np.linalg.norm(p - out[0]) < apart:
+            continue
+        out.append(p)
+    return np.array(out)
+
+
+def room_mesh(room: Room) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+    """The walls of ``room`` as triangles: vertices (V, 3), faces (T, 3) and each triangle's plane
+    (the open face has none). For handing the same room to the reference's mesh-based solver."""
+    from scipy.spatial import HalfspaceIntersection
+
+    halfspaces = np.column_stack([room.normals, -room.offsets])
+    interior = None
+    # a point well inside: the centre of the box the first six planes bound
+    lo = np.array([room.offsets[1 - 1] * -1, -room.offsets[2], -room.offsets[4]])
+    hi = np.array([room.offsets[1], room.offsets[3], room.offsets[5]])
+    interior = 0.5 * (lo + hi)
+    corners = HalfspaceIntersection(halfspaces, interior).intersections
+    verts, tris, owner = [], [], []
+    for f in range(len(room.offsets)):
+        if room.materials[f] is None:
+            continue
+        on = np.abs(corners @ room.normals[f] - room.offsets[f]) < 1e-9
+        pts = corners[on]
+        if len(pts) < 3:
+            continue
+        # distinct points, ordered round their centroid in the plane
+        pts = np.unique(np.round(pts, 12), axis=0)
+        c = pts.mean(axis=0)
+        nrm = room.normals[f]
+        e1 = pts[0] - c
+        e1 /= np.linalg.norm(e1)
+        e2 = np.cross(nrm, e1)
+        angle = np.arctan2((pts - c) @ e2, (pts - c) @ e1)
+        pts = pts[np.argsort(angle)]
+        base = len(verts)
+        verts.extend(pts)
+        for k in range(1, len(pts) - 1):
+            tris.append((base, base + k, base + k + 1))
+            owner.append(f)
+    return np.array(verts), np.array(tris, np.int64), np.array(owner, np.int64)
+
+
+def gaussian_drive(rate: float, steps: int, sigma_s: float = 0.5e-3) -> np.ndarray:
+    """A Gaussian pulse of ``sigma_s`` seconds sampled at ``rate``, centred at 6 sigma, peak 1."""
+    t = (np.arange(steps) - 6.0 * sigma_s * rate) / (sigma_s * rate)
+    return np.exp(-0.5 * t * t).astype(np.float32)
+
+
+@dataclass
+class Workload:
+    """A seeded room ready to step: its room, grid, layout, drive and description."""
+
+    name: str
+    room: Room
+    built: Built
+    source: np.ndarray
+    receivers: np.ndarray
+    signal: np.ndarray
+    description: dict
+
+
+def polyhedral_room(
+    seed: int = 0,
+    *,
+    box=(20.0, 15.0, 10.0),
+    cell: float = 0.04,
+    layer: int = LAYER_CELLS,
+    receivers: int = 16,
+    steps: int = 12000,
+    speed_of_sound: float = 343.0,
+) -> Workload:
+    """A seeded convex polyhedral room of 12 to 20 planar faces inscribed in ``box`` metres, open
+    through its +x face into the air round it, on a grid of ``cell`` metres spanning the box with
+    a ``layer``-cell matched layer inside its edge (damping 0.5). Each wall has a 2-pole
+    admittance: a real beta in [0.02, 0.1] and one passive resonant branch of seeded resonance
+    (30 to 300 Hz), quality (0.5 to 10) and conductance (0.005 to 0.5). One source and
+    ``receivers`` receivers at seeded points at least 0.5 m from every plane; the drive a 0.5 ms
+    Gaussian pulse. Walls on cell faces, 7-point stencil, at its Courant limit."""
+    rng = np.random.default_rng(seed)
+    rate = speed_of_sound / (COURANT * cell)
+    faces = int(rng.integers(12, 21))
+
+    def material(r):
+        return Material(
+            float(r.uniform(0.02, 0.1)),
+            resonant_branch(r.uniform(0.005, 0.5), r.uniform(0.5, 10.0), r.uniform(30.0, 300.0), rate),
+        )
+
+    margin = cell * (layer + 3)
+    room = convex_room(rng, box, faces=faces, margin=margin, open_face=1, material=material)
+    points = inside_points(rng, room, box, 1 + receivers, max(0.5, 3 * cell), apart=max(0.5, 4 * cell))
+    grid = Grid(-OFFSET * cell, cell, tuple(int(round(b / cell)) for b in box))
+    built = cell_face_layout(room, grid, points[0], points[1:], layer=layer, layer_damping=LAYER_DAMPING, rate=rate)
+    lay = built.layout
+    description = {
+        "room": f"convex polyhedron, {faces} planes in {box[0]:g}x{box[1]:g}x{box[2]:g} m, +x face open",
+        "grid": "x".join(str(v) for v in grid.shape),
+        "cell_m": cell,
+        "cells": grid.n,
+        "air_cells": built.air_cells,
+        "interior_cells": int(np.count_nonzero(lay["types"] == 1)),
+        "special_rows": len(lay["special"]),
+        "links": len(lay["link_direction"]),
+        "branch_states": len(lay["state_branch"]),
+        "layer_cells": len(lay["layer_cells"]),
+        "probes": receivers,
+        "steps": steps,
+        "rate_hz": rate,
+        "walls": "cell faces, 2-pole admittance per wall",
+        "stencil": 7,
+        "seed": seed,
+    }
+    return Workload("polyhedral_room", room, built, points[0], points[1:], gaussian_drive(rate, steps), description)

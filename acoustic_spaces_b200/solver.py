@@ -152,6 +152,11 @@ class B200WaveSolver:
         if status != _abi.FDTD_OK:
             _raise(self._lib, status, self._handle)
 
+    @property
+    def stream(self) -> int:
+        """The address of the solver's CUDA stream (for events and ordering)."""
+        return int(self._lib.fdtd_stream(self._handle) or 0)
+
     def synchronize(self) -> None:
         status = self._lib.fdtd_synchronize(self._handle)
         if status != _abi.FDTD_OK:

@@ -1,0 +1,395 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 wave stepper: FDTD Gcell-updates/s on the polyhedral-room workload.
+
+Workload (the FP32 forward configuration with walls and a matched layer): a seeded convex
+polyhedral room of 12 to 20 planar faces inscribed in 20 x 15 x 10 m, open through one face into
+the air round it, on a 500 x 375 x 250 grid of 4 cm cells (46.9M cells) with an 8-cell matched
+layer inside the grid's edge; every wall a 2-pole admittance (beta and one resonant branch);
+1 source, 16 receivers; built on the host by acoustic_spaces_b200.layouts with the reference's
+rules for walls on cell faces (the tests check it against the reference's own layouts).
+
+A step is one time step of the whole grid (WaveSolver::run's loop body, fdtd.hpp:838-886): probe
+records, interior air, special rows with their branch states, and the matched layer.
+
+``python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]`` prints one JSON
+line. ``value`` is air cells x steps / device time of K steps with every input resident in HBM
+(CUDA events on the solver's own stream; max over ranks); ``e2e`` is the same metric through the
+public API (``B200WaveSolver.run`` on a host drive, its probe series back on the host);
+``roofline`` relates the step kernel's algorithmic bytes per launch to the measured HBM peak;
+``cpu_baseline`` is the reference's own CPU solver (oracle/_ref, the reference's unmodified C++)
+timed on the host's cores on a bounded sample of the same workload. Under torchrun each rank steps
+its own replica of the room (a single grid does not shard without a halo exchange: replicas only).
+``--impl reference`` times the reference's CPU solver alone and prints its line.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "FDTD Gcell-updates/s (+HBM roofline %) at stated IR error vs FP64; adjoint/fwd"
+UNIT = "Gcell-updates/s"
+
+# Algorithmic bytes of one step per unit of each kind (FP32): what a step must move at least.
+BYTES_INTERIOR = 12  # read p, read p-, write p+
+BYTES_SPECIAL = 40  # read p, read/write p-, coef_a/b/inv/source, its index and two table starts
+BYTES_LINK = 5  # direction and weight
+BYTES_STATE = 28  # read/write w-, read w, its four coefficients
+BYTES_LAYER = 84  # read p, write p+, read/write nine state values, its index
+
+
+def algorithmic_bytes(d: dict) -> int:
+    return (
+        BYTES_INTERIOR * d["interior_cells"]
+        + BYTES_SPECIAL * d["special_rows"]
+        + BYTES_LINK * d["links"]
+        + BYTES_STATE * d["branch_states"]
+        + BYTES_LAYER * d["layer_cells"]
+    )
+
+
+def measured_peaks() -> tuple[float, str]:
+    path = ROOT / "MEASURED_PEAKS.json"
+    if path.exists():
+        return float(json.loads(path.read_text())["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    return 6650.0, "fallback 6.65 TB/s"
+
+
+class Clocks:
+    """nvidia-smi samples of SM clock and throttle reasons while it runs."""
+
+    QUERY = (
+        "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+        "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+        "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+    )
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL,
+                text=True,
+            )
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, max_sm, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                max_sm = float(parts[2])
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower().startswith("active"):
+                    reasons.add(name)
+        return {
+            "sm_mhz": statistics.median(sm) if sm else None,
+            "sm_max_mhz": max_sm,
+            "reasons": sorted(reasons),
+            "samples": len(sm),
+        }
+
+
+def build_workload(args):
+    from acoustic_spaces_b200 import layouts
+
+    return layouts.polyhedral_room(args.seed, cell=args.cell, steps=max(args.steps, 1))
+
+
+def cpu_reference_rate(workload, sample_steps: int) -> dict:
+    """The reference's own CPU solver (its unmodified C++, oracle/_ref) on the same room, timed
+    over ``sample_steps`` steps with every host thread; else the oracle's C port, one thread."""
+    from acoustic_spaces_b200 import layouts
+    from oracle import oracle
+
+    threads = os.cpu_count() or 1
+    native = oracle.reference_native()
+    air = workload.built.air_cells
+    signal = workload.signal[:sample_steps]
+    if native is not None:
+        room, grid = workload.room, workload.built.grid
+        vertices, faces, owner = layouts.room_mesh(room)
+        beta = np.array([0.0 if m is None else m.beta for m in room.materials])
+        rows, owners = [np.zeros((0, 3))], [np.zeros(0, np.int64)]
+        for k, m in enumerate(room.materials):
+            if m is not None:
+                rows.append(m.branches)
+                owners.append(np.full(len(m.branches), k, np.int64))
+        t0 = time.perf_counter()
+        solver = native.WaveSolver(
+            native.Bvh(vertices, faces), owner, beta, np.ascontiguousarray(np.vstack(rows)),
+            np.concatenate(owners), grid.origin, grid.cell, *grid.shape, workload.source,
+            workload.receivers, layer=8, layer_damping=0.5, threads=threads,
+        )  # fmt: skip
+        setup = time.perf_counter() - t0
+        solver.run(signal[:2])  # threads spun up once
+        t0 = time.perf_counter()
+        solver.run(signal)
+        seconds = time.perf_counter() - t0
+        kind, cores, ref_air = "reference", int(solver.threads), int(solver.air_cells)
+        if ref_air != air:
+            raise RuntimeError(f"the reference lays the room out with {ref_air} air cells, the builder {air}")
+        extra = {"setup_s": round(setup, 2)}
+    else:
+        ported = oracle.OracleSolver(workload.built.layout)
+        ported.run(signal[:2])
+        t0 = time.perf_counter()
+        ported.run(signal)
+        seconds = time.perf_counter() - t0
+        kind, cores, extra = "port", 1, {}
+    value = air * len(signal) / seconds / 1e9
+    return {
+        "value": round(value, 4),
+        "unit": UNIT,
+        "cores": cores,
+        "kind": kind,
+        "sample": f"{len(signal)} steps of the full {workload.description['grid']} grid "
+        f"({air} air cells), after 2 warm-up steps",
+        **extra,
+    }
+
+
+def run_reference(args, rank: int, world: int) -> None:
+    if rank != 0:
+        return
+    workload = build_workload(args)
+    steps = max(1, min(args.steps, args.reference_steps))
+    times = []
+    base = None
+    for _ in range(max(1, args.reference_repeats)):
+        base = cpu_reference_rate(workload, steps)
+        times.append(base["value"])
+    value = statistics.median(times)
+    base["value"] = round(value, 4)
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": round(value, 4),
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": steps,
+        "warmup": 2,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": "polyhedral_room", **workload.description, "sample_steps": steps},
+        "cpu_baseline": base,
+        "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    parser = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    parser.add_argument("--gpus", type=int, default=1)
+    parser.add_argument("--steps", type=int, default=2000)
+    parser.add_argument("--warmup", type=int, default=20)
+    parser.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    parser.add_argument("--seed", type=int, default=0)
+    parser.add_argument("--cell", type=float, default=0.04, help="cell size in metres (0.04: the full workload)")
+    parser.add_argument("--cpu-steps", type=int, default=10, help="steps of the CPU-baseline sample")
+    parser.add_argument("--reference-steps", type=int, default=10)
+    parser.add_argument("--reference-repeats", type=int, default=3)
+    parser.add_argument("--no-cpu-baseline", action="store_true")
+    parser.add_argument("--no-e2e", action="store_true")
+    args = parser.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    from acoustic_spaces_b200 import B200WaveSolver
+
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device (the B200 stepper has no CPU path)")
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    workload = build_workload(args)
+    desc = workload.description
+    solver = B200WaveSolver(workload.built.layout, device=local)
+    air = solver.air_cells
+    probes = solver.probes
+    steps, warmup = args.steps, args.warmup
+    if warmup < 3:
+        raise SystemExit("at least 3 warm-up steps")
+
+    signal = workload.signal
+    sig_dev = torch.from_numpy(np.ascontiguousarray(np.resize(signal, steps + warmup))).to(f"cuda:{local}")
+    out_dev = torch.zeros((probes, steps + warmup), dtype=torch.float64, device=f"cuda:{local}")
+    stream = torch.cuda.ExternalStream(solver.stream, device=f"cuda:{local}")
+    # Warm-up.
+    solver.run_device(sig_dev.data_ptr(), warmup, out_dev.data_ptr(), steps + warmup)
+    solver.synchronize()
+
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clocks:
+        barrier()
+        torch.cuda.synchronize()
+        solver.synchronize()
+        with torch.cuda.stream(stream):
+            start.record(stream)
+        solver.run_device(sig_dev.data_ptr() + 4 * warmup, steps, out_dev.data_ptr() + 8 * warmup, steps + warmup)
+        with torch.cuda.stream(stream):
+            end.record(stream)
+        solver.synchronize()
+        torch.cuda.synchronize()
+        barrier()
+    ms = start.elapsed_time(end)
+    if world > 1:
+        t = torch.tensor([ms], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * air * steps / (ms / 1e3) / 1e9
+
+    finite = bool(torch.isfinite(out_dev).all().item())
+
+    # End to end through the public API: a host drive in, the probes' series out.
+    e2e = None
+    if not args.no_e2e:
+        host_signal = np.ascontiguousarray(np.resize(signal, steps), dtype=np.float32)
+        solver.reset()
+        solver.run(host_signal[:warmup])
+        solver.reset()
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        recorded = solver.run(host_signal)
+        seconds = time.perf_counter() - t0
+        if world > 1:
+            t = torch.tensor([seconds], device=f"cuda:{local}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            seconds = float(t.item())
+        finite = finite and bool(np.isfinite(recorded).all())
+        e2e = {
+            "value": round(world * air * steps / seconds / 1e9, 4),
+            "unit": UNIT,
+            "h2d_bytes_per_step": 4,
+            "d2h_bytes_per_step": 8 * probes,
+            "api": "B200WaveSolver.run(host float32 drive) -> host float64 (probes, steps)",
+        }
+
+    bytes_per_step = algorithmic_bytes(desc)
+    peak, peak_source = measured_peaks()
+    achieved = bytes_per_step / (ms / 1e3 / steps) / 1e9
+    traffic = None
+    traffic_file = ROOT / "profiles" / "step_kernel_traffic.json"
+    if traffic_file.exists():
+        entry = json.loads(traffic_file.read_text())
+        cells = entry.get("cells_per_launch")
+        if cells:
+            traffic = int(entry["dram_bytes_per_launch"] * air / cells)
+
+    line = None
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            try:
+                cpu = cpu_reference_rate(workload, args.cpu_steps)
+            except Exception as error:  # the baseline is reported, not required
+                cpu = {"value": None, "unit": UNIT, "error": str(error)[:200]}
+        line = {
+            "metric": METRIC,
+            "value": round(value, 4),
+            "unit": UNIT,
+            "n_gpus": world,
+            "steps": steps,
+            "warmup": warmup,
+            "ms_per_step": round(ms / steps, 5),
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic",
+            "config": {
+                "workload": "polyhedral_room",
+                **desc,
+                "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                "l2": "inputs larger than L2 (two pressure levels alone are "
+                f"{2 * 4 * desc['cells'] / 1e6:.0f} MB vs 126 MB L2), no flush",
+                "precision": "FP32, bit-exact with the reference (no FMA, subnormals flushed)",
+            },
+            "e2e": e2e,
+            "gpu_launches": steps,
+            "roofline": {
+                "bound": "hbm",
+                "kernel": "step_kernel<float, 7-point> (one launch per step: interior, special rows, layer, probes)",
+                "achieved": round(achieved, 1),
+                "peak": peak,
+                "unit": "GB/s",
+                "frac": round(achieved / peak, 4),
+                "traffic": traffic,
+                "algorithmic_bytes_per_launch": bytes_per_step,
+                "peak_source": peak_source,
+                "bulk_12B_per_air_cell_frac": round(12 * air / (ms / 1e3 / steps) / 1e9 / peak, 4),
+            },
+            "cpu_baseline": cpu,
+            "clocks": clocks.summary(),
+            "finite": finite,
+        }
+        print(json.dumps(line), flush=True)
+    del solver
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

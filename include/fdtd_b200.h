@@ -141,6 +141,10 @@ int fdtd_run_device(fdtd_solver *solver, const float *d_signal, uint64_t steps, 
                     uint64_t out_stride);
 int fdtd_synchronize(fdtd_solver *solver);
 
+/* The handle's CUDA stream (a cudaStream_t), for callers that order their own work or events
+   with fdtd_run_device; NULL for a NULL handle. */
+void *fdtd_stream(const fdtd_solver *solver);
+
 /* Replaces WaveSolver::reset (fdtd.hpp:906-915): silences the grid. */
 int fdtd_reset(fdtd_solver *solver);
 
