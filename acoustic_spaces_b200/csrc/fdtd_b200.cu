@@ -52,11 +52,15 @@ struct fdtd_solver {
     int sms = 148;  // multiprocessors of the device
     int precision = FDTD_FP32;
     bool wide = false, scaled = false;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;  // the handle's stream: bulk sweep and matched layer
+    cudaStream_t side = nullptr;    // special rows and probes, beside them within each step
+    cudaEvent_t joined[2] = {nullptr, nullptr};  // each stream's end of a step
     std::string error;
     Tables tables{};
     BulkArgs bulk{};
-    uint32_t bulk_blocks = 0;
+    uint32_t bulk_blocks = 0;  // the persistent grid: resident blocks, at most one per tile
+    uint32_t bulk_tiles = 0;
+    int bulk_per_sm = 0;      // resident bulk blocks per multiprocessor
     uint64_t nx = 0, ny = 0, nz = 0, n = 0, pitch = 0, n_device = 0;
     uint64_t air = 0, interior = 0, links = 0, states = 0, layers = 0, probes = 0, specials = 0;
     uint64_t steps_done = 0;
@@ -66,7 +70,11 @@ struct fdtd_solver {
     // for the branch velocities w.
     void *u[2] = {nullptr, nullptr};
     void *w[2] = {nullptr, nullptr};
-    void *layer_state = nullptr;
+    void *layer_parts = nullptr;  // 3 arrays of the layer's cells: p_x, p_y, p_z
+    // Per axis, the velocity on each cell's + face (pitched, only the layer's faces used), in two
+    // buffers: faces[1] holds the latest values between runs, as u[1] does.
+    void *faces[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
+    uint32_t link_slots = 0;  // the most links of a special row (6 or 18 kernels)
     unsigned int *d_error = nullptr;  // set by a kernel whose wait gave up
     // Tensor maps of the bulk sweep: each level as the pressure tile (with halos) and as the
     // previous-pressure tile, the cell types and the scales.
@@ -259,7 +267,11 @@ Fields<T> fields_for(const fdtd_solver *s, bool flip) {
     f.a = static_cast<T *>(s->u[prev]);
     f.wb = static_cast<const T *>(s->w[cur]);
     f.wa = static_cast<T *>(s->w[prev]);
-    f.layer_state = static_cast<T *>(s->layer_state);
+    f.layer_parts = static_cast<T *>(s->layer_parts);
+    for (int axis = 0; axis < 3; ++axis) {
+        f.face_old[axis] = static_cast<const T *>(s->faces[cur][axis]);
+        f.face_new[axis] = static_cast<T *>(s->faces[prev][axis]);
+    }
     return f;
 }
 
@@ -267,6 +279,12 @@ template <typename T, bool WIDE, bool SCALED>
 int set_up_kernels(fdtd_solver *s) {
     CUDA_TRY(s, cudaFuncSetAttribute(bulk_kernel<T, WIDE, SCALED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)Stage<T, SCALED>::smem));
+    int per_sm = 0;
+    CUDA_TRY(s, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bulk_kernel<T, WIDE, SCALED>, kBlock,
+                                                              Stage<T, SCALED>::smem));
+    s->bulk_per_sm = per_sm;
+    // One tile per block: measured faster than a persistent grid of the resident blocks.
+    s->bulk_blocks = s->bulk_tiles;
     return FDTD_OK;
 }
 
@@ -275,14 +293,23 @@ int launch_steps(fdtd_solver *s, const float *d_signal, uint64_t steps, double *
     const Tables &g = s->tables;
     const uint32_t special_blocks = (uint32_t)((s->specials + kBlock - 1) / kBlock);
     const uint32_t layer_blocks = (uint32_t)((s->layers + kBlock - 1) / kBlock);
-    const uint32_t probe_blocks = (uint32_t)((s->probes + kBlock - 1) / kBlock);
+    const uint32_t probe_blocks = (uint32_t)((s->probes + kProbeWarps - 1) / kProbeWarps);
     const uint32_t smem = Stage<T, SCALED>::smem;
+    // Each step: the bulk sweep and the matched layer on the handle's stream, the special rows and
+    // the probes on the side stream beside them; each stream waits for the other's end of the step
+    // before.
+    CUDA_TRY(s, cudaEventRecord(s->joined[0], s->stream));
+    CUDA_TRY(s, cudaStreamWaitEvent(s->side, s->joined[0], 0));
     for (uint64_t k = 0; k < steps; ++k) {
         const bool flip = (k & 1) != 0;
         Fields<T> f = fields_for<T>(s, flip);
         f.signal = d_signal + k;
         f.out = d_out + k;
         f.out_stride = stride;
+        if (k > 0) {
+            CUDA_TRY(s, cudaStreamWaitEvent(s->stream, s->joined[1], 0));
+            CUDA_TRY(s, cudaStreamWaitEvent(s->side, s->joined[0], 0));
+        }
         if (s->bulk_blocks) {
             BulkArgs args = s->bulk;
             args.a = f.a;
@@ -290,10 +317,19 @@ int launch_steps(fdtd_solver *s, const float *d_signal, uint64_t steps, double *
             bulk_kernel<T, WIDE, SCALED><<<s->bulk_blocks, kBlock, smem, s->stream>>>(s->map_b[cur], s->map_a[prev],
                                                                                     s->map_t, s->map_s, args);
         }
-        if (special_blocks) special_kernel<T><<<special_blocks, kBlock, 0, s->stream>>>(g, f);
         if (layer_blocks) layer_kernel<T, SCALED><<<layer_blocks, kBlock, 0, s->stream>>>(g, f);
-        if (probe_blocks) probe_kernel<T><<<probe_blocks, kBlock, 0, s->stream>>>(g, f);
+        if (special_blocks) {
+            if (s->link_slots <= 6)
+                special_kernel<T, 6><<<special_blocks, kBlock, 0, s->side>>>(g, f);
+            else
+                special_kernel<T, 18><<<special_blocks, kBlock, 0, s->side>>>(g, f);
+        }
+        if (probe_blocks) probe_kernel<T><<<probe_blocks, kBlock, 0, s->side>>>(g, f);
+        CUDA_TRY(s, cudaEventRecord(s->joined[0], s->stream));
+        CUDA_TRY(s, cudaEventRecord(s->joined[1], s->side));
     }
+    // The handle's stream ends after both.
+    CUDA_TRY(s, cudaStreamWaitEvent(s->stream, s->joined[1], 0));
     CUDA_TRY(s, cudaGetLastError());
     return FDTD_OK;
 }
@@ -338,6 +374,7 @@ void settle(fdtd_solver *s, uint64_t steps) {
     if (steps % 2 == 1) {
         std::swap(s->u[0], s->u[1]);
         std::swap(s->w[0], s->w[1]);
+        for (int axis = 0; axis < 3; ++axis) std::swap(s->faces[0][axis], s->faces[1][axis]);
         std::swap(s->map_b[0], s->map_b[1]);
         std::swap(s->map_a[0], s->map_a[1]);
     }
@@ -370,6 +407,7 @@ int build(fdtd_solver *s, const fdtd_layout *L) {
     g.ny = (uint32_t)ny;
     g.nz = (uint32_t)nz;
     g.sz = (uint32_t)(s->pitch * ny);
+    g.plane = (uint32_t)(s->pitch * ny);
     for (int k = 0; k < 18; ++k)
         g.offset[k] = (int32_t)(kSteps[k][0] + kSteps[k][1] * (int64_t)s->pitch + kSteps[k][2] * (int64_t)(s->pitch * ny));
 
@@ -405,7 +443,11 @@ int build(fdtd_solver *s, const fdtd_layout *L) {
         if ((rc = zeros(s, e * s->n_device, &s->u[k]))) return rc;
         if ((rc = zeros(s, e * L->state_count, &s->w[k]))) return rc;
     }
-    if ((rc = zeros(s, e * 9 * L->layer_count, &s->layer_state))) return rc;
+    if ((rc = zeros(s, e * 3 * L->layer_count, &s->layer_parts))) return rc;
+    if (L->layer_count)
+        for (int k = 0; k < 2; ++k)
+            for (int axis = 0; axis < 3; ++axis)
+                if ((rc = zeros(s, e * s->n_device, &s->faces[k][axis]))) return rc;
     void *flag;
     if ((rc = zeros(s, sizeof(unsigned int), &flag))) return rc;
     s->d_error = static_cast<unsigned int *>(flag);
@@ -430,9 +472,10 @@ int build(fdtd_solver *s, const fdtd_layout *L) {
         uint64_t chunk = depth;
         while (chunk > 8 && columns * ((depth + chunk - 1) / chunk) < (uint64_t)s->sms * 8) chunk = (chunk + 1) / 2;
         bk.chunk = (uint32_t)std::max<uint64_t>(chunk, 1);
-        const uint64_t blocks = columns * ((depth + bk.chunk - 1) / bk.chunk);
-        if (blocks >= (1ull << 31)) return fail(s, FDTD_EINVAL, "the wave grid is too large for one launch");
-        s->bulk_blocks = (uint32_t)blocks;
+        bk.tiles_z = (uint32_t)((depth + bk.chunk - 1) / bk.chunk);
+        const uint64_t tiles = columns * bk.tiles_z;
+        if (tiles >= (1ull << 31)) return fail(s, FDTD_EINVAL, "the wave grid is too large for one launch");
+        s->bulk_tiles = (uint32_t)tiles;
         const CUtensorMapDataType ft = s->precision == FDTD_FP64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
         for (int k = 0; k < 2; ++k) {
             if ((rc = tensor_map(s, &s->map_b[k], s->u[k], ft, (uint32_t)e, kBX, kBY))) return rc;
@@ -450,27 +493,42 @@ int build(fdtd_solver *s, const fdtd_layout *L) {
     const uint64_t K = L->special_count;
     s->specials = K, s->links = L->link_count, s->states = L->state_count;
     g.specials = (uint32_t)K;
+    const float *fp;
+    const uint8_t *u8;
     {
-        std::vector<uint32_t> special(K), link_start(K + 1), state_start(K + 1);
-        for (uint64_t k = 0; k < K; ++k) special[k] = pitched(s, (uint64_t)L->special[k]);
-        for (uint64_t k = 0; k <= K; ++k) {
-            link_start[k] = (uint32_t)L->link_start[k];
-            state_start[k] = (uint32_t)L->state_start[k];
+        std::vector<uint32_t> special(K), state_start(K + 1);
+        uint64_t slots = 0;
+        for (uint64_t k = 0; k < K; ++k) {
+            special[k] = pitched(s, (uint64_t)L->special[k]);
+            slots = std::max<uint64_t>(slots, L->link_start[k + 1] - L->link_start[k]);
         }
+        for (uint64_t k = 0; k <= K; ++k) state_start[k] = (uint32_t)L->state_start[k];
+        if (slots > 18) return fail(s, FDTD_EINVAL, "a special cell has more than 18 links");
+        // The links, slot-major (ELL): slot l of row k at l * K + k.
+        std::vector<uint8_t> count(K), direction(slots * K, 0);
+        std::vector<float> weight(slots * K, 0.0f);
+        for (uint64_t k = 0; k < K; ++k) {
+            const uint64_t l0 = L->link_start[k], l1 = L->link_start[k + 1];
+            count[k] = (uint8_t)(l1 - l0);
+            for (uint64_t l = l0; l < l1; ++l) {
+                direction[(l - l0) * K + k] = L->link_direction[l];
+                weight[(l - l0) * K + k] = L->link_weight[l];
+            }
+        }
+        g.link_slots = (uint32_t)slots;
+        s->link_slots = (uint32_t)slots;
         const uint32_t *p;
         if ((rc = upload(s, special.data(), K, &p))) return rc;
         g.special = p;
-        if ((rc = upload(s, link_start.data(), K + 1, &p))) return rc;
-        g.link_start = p;
         if ((rc = upload(s, state_start.data(), K + 1, &p))) return rc;
         g.state_start = p;
+        if ((rc = upload(s, count.data(), K, &u8))) return rc;
+        g.link_count = u8;
+        if ((rc = upload(s, direction.data(), direction.size(), &u8))) return rc;
+        g.link_direction = u8;
+        if ((rc = upload(s, weight.data(), weight.size(), &fp))) return rc;
+        g.link_weight = fp;
     }
-    const float *fp;
-    const uint8_t *u8;
-    if ((rc = upload(s, L->link_direction, L->link_count, &u8))) return rc;
-    g.link_direction = u8;
-    if ((rc = upload(s, L->link_weight, L->link_count, &fp))) return rc;
-    g.link_weight = fp;
     if ((rc = upload(s, L->coef_a, K, &fp))) return rc;
     g.coef_a = fp;
     if ((rc = upload(s, L->coef_b, K, &fp))) return rc;
@@ -505,9 +563,17 @@ int build(fdtd_solver *s, const fdtd_layout *L) {
     if (Lc) {
         std::vector<uint32_t> cells(Lc);
         for (uint64_t c = 0; c < Lc; ++c) cells[c] = pitched(s, (uint64_t)L->layer_cells[c]);
+        // Which of each layer cell's lower neighbours are in the layer too (their face is theirs).
+        std::vector<uint8_t> below(Lc, 0);
+        const uint64_t strides[3] = {1, nx, nx * ny};
+        for (uint64_t c = 0; c < Lc; ++c)
+            for (int axis = 0; axis < 3; ++axis)
+                if (L->types[(uint64_t)L->layer_cells[c] - strides[axis]] == kLayer) below[c] |= (uint8_t)(1u << axis);
         const uint32_t *p;
         if ((rc = upload(s, cells.data(), Lc, &p))) return rc;
         g.layer_cells = p;
+        if ((rc = upload(s, below.data(), Lc, &u8))) return rc;
+        g.layer_below = u8;
         const uint64_t len[3] = {nx + 1, ny + 1, nz + 1};
         for (int axis = 0; axis < 3; ++axis) {
             std::vector<float4> packed(len[axis]);
@@ -553,6 +619,10 @@ void release(fdtd_solver *s) {
     for (void *p : s->allocations) cudaFree(p);
     if (s->stage_signal) cudaFreeHost(s->stage_signal);
     if (s->stage_out) cudaFreeHost(s->stage_out);
+    if (s->side) cudaStreamSynchronize(s->side);
+    for (cudaEvent_t e : s->joined)
+        if (e) cudaEventDestroy(e);
+    if (s->side) cudaStreamDestroy(s->side);
     if (s->stream) cudaStreamDestroy(s->stream);
     cudaSetDevice(current);
 }
@@ -632,8 +702,12 @@ int fdtd_create(const fdtd_layout *layout, int precision, int device, fdtd_solve
     s->sms = prop.multiProcessorCount;
     s->precision = precision;
     cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->joined[0], cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->joined[1], cudaEventDisableTiming);
     if (e != cudaSuccess) {
         const int rc = cuda_fail(nullptr, e, "cudaStreamCreate");
+        release(s);
         delete s;
         return rc;
     }
@@ -730,7 +804,12 @@ int fdtd_reset(fdtd_solver *s) {
         CUDA_TRY(s, cudaMemsetAsync(s->u[k], 0, e * s->n_device, s->stream));
         if (s->states) CUDA_TRY(s, cudaMemsetAsync(s->w[k], 0, e * s->states, s->stream));
     }
-    if (s->layers) CUDA_TRY(s, cudaMemsetAsync(s->layer_state, 0, e * 9 * s->layers, s->stream));
+    if (s->layers) {
+        CUDA_TRY(s, cudaMemsetAsync(s->layer_parts, 0, e * 3 * s->layers, s->stream));
+        for (int k = 0; k < 2; ++k)
+            for (int axis = 0; axis < 3; ++axis)
+                CUDA_TRY(s, cudaMemsetAsync(s->faces[k][axis], 0, e * s->n_device, s->stream));
+    }
     CUDA_TRY(s, cudaStreamSynchronize(s->stream));
     s->steps_done = 0;
     return FDTD_OK;
@@ -779,13 +858,25 @@ int fdtd_read_state(const fdtd_solver *cs, void *current, void *previous, void *
     if (branch_current && s->states) CUDA_TRY(s, cudaMemcpy(branch_current, s->w[1], e * s->states, cudaMemcpyDeviceToHost));
     if (branch_previous && s->states) CUDA_TRY(s, cudaMemcpy(branch_previous, s->w[0], e * s->states, cudaMemcpyDeviceToHost));
     if (layer_state && s->layers) {
-        // The device keeps the layer's state as 9 arrays; the reference keeps 9 values per cell.
-        std::vector<char> soa(e * 9 * s->layers);
-        CUDA_TRY(s, cudaMemcpy(soa.data(), s->layer_state, soa.size(), cudaMemcpyDeviceToHost));
+        // The reference's nine values per cell (fdtd.hpp:2245): the parts, then per axis the
+        // velocity of the - face (the + face of the cell below) and of the + face.
+        std::vector<char> parts(e * 3 * s->layers);
+        CUDA_TRY(s, cudaMemcpy(parts.data(), s->layer_parts, parts.size(), cudaMemcpyDeviceToHost));
+        std::vector<uint32_t> cells(s->layers);
+        CUDA_TRY(s, cudaMemcpy(cells.data(), s->tables.layer_cells, 4 * s->layers, cudaMemcpyDeviceToHost));
+        std::vector<char> face(e * s->n_device);
         char *dst = static_cast<char *>(layer_state);
         for (uint64_t c = 0; c < s->layers; ++c)
-            for (int k = 0; k < 9; ++k)
-                std::memcpy(dst + e * (9 * c + k), soa.data() + e * (k * s->layers + c), e);
+            for (int k = 0; k < 3; ++k) std::memcpy(dst + e * (9 * c + k), parts.data() + e * (k * s->layers + c), e);
+        const uint64_t strides[3] = {1, s->pitch, s->pitch * s->ny};
+        for (int axis = 0; axis < 3; ++axis) {
+            CUDA_TRY(s, cudaMemcpy(face.data(), s->faces[1][axis], face.size(), cudaMemcpyDeviceToHost));
+            for (uint64_t c = 0; c < s->layers; ++c) {
+                const uint64_t i = cells[c];
+                std::memcpy(dst + e * (9 * c + 3 + 2 * axis), face.data() + e * (i - strides[axis]), e);
+                std::memcpy(dst + e * (9 * c + 4 + 2 * axis), face.data() + e * i, e);
+            }
+        }
     }
     return FDTD_OK;
 }

@@ -62,7 +62,7 @@ struct BulkArgs {
     void *a;  // the previous pressure, overwritten with the next (T)
     uint32_t pitch, ny;
     uint32_t xa, y0, z0, x1, y1, z1;  // tiles start at xa (16-aligned), y0, z0; the box ends x1, y1, z1
-    uint32_t tiles_x, tiles_y, chunk;
+    uint32_t tiles_x, tiles_y, tiles_z, chunk;
     float axial, diagonal, centre, total;
     unsigned int *error;  // set to 1 when a wait gives up
 };
@@ -124,29 +124,34 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map
 
 // ---- interior air ------------------------------------------------------------------------------
 
-// Thread 0 of a bulk block: the copies of plane k (the block's index-th stage) into its slot of
-// the ring, all completing on the slot's barrier.
-template <typename T, bool SCALED>
-__device__ __forceinline__ void issue_stage(uint32_t base, uint32_t bars, int index, int k, int xt, int yt,
-                                            const CUtensorMap *map_b, const CUtensorMap *map_a,
-                                            const CUtensorMap *map_t, const CUtensorMap *map_s) {
-    using S = Stage<T, SCALED>;
-    const int slot = index % kStages;
-    const uint32_t stage = base + slot * S::bytes, bar = bars + 8 * slot;
-    mbar_expect_tx(bar, S::tx_bytes);
-    tma_load_3d(stage + S::b_off, map_b, xt - kHX, yt - 1, k, bar);
-    tma_load_3d(stage + S::a_off, map_a, xt, yt, k, bar);
-    tma_load_3d(stage + S::t_off, map_t, xt, yt, k, bar);
-    if (SCALED) tma_load_3d(stage + S::s_off, map_s, xt, yt, k, bar);
+// Interior air (fdtd.hpp:242-288). The box of the interior cells is cut into tiles of kTX x kTY
+// cells by a chunk of planes along z; each resident block (a persistent grid) takes tiles
+// blockIdx.x, + gridDim.x, ... and marches each along z. Its planes' stages — plane k's pressure
+// tile with halos, previous pressure, types and scales — form one sequence over all its tiles:
+// tile m's stages are planes z0-1 .. z_end. Thread 0 issues the sequence with TMA, kAhead stages
+// ahead of the three in use (across tile boundaries too), into a ring of kStages slots in shared
+// memory, each completed on its slot's mbarrier; the block updates plane z from the stages of
+// planes z-1, z and z+1, each thread 8 rows of one column, and stores the new pressure of the
+// interior cells. Every wait is bounded: a block that gives up sets the error flag, lets its
+// copies in flight land, and stops.
+// The reference's sums in its order: x-1, x+1, y-1, y+1, z-1, z+1, then the twelve edges.
+struct TileSpan {
+    int xt, yt, z0, z_end;  // the tile's corner and its planes z0 .. z_end-1
+};
+
+__device__ __forceinline__ TileSpan tile_span(const BulkArgs &p, uint32_t tile) {
+    const uint32_t bx = tile % p.tiles_x;
+    tile /= p.tiles_x;
+    const uint32_t by = tile % p.tiles_y;
+    const uint32_t bz = tile / p.tiles_y;
+    TileSpan t;
+    t.xt = (int)(p.xa + bx * kTX);
+    t.yt = (int)(p.y0 + by * kTY);
+    t.z0 = (int)(p.z0 + bz * p.chunk);
+    t.z_end = min(t.z0 + (int)p.chunk, (int)p.z1);
+    return t;
 }
 
-// Interior air (fdtd.hpp:242-288). A block owns a tile of kTX x kTY cells of the interior cells'
-// bounding box and marches it along z through a chunk of planes. One thread issues, with TMA, each
-// plane's stage kAhead planes ahead into a ring of kStages stages in shared memory, each completed
-// on its own mbarrier; the block updates plane z from the stages of planes z-1, z and z+1, each
-// thread 8 rows of one column. Neighbours come from shared memory, so that every value is read
-// from HBM once per block; the new pressure of interior cells is stored to global memory.
-// The reference's sums in its order: x-1, x+1, y-1, y+1, z-1, z+1, then the twelve edges.
 template <typename T, bool WIDE, bool SCALED>
 __global__ void __launch_bounds__(kBlock) bulk_kernel(const __grid_constant__ CUtensorMap map_b,
                                                       const __grid_constant__ CUtensorMap map_a,
@@ -157,18 +162,8 @@ __global__ void __launch_bounds__(kBlock) bulk_kernel(const __grid_constant__ CU
     extern __shared__ __align__(128) unsigned char smem[];
     const uint32_t base = smem_address(smem);
     const uint32_t bars = base + kStages * S::bytes;
-
-    uint32_t tile = blockIdx.x;
-    const uint32_t bx = tile % p.tiles_x;
-    tile /= p.tiles_x;
-    const uint32_t by = tile % p.tiles_y;
-    const uint32_t bz = tile / p.tiles_y;
-    const int xt = (int)(p.xa + bx * kTX), yt = (int)(p.y0 + by * kTY);
-    const int z0 = (int)(p.z0 + bz * p.chunk);
-    const int z_end = min(z0 + (int)p.chunk, (int)p.z1);
-    if (z0 >= z_end) return;  // the whole block alike
-    // Stages first .. last: planes z0-1 .. z_end, all inside the grid (z0 >= 1, z_end <= nz-1).
-    const int first = z0 - 1, last = z_end;
+    const uint32_t tiles = p.tiles_x * p.tiles_y * p.tiles_z;
+    if (blockIdx.x >= tiles) return;  // the whole block alike
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < kStages; ++s) mbar_init(bars + 8 * s, 1);
@@ -176,92 +171,105 @@ __global__ void __launch_bounds__(kBlock) bulk_kernel(const __grid_constant__ CU
     }
     __syncthreads();
 
-    int issued = min(last, first + kAhead + 1);  // the last stage issued (thread 0's count)
-    if (threadIdx.x == 0) {
-        fence_proxy_async();
-        for (int k = first; k <= issued; ++k)
-            issue_stage<T, SCALED>(base, bars, k - first, k, xt, yt, &map_b, &map_a, &map_t, &map_s);
-    }
-
+    // The producer's place in the sequence (thread 0 only): its tile, the next plane to issue,
+    // and the count of stages issued.
+    uint32_t p_tile = blockIdx.x;
+    TileSpan p_span = tile_span(p, p_tile);
+    int p_k = p_span.z0 - 1;
+    int issued = 0;
     const T axial = (T)p.axial, centre = (T)p.centre, diagonal = (T)p.diagonal, total = (T)p.total;
     const int xl = threadIdx.x % kTX;
     const int r0 = (threadIdx.x / kTX) * kRowsPerThread;
-    const int x = xt + xl;
     T *__restrict__ a = static_cast<T *>(p.a);
     const uint64_t plane = (uint64_t)p.pitch * p.ny;
     bool ok = true, failed = false;
-    int waited = first - 1;  // the last stage waited for
+    int waited = 0;    // stages 0 .. waited-1 complete (this thread's view)
+    int position = 0;  // the sequence position of the current tile's stage z0-1
 
-    for (int z = z0; z < z_end; ++z) {
-        // Refill the slot of plane z-2 (its last use, plane z-1's update, is over) with plane
-        // z+1+kAhead.
-        if (threadIdx.x == 0 && z + 1 + kAhead <= last) {
-            fence_proxy_async();
-            issued = z + 1 + kAhead;
-            issue_stage<T, SCALED>(base, bars, issued - first, issued, xt, yt, &map_b, &map_a, &map_t, &map_s);
-        }
-        // Stages z-1, z and z+1 complete (each waited for once).
-        for (int k = waited + 1; k <= z + 1 && ok; ++k) {
-            const int index = k - first;
-            ok = mbar_wait(bars + 8 * (index % kStages), (index / kStages) & 1);
-            waited = k;
-        }
-        if (ok) {
-            const int index = z - first;
-            const unsigned char *s0 = smem + (index % kStages) * S::bytes;
-            const T *bm = reinterpret_cast<const T *>(smem + ((index - 1) % kStages) * S::bytes + S::b_off);
-            const T *b0 = reinterpret_cast<const T *>(s0 + S::b_off);
-            const T *bp = reinterpret_cast<const T *>(smem + ((index + 1) % kStages) * S::bytes + S::b_off);
-            const T *pa = reinterpret_cast<const T *>(s0 + S::a_off);
-            const uint8_t *pt = reinterpret_cast<const uint8_t *>(s0 + S::t_off);
-            const float *ps = reinterpret_cast<const float *>(s0 + S::s_off);
-#pragma unroll
-            for (int r = 0; r < kRowsPerThread; ++r) {
-                const int yl = r0 + r;
-                const int c = yl * kTX + xl;
-                // Outside the interior cells' box, and outside the grid (zero fill), no cell is
-                // interior.
-                if (pt[c] != kInterior) continue;
-                const int q = (yl + 1) * kBX + (xl + kHX);
-                const T here = b0[q];
-                const T sum = b0[q - 1] + b0[q + 1] + b0[q - kBX] + b0[q + kBX] + bm[q] + bp[q];
-                T next;
-                if (WIDE) {
-                    const T edges = b0[q - 1 - kBX] + b0[q + 1 - kBX] + b0[q - 1 + kBX] + b0[q + 1 + kBX] +
-                                    bm[q - 1] + bm[q + 1] + bp[q - 1] + bp[q + 1] +
-                                    bm[q - kBX] + bm[q + kBX] + bp[q - kBX] + bp[q + kBX];
-                    if (SCALED) {
-                        const T s = (T)ps[c];
-                        next = ((T)2 - total * s) * here + (s * axial) * sum + (s * diagonal) * edges - pa[c];
-                    } else {
-                        next = centre * here + axial * sum + diagonal * edges - pa[c];
-                    }
-                } else {
-                    if (SCALED) {
-                        const T s = (T)ps[c];
-                        next = ((T)2 - total * s) * here + (s * axial) * sum - pa[c];
-                    } else {
-                        next = centre * here + axial * sum - pa[c];
+    for (uint32_t tile = blockIdx.x; tile < tiles && !failed; tile += gridDim.x) {
+        const TileSpan t = tile_span(p, tile);
+        const int x = t.xt + xl;
+        for (int z = t.z0; z < t.z_end; ++z) {
+            const int centre_at = position + (z - t.z0 + 1);  // plane z's stage
+            // Refill the slots whose stages are over (up to plane z-2's) with the stages up to
+            // kAhead beyond plane z+1's.
+            if (threadIdx.x == 0) {
+                fence_proxy_async();
+                const int target = centre_at + 2 + kAhead;  // issue stages .. target-1
+                while (issued < target && p_tile < tiles) {
+                    const int slot = issued % kStages;
+                    const uint32_t stage = base + slot * S::bytes, bar = bars + 8 * slot;
+                    mbar_expect_tx(bar, S::tx_bytes);
+                    tma_load_3d(stage + S::b_off, &map_b, p_span.xt - kHX, p_span.yt - 1, p_k, bar);
+                    tma_load_3d(stage + S::a_off, &map_a, p_span.xt, p_span.yt, p_k, bar);
+                    tma_load_3d(stage + S::t_off, &map_t, p_span.xt, p_span.yt, p_k, bar);
+                    if (SCALED) tma_load_3d(stage + S::s_off, &map_s, p_span.xt, p_span.yt, p_k, bar);
+                    ++issued;
+                    if (++p_k > p_span.z_end) {
+                        p_tile += gridDim.x;
+                        if (p_tile < tiles) {
+                            p_span = tile_span(p, p_tile);
+                            p_k = p_span.z0 - 1;
+                        }
                     }
                 }
-                a[(uint64_t)x + (uint64_t)(yt + yl) * p.pitch + (uint64_t)z * plane] = next;
+            }
+            for (; waited <= centre_at + 1 && ok; ++waited)
+                ok = mbar_wait(bars + 8 * (waited % kStages), (waited / kStages) & 1);
+            if (ok) {
+                const unsigned char *s0 = smem + (centre_at % kStages) * S::bytes;
+                const T *bm = reinterpret_cast<const T *>(smem + ((centre_at - 1) % kStages) * S::bytes + S::b_off);
+                const T *b0 = reinterpret_cast<const T *>(s0 + S::b_off);
+                const T *bp = reinterpret_cast<const T *>(smem + ((centre_at + 1) % kStages) * S::bytes + S::b_off);
+                const T *pa = reinterpret_cast<const T *>(s0 + S::a_off);
+                const uint8_t *pt = reinterpret_cast<const uint8_t *>(s0 + S::t_off);
+                const float *ps = reinterpret_cast<const float *>(s0 + S::s_off);
+#pragma unroll
+                for (int r = 0; r < kRowsPerThread; ++r) {
+                    const int yl = r0 + r;
+                    const int c = yl * kTX + xl;
+                    // Outside the interior cells' box, and outside the grid (zero fill), no cell
+                    // is interior.
+                    if (pt[c] != kInterior) continue;
+                    const int q = (yl + 1) * kBX + (xl + kHX);
+                    const T here = b0[q];
+                    const T sum = b0[q - 1] + b0[q + 1] + b0[q - kBX] + b0[q + kBX] + bm[q] + bp[q];
+                    T next;
+                    if (WIDE) {
+                        const T edges = b0[q - 1 - kBX] + b0[q + 1 - kBX] + b0[q - 1 + kBX] + b0[q + 1 + kBX] +
+                                        bm[q - 1] + bm[q + 1] + bp[q - 1] + bp[q + 1] +
+                                        bm[q - kBX] + bm[q + kBX] + bp[q - kBX] + bp[q + kBX];
+                        if (SCALED) {
+                            const T sc = (T)ps[c];
+                            next = ((T)2 - total * sc) * here + (sc * axial) * sum + (sc * diagonal) * edges - pa[c];
+                        } else {
+                            next = centre * here + axial * sum + diagonal * edges - pa[c];
+                        }
+                    } else {
+                        if (SCALED) {
+                            const T sc = (T)ps[c];
+                            next = ((T)2 - total * sc) * here + (sc * axial) * sum - pa[c];
+                        } else {
+                            next = centre * here + axial * sum - pa[c];
+                        }
+                    }
+                    a[(uint64_t)x + (uint64_t)(t.yt + yl) * p.pitch + (uint64_t)z * plane] = next;
+                }
+            }
+            // Every thread is done with plane z-1's stage; stop the block alike if a wait gave up.
+            if (__syncthreads_or(!ok)) {
+                failed = true;
+                break;
             }
         }
-        // Every thread is done with plane z-1's stage; stop the block alike if a wait gave up.
-        if (__syncthreads_or(!ok)) {
-            failed = true;
-            break;
-        }
+        position += t.z_end - t.z0 + 2;
     }
     if (failed) {  // the same in every thread of the block
         // Give up: report it, and let the copies in flight land before the block's shared
         // memory is released (each wait bounded again).
         if (threadIdx.x == 0) {
             atomicOr(p.error, 1u);
-            for (int k = waited + 1; k <= issued; ++k) {
-                const int index = k - first;
-                mbar_wait(bars + 8 * (index % kStages), (index / kStages) & 1);
-            }
+            for (int k = waited; k < issued; ++k) mbar_wait(bars + 8 * (k % kStages), (k / kStages) & 1);
         }
         __syncthreads();
     }
@@ -273,8 +281,11 @@ struct Tables {
     uint32_t pitch, ny, nz, sz;
     // Special rows (fdtd.hpp:860-881), as structure of arrays.
     uint32_t specials;
-    const uint32_t *special, *link_start, *state_start;
-    const uint8_t *link_direction;
+    const uint32_t *special, *state_start;
+    // Each row's links as a slot-major table (slot l of row k at l * specials + k), in the
+    // layout's order, and each row's count of links.
+    uint32_t link_slots;
+    const uint8_t *link_count, *link_direction;
     const float *link_weight, *coef_a, *coef_b, *coef_inv, *source;
     const float *state_weight, *state_now, *state_before, *state_gain;
     int32_t offset[18];
@@ -285,6 +296,8 @@ struct Tables {
     const uint32_t *layer_cells;
     const float *layer_scale;
     const float4 *layer_coef[3];
+    const uint8_t *layer_below;  // bit a: the cell below along axis a is in the layer too
+    uint32_t plane;  // pitch * ny
     // Probes (fdtd.hpp:3525-3533).
     uint32_t probes;
     const uint32_t *probe_start, *probe_cells;
@@ -297,26 +310,43 @@ struct Fields {
     const T *b;        // the current pressure
     T *wa;             // branch velocities a step before, overwritten with the next
     const T *wb;       // current branch velocities
-    T *layer_state;    // 9 arrays of `layers`: p_x, p_y, p_z, u-_x, u+_x, u-_y, u+_y, u-_z, u+_z
+    T *layer_parts;    // 3 arrays of `layers`: the pressure parts p_x, p_y, p_z
+    const T *face_old[3];  // per axis, the velocity on each cell's + face (pitched), a step before
+    T *face_new[3];        // the same, this step
     const float *signal;  // the step's drive at signal[0]
     double *out;       // probe p's record at out[p * out_stride]
     uint64_t out_stride;
 };
 
 // Special rows (fdtd.hpp:860-881), one a thread: its links, its branch states' flow, the update,
-// then the branch velocities. A state's term now * wb - before * wa is worked out again for the
+// then the branch velocities. The links' table is slot-major, so that a warp's loads of a slot
+// are coalesced; all of a row's link loads are issued before the sum, which then adds them in
+// the layout's order. A state's term now * wb - before * wa is worked out again for the
 // velocities' update rather than kept: wa has not changed in between, so it is the same value.
-template <typename T>
+template <typename T, int SLOTS>
 __global__ void __launch_bounds__(kBlock) special_kernel(const Tables g, const Fields<T> f) {
     const uint32_t k = blockIdx.x * kBlock + threadIdx.x;
-    if (k >= g.specials) return;
+    const uint32_t K = g.specials;
+    if (k >= K) return;
     const uint32_t i = g.special[k];
+    const uint32_t links = g.link_count[k];
     const T *__restrict__ b = f.b;
-    T sum = 0;
-    for (uint32_t l = g.link_start[k], e = g.link_start[k + 1]; l < e; ++l) {
-        const uint32_t j = (uint32_t)((int64_t)i + g.offset[g.link_direction[l]]);
-        sum += (T)g.link_weight[l] * b[j];
+    T value[SLOTS];
+    float weight[SLOTS];
+#pragma unroll
+    for (int l = 0; l < SLOTS; ++l) {
+        value[l] = (T)0;
+        weight[l] = 0.0f;
+        if ((uint32_t)l < links) {
+            const uint32_t at = l * K + k;
+            weight[l] = g.link_weight[at];
+            value[l] = b[(uint32_t)((int64_t)i + g.offset[g.link_direction[at]])];
+        }
     }
+    T sum = 0;
+#pragma unroll
+    for (int l = 0; l < SLOTS; ++l)
+        if ((uint32_t)l < links) sum += (T)weight[l] * value[l];
     const uint32_t s0 = g.state_start[k], s1 = g.state_start[k + 1];
     T flow = 0;
     for (uint32_t j = s0; j < s1; ++j) {
@@ -334,62 +364,77 @@ __global__ void __launch_bounds__(kBlock) special_kernel(const Tables g, const F
 }
 
 // Matched-layer cells (fdtd.hpp:2242-2264), one a thread: per axis the cell's two face
-// velocities, then its pressure part; the cell's pressure is the parts' sum. The state (nine
-// arrays over the layer's cells, coalesced) is loaded before anything that depends on the cell's
-// place.
+// velocities, then its pressure part; the cell's pressure is the parts' sum.
+//
+// The reference keeps, per layer cell, its own copy of the velocity on each of its six faces
+// (fdtd.hpp:2245), and both cells of a face update their copies alike: cell i's + face along an
+// axis of stride s and cell i+s's - face take keep_face[x+1] * u - push_face[x+1] * (b[i+s] -
+// b[i]) from the same value, so that, both starting at 0, the two copies stay equal to the bit.
+// Here each face is kept once, on the cell below it (face[i] is cell i's + face), in two buffers
+// that alternate with the steps: every cell reads the old values of its two faces and works both
+// out again, and writes the new value of its + face, and of its - face too where the cell below
+// is not in the layer (no one else writes that face). The pressure parts stay per cell.
 template <typename T, bool SCALED>
 __global__ void __launch_bounds__(kBlock) layer_kernel(const Tables g, const Fields<T> f) {
     const uint32_t c = blockIdx.x * kBlock + threadIdx.x;
     const uint32_t L = g.layers;
     if (c >= L) return;
-    T *st = f.layer_state;
-    T part[3], below[3], above[3];
+    T *parts = f.layer_parts;
+    T part[3];
 #pragma unroll
-    for (int axis = 0; axis < 3; ++axis) {
-        part[axis] = st[axis * L + c];
-        below[axis] = st[(3 + 2 * axis) * L + c];
-        above[axis] = st[(4 + 2 * axis) * L + c];
-    }
+    for (int axis = 0; axis < 3; ++axis) part[axis] = parts[axis * L + c];
     const uint32_t i = g.layer_cells[c];
-    const uint32_t at[3] = {i % g.pitch, (i / g.pitch) % g.ny, i / g.sz};
-    const uint32_t strides[3] = {1u, g.pitch, g.sz};
+    const uint32_t at[3] = {i % g.pitch, (i / g.pitch) % g.ny, i / g.plane};
+    const uint32_t strides[3] = {1u, g.pitch, g.plane};
     const T *__restrict__ b = f.b;
     const T here = b[i];
     const T scale = SCALED ? (T)g.layer_scale[c] : (T)1;
+    const uint32_t shared_below = g.layer_below[c];
     T total = 0;
 #pragma unroll
     for (int axis = 0; axis < 3; ++axis) {
         const uint32_t stride = strides[axis], x = at[axis];
         const float4 c0 = g.layer_coef[axis][x], c1 = g.layer_coef[axis][x + 1];
-        below[axis] = (T)c0.z * below[axis] - (T)c0.w * (here - b[i - stride]);
-        above[axis] = (T)c1.z * above[axis] - (T)c1.w * (b[i + stride] - here);
+        const T below = (T)c0.z * f.face_old[axis][i - stride] - (T)c0.w * (here - b[i - stride]);
+        const T above = (T)c1.z * f.face_old[axis][i] - (T)c1.w * (b[i + stride] - here);
+        f.face_new[axis][i] = above;
+        // The cell below owns the face when it is in the layer.
+        if (!(shared_below & (1u << axis))) f.face_new[axis][i - stride] = below;
         if (SCALED) {
-            part[axis] = (T)c0.x * part[axis] - ((T)c0.y * scale) * (above[axis] - below[axis]);
+            part[axis] = (T)c0.x * part[axis] - ((T)c0.y * scale) * (above - below);
         } else {
-            part[axis] = (T)c0.x * part[axis] - (T)c0.y * (above[axis] - below[axis]);
+            part[axis] = (T)c0.x * part[axis] - (T)c0.y * (above - below);
         }
         total += part[axis];
     }
 #pragma unroll
-    for (int axis = 0; axis < 3; ++axis) {
-        st[axis * L + c] = part[axis];
-        st[(3 + 2 * axis) * L + c] = below[axis];
-        st[(4 + 2 * axis) * L + c] = above[axis];
-    }
+    for (int axis = 0; axis < 3; ++axis) parts[axis * L + c] = part[axis];
     f.a[i] = total;
 }
 
 // Probe p's pressure before the step (fdtd.hpp:3525-3533): its cells' weighted sum in double, in
-// the layout's order.
+// the layout's order. A warp per probe: the lanes load the cells and form the products (each
+// product is the reference's own), then lane 0 adds them up in the layout's order, so that the
+// sum rounds as the reference's sequential one.
+constexpr int kProbeWarps = kBlock / 32;
+
 template <typename T>
 __global__ void __launch_bounds__(kBlock) probe_kernel(const Tables g, const Fields<T> f) {
-    const uint32_t p = blockIdx.x * kBlock + threadIdx.x;
-    if (p >= g.probes) return;
+    const uint32_t p = blockIdx.x * kProbeWarps + threadIdx.x / 32;
+    const uint32_t lane = threadIdx.x % 32;
+    if (p >= g.probes) return;  // the whole warp alike
+    const uint32_t start = g.probe_start[p], end = g.probe_start[p + 1];
     double value = 0.0;
-    for (uint32_t k = g.probe_start[p], e = g.probe_start[p + 1]; k < e; ++k) {
-        value += g.probe_weights[k] * (double)f.b[g.probe_cells[k]];
+    for (uint32_t base = start; base < end; base += 32) {
+        const uint32_t k = base + lane;
+        const double product = k < end ? g.probe_weights[k] * (double)f.b[g.probe_cells[k]] : 0.0;
+        const uint32_t count = min(32u, end - base);
+        for (uint32_t l = 0; l < count; ++l) {
+            const double term = __shfl_sync(0xffffffffu, product, l);
+            if (lane == 0) value += term;
+        }
     }
-    f.out[(uint64_t)p * f.out_stride] = value;
+    if (lane == 0) f.out[(uint64_t)p * f.out_stride] = value;
 }
 
 }  // namespace fdtd

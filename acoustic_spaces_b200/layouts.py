@@ -320,7 +320,13 @@ def cell_face_layout(
     branch_before = ((2.0 * branch_rows[:, 0] + branch_rows[:, 2]) / a_of).astype(np.float32)
     branch_gain = (0.5 / a_of).astype(np.float32)
 
-    s = 1.0 if speed is None else float(np.float32(speed * speed))
+    # Each cell's scale is its speed ratio (a float) squared, rounded to a float (fdtd.hpp:415-425);
+    # its boundary terms take the square root of that scale.
+    if speed is None:
+        s = 1.0
+    else:
+        ratio = float(np.float32(speed))
+        s = float(np.float32(ratio * ratio))
     r = math.sqrt(s)
 
     # Boundary rows (fdtd.hpp:560-623), vectorised over the rows, in the reference's order of

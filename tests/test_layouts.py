@@ -1,0 +1,117 @@
+"""The host layout builder (acoustic_spaces_b200.layouts) against the reference's own layouts.
+
+A convex room handed to the reference's WaveSolver as a triangle mesh (walls on cell faces, the
+7-point stencil) and built here from its planes must give the same layout, array for array
+(cpp/include/acoustic_spaces/fdtd.hpp:452-690 against layouts.cell_face_layout). Without the
+reference sources, the builder's invariants are checked instead.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import cases
+from acoustic_spaces_b200 import layouts as L
+from oracle.oracle import OracleSolver
+
+H = 0.1
+BOX = (4.0, 3.0, 2.4)
+RATE = 343.0 / (L.COURANT * H)
+
+
+def _material(rng):
+    return L.Material(
+        float(rng.uniform(0.02, 0.1)),
+        L.resonant_branch(rng.uniform(0.005, 0.5), rng.uniform(0.5, 10.0), rng.uniform(30.0, 300.0), RATE),
+    )
+
+
+def _room(seed: int, open_face: int | None, layer: int, faces: int = 14, speed=None):
+    rng = np.random.default_rng(seed)
+    room = L.convex_room(rng, BOX, faces=faces, margin=H * (layer + 3), open_face=open_face, material=_material)
+    points = L.inside_points(rng, room, BOX, 5, 0.35, apart=0.35)
+    grid = L.Grid(-L.OFFSET * H, H, tuple(int(round(b / H)) for b in BOX))
+    built = L.cell_face_layout(
+        room, grid, points[0], points[1:], layer=layer, layer_damping=0.5 if layer else 0.0, speed=speed
+    )
+    return room, grid, points, built
+
+
+def _reference_layout(room, grid, points, layer, speed=None):
+    native = cases.reference_native()
+    vertices, faces, owner = L.room_mesh(room)
+    beta = np.array([0.0 if m is None else m.beta for m in room.materials])
+    rows, owners = [np.zeros((0, 3))], [np.zeros(0, np.int64)]
+    for k, m in enumerate(room.materials):
+        if m is not None:
+            rows.append(m.branches)
+            owners.append(np.full(len(m.branches), k, np.int64))
+    speeds = None if speed is None else np.full(grid.n, speed, np.float32)
+    solver = native.WaveSolver(
+        native.Bvh(vertices, faces), owner, beta, np.ascontiguousarray(np.vstack(rows)), np.concatenate(owners),
+        grid.origin, grid.cell, *grid.shape, points[0], points[1:], layer=layer,
+        layer_damping=0.5 if layer else 0.0, threads=2, speed=speeds,
+    )  # fmt: skip
+    return solver, solver.layout()
+
+
+ROOMS = [(3, 1, 4, None), (4, None, 0, None), (5, 1, 4, 0.93), (6, None, 0, 0.99)]
+
+
+@pytest.mark.parametrize("seed, open_face, layer, speed", ROOMS)
+def test_the_builder_lays_a_room_out_as_the_reference_does(seed, open_face, layer, speed):
+    if not cases.available():
+        pytest.skip("the reference sources are not here")
+    room, grid, points, built = _room(seed, open_face, layer, speed=speed)
+    solver, ref = _reference_layout(room, grid, points, layer, speed)
+    assert solver.air_cells == built.air_cells
+    assert solver.boundary_cells == built.boundary_cells
+    for name, value in built.layout.items():
+        mine, theirs = np.asarray(value), np.asarray(ref[name])
+        assert mine.dtype == theirs.dtype, name
+        assert np.array_equal(mine, theirs), name
+
+
+@pytest.mark.parametrize("seed, open_face, layer, speed", ROOMS)
+def test_the_builders_layout_is_consistent(seed, open_face, layer, speed):
+    _, grid, _, built = _room(seed, open_face, layer, speed=speed)
+    lay = built.layout
+    types = lay["types"]
+    assert np.all(types[lay["special"]] == 2)
+    assert np.all(types[lay["layer_cells"]] == 3)
+    assert len(lay["special"]) == np.count_nonzero(types == 2)
+    assert len(lay["layer_cells"]) == np.count_nonzero(types == 3)
+    assert built.air_cells == np.count_nonzero(types)
+    assert np.all(np.diff(lay["link_start"].astype(np.int64)) >= 0)
+    assert abs(float(np.sum(lay["source"])) - (1.0 if speed is None else np.float32(speed * speed))) < 1e-5
+    # every interior cell's six neighbours are air
+    nx, ny, _ = grid.shape
+    interior = np.flatnonzero(types == 1)
+    for off in (1, -1, nx, -nx, nx * ny, -nx * ny):
+        assert np.all(types[interior + off] != 0)
+
+
+def test_the_builders_room_steps_stably_in_the_oracle():
+    _, _, _, built = _room(3, 1, 4)
+    signal = L.gaussian_drive(RATE, 300)
+    out = OracleSolver(built.layout).run(signal)
+    assert np.all(np.isfinite(out)) and np.abs(out).max() > 0.0
+
+
+def test_the_builder_refuses_a_probe_next_to_the_source():
+    rng = np.random.default_rng(1)
+    room = L.convex_room(rng, BOX, faces=8, margin=0.3, open_face=None, material=_material)
+    points = L.inside_points(rng, room, BOX, 1, 0.35)
+    grid = L.Grid(-L.OFFSET * H, H, tuple(int(round(b / H)) for b in BOX))
+    with pytest.raises(ValueError, match="three cells"):
+        L.cell_face_layout(room, grid, points[0], points[:1] + 0.05)
+
+
+def test_the_polyhedral_workload_is_seeded():
+    a = L.polyhedral_room(0, cell=0.2, steps=10)
+    b = L.polyhedral_room(0, cell=0.2, steps=10)
+    assert a.description == b.description
+    for name in a.built.layout:
+        assert np.array_equal(a.built.layout[name], b.built.layout[name])
+    assert 12 <= int(a.description["room"].split(",")[1].split()[0]) <= 20
