@@ -40,6 +40,7 @@ constexpr int kSteps[18][3] = {
     {-1, 0, 1},  {1, 0, 1},  {0, -1, -1}, {0, 1, -1}, {0, -1, 1},  {0, 1, 1}};
 
 constexpr uint64_t kPitchCells = 16;  // rows padded to a multiple of 16 cells
+constexpr uint64_t kGraphSteps = 64;  // steps of fdtd_run's captured chunk (even: the roles return)
 
 using EncodeTiled = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
@@ -79,6 +80,16 @@ struct fdtd_solver {
     // Tensor maps of the bulk sweep: each level as the pressure tile (with halos) and as the
     // previous-pressure tile, the cell types and the scales.
     CUtensorMap map_b[2], map_a[2], map_t, map_s;
+    // fdtd_run's chunks: the drive and the records of kGraphSteps steps on the device, and the
+    // graph of a chunk's launches for each of the levels' two roles (captured on first use).
+    float *d_sig = nullptr;
+    double *d_rec = nullptr;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    bool flipped = false;  // the levels' roles swapped from the handle's first (an odd count of steps)
+    // Per-kernel timing (fdtd_set_timing): per timed step, a start and an end event per kind.
+    bool timing = false;
+    std::vector<cudaEvent_t> timing_events;  // 8 per step: (start, end) of bulk, layer, special, probe
+    uint64_t timed_steps = 0;
     // Staging for fdtd_run's host buffers, grown on demand.
     float *stage_signal = nullptr;
     double *stage_out = nullptr;
@@ -310,6 +321,19 @@ int launch_steps(fdtd_solver *s, const float *d_signal, uint64_t steps, double *
             CUDA_TRY(s, cudaStreamWaitEvent(s->stream, s->joined[1], 0));
             CUDA_TRY(s, cudaStreamWaitEvent(s->side, s->joined[0], 0));
         }
+        cudaEvent_t *ev = nullptr;
+        if (s->timing) {
+            // (Created on demand; recorded only outside graph captures.)
+            const size_t base = s->timing_events.size();
+            for (int e = 0; e < 8; ++e) {
+                cudaEvent_t event;
+                CUDA_TRY(s, cudaEventCreate(&event));
+                s->timing_events.push_back(event);
+            }
+            ev = &s->timing_events[base];
+            ++s->timed_steps;
+        }
+        if (ev) CUDA_TRY(s, cudaEventRecord(ev[0], s->stream));
         if (s->bulk_blocks) {
             BulkArgs args = s->bulk;
             args.a = f.a;
@@ -317,14 +341,21 @@ int launch_steps(fdtd_solver *s, const float *d_signal, uint64_t steps, double *
             bulk_kernel<T, WIDE, SCALED><<<s->bulk_blocks, kBlock, smem, s->stream>>>(s->map_b[cur], s->map_a[prev],
                                                                                     s->map_t, s->map_s, args);
         }
+        if (ev) CUDA_TRY(s, cudaEventRecord(ev[1], s->stream));
+        if (ev) CUDA_TRY(s, cudaEventRecord(ev[2], s->stream));
         if (layer_blocks) layer_kernel<T, SCALED><<<layer_blocks, kBlock, 0, s->stream>>>(g, f);
+        if (ev) CUDA_TRY(s, cudaEventRecord(ev[3], s->stream));
+        if (ev) CUDA_TRY(s, cudaEventRecord(ev[4], s->side));
         if (special_blocks) {
             if (s->link_slots <= 6)
                 special_kernel<T, 6><<<special_blocks, kBlock, 0, s->side>>>(g, f);
             else
                 special_kernel<T, 18><<<special_blocks, kBlock, 0, s->side>>>(g, f);
         }
+        if (ev) CUDA_TRY(s, cudaEventRecord(ev[5], s->side));
+        if (ev) CUDA_TRY(s, cudaEventRecord(ev[6], s->side));
         if (probe_blocks) probe_kernel<T><<<probe_blocks, kBlock, 0, s->side>>>(g, f);
+        if (ev) CUDA_TRY(s, cudaEventRecord(ev[7], s->side));
         CUDA_TRY(s, cudaEventRecord(s->joined[0], s->stream));
         CUDA_TRY(s, cudaEventRecord(s->joined[1], s->side));
     }
@@ -372,6 +403,7 @@ int set_up(fdtd_solver *s) {
 // After `steps` steps the parity swap of fdtd.hpp:900-903: u[1] stays the current level.
 void settle(fdtd_solver *s, uint64_t steps) {
     if (steps % 2 == 1) {
+        s->flipped = !s->flipped;
         std::swap(s->u[0], s->u[1]);
         std::swap(s->w[0], s->w[1]);
         for (int axis = 0; axis < 3; ++axis) std::swap(s->faces[0][axis], s->faces[1][axis]);
@@ -390,6 +422,27 @@ int check_device_error(fdtd_solver *s) {
         CUDA_TRY(s, cudaMemsetAsync(s->d_error, 0, sizeof flag, s->stream));
         return fail(s, FDTD_ECUDA, "a pipeline wait of the interior sweep gave up; the step's results are not valid");
     }
+    return FDTD_OK;
+}
+
+// Captures the launches of kGraphSteps steps on the handle's chunk buffers, for the levels'
+// present roles, as one executable graph (its side-stream branch forked and joined by events).
+int capture(fdtd_solver *s, cudaGraphExec_t *out) {
+    const bool timing = s->timing;
+    s->timing = false;  // no timing events inside a graph
+    CUDA_TRY(s, cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+    const int rc = dispatch(s, s->d_sig, kGraphSteps, s->d_rec, kGraphSteps);
+    s->timing = timing;
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(s->stream, &graph);
+    if (rc != FDTD_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+    }
+    if (e != cudaSuccess) return cuda_fail(s, e, "cudaStreamEndCapture");
+    const cudaError_t i = cudaGraphInstantiate(out, graph, 0);
+    cudaGraphDestroy(graph);
+    if (i != cudaSuccess) return cuda_fail(s, i, "cudaGraphInstantiate");
     return FDTD_OK;
 }
 
@@ -451,6 +504,11 @@ int build(fdtd_solver *s, const fdtd_layout *L) {
     void *flag;
     if ((rc = zeros(s, sizeof(unsigned int), &flag))) return rc;
     s->d_error = static_cast<unsigned int *>(flag);
+    void *chunk;
+    if ((rc = zeros(s, sizeof(float) * kGraphSteps, &chunk))) return rc;
+    s->d_sig = static_cast<float *>(chunk);
+    if ((rc = zeros(s, sizeof(double) * kGraphSteps * std::max<uint64_t>(1, L->probe_count), &chunk))) return rc;
+    s->d_rec = static_cast<double *>(chunk);
 
     // The bulk sweep: tiles of kTX x kTY over the box, x from a 16-aligned start; chunks of planes
     // enough for every multiprocessor several times over.
@@ -466,16 +524,46 @@ int build(fdtd_solver *s, const fdtd_layout *L) {
         bk.xa = (uint32_t)(x0 / 16 * 16);
         bk.y0 = (uint32_t)y0, bk.z0 = (uint32_t)z0;
         bk.x1 = (uint32_t)x1, bk.y1 = (uint32_t)y1, bk.z1 = (uint32_t)z1;
-        bk.tiles_x = (uint32_t)((x1 - bk.xa + kTX - 1) / kTX);
-        bk.tiles_y = (uint32_t)((y1 - y0 + kTY - 1) / kTY);
-        const uint64_t columns = (uint64_t)bk.tiles_x * bk.tiles_y, depth = z1 - z0;
-        uint64_t chunk = depth;
-        while (chunk > 8 && columns * ((depth + chunk - 1) / chunk) < (uint64_t)s->sms * 8) chunk = (chunk + 1) / 2;
-        bk.chunk = (uint32_t)std::max<uint64_t>(chunk, 1);
-        bk.tiles_z = (uint32_t)((depth + bk.chunk - 1) / bk.chunk);
-        const uint64_t tiles = columns * bk.tiles_z;
-        if (tiles >= (1ull << 31)) return fail(s, FDTD_EINVAL, "the wave grid is too large for one launch");
-        s->bulk_tiles = (uint32_t)tiles;
+        // The tile list: the columns of kTX x kTY cells over the box, and in each the runs of
+        // planes that hold interior cells, cut into chunks of at most `chunk` planes, so that
+        // there are blocks enough for every multiprocessor several times over. Grids of many
+        // rooms (stacked along z) skip the planes between the rooms.
+        const uint64_t tiles_x = (x1 - bk.xa + kTX - 1) / kTX, tiles_y = (y1 - y0 + kTY - 1) / kTY;
+        const uint64_t columns = tiles_x * tiles_y;
+        std::vector<uint8_t> occupied(columns * nz, 0);
+        uint64_t planes = 0;
+        for (uint64_t z = z0; z < z1; ++z)
+            for (uint64_t y = y0; y < y1; ++y) {
+                const uint8_t *row = &L->types[nx * (y + ny * z)];
+                for (uint64_t x = x0; x < x1; ++x) {
+                    if (row[x] != kInterior) continue;
+                    uint8_t &o = occupied[((y - y0) / kTY * tiles_x + (x - bk.xa) / kTX) * nz + z];
+                    planes += o == 0;
+                    o = 1;
+                }
+            }
+        uint64_t chunk = 64;
+        while (chunk > 8 && planes / chunk < (uint64_t)s->sms * 8) chunk /= 2;
+        std::vector<int4> list;
+        for (uint64_t c = 0; c < columns; ++c) {
+            const int xt = (int)(bk.xa + (c % tiles_x) * kTX), yt = (int)(y0 + (c / tiles_x) * kTY);
+            for (uint64_t z = 0; z < nz;) {
+                if (!occupied[c * nz + z]) {
+                    ++z;
+                    continue;
+                }
+                uint64_t end = z;
+                while (end < nz && occupied[c * nz + end] && end - z < chunk) ++end;
+                list.push_back(make_int4(xt, yt, (int)z, (int)end));
+                z = end;
+            }
+        }
+        if (list.size() >= (1ull << 31)) return fail(s, FDTD_EINVAL, "the wave grid is too large for one launch");
+        s->bulk_tiles = (uint32_t)list.size();
+        bk.tiles = s->bulk_tiles;
+        const int4 *d_list;
+        if ((rc = upload(s, list.data(), list.size(), &d_list))) return rc;
+        bk.tile_list = d_list;
         const CUtensorMapDataType ft = s->precision == FDTD_FP64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
         for (int k = 0; k < 2; ++k) {
             if ((rc = tensor_map(s, &s->map_b[k], s->u[k], ft, (uint32_t)e, kBX, kBY))) return rc;
@@ -616,6 +704,9 @@ void release(fdtd_solver *s) {
     cudaGetDevice(&current);
     cudaSetDevice(s->device);
     if (s->stream) cudaStreamSynchronize(s->stream);
+    for (cudaGraphExec_t g : s->graph)
+        if (g) cudaGraphExecDestroy(g);
+    for (cudaEvent_t e : s->timing_events) cudaEventDestroy(e);
     for (void *p : s->allocations) cudaFree(p);
     if (s->stage_signal) cudaFreeHost(s->stage_signal);
     if (s->stage_out) cudaFreeHost(s->stage_out);
@@ -748,51 +839,79 @@ int fdtd_run(fdtd_solver *s, const float *signal, uint64_t steps, double *out) {
     if (steps == 0) return FDTD_OK;
     if (!signal || (s->probes && !out)) return fail(s, FDTD_EINVAL, "no signal or output buffer");
     DeviceGuard guard(s->device);
-    // Device staging in pieces of bounded size (the probes' records of a piece).
-    const uint64_t piece = std::min<uint64_t>(steps, std::max<uint64_t>(1024, (64ull << 20) / (8 * std::max<uint64_t>(1, s->probes))));
+    // Pinned host staging for a piece of the run (the drive and the probes' records), grown on
+    // demand; the device side is the handle's chunk buffers, kGraphSteps steps at a time.
+    const uint64_t P = std::max<uint64_t>(1, s->probes);
+    const uint64_t piece = std::min<uint64_t>(steps, std::max<uint64_t>(kGraphSteps, (64ull << 20) / (8 * P)));
     if (s->stage_steps < piece) {
         if (s->stage_signal) cudaFreeHost(s->stage_signal);
         if (s->stage_out) cudaFreeHost(s->stage_out);
         s->stage_signal = nullptr, s->stage_out = nullptr, s->stage_steps = 0;
         CUDA_TRY(s, cudaMallocHost((void **)&s->stage_signal, piece * sizeof(float)));
-        CUDA_TRY(s, cudaMallocHost((void **)&s->stage_out, piece * std::max<uint64_t>(1, s->probes) * sizeof(double)));
+        CUDA_TRY(s, cudaMallocHost((void **)&s->stage_out, piece * P * sizeof(double)));
         s->stage_steps = piece;
-    }
-    // Device copies: the signal and the records of one piece.
-    float *d_signal = nullptr;
-    double *d_out = nullptr;
-    CUDA_TRY(s, cudaMallocAsync((void **)&d_signal, piece * sizeof(float), s->stream));
-    cudaError_t e = cudaMallocAsync((void **)&d_out, piece * std::max<uint64_t>(1, s->probes) * sizeof(double), s->stream);
-    if (e != cudaSuccess) {
-        cudaFreeAsync(d_signal, s->stream);
-        return cuda_fail(s, e, "cudaMallocAsync");
     }
     int rc = FDTD_OK;
     for (uint64_t begin = 0; begin < steps && rc == FDTD_OK; begin += piece) {
         const uint64_t count = std::min(piece, steps - begin);
         std::memcpy(s->stage_signal, signal + begin, count * sizeof(float));
-        e = cudaMemcpyAsync(d_signal, s->stage_signal, count * sizeof(float), cudaMemcpyHostToDevice, s->stream);
-        if (e != cudaSuccess) { rc = cuda_fail(s, e, "cudaMemcpyAsync"); break; }
-        rc = dispatch(s, d_signal, count, d_out, count);
-        if (rc != FDTD_OK) break;
-        settle(s, count);
-        if (s->probes) {
-            e = cudaMemcpyAsync(s->stage_out, d_out, count * s->probes * sizeof(double), cudaMemcpyDeviceToHost, s->stream);
-            if (e != cudaSuccess) { rc = cuda_fail(s, e, "cudaMemcpyAsync"); break; }
+        for (uint64_t done = 0; done < count && rc == FDTD_OK;) {
+            const uint64_t chunk = std::min<uint64_t>(kGraphSteps, count - done);
+            CUDA_TRY(s, cudaMemcpyAsync(s->d_sig, s->stage_signal + done, chunk * sizeof(float), cudaMemcpyHostToDevice,
+                                        s->stream));
+            if (chunk == kGraphSteps) {
+                // A whole chunk: the captured graph of its steps for the levels' present roles.
+                cudaGraphExec_t &graph = s->graph[s->flipped ? 1 : 0];
+                if (!graph && (rc = capture(s, &graph)) != FDTD_OK) break;
+                CUDA_TRY(s, cudaGraphLaunch(graph, s->stream));
+            } else if ((rc = dispatch(s, s->d_sig, chunk, s->d_rec, kGraphSteps)) != FDTD_OK) {
+                break;
+            }
+            settle(s, chunk);
+            if (s->probes) {
+                CUDA_TRY(s, cudaMemcpy2DAsync(s->stage_out + done, count * sizeof(double), s->d_rec,
+                                              kGraphSteps * sizeof(double), chunk * sizeof(double), s->probes,
+                                              cudaMemcpyDeviceToHost, s->stream));
+            }
+            done += chunk;
         }
-        e = cudaStreamSynchronize(s->stream);
-        if (e != cudaSuccess) { rc = cuda_fail(s, e, "cudaStreamSynchronize"); break; }
+        if (rc != FDTD_OK) break;
+        CUDA_TRY(s, cudaStreamSynchronize(s->stream));
         for (uint64_t p = 0; p < s->probes; ++p)
             std::memcpy(out + p * steps + begin, s->stage_out + p * count, count * sizeof(double));
     }
-    cudaFreeAsync(d_signal, s->stream);
-    cudaFreeAsync(d_out, s->stream);
     if (rc != FDTD_OK) return rc;
     CUDA_TRY(s, cudaStreamSynchronize(s->stream));
     if ((rc = check_device_error(s)) != FDTD_OK) return rc;
     for (uint64_t k = 0; k < s->probes * steps; ++k) {
         if (!std::isfinite(out[k])) return fail(s, FDTD_ENONFINITE, "the wave solver's run did not stay finite");
     }
+    return FDTD_OK;
+}
+
+int fdtd_set_timing(fdtd_solver *s, int enable) {
+    if (!s) return set_global(FDTD_EINVAL, "no solver");
+    s->timing = enable != 0;
+    return FDTD_OK;
+}
+
+int fdtd_get_timing(fdtd_solver *s, double ms[4], uint64_t *steps) {
+    if (!s || !ms) return set_global(FDTD_EINVAL, "no solver or buffer");
+    DeviceGuard guard(s->device);
+    CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+    CUDA_TRY(s, cudaStreamSynchronize(s->side));
+    for (int k = 0; k < 4; ++k) ms[k] = 0.0;
+    for (size_t base = 0; base + 8 <= s->timing_events.size(); base += 8) {
+        for (int k = 0; k < 4; ++k) {
+            float t = 0.0f;
+            CUDA_TRY(s, cudaEventElapsedTime(&t, s->timing_events[base + 2 * k], s->timing_events[base + 2 * k + 1]));
+            ms[k] += t;
+        }
+    }
+    if (steps) *steps = s->timed_steps;
+    for (cudaEvent_t e : s->timing_events) cudaEventDestroy(e);
+    s->timing_events.clear();
+    s->timed_steps = 0;
     return FDTD_OK;
 }
 

@@ -62,7 +62,10 @@ struct BulkArgs {
     void *a;  // the previous pressure, overwritten with the next (T)
     uint32_t pitch, ny;
     uint32_t xa, y0, z0, x1, y1, z1;  // tiles start at xa (16-aligned), y0, z0; the box ends x1, y1, z1
-    uint32_t tiles_x, tiles_y, tiles_z, chunk;
+    // The tiles that hold interior cells: {x, y, z0, z_end} each, x 16-aligned; a tile spans
+    // kTX x kTY cells from (x, y) and the planes z0 .. z_end-1.
+    const int4 *tile_list;
+    uint32_t tiles;
     float axial, diagonal, centre, total;
     unsigned int *error;  // set to 1 when a wait gives up
 };
@@ -124,8 +127,8 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map
 
 // ---- interior air ------------------------------------------------------------------------------
 
-// Interior air (fdtd.hpp:242-288). The box of the interior cells is cut into tiles of kTX x kTY
-// cells by a chunk of planes along z; each resident block (a persistent grid) takes tiles
+// Interior air (fdtd.hpp:242-288). The interior cells are covered by tiles of kTX x kTY cells by a
+// chunk of planes along z (a list, only tiles that hold interior cells); each block takes tiles
 // blockIdx.x, + gridDim.x, ... and marches each along z. Its planes' stages — plane k's pressure
 // tile with halos, previous pressure, types and scales — form one sequence over all its tiles:
 // tile m's stages are planes z0-1 .. z_end. Thread 0 issues the sequence with TMA, kAhead stages
@@ -140,16 +143,8 @@ struct TileSpan {
 };
 
 __device__ __forceinline__ TileSpan tile_span(const BulkArgs &p, uint32_t tile) {
-    const uint32_t bx = tile % p.tiles_x;
-    tile /= p.tiles_x;
-    const uint32_t by = tile % p.tiles_y;
-    const uint32_t bz = tile / p.tiles_y;
-    TileSpan t;
-    t.xt = (int)(p.xa + bx * kTX);
-    t.yt = (int)(p.y0 + by * kTY);
-    t.z0 = (int)(p.z0 + bz * p.chunk);
-    t.z_end = min(t.z0 + (int)p.chunk, (int)p.z1);
-    return t;
+    const int4 t = p.tile_list[tile];
+    return TileSpan{t.x, t.y, t.z, t.w};
 }
 
 template <typename T, bool WIDE, bool SCALED>
@@ -162,7 +157,7 @@ __global__ void __launch_bounds__(kBlock) bulk_kernel(const __grid_constant__ CU
     extern __shared__ __align__(128) unsigned char smem[];
     const uint32_t base = smem_address(smem);
     const uint32_t bars = base + kStages * S::bytes;
-    const uint32_t tiles = p.tiles_x * p.tiles_y * p.tiles_z;
+    const uint32_t tiles = p.tiles;
     if (blockIdx.x >= tiles) return;  // the whole block alike
 
     if (threadIdx.x == 0) {

@@ -236,10 +236,17 @@ def _layer_tables(size: int, layer: int, damping: float, courant: float):
     return f32(ck), f32(cp), f32(fk), f32(fp)
 
 
-def cell_face_layout(
+def cell_face_layout(room: Room, grid: Grid, source, probes, **options) -> Built:
+    """The reference's layout of ``room`` on ``grid`` with walls on cell faces, the 7-point
+    stencil, a uniform speed ratio ``speed`` (None: the grid's), the source at ``source`` and
+    the probes at ``probes`` (each at least two cells from every wall and from the layer)."""
+    return cell_face_layouts(room, grid, [source], probes, **options)[0]
+
+
+def cell_face_layouts(
     room: Room,
     grid: Grid,
-    source,
+    sources,
     probes,
     *,
     layer: int = 0,
@@ -247,10 +254,9 @@ def cell_face_layout(
     edge_admittance: float = 1.0,
     speed: float | None = None,
     rate: float | None = None,
-) -> Built:
-    """The reference's layout of ``room`` on ``grid`` with walls on cell faces, the 7-point
-    stencil, a uniform speed ratio ``speed`` (None: the grid's), the source at ``source`` and
-    the probes at ``probes`` (each at least two cells from every wall and from the layer)."""
+) -> list[Built]:
+    """The layouts of one room with each of ``sources`` in turn (the same probes): the room's
+    rows are worked out once."""
     nx, ny, nz = grid.shape
     n = grid.n
     sy, sz = nx, nx * ny
@@ -396,101 +402,108 @@ def cell_face_layout(
     special = list(boundary.astype(np.int64))
     link_start = np.concatenate([[0], np.cumsum(links_per_row)]).astype(np.uint64)
     state_start = np.concatenate([[0], np.cumsum(states_per_row)]).astype(np.uint64)
-    source_values = np.zeros(B, np.float32)
+    base_types = types
 
-    # The source's cells (fdtd.hpp:627-638): made special with the stencil's own weights, each
-    # source term summed in float as the reference's source_[k] += float(s w).
-    extra_link_dir: list[np.ndarray] = []
-    accumulated: dict[int, np.float32] = {}
-    made: dict[int, int] = {}
-    for ci, w in cubic_cells(grid, source):
-        t = types[ci]
-        if t == 3:
-            raise ValueError("the source is in the matched layer")
-        if t == 0:
-            raise ValueError("the source sees no cell of the wave grid")
-        if t == 2:
-            k = made.get(ci)
-            if k is None:
-                k = int(np.searchsorted(boundary, ci))
-                if k >= B or boundary[k] != ci:
-                    raise ValueError("a source cell is special but not a boundary row")
-        else:
-            types[ci] = 2
-            k = len(special)
-            special.append(ci)
-            made[ci] = k
-            extra_link_dir.append(np.arange(6, dtype=np.uint8))
-        accumulated[k] = np.float32(accumulated.get(k, np.float32(0.0)) + np.float32(s * w))
-    E = len(made)
-    extra_source = np.zeros(E, np.float32)
-    for k, value in accumulated.items():
-        if k < B:
-            source_values[k] = value
-        else:
-            extra_source[k - B] = value
-    exact_total = 0.0
-    for _ in range(6):
-        exact_total += AXIAL
-    extra_coef_a = np.full(E, np.float32(2.0 - s * exact_total * (1.0 - MARGIN)), np.float32)
+    def place(source) -> Built:
+        types = base_types.copy()
+        special = list(base_special)
+        source_values = np.zeros(B, np.float32)
 
-    layout: dict[str, np.ndarray] = {}
-    weights = np.full(6, lowered(AXIAL), np.float32)
-    tot = 0.0
-    for w in weights:
-        tot += float(w)
-    layout["shape"] = np.array(grid.shape, np.uint64)
-    layout["stencil"] = np.array([7], np.uint64)
-    layout["weights"] = weights
-    layout["centre"] = np.array([2.0 - tot], np.float32)
-    layout["total"] = np.array([tot], np.float32)
-    layout["scaled"] = np.array([0 if speed is None else 1], np.uint64)
-    layout["scale"] = np.full(n, np.float32(s), np.float32) if speed is not None else np.zeros(0, np.float32)
-    layout["layer_scale"] = (
-        np.full(len(layer_cells), np.float32(s), np.float32) if speed is not None else np.zeros(0, np.float32)
-    )
-    layout["types"] = types
-    layout["special"] = np.array(special, np.int64)
-    layout["link_start"] = np.concatenate([link_start, link_start[-1] + 6 * np.arange(1, E + 1, dtype=np.uint64)])
-    layout["link_direction"] = np.concatenate([link_direction] + extra_link_dir).astype(np.uint8)
-    layout["link_weight"] = np.full(len(layout["link_direction"]), link_w, np.float32)
-    layout["coef_a"] = np.concatenate([coef_a, extra_coef_a])
-    layout["coef_b"] = np.concatenate([coef_b, np.ones(E, np.float32)])
-    layout["coef_inv"] = np.concatenate([coef_inv, np.ones(E, np.float32)])
-    layout["source"] = np.concatenate([source_values, extra_source])
-    layout["state_start"] = np.concatenate([state_start, np.full(E, state_start[-1], np.uint64)])
-    layout["state_branch"] = st_branch.astype(np.int32)
-    layout["state_weight"] = st_weight.astype(np.float32)
-    layout["branch_now"] = branch_now
-    layout["branch_before"] = branch_before
-    layout["branch_gain"] = branch_gain
-    layout["layer_cells"] = layer_cells
-    courant = math.sqrt(float(weights[0]))
-    for a, name in enumerate("xyz"):
-        if len(layer_cells):
-            ck, cp, fk, fp = _layer_tables(grid.shape[a], layer, layer_damping, courant)
-        else:
-            ck = cp = fk = fp = np.zeros(0, np.float32)
-        layout[f"keep_{name}"], layout[f"push_{name}"] = ck, cp
-        layout[f"keep_face_{name}"], layout[f"push_face_{name}"] = fk, fp
-    starts, cells, pweights = [0], [], []
-    for p in np.asarray(probes, float).reshape(-1, 3):
-        if np.linalg.norm(p - np.asarray(source, float)) < (3.0 - 1e-9) * grid.cell:
-            # the reference reads such a probe from the eight cells round it (fdtd.hpp:645-646)
-            raise ValueError("a probe lies within three cells of the source")
-        for ci, w in cubic_cells(grid, p):
-            if types[ci] not in (1, 2):
-                raise ValueError("a probe reads a cell outside the air")
-            cells.append(ci)
-            pweights.append(w)
-        starts.append(len(cells))
-    layout["probe_start"] = np.array(starts, np.uint64)
-    layout["probe_cells"] = np.array(cells, np.uint64)
-    layout["probe_weights"] = np.array(pweights, np.float64)
-    layout["flow_mask"] = np.zeros(0, np.uint8)
-    air_cells = int(np.count_nonzero(types))
-    return Built(layout, grid, air_cells, B, E, rate or 0.0)
+        # The source's cells (fdtd.hpp:627-638): made special with the stencil's own weights, each
+        # source term summed in float as the reference's source_[k] += float(s w).
+        extra_link_dir: list[np.ndarray] = []
+        accumulated: dict[int, np.float32] = {}
+        made: dict[int, int] = {}
+        for ci, w in cubic_cells(grid, source):
+            t = types[ci]
+            if t == 3:
+                raise ValueError("the source is in the matched layer")
+            if t == 0:
+                raise ValueError("the source sees no cell of the wave grid")
+            if t == 2:
+                k = made.get(ci)
+                if k is None:
+                    k = int(np.searchsorted(boundary, ci))
+                    if k >= B or boundary[k] != ci:
+                        raise ValueError("a source cell is special but not a boundary row")
+            else:
+                types[ci] = 2
+                k = len(special)
+                special.append(ci)
+                made[ci] = k
+                extra_link_dir.append(np.arange(6, dtype=np.uint8))
+            accumulated[k] = np.float32(accumulated.get(k, np.float32(0.0)) + np.float32(s * w))
+        E = len(made)
+        extra_source = np.zeros(E, np.float32)
+        for k, value in accumulated.items():
+            if k < B:
+                source_values[k] = value
+            else:
+                extra_source[k - B] = value
+        exact_total = 0.0
+        for _ in range(6):
+            exact_total += AXIAL
+        extra_coef_a = np.full(E, np.float32(2.0 - s * exact_total * (1.0 - MARGIN)), np.float32)
 
+        layout: dict[str, np.ndarray] = {}
+        weights = np.full(6, lowered(AXIAL), np.float32)
+        tot = 0.0
+        for w in weights:
+            tot += float(w)
+        layout["shape"] = np.array(grid.shape, np.uint64)
+        layout["stencil"] = np.array([7], np.uint64)
+        layout["weights"] = weights
+        layout["centre"] = np.array([2.0 - tot], np.float32)
+        layout["total"] = np.array([tot], np.float32)
+        layout["scaled"] = np.array([0 if speed is None else 1], np.uint64)
+        layout["scale"] = np.full(n, np.float32(s), np.float32) if speed is not None else np.zeros(0, np.float32)
+        layout["layer_scale"] = (
+            np.full(len(layer_cells), np.float32(s), np.float32) if speed is not None else np.zeros(0, np.float32)
+        )
+        layout["types"] = types
+        layout["special"] = np.array(special, np.int64)
+        layout["link_start"] = np.concatenate([link_start, link_start[-1] + 6 * np.arange(1, E + 1, dtype=np.uint64)])
+        layout["link_direction"] = np.concatenate([link_direction] + extra_link_dir).astype(np.uint8)
+        layout["link_weight"] = np.full(len(layout["link_direction"]), link_w, np.float32)
+        layout["coef_a"] = np.concatenate([coef_a, extra_coef_a])
+        layout["coef_b"] = np.concatenate([coef_b, np.ones(E, np.float32)])
+        layout["coef_inv"] = np.concatenate([coef_inv, np.ones(E, np.float32)])
+        layout["source"] = np.concatenate([source_values, extra_source])
+        layout["state_start"] = np.concatenate([state_start, np.full(E, state_start[-1], np.uint64)])
+        layout["state_branch"] = st_branch.astype(np.int32)
+        layout["state_weight"] = st_weight.astype(np.float32)
+        layout["branch_now"] = branch_now
+        layout["branch_before"] = branch_before
+        layout["branch_gain"] = branch_gain
+        layout["layer_cells"] = layer_cells
+        courant = math.sqrt(float(weights[0]))
+        for a, name in enumerate("xyz"):
+            if len(layer_cells):
+                ck, cp, fk, fp = _layer_tables(grid.shape[a], layer, layer_damping, courant)
+            else:
+                ck = cp = fk = fp = np.zeros(0, np.float32)
+            layout[f"keep_{name}"], layout[f"push_{name}"] = ck, cp
+            layout[f"keep_face_{name}"], layout[f"push_face_{name}"] = fk, fp
+        starts, cells, pweights = [0], [], []
+        for p in np.asarray(probes, float).reshape(-1, 3):
+            if np.linalg.norm(p - np.asarray(source, float)) < (3.0 - 1e-9) * grid.cell:
+                # the reference reads such a probe from the eight cells round it (fdtd.hpp:645-646)
+                raise ValueError("a probe lies within three cells of the source")
+            for ci, w in cubic_cells(grid, p):
+                if types[ci] not in (1, 2):
+                    raise ValueError("a probe reads a cell outside the air")
+                cells.append(ci)
+                pweights.append(w)
+            starts.append(len(cells))
+        layout["probe_start"] = np.array(starts, np.uint64)
+        layout["probe_cells"] = np.array(cells, np.uint64)
+        layout["probe_weights"] = np.array(pweights, np.float64)
+        layout["flow_mask"] = np.zeros(0, np.uint8)
+        air_cells = int(np.count_nonzero(types))
+        return Built(layout, grid, air_cells, B, E, rate or 0.0)
+
+    base_special = special
+    return [place(source) for source in sources]
 
 
 # ---- seeded synthetic rooms ------------------------------------------------------------------
@@ -661,3 +674,213 @@ def polyhedral_room(
         "seed": seed,
     }
     return Workload("polyhedral_room", room, built, points[0], points[1:], gaussian_drive(rate, steps), description)
+
+
+# ---- many rooms in one grid ------------------------------------------------------------------
+
+
+def paris_absorption(impedance):
+    """Random-incidence absorption of a locally reacting surface of real normalised impedance z,
+    Paris's formula for a diffuse field: 8/z (1 + 1/(1+z) - 2/z ln(1+z))
+    (engine/impedance.py:52-56 of the reference states the same formula)."""
+    z = np.asarray(impedance, float)
+    return 8.0 / z * (1.0 + 1.0 / (1.0 + z) - 2.0 / z * np.log1p(z))
+
+
+def paris_admittance(absorption):
+    """The real admittance 1/z whose random-incidence absorption is ``absorption``, on the side of
+    hard surfaces (z above the impedance of the most absorbing real surface, about 1.5672): the
+    inverse of :func:`paris_absorption` by bisection in log z."""
+    alpha = np.clip(np.asarray(absorption, float), 0.0, 1.0)
+    low = np.full(alpha.shape, math.log(1.5672))
+    high = np.full(alpha.shape, math.log(1e9))
+    for _ in range(60):
+        mid = 0.5 * (low + high)
+        above = paris_absorption(np.exp(mid)) > alpha
+        low = np.where(above, mid, low)
+        high = np.where(above, high, mid)
+    return np.where(alpha <= 0.0, 0.0, np.exp(-0.5 * (low + high)))
+
+
+def shoebox(size, materials) -> Room:
+    """A closed box room from the origin to ``size``: its six walls -x, +x, -y, +y, -z, +z with
+    ``materials``."""
+    normals, offsets = [], []
+    for a in range(3):
+        for sign in (-1.0, 1.0):
+            nrm = np.zeros(3)
+            nrm[a] = sign
+            normals.append(nrm)
+            offsets.append(size[a] if sign > 0 else 0.0)
+    return Room(np.array(normals), np.array(offsets), list(materials))
+
+
+def room_grid(size, cell: float) -> Grid:
+    """The grid of a box room as the reference's tests lay it out (tests/test_wave.py:80-82): the
+    origin two cells and a fraction of a cell below the room, two cells beyond it."""
+    origin = -cell * (2.0 + OFFSET)
+    shape = tuple(int(v) for v in np.ceil((np.asarray(size, float) - origin) / cell).astype(int) + 2)
+    return Grid(origin, cell, shape)
+
+
+@dataclass
+class Stacked:
+    """Layouts of several grids stepped as one: ``layout`` the combined grid; ``parts[k]`` the k-th
+    input's (first probe, last probe + 1, air cells, first plane)."""
+
+    layout: dict[str, np.ndarray]
+    parts: list[tuple[int, int, int, int]]
+
+    @property
+    def air_cells(self) -> int:
+        return sum(part[2] for part in self.parts)
+
+
+def stack(layouts: list[dict[str, np.ndarray]]) -> Stacked:
+    """One layout of many grids without matched layers: grid k's cells at its own (x, y) of a
+    plane of the largest nx x ny, its planes after grid k-1's. Each grid's outermost layer of cells
+    is never air, so no link joins two grids, and each grid is stepped exactly as on its own:
+    every row keeps its coefficients, every link its neighbour."""
+    first = layouts[0]
+    for lay in layouts:
+        if int(lay["stencil"][0]) != int(first["stencil"][0]) or not np.array_equal(lay["weights"], first["weights"]):
+            raise ValueError("the grids to stack have different stencils")
+        if not (np.array_equal(lay["centre"], first["centre"]) and np.array_equal(lay["total"], first["total"])):
+            raise ValueError("the grids to stack have different centres")
+        if int(lay["scaled"][0]) != int(first["scaled"][0]):
+            raise ValueError("the grids to stack are not all scaled or all unscaled")
+        if len(lay["layer_cells"]):
+            raise ValueError("grids with a matched layer cannot be stacked (its tables are the grid's own)")
+        if len(lay.get("flow_mask", [])):
+            raise ValueError("moving air cannot be stacked")
+    shapes = [tuple(int(v) for v in lay["shape"]) for lay in layouts]
+    NX = max(s[0] for s in shapes)
+    NY = max(s[1] for s in shapes)
+    NZ = sum(s[2] for s in shapes)
+    scaled = int(first["scaled"][0]) == 1
+    types = np.zeros((NZ, NY, NX), np.uint8)
+    scale = np.ones((NZ, NY, NX), np.float32) if scaled else None
+    z0 = 0
+    out = {k: [] for k in ("special", "link_direction", "link_weight", "coef_a", "coef_b", "coef_inv", "source",
+                           "state_branch", "state_weight", "branch_now", "branch_before", "branch_gain",
+                           "probe_cells", "probe_weights")}  # fmt: skip
+    link_start, state_start, probe_start = [np.zeros(1, np.uint64)], [np.zeros(1, np.uint64)], [np.zeros(1, np.uint64)]
+    links = states = branches = probes = reads = 0
+    parts = []
+
+    def mapped(index, shape, z_first):
+        nx, ny, _ = shape
+        i = np.asarray(index, np.int64)
+        return (i % nx) + NX * ((i // nx) % ny + NY * (i // (nx * ny) + z_first))
+
+    for lay, shape in zip(layouts, shapes):
+        nx, ny, nz = shape
+        t = np.asarray(lay["types"]).reshape(nz, ny, nx)
+        types[z0 : z0 + nz, :ny, :nx] = t
+        if scaled:
+            scale[z0 : z0 + nz, :ny, :nx] = np.asarray(lay["scale"]).reshape(nz, ny, nx)
+        out["special"].append(mapped(lay["special"], shape, z0))
+        for name in ("link_direction", "link_weight", "coef_a", "coef_b", "coef_inv", "source", "state_weight",
+                     "branch_now", "branch_before", "branch_gain", "probe_weights"):  # fmt: skip
+            out[name].append(np.asarray(lay[name]))
+        out["state_branch"].append(np.asarray(lay["state_branch"], np.int64) + branches)
+        out["probe_cells"].append(mapped(lay["probe_cells"], shape, z0).astype(np.uint64))
+        link_start.append(np.asarray(lay["link_start"], np.uint64)[1:] + np.uint64(links))
+        state_start.append(np.asarray(lay["state_start"], np.uint64)[1:] + np.uint64(states))
+        probe_start.append(np.asarray(lay["probe_start"], np.uint64)[1:] + np.uint64(reads))
+        p = len(lay["probe_start"]) - 1
+        parts.append((probes, probes + p, int(np.count_nonzero(t)), z0))
+        links += len(lay["link_direction"])
+        states += len(lay["state_branch"])
+        branches += len(lay["branch_now"])
+        probes += p
+        reads += len(lay["probe_cells"])
+        z0 += nz
+    layout = {
+        "shape": np.array([NX, NY, NZ], np.uint64),
+        "stencil": np.asarray(first["stencil"]).copy(),
+        "weights": np.asarray(first["weights"]).copy(),
+        "centre": np.asarray(first["centre"]).copy(),
+        "total": np.asarray(first["total"]).copy(),
+        "scaled": np.asarray(first["scaled"]).copy(),
+        "scale": scale.reshape(-1) if scaled else np.zeros(0, np.float32),
+        "layer_scale": np.zeros(0, np.float32),
+        "types": types.reshape(-1),
+        "link_start": np.concatenate(link_start),
+        "state_start": np.concatenate(state_start),
+        "probe_start": np.concatenate(probe_start),
+        "layer_cells": np.zeros(0, np.int64),
+        "flow_mask": np.zeros(0, np.uint8),
+        **{k: np.zeros(0, np.float32) for k in ("keep_x", "keep_face_x", "keep_y", "keep_face_y", "keep_z",
+                                                 "keep_face_z", "push_x", "push_face_x", "push_y", "push_face_y",
+                                                 "push_z", "push_face_z")},  # fmt: skip
+    }
+    dtypes = {"special": np.int64, "link_direction": np.uint8, "state_branch": np.int32, "probe_cells": np.uint64,
+              "probe_weights": np.float64}  # fmt: skip
+    for name, pieces in out.items():
+        layout[name] = np.concatenate(pieces).astype(dtypes.get(name, np.float32))
+    return Stacked(layout, parts)
+
+
+@dataclass
+class Batch:
+    """Many rooms with several sources each, stacked into one grid."""
+
+    stacked: Stacked
+    layouts: list[dict[str, np.ndarray]]  # each solve's own layout (room, source)
+    signal: np.ndarray
+    rate: float
+    description: dict
+
+
+def batched_rooms(
+    seed: int = 0,
+    *,
+    rooms: int = 64,
+    sources: int = 4,
+    cell: float = 0.05,
+    dims=(3.0, 12.0),
+    absorption=(0.02, 0.5),
+    receivers: int = 4,
+    steps: int = 6000,
+    speed_of_sound: float = 343.0,
+) -> Batch:
+    """``rooms`` seeded shoebox rooms of dims uniform in ``dims`` metres per axis on cells of
+    ``cell`` metres, each wall's absorption uniform in ``absorption`` (a real admittance by Paris's
+    formula), each room with ``sources`` seeded source positions (separate solves) and
+    ``receivers`` receivers, all at least 0.5 m from the walls; one 0.5 ms Gaussian drive. Every
+    (room, source) is a solve of its own, and all are stacked into one grid."""
+    rng = np.random.default_rng(seed)
+    rate = speed_of_sound / (COURANT * cell)
+    layouts, cells = [], []
+    for _ in range(rooms):
+        size = rng.uniform(dims[0], dims[1], 3)
+        betas = paris_admittance(rng.uniform(absorption[0], absorption[1], 6))
+        room = shoebox(size, [Material(float(b)) for b in betas])
+        points = inside_points(rng, room, size, sources + receivers, 0.5, apart=0.0)
+        src, rec = points[:sources], points[sources:]
+        # every receiver three cells at least from every source (the reference's cubic reading)
+        for k in range(len(rec)):
+            while np.min(np.linalg.norm(src - rec[k], axis=1)) < 4 * cell:
+                rec[k] = inside_points(rng, room, size, 1, 0.5)[0]
+        grid = room_grid(size, cell)
+        for built in cell_face_layouts(room, grid, list(src), rec, rate=rate):
+            layouts.append(built.layout)
+            cells.append(built.air_cells)
+    stacked = stack(layouts)
+    description = {
+        "rooms": rooms,
+        "sources_per_room": sources,
+        "solves": len(layouts),
+        "cell_m": cell,
+        "air_cells": int(sum(cells)),
+        "smallest_solve_cells": int(min(cells)),
+        "largest_solve_cells": int(max(cells)),
+        "stacked_grid": "x".join(str(int(v)) for v in stacked.layout["shape"]),
+        "receivers_per_room": receivers,
+        "steps": steps,
+        "rate_hz": rate,
+        "walls": "cell faces, real admittance per wall from absorption U[%g, %g]" % absorption,
+        "seed": seed,
+    }
+    return Batch(stacked, layouts, gaussian_drive(rate, steps), rate, description)

@@ -157,6 +157,22 @@ class B200WaveSolver:
         """The address of the solver's CUDA stream (for events and ordering)."""
         return int(self._lib.fdtd_stream(self._handle) or 0)
 
+    def set_timing(self, enable: bool) -> None:
+        """Brackets each kernel of the following run_device steps with CUDA events."""
+        status = self._lib.fdtd_set_timing(self._handle, int(bool(enable)))
+        if status != _abi.FDTD_OK:
+            _raise(self._lib, status, self._handle)
+
+    def timing(self) -> dict[str, float]:
+        """Milliseconds per kind of kernel summed over the steps timed since the last call, and
+        the steps: {"bulk", "layer", "special", "probe", "steps"}."""
+        ms = (ctypes.c_double * 4)()
+        steps = ctypes.c_uint64()
+        status = self._lib.fdtd_get_timing(self._handle, ms, ctypes.byref(steps))
+        if status != _abi.FDTD_OK:
+            _raise(self._lib, status, self._handle)
+        return {"bulk": ms[0], "layer": ms[1], "special": ms[2], "probe": ms[3], "steps": int(steps.value)}
+
     def synchronize(self) -> None:
         status = self._lib.fdtd_synchronize(self._handle)
         if status != _abi.FDTD_OK:

@@ -48,7 +48,9 @@ BYTES_INTERIOR = 12  # read p, read p-, write p+
 BYTES_SPECIAL = 40  # read p, read/write p-, coef_a/b/inv/source, its index and two table starts
 BYTES_LINK = 5  # direction and weight
 BYTES_STATE = 28  # read/write w-, read w, its four coefficients
-BYTES_LAYER = 84  # read p, write p+, read/write nine state values, its index
+# A layer cell keeps three pressure parts and, on the cell below each face, one velocity per
+# face (the reference's nine values per cell hold every face twice, 84 B):
+BYTES_LAYER = 60  # read p, write p+, read/write three parts, read/write three faces, its index
 
 
 def algorithmic_bytes(d: dict) -> int:
@@ -59,6 +61,31 @@ def algorithmic_bytes(d: dict) -> int:
         + BYTES_STATE * d["branch_states"]
         + BYTES_LAYER * d["layer_cells"]
     )
+
+
+def ir_errors(p32: np.ndarray, p64: np.ndarray, rate: float) -> dict:
+    """FP32 against FP64 impulse responses (probes, steps): the relative L2 error of each receiver,
+    and of its energy-decay curve (Schroeder's backward integral) the largest difference in dB
+    down to 60 dB below its start."""
+    energy = np.linalg.norm(p64, axis=1)
+    reached = energy > 1e-3 * energy.max()  # receivers the sound has reached
+    rel = np.linalg.norm(p32 - p64, axis=1)[reached] / energy[reached]
+    worst_db = 0.0
+    for a, b in zip(p32[reached], p64[reached]):
+        ea = np.cumsum((a * a)[::-1])[::-1]
+        eb = np.cumsum((b * b)[::-1])[::-1]
+        keep = eb > eb[0] * 1e-6
+        if np.any(keep) and eb[0] > 0:
+            da = 10 * np.log10(np.maximum(ea[keep], 1e-300) / ea[0])
+            db = 10 * np.log10(eb[keep] / eb[0])
+            worst_db = max(worst_db, float(np.max(np.abs(da - db))))
+    return {
+        "ir_rel_l2_max": float(rel.max()),
+        "ir_rel_l2_median": float(np.median(rel)),
+        "edc_db_max_abs": worst_db,
+        "seconds": float(p64.shape[1] / rate),
+        "receivers": int(reached.sum()),
+    }
 
 
 def measured_peaks() -> tuple[float, str]:
@@ -222,6 +249,92 @@ def run_reference(args, rank: int, world: int) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_batched(args, world: int, rank: int, local: int) -> None:
+    """The batched configuration: many shoebox rooms with several sources each, every (room,
+    source) a solve of its own, stacked into one grid and stepped by one launch per kind per step
+    Beside it, a sample of the same solves stepped one after another through
+    the same public API, and each solve's FP32 error against FP64."""
+    import torch
+
+    from acoustic_spaces_b200 import B200WaveSolver, layouts
+
+    batch = layouts.batched_rooms(args.seed, rooms=args.rooms, sources=args.sources, steps=args.steps + args.warmup)
+    desc = batch.description
+    solver = B200WaveSolver(batch.stacked.layout, device=local)
+    air = batch.stacked.air_cells
+    steps, warmup = args.steps, args.warmup
+    sig = torch.from_numpy(np.ascontiguousarray(batch.signal)).to(f"cuda:{local}")
+    out = torch.zeros((solver.probes, steps + warmup), dtype=torch.float64, device=f"cuda:{local}")
+    stream = torch.cuda.ExternalStream(solver.stream, device=f"cuda:{local}")
+    solver.run_device(sig.data_ptr(), warmup, out.data_ptr(), steps + warmup)
+    solver.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clocks:
+        torch.cuda.synchronize()
+        start.record(stream)
+        solver.run_device(sig.data_ptr() + 4 * warmup, steps, out.data_ptr() + 8 * warmup, steps + warmup)
+        end.record(stream)
+        solver.synchronize()
+        torch.cuda.synchronize()
+    ms = start.elapsed_time(end)
+    value = air * steps / (ms / 1e3) / 1e9
+    # End to end, the whole batch through the public API.
+    solver.reset()
+    t0 = time.perf_counter()
+    solver.run(batch.signal[:steps])
+    e2e_s = time.perf_counter() - t0
+    # A sample of the solves one after another (each its own grid), through the same API.
+    rng = np.random.default_rng(1)
+    sample = sorted(rng.choice(len(batch.layouts), size=min(args.sequential_sample, len(batch.layouts)), replace=False))
+    seq_cells, seq_s = 0, 0.0
+    for k in sample:
+        one = B200WaveSolver(batch.layouts[k], device=local)
+        one.run(batch.signal[:warmup])
+        one.reset()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        one.run(batch.signal[:steps])
+        seq_s += time.perf_counter() - t0
+        seq_cells += one.air_cells * steps
+        one.close()
+    sequential = seq_cells / seq_s / 1e9
+    # Each solve's FP32 response against FP64 (the stacked grid in both).
+    m = min(args.ir_steps, steps)
+    solver.reset()
+    p32 = solver.run(batch.signal[:m])
+    fp64 = B200WaveSolver(batch.stacked.layout, precision="fp64", device=local)
+    p64 = fp64.run(batch.signal[:m])
+    fp64.close()
+    worst = []
+    for p0, p1, _, _ in batch.stacked.parts:
+        worst.append(ir_errors(p32[p0:p1], p64[p0:p1], batch.rate)["ir_rel_l2_max"])
+    line = {
+        "metric": METRIC,
+        "value": round(value, 4),
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": steps,
+        "warmup": warmup,
+        "ms_per_step": round(ms / steps, 5),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": "batched_rooms", **desc, "parallelism": "single GPU"},
+        "e2e": {"value": round(air * steps / e2e_s / 1e9, 4), "unit": UNIT, "h2d_bytes_per_step": 4,
+                "d2h_bytes_per_step": 8 * solver.probes},  # fmt: skip
+        "sequential_solves": {"value": round(sequential, 4), "unit": UNIT, "solves_timed": len(sample),
+                              "api": "B200WaveSolver.run, one solve after another"},  # fmt: skip
+        "batched_over_sequential": round(value / sequential, 3),
+        "per_solve_ir_rel_l2_vs_fp64": {"max": float(max(worst)), "median": float(np.median(worst)), "steps": m},
+        "clocks": clocks.summary(),
+        "gpu_launches": 4 * steps,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     parser = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     parser.add_argument("--gpus", type=int, default=1)
@@ -235,6 +348,12 @@ def main() -> None:
     parser.add_argument("--reference-repeats", type=int, default=3)
     parser.add_argument("--no-cpu-baseline", action="store_true")
     parser.add_argument("--no-e2e", action="store_true")
+    parser.add_argument("--workload", choices=["polyhedral_room", "batched_rooms"], default="polyhedral_room")
+    parser.add_argument("--rooms", type=int, default=64)
+    parser.add_argument("--sources", type=int, default=4)
+    parser.add_argument("--sequential-sample", type=int, default=16)
+    parser.add_argument("--no-ir-error", action="store_true")
+    parser.add_argument("--ir-steps", type=int, default=2000, help="steps of the FP32-vs-FP64 comparison")
     args = parser.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -253,6 +372,9 @@ def main() -> None:
     if not torch.cuda.is_available():
         raise SystemExit("bench.py needs a CUDA device (the B200 stepper has no CPU path)")
     torch.cuda.set_device(local)
+    if args.workload == "batched_rooms":
+        run_batched(args, world, rank, local)
+        return
     if world > 1:
         from datetime import timedelta
 
@@ -284,6 +406,7 @@ def main() -> None:
         barrier()
         torch.cuda.synchronize()
         solver.synchronize()
+        solver.set_timing(True)  # CUDA events around each kernel, on its own stream
         with torch.cuda.stream(stream):
             start.record(stream)
         solver.run_device(sig_dev.data_ptr() + 4 * warmup, steps, out_dev.data_ptr() + 8 * warmup, steps + warmup)
@@ -293,6 +416,8 @@ def main() -> None:
         torch.cuda.synchronize()
         barrier()
     ms = start.elapsed_time(end)
+    solver.set_timing(False)
+    kernel_ms = solver.timing()
     if world > 1:
         t = torch.tensor([ms], device=f"cuda:{local}")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -326,16 +451,45 @@ def main() -> None:
             "api": "B200WaveSolver.run(host float32 drive) -> host float64 (probes, steps)",
         }
 
+    # The IR error against FP64 on the same grid: both run from rest over the same drive.
+    ir_error = None
+    if not args.no_ir_error:
+        fp64 = B200WaveSolver(workload.built.layout, precision="fp64", device=local)
+        m = min(args.ir_steps, len(signal))
+        solver.reset()
+        p32 = solver.run(signal[:m])
+        p64 = fp64.run(signal[:m])
+        fp64.close()
+        ir_error = ir_errors(p32, p64, workload.built.rate)
+        ir_error["steps"] = m
+        ir_error["vs"] = "the same layout stepped in FP64 on the GPU (bit-exact with the FP64 oracle on the golden grids)"
+
     bytes_per_step = algorithmic_bytes(desc)
     peak, peak_source = measured_peaks()
     achieved = bytes_per_step / (ms / 1e3 / steps) / 1e9
-    traffic = None
-    traffic_file = ROOT / "profiles" / "step_kernel_traffic.json"
-    if traffic_file.exists():
-        entry = json.loads(traffic_file.read_text())
-        cells = entry.get("cells_per_launch")
-        if cells:
-            traffic = int(entry["dram_bytes_per_launch"] * air / cells)
+    # Each kernel's algorithmic bytes per launch and its average launch time, live.
+    per_kernel_bytes = {
+        "bulk": BYTES_INTERIOR * desc["interior_cells"],
+        "layer": BYTES_LAYER * desc["layer_cells"],
+        "special": BYTES_SPECIAL * desc["special_rows"] + BYTES_LINK * desc["links"] + BYTES_STATE * desc["branch_states"],
+    }
+    traffic_table = {}
+    traffic_file = ROOT / "profiles" / "kernel_traffic_polyhedral_room.json"
+    if traffic_file.exists() and args.cell == 0.04:
+        traffic_table = json.loads(traffic_file.read_text()).get("dram_bytes_per_launch", {})
+    kernels = {}
+    for kind, nbytes in per_kernel_bytes.items():
+        launch_s = kernel_ms[kind] / 1e3 / max(1, kernel_ms["steps"])
+        got = nbytes / launch_s / 1e9 if launch_s > 0 else None
+        kernels[kind] = {
+            "algorithmic_bytes_per_launch": nbytes,
+            "mean_launch_us": round(launch_s * 1e6, 2),
+            "achieved": round(got, 1) if got else None,
+            "frac": round(got / peak, 4) if got else None,
+            "traffic": traffic_table.get(kind),
+        }
+    kernels["probe"] = {"mean_launch_us": round(kernel_ms["probe"] / max(1, kernel_ms["steps"]) * 1e3, 2)}
+    dominant = max(per_kernel_bytes, key=lambda k: kernel_ms[k])
 
     line = None
     if rank == 0:
@@ -367,20 +521,28 @@ def main() -> None:
                 "precision": "FP32, bit-exact with the reference (no FMA, subnormals flushed)",
             },
             "e2e": e2e,
-            "gpu_launches": steps,
+            "gpu_launches": 4 * steps,
             "roofline": {
                 "bound": "hbm",
-                "kernel": "step_kernel<float, 7-point> (one launch per step: interior, special rows, layer, probes)",
-                "achieved": round(achieved, 1),
+                "kernel": f"{dominant}_kernel (the longest of the step's four, by CUDA events)",
+                "achieved": kernels[dominant]["achieved"],
                 "peak": peak,
                 "unit": "GB/s",
-                "frac": round(achieved / peak, 4),
-                "traffic": traffic,
-                "algorithmic_bytes_per_launch": bytes_per_step,
+                "frac": kernels[dominant]["frac"],
+                "traffic": kernels[dominant]["traffic"],
+                "algorithmic_bytes_per_launch": per_kernel_bytes[dominant],
                 "peak_source": peak_source,
-                "bulk_12B_per_air_cell_frac": round(12 * air / (ms / 1e3 / steps) / 1e9 / peak, 4),
+                "kernels": kernels,
+                "step": {
+                    "algorithmic_bytes": bytes_per_step,
+                    "achieved": round(achieved, 1),
+                    "frac": round(achieved / peak, 4),
+                    "bulk_12B_per_air_cell_frac": round(12 * air / (ms / 1e3 / steps) / 1e9 / peak, 4),
+                },
             },
             "cpu_baseline": cpu,
+            "ir_error_vs_fp64": ir_error,
+            "adjoint_over_forward": None,
             "clocks": clocks.summary(),
             "finite": finite,
         }

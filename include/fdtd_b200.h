@@ -145,6 +145,16 @@ int fdtd_synchronize(fdtd_solver *solver);
    with fdtd_run_device; NULL for a NULL handle. */
 void *fdtd_stream(const fdtd_solver *solver);
 
+/*
+ * Per-kernel timing of fdtd_run_device (no counterpart in the reference): with `enable` set, each
+ * step's four kernels are bracketed by CUDA events on the streams they run on, and
+ * fdtd_get_timing adds up, since the last call, the milliseconds each kind took — ms[0] the
+ * interior sweep, ms[1] the matched layer, ms[2] the special rows, ms[3] the probe records — over
+ * *steps steps. The work done is the same; only events are added between the launches.
+ */
+int fdtd_set_timing(fdtd_solver *solver, int enable);
+int fdtd_get_timing(fdtd_solver *solver, double ms[4], uint64_t *steps);
+
 /* Replaces WaveSolver::reset (fdtd.hpp:906-915): silences the grid. */
 int fdtd_reset(fdtd_solver *solver);
 

@@ -166,7 +166,16 @@ PYBIND11_MODULE(_native, m) {
 
     py::class_<BvhHolder, std::shared_ptr<BvhHolder>>(m, "Bvh")
         .def(py::init(&make_bvh), py::arg("vertices"), py::arg("faces"), py::arg("split") = "sah")
-        .def_property_readonly("face_count", [](const BvhHolder &h) { return h.bvh->face_count(); });
+        .def_property_readonly("face_count", [](const BvhHolder &h) { return h.bvh->face_count(); })
+        .def(
+            "set_facing",
+            [](BvhHolder &h, const CArray<std::int8_t> &facing) {
+                if (static_cast<std::size_t>(facing.size()) != h.bvh->face_count())
+                    throw std::invalid_argument("Bvh.set_facing: one value per face");
+                h.bvh->set_facing(facing.data());
+            },
+            py::arg("facing"))
+        .def_property_readonly("has_facing", [](const BvhHolder &h) { return h.bvh->has_facing(); });
 
     py::class_<SolverHolder, std::shared_ptr<SolverHolder>>(m, "WaveSolver")
         .def(py::init(&make_solver), py::arg("bvh"), py::arg("face_material"), py::arg("beta"), py::arg("branches"),

@@ -13,7 +13,7 @@ import math
 
 import numpy as np
 
-from oracle.oracle import reference_native, reference_python
+from oracle.oracle import REFERENCE, reference_native, reference_python
 
 C = 343.0
 OFFSET = np.array([0.0137, 0.0219, 0.0291])  # tests/test_fitted_walls.py:41

@@ -94,3 +94,87 @@ def test_gpu_info_counts_the_layout():
     assert info.special_cells == len(layout["special"])
     assert info.layer_cells == len(layout["layer_cells"])
     assert info.probes == gpu.probes == len(layout["probe_start"]) - 1
+
+
+@pytest.mark.parametrize("name", ["resonant7", "open_layer_speed", "fitted_open"])
+def test_gpu_runs_in_pieces_that_flip_the_levels(name):
+    # Chunks of the captured graph (64 steps) and remainders of odd lengths, so that the levels'
+    # roles flip between the graph's captures.
+    layout, signal, reference = load_golden(name)
+    gpu = B200WaveSolver(layout)
+    cuts = [0, 1, 66, 130, 131, 259, 323, len(signal)]
+    assert np.array_equal(_pieces(gpu, signal, cuts), reference)
+
+
+def test_gpu_run_device_equals_run():
+    import torch
+
+    layout, signal, reference = load_golden("resonant19")
+    gpu = B200WaveSolver(layout)
+    sig = torch.from_numpy(signal).cuda()
+    out = torch.zeros((gpu.probes, len(signal)), dtype=torch.float64, device="cuda")
+    gpu.run_device(sig.data_ptr(), 200, out.data_ptr(), len(signal))
+    gpu.run_device(sig.data_ptr() + 4 * 200, len(signal) - 200, out.data_ptr() + 8 * 200, len(signal))
+    gpu.synchronize()
+    assert np.array_equal(out.cpu().numpy(), reference)
+
+
+# ---- the benchmark's room, laid out by the host builder --------------------------------------
+
+from acoustic_spaces_b200 import layouts  # noqa: E402
+
+
+def test_gpu_steps_a_polyhedral_room_as_the_oracle_does():
+    # The benchmark's workload at 20 cm cells (100 x 75 x 50): 19 planes, an open face, an 8-cell
+    # matched layer, resonant walls; the whole state equal to the oracle's after 300 steps.
+    w = layouts.polyhedral_room(0, cell=0.2, steps=300)
+    gpu = B200WaveSolver(w.built.layout)
+    oracle = OracleSolver(w.built.layout)
+    a = _pieces(gpu, w.signal, [0, 129, 300])
+    b = oracle.run(w.signal)
+    assert np.array_equal(a, b)
+    sa, sb = gpu.state(), oracle.state()
+    for key in sa:
+        assert np.array_equal(sa[key], sb[key]), key
+
+
+@pytest.fixture(scope="module")
+def full_room():
+    return layouts.polyhedral_room(0, steps=600)
+
+
+def test_gpu_full_size_run_in_pieces_equals_one_run(full_room):
+    # At the benchmark's full size (500 x 375 x 250): a run cut into pieces is the run, to the bit,
+    # and a reset run repeats it.
+    w = full_room
+    gpu = B200WaveSolver(w.built.layout)
+    whole = gpu.run(w.signal)
+    gpu.reset()
+    pieces = _pieces(gpu, w.signal, [0, 77, 300, 301, 600])
+    assert np.array_equal(whole, pieces)
+    assert np.all(np.isfinite(whole)) and np.abs(whole).max() > 0.0
+
+
+def test_gpu_full_size_fp32_stays_within_1e4_of_fp64(full_room):
+    # The north star's accuracy bar on the full grid: FP32 against FP64 stepping of the same
+    # layout, relative L2 of every receiver's response within 1e-4.
+    w = full_room
+    p32 = B200WaveSolver(w.built.layout).run(w.signal)
+    p64 = B200WaveSolver(w.built.layout, precision="fp64").run(w.signal)
+    # (Receivers the sound has reached in 600 steps, 14 m at its speed: the others hold only the
+    # grid's numerical precursor, which single precision flushes to zero.)
+    energy = np.linalg.norm(p64, axis=1)
+    reached = energy > 1e-3 * energy.max()
+    assert reached.sum() >= 4
+    rel = np.linalg.norm(p32 - p64, axis=1)[reached] / energy[reached]
+    assert rel.max() < 1e-4, rel.max()
+
+
+def test_gpu_steps_a_stack_of_rooms_as_each_alone():
+    # Many rooms with several sources each, stacked into one grid and stepped by one launch per
+    # kind: each solve equals the oracle's run of its own layout, to the bit.
+    b = layouts.batched_rooms(3, rooms=3, sources=3, cell=0.1, dims=(2.0, 5.0), steps=200)
+    gpu = B200WaveSolver(b.stacked.layout)
+    together = _pieces(gpu, b.signal, [0, 64, 65, 200])
+    for lay, (p0, p1, _, _) in zip(b.layouts, b.stacked.parts):
+        assert np.array_equal(OracleSolver(lay).run(b.signal), together[p0:p1])

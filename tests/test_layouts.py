@@ -115,3 +115,43 @@ def test_the_polyhedral_workload_is_seeded():
     for name in a.built.layout:
         assert np.array_equal(a.built.layout[name], b.built.layout[name])
     assert 12 <= int(a.description["room"].split(",")[1].split()[0]) <= 20
+
+
+# ---- many grids stacked into one ---------------------------------------------------------------
+
+
+def test_paris_admittance_inverts_paris_absorption():
+    alpha = np.array([0.02, 0.1, 0.3, 0.5, 0.9])
+    beta = L.paris_admittance(alpha)
+    assert np.allclose(L.paris_absorption(1.0 / beta), alpha, rtol=1e-9)
+    assert np.all(np.diff(beta) > 0)
+
+
+def test_a_stack_steps_each_grid_as_it_steps_alone():
+    # Two rooms with two sources each, stacked: every solve's probes equal its own run's, to the
+    # bit, in the oracle (float) — the stack changes no row's coefficients or neighbours.
+    b = L.batched_rooms(1, rooms=2, sources=2, cell=0.1, dims=(2.0, 4.0), steps=120)
+    stacked = OracleSolver(b.stacked.layout).run(b.signal)
+    for lay, (p0, p1, air, _) in zip(b.layouts, b.stacked.parts):
+        assert np.array_equal(OracleSolver(lay).run(b.signal), stacked[p0:p1])
+        assert air == np.count_nonzero(lay["types"])
+
+
+def test_golden_grids_stack_with_their_own_runs():
+    from conftest import golden_names, load_golden
+
+    names = [n for n in golden_names() if len(load_golden(n)[0]["layer_cells"]) == 0 and load_golden(n)[0]["scaled"][0] == 0]
+    layouts = [load_golden(n)[0] for n in names]
+    sevens = [lay for lay in layouts if int(lay["stencil"][0]) == 7]
+    stacked = L.stack(sevens)
+    signal = np.random.default_rng(2).standard_normal(150).astype(np.float32)
+    together = OracleSolver(stacked.layout).run(signal)
+    for lay, (p0, p1, _, _) in zip(sevens, stacked.parts):
+        assert np.array_equal(OracleSolver(lay).run(signal), together[p0:p1])
+
+
+def test_stacking_refuses_a_matched_layer():
+    from conftest import load_golden
+
+    with pytest.raises(ValueError, match="matched layer"):
+        L.stack([load_golden("resonant7")[0], load_golden("open_layer")[0]])
