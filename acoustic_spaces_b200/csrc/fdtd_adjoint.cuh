@@ -1,0 +1,148 @@
+// Device code of the reverse-time (adjoint) stepper: the gradient of a loss of the probes'
+// series with respect to the special rows' coefficients, for grids of the 7-point stencil without
+// a matched layer or a speed field.
+//
+// A forward step maps the levels (u_n, u_{n-1}) and branch velocities (w_n, w_{n-1}) to u_{n+1},
+// w_{n+1}: z_{n+1} = G z_n - H z_{n-1} (+ the source), z = (u, w). For a special row (cell i,
+// states j; fdtd.hpp:860-881):
+//   x = ca u_n[i] + sum_l wl u_n[i + o_l] - cb u_{n-1}[i] - sum_j W_j (now_j w_n[j] - before_j w_{n-1}[j]) + src s
+//   u_{n+1}[i] = ci x,   w_{n+1}[j] = w_{n-1}[j] + gain_j (u_{n+1}[i] - u_{n-1}[i]) + now_j w_n[j] - before_j w_{n-1}[j]
+// and interior cells have G = centre on the diagonal and axial to each neighbour, H = 1.
+// The adjoint z~_n = dL/dz_n obeys z~_n = G^T z~_{n+1} - H^T z~_{n+2} + P_n (P_n the probes'
+// terms), a leapfrog run backwards in time with the transposed operator. With a row's effective
+// adjoint L~ = lam[i] + sum_j gain_j om[j] (lam, om: the adjoints of u and w):
+//   lam_n[i] = sum over the cells r reading u_i of G_{r,i} L~_{n+1}[r]  -  (ci cb L~_{n+2}[i] + sum_j gain_j om_{n+2}[j])
+//   om_n[j]  = -ci W_j now_j L~_{n+1}[i] + now_j om_{n+1}[j] + ci W_j before_j L~_{n+2}[i] + (1 - before_j) om_{n+2}[j]
+// (an interior cell's L~ is its lam). Interior cells take the forward bulk sweep on the adjoint
+// levels (all their readers being interior to within the rows next to special cells, which a
+// correction list fixes), special rows a gather over their readers (a transposed list).
+// The gradient of step n, with U = L~_{n+1}[i] and own~_j = om_{n+1}[j] - W_j ci U:
+//   dL/dci += U x,  dL/dcb += -U ci u_{n-1}[i],  dL/dnow_j += own~_j w_n[j],
+//   dL/dbefore_j += -own~_j w_{n-1}[j],  dL/dgain_j += om_{n+1}[j] (u_{n+1}[i] - u_{n-1}[i])
+// needs only the special rows' own forward values, recorded as a trajectory per step; the sums
+// over steps are kept in double.
+#pragma once
+
+#include "fdtd_kernels.cuh"
+
+namespace fdtd {
+
+struct AdjointTables {
+    uint32_t specials, states;
+    const uint32_t *special;  // pitched cell of each row
+    const uint32_t *state_start;
+    const float *state_weight, *state_now, *state_before, *state_gain;
+    const float *coef_b, *coef_inv;
+    // Readers of each special row's cell (transposed links): reader_start[k] .. reader_start[k+1];
+    // an entry's index is a special row (its L~) when the kind bit is set, else a pitched cell
+    // (interior: its lam), and its coefficient G_{reader, cell}.
+    const uint32_t *reader_start, *reader_index;
+    const uint8_t *reader_kind;
+    const double *reader_coef;
+    // Interior cells next to special rows: corrected_start .. per cell, entries (special row, its
+    // coefficient on the cell); the bulk sweep took axial * lam of those rows' cells instead.
+    uint32_t corrected;
+    const uint32_t *corrected_cell, *corrected_start, *corrected_row;
+    const double *corrected_coef;
+    float axial;
+    // Probes: CSR of pitched cells and weights.
+    uint32_t probes;
+    const uint32_t *probe_start, *probe_cells;
+    const double *probe_weights;
+};
+
+// The trajectory of a run: level l of the special rows' pressure at traj_u[l * specials + k] and
+// of the branch velocities at traj_w[l * states + j].
+template <typename T>
+__global__ void __launch_bounds__(kBlock) record_kernel(const AdjointTables t, const T *u, const T *w, T *traj_u,
+                                                        T *traj_w) {
+    const uint32_t k = blockIdx.x * kBlock + threadIdx.x;
+    if (k < t.specials) traj_u[k] = u[t.special[k]];
+    if (k < t.states) traj_w[k] = w[k];
+}
+
+// L~ of every special row from the adjoint level (lam, om).
+template <typename T>
+__global__ void __launch_bounds__(kBlock) tilde_kernel(const AdjointTables t, const T *lam, const T *om, T *tilde) {
+    const uint32_t k = blockIdx.x * kBlock + threadIdx.x;
+    if (k >= t.specials) return;
+    T value = lam[t.special[k]];
+    for (uint32_t j = t.state_start[k], e = t.state_start[k + 1]; j < e; ++j) value += (T)t.state_gain[j] * om[j];
+    tilde[k] = value;
+}
+
+// Interior cells next to special rows: the bulk sweep added axial * lam[cell of row r]; the
+// transposed operator has G_{r, cell} L~[r] there.
+template <typename T>
+__global__ void __launch_bounds__(kBlock) correct_kernel(const AdjointTables t, const T *lam_next, const T *tilde,
+                                                         T *lam_out) {
+    const uint32_t c = blockIdx.x * kBlock + threadIdx.x;
+    if (c >= t.corrected) return;
+    const uint32_t cell = t.corrected_cell[c];
+    T delta = 0;
+    for (uint32_t e = t.corrected_start[c], end = t.corrected_start[c + 1]; e < end; ++e) {
+        const uint32_t r = t.corrected_row[e];
+        delta += (T)t.corrected_coef[e] * tilde[r] - (T)t.axial * lam_next[t.special[r]];
+    }
+    lam_out[cell] += delta;
+}
+
+// Special rows: the adjoint of their cells and branch states, and the gradient of step n.
+// lam_next/om_next: level n+1 (complete), lam_out/om_out: hold level n+2 on entry (own row only)
+// and level n on exit; traj levels of u_{n-1}, u_n... at l0 = n - s0, then l0 + 1, l0 + 2.
+template <typename T>
+__global__ void __launch_bounds__(kBlock) special_adjoint_kernel(const AdjointTables t, const T *lam_next,
+                                                                 const T *om_next, const T *tilde, T *lam_out,
+                                                                 T *om_out, const T *traj_u, const T *traj_w,
+                                                                 uint32_t level, double *g_ci, double *g_cb,
+                                                                 double *g_now, double *g_before, double *g_gain) {
+    const uint32_t k = blockIdx.x * kBlock + threadIdx.x;
+    if (k >= t.specials) return;
+    const uint32_t i = t.special[k];
+    const T ci = (T)t.coef_inv[k], cb = (T)t.coef_b[k];
+    T gathered = 0;
+    for (uint32_t e = t.reader_start[k], end = t.reader_start[k + 1]; e < end; ++e) {
+        const uint32_t idx = t.reader_index[e];
+        gathered += (T)t.reader_coef[e] * (t.reader_kind[e] ? tilde[idx] : lam_next[idx]);
+    }
+    const uint32_t s0 = t.state_start[k], s1 = t.state_start[k + 1];
+    const T lam2 = lam_out[i];  // level n+2
+    T tilde2 = lam2, gain_om2 = 0;
+    for (uint32_t j = s0; j < s1; ++j) {
+        const T term = (T)t.state_gain[j] * om_out[j];
+        tilde2 += term;
+        gain_om2 += term;
+    }
+    const T U = tilde[k];
+    lam_out[i] = gathered - (ci * cb * tilde2 + gain_om2);
+    // The gradient of step n (forward values: u_{n-1}, u_n, u_{n+1} at levels l, l+1, l+2).
+    const T u_prev = traj_u[(uint64_t)level * t.specials + k];
+    const T u_next = traj_u[(uint64_t)(level + 2) * t.specials + k];
+    g_ci[k] += (double)U * ((double)u_next / (double)ci);
+    g_cb[k] += -(double)U * (double)ci * (double)u_prev;
+    for (uint32_t j = s0; j < s1; ++j) {
+        const T W = (T)t.state_weight[j], now = (T)t.state_now[j], before = (T)t.state_before[j];
+        const T om1 = om_next[j], om2 = om_out[j];
+        om_out[j] = -ci * W * now * U + now * om1 + ci * W * before * tilde2 + ((T)1 - before) * om2;
+        const double own_bar = (double)om1 - (double)W * (double)ci * (double)U;
+        const double w_n = (double)traj_w[(uint64_t)(level + 1) * t.states + j];
+        const double w_prev = (double)traj_w[(uint64_t)level * t.states + j];
+        g_now[j] += own_bar * w_n;
+        g_before[j] += -own_bar * w_prev;
+        g_gain[j] += (double)om1 * ((double)u_next - (double)u_prev);
+    }
+}
+
+// The probes' terms of level n: lam_n[cell] += weight * dL/dy_p^n.
+template <typename T>
+__global__ void __launch_bounds__(kBlock) probe_adjoint_kernel(const AdjointTables t, const double *dloss, uint64_t stride,
+                                                               uint64_t step, T *lam_out) {
+    const uint32_t p = blockIdx.x * kBlock + threadIdx.x;
+    if (p >= t.probes) return;
+    const double g = dloss[(uint64_t)p * stride + step];
+    if (g == 0.0) return;
+    for (uint32_t e = t.probe_start[p], end = t.probe_start[p + 1]; e < end; ++e)
+        atomicAdd(&lam_out[t.probe_cells[e]], (T)(t.probe_weights[e] * g));
+}
+
+}  // namespace fdtd

@@ -17,8 +17,10 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
+#include "fdtd_adjoint.cuh"
 #include "fdtd_b200.h"
 #include "fdtd_kernels.cuh"
 
@@ -53,7 +55,7 @@ struct fdtd_solver {
     int sms = 148;  // multiprocessors of the device
     int precision = FDTD_FP32;
     bool wide = false, scaled = false;
-    cudaStream_t stream = nullptr;  // the handle's stream: bulk sweep and matched layer
+    cudaStream_t stream = nullptr;  // the handle's stream: the sweep of interior and matched-layer cells
     cudaStream_t side = nullptr;    // special rows and probes, beside them within each step
     cudaEvent_t joined[2] = {nullptr, nullptr};  // each stream's end of a step
     std::string error;
@@ -71,7 +73,10 @@ struct fdtd_solver {
     // for the branch velocities w.
     void *u[2] = {nullptr, nullptr};
     void *w[2] = {nullptr, nullptr};
-    void *layer_parts = nullptr;  // 3 arrays of the layer's cells: p_x, p_y, p_z
+    // The matched layer's pressure parts p_x, p_y, p_z: three pitched arrays, the layer's cells used.
+    void *layer_parts = nullptr;
+    std::vector<uint32_t> layer_cells;      // pitched, in the layout's order (for fdtd_read_state)
+    const uint8_t *types_device = nullptr;  // the pitched cell types (a layer cell's with its below bits)
     // Per axis, the velocity on each cell's + face (pitched, only the layer's faces used), in two
     // buffers: faces[1] holds the latest values between runs, as u[1] does.
     void *faces[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
@@ -90,6 +95,14 @@ struct fdtd_solver {
     bool timing = false;
     std::vector<cudaEvent_t> timing_events;  // 8 per step: (start, end) of bulk, layer, special, probe
     uint64_t timed_steps = 0;
+    // The adjoint (fdtd_gradient), set up on first use: its tables, the two adjoint levels of the
+    // field and of the branch velocities, each row's L~, and the tensor maps of the adjoint levels.
+    bool adjoint_ready = false;
+    AdjointTables adjoint{};
+    void *lam[2] = {nullptr, nullptr};
+    void *om[2] = {nullptr, nullptr};
+    void *tilde = nullptr;
+    CUtensorMap lam_b[2], lam_a[2];
     // Staging for fdtd_run's host buffers, grown on demand.
     float *stage_signal = nullptr;
     double *stage_out = nullptr;
@@ -201,6 +214,7 @@ int validate(const fdtd_layout *L, std::string &why) {
             return refuse("a branch state has no branch");
     }
     if (L->layer_count) {
+        if (L->stencil != 7) return refuse("the matched layer needs the 7-point stencil");
         if (!L->layer_cells) return refuse("the matched layer has no cells");
         for (int k = 0; k < 6; ++k)
             if (!L->keep[k] || !L->push[k]) return refuse("the matched layer misses its coefficients");
@@ -222,6 +236,10 @@ int validate(const fdtd_layout *L, std::string &why) {
         for (uint64_t c = 0; c < L->layer_count; ++c) {
             if (seen[L->layer_cells[c]]++) return refuse("a matched-layer cell is listed twice");
         }
+        // The matched layer is swept by type: every cell of type layer is one of its cells.
+        uint64_t typed = 0;
+        for (uint64_t i = 0; i < n; ++i) typed += L->types[i] == kLayer;
+        if (typed != L->layer_count) return refuse("a cell of type layer is not in the matched layer");
     }
     if (!L->probe_start || L->probe_start[0] != 0) return refuse("probe_start does not start at 0");
     const uint64_t pc = L->probe_start[L->probe_count];
@@ -278,20 +296,15 @@ Fields<T> fields_for(const fdtd_solver *s, bool flip) {
     f.a = static_cast<T *>(s->u[prev]);
     f.wb = static_cast<const T *>(s->w[cur]);
     f.wa = static_cast<T *>(s->w[prev]);
-    f.layer_parts = static_cast<T *>(s->layer_parts);
-    for (int axis = 0; axis < 3; ++axis) {
-        f.face_old[axis] = static_cast<const T *>(s->faces[cur][axis]);
-        f.face_new[axis] = static_cast<T *>(s->faces[prev][axis]);
-    }
     return f;
 }
 
-template <typename T, bool WIDE, bool SCALED>
+template <typename T, bool WIDE, bool SCALED, bool LAYER>
 int set_up_kernels(fdtd_solver *s) {
-    CUDA_TRY(s, cudaFuncSetAttribute(bulk_kernel<T, WIDE, SCALED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    CUDA_TRY(s, cudaFuncSetAttribute(bulk_kernel<T, WIDE, SCALED, LAYER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)Stage<T, SCALED>::smem));
     int per_sm = 0;
-    CUDA_TRY(s, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bulk_kernel<T, WIDE, SCALED>, kBlock,
+    CUDA_TRY(s, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bulk_kernel<T, WIDE, SCALED, LAYER>, kBlock,
                                                               Stage<T, SCALED>::smem));
     s->bulk_per_sm = per_sm;
     // One tile per block: measured faster than a persistent grid of the resident blocks.
@@ -299,16 +312,18 @@ int set_up_kernels(fdtd_solver *s) {
     return FDTD_OK;
 }
 
-template <typename T, bool WIDE, bool SCALED>
+template <typename T, bool WIDE, bool SCALED, bool LAYER>
 int launch_steps(fdtd_solver *s, const float *d_signal, uint64_t steps, double *d_out, uint64_t stride) {
     const Tables &g = s->tables;
     const uint32_t special_blocks = (uint32_t)((s->specials + kBlock - 1) / kBlock);
-    const uint32_t layer_blocks = (uint32_t)((s->layers + kBlock - 1) / kBlock);
     const uint32_t probe_blocks = (uint32_t)((s->probes + kProbeWarps - 1) / kProbeWarps);
     const uint32_t smem = Stage<T, SCALED>::smem;
-    // Each step: the bulk sweep and the matched layer on the handle's stream, the special rows and
-    // the probes on the side stream beside them; each stream waits for the other's end of the step
-    // before.
+    // Each step: the sweep of the interior and matched-layer cells on the handle's stream, the
+    // special rows and the probes on the side stream beside them; each stream waits for the
+    // other's end of the step before. While timing, all run one after another on the handle's
+    // stream, so that each kernel's events bracket that kernel alone (the layer's pair brackets
+    // nothing: its cells are swept with the interior).
+    cudaStream_t side = s->timing ? s->stream : s->side;
     CUDA_TRY(s, cudaEventRecord(s->joined[0], s->stream));
     CUDA_TRY(s, cudaStreamWaitEvent(s->side, s->joined[0], 0));
     for (uint64_t k = 0; k < steps; ++k) {
@@ -338,24 +353,27 @@ int launch_steps(fdtd_solver *s, const float *d_signal, uint64_t steps, double *
             BulkArgs args = s->bulk;
             args.a = f.a;
             const int cur = flip ? 0 : 1, prev = flip ? 1 : 0;
-            bulk_kernel<T, WIDE, SCALED><<<s->bulk_blocks, kBlock, smem, s->stream>>>(s->map_b[cur], s->map_a[prev],
-                                                                                    s->map_t, s->map_s, args);
+            for (int axis = 0; axis < 3; ++axis) {
+                args.face_old[axis] = s->faces[cur][axis];
+                args.face_new[axis] = s->faces[prev][axis];
+            }
+            bulk_kernel<T, WIDE, SCALED, LAYER><<<s->bulk_blocks, kBlock, smem, s->stream>>>(
+                s->map_b[cur], s->map_a[prev], s->map_t, s->map_s, args);
         }
         if (ev) CUDA_TRY(s, cudaEventRecord(ev[1], s->stream));
         if (ev) CUDA_TRY(s, cudaEventRecord(ev[2], s->stream));
-        if (layer_blocks) layer_kernel<T, SCALED><<<layer_blocks, kBlock, 0, s->stream>>>(g, f);
         if (ev) CUDA_TRY(s, cudaEventRecord(ev[3], s->stream));
-        if (ev) CUDA_TRY(s, cudaEventRecord(ev[4], s->side));
+        if (ev) CUDA_TRY(s, cudaEventRecord(ev[4], side));
         if (special_blocks) {
             if (s->link_slots <= 6)
-                special_kernel<T, 6><<<special_blocks, kBlock, 0, s->side>>>(g, f);
+                special_kernel<T, 6><<<special_blocks, kBlock, 0, side>>>(g, f);
             else
-                special_kernel<T, 18><<<special_blocks, kBlock, 0, s->side>>>(g, f);
+                special_kernel<T, 18><<<special_blocks, kBlock, 0, side>>>(g, f);
         }
-        if (ev) CUDA_TRY(s, cudaEventRecord(ev[5], s->side));
-        if (ev) CUDA_TRY(s, cudaEventRecord(ev[6], s->side));
-        if (probe_blocks) probe_kernel<T><<<probe_blocks, kBlock, 0, s->side>>>(g, f);
-        if (ev) CUDA_TRY(s, cudaEventRecord(ev[7], s->side));
+        if (ev) CUDA_TRY(s, cudaEventRecord(ev[5], side));
+        if (ev) CUDA_TRY(s, cudaEventRecord(ev[6], side));
+        if (probe_blocks) probe_kernel<T><<<probe_blocks, kBlock, 0, side>>>(g, f);
+        if (ev) CUDA_TRY(s, cudaEventRecord(ev[7], side));
         CUDA_TRY(s, cudaEventRecord(s->joined[0], s->stream));
         CUDA_TRY(s, cudaEventRecord(s->joined[1], s->side));
     }
@@ -365,38 +383,34 @@ int launch_steps(fdtd_solver *s, const float *d_signal, uint64_t steps, double *
     return FDTD_OK;
 }
 
-template <typename T, bool W, bool S>
+template <typename T, bool W, bool S, bool LY>
 int dispatch_run(fdtd_solver *s, const float *d_signal, uint64_t steps, double *d_out, uint64_t stride) {
-    return launch_steps<T, W, S>(s, d_signal, steps, d_out, stride);
+    return launch_steps<T, W, S, LY>(s, d_signal, steps, d_out, stride);
 }
 
+// The instantiation for the grid: precision, stencil, speed field, matched layer (which takes the
+// 7-point stencil only).
+#define FDTD_BY_KIND(CALL)                                                              \
+    do {                                                                                \
+        if (s->precision == FDTD_FP64) {                                                \
+            if (s->layers) return s->scaled ? CALL(double, false, true, true) : CALL(double, false, false, true); \
+            if (!s->wide) return s->scaled ? CALL(double, false, true, false) : CALL(double, false, false, false); \
+            return s->scaled ? CALL(double, true, true, false) : CALL(double, true, false, false); \
+        }                                                                               \
+        if (s->layers) return s->scaled ? CALL(float, false, true, true) : CALL(float, false, false, true); \
+        if (!s->wide) return s->scaled ? CALL(float, false, true, false) : CALL(float, false, false, false); \
+        return s->scaled ? CALL(float, true, true, false) : CALL(float, true, false, false); \
+    } while (0)
+
 int dispatch(fdtd_solver *s, const float *d_signal, uint64_t steps, double *d_out, uint64_t stride) {
-#define RUN_CALL(T, W, S) dispatch_run<T, W, S>(s, d_signal, steps, d_out, stride)
-    if (s->precision == FDTD_FP64) {
-        if (!s->wide && !s->scaled) return RUN_CALL(double, false, false);
-        if (!s->wide && s->scaled) return RUN_CALL(double, false, true);
-        if (s->wide && !s->scaled) return RUN_CALL(double, true, false);
-        return RUN_CALL(double, true, true);
-    }
-    if (!s->wide && !s->scaled) return RUN_CALL(float, false, false);
-    if (!s->wide && s->scaled) return RUN_CALL(float, false, true);
-    if (s->wide && !s->scaled) return RUN_CALL(float, true, false);
-    return RUN_CALL(float, true, true);
+#define RUN_CALL(T, W, S, LY) dispatch_run<T, W, S, LY>(s, d_signal, steps, d_out, stride)
+    FDTD_BY_KIND(RUN_CALL);
 #undef RUN_CALL
 }
 
 int set_up(fdtd_solver *s) {
-#define SET_CALL(T, W, S) set_up_kernels<T, W, S>(s)
-    if (s->precision == FDTD_FP64) {
-        if (!s->wide && !s->scaled) return SET_CALL(double, false, false);
-        if (!s->wide && s->scaled) return SET_CALL(double, false, true);
-        if (s->wide && !s->scaled) return SET_CALL(double, true, false);
-        return SET_CALL(double, true, true);
-    }
-    if (!s->wide && !s->scaled) return SET_CALL(float, false, false);
-    if (!s->wide && s->scaled) return SET_CALL(float, false, true);
-    if (s->wide && !s->scaled) return SET_CALL(float, true, false);
-    return SET_CALL(float, true, true);
+#define SET_CALL(T, W, S, LY) set_up_kernels<T, W, S, LY>(s)
+    FDTD_BY_KIND(SET_CALL);
 #undef SET_CALL
 }
 
@@ -454,20 +468,23 @@ int build(fdtd_solver *s, const fdtd_layout *L) {
     if (s->n_device >= (1ull << 32)) return fail(s, FDTD_EINVAL, "the wave grid is too large for the GPU's 32-bit indices");
     s->wide = L->stencil == 19;
     s->scaled = L->scaled != 0;
+    s->layers = L->layer_count;  // the sweep's instantiation depends on it
     const size_t e = s->precision == FDTD_FP64 ? 8 : 4;
     Tables &g = s->tables;
     g.pitch = (uint32_t)s->pitch;
     g.ny = (uint32_t)ny;
     g.nz = (uint32_t)nz;
     g.sz = (uint32_t)(s->pitch * ny);
-    g.plane = (uint32_t)(s->pitch * ny);
     for (int k = 0; k < 18; ++k)
         g.offset[k] = (int32_t)(kSteps[k][0] + kSteps[k][1] * (int64_t)s->pitch + kSteps[k][2] * (int64_t)(s->pitch * ny));
 
-    // Cell types and scales, pitched; the interior cells' bounding box and the air count.
+    // Cell types and scales, pitched; the swept cells' (interior and matched layer) bounding box
+    // and the air count. A layer cell's type byte also carries which of its lower neighbours are
+    // in the layer; with a speed field its scale is the layer's scale of the cell.
     std::vector<uint8_t> types(s->n_device, (uint8_t)kSolid);
     std::vector<float> scale(s->scaled ? s->n_device : 0, 0.0f);
     uint64_t x0 = nx, y0 = ny, z0 = nz, x1 = 0, y1 = 0, z1 = 0, interior = 0, air = 0;
+    const uint64_t strides[3] = {1, nx, nx * ny};
     for (uint64_t z = 0; z < nz; ++z)
         for (uint64_t y = 0; y < ny; ++y) {
             const uint64_t row = nx * (y + ny * z), drow = s->pitch * (y + ny * z);
@@ -476,18 +493,27 @@ int build(fdtd_solver *s, const fdtd_layout *L) {
             for (uint64_t x = 0; x < nx; ++x) {
                 const uint8_t t = L->types[row + x];
                 if (t != kSolid) ++air;
-                if (t != kInterior) continue;
-                ++interior;
+                if (t == kLayer) {
+                    for (int axis = 0; axis < 3; ++axis)
+                        if (L->types[row + x - strides[axis]] == kLayer)
+                            types[drow + x] |= (uint8_t)(1u << (kBelowShift + axis));
+                } else if (t != kInterior) {
+                    continue;
+                }
+                interior += t == kInterior;
                 x0 = std::min(x0, x), x1 = std::max(x1, x + 1);
                 y0 = std::min(y0, y), y1 = std::max(y1, y + 1);
                 z0 = std::min(z0, z), z1 = std::max(z1, z + 1);
             }
         }
+    if (s->scaled)
+        for (uint64_t c = 0; c < L->layer_count; ++c) scale[pitched(s, (uint64_t)L->layer_cells[c])] = L->layer_scale[c];
     s->interior = interior, s->air = air;
 
     int rc;
     const uint8_t *d_types;
     if ((rc = upload(s, types.data(), types.size(), &d_types))) return rc;
+    s->types_device = d_types;
     const float *d_scale = nullptr;
     if (s->scaled && (rc = upload(s, scale.data(), scale.size(), &d_scale))) return rc;
 
@@ -496,7 +522,7 @@ int build(fdtd_solver *s, const fdtd_layout *L) {
         if ((rc = zeros(s, e * s->n_device, &s->u[k]))) return rc;
         if ((rc = zeros(s, e * L->state_count, &s->w[k]))) return rc;
     }
-    if ((rc = zeros(s, e * 3 * L->layer_count, &s->layer_parts))) return rc;
+    if (L->layer_count && (rc = zeros(s, e * 3 * s->n_device, &s->layer_parts))) return rc;
     if (L->layer_count)
         for (int k = 0; k < 2; ++k)
             for (int axis = 0; axis < 3; ++axis)
@@ -520,12 +546,12 @@ int build(fdtd_solver *s, const fdtd_layout *L) {
     bk.centre = L->centre;
     bk.total = L->total;
     bk.error = s->d_error;
-    if (interior) {
+    if (interior || L->layer_count) {
         bk.xa = (uint32_t)(x0 / 16 * 16);
         bk.y0 = (uint32_t)y0, bk.z0 = (uint32_t)z0;
         bk.x1 = (uint32_t)x1, bk.y1 = (uint32_t)y1, bk.z1 = (uint32_t)z1;
         // The tile list: the columns of kTX x kTY cells over the box, and in each the runs of
-        // planes that hold interior cells, cut into chunks of at most `chunk` planes, so that
+        // planes that hold interior or layer cells, cut into chunks of at most `chunk` planes, so that
         // there are blocks enough for every multiprocessor several times over. Grids of many
         // rooms (stacked along z) skip the planes between the rooms.
         const uint64_t tiles_x = (x1 - bk.xa + kTX - 1) / kTX, tiles_y = (y1 - y0 + kTY - 1) / kTY;
@@ -536,7 +562,7 @@ int build(fdtd_solver *s, const fdtd_layout *L) {
             for (uint64_t y = y0; y < y1; ++y) {
                 const uint8_t *row = &L->types[nx * (y + ny * z)];
                 for (uint64_t x = x0; x < x1; ++x) {
-                    if (row[x] != kInterior) continue;
+                    if (row[x] != kInterior && row[x] != kLayer) continue;
                     uint8_t &o = occupied[((y - y0) / kTY * tiles_x + (x - bk.xa) / kTX) * nz + z];
                     planes += o == 0;
                     o = 1;
@@ -644,24 +670,13 @@ int build(fdtd_solver *s, const fdtd_layout *L) {
         g.state_gain = fp;
     }
 
-    // Matched layer.
+    // Matched layer: swept with the interior (its pressure parts and faces pitched); per axis and
+    // grid coordinate {keep, push, keep_face, push_face} (layer_coefficients, fdtd.hpp:2219-2238).
     const uint64_t Lc = L->layer_count;
     s->layers = Lc;
-    g.layers = (uint32_t)Lc;
     if (Lc) {
-        std::vector<uint32_t> cells(Lc);
-        for (uint64_t c = 0; c < Lc; ++c) cells[c] = pitched(s, (uint64_t)L->layer_cells[c]);
-        // Which of each layer cell's lower neighbours are in the layer too (their face is theirs).
-        std::vector<uint8_t> below(Lc, 0);
-        const uint64_t strides[3] = {1, nx, nx * ny};
-        for (uint64_t c = 0; c < Lc; ++c)
-            for (int axis = 0; axis < 3; ++axis)
-                if (L->types[(uint64_t)L->layer_cells[c] - strides[axis]] == kLayer) below[c] |= (uint8_t)(1u << axis);
-        const uint32_t *p;
-        if ((rc = upload(s, cells.data(), Lc, &p))) return rc;
-        g.layer_cells = p;
-        if ((rc = upload(s, below.data(), Lc, &u8))) return rc;
-        g.layer_below = u8;
+        s->layer_cells.resize(Lc);
+        for (uint64_t c = 0; c < Lc; ++c) s->layer_cells[c] = pitched(s, (uint64_t)L->layer_cells[c]);
         const uint64_t len[3] = {nx + 1, ny + 1, nz + 1};
         for (int axis = 0; axis < 3; ++axis) {
             std::vector<float4> packed(len[axis]);
@@ -670,11 +685,8 @@ int build(fdtd_solver *s, const fdtd_layout *L) {
                                         L->push[2 * axis + 1][x]);
             const float4 *p4;
             if ((rc = upload(s, packed.data(), len[axis], &p4))) return rc;
-            g.layer_coef[axis] = p4;
-        }
-        if (s->scaled) {
-            if ((rc = upload(s, L->layer_scale, Lc, &fp))) return rc;
-            g.layer_scale = fp;
+            s->bulk.layer_coef[axis] = p4;
+            s->bulk.parts[axis] = static_cast<char *>(s->layer_parts) + e * s->n_device * axis;
         }
     }
 
@@ -716,6 +728,269 @@ void release(fdtd_solver *s) {
     if (s->side) cudaStreamDestroy(s->side);
     if (s->stream) cudaStreamDestroy(s->stream);
     cudaSetDevice(current);
+}
+
+// ---------------------------------------------------------------------------------------------
+// The adjoint (see fdtd_adjoint.cuh)
+// ---------------------------------------------------------------------------------------------
+
+template <typename V>
+int download(fdtd_solver *s, const V *device, size_t count, std::vector<V> &host) {
+    host.resize(count);
+    if (count) CUDA_TRY(s, cudaMemcpy(host.data(), device, count * sizeof(V), cudaMemcpyDeviceToHost));
+    return FDTD_OK;
+}
+
+// The transposed links and the correction list, from the handle's own device tables.
+int set_up_adjoint(fdtd_solver *s) {
+    if (s->adjoint_ready) return FDTD_OK;
+    if (s->wide || s->scaled || s->layers)
+        return fail(s, FDTD_EINVAL,
+                    "the adjoint takes the 7-point stencil without a matched layer or a speed of sound per cell");
+    const Tables &g = s->tables;
+    const uint64_t K = s->specials, S = s->states;
+    const size_t e = s->precision == FDTD_FP64 ? 8 : 4;
+    std::vector<uint32_t> special;
+    std::vector<uint8_t> count, direction, types;
+    std::vector<float> weight, coef_a, coef_inv;
+    int rc;
+    if ((rc = download(s, g.special, K, special))) return rc;
+    if ((rc = download(s, g.link_count, K, count))) return rc;
+    if ((rc = download(s, g.link_direction, (size_t)g.link_slots * K, direction))) return rc;
+    if ((rc = download(s, g.link_weight, (size_t)g.link_slots * K, weight))) return rc;
+    if ((rc = download(s, g.coef_a, K, coef_a))) return rc;
+    if ((rc = download(s, g.coef_inv, K, coef_inv))) return rc;
+    if ((rc = download(s, s->types_device, s->n_device, types))) return rc;
+    const double axial = (double)s->bulk.axial;
+    std::unordered_map<uint32_t, uint32_t> row_of;
+    row_of.reserve(K * 2);
+    for (uint64_t k = 0; k < K; ++k) row_of[special[k]] = (uint32_t)k;
+    // Readers of each special row's cell: the row itself, its interior neighbours, the special
+    // rows linking to it; and the interior cells special rows link to.
+    std::vector<std::vector<std::pair<uint64_t, double>>> readers(K);  // (index | kind << 63, coef)
+    std::unordered_map<uint32_t, std::vector<std::pair<uint32_t, double>>> corrected;
+    const uint64_t kind_bit = 1ull << 63;
+    for (uint64_t k = 0; k < K; ++k) {
+        const uint32_t i = special[k];
+        readers[k].push_back({kind_bit | k, (double)coef_inv[k] * (double)coef_a[k]});
+        for (int d = 0; d < 6; ++d) {
+            const uint32_t j = (uint32_t)((int64_t)i + g.offset[d]);
+            if (types[j] == kInterior) readers[k].push_back({j, axial});
+        }
+        for (uint32_t l = 0; l < count[k]; ++l) {
+            const uint64_t at = (uint64_t)l * K + k;
+            const uint32_t j = (uint32_t)((int64_t)i + g.offset[direction[at]]);
+            const double coef = (double)coef_inv[k] * (double)weight[at];
+            auto it = row_of.find(j);
+            if (it != row_of.end()) {
+                readers[it->second].push_back({kind_bit | k, coef});
+            } else if (types[j] == kInterior) {
+                corrected[j].push_back({(uint32_t)k, coef});
+            } else {
+                return fail(s, FDTD_EINVAL, "a special row links to a cell that is neither interior nor special");
+            }
+        }
+    }
+    std::vector<uint32_t> reader_start(K + 1, 0), reader_index;
+    std::vector<uint8_t> reader_kind;
+    std::vector<double> reader_coef;
+    for (uint64_t k = 0; k < K; ++k) {
+        for (const auto &[idx, coef] : readers[k]) {
+            reader_index.push_back((uint32_t)(idx & ~kind_bit));
+            reader_kind.push_back((idx & kind_bit) ? 1 : 0);
+            reader_coef.push_back(coef);
+        }
+        reader_start[k + 1] = (uint32_t)reader_index.size();
+    }
+    std::vector<uint32_t> cells, starts{0}, rows;
+    std::vector<double> coefs;
+    for (auto &[cell, list] : corrected) {
+        cells.push_back(cell);
+        for (const auto &[r, c] : list) rows.push_back(r), coefs.push_back(c);
+        starts.push_back((uint32_t)rows.size());
+    }
+    AdjointTables &t = s->adjoint;
+    t.specials = (uint32_t)K, t.states = (uint32_t)S;
+    t.special = g.special, t.state_start = g.state_start;
+    t.state_weight = g.state_weight, t.state_now = g.state_now, t.state_before = g.state_before, t.state_gain = g.state_gain;
+    t.coef_b = g.coef_b, t.coef_inv = g.coef_inv;
+    t.axial = s->bulk.axial;
+    t.probes = g.probes, t.probe_start = g.probe_start, t.probe_cells = g.probe_cells, t.probe_weights = g.probe_weights;
+    t.corrected = (uint32_t)cells.size();
+    const uint32_t *p32;
+    const uint8_t *p8;
+    const double *pd;
+    if ((rc = upload(s, reader_start.data(), reader_start.size(), &p32))) return rc;
+    t.reader_start = p32;
+    if ((rc = upload(s, reader_index.data(), reader_index.size(), &p32))) return rc;
+    t.reader_index = p32;
+    if ((rc = upload(s, reader_kind.data(), reader_kind.size(), &p8))) return rc;
+    t.reader_kind = p8;
+    if ((rc = upload(s, reader_coef.data(), reader_coef.size(), &pd))) return rc;
+    t.reader_coef = pd;
+    if ((rc = upload(s, cells.data(), cells.size(), &p32))) return rc;
+    t.corrected_cell = p32;
+    if ((rc = upload(s, starts.data(), starts.size(), &p32))) return rc;
+    t.corrected_start = p32;
+    if ((rc = upload(s, rows.data(), rows.size(), &p32))) return rc;
+    t.corrected_row = p32;
+    if ((rc = upload(s, coefs.data(), coefs.size(), &pd))) return rc;
+    t.corrected_coef = pd;
+    for (int k = 0; k < 2; ++k) {
+        if ((rc = zeros(s, e * s->n_device, &s->lam[k]))) return rc;
+        if ((rc = zeros(s, e * S, &s->om[k]))) return rc;
+    }
+    if ((rc = zeros(s, e * K, &s->tilde))) return rc;
+    if (s->bulk_blocks) {
+        const CUtensorMapDataType ft = s->precision == FDTD_FP64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+        for (int k = 0; k < 2; ++k) {
+            if ((rc = tensor_map(s, &s->lam_b[k], s->lam[k], ft, (uint32_t)e, kBX, kBY))) return rc;
+            if ((rc = tensor_map(s, &s->lam_a[k], s->lam[k], ft, (uint32_t)e, kTX, kTY))) return rc;
+        }
+    }
+    s->adjoint_ready = true;
+    return FDTD_OK;
+}
+
+// Device scratch of one fdtd_gradient call, freed at its end.
+struct Scratch {
+    fdtd_solver *s;
+    std::vector<void *> blocks;
+    explicit Scratch(fdtd_solver *solver) : s(solver) {}
+    ~Scratch() {
+        for (void *p : blocks) cudaFree(p);
+    }
+    int take(size_t bytes, void **out) {
+        *out = nullptr;
+        void *p = nullptr;
+        CUDA_TRY(s, cudaMalloc(&p, bytes ? bytes : 16));
+        blocks.push_back(p);
+        CUDA_TRY(s, cudaMemset(p, 0, bytes ? bytes : 16));
+        *out = p;
+        return FDTD_OK;
+    }
+};
+
+template <typename T>
+int gradient(fdtd_solver *s, const float *signal, uint64_t steps, const double *dloss, uint64_t segment,
+             double *grads[5]) {
+    const uint64_t K = s->specials, S = s->states, P = s->probes;
+    const size_t e = sizeof(T);
+    if (segment == 0 || segment > steps) segment = steps;
+    const uint64_t segments = (steps + segment - 1) / segment;
+    Scratch scratch(s);
+    void *p;
+    int rc;
+    // On the device: the drive, dL/dy, one segment's trajectory, the gradient's sums, and the
+    // state at the start of every segment after the first (the checkpoints).
+    if ((rc = scratch.take(sizeof(float) * steps, &p))) return rc;
+    float *d_signal = static_cast<float *>(p);
+    CUDA_TRY(s, cudaMemcpy(d_signal, signal, sizeof(float) * steps, cudaMemcpyHostToDevice));
+    if ((rc = scratch.take(sizeof(double) * std::max<uint64_t>(1, P) * steps, &p))) return rc;
+    double *d_dloss = static_cast<double *>(p);
+    if (P) CUDA_TRY(s, cudaMemcpy(d_dloss, dloss, sizeof(double) * P * steps, cudaMemcpyHostToDevice));
+    if ((rc = scratch.take(e * K * (segment + 2), &p))) return rc;
+    T *traj_u = static_cast<T *>(p);
+    if ((rc = scratch.take(e * S * (segment + 2), &p))) return rc;
+    T *traj_w = static_cast<T *>(p);
+    if ((rc = scratch.take(sizeof(double) * std::max<uint64_t>(1, P) * segment, &p))) return rc;
+    double *d_out = static_cast<double *>(p);
+    double *g[5];
+    const uint64_t g_len[5] = {K, K, S, S, S};  // coef_b, coef_inv, now, before, gain
+    for (int k = 0; k < 5; ++k) {
+        if ((rc = scratch.take(sizeof(double) * g_len[k], &p))) return rc;
+        g[k] = static_cast<double *>(p);
+    }
+    const uint64_t level_bytes = e * s->n_device, state_bytes = e * S;
+    auto save = [&](char *c) -> int {
+        CUDA_TRY(s, cudaMemcpyAsync(c, s->u[1], level_bytes, cudaMemcpyDeviceToDevice, s->stream));
+        CUDA_TRY(s, cudaMemcpyAsync(c + level_bytes, s->u[0], level_bytes, cudaMemcpyDeviceToDevice, s->stream));
+        if (S) {
+            CUDA_TRY(s, cudaMemcpyAsync(c + 2 * level_bytes, s->w[1], state_bytes, cudaMemcpyDeviceToDevice, s->stream));
+            CUDA_TRY(s, cudaMemcpyAsync(c + 2 * level_bytes + state_bytes, s->w[0], state_bytes,
+                                        cudaMemcpyDeviceToDevice, s->stream));
+        }
+        return FDTD_OK;
+    };
+    auto restore = [&](const char *c) -> int {
+        CUDA_TRY(s, cudaMemcpyAsync(s->u[1], c, level_bytes, cudaMemcpyDeviceToDevice, s->stream));
+        CUDA_TRY(s, cudaMemcpyAsync(s->u[0], c + level_bytes, level_bytes, cudaMemcpyDeviceToDevice, s->stream));
+        if (S) {
+            CUDA_TRY(s, cudaMemcpyAsync(s->w[1], c + 2 * level_bytes, state_bytes, cudaMemcpyDeviceToDevice, s->stream));
+            CUDA_TRY(s, cudaMemcpyAsync(s->w[0], c + 2 * level_bytes + state_bytes, state_bytes,
+                                        cudaMemcpyDeviceToDevice, s->stream));
+        }
+        return FDTD_OK;
+    };
+    // The forward pass from rest, keeping checkpoints[m] = the state at the start of segment m+1.
+    if ((rc = fdtd_reset(s)) != FDTD_OK) return rc;
+    std::vector<char *> checkpoints;
+    for (uint64_t k = 0; k + 1 < segments; ++k) {
+        if ((rc = dispatch(s, d_signal + k * segment, segment, d_out, segment)) != FDTD_OK) return rc;
+        settle(s, segment);
+        if ((rc = scratch.take(2 * level_bytes + 2 * state_bytes, &p))) return rc;
+        checkpoints.push_back(static_cast<char *>(p));
+        if ((rc = save(checkpoints.back())) != FDTD_OK) return rc;
+    }
+    // The adjoint levels beyond the end are at rest; the sums start at 0.
+    for (int k = 0; k < 2; ++k) {
+        CUDA_TRY(s, cudaMemsetAsync(s->lam[k], 0, level_bytes, s->stream));
+        if (S) CUDA_TRY(s, cudaMemsetAsync(s->om[k], 0, state_bytes, s->stream));
+    }
+    const AdjointTables &t = s->adjoint;
+    const uint32_t row_blocks = (uint32_t)((std::max<uint64_t>(std::max<uint64_t>(K, S), 1) + kBlock - 1) / kBlock);
+    const uint32_t special_blocks = (uint32_t)((K + kBlock - 1) / kBlock);
+    const uint32_t corrected_blocks = (uint32_t)((t.corrected + kBlock - 1) / kBlock);
+    const uint32_t probe_blocks = (uint32_t)((P + kBlock - 1) / kBlock);
+    const uint32_t smem = Stage<T, false>::smem;
+    T *tilde = static_cast<T *>(s->tilde);
+    int x = 0;  // lam[x], om[x]: level n+1; lam[1-x], om[1-x]: level n+2, then level n
+    for (uint64_t k = segments; k-- > 0;) {
+        const uint64_t s0 = k * segment, s1 = std::min(steps, s0 + segment);
+        // Recompute the segment from its start, recording each level of the special rows.
+        if (k == 0) {
+            if ((rc = fdtd_reset(s)) != FDTD_OK) return rc;
+        } else if ((rc = restore(checkpoints[k - 1])) != FDTD_OK) {
+            return rc;
+        }
+        record_kernel<T><<<row_blocks, kBlock, 0, s->stream>>>(t, static_cast<const T *>(s->u[0]),
+                                                               static_cast<const T *>(s->w[0]), traj_u, traj_w);
+        for (uint64_t n = s0; n < s1; ++n) {
+            const uint64_t level = n - s0 + 1;
+            record_kernel<T><<<row_blocks, kBlock, 0, s->stream>>>(
+                t, static_cast<const T *>(s->u[1]), static_cast<const T *>(s->w[1]), traj_u + level * K, traj_w + level * S);
+            if ((rc = dispatch(s, d_signal + n, 1, d_out, 1)) != FDTD_OK) return rc;
+            settle(s, 1);
+        }
+        record_kernel<T><<<row_blocks, kBlock, 0, s->stream>>>(t, static_cast<const T *>(s->u[1]),
+                                                               static_cast<const T *>(s->w[1]),
+                                                               traj_u + (s1 - s0 + 1) * K, traj_w + (s1 - s0 + 1) * S);
+        // The reverse steps of the segment.
+        for (uint64_t n = s1; n-- > s0;) {
+            T *lam_next = static_cast<T *>(s->lam[x]), *lam_out = static_cast<T *>(s->lam[1 - x]);
+            T *om_next = static_cast<T *>(s->om[x]), *om_out = static_cast<T *>(s->om[1 - x]);
+            if (special_blocks) tilde_kernel<T><<<special_blocks, kBlock, 0, s->stream>>>(t, lam_next, om_next, tilde);
+            if (s->bulk_blocks) {
+                BulkArgs args = s->bulk;
+                args.a = lam_out;
+                bulk_kernel<T, false, false, false><<<s->bulk_blocks, kBlock, smem, s->stream>>>(s->lam_b[x], s->lam_a[1 - x],
+                                                                                        s->map_t, s->map_s, args);
+            }
+            if (corrected_blocks) correct_kernel<T><<<corrected_blocks, kBlock, 0, s->stream>>>(t, lam_next, tilde, lam_out);
+            if (special_blocks)
+                special_adjoint_kernel<T><<<special_blocks, kBlock, 0, s->stream>>>(
+                    t, lam_next, om_next, tilde, lam_out, om_out, traj_u, traj_w, (uint32_t)(n - s0), g[1], g[0], g[2],
+                    g[3], g[4]);
+            if (probe_blocks) probe_adjoint_kernel<T><<<probe_blocks, kBlock, 0, s->stream>>>(t, d_dloss, steps, n, lam_out);
+            x = 1 - x;
+        }
+        CUDA_TRY(s, cudaGetLastError());
+    }
+    CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+    if ((rc = check_device_error(s)) != FDTD_OK) return rc;
+    for (int k = 0; k < 5; ++k)
+        if (grads[k] && g_len[k]) CUDA_TRY(s, cudaMemcpy(grads[k], g[k], sizeof(double) * g_len[k], cudaMemcpyDeviceToHost));
+    return fdtd_reset(s);
 }
 
 struct DeviceGuard {
@@ -915,6 +1190,19 @@ int fdtd_get_timing(fdtd_solver *s, double ms[4], uint64_t *steps) {
     return FDTD_OK;
 }
 
+int fdtd_gradient(fdtd_solver *s, const float *signal, uint64_t steps, const double *dloss_dy, uint64_t segment,
+                  double *grad_coef_b, double *grad_coef_inv, double *grad_now, double *grad_before, double *grad_gain) {
+    if (!s) return set_global(FDTD_EINVAL, "no solver");
+    if (steps == 0) return fail(s, FDTD_EINVAL, "no steps to differentiate");
+    if (!signal || (s->probes && !dloss_dy)) return fail(s, FDTD_EINVAL, "no signal or loss gradient");
+    DeviceGuard guard(s->device);
+    int rc = set_up_adjoint(s);
+    if (rc != FDTD_OK) return rc;
+    double *grads[5] = {grad_coef_b, grad_coef_inv, grad_now, grad_before, grad_gain};
+    return s->precision == FDTD_FP64 ? gradient<double>(s, signal, steps, dloss_dy, segment, grads)
+                                     : gradient<float>(s, signal, steps, dloss_dy, segment, grads);
+}
+
 int fdtd_reset(fdtd_solver *s) {
     if (!s) return set_global(FDTD_EINVAL, "no solver");
     DeviceGuard guard(s->device);
@@ -924,7 +1212,7 @@ int fdtd_reset(fdtd_solver *s) {
         if (s->states) CUDA_TRY(s, cudaMemsetAsync(s->w[k], 0, e * s->states, s->stream));
     }
     if (s->layers) {
-        CUDA_TRY(s, cudaMemsetAsync(s->layer_parts, 0, e * 3 * s->layers, s->stream));
+        CUDA_TRY(s, cudaMemsetAsync(s->layer_parts, 0, e * 3 * s->n_device, s->stream));
         for (int k = 0; k < 2; ++k)
             for (int axis = 0; axis < 3; ++axis)
                 CUDA_TRY(s, cudaMemsetAsync(s->faces[k][axis], 0, e * s->n_device, s->stream));
@@ -979,14 +1267,15 @@ int fdtd_read_state(const fdtd_solver *cs, void *current, void *previous, void *
     if (layer_state && s->layers) {
         // The reference's nine values per cell (fdtd.hpp:2245): the parts, then per axis the
         // velocity of the - face (the + face of the cell below) and of the + face.
-        std::vector<char> parts(e * 3 * s->layers);
-        CUDA_TRY(s, cudaMemcpy(parts.data(), s->layer_parts, parts.size(), cudaMemcpyDeviceToHost));
-        std::vector<uint32_t> cells(s->layers);
-        CUDA_TRY(s, cudaMemcpy(cells.data(), s->tables.layer_cells, 4 * s->layers, cudaMemcpyDeviceToHost));
-        std::vector<char> face(e * s->n_device);
+        const std::vector<uint32_t> &cells = s->layer_cells;
+        std::vector<char> field(e * s->n_device);
         char *dst = static_cast<char *>(layer_state);
-        for (uint64_t c = 0; c < s->layers; ++c)
-            for (int k = 0; k < 3; ++k) std::memcpy(dst + e * (9 * c + k), parts.data() + e * (k * s->layers + c), e);
+        for (int k = 0; k < 3; ++k) {
+            CUDA_TRY(s, cudaMemcpy(field.data(), static_cast<char *>(s->layer_parts) + e * s->n_device * k, field.size(),
+                                   cudaMemcpyDeviceToHost));
+            for (uint64_t c = 0; c < s->layers; ++c) std::memcpy(dst + e * (9 * c + k), field.data() + e * cells[c], e);
+        }
+        std::vector<char> &face = field;
         const uint64_t strides[3] = {1, s->pitch, s->pitch * s->ny};
         for (int axis = 0; axis < 3; ++axis) {
             CUDA_TRY(s, cudaMemcpy(face.data(), s->faces[1][axis], face.size(), cudaMemcpyDeviceToHost));

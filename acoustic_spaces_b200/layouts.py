@@ -96,11 +96,18 @@ class Grid:
 @dataclass
 class Room:
     """A convex room: the cells with n_f . x < d_f for every plane f. ``materials[f]`` is plane
-    f's wall, or None for an open face (no wall: the air goes through)."""
+    f's wall, or None for an open face (no wall: the air goes through). With ``patches``, the walls
+    are cut into patches: ``patches(planes, points)`` gives the index into ``patch_materials`` of
+    the wall at each crossing point of a plane (arrays)."""
 
     normals: np.ndarray  # (F, 3), unit
     offsets: np.ndarray  # (F,)
     materials: list[Material | None]
+    patches: object = None
+    patch_materials: list[Material] | None = None
+
+    def wall_materials(self) -> list[Material | None]:
+        return list(self.patch_materials) if self.patches is not None else list(self.materials)
 
     @property
     def open(self) -> bool:
@@ -117,6 +124,7 @@ class Built:
     boundary_cells: int
     source_cells: int
     rate: float
+    sensitivity: dict | None = None
 
 
 def _signed(room: Room, grid: Grid, f: int, zs: slice | None = None) -> np.ndarray:
@@ -181,7 +189,17 @@ def _first_wall(room: Room, grid: Grid, start: np.ndarray, end: np.ndarray) -> n
     walls = np.array([mat is not None for mat in room.materials] + [False])
     enter_wall = crosses & (enter >= 0) & walls[enter]
     leave_wall = crosses & (leave >= 0) & walls[leave]
-    return np.where(enter_wall, enter, np.where(leave_wall, leave, -1))
+    face = np.where(enter_wall, enter, np.where(leave_wall, leave, -1))
+    if room.patches is None:
+        return face
+    # The patch of the wall where the link crosses it.
+    hit = face >= 0
+    t = np.where(enter_wall, t_in, t_out)
+    points = ca + t[:, None] * (cb - ca)
+    out = np.full(len(face), -1, np.int64)
+    if np.any(hit):
+        out[hit] = np.asarray(room.patches(face[hit], points[hit]), np.int64)
+    return out
 
 
 def cubic_cells(grid: Grid, point) -> list[tuple[int, float]]:
@@ -308,7 +326,7 @@ def cell_face_layouts(
             raise ValueError("the model reaches into the matched layer")
 
     # Materials: beta and branches.
-    mats = room.materials
+    mats = room.wall_materials()
     betas = np.array([0.0 if m is None else m.beta for m in mats])
     branch_rows, branch_owner = [], []
     for f, m in enumerate(mats):
@@ -503,7 +521,34 @@ def cell_face_layouts(
         return Built(layout, grid, air_cells, B, E, rate or 0.0)
 
     base_special = special
-    return [place(source) for source in sources]
+    # How each boundary row's coefficients depend on the materials (for gradients): per row, each
+    # material's weight of cut links (the kinds above) and the weight of its links to the grid's
+    # edge; each branch's material and (m, r, q).
+    rows_, mats_, weights_ = [], [], []
+    for slot in range(6):
+        has = kinds[slot] >= 0
+        rows_.append(np.flatnonzero(has))
+        mats_.append(kinds[slot][has])
+        weights_.append(kind_weight[slot][has])
+    edge_weight = np.zeros(B)
+    for k in range(6):
+        edge_weight = edge_weight + np.where(blk[k] & (mat[k] == -2), BOUNDARY, 0.0)
+    sensitivity = {
+        "row": np.concatenate(rows_) if rows_ else np.zeros(0, np.int64),
+        "material": np.concatenate(mats_) if mats_ else np.zeros(0, np.int64),
+        "weight": np.concatenate(weights_) if weights_ else np.zeros(0),
+        "edge_weight": edge_weight,
+        "edge_admittance": edge_admittance,
+        "boundary_rows": B,
+        "r": r,
+        "branch_material": branch_owner,
+        "branch_mrq": branch_rows,
+        "materials": len(mats),
+    }
+    built = [place(source) for source in sources]
+    for b in built:
+        b.sensitivity = sensitivity
+    return built
 
 
 # ---- seeded synthetic rooms ------------------------------------------------------------------

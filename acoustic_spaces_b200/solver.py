@@ -157,6 +157,37 @@ class B200WaveSolver:
         """The address of the solver's CUDA stream (for events and ordering)."""
         return int(self._lib.fdtd_stream(self._handle) or 0)
 
+    def gradient(self, signal: np.ndarray, dloss_dy: np.ndarray, segment: int = 250) -> dict[str, np.ndarray]:
+        """The gradient of a loss L of the probes' series with respect to the layout's
+        coefficients, by the reverse-time stepper: the run from rest on ``signal`` gives the
+        series y (probes, steps); ``dloss_dy`` is dL/dy. Returns dL/d ``coef_b``, ``coef_inv``
+        (one per special row) and dL/d ``now``, ``before``, ``gain`` (one per branch state). The
+        forward pass is recomputed in segments of ``segment`` steps from checkpoints. The solver
+        is left at rest."""
+        signal = np.ascontiguousarray(signal, np.float32).reshape(-1)
+        steps = len(signal)
+        dloss = np.ascontiguousarray(dloss_dy, np.float64).reshape(self._probes, steps)
+        info = self.info()
+        out = {
+            "coef_b": np.zeros(int(info.special_cells)),
+            "coef_inv": np.zeros(int(info.special_cells)),
+            "now": np.zeros(int(info.branch_states)),
+            "before": np.zeros(int(info.branch_states)),
+            "gain": np.zeros(int(info.branch_states)),
+        }
+        f64 = ctypes.POINTER(ctypes.c_double)
+        status = self._lib.fdtd_gradient(
+            self._handle,
+            signal.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+            steps,
+            dloss.ctypes.data_as(f64),
+            int(segment),
+            *(a.ctypes.data_as(f64) for a in out.values()),
+        )
+        if status != _abi.FDTD_OK:
+            _raise(self._lib, status, self._handle)
+        return out
+
     def set_timing(self, enable: bool) -> None:
         """Brackets each kernel of the following run_device steps with CUDA events."""
         status = self._lib.fdtd_set_timing(self._handle, int(bool(enable)))

@@ -49,8 +49,9 @@ BYTES_SPECIAL = 40  # read p, read/write p-, coef_a/b/inv/source, its index and 
 BYTES_LINK = 5  # direction and weight
 BYTES_STATE = 28  # read/write w-, read w, its four coefficients
 # A layer cell keeps three pressure parts and, on the cell below each face, one velocity per
-# face (the reference's nine values per cell hold every face twice, 84 B):
-BYTES_LAYER = 60  # read p, write p+, read/write three parts, read/write three faces, its index
+# face (the reference's nine values per cell hold every face twice, 84 B); it is swept with the
+# interior, so it has no index of its own:
+BYTES_LAYER = 56  # read p, write p+, read/write three parts, read/write three faces
 
 
 def algorithmic_bytes(d: dict) -> int:
@@ -252,7 +253,7 @@ def run_reference(args, rank: int, world: int) -> None:
 def run_batched(args, world: int, rank: int, local: int) -> None:
     """The batched configuration: many shoebox rooms with several sources each, every (room,
     source) a solve of its own, stacked into one grid and stepped by one launch per kind per step
-    Beside it, a sample of the same solves stepped one after another through
+    (64 rooms of 3-12 m at 5 cm cells, 4 sources each: 256 solves). Beside it, a sample of the same solves stepped one after another through
     the same public API, and each solve's FP32 error against FP64."""
     import torch
 
@@ -329,7 +330,85 @@ def run_batched(args, world: int, rank: int, local: int) -> None:
         "batched_over_sequential": round(value / sequential, 3),
         "per_solve_ir_rel_l2_vs_fp64": {"max": float(max(worst)), "median": float(np.median(worst)), "steps": m},
         "clocks": clocks.summary(),
-        "gpu_launches": 4 * steps,
+        "gpu_launches": 3 * steps,  # the sweep, the special rows, the probes
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def run_adjoint(args, world: int, rank: int, local: int) -> None:
+    """The adjoint fit: a 10 x 8 x 4 m room at 5 cm cells with 8
+    materials on seeded patches, a 1-pole admittance each (16 parameters); the misfit of the
+    responses at 4 receivers over 3000 steps to those at seeded true parameters, from parameters
+    off by up to 30 %; checkpoints every 250 steps. Reports the forward and forward + adjoint
+    times, the gradient against central differences (relative step 1e-4, taken in the layout's
+    float32 coefficients along each parameter's tangent) and the FP32 gradient against the FP64
+    one, the peak device memory, and the Adam iterations to recover every parameter to 1 %."""
+    import torch
+
+    from acoustic_spaces_b200 import fit
+
+    problem = fit.patched_room(args.seed, steps=args.adjoint_steps, segment=250)
+    f = problem.fit
+    params = problem.start
+    f.responses(params, "fp32")  # warm-up
+    times = []
+    for _ in range(3):
+        f.loss_and_gradient(params, "fp32")
+        times.append((f.forward_s, f.gradient_s))
+    forward_s = min(t[0] for t in times)
+    gradient_s = min(t[1] for t in times)
+    # Peak device memory of a gradient: free memory sampled while it runs.
+    free_min = [torch.cuda.mem_get_info(local)[0]]
+    stop = threading.Event()
+
+    def watch():
+        while not stop.is_set():
+            free_min[0] = min(free_min[0], torch.cuda.mem_get_info(local)[0])
+            time.sleep(0.002)
+
+    total = torch.cuda.mem_get_info(local)[1]
+    watcher = threading.Thread(target=watch, daemon=True)
+    watcher.start()
+    _, g32 = f.loss_and_gradient(params, "fp32")
+    stop.set()
+    watcher.join()
+    _, g64, G64 = f.loss_and_gradient(params, "fp64", coefficients=True)
+    _, _, G32 = f.loss_and_gradient(params, "fp32", coefficients=True)
+    # Central differences of L in the coefficients along each parameter's tangent (relative step
+    # 1e-4, exactly symmetric float32 steps), against the FP64 and the FP32 adjoint.
+    cd64, cd32 = [], []
+    for i in range(len(params.vector())):
+        p64, measured = f.central_difference(params, i, G64)
+        p32, _ = f.central_difference(params, i, G32)
+        cd64.append(abs(p64 - measured) / abs(measured))
+        cd32.append(abs(p32 - measured) / abs(measured))
+    rel = lambda a, b: float(np.max(np.abs(a - b)) / np.max(np.abs(b)))  # noqa: E731
+    result = fit.adam(problem, iterations=args.adam_iterations, rate=0.03)
+    line = {
+        "metric": METRIC,
+        "value": round(f.built.air_cells * len(f.signal) / forward_s / 1e9, 4),
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": len(f.signal),
+        "warmup": 1,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": "adjoint_fit", **problem.description},
+        "adjoint_over_forward": round((forward_s + gradient_s) / forward_s, 3),
+        "forward_s": round(forward_s, 4),
+        "gradient_s": round(gradient_s, 4),
+        "gradient_vs_central_differences": {
+            "max_rel": max(cd64), "h": 1e-4, "precision": "fp64",
+            "difference": "L(c + d) - L(c - d) over 2, d the coefficients' change along each parameter, exact float32 steps",
+        },
+        "fp32_gradient_vs_central_differences": {"max_rel": max(cd32)},
+        "fp32_gradient_vs_fp64": {"max_rel": rel(g32, g64)},
+        "peak_device_bytes": int(total - free_min[0]),
+        "adam": {k: result[k] for k in ("iterations", "converged", "worst_relative_error")},
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -348,11 +427,14 @@ def main() -> None:
     parser.add_argument("--reference-repeats", type=int, default=3)
     parser.add_argument("--no-cpu-baseline", action="store_true")
     parser.add_argument("--no-e2e", action="store_true")
-    parser.add_argument("--workload", choices=["polyhedral_room", "batched_rooms"], default="polyhedral_room")
+    parser.add_argument("--workload", choices=["polyhedral_room", "batched_rooms", "adjoint_fit"], default="polyhedral_room")
+    parser.add_argument("--adjoint-steps", type=int, default=3000)
+    parser.add_argument("--adam-iterations", type=int, default=300)
     parser.add_argument("--rooms", type=int, default=64)
     parser.add_argument("--sources", type=int, default=4)
     parser.add_argument("--sequential-sample", type=int, default=16)
     parser.add_argument("--no-ir-error", action="store_true")
+    parser.add_argument("--kernel-steps", type=int, default=200, help="steps of the per-kernel timing pass")
     parser.add_argument("--ir-steps", type=int, default=2000, help="steps of the FP32-vs-FP64 comparison")
     args = parser.parse_args()
 
@@ -374,6 +456,9 @@ def main() -> None:
     torch.cuda.set_device(local)
     if args.workload == "batched_rooms":
         run_batched(args, world, rank, local)
+        return
+    if args.workload == "adjoint_fit":
+        run_adjoint(args, world, rank, local)
         return
     if world > 1:
         from datetime import timedelta
@@ -406,7 +491,6 @@ def main() -> None:
         barrier()
         torch.cuda.synchronize()
         solver.synchronize()
-        solver.set_timing(True)  # CUDA events around each kernel, on its own stream
         with torch.cuda.stream(stream):
             start.record(stream)
         solver.run_device(sig_dev.data_ptr() + 4 * warmup, steps, out_dev.data_ptr() + 8 * warmup, steps + warmup)
@@ -416,6 +500,12 @@ def main() -> None:
         torch.cuda.synchronize()
         barrier()
     ms = start.elapsed_time(end)
+    # Each kernel's own duration: a second timed pass with CUDA events around every launch, the
+    # step's kernels one after another on the solver's stream.
+    timed = max(3, min(steps, args.kernel_steps))
+    solver.set_timing(True)
+    solver.run_device(sig_dev.data_ptr(), timed, out_dev.data_ptr(), steps + warmup)
+    solver.synchronize()
     solver.set_timing(False)
     kernel_ms = solver.timing()
     if world > 1:
@@ -468,9 +558,9 @@ def main() -> None:
     peak, peak_source = measured_peaks()
     achieved = bytes_per_step / (ms / 1e3 / steps) / 1e9
     # Each kernel's algorithmic bytes per launch and its average launch time, live.
+    # (The sweep kernel steps the interior and the matched-layer cells.)
     per_kernel_bytes = {
-        "bulk": BYTES_INTERIOR * desc["interior_cells"],
-        "layer": BYTES_LAYER * desc["layer_cells"],
+        "bulk": BYTES_INTERIOR * desc["interior_cells"] + BYTES_LAYER * desc["layer_cells"],
         "special": BYTES_SPECIAL * desc["special_rows"] + BYTES_LINK * desc["links"] + BYTES_STATE * desc["branch_states"],
     }
     traffic_table = {}
@@ -490,6 +580,8 @@ def main() -> None:
         }
     kernels["probe"] = {"mean_launch_us": round(kernel_ms["probe"] / max(1, kernel_ms["steps"]) * 1e3, 2)}
     dominant = max(per_kernel_bytes, key=lambda k: kernel_ms[k])
+    # Launches a step: the sweep, the special rows, the probes (each when the grid has its cells).
+    launches_per_step = int(desc["interior_cells"] + desc["layer_cells"] > 0) + int(desc["special_rows"] > 0) + int(solver.probes > 0)
 
     line = None
     if rank == 0:
@@ -521,10 +613,10 @@ def main() -> None:
                 "precision": "FP32, bit-exact with the reference (no FMA, subnormals flushed)",
             },
             "e2e": e2e,
-            "gpu_launches": 4 * steps,
+            "gpu_launches": launches_per_step * steps,
             "roofline": {
                 "bound": "hbm",
-                "kernel": f"{dominant}_kernel (the longest of the step's four, by CUDA events)",
+                "kernel": f"{dominant}_kernel (the longest of the step's kernels, by CUDA events)",
                 "achieved": kernels[dominant]["achieved"],
                 "peak": peak,
                 "unit": "GB/s",

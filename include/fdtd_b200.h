@@ -147,13 +147,30 @@ void *fdtd_stream(const fdtd_solver *solver);
 
 /*
  * Per-kernel timing of fdtd_run_device (no counterpart in the reference): with `enable` set, each
- * step's four kernels are bracketed by CUDA events on the streams they run on, and
- * fdtd_get_timing adds up, since the last call, the milliseconds each kind took — ms[0] the
- * interior sweep, ms[1] the matched layer, ms[2] the special rows, ms[3] the probe records — over
- * *steps steps. The work done is the same; only events are added between the launches.
+ * step's kernels run one after another on the handle's stream, each bracketed by CUDA events, and
+ * fdtd_get_timing adds up, since the last call, the milliseconds each kind took — ms[0] the sweep
+ * of the interior and matched-layer cells, ms[1] 0 (the matched layer has no kernel of its own),
+ * ms[2] the special rows, ms[3] the probe records — over *steps steps. The work done is the same.
  */
 int fdtd_set_timing(fdtd_solver *solver, int enable);
 int fdtd_get_timing(fdtd_solver *solver, double ms[4], uint64_t *steps);
+
+/*
+ * The gradient of a loss of the probes' series by the reverse-time (adjoint) stepper; no
+ * counterpart in the reference, whose absorption fit searches by finite differences
+ * (engine/impedance.py:379-440). From rest, a run of `steps` steps on `signal` gives the series
+ * y (probes x steps); given dloss_dy = dL/dy (host, probes x steps), fdtd_gradient returns dL/d of
+ * each special row's coef_b and coef_inv (special_count each) and of each branch state's now,
+ * before and gain coefficients (state_count each; the state's branch's, fdtd.hpp:797-805), summed
+ * over the run in double; any output may be NULL. The forward pass is recomputed in segments of
+ * `segment` steps from checkpoints of the whole state kept at each segment's start (0: one
+ * segment), recording each step's values at the special rows; the adjoint then steps back
+ * through each segment. Grids of the 7-point stencil without a matched layer or a speed field
+ * only (FDTD_EINVAL otherwise). The solver is left at rest.
+ */
+int fdtd_gradient(fdtd_solver *solver, const float *signal, uint64_t steps, const double *dloss_dy,
+                  uint64_t segment, double *grad_coef_b, double *grad_coef_inv, double *grad_now,
+                  double *grad_before, double *grad_gain);
 
 /* Replaces WaveSolver::reset (fdtd.hpp:906-915): silences the grid. */
 int fdtd_reset(fdtd_solver *solver);

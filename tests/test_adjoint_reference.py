@@ -1,0 +1,102 @@
+"""The autograd checker of the reverse-time stepper, pinned on the CPU (no GPU).
+
+Its forward equals the FP64 oracle's, and its gradient equals central differences of the loss taken
+with exactly symmetric float32 steps of the coefficients (a coefficient of the layout is a float32,
+so a step is a whole number of units in the last place: c + d and c - d are then both exact, and
+the central difference keeps no second-order term). The material fit's ``central_difference``
+is checked the same way, with the oracle standing in for the B200 stepper.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+from conftest import load_golden
+
+import adjoint_reference
+from acoustic_spaces_b200 import fit
+from oracle.oracle import OracleSolver
+
+_FAMILIES = (("coef_b", "coef_b"), ("coef_inv", "coef_inv"), ("branch_now", "now"),
+             ("branch_before", "before"), ("branch_gain", "gain"))  # fmt: skip
+
+
+def _misfit(layout, signal, seed=0):
+    rng = np.random.default_rng(seed)
+    base = OracleSolver(layout, "fp64").run(signal)
+    target = 0.8 * base + 0.01 * np.abs(base).max() * rng.standard_normal(base.shape)
+    return base, target
+
+
+@pytest.mark.parametrize("name", ["resonant7", "drive7", "fitted_closed"])
+def test_the_autograd_stepper_steps_as_the_oracle(name):
+    layout, signal, _ = load_golden(name)
+    ours = adjoint_reference.series(layout, signal[:200])
+    oracle = OracleSolver(layout, "fp64").run(signal[:200])
+    assert np.max(np.abs(ours - oracle)) <= 1e-12 * np.max(np.abs(oracle))
+
+
+@pytest.mark.parametrize("name", ["resonant7", "drive7", "fitted_closed"])
+def test_the_autograd_gradient_matches_symmetric_central_differences(name):
+    layout, signal, _ = load_golden(name)
+    signal = signal[:300]
+    y, target = _misfit(layout, signal)
+    grad = adjoint_reference.gradient(layout, signal, 2.0 * (y - target))
+    rng = np.random.default_rng(1)
+    branch = np.asarray(layout["state_branch"], np.int64)
+    plus, minus = dict(layout), dict(layout)
+    predicted = 0.0
+    for name_, key in _FAMILIES:
+        c0 = np.asarray(layout[name_], np.float32)
+        unit = np.spacing(np.abs(c0)).astype(np.float64)
+        d = np.round(1e-6 * c0.astype(np.float64) * rng.uniform(-1, 1, len(c0)) / unit) * unit
+        plus[name_] = (c0.astype(np.float64) + d).astype(np.float32)
+        minus[name_] = (c0.astype(np.float64) - d).astype(np.float32)
+        assert np.array_equal(plus[name_].astype(np.float64) - c0, d)
+        assert np.array_equal(c0 - minus[name_].astype(np.float64), d)
+        predicted += float(np.sum(grad[key] * (d[branch] if name_.startswith("branch") else d)))
+    loss = lambda lay: float(np.sum((OracleSolver(lay, "fp64").run(signal) - target) ** 2))  # noqa: E731
+    measured = 0.5 * (loss(plus) - loss(minus))
+    assert abs(predicted - measured) <= 1e-4 * abs(measured), (predicted, measured)
+
+
+class _OracleStepper:
+    """The oracle behind the B200 stepper's forward interface, for host-side tests."""
+
+    def __init__(self, layout, precision="fp32"):
+        self._solver = OracleSolver(layout, precision)
+
+    def run(self, signal):
+        return self._solver.run(signal)
+
+    def close(self):
+        pass
+
+
+def test_central_difference_of_the_material_parameters(monkeypatch):
+    monkeypatch.setattr(fit, "B200WaveSolver", _OracleStepper)
+    problem = fit.patched_room(1, size=(3.0, 2.4, 1.6), cell=0.1, steps=400, precision="fp64", segment=100)
+    f, params = problem.fit, problem.start
+    lay = f.layout(params)
+    y = OracleSolver(lay, "fp64").run(f.signal)
+    G = adjoint_reference.gradient(lay, f.signal, 2.0 * (y - f.target))
+    for index in (0, 3, 9, 14):  # conductances and corner frequencies of several materials
+        predicted, measured = f.central_difference(params, index, G)
+        assert abs(predicted - measured) <= 1e-4 * abs(measured), (index, predicted, measured)
+    # the chain rule: dL/dparameter = G . (the coefficients' tangent), the tangent in float64
+    grad = f.chain(params, lay, G)
+    v = params.vector()
+    branch = np.asarray(lay["state_branch"], np.int64)
+    B = f.sens["boundary_rows"]
+    for index in range(len(v)):
+        h = 1e-6 * v[index]
+        up, down = v.copy(), v.copy()
+        up[index] += h
+        down[index] -= h
+        cu = f.coefficients(fit.Relaxation.from_vector(params.beta, up))
+        cd = f.coefficients(fit.Relaxation.from_vector(params.beta, down))
+        tangent = 0.0
+        for name, key in _FAMILIES:
+            t = (cu[name] - cd[name]) / (2 * h)
+            tangent += float(np.sum(G[key][:B] * t) if name.startswith("coef") else np.sum(G[key] * t[branch]))
+        assert abs(grad[index] - tangent) <= 1e-5 * np.max(np.abs(grad)), (index, grad[index], tangent)

@@ -156,7 +156,7 @@ def test_gpu_full_size_run_in_pieces_equals_one_run(full_room):
 
 
 def test_gpu_full_size_fp32_stays_within_1e4_of_fp64(full_room):
-    # The north star's accuracy bar on the full grid: FP32 against FP64 stepping of the same
+    # The accuracy bar on the full grid: FP32 against FP64 stepping of the same
     # layout, relative L2 of every receiver's response within 1e-4.
     w = full_room
     p32 = B200WaveSolver(w.built.layout).run(w.signal)
