@@ -35,7 +35,7 @@ def nvcc() -> str:
 
 def build(verbose: bool = False, force: bool = False) -> Path:
     """Compiles the library unless it is newer than its sources; returns its path."""
-    deps = SOURCES + sorted((ROOT / "include").glob("*.h")) + [Path(__file__)]
+    deps = SOURCES + sorted((HERE / "csrc").glob("*.cuh")) + sorted((ROOT / "include").glob("*.h")) + [Path(__file__)]
     if not force and OUTPUT.exists():
         built = OUTPUT.stat().st_mtime
         if all(p.stat().st_mtime <= built for p in deps):

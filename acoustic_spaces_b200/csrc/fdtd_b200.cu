@@ -4,8 +4,9 @@
 // fdtd_create validates a layout (WaveSolver::layout(), cpp/include/acoustic_spaces/
 // fdtd.hpp:727-782 of naelolaiz/acoustic-spaces) on the host, copies it to the device in a pitched
 // layout, and builds the TMA tensor maps of the bulk sweep. A time step (fdtd.hpp:838-886) is four
-// launches on the handle's stream: the interior air (TMA-pipelined, bulk_kernel), the special rows,
-// the matched layer and the probe records; the levels swap between steps by the launches' pointers.
+// launches: the interior air (TMA-pipelined, bulk_kernel) on the handle's stream, beside it the
+// matched layer on a stream of its own and the special rows and probe records on a side stream; the
+// levels swap between steps by the launches' pointers.
 
 #include <cuda.h>
 #include <cuda_runtime.h>
@@ -48,6 +49,16 @@ using EncodeTiled = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t,
                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
+// The adjoint's device state (fdtd_adjoint.cuh): its tables, the two adjoint levels of the field
+// and of the branch velocities, each row's L~, and the tensor maps of the sweep over the levels.
+struct AdjointState {
+    AdjointTables t{};
+    void *lam[2] = {nullptr, nullptr};
+    void *om[2] = {nullptr, nullptr};
+    void *tilde = nullptr;
+    CUtensorMap lam_b[2], lam_a[2];
+};
+
 }  // namespace
 
 struct fdtd_solver {
@@ -55,9 +66,12 @@ struct fdtd_solver {
     int sms = 148;  // multiprocessors of the device
     int precision = FDTD_FP32;
     bool wide = false, scaled = false;
-    cudaStream_t stream = nullptr;  // the handle's stream: the sweep of interior and matched-layer cells
-    cudaStream_t side = nullptr;    // special rows and probes, beside them within each step
-    cudaEvent_t joined[2] = {nullptr, nullptr};  // each stream's end of a step
+    cudaStream_t stream = nullptr;  // the handle's stream: the interior sweep
+    cudaStream_t side = nullptr;    // special rows and probes, beside the sweep within each step
+    cudaStream_t layer_stream = nullptr;  // the matched layer, beside the sweep within each step
+    int layer_priority = 0;               // the device's highest stream priority
+    // A step's start on the handle's stream, and the side and layer streams' ends of a step.
+    cudaEvent_t joined[3] = {nullptr, nullptr, nullptr};
     std::string error;
     Tables tables{};
     BulkArgs bulk{};
@@ -73,10 +87,9 @@ struct fdtd_solver {
     // for the branch velocities w.
     void *u[2] = {nullptr, nullptr};
     void *w[2] = {nullptr, nullptr};
-    // The matched layer's pressure parts p_x, p_y, p_z: three pitched arrays, the layer's cells used.
-    void *layer_parts = nullptr;
+    void *layer_parts = nullptr;            // 3 arrays of the layer's cells: p_x, p_y, p_z
     std::vector<uint32_t> layer_cells;      // pitched, in the layout's order (for fdtd_read_state)
-    const uint8_t *types_device = nullptr;  // the pitched cell types (a layer cell's with its below bits)
+    const uint8_t *types_device = nullptr;  // the pitched cell types
     // Per axis, the velocity on each cell's + face (pitched, only the layer's faces used), in two
     // buffers: faces[1] holds the latest values between runs, as u[1] does.
     void *faces[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
@@ -95,14 +108,9 @@ struct fdtd_solver {
     bool timing = false;
     std::vector<cudaEvent_t> timing_events;  // 8 per step: (start, end) of bulk, layer, special, probe
     uint64_t timed_steps = 0;
-    // The adjoint (fdtd_gradient), set up on first use: its tables, the two adjoint levels of the
-    // field and of the branch velocities, each row's L~, and the tensor maps of the adjoint levels.
+    // The adjoint (fdtd_gradient), set up on first use and kept.
     bool adjoint_ready = false;
-    AdjointTables adjoint{};
-    void *lam[2] = {nullptr, nullptr};
-    void *om[2] = {nullptr, nullptr};
-    void *tilde = nullptr;
-    CUtensorMap lam_b[2], lam_a[2];
+    AdjointState adjoint;
     // Staging for fdtd_run's host buffers, grown on demand.
     float *stage_signal = nullptr;
     double *stage_out = nullptr;
@@ -236,10 +244,6 @@ int validate(const fdtd_layout *L, std::string &why) {
         for (uint64_t c = 0; c < L->layer_count; ++c) {
             if (seen[L->layer_cells[c]]++) return refuse("a matched-layer cell is listed twice");
         }
-        // The matched layer is swept by type: every cell of type layer is one of its cells.
-        uint64_t typed = 0;
-        for (uint64_t i = 0; i < n; ++i) typed += L->types[i] == kLayer;
-        if (typed != L->layer_count) return refuse("a cell of type layer is not in the matched layer");
     }
     if (!L->probe_start || L->probe_start[0] != 0) return refuse("probe_start does not start at 0");
     const uint64_t pc = L->probe_start[L->probe_count];
@@ -296,15 +300,20 @@ Fields<T> fields_for(const fdtd_solver *s, bool flip) {
     f.a = static_cast<T *>(s->u[prev]);
     f.wb = static_cast<const T *>(s->w[cur]);
     f.wa = static_cast<T *>(s->w[prev]);
+    f.layer_parts = static_cast<T *>(s->layer_parts);
+    for (int axis = 0; axis < 3; ++axis) {
+        f.face_old[axis] = static_cast<const T *>(s->faces[cur][axis]);
+        f.face_new[axis] = static_cast<T *>(s->faces[prev][axis]);
+    }
     return f;
 }
 
-template <typename T, bool WIDE, bool SCALED, bool LAYER>
+template <typename T, bool WIDE, bool SCALED>
 int set_up_kernels(fdtd_solver *s) {
-    CUDA_TRY(s, cudaFuncSetAttribute(bulk_kernel<T, WIDE, SCALED, LAYER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    CUDA_TRY(s, cudaFuncSetAttribute(bulk_kernel<T, WIDE, SCALED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)Stage<T, SCALED>::smem));
     int per_sm = 0;
-    CUDA_TRY(s, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bulk_kernel<T, WIDE, SCALED, LAYER>, kBlock,
+    CUDA_TRY(s, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bulk_kernel<T, WIDE, SCALED>, kBlock,
                                                               Stage<T, SCALED>::smem));
     s->bulk_per_sm = per_sm;
     // One tile per block: measured faster than a persistent grid of the resident blocks.
@@ -312,29 +321,35 @@ int set_up_kernels(fdtd_solver *s) {
     return FDTD_OK;
 }
 
-template <typename T, bool WIDE, bool SCALED, bool LAYER>
+template <typename T, bool WIDE, bool SCALED>
 int launch_steps(fdtd_solver *s, const float *d_signal, uint64_t steps, double *d_out, uint64_t stride) {
     const Tables &g = s->tables;
     const uint32_t special_blocks = (uint32_t)((s->specials + kBlock - 1) / kBlock);
     const uint32_t probe_blocks = (uint32_t)((s->probes + kProbeWarps - 1) / kProbeWarps);
     const uint32_t smem = Stage<T, SCALED>::smem;
-    // Each step: the sweep of the interior and matched-layer cells on the handle's stream, the
-    // special rows and the probes on the side stream beside them; each stream waits for the
-    // other's end of the step before. While timing, all run one after another on the handle's
-    // stream, so that each kernel's events bracket that kernel alone (the layer's pair brackets
-    // nothing: its cells are swept with the interior).
-    cudaStream_t side = s->timing ? s->stream : s->side;
-    CUDA_TRY(s, cudaEventRecord(s->joined[0], s->stream));
-    CUDA_TRY(s, cudaStreamWaitEvent(s->side, s->joined[0], 0));
+    const uint32_t layer_blocks = (uint32_t)((s->layers + kBlock - 1) / kBlock);
+    // Each step: the interior sweep on the handle's stream; beside it the matched layer on the
+    // layer stream, of the highest priority (its blocks take the thread slots that the sweep's
+    // shared memory leaves free on every multiprocessor), and the special rows and probes on the
+    // side stream. The three write disjoint memory; each step starts when all three have ended the
+    // step before. While timing, all run one after another on the handle's stream, so that each
+    // kernel's events bracket that kernel alone.
+    const bool fork = !s->timing;
+    cudaStream_t side = fork ? s->side : s->stream, layer = fork ? s->layer_stream : s->stream;
     for (uint64_t k = 0; k < steps; ++k) {
         const bool flip = (k & 1) != 0;
         Fields<T> f = fields_for<T>(s, flip);
         f.signal = d_signal + k;
         f.out = d_out + k;
         f.out_stride = stride;
-        if (k > 0) {
-            CUDA_TRY(s, cudaStreamWaitEvent(s->stream, s->joined[1], 0));
-            CUDA_TRY(s, cudaStreamWaitEvent(s->side, s->joined[0], 0));
+        if (fork) {
+            if (k > 0) {
+                CUDA_TRY(s, cudaStreamWaitEvent(s->stream, s->joined[1], 0));
+                CUDA_TRY(s, cudaStreamWaitEvent(s->stream, s->joined[2], 0));
+            }
+            CUDA_TRY(s, cudaEventRecord(s->joined[0], s->stream));
+            CUDA_TRY(s, cudaStreamWaitEvent(side, s->joined[0], 0));
+            CUDA_TRY(s, cudaStreamWaitEvent(layer, s->joined[0], 0));
         }
         cudaEvent_t *ev = nullptr;
         if (s->timing) {
@@ -353,16 +368,25 @@ int launch_steps(fdtd_solver *s, const float *d_signal, uint64_t steps, double *
             BulkArgs args = s->bulk;
             args.a = f.a;
             const int cur = flip ? 0 : 1, prev = flip ? 1 : 0;
-            for (int axis = 0; axis < 3; ++axis) {
-                args.face_old[axis] = s->faces[cur][axis];
-                args.face_new[axis] = s->faces[prev][axis];
-            }
-            bulk_kernel<T, WIDE, SCALED, LAYER><<<s->bulk_blocks, kBlock, smem, s->stream>>>(
+            bulk_kernel<T, WIDE, SCALED><<<s->bulk_blocks, kBlock, smem, s->stream>>>(
                 s->map_b[cur], s->map_a[prev], s->map_t, s->map_s, args);
         }
         if (ev) CUDA_TRY(s, cudaEventRecord(ev[1], s->stream));
-        if (ev) CUDA_TRY(s, cudaEventRecord(ev[2], s->stream));
-        if (ev) CUDA_TRY(s, cudaEventRecord(ev[3], s->stream));
+        if (ev) CUDA_TRY(s, cudaEventRecord(ev[2], layer));
+        if (layer_blocks) {
+            // With the priority as a launch attribute too, so that a captured graph keeps it.
+            cudaLaunchConfig_t config{};
+            config.gridDim = dim3(layer_blocks);
+            config.blockDim = dim3(kBlock);
+            config.stream = layer;
+            cudaLaunchAttribute priority{};
+            priority.id = cudaLaunchAttributePriority;
+            priority.val.priority = s->layer_priority;
+            config.attrs = &priority;
+            config.numAttrs = 1;
+            CUDA_TRY(s, cudaLaunchKernelEx(&config, layer_kernel<T, SCALED>, g, f));
+        }
+        if (ev) CUDA_TRY(s, cudaEventRecord(ev[3], layer));
         if (ev) CUDA_TRY(s, cudaEventRecord(ev[4], side));
         if (special_blocks) {
             if (s->link_slots <= 6)
@@ -374,42 +398,44 @@ int launch_steps(fdtd_solver *s, const float *d_signal, uint64_t steps, double *
         if (ev) CUDA_TRY(s, cudaEventRecord(ev[6], side));
         if (probe_blocks) probe_kernel<T><<<probe_blocks, kBlock, 0, side>>>(g, f);
         if (ev) CUDA_TRY(s, cudaEventRecord(ev[7], side));
-        CUDA_TRY(s, cudaEventRecord(s->joined[0], s->stream));
-        CUDA_TRY(s, cudaEventRecord(s->joined[1], s->side));
+        if (fork) {
+            CUDA_TRY(s, cudaEventRecord(s->joined[1], side));
+            CUDA_TRY(s, cudaEventRecord(s->joined[2], layer));
+        }
     }
-    // The handle's stream ends after both.
-    CUDA_TRY(s, cudaStreamWaitEvent(s->stream, s->joined[1], 0));
+    // The handle's stream ends after all three.
+    if (fork && steps) {
+        CUDA_TRY(s, cudaStreamWaitEvent(s->stream, s->joined[1], 0));
+        CUDA_TRY(s, cudaStreamWaitEvent(s->stream, s->joined[2], 0));
+    }
     CUDA_TRY(s, cudaGetLastError());
     return FDTD_OK;
 }
 
-template <typename T, bool W, bool S, bool LY>
+template <typename T, bool W, bool S>
 int dispatch_run(fdtd_solver *s, const float *d_signal, uint64_t steps, double *d_out, uint64_t stride) {
-    return launch_steps<T, W, S, LY>(s, d_signal, steps, d_out, stride);
+    return launch_steps<T, W, S>(s, d_signal, steps, d_out, stride);
 }
 
-// The instantiation for the grid: precision, stencil, speed field, matched layer (which takes the
-// 7-point stencil only).
-#define FDTD_BY_KIND(CALL)                                                              \
-    do {                                                                                \
-        if (s->precision == FDTD_FP64) {                                                \
-            if (s->layers) return s->scaled ? CALL(double, false, true, true) : CALL(double, false, false, true); \
-            if (!s->wide) return s->scaled ? CALL(double, false, true, false) : CALL(double, false, false, false); \
-            return s->scaled ? CALL(double, true, true, false) : CALL(double, true, false, false); \
-        }                                                                               \
-        if (s->layers) return s->scaled ? CALL(float, false, true, true) : CALL(float, false, false, true); \
-        if (!s->wide) return s->scaled ? CALL(float, false, true, false) : CALL(float, false, false, false); \
-        return s->scaled ? CALL(float, true, true, false) : CALL(float, true, false, false); \
+// The instantiation for the grid: precision, stencil, speed field.
+#define FDTD_BY_KIND(CALL)                                                                          \
+    do {                                                                                            \
+        if (s->precision == FDTD_FP64) {                                                            \
+            if (!s->wide) return s->scaled ? CALL(double, false, true) : CALL(double, false, false); \
+            return s->scaled ? CALL(double, true, true) : CALL(double, true, false);                \
+        }                                                                                           \
+        if (!s->wide) return s->scaled ? CALL(float, false, true) : CALL(float, false, false);      \
+        return s->scaled ? CALL(float, true, true) : CALL(float, true, false);                      \
     } while (0)
 
 int dispatch(fdtd_solver *s, const float *d_signal, uint64_t steps, double *d_out, uint64_t stride) {
-#define RUN_CALL(T, W, S, LY) dispatch_run<T, W, S, LY>(s, d_signal, steps, d_out, stride)
+#define RUN_CALL(T, W, S) dispatch_run<T, W, S>(s, d_signal, steps, d_out, stride)
     FDTD_BY_KIND(RUN_CALL);
 #undef RUN_CALL
 }
 
 int set_up(fdtd_solver *s) {
-#define SET_CALL(T, W, S, LY) set_up_kernels<T, W, S, LY>(s)
+#define SET_CALL(T, W, S) set_up_kernels<T, W, S>(s)
     FDTD_BY_KIND(SET_CALL);
 #undef SET_CALL
 }
@@ -454,7 +480,8 @@ int capture(fdtd_solver *s, cudaGraphExec_t *out) {
         return rc;
     }
     if (e != cudaSuccess) return cuda_fail(s, e, "cudaStreamEndCapture");
-    const cudaError_t i = cudaGraphInstantiate(out, graph, 0);
+    // The nodes' own priorities (the matched layer's), not the launching stream's.
+    const cudaError_t i = cudaGraphInstantiateWithFlags(out, graph, cudaGraphInstantiateFlagUseNodePriority);
     cudaGraphDestroy(graph);
     if (i != cudaSuccess) return cuda_fail(s, i, "cudaGraphInstantiate");
     return FDTD_OK;
@@ -475,16 +502,14 @@ int build(fdtd_solver *s, const fdtd_layout *L) {
     g.ny = (uint32_t)ny;
     g.nz = (uint32_t)nz;
     g.sz = (uint32_t)(s->pitch * ny);
+    g.plane = (uint32_t)(s->pitch * ny);
     for (int k = 0; k < 18; ++k)
         g.offset[k] = (int32_t)(kSteps[k][0] + kSteps[k][1] * (int64_t)s->pitch + kSteps[k][2] * (int64_t)(s->pitch * ny));
 
-    // Cell types and scales, pitched; the swept cells' (interior and matched layer) bounding box
-    // and the air count. A layer cell's type byte also carries which of its lower neighbours are
-    // in the layer; with a speed field its scale is the layer's scale of the cell.
+    // Cell types and scales, pitched; the interior cells' bounding box and the air count.
     std::vector<uint8_t> types(s->n_device, (uint8_t)kSolid);
     std::vector<float> scale(s->scaled ? s->n_device : 0, 0.0f);
     uint64_t x0 = nx, y0 = ny, z0 = nz, x1 = 0, y1 = 0, z1 = 0, interior = 0, air = 0;
-    const uint64_t strides[3] = {1, nx, nx * ny};
     for (uint64_t z = 0; z < nz; ++z)
         for (uint64_t y = 0; y < ny; ++y) {
             const uint64_t row = nx * (y + ny * z), drow = s->pitch * (y + ny * z);
@@ -493,21 +518,13 @@ int build(fdtd_solver *s, const fdtd_layout *L) {
             for (uint64_t x = 0; x < nx; ++x) {
                 const uint8_t t = L->types[row + x];
                 if (t != kSolid) ++air;
-                if (t == kLayer) {
-                    for (int axis = 0; axis < 3; ++axis)
-                        if (L->types[row + x - strides[axis]] == kLayer)
-                            types[drow + x] |= (uint8_t)(1u << (kBelowShift + axis));
-                } else if (t != kInterior) {
-                    continue;
-                }
-                interior += t == kInterior;
+                if (t != kInterior) continue;
+                ++interior;
                 x0 = std::min(x0, x), x1 = std::max(x1, x + 1);
                 y0 = std::min(y0, y), y1 = std::max(y1, y + 1);
                 z0 = std::min(z0, z), z1 = std::max(z1, z + 1);
             }
         }
-    if (s->scaled)
-        for (uint64_t c = 0; c < L->layer_count; ++c) scale[pitched(s, (uint64_t)L->layer_cells[c])] = L->layer_scale[c];
     s->interior = interior, s->air = air;
 
     int rc;
@@ -522,7 +539,7 @@ int build(fdtd_solver *s, const fdtd_layout *L) {
         if ((rc = zeros(s, e * s->n_device, &s->u[k]))) return rc;
         if ((rc = zeros(s, e * L->state_count, &s->w[k]))) return rc;
     }
-    if (L->layer_count && (rc = zeros(s, e * 3 * s->n_device, &s->layer_parts))) return rc;
+    if ((rc = zeros(s, e * 3 * L->layer_count, &s->layer_parts))) return rc;
     if (L->layer_count)
         for (int k = 0; k < 2; ++k)
             for (int axis = 0; axis < 3; ++axis)
@@ -546,12 +563,12 @@ int build(fdtd_solver *s, const fdtd_layout *L) {
     bk.centre = L->centre;
     bk.total = L->total;
     bk.error = s->d_error;
-    if (interior || L->layer_count) {
+    if (interior) {
         bk.xa = (uint32_t)(x0 / 16 * 16);
         bk.y0 = (uint32_t)y0, bk.z0 = (uint32_t)z0;
         bk.x1 = (uint32_t)x1, bk.y1 = (uint32_t)y1, bk.z1 = (uint32_t)z1;
         // The tile list: the columns of kTX x kTY cells over the box, and in each the runs of
-        // planes that hold interior or layer cells, cut into chunks of at most `chunk` planes, so that
+        // planes that hold interior cells, cut into chunks of at most `chunk` planes, so that
         // there are blocks enough for every multiprocessor several times over. Grids of many
         // rooms (stacked along z) skip the planes between the rooms.
         const uint64_t tiles_x = (x1 - bk.xa + kTX - 1) / kTX, tiles_y = (y1 - y0 + kTY - 1) / kTY;
@@ -562,7 +579,7 @@ int build(fdtd_solver *s, const fdtd_layout *L) {
             for (uint64_t y = y0; y < y1; ++y) {
                 const uint8_t *row = &L->types[nx * (y + ny * z)];
                 for (uint64_t x = x0; x < x1; ++x) {
-                    if (row[x] != kInterior && row[x] != kLayer) continue;
+                    if (row[x] != kInterior) continue;
                     uint8_t &o = occupied[((y - y0) / kTY * tiles_x + (x - bk.xa) / kTX) * nz + z];
                     planes += o == 0;
                     o = 1;
@@ -670,13 +687,25 @@ int build(fdtd_solver *s, const fdtd_layout *L) {
         g.state_gain = fp;
     }
 
-    // Matched layer: swept with the interior (its pressure parts and faces pitched); per axis and
-    // grid coordinate {keep, push, keep_face, push_face} (layer_coefficients, fdtd.hpp:2219-2238).
+    // Matched layer.
     const uint64_t Lc = L->layer_count;
     s->layers = Lc;
+    g.layers = (uint32_t)Lc;
     if (Lc) {
-        s->layer_cells.resize(Lc);
-        for (uint64_t c = 0; c < Lc; ++c) s->layer_cells[c] = pitched(s, (uint64_t)L->layer_cells[c]);
+        std::vector<uint32_t> cells(Lc);
+        for (uint64_t c = 0; c < Lc; ++c) cells[c] = pitched(s, (uint64_t)L->layer_cells[c]);
+        // Which of each layer cell's lower neighbours are in the layer too (their face is theirs).
+        std::vector<uint8_t> below(Lc, 0);
+        const uint64_t strides[3] = {1, nx, nx * ny};
+        for (uint64_t c = 0; c < Lc; ++c)
+            for (int axis = 0; axis < 3; ++axis)
+                if (L->types[(uint64_t)L->layer_cells[c] - strides[axis]] == kLayer) below[c] |= (uint8_t)(1u << axis);
+        s->layer_cells = cells;
+        const uint32_t *p;
+        if ((rc = upload(s, cells.data(), Lc, &p))) return rc;
+        g.layer_cells = p;
+        if ((rc = upload(s, below.data(), Lc, &u8))) return rc;
+        g.layer_below = u8;
         const uint64_t len[3] = {nx + 1, ny + 1, nz + 1};
         for (int axis = 0; axis < 3; ++axis) {
             std::vector<float4> packed(len[axis]);
@@ -685,8 +714,11 @@ int build(fdtd_solver *s, const fdtd_layout *L) {
                                         L->push[2 * axis + 1][x]);
             const float4 *p4;
             if ((rc = upload(s, packed.data(), len[axis], &p4))) return rc;
-            s->bulk.layer_coef[axis] = p4;
-            s->bulk.parts[axis] = static_cast<char *>(s->layer_parts) + e * s->n_device * axis;
+            g.layer_coef[axis] = p4;
+        }
+        if (s->scaled) {
+            if ((rc = upload(s, L->layer_scale, Lc, &fp))) return rc;
+            g.layer_scale = fp;
         }
     }
 
@@ -715,18 +747,18 @@ void release(fdtd_solver *s) {
     int current = 0;
     cudaGetDevice(&current);
     cudaSetDevice(s->device);
-    if (s->stream) cudaStreamSynchronize(s->stream);
+    for (cudaStream_t stream : {s->stream, s->side, s->layer_stream})
+        if (stream) cudaStreamSynchronize(stream);
     for (cudaGraphExec_t g : s->graph)
         if (g) cudaGraphExecDestroy(g);
     for (cudaEvent_t e : s->timing_events) cudaEventDestroy(e);
     for (void *p : s->allocations) cudaFree(p);
     if (s->stage_signal) cudaFreeHost(s->stage_signal);
     if (s->stage_out) cudaFreeHost(s->stage_out);
-    if (s->side) cudaStreamSynchronize(s->side);
     for (cudaEvent_t e : s->joined)
         if (e) cudaEventDestroy(e);
-    if (s->side) cudaStreamDestroy(s->side);
-    if (s->stream) cudaStreamDestroy(s->stream);
+    for (cudaStream_t stream : {s->layer_stream, s->side, s->stream})
+        if (stream) cudaStreamDestroy(stream);
     cudaSetDevice(current);
 }
 
@@ -741,15 +773,21 @@ int download(fdtd_solver *s, const V *device, size_t count, std::vector<V> &host
     return FDTD_OK;
 }
 
-// The transposed links and the correction list, from the handle's own device tables.
-int set_up_adjoint(fdtd_solver *s) {
-    if (s->adjoint_ready) return FDTD_OK;
+// The adjoint's tables on the host: the readers of each special row's cell (the transposed links)
+// and the interior cells next to special rows with their corrections.
+struct AdjointLists {
+    std::vector<uint32_t> reader_start, reader_index, cells, starts, rows;
+    std::vector<uint8_t> reader_kind;
+    std::vector<double> reader_coef, coefs;
+};
+
+// The lists from the handle's own device tables.
+int adjoint_lists(fdtd_solver *s, AdjointLists &out) {
     if (s->wide || s->scaled || s->layers)
         return fail(s, FDTD_EINVAL,
                     "the adjoint takes the 7-point stencil without a matched layer or a speed of sound per cell");
     const Tables &g = s->tables;
-    const uint64_t K = s->specials, S = s->states;
-    const size_t e = s->precision == FDTD_FP64 ? 8 : 4;
+    const uint64_t K = s->specials;
     std::vector<uint32_t> special;
     std::vector<uint8_t> count, direction, types;
     std::vector<float> weight, coef_a, coef_inv;
@@ -791,73 +829,112 @@ int set_up_adjoint(fdtd_solver *s) {
             }
         }
     }
-    std::vector<uint32_t> reader_start(K + 1, 0), reader_index;
-    std::vector<uint8_t> reader_kind;
-    std::vector<double> reader_coef;
+    out.reader_start.assign(K + 1, 0);
     for (uint64_t k = 0; k < K; ++k) {
         for (const auto &[idx, coef] : readers[k]) {
-            reader_index.push_back((uint32_t)(idx & ~kind_bit));
-            reader_kind.push_back((idx & kind_bit) ? 1 : 0);
-            reader_coef.push_back(coef);
+            out.reader_index.push_back((uint32_t)(idx & ~kind_bit));
+            out.reader_kind.push_back((idx & kind_bit) ? 1 : 0);
+            out.reader_coef.push_back(coef);
         }
-        reader_start[k + 1] = (uint32_t)reader_index.size();
+        out.reader_start[k + 1] = (uint32_t)out.reader_index.size();
     }
-    std::vector<uint32_t> cells, starts{0}, rows;
-    std::vector<double> coefs;
+    out.starts.assign(1, 0);
     for (auto &[cell, list] : corrected) {
-        cells.push_back(cell);
-        for (const auto &[r, c] : list) rows.push_back(r), coefs.push_back(c);
-        starts.push_back((uint32_t)rows.size());
+        out.cells.push_back(cell);
+        for (const auto &[r, c] : list) out.rows.push_back(r), out.coefs.push_back(c);
+        out.starts.push_back((uint32_t)out.rows.size());
     }
-    AdjointTables &t = s->adjoint;
+    return FDTD_OK;
+}
+
+// A host array copied into device memory from `pool` (pool.take(bytes, &p, zero) gives the
+// memory), in order on the handle's stream (the host array is staged before the call returns).
+template <class Pool, typename V>
+int place(fdtd_solver *s, Pool &pool, const std::vector<V> &host, const V **out) {
+    *out = nullptr;
+    if (host.empty()) return FDTD_OK;
+    void *p;
+    int rc;
+    if ((rc = pool.take(host.size() * sizeof(V), &p, false))) return rc;
+    CUDA_TRY(s, cudaMemcpyAsync(p, host.data(), host.size() * sizeof(V), cudaMemcpyHostToDevice, s->stream));
+    *out = static_cast<const V *>(p);
+    return FDTD_OK;
+}
+
+// The adjoint's device state from its lists, in memory from `pool`.
+template <class Pool>
+int place_adjoint(fdtd_solver *s, const AdjointLists &l, Pool &pool, AdjointState &a) {
+    const Tables &g = s->tables;
+    const uint64_t K = s->specials, S = s->states;
+    const size_t e = s->precision == FDTD_FP64 ? 8 : 4;
+    AdjointTables &t = a.t;
     t.specials = (uint32_t)K, t.states = (uint32_t)S;
     t.special = g.special, t.state_start = g.state_start;
     t.state_weight = g.state_weight, t.state_now = g.state_now, t.state_before = g.state_before, t.state_gain = g.state_gain;
     t.coef_b = g.coef_b, t.coef_inv = g.coef_inv;
     t.axial = s->bulk.axial;
     t.probes = g.probes, t.probe_start = g.probe_start, t.probe_cells = g.probe_cells, t.probe_weights = g.probe_weights;
-    t.corrected = (uint32_t)cells.size();
-    const uint32_t *p32;
-    const uint8_t *p8;
-    const double *pd;
-    if ((rc = upload(s, reader_start.data(), reader_start.size(), &p32))) return rc;
-    t.reader_start = p32;
-    if ((rc = upload(s, reader_index.data(), reader_index.size(), &p32))) return rc;
-    t.reader_index = p32;
-    if ((rc = upload(s, reader_kind.data(), reader_kind.size(), &p8))) return rc;
-    t.reader_kind = p8;
-    if ((rc = upload(s, reader_coef.data(), reader_coef.size(), &pd))) return rc;
-    t.reader_coef = pd;
-    if ((rc = upload(s, cells.data(), cells.size(), &p32))) return rc;
-    t.corrected_cell = p32;
-    if ((rc = upload(s, starts.data(), starts.size(), &p32))) return rc;
-    t.corrected_start = p32;
-    if ((rc = upload(s, rows.data(), rows.size(), &p32))) return rc;
-    t.corrected_row = p32;
-    if ((rc = upload(s, coefs.data(), coefs.size(), &pd))) return rc;
-    t.corrected_coef = pd;
+    t.corrected = (uint32_t)l.cells.size();
+    int rc;
+    if ((rc = place(s, pool, l.reader_start, &t.reader_start))) return rc;
+    if ((rc = place(s, pool, l.reader_index, &t.reader_index))) return rc;
+    if ((rc = place(s, pool, l.reader_kind, &t.reader_kind))) return rc;
+    if ((rc = place(s, pool, l.reader_coef, &t.reader_coef))) return rc;
+    if ((rc = place(s, pool, l.cells, &t.corrected_cell))) return rc;
+    if ((rc = place(s, pool, l.starts, &t.corrected_start))) return rc;
+    if ((rc = place(s, pool, l.rows, &t.corrected_row))) return rc;
+    if ((rc = place(s, pool, l.coefs, &t.corrected_coef))) return rc;
     for (int k = 0; k < 2; ++k) {
-        if ((rc = zeros(s, e * s->n_device, &s->lam[k]))) return rc;
-        if ((rc = zeros(s, e * S, &s->om[k]))) return rc;
+        if ((rc = pool.take(e * s->n_device, &a.lam[k], true))) return rc;
+        if ((rc = pool.take(e * S, &a.om[k], true))) return rc;
     }
-    if ((rc = zeros(s, e * K, &s->tilde))) return rc;
+    if ((rc = pool.take(e * K, &a.tilde, true))) return rc;
     if (s->bulk_blocks) {
         const CUtensorMapDataType ft = s->precision == FDTD_FP64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
         for (int k = 0; k < 2; ++k) {
-            if ((rc = tensor_map(s, &s->lam_b[k], s->lam[k], ft, (uint32_t)e, kBX, kBY))) return rc;
-            if ((rc = tensor_map(s, &s->lam_a[k], s->lam[k], ft, (uint32_t)e, kTX, kTY))) return rc;
+            if ((rc = tensor_map(s, &a.lam_b[k], a.lam[k], ft, (uint32_t)e, kBX, kBY))) return rc;
+            if ((rc = tensor_map(s, &a.lam_a[k], a.lam[k], ft, (uint32_t)e, kTX, kTY))) return rc;
         }
     }
+    return FDTD_OK;
+}
+
+// Device memory the handle owns until fdtd_destroy.
+struct Owned {
+    fdtd_solver *s;
+    int take(size_t bytes, void **out, bool zero) {
+        if (zero) return zeros(s, bytes, out);
+        *out = nullptr;
+        void *p = nullptr;
+        CUDA_TRY(s, cudaMalloc(&p, bytes ? bytes : 16));
+        s->allocations.push_back(p);
+        s->device_bytes += bytes;
+        *out = p;
+        return FDTD_OK;
+    }
+};
+
+// The handle's adjoint, set up on first use and kept; every copy and clear has ended on return.
+int set_up_adjoint(fdtd_solver *s) {
+    if (s->adjoint_ready) return FDTD_OK;
+    AdjointLists lists;
+    int rc;
+    if ((rc = adjoint_lists(s, lists))) return rc;
+    Owned owned{s};
+    if ((rc = place_adjoint(s, lists, owned, s->adjoint))) return rc;
+    CUDA_TRY(s, cudaDeviceSynchronize());  // the clears (default stream) and copies (handle's stream)
     s->adjoint_ready = true;
     return FDTD_OK;
 }
 
-// Device scratch of one fdtd_gradient call, freed at its end.
+// Device scratch of one fdtd_gradient call, freed at its end (the handle's stream has ended by
+// then). Each block is cleared on the handle's stream, in order with the gradient's own work.
 struct Scratch {
     fdtd_solver *s;
     std::vector<void *> blocks;
     explicit Scratch(fdtd_solver *solver) : s(solver) {}
     ~Scratch() {
+        cudaStreamSynchronize(s->stream);
         for (void *p : blocks) cudaFree(p);
     }
     int take(size_t bytes, void **out) {
@@ -865,30 +942,31 @@ struct Scratch {
         void *p = nullptr;
         CUDA_TRY(s, cudaMalloc(&p, bytes ? bytes : 16));
         blocks.push_back(p);
-        CUDA_TRY(s, cudaMemset(p, 0, bytes ? bytes : 16));
+        CUDA_TRY(s, cudaMemsetAsync(p, 0, bytes ? bytes : 16, s->stream));
         *out = p;
         return FDTD_OK;
     }
 };
 
-template <typename T>
-int gradient(fdtd_solver *s, const float *signal, uint64_t steps, const double *dloss, uint64_t segment,
-             double *grads[5]) {
+// The gradient (fdtd_gradient) with the adjoint state `adj` and scratch from `scratch`
+// (scratch.take(bytes, &p): device memory cleared to 0 in order on the handle's stream).
+template <typename T, class Pool>
+int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float *signal, uint64_t steps,
+             const double *dloss, uint64_t segment, double *grads[5]) {
     const uint64_t K = s->specials, S = s->states, P = s->probes;
     const size_t e = sizeof(T);
     if (segment == 0 || segment > steps) segment = steps;
     const uint64_t segments = (steps + segment - 1) / segment;
-    Scratch scratch(s);
     void *p;
     int rc;
     // On the device: the drive, dL/dy, one segment's trajectory, the gradient's sums, and the
     // state at the start of every segment after the first (the checkpoints).
     if ((rc = scratch.take(sizeof(float) * steps, &p))) return rc;
     float *d_signal = static_cast<float *>(p);
-    CUDA_TRY(s, cudaMemcpy(d_signal, signal, sizeof(float) * steps, cudaMemcpyHostToDevice));
+    CUDA_TRY(s, cudaMemcpyAsync(d_signal, signal, sizeof(float) * steps, cudaMemcpyHostToDevice, s->stream));
     if ((rc = scratch.take(sizeof(double) * std::max<uint64_t>(1, P) * steps, &p))) return rc;
     double *d_dloss = static_cast<double *>(p);
-    if (P) CUDA_TRY(s, cudaMemcpy(d_dloss, dloss, sizeof(double) * P * steps, cudaMemcpyHostToDevice));
+    if (P) CUDA_TRY(s, cudaMemcpyAsync(d_dloss, dloss, sizeof(double) * P * steps, cudaMemcpyHostToDevice, s->stream));
     if ((rc = scratch.take(e * K * (segment + 2), &p))) return rc;
     T *traj_u = static_cast<T *>(p);
     if ((rc = scratch.take(e * S * (segment + 2), &p))) return rc;
@@ -934,16 +1012,16 @@ int gradient(fdtd_solver *s, const float *signal, uint64_t steps, const double *
     }
     // The adjoint levels beyond the end are at rest; the sums start at 0.
     for (int k = 0; k < 2; ++k) {
-        CUDA_TRY(s, cudaMemsetAsync(s->lam[k], 0, level_bytes, s->stream));
-        if (S) CUDA_TRY(s, cudaMemsetAsync(s->om[k], 0, state_bytes, s->stream));
+        CUDA_TRY(s, cudaMemsetAsync(adj.lam[k], 0, level_bytes, s->stream));
+        if (S) CUDA_TRY(s, cudaMemsetAsync(adj.om[k], 0, state_bytes, s->stream));
     }
-    const AdjointTables &t = s->adjoint;
+    const AdjointTables &t = adj.t;
     const uint32_t row_blocks = (uint32_t)((std::max<uint64_t>(std::max<uint64_t>(K, S), 1) + kBlock - 1) / kBlock);
     const uint32_t special_blocks = (uint32_t)((K + kBlock - 1) / kBlock);
     const uint32_t corrected_blocks = (uint32_t)((t.corrected + kBlock - 1) / kBlock);
     const uint32_t probe_blocks = (uint32_t)((P + kBlock - 1) / kBlock);
     const uint32_t smem = Stage<T, false>::smem;
-    T *tilde = static_cast<T *>(s->tilde);
+    T *tilde = static_cast<T *>(adj.tilde);
     int x = 0;  // lam[x], om[x]: level n+1; lam[1-x], om[1-x]: level n+2, then level n
     for (uint64_t k = segments; k-- > 0;) {
         const uint64_t s0 = k * segment, s1 = std::min(steps, s0 + segment);
@@ -967,13 +1045,13 @@ int gradient(fdtd_solver *s, const float *signal, uint64_t steps, const double *
                                                                traj_u + (s1 - s0 + 1) * K, traj_w + (s1 - s0 + 1) * S);
         // The reverse steps of the segment.
         for (uint64_t n = s1; n-- > s0;) {
-            T *lam_next = static_cast<T *>(s->lam[x]), *lam_out = static_cast<T *>(s->lam[1 - x]);
-            T *om_next = static_cast<T *>(s->om[x]), *om_out = static_cast<T *>(s->om[1 - x]);
+            T *lam_next = static_cast<T *>(adj.lam[x]), *lam_out = static_cast<T *>(adj.lam[1 - x]);
+            T *om_next = static_cast<T *>(adj.om[x]), *om_out = static_cast<T *>(adj.om[1 - x]);
             if (special_blocks) tilde_kernel<T><<<special_blocks, kBlock, 0, s->stream>>>(t, lam_next, om_next, tilde);
             if (s->bulk_blocks) {
                 BulkArgs args = s->bulk;
                 args.a = lam_out;
-                bulk_kernel<T, false, false, false><<<s->bulk_blocks, kBlock, smem, s->stream>>>(s->lam_b[x], s->lam_a[1 - x],
+                bulk_kernel<T, false, false><<<s->bulk_blocks, kBlock, smem, s->stream>>>(adj.lam_b[x], adj.lam_a[1 - x],
                                                                                         s->map_t, s->map_s, args);
             }
             if (corrected_blocks) correct_kernel<T><<<corrected_blocks, kBlock, 0, s->stream>>>(t, lam_next, tilde, lam_out);
@@ -1069,8 +1147,14 @@ int fdtd_create(const fdtd_layout *layout, int precision, int device, fdtd_solve
     s->precision = precision;
     cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->joined[0], cudaEventDisableTiming);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->joined[1], cudaEventDisableTiming);
+    // The matched layer's stream at the highest priority: its blocks are placed as soon as a
+    // multiprocessor has room, beside the sweep's, rather than after the sweep's last wave.
+    int lowest = 0, highest = 0;
+    if (e == cudaSuccess) e = cudaDeviceGetStreamPriorityRange(&lowest, &highest);
+    if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&s->layer_stream, cudaStreamNonBlocking, highest);
+    s->layer_priority = highest;
+    for (cudaEvent_t &event : s->joined)
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&event, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         const int rc = cuda_fail(nullptr, e, "cudaStreamCreate");
         release(s);
@@ -1199,8 +1283,10 @@ int fdtd_gradient(fdtd_solver *s, const float *signal, uint64_t steps, const dou
     int rc = set_up_adjoint(s);
     if (rc != FDTD_OK) return rc;
     double *grads[5] = {grad_coef_b, grad_coef_inv, grad_now, grad_before, grad_gain};
-    return s->precision == FDTD_FP64 ? gradient<double>(s, signal, steps, dloss_dy, segment, grads)
-                                     : gradient<float>(s, signal, steps, dloss_dy, segment, grads);
+    Scratch scratch(s);
+    return s->precision == FDTD_FP64
+               ? gradient<double>(s, s->adjoint, scratch, signal, steps, dloss_dy, segment, grads)
+               : gradient<float>(s, s->adjoint, scratch, signal, steps, dloss_dy, segment, grads);
 }
 
 int fdtd_reset(fdtd_solver *s) {
@@ -1212,7 +1298,7 @@ int fdtd_reset(fdtd_solver *s) {
         if (s->states) CUDA_TRY(s, cudaMemsetAsync(s->w[k], 0, e * s->states, s->stream));
     }
     if (s->layers) {
-        CUDA_TRY(s, cudaMemsetAsync(s->layer_parts, 0, e * 3 * s->n_device, s->stream));
+        CUDA_TRY(s, cudaMemsetAsync(s->layer_parts, 0, e * 3 * s->layers, s->stream));
         for (int k = 0; k < 2; ++k)
             for (int axis = 0; axis < 3; ++axis)
                 CUDA_TRY(s, cudaMemsetAsync(s->faces[k][axis], 0, e * s->n_device, s->stream));
@@ -1268,14 +1354,12 @@ int fdtd_read_state(const fdtd_solver *cs, void *current, void *previous, void *
         // The reference's nine values per cell (fdtd.hpp:2245): the parts, then per axis the
         // velocity of the - face (the + face of the cell below) and of the + face.
         const std::vector<uint32_t> &cells = s->layer_cells;
-        std::vector<char> field(e * s->n_device);
+        std::vector<char> parts(e * 3 * s->layers);
+        CUDA_TRY(s, cudaMemcpy(parts.data(), s->layer_parts, parts.size(), cudaMemcpyDeviceToHost));
         char *dst = static_cast<char *>(layer_state);
-        for (int k = 0; k < 3; ++k) {
-            CUDA_TRY(s, cudaMemcpy(field.data(), static_cast<char *>(s->layer_parts) + e * s->n_device * k, field.size(),
-                                   cudaMemcpyDeviceToHost));
-            for (uint64_t c = 0; c < s->layers; ++c) std::memcpy(dst + e * (9 * c + k), field.data() + e * cells[c], e);
-        }
-        std::vector<char> &face = field;
+        for (uint64_t c = 0; c < s->layers; ++c)
+            for (int k = 0; k < 3; ++k) std::memcpy(dst + e * (9 * c + k), parts.data() + e * (k * s->layers + c), e);
+        std::vector<char> face(e * s->n_device);
         const uint64_t strides[3] = {1, s->pitch, s->pitch * s->ny};
         for (int axis = 0; axis < 3; ++axis) {
             CUDA_TRY(s, cudaMemcpy(face.data(), s->faces[1][axis], face.size(), cudaMemcpyDeviceToHost));

@@ -1,11 +1,10 @@
 // Device code of the B200 wave stepper: one time step of WaveSolver::run
-// (cpp/include/acoustic_spaces/fdtd.hpp:786-904 of naelolaiz/acoustic-spaces) as three kernels.
+// (cpp/include/acoustic_spaces/fdtd.hpp:786-904 of naelolaiz/acoustic-spaces) as four kernels.
 //
 // A step reads the current pressure b and branch velocities wb, and writes the next pressure over
-// the previous one in a, the branch velocities over wa and the matched layer's state (its parts in
-// place, its faces into the other of two buffers). Each cell's new value depends only on b, wb and
-// its own a, wa and layer state, so the kinds of work (the sweep of the interior air and the
-// matched layer, the special rows, the probe records) write disjoint memory.
+// the previous one in a, the branch velocities over wa and the matched layer's state in place.
+// Each cell's new value depends only on b, wb and its own a, wa and layer state, so the four kinds
+// of work (interior air, special rows, matched-layer cells, probe records) write disjoint memory.
 //
 // Fields live on the device in a pitched layout: cell (x, y, z) at x + pitch * (y + ny * z), with
 // pitch = nx rounded up to 16 cells, so that every row starts 64-byte aligned and the tensor maps
@@ -69,19 +68,7 @@ struct BulkArgs {
     uint32_t tiles;
     float axial, diagonal, centre, total;
     unsigned int *error;  // set to 1 when a wait gives up
-    // The matched layer (fdtd.hpp:2242-2264), swept with the interior: per axis the pressure part
-    // of each layer cell and the velocity on its + face, pitched (T); the face velocities a step
-    // before and this step; per axis and grid coordinate {keep, push, keep_face, push_face}.
-    void *parts[3];
-    const void *face_old[3];
-    void *face_new[3];
-    const float4 *layer_coef[3];
 };
-
-// A matched-layer cell's type byte carries, above the type, which of its lower neighbours (bit
-// 2 + axis) are in the layer too.
-constexpr uint32_t kTypeMask = 3u;
-constexpr uint32_t kBelowShift = 2u;
 
 // ---- PTX helpers (mbarrier, TMA) ---------------------------------------------------------------
 
@@ -140,16 +127,15 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map
 
 // ---- interior air ------------------------------------------------------------------------------
 
-// Interior air (fdtd.hpp:242-288) and the matched layer (fdtd.hpp:2242-2264, layer_cell above). The
-// swept cells are covered by tiles of kTX x kTY cells by a chunk of planes along z (a list, only
-// tiles that hold interior or layer cells); each block takes tiles
+// Interior air (fdtd.hpp:242-288). The interior cells are covered by tiles of kTX x kTY cells by a
+// chunk of planes along z (a list, only tiles that hold interior cells); each block takes tiles
 // blockIdx.x, + gridDim.x, ... and marches each along z. Its planes' stages — plane k's pressure
 // tile with halos, previous pressure, types and scales — form one sequence over all its tiles:
 // tile m's stages are planes z0-1 .. z_end. Thread 0 issues the sequence with TMA, kAhead stages
 // ahead of the three in use (across tile boundaries too), into a ring of kStages slots in shared
 // memory, each completed on its slot's mbarrier; the block updates plane z from the stages of
 // planes z-1, z and z+1, each thread 8 rows of one column, and stores the new pressure of the
-// interior and layer cells (a layer cell also its parts and faces). Every wait is bounded: a block that gives up sets the error flag, lets its
+// interior cells. Every wait is bounded: a block that gives up sets the error flag, lets its
 // copies in flight land, and stops.
 // The reference's sums in its order: x-1, x+1, y-1, y+1, z-1, z+1, then the twelve edges.
 struct TileSpan {
@@ -161,52 +147,7 @@ __device__ __forceinline__ TileSpan tile_span(const BulkArgs &p, uint32_t tile) 
     return TileSpan{t.x, t.y, t.z, t.w};
 }
 
-// A matched-layer cell (fdtd.hpp:2242-2264): per axis its two face velocities, then its pressure
-// part; the cell's pressure is the parts' sum. The neighbours' pressures come from the tile's
-// stages in shared memory.
-//
-// The reference keeps, per layer cell, its own copy of the velocity on each of its six faces
-// (fdtd.hpp:2245), and both cells of a face update their copies alike: cell i's + face along an
-// axis of stride s and cell i+s's - face take keep_face[x+1] * u - push_face[x+1] * (b[i+s] -
-// b[i]) from the same value, so that, both starting at 0, the two copies stay equal to the bit.
-// Here each face is kept once, on the cell below it (face[i] is cell i's + face), in two buffers
-// that alternate with the steps: every cell reads the old values of its two faces and works both
-// out again, and writes the new value of its + face, and of its - face too where the cell below
-// is not in the layer (no one else writes that face).
-template <typename T, bool SCALED>
-__device__ __forceinline__ void layer_cell(const BulkArgs &p, uint64_t at, uint32_t type, uint32_t x, uint32_t y,
-                                           uint32_t z, T here, T x_lo, T x_hi, T y_lo, T y_hi, T z_lo, T z_hi,
-                                           float scale_f, T *__restrict__ a, uint64_t plane) {
-    const uint32_t coord[3] = {x, y, z};
-    const uint64_t strides[3] = {1u, p.pitch, plane};
-    const T lo[3] = {x_lo, y_lo, z_lo}, hi[3] = {x_hi, y_hi, z_hi};
-    const T scale = (T)scale_f;
-    T total = 0;
-#pragma unroll
-    for (int axis = 0; axis < 3; ++axis) {
-        const T *face_old = static_cast<const T *>(p.face_old[axis]);
-        T *face_new = static_cast<T *>(p.face_new[axis]);
-        T *parts = static_cast<T *>(p.parts[axis]);
-        const uint64_t stride = strides[axis];
-        const float4 c0 = p.layer_coef[axis][coord[axis]], c1 = p.layer_coef[axis][coord[axis] + 1];
-        const T below = (T)c0.z * face_old[at - stride] - (T)c0.w * (here - lo[axis]);
-        const T above = (T)c1.z * face_old[at] - (T)c1.w * (hi[axis] - here);
-        face_new[at] = above;
-        // The cell below owns the face when it is in the layer.
-        if (!(type & (1u << (kBelowShift + axis)))) face_new[at - stride] = below;
-        T part = parts[at];
-        if (SCALED) {
-            part = (T)c0.x * part - ((T)c0.y * scale) * (above - below);
-        } else {
-            part = (T)c0.x * part - (T)c0.y * (above - below);
-        }
-        parts[at] = part;
-        total += part;
-    }
-    a[at] = total;
-}
-
-template <typename T, bool WIDE, bool SCALED, bool LAYER>
+template <typename T, bool WIDE, bool SCALED>
 __global__ void __launch_bounds__(kBlock) bulk_kernel(const __grid_constant__ CUtensorMap map_b,
                                                       const __grid_constant__ CUtensorMap map_a,
                                                       const __grid_constant__ CUtensorMap map_t,
@@ -282,17 +223,10 @@ __global__ void __launch_bounds__(kBlock) bulk_kernel(const __grid_constant__ CU
                 for (int r = 0; r < kRowsPerThread; ++r) {
                     const int yl = r0 + r;
                     const int c = yl * kTX + xl;
-                    // Outside the swept cells' box, and outside the grid (zero fill), no cell is
-                    // interior or in the layer.
-                    const uint32_t type = pt[c];
+                    // Outside the interior cells' box, and outside the grid (zero fill), no cell
+                    // is interior.
+                    if (pt[c] != kInterior) continue;
                     const int q = (yl + 1) * kBX + (xl + kHX);
-                    const uint64_t at = (uint64_t)x + (uint64_t)(t.yt + yl) * p.pitch + (uint64_t)z * plane;
-                    if (LAYER && (type & kTypeMask) == kLayer) {
-                        layer_cell<T, SCALED>(p, at, type, x, t.yt + yl, z, b0[q], b0[q - 1], b0[q + 1], b0[q - kBX],
-                                              b0[q + kBX], bm[q], bp[q], SCALED ? ps[c] : 1.0f, a, plane);
-                        continue;
-                    }
-                    if (type != kInterior) continue;
                     const T here = b0[q];
                     const T sum = b0[q - 1] + b0[q + 1] + b0[q - kBX] + b0[q + kBX] + bm[q] + bp[q];
                     T next;
@@ -314,7 +248,7 @@ __global__ void __launch_bounds__(kBlock) bulk_kernel(const __grid_constant__ CU
                             next = centre * here + axial * sum - pa[c];
                         }
                     }
-                    a[at] = next;
+                    a[(uint64_t)x + (uint64_t)(t.yt + yl) * p.pitch + (uint64_t)z * plane] = next;
                 }
             }
             // Every thread is done with plane z-1's stage; stop the block alike if a wait gave up.
@@ -336,7 +270,7 @@ __global__ void __launch_bounds__(kBlock) bulk_kernel(const __grid_constant__ CU
     }
 }
 
-// ---- special rows, probes -------------------------------------------------------
+// ---- special rows, matched layer, probes -------------------------------------------------------
 
 struct Tables {
     uint32_t pitch, ny, nz, sz;
@@ -350,6 +284,15 @@ struct Tables {
     const float *link_weight, *coef_a, *coef_b, *coef_inv, *source;
     const float *state_weight, *state_now, *state_before, *state_gain;
     int32_t offset[18];
+    // Matched layer (fdtd.hpp:2242-2264): cells, and per axis and grid coordinate x (0..n_axis)
+    // {keep of the centre, push of the centre, keep of the face below, push of the face below}
+    // (layer_coefficients, fdtd.hpp:2219-2238); with a speed field each cell's scale.
+    uint32_t layers;
+    const uint32_t *layer_cells;
+    const float *layer_scale;
+    const float4 *layer_coef[3];
+    const uint8_t *layer_below;  // bit a: the cell below along axis a is in the layer too
+    uint32_t plane;  // pitch * ny
     // Probes (fdtd.hpp:3525-3533).
     uint32_t probes;
     const uint32_t *probe_start, *probe_cells;
@@ -362,6 +305,9 @@ struct Fields {
     const T *b;        // the current pressure
     T *wa;             // branch velocities a step before, overwritten with the next
     const T *wb;       // current branch velocities
+    T *layer_parts;    // 3 arrays of `layers`: the pressure parts p_x, p_y, p_z
+    const T *face_old[3];  // per axis, the velocity on each cell's + face (pitched), a step before
+    T *face_new[3];        // the same, this step
     const float *signal;  // the step's drive at signal[0]
     double *out;       // probe p's record at out[p * out_stride]
     uint64_t out_stride;
@@ -410,6 +356,55 @@ __global__ void __launch_bounds__(kBlock) special_kernel(const Tables g, const F
         const T own = (T)g.state_now[j] * f.wb[j] - (T)g.state_before[j] * f.wa[j];
         f.wa[j] = f.wa[j] + ((next - previous) * (T)g.state_gain[j] + own);
     }
+}
+
+// Matched-layer cells (fdtd.hpp:2242-2264), one a thread: per axis the cell's two face
+// velocities, then its pressure part; the cell's pressure is the parts' sum.
+//
+// The reference keeps, per layer cell, its own copy of the velocity on each of its six faces
+// (fdtd.hpp:2245), and both cells of a face update their copies alike: cell i's + face along an
+// axis of stride s and cell i+s's - face take keep_face[x+1] * u - push_face[x+1] * (b[i+s] -
+// b[i]) from the same value, so that, both starting at 0, the two copies stay equal to the bit.
+// Here each face is kept once, on the cell below it (face[i] is cell i's + face), in two buffers
+// that alternate with the steps: every cell reads the old values of its two faces and works both
+// out again, and writes the new value of its + face, and of its - face too where the cell below
+// is not in the layer (no one else writes that face). The pressure parts stay per cell.
+template <typename T, bool SCALED>
+__global__ void __launch_bounds__(kBlock) layer_kernel(const Tables g, const Fields<T> f) {
+    const uint32_t c = blockIdx.x * kBlock + threadIdx.x;
+    const uint32_t L = g.layers;
+    if (c >= L) return;
+    T *parts = f.layer_parts;
+    T part[3];
+#pragma unroll
+    for (int axis = 0; axis < 3; ++axis) part[axis] = parts[axis * L + c];
+    const uint32_t i = g.layer_cells[c];
+    const uint32_t at[3] = {i % g.pitch, (i / g.pitch) % g.ny, i / g.plane};
+    const uint32_t strides[3] = {1u, g.pitch, g.plane};
+    const T *__restrict__ b = f.b;
+    const T here = b[i];
+    const T scale = SCALED ? (T)g.layer_scale[c] : (T)1;
+    const uint32_t shared_below = g.layer_below[c];
+    T total = 0;
+#pragma unroll
+    for (int axis = 0; axis < 3; ++axis) {
+        const uint32_t stride = strides[axis], x = at[axis];
+        const float4 c0 = g.layer_coef[axis][x], c1 = g.layer_coef[axis][x + 1];
+        const T below = (T)c0.z * f.face_old[axis][i - stride] - (T)c0.w * (here - b[i - stride]);
+        const T above = (T)c1.z * f.face_old[axis][i] - (T)c1.w * (b[i + stride] - here);
+        f.face_new[axis][i] = above;
+        // The cell below owns the face when it is in the layer.
+        if (!(shared_below & (1u << axis))) f.face_new[axis][i - stride] = below;
+        if (SCALED) {
+            part[axis] = (T)c0.x * part[axis] - ((T)c0.y * scale) * (above - below);
+        } else {
+            part[axis] = (T)c0.x * part[axis] - (T)c0.y * (above - below);
+        }
+        total += part[axis];
+    }
+#pragma unroll
+    for (int axis = 0; axis < 3; ++axis) parts[axis * L + c] = part[axis];
+    f.a[i] = total;
 }
 
 // Probe p's pressure before the step (fdtd.hpp:3525-3533): its cells' weighted sum in double, in

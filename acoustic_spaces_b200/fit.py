@@ -274,17 +274,20 @@ class FitProblem:
 
 def patched_room(seed: int = 0, *, size=(10.0, 8.0, 4.0), cell: float = 0.05, receivers: int = 4,
                  steps: int = 3000, precision: str = "fp32", segment: int = 250, perturbation: float = 0.3,
-                 speed_of_sound: float = 343.0) -> FitProblem:  # fmt: skip
+                 speed_of_sound: float = 343.0, split: bool = True, drive: str = "ricker") -> FitProblem:  # fmt: skip
     """A box room of ``size`` metres on cells of ``cell`` with 8 materials on seeded patches (the
-    floor cut in two along x and the ceiling along y at seeded places, and the four side walls),
-    each a 1-pole admittance (a relaxation branch: conductance uniform in [0.05, 0.5], corner
-    frequency log-uniform in [50, 500] Hz); one source and ``receivers`` receivers at seeded places
-    0.5 m from the walls; the target is the room's responses at the seeded true parameters, and
-    the fit starts from them each perturbed by a seeded factor within +-``perturbation``."""
+    floor cut in two along x and the ceiling along y at seeded places, and the four side walls;
+    with ``split`` false, 6 materials, one a face), each a 1-pole admittance (a relaxation branch:
+    conductance uniform in [0.05, 0.5], corner frequency log-uniform in [50, 500] Hz); one source
+    and ``receivers`` receivers at seeded places 0.5 m from the walls; the drive a 0.5 ms Ricker
+    wavelet (``drive="gaussian"``: a Gaussian pulse, which adds net mass, so that the closed room's
+    pressure drifts and the drift, which the walls barely change, dominates the misfit); the target
+    is the room's responses at the seeded true parameters, and the fit starts from them each
+    perturbed by a seeded factor within +-``perturbation``."""
     rng = np.random.default_rng(seed)
     size = np.asarray(size, float)
     rate = speed_of_sound / (layouts.COURANT * cell)
-    materials = 8
+    materials = 8 if split else 6
     conductance = rng.uniform(0.05, 0.5, materials)
     corner = np.exp(rng.uniform(math.log(50.0), math.log(500.0), materials))
     truth = Relaxation(np.zeros(materials), conductance, corner)
@@ -294,6 +297,8 @@ def patched_room(seed: int = 0, *, size=(10.0, 8.0, 4.0), cell: float = 0.05, re
 
     def patches(planes, points):
         planes = np.asarray(planes)
+        if not split:
+            return order[planes]
         patch = np.where(planes == 4, np.where(points[:, 0] < x_cut, 0, 1),
                  np.where(planes == 5, np.where(points[:, 1] < y_cut, 2, 3),
                           4 + np.clip(planes, 0, 3)))  # fmt: skip
@@ -305,13 +310,14 @@ def patched_room(seed: int = 0, *, size=(10.0, 8.0, 4.0), cell: float = 0.05, re
     points = layouts.inside_points(rng, room, size, 1 + receivers, 0.5, apart=4 * cell)
     grid = layouts.room_grid(size, cell)
     built = layouts.cell_face_layout(room, grid, points[0], points[1:], rate=rate)
-    signal = layouts.gaussian_drive(rate, steps)
+    signal = layouts.ricker_drive(rate, steps) if drive == "ricker" else layouts.gaussian_drive(rate, steps)
     fit = AdjointFit(built, signal, np.zeros((receivers, steps)), rate, truth.beta, precision, segment)
     fit.target = fit.responses(truth, "fp64")
     factors = 1.0 + rng.uniform(-perturbation, perturbation, 2 * materials)
     start = Relaxation.from_vector(truth.beta, truth.vector() * factors)
     description = {
-        "room": f"box {size[0]:g}x{size[1]:g}x{size[2]:g} m, 8 materials on patches, 1-pole each",
+        "room": f"box {size[0]:g}x{size[1]:g}x{size[2]:g} m, {materials} materials on "
+        + ("patches" if split else "its faces") + ", 1-pole each",
         "grid": "x".join(str(v) for v in grid.shape),
         "cell_m": cell,
         "air_cells": built.air_cells,
@@ -320,6 +326,7 @@ def patched_room(seed: int = 0, *, size=(10.0, 8.0, 4.0), cell: float = 0.05, re
         "receivers": receivers,
         "steps": steps,
         "parameters": 2 * materials,
+        "drive": "0.5 ms Ricker wavelet" if drive == "ricker" else "0.5 ms Gaussian pulse",
         "checkpoint_every": segment,
         "seed": seed,
     }

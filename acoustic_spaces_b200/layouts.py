@@ -654,6 +654,15 @@ def gaussian_drive(rate: float, steps: int, sigma_s: float = 0.5e-3) -> np.ndarr
     return np.exp(-0.5 * t * t).astype(np.float32)
 
 
+def ricker_drive(rate: float, steps: int, sigma_s: float = 0.5e-3) -> np.ndarray:
+    """The second derivative of a Gaussian of ``sigma_s`` seconds (a Ricker wavelet), sampled at
+    ``rate``, centred at 6 sigma, peak 1: a drive that adds no net mass to a closed room (zero mean
+    and zero first moment, as the reference's twice high-passed drive, engine/wave.py:135-139), so
+    that a closed room's pressure does not drift."""
+    t = (np.arange(steps) - 6.0 * sigma_s * rate) / (sigma_s * rate)
+    return ((1.0 - t * t) * np.exp(-0.5 * t * t)).astype(np.float32)
+
+
 @dataclass
 class Workload:
     """A seeded room ready to step: its room, grid, layout, drive and description."""

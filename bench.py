@@ -49,9 +49,8 @@ BYTES_SPECIAL = 40  # read p, read/write p-, coef_a/b/inv/source, its index and 
 BYTES_LINK = 5  # direction and weight
 BYTES_STATE = 28  # read/write w-, read w, its four coefficients
 # A layer cell keeps three pressure parts and, on the cell below each face, one velocity per
-# face (the reference's nine values per cell hold every face twice, 84 B); it is swept with the
-# interior, so it has no index of its own:
-BYTES_LAYER = 56  # read p, write p+, read/write three parts, read/write three faces
+# face (the reference's nine values per cell hold every face twice, 84 B):
+BYTES_LAYER = 60  # read p, write p+, read/write three parts, read/write three faces, its index
 
 
 def algorithmic_bytes(d: dict) -> int:
@@ -558,9 +557,9 @@ def main() -> None:
     peak, peak_source = measured_peaks()
     achieved = bytes_per_step / (ms / 1e3 / steps) / 1e9
     # Each kernel's algorithmic bytes per launch and its average launch time, live.
-    # (The sweep kernel steps the interior and the matched-layer cells.)
     per_kernel_bytes = {
-        "bulk": BYTES_INTERIOR * desc["interior_cells"] + BYTES_LAYER * desc["layer_cells"],
+        "bulk": BYTES_INTERIOR * desc["interior_cells"],
+        "layer": BYTES_LAYER * desc["layer_cells"],
         "special": BYTES_SPECIAL * desc["special_rows"] + BYTES_LINK * desc["links"] + BYTES_STATE * desc["branch_states"],
     }
     traffic_table = {}
@@ -580,8 +579,9 @@ def main() -> None:
         }
     kernels["probe"] = {"mean_launch_us": round(kernel_ms["probe"] / max(1, kernel_ms["steps"]) * 1e3, 2)}
     dominant = max(per_kernel_bytes, key=lambda k: kernel_ms[k])
-    # Launches a step: the sweep, the special rows, the probes (each when the grid has its cells).
-    launches_per_step = int(desc["interior_cells"] + desc["layer_cells"] > 0) + int(desc["special_rows"] > 0) + int(solver.probes > 0)
+    # Launches a step: the interior sweep, the matched layer, the special rows, the probes (each
+    # when the grid has such cells).
+    launches_per_step = sum(int(desc[k] > 0) for k in ("interior_cells", "layer_cells", "special_rows")) + int(solver.probes > 0)
 
     line = None
     if rank == 0:

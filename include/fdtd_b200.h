@@ -148,9 +148,9 @@ void *fdtd_stream(const fdtd_solver *solver);
 /*
  * Per-kernel timing of fdtd_run_device (no counterpart in the reference): with `enable` set, each
  * step's kernels run one after another on the handle's stream, each bracketed by CUDA events, and
- * fdtd_get_timing adds up, since the last call, the milliseconds each kind took — ms[0] the sweep
- * of the interior and matched-layer cells, ms[1] 0 (the matched layer has no kernel of its own),
- * ms[2] the special rows, ms[3] the probe records — over *steps steps. The work done is the same.
+ * fdtd_get_timing adds up, since the last call, the milliseconds each kind took — ms[0] the
+ * interior sweep, ms[1] the matched layer, ms[2] the special rows, ms[3] the probe records — over
+ * *steps steps. The work done is the same.
  */
 int fdtd_set_timing(fdtd_solver *solver, int enable);
 int fdtd_get_timing(fdtd_solver *solver, double ms[4], uint64_t *steps);
