@@ -16,6 +16,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <unordered_map>
@@ -1071,6 +1072,73 @@ int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float
     return fdtd_reset(s);
 }
 
+// ---- fdtd_gradient_noalloc: the gradient's device memory from a static pool ------------------------
+
+// The pool, in static device memory (one per device, held until the process exits); aligned for
+// the tensor maps over the adjoint levels (16 bytes) and for coalesced access. Host code reaches it
+// only through the address cudaGetSymbolAddress gives (pool_address).
+constexpr size_t kPoolBytes = FDTD_GRADIENT_STATIC_BYTES;
+constexpr size_t kPoolAlign = 256;
+static __device__ __align__(256) unsigned char g_gradient_pool[kPoolBytes];
+
+constexpr size_t pool_round(size_t bytes) { return ((bytes ? bytes : 16) + kPoolAlign - 1) / kPoolAlign * kPoolAlign; }
+
+// The pool's address on each device, looked up once per device with that device current.
+constexpr int kPoolDevices = 64;
+std::mutex g_pool_mutex;
+void *g_pool_address[kPoolDevices] = {};
+
+int pool_address(fdtd_solver *s, void **out) {
+    *out = nullptr;
+    if (s->device < 0 || s->device >= kPoolDevices) return fail(s, FDTD_EINVAL, "the static pool serves devices 0 to 63");
+    std::lock_guard<std::mutex> lock(g_pool_mutex);
+    if (!g_pool_address[s->device]) {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_gradient_pool);
+        if (e != cudaSuccess) return cuda_fail(s, e, "cudaGetSymbolAddress of the gradient's static pool");
+        g_pool_address[s->device] = p;
+    }
+    *out = g_pool_address[s->device];
+    return FDTD_OK;
+}
+
+// Blocks of the pool handed out in order; each to be cleared is cleared on the handle's stream,
+// in order with the gradient's own work.
+struct StaticPool {
+    fdtd_solver *s;
+    char *base;
+    size_t used = 0;
+    int take(size_t bytes, void **out, bool zero) {
+        *out = nullptr;
+        const size_t size = pool_round(bytes);
+        if (used + size > kPoolBytes) return fail(s, FDTD_EINVAL, "the gradient's buffers outgrow the static pool");
+        *out = base + used;
+        used += size;
+        if (zero) CUDA_TRY(s, cudaMemsetAsync(*out, 0, size, s->stream));
+        return FDTD_OK;
+    }
+    int take(size_t bytes, void **out) { return take(bytes, out, true); }  // gradient<T>'s scratch
+};
+
+// The pool's bytes for one gradient: the blocks place_adjoint and then gradient<T> take, in order.
+size_t pool_bytes(const fdtd_solver *s, const AdjointLists &l, uint64_t steps, uint64_t segment) {
+    const size_t e = s->precision == FDTD_FP64 ? 8 : 4;
+    const uint64_t K = s->specials, S = s->states, P = std::max<uint64_t>(1, s->probes), n = s->n_device;
+    size_t total = 0;
+    auto list = [&](size_t count, size_t unit) { total += count ? pool_round(count * unit) : 0; };
+    list(l.reader_start.size(), 4), list(l.reader_index.size(), 4), list(l.reader_kind.size(), 1);
+    list(l.reader_coef.size(), 8), list(l.cells.size(), 4), list(l.starts.size(), 4), list(l.rows.size(), 4);
+    list(l.coefs.size(), 8);
+    total += 2 * (pool_round(e * n) + pool_round(e * S)) + pool_round(e * K);
+    if (segment == 0 || segment > steps) segment = steps;
+    const uint64_t segments = (steps + segment - 1) / segment;
+    total += pool_round(4 * steps) + pool_round(8 * P * steps) + pool_round(e * K * (segment + 2)) +
+             pool_round(e * S * (segment + 2)) + pool_round(8 * P * segment);
+    total += 2 * pool_round(8 * K) + 3 * pool_round(8 * S);
+    total += (segments - 1) * pool_round(2 * e * n + 2 * e * S);
+    return total;
+}
+
 struct DeviceGuard {
     int previous = -1;
     explicit DeviceGuard(int device) {
@@ -1246,6 +1314,37 @@ int fdtd_run(fdtd_solver *s, const float *signal, uint64_t steps, double *out) {
         if (!std::isfinite(out[k])) return fail(s, FDTD_ENONFINITE, "the wave solver's run did not stay finite");
     }
     return FDTD_OK;
+}
+
+int fdtd_gradient_noalloc(fdtd_solver *s, const float *signal, uint64_t steps, const double *dloss_dy,
+                          uint64_t segment, double *grad_coef_b, double *grad_coef_inv, double *grad_now,
+                          double *grad_before, double *grad_gain) {
+    if (!s) return set_global(FDTD_EINVAL, "no solver");
+    if (steps == 0) return fail(s, FDTD_EINVAL, "no steps to differentiate");
+    if (!signal || (s->probes && !dloss_dy)) return fail(s, FDTD_EINVAL, "no signal or loss gradient");
+    DeviceGuard guard(s->device);
+    void *base;
+    int rc;
+    if ((rc = pool_address(s, &base)) != FDTD_OK) return rc;
+    AdjointLists lists;
+    if ((rc = adjoint_lists(s, lists)) != FDTD_OK) return rc;
+    const size_t need = pool_bytes(s, lists, steps, segment);
+    if (need > kPoolBytes) {
+        char message[200];
+        std::snprintf(message, sizeof message,
+                      "the gradient needs %llu bytes of device memory; the static pool holds %llu: fewer steps, a "
+                      "longer segment, or fdtd_gradient",
+                      (unsigned long long)need, (unsigned long long)kPoolBytes);
+        return fail(s, FDTD_EINVAL, message);
+    }
+    // This handle's earlier calls have ended (each ends with its stream), so the pool is free here
+    // unless another call overlaps this one, which the header warns of.
+    StaticPool pool{s, static_cast<char *>(base)};
+    AdjointState adj;
+    if ((rc = place_adjoint(s, lists, pool, adj)) != FDTD_OK) return rc;
+    double *grads[5] = {grad_coef_b, grad_coef_inv, grad_now, grad_before, grad_gain};
+    return s->precision == FDTD_FP64 ? gradient<double>(s, adj, pool, signal, steps, dloss_dy, segment, grads)
+                                     : gradient<float>(s, adj, pool, signal, steps, dloss_dy, segment, grads);
 }
 
 int fdtd_set_timing(fdtd_solver *s, int enable) {

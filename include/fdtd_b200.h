@@ -172,6 +172,33 @@ int fdtd_gradient(fdtd_solver *solver, const float *signal, uint64_t steps, cons
                   uint64_t segment, double *grad_coef_b, double *grad_coef_inv, double *grad_now,
                   double *grad_before, double *grad_gain);
 
+/* Bytes of the static device pool of fdtd_gradient_noalloc: 16 MiB, held on every device the
+   library runs on until the process exits. */
+#define FDTD_GRADIENT_STATIC_BYTES (16ull << 20)
+
+/*
+ * fdtd_gradient without a device allocation; it has no counterpart in the reference. It computes
+ * the same gradient with the same kernels in the same order, but every device buffer it needs —
+ * the adjoint's tables and levels, the drive and dL/dy, the trajectory, the checkpoints, the sums —
+ * is carved from a pool of FDTD_GRADIENT_STATIC_BYTES that the library keeps in static device
+ * memory, so the call makes no cudaMalloc or cudaFree and keeps nothing on the handle. It is for
+ * callers that must not allocate while they run: cudaMalloc and cudaFree can synchronize the whole
+ * device and so stall every other stream on it (another solver's steps, a renderer's or a model's
+ * kernels), and a process whose device memory belongs to a caching allocator (PyTorch's) may have
+ * none left to give. A run whose buffers do not fit the pool is refused with FDTD_EINVAL before any
+ * device work, the message giving the bytes it needs (take fewer steps, a longer `segment`, or
+ * fdtd_gradient). The first call on a device looks up the pool's device address
+ * (cudaGetSymbolAddress) with that device current; make that first call before any stream capture
+ * on the device. There is one pool per device, shared by every handle and kept between calls:
+ * what must start at zero is cleared by each call, but calls whose work overlaps on a device — from
+ * two threads, or on two handles — race on the pool and give wrong results. A call returns only
+ * when its work has ended, so calls made one after another are safe. Arguments, results and
+ * refusals are otherwise those of fdtd_gradient.
+ */
+int fdtd_gradient_noalloc(fdtd_solver *solver, const float *signal, uint64_t steps, const double *dloss_dy,
+                          uint64_t segment, double *grad_coef_b, double *grad_coef_inv, double *grad_now,
+                          double *grad_before, double *grad_gain);
+
 /* Replaces WaveSolver::reset (fdtd.hpp:906-915): silences the grid. */
 int fdtd_reset(fdtd_solver *solver);
 
