@@ -45,10 +45,14 @@ struct AdjointTables {
     const uint32_t *corrected_cell, *corrected_start, *corrected_row;
     const double *corrected_coef;
     float axial;
-    // Probes: CSR of pitched cells and weights.
+    // Probes: CSR of pitched cells and weights; and by the cells they read, each cell's
+    // (probe, weight) terms: read_start[c] .. read_start[c + 1].
     uint32_t probes;
     const uint32_t *probe_start, *probe_cells;
     const double *probe_weights;
+    uint32_t read_cells;
+    const uint32_t *read_cell, *read_start, *read_probe;
+    const double *read_weight;
 };
 
 // The trajectory of a run: level l of the special rows' pressure at traj_u[l * specials + k] and
@@ -133,16 +137,18 @@ __global__ void __launch_bounds__(kBlock) special_adjoint_kernel(const AdjointTa
     }
 }
 
-// The probes' terms of level n: lam_n[cell] += weight * dL/dy_p^n.
+// The probes' terms of level n: lam_n[cell] += sum over the probes reading the cell of weight *
+// dL/dy_p^n, a thread per cell that probes read, its terms summed in double in a fixed order (so
+// that the result does not depend on the threads' timing).
 template <typename T>
 __global__ void __launch_bounds__(kBlock) probe_adjoint_kernel(const AdjointTables t, const double *dloss, uint64_t stride,
                                                                uint64_t step, T *lam_out) {
-    const uint32_t p = blockIdx.x * kBlock + threadIdx.x;
-    if (p >= t.probes) return;
-    const double g = dloss[(uint64_t)p * stride + step];
-    if (g == 0.0) return;
-    for (uint32_t e = t.probe_start[p], end = t.probe_start[p + 1]; e < end; ++e)
-        atomicAdd(&lam_out[t.probe_cells[e]], (T)(t.probe_weights[e] * g));
+    const uint32_t c = blockIdx.x * kBlock + threadIdx.x;
+    if (c >= t.read_cells) return;
+    double sum = 0.0;
+    for (uint32_t e = t.read_start[c], end = t.read_start[c + 1]; e < end; ++e)
+        sum += t.read_weight[e] * dloss[(uint64_t)t.read_probe[e] * stride + step];
+    if (sum != 0.0) lam_out[t.read_cell[c]] += (T)sum;
 }
 
 }  // namespace fdtd

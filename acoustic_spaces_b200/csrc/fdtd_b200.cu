@@ -45,6 +45,12 @@ constexpr int kSteps[18][3] = {
 
 constexpr uint64_t kPitchCells = 16;  // rows padded to a multiple of 16 cells
 constexpr uint64_t kGraphSteps = 64;  // steps of fdtd_run's captured chunk (even: the roles return)
+// Grids of at least this many (pitched) cells step by direct launches in fdtd_run: their steps are
+// long enough (a quarter of a millisecond and more) that launching costs nothing, and replaying a
+// captured graph measured 8 % slower than the launches on the 47M-cell room (the streams
+// overlapped less). Smaller grids replay the graph: below some 10M cells a step's launches and
+// event waits cost as much host time as the step takes on the device.
+constexpr uint64_t kGraphCells = 1ull << 25;
 
 using EncodeTiled = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
@@ -112,6 +118,16 @@ struct fdtd_solver {
     // The adjoint (fdtd_gradient), set up on first use and kept.
     bool adjoint_ready = false;
     AdjointState adjoint;
+    // While the gradient recomputes a segment: the special rows' values after each step of a
+    // dispatch, recorded as level k + 2 of the trajectory after the dispatch's step k.
+    const AdjointTables *record_tables = nullptr;
+    void *record_u = nullptr, *record_w = nullptr;
+    // The tape (fdtd_set_tape): a run of fdtd_run from rest keeps the state at every multiple of
+    // tape_segment steps before its end, and its drive, for the gradient that follows.
+    uint64_t tape_segment = 0;
+    bool tape_valid = false;
+    std::vector<float> tape_signal;
+    std::vector<void *> tape_checkpoints;
     // Staging for fdtd_run's host buffers, grown on demand.
     float *stage_signal = nullptr;
     double *stage_out = nullptr;
@@ -397,8 +413,17 @@ int launch_steps(fdtd_solver *s, const float *d_signal, uint64_t steps, double *
         }
         if (ev) CUDA_TRY(s, cudaEventRecord(ev[5], side));
         if (ev) CUDA_TRY(s, cudaEventRecord(ev[6], side));
-        if (probe_blocks) probe_kernel<T><<<probe_blocks, kBlock, 0, side>>>(g, f);
+        // (A recomputation for the gradient records the special rows instead of the probes.)
+        if (probe_blocks && !s->record_tables) probe_kernel<T><<<probe_blocks, kBlock, 0, side>>>(g, f);
         if (ev) CUDA_TRY(s, cudaEventRecord(ev[7], side));
+        if (s->record_tables) {
+            // The special rows' new values (the special kernel's, on the same stream before).
+            const AdjointTables &t = *s->record_tables;
+            const uint32_t rows = (uint32_t)((std::max<uint32_t>(std::max(t.specials, t.states), 1u) + kBlock - 1) / kBlock);
+            record_kernel<T><<<rows, kBlock, 0, side>>>(t, f.a, f.wa,
+                                                        static_cast<T *>(s->record_u) + (k + 2) * (uint64_t)t.specials,
+                                                        static_cast<T *>(s->record_w) + (k + 2) * (uint64_t)t.states);
+        }
         if (fork) {
             CUDA_TRY(s, cudaEventRecord(s->joined[1], side));
             CUDA_TRY(s, cudaEventRecord(s->joined[2], layer));
@@ -778,6 +803,8 @@ int download(fdtd_solver *s, const V *device, size_t count, std::vector<V> &host
 // and the interior cells next to special rows with their corrections.
 struct AdjointLists {
     std::vector<uint32_t> reader_start, reader_index, cells, starts, rows;
+    std::vector<uint32_t> read_cell, read_start, read_probe;  // the probes' terms by cell
+    std::vector<double> read_weight;
     std::vector<uint8_t> reader_kind;
     std::vector<double> reader_coef, coefs;
 };
@@ -839,6 +866,29 @@ int adjoint_lists(fdtd_solver *s, AdjointLists &out) {
         }
         out.reader_start[k + 1] = (uint32_t)out.reader_index.size();
     }
+    // The probes' terms grouped by cell, each cell's in the order of the probes and their cells.
+    std::vector<uint32_t> probe_start, probe_cells;
+    std::vector<double> probe_weights;
+    if ((rc = download(s, g.probe_start, (size_t)g.probes + 1, probe_start))) return rc;
+    if ((rc = download(s, g.probe_cells, (size_t)probe_start[g.probes], probe_cells))) return rc;
+    if ((rc = download(s, g.probe_weights, (size_t)probe_start[g.probes], probe_weights))) return rc;
+    std::vector<std::pair<uint32_t, uint32_t>> by_cell;  // (cell, entry)
+    for (uint32_t p = 0; p < g.probes; ++p)
+        for (uint32_t e = probe_start[p]; e < probe_start[p + 1]; ++e) by_cell.push_back({probe_cells[e], e});
+    std::stable_sort(by_cell.begin(), by_cell.end(),
+                     [](const auto &a, const auto &b) { return a.first < b.first; });
+    std::vector<uint32_t> owner(probe_start.empty() ? 0 : probe_start[g.probes]);
+    for (uint32_t p = 0; p < g.probes; ++p)
+        for (uint32_t e = probe_start[p]; e < probe_start[p + 1]; ++e) owner[e] = p;
+    for (size_t i = 0; i < by_cell.size(); ++i) {
+        if (i == 0 || by_cell[i].first != by_cell[i - 1].first) {
+            out.read_cell.push_back(by_cell[i].first);
+            out.read_start.push_back((uint32_t)out.read_probe.size());
+        }
+        out.read_probe.push_back(owner[by_cell[i].second]);
+        out.read_weight.push_back(probe_weights[by_cell[i].second]);
+    }
+    out.read_start.push_back((uint32_t)out.read_probe.size());
     out.starts.assign(1, 0);
     for (auto &[cell, list] : corrected) {
         out.cells.push_back(cell);
@@ -885,6 +935,11 @@ int place_adjoint(fdtd_solver *s, const AdjointLists &l, Pool &pool, AdjointStat
     if ((rc = place(s, pool, l.starts, &t.corrected_start))) return rc;
     if ((rc = place(s, pool, l.rows, &t.corrected_row))) return rc;
     if ((rc = place(s, pool, l.coefs, &t.corrected_coef))) return rc;
+    if ((rc = place(s, pool, l.read_cell, &t.read_cell))) return rc;
+    if ((rc = place(s, pool, l.read_start, &t.read_start))) return rc;
+    if ((rc = place(s, pool, l.read_probe, &t.read_probe))) return rc;
+    if ((rc = place(s, pool, l.read_weight, &t.read_weight))) return rc;
+    t.read_cells = (uint32_t)l.read_cell.size();
     for (int k = 0; k < 2; ++k) {
         if ((rc = pool.take(e * s->n_device, &a.lam[k], true))) return rc;
         if ((rc = pool.take(e * S, &a.om[k], true))) return rc;
@@ -974,6 +1029,11 @@ int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float
     T *traj_w = static_cast<T *>(p);
     if ((rc = scratch.take(sizeof(double) * std::max<uint64_t>(1, P) * segment, &p))) return rc;
     double *d_out = static_cast<double *>(p);
+    // The drive and dL/dy of the segment at hand.
+    if ((rc = scratch.take(sizeof(float) * segment, &p))) return rc;
+    float *seg_signal = static_cast<float *>(p);
+    if ((rc = scratch.take(sizeof(double) * std::max<uint64_t>(1, P) * segment, &p))) return rc;
+    double *seg_dloss = static_cast<double *>(p);
     double *g[5];
     const uint64_t g_len[5] = {K, K, S, S, S};  // coef_b, coef_inv, now, before, gain
     for (int k = 0; k < 5; ++k) {
@@ -1001,10 +1061,17 @@ int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float
         }
         return FDTD_OK;
     };
-    // The forward pass from rest, keeping checkpoints[m] = the state at the start of segment m+1.
-    if ((rc = fdtd_reset(s)) != FDTD_OK) return rc;
+    // The forward pass from rest, keeping checkpoints[m] = the state at the start of segment m+1;
+    // or, when the handle holds the tape of a run of this drive with these segments, its states.
+    const bool taped = s->tape_valid && s->tape_signal.size() == steps &&
+                       std::min<uint64_t>(s->tape_segment, steps) == segment &&
+                       std::memcmp(s->tape_signal.data(), signal, sizeof(float) * steps) == 0;
     std::vector<char *> checkpoints;
-    for (uint64_t k = 0; k + 1 < segments; ++k) {
+    if (taped)
+        for (uint64_t k = 0; k + 1 < segments; ++k) checkpoints.push_back(static_cast<char *>(s->tape_checkpoints[k]));
+    else if ((rc = fdtd_reset(s)) != FDTD_OK)
+        return rc;
+    for (uint64_t k = 0; !taped && k + 1 < segments; ++k) {
         if ((rc = dispatch(s, d_signal + k * segment, segment, d_out, segment)) != FDTD_OK) return rc;
         settle(s, segment);
         if ((rc = scratch.take(2 * level_bytes + 2 * state_bytes, &p))) return rc;
@@ -1020,50 +1087,71 @@ int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float
     const uint32_t row_blocks = (uint32_t)((std::max<uint64_t>(std::max<uint64_t>(K, S), 1) + kBlock - 1) / kBlock);
     const uint32_t special_blocks = (uint32_t)((K + kBlock - 1) / kBlock);
     const uint32_t corrected_blocks = (uint32_t)((t.corrected + kBlock - 1) / kBlock);
-    const uint32_t probe_blocks = (uint32_t)((P + kBlock - 1) / kBlock);
+    const uint32_t probe_blocks = (uint32_t)((t.read_cells + kBlock - 1) / kBlock);
     const uint32_t smem = Stage<T, false>::smem;
     T *tilde = static_cast<T *>(adj.tilde);
     int x = 0;  // lam[x], om[x]: level n+1; lam[1-x], om[1-x]: level n+2, then level n
+    // A segment's recomputation (the dispatch of its steps, recording the special rows), and its
+    // reverse steps.
+    auto recompute = [&](uint64_t count) -> int {
+        s->record_tables = &t, s->record_u = traj_u, s->record_w = traj_w;
+        const int r = dispatch(s, seg_signal, count, d_out, segment);
+        s->record_tables = nullptr, s->record_u = s->record_w = nullptr;
+        return r;
+    };
+    auto reverse = [&](uint64_t count) -> int {
+        int xx = x;
+        for (uint64_t m = count; m-- > 0;) {
+            T *lam_next = static_cast<T *>(adj.lam[xx]), *lam_out = static_cast<T *>(adj.lam[1 - xx]);
+            T *om_next = static_cast<T *>(adj.om[xx]), *om_out = static_cast<T *>(adj.om[1 - xx]);
+            // L~ of level n+1; then the interior (the sweep and its corrections) on the handle's
+            // stream beside the special rows on the side stream (they write disjoint cells); then
+            // the probes' terms, which may land on either.
+            if (special_blocks) tilde_kernel<T><<<special_blocks, kBlock, 0, s->stream>>>(t, lam_next, om_next, tilde);
+            CUDA_TRY(s, cudaEventRecord(s->joined[0], s->stream));
+            CUDA_TRY(s, cudaStreamWaitEvent(s->side, s->joined[0], 0));
+            if (special_blocks)
+                special_adjoint_kernel<T><<<special_blocks, kBlock, 0, s->side>>>(
+                    t, lam_next, om_next, tilde, lam_out, om_out, traj_u, traj_w, (uint32_t)m, g[1], g[0], g[2], g[3], g[4]);
+            CUDA_TRY(s, cudaEventRecord(s->joined[1], s->side));
+            if (s->bulk_blocks) {
+                BulkArgs args = s->bulk;
+                args.a = lam_out;
+                bulk_kernel<T, false, false><<<s->bulk_blocks, kBlock, smem, s->stream>>>(adj.lam_b[xx], adj.lam_a[1 - xx],
+                                                                                        s->map_t, s->map_s, args);
+            }
+            if (corrected_blocks) correct_kernel<T><<<corrected_blocks, kBlock, 0, s->stream>>>(t, lam_next, tilde, lam_out);
+            CUDA_TRY(s, cudaStreamWaitEvent(s->stream, s->joined[1], 0));
+            if (probe_blocks)
+                probe_adjoint_kernel<T><<<probe_blocks, kBlock, 0, s->stream>>>(t, seg_dloss, segment, m, lam_out);
+            xx = 1 - xx;
+        }
+        CUDA_TRY(s, cudaGetLastError());
+        return FDTD_OK;
+    };
     for (uint64_t k = segments; k-- > 0;) {
-        const uint64_t s0 = k * segment, s1 = std::min(steps, s0 + segment);
+        const uint64_t s0 = k * segment, s1 = std::min(steps, s0 + segment), count = s1 - s0;
         // Recompute the segment from its start, recording each level of the special rows.
         if (k == 0) {
             if ((rc = fdtd_reset(s)) != FDTD_OK) return rc;
         } else if ((rc = restore(checkpoints[k - 1])) != FDTD_OK) {
             return rc;
         }
+        // Level 0 is the segment's previous level, level 1 its current one, level l + 1 the one
+        // after the segment's step l (recorded by the dispatch).
         record_kernel<T><<<row_blocks, kBlock, 0, s->stream>>>(t, static_cast<const T *>(s->u[0]),
                                                                static_cast<const T *>(s->w[0]), traj_u, traj_w);
-        for (uint64_t n = s0; n < s1; ++n) {
-            const uint64_t level = n - s0 + 1;
-            record_kernel<T><<<row_blocks, kBlock, 0, s->stream>>>(
-                t, static_cast<const T *>(s->u[1]), static_cast<const T *>(s->w[1]), traj_u + level * K, traj_w + level * S);
-            if ((rc = dispatch(s, d_signal + n, 1, d_out, 1)) != FDTD_OK) return rc;
-            settle(s, 1);
-        }
         record_kernel<T><<<row_blocks, kBlock, 0, s->stream>>>(t, static_cast<const T *>(s->u[1]),
-                                                               static_cast<const T *>(s->w[1]),
-                                                               traj_u + (s1 - s0 + 1) * K, traj_w + (s1 - s0 + 1) * S);
-        // The reverse steps of the segment.
-        for (uint64_t n = s1; n-- > s0;) {
-            T *lam_next = static_cast<T *>(adj.lam[x]), *lam_out = static_cast<T *>(adj.lam[1 - x]);
-            T *om_next = static_cast<T *>(adj.om[x]), *om_out = static_cast<T *>(adj.om[1 - x]);
-            if (special_blocks) tilde_kernel<T><<<special_blocks, kBlock, 0, s->stream>>>(t, lam_next, om_next, tilde);
-            if (s->bulk_blocks) {
-                BulkArgs args = s->bulk;
-                args.a = lam_out;
-                bulk_kernel<T, false, false><<<s->bulk_blocks, kBlock, smem, s->stream>>>(adj.lam_b[x], adj.lam_a[1 - x],
-                                                                                        s->map_t, s->map_s, args);
-            }
-            if (corrected_blocks) correct_kernel<T><<<corrected_blocks, kBlock, 0, s->stream>>>(t, lam_next, tilde, lam_out);
-            if (special_blocks)
-                special_adjoint_kernel<T><<<special_blocks, kBlock, 0, s->stream>>>(
-                    t, lam_next, om_next, tilde, lam_out, om_out, traj_u, traj_w, (uint32_t)(n - s0), g[1], g[0], g[2],
-                    g[3], g[4]);
-            if (probe_blocks) probe_adjoint_kernel<T><<<probe_blocks, kBlock, 0, s->stream>>>(t, d_dloss, steps, n, lam_out);
-            x = 1 - x;
-        }
-        CUDA_TRY(s, cudaGetLastError());
+                                                               static_cast<const T *>(s->w[1]), traj_u + K, traj_w + S);
+        CUDA_TRY(s, cudaMemcpyAsync(seg_signal, d_signal + s0, sizeof(float) * count, cudaMemcpyDeviceToDevice, s->stream));
+        if ((rc = recompute(count)) != FDTD_OK) return rc;
+        settle(s, count);
+        // The reverse steps of the segment, with its columns of dL/dy.
+        if (P)
+            CUDA_TRY(s, cudaMemcpy2DAsync(seg_dloss, sizeof(double) * segment, d_dloss + s0, sizeof(double) * steps,
+                                          sizeof(double) * count, P, cudaMemcpyDeviceToDevice, s->stream));
+        if ((rc = reverse(count)) != FDTD_OK) return rc;
+        if (count & 1) x = 1 - x;
     }
     CUDA_TRY(s, cudaStreamSynchronize(s->stream));
     if ((rc = check_device_error(s)) != FDTD_OK) return rc;
@@ -1128,12 +1216,14 @@ size_t pool_bytes(const fdtd_solver *s, const AdjointLists &l, uint64_t steps, u
     auto list = [&](size_t count, size_t unit) { total += count ? pool_round(count * unit) : 0; };
     list(l.reader_start.size(), 4), list(l.reader_index.size(), 4), list(l.reader_kind.size(), 1);
     list(l.reader_coef.size(), 8), list(l.cells.size(), 4), list(l.starts.size(), 4), list(l.rows.size(), 4);
-    list(l.coefs.size(), 8);
+    list(l.coefs.size(), 8), list(l.read_cell.size(), 4), list(l.read_start.size(), 4);
+    list(l.read_probe.size(), 4), list(l.read_weight.size(), 8);
     total += 2 * (pool_round(e * n) + pool_round(e * S)) + pool_round(e * K);
     if (segment == 0 || segment > steps) segment = steps;
     const uint64_t segments = (steps + segment - 1) / segment;
     total += pool_round(4 * steps) + pool_round(8 * P * steps) + pool_round(e * K * (segment + 2)) +
-             pool_round(e * S * (segment + 2)) + pool_round(8 * P * segment);
+             pool_round(e * S * (segment + 2)) + pool_round(8 * P * segment) + pool_round(4 * segment) +
+             pool_round(8 * P * segment);
     total += 2 * pool_round(8 * K) + 3 * pool_round(8 * S);
     total += (segments - 1) * pool_round(2 * e * n + 2 * e * S);
     return total;
@@ -1278,15 +1368,35 @@ int fdtd_run(fdtd_solver *s, const float *signal, uint64_t steps, double *out) {
         CUDA_TRY(s, cudaMallocHost((void **)&s->stage_out, piece * P * sizeof(double)));
         s->stage_steps = piece;
     }
+    // A tape (fdtd_set_tape) of a run from rest: the state at every multiple of the segment before
+    // the run's end, in the checkpoints' layout of the gradient (current level, previous level,
+    // current and previous branch velocities).
+    const bool taping = s->tape_segment && s->steps_done == 0;
+    const uint64_t tape_segment = taping ? std::min(s->tape_segment, steps) : 0;
+    const size_t e = s->precision == FDTD_FP64 ? 8 : 4;
+    const uint64_t level_bytes = e * s->n_device, state_bytes = e * s->states;
+    if (taping) {
+        s->tape_valid = false;
+        const uint64_t needed = (steps + tape_segment - 1) / tape_segment - 1;
+        while (s->tape_checkpoints.size() < needed) {
+            void *p = nullptr;
+            CUDA_TRY(s, cudaMalloc(&p, 2 * level_bytes + 2 * state_bytes));
+            s->allocations.push_back(p);
+            s->device_bytes += 2 * level_bytes + 2 * state_bytes;
+            s->tape_checkpoints.push_back(p);
+        }
+    }
     int rc = FDTD_OK;
     for (uint64_t begin = 0; begin < steps && rc == FDTD_OK; begin += piece) {
         const uint64_t count = std::min(piece, steps - begin);
         std::memcpy(s->stage_signal, signal + begin, count * sizeof(float));
         for (uint64_t done = 0; done < count && rc == FDTD_OK;) {
-            const uint64_t chunk = std::min<uint64_t>(kGraphSteps, count - done);
+            uint64_t chunk = std::min<uint64_t>(kGraphSteps, count - done);
+            const uint64_t at = begin + done;  // steps of this run done before the chunk
+            if (taping) chunk = std::min(chunk, (at / tape_segment + 1) * tape_segment - at);
             CUDA_TRY(s, cudaMemcpyAsync(s->d_sig, s->stage_signal + done, chunk * sizeof(float), cudaMemcpyHostToDevice,
                                         s->stream));
-            if (chunk == kGraphSteps) {
+            if (chunk == kGraphSteps && s->n_device < kGraphCells) {
                 // A whole chunk: the captured graph of its steps for the levels' present roles.
                 cudaGraphExec_t &graph = s->graph[s->flipped ? 1 : 0];
                 if (!graph && (rc = capture(s, &graph)) != FDTD_OK) break;
@@ -1295,6 +1405,17 @@ int fdtd_run(fdtd_solver *s, const float *signal, uint64_t steps, double *out) {
                 break;
             }
             settle(s, chunk);
+            if (taping && (at + chunk) % tape_segment == 0 && at + chunk < steps) {
+                char *c = static_cast<char *>(s->tape_checkpoints[(at + chunk) / tape_segment - 1]);
+                CUDA_TRY(s, cudaMemcpyAsync(c, s->u[1], level_bytes, cudaMemcpyDeviceToDevice, s->stream));
+                CUDA_TRY(s, cudaMemcpyAsync(c + level_bytes, s->u[0], level_bytes, cudaMemcpyDeviceToDevice, s->stream));
+                if (s->states) {
+                    CUDA_TRY(s, cudaMemcpyAsync(c + 2 * level_bytes, s->w[1], state_bytes, cudaMemcpyDeviceToDevice,
+                                                s->stream));
+                    CUDA_TRY(s, cudaMemcpyAsync(c + 2 * level_bytes + state_bytes, s->w[0], state_bytes,
+                                                cudaMemcpyDeviceToDevice, s->stream));
+                }
+            }
             if (s->probes) {
                 CUDA_TRY(s, cudaMemcpy2DAsync(s->stage_out + done, count * sizeof(double), s->d_rec,
                                               kGraphSteps * sizeof(double), chunk * sizeof(double), s->probes,
@@ -1310,6 +1431,10 @@ int fdtd_run(fdtd_solver *s, const float *signal, uint64_t steps, double *out) {
     if (rc != FDTD_OK) return rc;
     CUDA_TRY(s, cudaStreamSynchronize(s->stream));
     if ((rc = check_device_error(s)) != FDTD_OK) return rc;
+    if (taping) {
+        s->tape_signal.assign(signal, signal + steps);
+        s->tape_valid = true;
+    }
     for (uint64_t k = 0; k < s->probes * steps; ++k) {
         if (!std::isfinite(out[k])) return fail(s, FDTD_ENONFINITE, "the wave solver's run did not stay finite");
     }
@@ -1345,6 +1470,13 @@ int fdtd_gradient_noalloc(fdtd_solver *s, const float *signal, uint64_t steps, c
     double *grads[5] = {grad_coef_b, grad_coef_inv, grad_now, grad_before, grad_gain};
     return s->precision == FDTD_FP64 ? gradient<double>(s, adj, pool, signal, steps, dloss_dy, segment, grads)
                                      : gradient<float>(s, adj, pool, signal, steps, dloss_dy, segment, grads);
+}
+
+int fdtd_set_tape(fdtd_solver *s, uint64_t segment) {
+    if (!s) return set_global(FDTD_EINVAL, "no solver");
+    s->tape_segment = segment;
+    s->tape_valid = false;
+    return FDTD_OK;
 }
 
 int fdtd_set_timing(fdtd_solver *s, int enable) {

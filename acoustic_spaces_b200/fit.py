@@ -174,6 +174,7 @@ class AdjointFit:
         precision = precision or self.precision
         lay = self.layout(params)
         solver = B200WaveSolver(lay, precision=precision)
+        solver.set_tape(self.segment)  # the run keeps its checkpoints for the gradient
         t0 = time.perf_counter()
         y = solver.run(self.signal)
         self.forward_s = time.perf_counter() - t0

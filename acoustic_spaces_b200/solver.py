@@ -188,6 +188,14 @@ class B200WaveSolver:
             _raise(self._lib, status, self._handle)
         return out
 
+    def set_tape(self, segment: int) -> None:
+        """With ``segment`` > 0, each :meth:`run` from rest keeps the state every ``segment`` steps
+        (and its drive), so that a following :meth:`gradient` of that drive with that ``segment``
+        does not run the forward pass again; 0 turns it off."""
+        status = self._lib.fdtd_set_tape(self._handle, int(segment))
+        if status != _abi.FDTD_OK:
+            _raise(self._lib, status, self._handle)
+
     def set_timing(self, enable: bool) -> None:
         """Brackets each kernel of the following run_device steps with CUDA events."""
         status = self._lib.fdtd_set_timing(self._handle, int(bool(enable)))

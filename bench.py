@@ -289,7 +289,7 @@ def run_batched(args, world: int, rank: int, local: int) -> None:
     seq_cells, seq_s = 0, 0.0
     for k in sample:
         one = B200WaveSolver(batch.layouts[k], device=local)
-        one.run(batch.signal[:warmup])
+        one.run(batch.signal[: max(warmup, 130)])  # both of its step graphs captured before timing
         one.reset()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -353,10 +353,13 @@ def run_adjoint(args, world: int, rank: int, local: int) -> None:
     f.responses(params, "fp32")  # warm-up
     times = []
     for _ in range(3):
-        f.loss_and_gradient(params, "fp32")
-        times.append((f.forward_s, f.gradient_s))
+        f.responses(params, "fp32")  # a plain forward run
+        plain_s = f.forward_s
+        f.loss_and_gradient(params, "fp32")  # the taped forward run, then the gradient
+        times.append((plain_s, f.forward_s, f.gradient_s))
     forward_s = min(t[0] for t in times)
-    gradient_s = min(t[1] for t in times)
+    taped_s = min(t[1] for t in times)
+    gradient_s = min(t[2] for t in times)
     # Peak device memory of a gradient: free memory sampled while it runs.
     free_min = [torch.cuda.mem_get_info(local)[0]]
     stop = threading.Event()
@@ -383,7 +386,10 @@ def run_adjoint(args, world: int, rank: int, local: int) -> None:
         cd64.append(abs(p64 - measured) / abs(measured))
         cd32.append(abs(p32 - measured) / abs(measured))
     rel = lambda a, b: float(np.max(np.abs(a - b)) / np.max(np.abs(b)))  # noqa: E731
-    result = fit.adam(problem, iterations=args.adam_iterations, rate=0.03)
+    result = fit.adam(problem, iterations=args.adam_iterations, rate=0.05)
+    t0 = time.perf_counter()
+    quasi = fit.lbfgs(problem, iterations=args.adam_iterations)
+    quasi["seconds"] = round(time.perf_counter() - t0, 2)
     line = {
         "metric": METRIC,
         "value": round(f.built.air_cells * len(f.signal) / forward_s / 1e9, 4),
@@ -397,9 +403,11 @@ def run_adjoint(args, world: int, rank: int, local: int) -> None:
         "dtype": "f32",
         "data": "synthetic",
         "config": {"workload": "adjoint_fit", **problem.description},
-        "adjoint_over_forward": round((forward_s + gradient_s) / forward_s, 3),
+        "adjoint_over_forward": round((taped_s + gradient_s) / forward_s, 3),
         "forward_s": round(forward_s, 4),
+        "taped_forward_s": round(taped_s, 4),
         "gradient_s": round(gradient_s, 4),
+        "adjoint_over_forward_means": "(the forward run that keeps its checkpoints + the gradient: recomputation and the reverse steps) / a plain forward run, host buffers both",
         "gradient_vs_central_differences": {
             "max_rel": max(cd64), "h": 1e-4, "precision": "fp64",
             "difference": "L(c + d) - L(c - d) over 2, d the coefficients' change along each parameter, exact float32 steps",
@@ -408,6 +416,7 @@ def run_adjoint(args, world: int, rank: int, local: int) -> None:
         "fp32_gradient_vs_fp64": {"max_rel": rel(g32, g64)},
         "peak_device_bytes": int(total - free_min[0]),
         "adam": {k: result[k] for k in ("iterations", "converged", "worst_relative_error")},
+        "lbfgs": {k: quasi[k] for k in ("iterations", "evaluations", "converged", "worst_relative_error", "seconds")},
     }
     if rank == 0:
         print(json.dumps(line), flush=True)

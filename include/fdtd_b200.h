@@ -172,6 +172,17 @@ int fdtd_gradient(fdtd_solver *solver, const float *signal, uint64_t steps, cons
                   uint64_t segment, double *grad_coef_b, double *grad_coef_inv, double *grad_now,
                   double *grad_before, double *grad_gain);
 
+/*
+ * The tape of a run for a gradient that follows (no counterpart in the reference). With `segment`
+ * > 0, each fdtd_run that starts from rest keeps on the device the state at every multiple of
+ * `segment` steps before its end, and a copy of its drive; a following fdtd_gradient of the same
+ * drive and steps with the same `segment` starts from those states instead of running the forward
+ * pass again, so that a fit's forward run and its gradient together step the grid twice rather
+ * than three times. The result is the same to the bit. 0 turns the tape off. The states take
+ * (steps / segment - 1) x (2 levels + 2 branch-velocity sets) of device memory, kept by the handle.
+ */
+int fdtd_set_tape(fdtd_solver *solver, uint64_t segment);
+
 /* Bytes of the static device pool of fdtd_gradient_noalloc: 16 MiB, held on every device the
    library runs on until the process exits. */
 #define FDTD_GRADIENT_STATIC_BYTES (16ull << 20)

@@ -156,3 +156,26 @@ def test_the_autograd_function_gives_the_material_gradient():
     expected_loss, expected = f.loss_and_gradient(params, "fp64")
     assert abs(float(loss) - expected_loss) <= 1e-12 * expected_loss
     np.testing.assert_allclose(ours, expected, rtol=1e-9, atol=1e-12 * np.abs(expected).max())
+
+
+def test_a_taped_run_gives_the_gradient_to_the_bit():
+    # fdtd_set_tape: the run keeps its checkpoints and the gradient starts from them; a gradient of
+    # another drive does not use them.
+    layout, signal, _ = load_golden("resonant7")
+    signal = np.ascontiguousarray(signal[:300])
+    y = B200WaveSolver(layout, precision="fp64").run(signal)
+    dloss = 2.0 * (y - 0.5 * y)
+    plain = B200WaveSolver(layout, precision="fp64").gradient(signal, dloss, segment=37)
+    taped = B200WaveSolver(layout, precision="fp64")
+    taped.set_tape(37)
+    np.testing.assert_array_equal(taped.run(signal), y)
+    taped.reset()
+    got = taped.gradient(signal, dloss, segment=37)
+    for key in plain:
+        np.testing.assert_array_equal(got[key], plain[key], err_msg=key)
+    other = signal * 0.5
+    y2 = B200WaveSolver(layout, precision="fp64").run(other)
+    expected = B200WaveSolver(layout, precision="fp64").gradient(other, 2.0 * y2, segment=37)
+    got = taped.gradient(other, 2.0 * y2, segment=37)
+    for key in expected:
+        np.testing.assert_array_equal(got[key], expected[key], err_msg=key)
