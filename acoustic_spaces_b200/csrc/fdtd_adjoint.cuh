@@ -14,8 +14,8 @@
 //   lam_n[i] = sum over the cells r reading u_i of G_{r,i} L~_{n+1}[r]  -  (ci cb L~_{n+2}[i] + sum_j gain_j om_{n+2}[j])
 //   om_n[j]  = -ci W_j now_j L~_{n+1}[i] + now_j om_{n+1}[j] + ci W_j before_j L~_{n+2}[i] + (1 - before_j) om_{n+2}[j]
 // (an interior cell's L~ is its lam). Interior cells take the forward bulk sweep on the adjoint
-// levels (all their readers being interior to within the rows next to special cells, which a
-// correction list fixes), special rows a gather over their readers (a transposed list).
+// levels (their readers are interior and axial), except the cells that special rows read, which
+// correct_kernel forms whole; special rows a gather over their readers (a transposed list).
 // The gradient of step n, with U = L~_{n+1}[i] and own~_j = om_{n+1}[j] - W_j ci U:
 //   dL/dci += U x,  dL/dcb += -U ci u_{n-1}[i],  dL/dnow_j += own~_j w_n[j],
 //   dL/dbefore_j += -own~_j w_{n-1}[j],  dL/dgain_j += om_{n+1}[j] (u_{n+1}[i] - u_{n-1}[i])
@@ -39,19 +39,21 @@ struct AdjointTables {
     const uint32_t *reader_start, *reader_index;
     const uint8_t *reader_kind;
     const double *reader_coef;
-    // Interior cells next to special rows: corrected_start .. per cell, entries (special row, its
-    // coefficient on the cell); the bulk sweep took axial * lam of those rows' cells instead.
+    // Interior cells that special rows read: corrected_start .. per cell, entries (special row,
+    // its coefficient on the cell), and which of the cell's six axial neighbours are special rows
+    // (bit d, in the order of the stencil's directions). The adjoint sweep leaves these cells to
+    // correct_kernel.
     uint32_t corrected;
     const uint32_t *corrected_cell, *corrected_start, *corrected_row;
+    const uint8_t *corrected_mask;
     const double *corrected_coef;
-    float axial;
-    // Probes: CSR of pitched cells and weights; and by the cells they read, each cell's
-    // (probe, weight) terms: read_start[c] .. read_start[c + 1].
-    uint32_t probes;
-    const uint32_t *probe_start, *probe_cells;
-    const double *probe_weights;
-    uint32_t read_cells;
-    const uint32_t *read_cell, *read_start, *read_probe;
+    float axial, centre;
+    int32_t offset[6];
+    // The probes' terms dL/dy_p x weight on the cells they read, by cell: a special row's at
+    // special_read_start[k] .. [k + 1], a corrected cell's at corrected_read_start[c] .. [c + 1], of
+    // (read_probe, read_weight). (Probes read no other cells that the adjoint carries: a solid
+    // cell's pressure never changes.)
+    const uint32_t *special_read_start, *corrected_read_start, *read_probe;
     const double *read_weight;
 };
 
@@ -65,41 +67,52 @@ __global__ void __launch_bounds__(kBlock) record_kernel(const AdjointTables t, c
     if (k < t.states) traj_w[k] = w[k];
 }
 
-// L~ of every special row from the adjoint level (lam, om).
-template <typename T>
-__global__ void __launch_bounds__(kBlock) tilde_kernel(const AdjointTables t, const T *lam, const T *om, T *tilde) {
-    const uint32_t k = blockIdx.x * kBlock + threadIdx.x;
-    if (k >= t.specials) return;
-    T value = lam[t.special[k]];
-    for (uint32_t j = t.state_start[k], e = t.state_start[k + 1]; j < e; ++j) value += (T)t.state_gain[j] * om[j];
-    tilde[k] = value;
+// The probes' terms of step n at a cell: sum over (probe, weight) of weight x dL/dy_p^n, in double,
+// in a fixed order.
+__device__ __forceinline__ double probe_terms(const AdjointTables &t, uint32_t begin, uint32_t end, const double *dloss,
+                                              uint64_t stride, uint64_t step) {
+    double sum = 0.0;
+    for (uint32_t e = begin; e < end; ++e) sum += t.read_weight[e] * dloss[(uint64_t)t.read_probe[e] * stride + step];
+    return sum;
 }
 
-// Interior cells next to special rows: the bulk sweep added axial * lam[cell of row r]; the
-// transposed operator has G_{r, cell} L~[r] there.
+// Interior cells that special rows read, or that probes read, whole: the transposed stencil of
+// their interior (and solid) axial neighbours, as the sweep forms it, plus each reading row's
+// coefficient times its L~, minus the level two steps on (lam_out holds it on entry), plus the
+// probes' terms of step n. The sweep leaves these cells alone.
 template <typename T>
 __global__ void __launch_bounds__(kBlock) correct_kernel(const AdjointTables t, const T *lam_next, const T *tilde,
-                                                         T *lam_out) {
+                                                         T *lam_out, const double *dloss, uint64_t stride,
+                                                         uint64_t step) {
     const uint32_t c = blockIdx.x * kBlock + threadIdx.x;
     if (c >= t.corrected) return;
     const uint32_t cell = t.corrected_cell[c];
-    T delta = 0;
-    for (uint32_t e = t.corrected_start[c], end = t.corrected_start[c + 1]; e < end; ++e) {
-        const uint32_t r = t.corrected_row[e];
-        delta += (T)t.corrected_coef[e] * tilde[r] - (T)t.axial * lam_next[t.special[r]];
-    }
-    lam_out[cell] += delta;
+    const uint32_t special = t.corrected_mask[c];
+    T sum = 0;
+#pragma unroll
+    for (int d = 0; d < 6; ++d)
+        if (!(special & (1u << d))) sum += lam_next[(uint32_t)((int64_t)cell + t.offset[d])];
+    T value = (T)t.centre * lam_next[cell] + (T)t.axial * sum - lam_out[cell];
+    for (uint32_t e = t.corrected_start[c], end = t.corrected_start[c + 1]; e < end; ++e)
+        value += (T)t.corrected_coef[e] * tilde[t.corrected_row[e]];
+    const double probed = probe_terms(t, t.corrected_read_start[c], t.corrected_read_start[c + 1], dloss, stride, step);
+    if (probed != 0.0) value += (T)probed;
+    lam_out[cell] = value;
 }
 
-// Special rows: the adjoint of their cells and branch states, and the gradient of step n.
-// lam_next/om_next: level n+1 (complete), lam_out/om_out: hold level n+2 on entry (own row only)
-// and level n on exit; traj levels of u_{n-1}, u_n... at l0 = n - s0, then l0 + 1, l0 + 2.
+// Special rows: the adjoint of their cells (with the probes' terms of step n) and branch states,
+// their L~ of level n for the next reverse step (tilde_out), and the gradient of step n.
+// lam_next/om_next: level n+1 (complete), tilde its L~; lam_out/om_out: hold level n+2 on entry
+// (own row only) and level n on exit; traj levels of u_{n-1}, u_n... at l0 = n - s0, then l0 + 1,
+// l0 + 2.
 template <typename T>
 __global__ void __launch_bounds__(kBlock) special_adjoint_kernel(const AdjointTables t, const T *lam_next,
                                                                  const T *om_next, const T *tilde, T *lam_out,
                                                                  T *om_out, const T *traj_u, const T *traj_w,
                                                                  uint32_t level, double *g_ci, double *g_cb,
-                                                                 double *g_now, double *g_before, double *g_gain) {
+                                                                 double *g_now, double *g_before, double *g_gain,
+                                                                 T *tilde_out, const double *dloss, uint64_t stride,
+                                                                 uint64_t step) {
     const uint32_t k = blockIdx.x * kBlock + threadIdx.x;
     if (k >= t.specials) return;
     const uint32_t i = t.special[k];
@@ -118,7 +131,11 @@ __global__ void __launch_bounds__(kBlock) special_adjoint_kernel(const AdjointTa
         gain_om2 += term;
     }
     const T U = tilde[k];
-    lam_out[i] = gathered - (ci * cb * tilde2 + gain_om2);
+    T lam = gathered - (ci * cb * tilde2 + gain_om2);
+    const double probed = probe_terms(t, t.special_read_start[k], t.special_read_start[k + 1], dloss, stride, step);
+    if (probed != 0.0) lam += (T)probed;
+    lam_out[i] = lam;
+    T next_tilde = lam;
     // The gradient of step n (forward values: u_{n-1}, u_n, u_{n+1} at levels l, l+1, l+2).
     const T u_prev = traj_u[(uint64_t)level * t.specials + k];
     const T u_next = traj_u[(uint64_t)(level + 2) * t.specials + k];
@@ -127,7 +144,9 @@ __global__ void __launch_bounds__(kBlock) special_adjoint_kernel(const AdjointTa
     for (uint32_t j = s0; j < s1; ++j) {
         const T W = (T)t.state_weight[j], now = (T)t.state_now[j], before = (T)t.state_before[j];
         const T om1 = om_next[j], om2 = om_out[j];
-        om_out[j] = -ci * W * now * U + now * om1 + ci * W * before * tilde2 + ((T)1 - before) * om2;
+        const T om = -ci * W * now * U + now * om1 + ci * W * before * tilde2 + ((T)1 - before) * om2;
+        om_out[j] = om;
+        next_tilde += (T)t.state_gain[j] * om;
         const double own_bar = (double)om1 - (double)W * (double)ci * (double)U;
         const double w_n = (double)traj_w[(uint64_t)(level + 1) * t.states + j];
         const double w_prev = (double)traj_w[(uint64_t)level * t.states + j];
@@ -135,20 +154,7 @@ __global__ void __launch_bounds__(kBlock) special_adjoint_kernel(const AdjointTa
         g_before[j] += -own_bar * w_prev;
         g_gain[j] += (double)om1 * ((double)u_next - (double)u_prev);
     }
-}
-
-// The probes' terms of level n: lam_n[cell] += sum over the probes reading the cell of weight *
-// dL/dy_p^n, a thread per cell that probes read, its terms summed in double in a fixed order (so
-// that the result does not depend on the threads' timing).
-template <typename T>
-__global__ void __launch_bounds__(kBlock) probe_adjoint_kernel(const AdjointTables t, const double *dloss, uint64_t stride,
-                                                               uint64_t step, T *lam_out) {
-    const uint32_t c = blockIdx.x * kBlock + threadIdx.x;
-    if (c >= t.read_cells) return;
-    double sum = 0.0;
-    for (uint32_t e = t.read_start[c], end = t.read_start[c + 1]; e < end; ++e)
-        sum += t.read_weight[e] * dloss[(uint64_t)t.read_probe[e] * stride + step];
-    if (sum != 0.0) lam_out[t.read_cell[c]] += (T)sum;
+    tilde_out[k] = next_tilde;
 }
 
 }  // namespace fdtd

@@ -60,9 +60,10 @@ using EncodeTiled = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t,
 // and of the branch velocities, each row's L~, and the tensor maps of the sweep over the levels.
 struct AdjointState {
     AdjointTables t{};
+    CUtensorMap map_t;  // the cell types of the adjoint sweep: the cells special rows read left out
     void *lam[2] = {nullptr, nullptr};
     void *om[2] = {nullptr, nullptr};
-    void *tilde = nullptr;
+    void *tilde[2] = {nullptr, nullptr};  // L~ of the level at hand, and of the next (alternating)
     CUtensorMap lam_b[2], lam_a[2];
 };
 
@@ -118,6 +119,18 @@ struct fdtd_solver {
     // The adjoint (fdtd_gradient), set up on first use and kept.
     bool adjoint_ready = false;
     AdjointState adjoint;
+    std::vector<int32_t> adjoint_reader_row;  // of the kept adjoint (fdtd_set_coefficients)
+    std::vector<uint32_t> adjoint_corrected_row;
+    std::vector<double> adjoint_reader_base, adjoint_corrected_base;
+    std::vector<int32_t> state_branch;  // each branch state's branch
+    uint64_t branches = 0;
+    // fdtd_gradient's device workspace, kept and handed out again in the same order while the
+    // sizes asked for stay the same (a fit's iterations then allocate nothing).
+    struct Block {
+        void *p;
+        size_t bytes;
+    };
+    std::vector<Block> work;
     // While the gradient recomputes a segment: the special rows' values after each step of a
     // dispatch, recorded as level k + 2 of the trajectory after the dispatch's step k.
     const AdjointTables *record_tables = nullptr;
@@ -698,6 +711,8 @@ int build(fdtd_solver *s, const fdtd_layout *L) {
         // Each state's branch coefficients gathered per state, as run() gathers them
         // (fdtd.hpp:797-805).
         const uint64_t S = L->state_count;
+        s->state_branch.assign(L->state_branch, L->state_branch + S);
+        s->branches = L->branch_count;
         std::vector<float> now(S), before(S), gain(S);
         for (uint64_t j = 0; j < S; ++j) {
             const int32_t br = L->state_branch[j];
@@ -777,6 +792,7 @@ void release(fdtd_solver *s) {
         if (stream) cudaStreamSynchronize(stream);
     for (cudaGraphExec_t g : s->graph)
         if (g) cudaGraphExecDestroy(g);
+    for (const auto &b : s->work) cudaFree(b.p);
     for (cudaEvent_t e : s->timing_events) cudaEventDestroy(e);
     for (void *p : s->allocations) cudaFree(p);
     if (s->stage_signal) cudaFreeHost(s->stage_signal);
@@ -803,8 +819,13 @@ int download(fdtd_solver *s, const V *device, size_t count, std::vector<V> &host
 // and the interior cells next to special rows with their corrections.
 struct AdjointLists {
     std::vector<uint32_t> reader_start, reader_index, cells, starts, rows;
-    std::vector<uint32_t> read_cell, read_start, read_probe;  // the probes' terms by cell
+    std::vector<uint8_t> masks, types;  // each corrected cell's special axial neighbours; the sweep's types
+    std::vector<uint32_t> special_read_start, corrected_read_start, read_probe;  // the probes' terms by cell
     std::vector<double> read_weight;
+    // Each reader's and correction's coefficient as coef_inv[row] x base (row -1: the base alone),
+    // so that new coefficients (fdtd_set_coefficients) give new products without a new set-up.
+    std::vector<int32_t> reader_row;
+    std::vector<double> reader_base, corrected_base;
     std::vector<uint8_t> reader_kind;
     std::vector<double> reader_coef, coefs;
 };
@@ -833,25 +854,32 @@ int adjoint_lists(fdtd_solver *s, AdjointLists &out) {
     for (uint64_t k = 0; k < K; ++k) row_of[special[k]] = (uint32_t)k;
     // Readers of each special row's cell: the row itself, its interior neighbours, the special
     // rows linking to it; and the interior cells special rows link to.
-    std::vector<std::vector<std::pair<uint64_t, double>>> readers(K);  // (index | kind << 63, coef)
-    std::unordered_map<uint32_t, std::vector<std::pair<uint32_t, double>>> corrected;
+    struct Reader {
+        uint64_t index;  // | kind << 63
+        int32_t row;     // the reading row whose coef_inv multiplies `base`, or -1
+        double base;
+    };
+    std::vector<std::vector<Reader>> readers(K);
+    std::unordered_map<uint32_t, std::vector<std::pair<uint32_t, double>>> corrected;  // (row, base)
     const uint64_t kind_bit = 1ull << 63;
     for (uint64_t k = 0; k < K; ++k) {
         const uint32_t i = special[k];
-        readers[k].push_back({kind_bit | k, (double)coef_inv[k] * (double)coef_a[k]});
+        readers[k].push_back({kind_bit | k, (int32_t)k, (double)coef_a[k]});
         for (int d = 0; d < 6; ++d) {
             const uint32_t j = (uint32_t)((int64_t)i + g.offset[d]);
-            if (types[j] == kInterior) readers[k].push_back({j, axial});
+            if (types[j] == kInterior) {
+                readers[k].push_back({j, -1, axial});
+                corrected[j];  // an interior cell next to a special row: formed by correct_kernel
+            }
         }
         for (uint32_t l = 0; l < count[k]; ++l) {
             const uint64_t at = (uint64_t)l * K + k;
             const uint32_t j = (uint32_t)((int64_t)i + g.offset[direction[at]]);
-            const double coef = (double)coef_inv[k] * (double)weight[at];
             auto it = row_of.find(j);
             if (it != row_of.end()) {
-                readers[it->second].push_back({kind_bit | k, coef});
+                readers[it->second].push_back({kind_bit | k, (int32_t)k, (double)weight[at]});
             } else if (types[j] == kInterior) {
-                corrected[j].push_back({(uint32_t)k, coef});
+                corrected[j].push_back({(uint32_t)k, (double)weight[at]});
             } else {
                 return fail(s, FDTD_EINVAL, "a special row links to a cell that is neither interior nor special");
             }
@@ -859,40 +887,53 @@ int adjoint_lists(fdtd_solver *s, AdjointLists &out) {
     }
     out.reader_start.assign(K + 1, 0);
     for (uint64_t k = 0; k < K; ++k) {
-        for (const auto &[idx, coef] : readers[k]) {
-            out.reader_index.push_back((uint32_t)(idx & ~kind_bit));
-            out.reader_kind.push_back((idx & kind_bit) ? 1 : 0);
-            out.reader_coef.push_back(coef);
+        for (const Reader &r : readers[k]) {
+            out.reader_index.push_back((uint32_t)(r.index & ~kind_bit));
+            out.reader_kind.push_back((r.index & kind_bit) ? 1 : 0);
+            out.reader_row.push_back(r.row);
+            out.reader_base.push_back(r.base);
+            out.reader_coef.push_back(r.row >= 0 ? (double)coef_inv[r.row] * r.base : r.base);
         }
         out.reader_start[k + 1] = (uint32_t)out.reader_index.size();
     }
-    // The probes' terms grouped by cell, each cell's in the order of the probes and their cells.
+    // The probes' terms grouped by cell, each cell's in the order of the probes and their cells;
+    // the interior cells that probes read are formed whole by correct_kernel too.
     std::vector<uint32_t> probe_start, probe_cells;
     std::vector<double> probe_weights;
     if ((rc = download(s, g.probe_start, (size_t)g.probes + 1, probe_start))) return rc;
     if ((rc = download(s, g.probe_cells, (size_t)probe_start[g.probes], probe_cells))) return rc;
     if ((rc = download(s, g.probe_weights, (size_t)probe_start[g.probes], probe_weights))) return rc;
-    std::vector<std::pair<uint32_t, uint32_t>> by_cell;  // (cell, entry)
+    std::unordered_map<uint32_t, std::vector<std::pair<uint32_t, double>>> probed;  // cell: (probe, weight)
     for (uint32_t p = 0; p < g.probes; ++p)
-        for (uint32_t e = probe_start[p]; e < probe_start[p + 1]; ++e) by_cell.push_back({probe_cells[e], e});
-    std::stable_sort(by_cell.begin(), by_cell.end(),
-                     [](const auto &a, const auto &b) { return a.first < b.first; });
-    std::vector<uint32_t> owner(probe_start.empty() ? 0 : probe_start[g.probes]);
-    for (uint32_t p = 0; p < g.probes; ++p)
-        for (uint32_t e = probe_start[p]; e < probe_start[p + 1]; ++e) owner[e] = p;
-    for (size_t i = 0; i < by_cell.size(); ++i) {
-        if (i == 0 || by_cell[i].first != by_cell[i - 1].first) {
-            out.read_cell.push_back(by_cell[i].first);
-            out.read_start.push_back((uint32_t)out.read_probe.size());
+        for (uint32_t e = probe_start[p]; e < probe_start[p + 1]; ++e) {
+            const uint32_t cell = probe_cells[e];
+            if (row_of.count(cell) || types[cell] == kInterior) probed[cell].push_back({p, probe_weights[e]});
+            if (types[cell] == kInterior) corrected[cell];
         }
-        out.read_probe.push_back(owner[by_cell[i].second]);
-        out.read_weight.push_back(probe_weights[by_cell[i].second]);
-    }
-    out.read_start.push_back((uint32_t)out.read_probe.size());
+    auto read_terms = [&](uint32_t cell) {
+        auto it = probed.find(cell);
+        if (it != probed.end())
+            for (const auto &[p, w] : it->second) out.read_probe.push_back(p), out.read_weight.push_back(w);
+        return (uint32_t)out.read_probe.size();
+    };
+    out.special_read_start.assign(1, 0);
+    for (uint64_t k = 0; k < K; ++k) out.special_read_start.push_back(read_terms(special[k]));
+    out.corrected_read_start.assign(1, out.special_read_start.back());
     out.starts.assign(1, 0);
+    out.types = types;
     for (auto &[cell, list] : corrected) {
         out.cells.push_back(cell);
-        for (const auto &[r, c] : list) out.rows.push_back(r), out.coefs.push_back(c);
+        out.corrected_read_start.push_back(read_terms(cell));
+        out.types[cell] = kSpecial;  // left to correct_kernel
+        uint8_t mask = 0;
+        for (int d = 0; d < 6; ++d)
+            if (row_of.count((uint32_t)((int64_t)cell + g.offset[d]))) mask |= (uint8_t)(1u << d);
+        out.masks.push_back(mask);
+        for (const auto &[r, base] : list) {
+            out.rows.push_back(r);
+            out.corrected_base.push_back(base);
+            out.coefs.push_back((double)coef_inv[r] * base);
+        }
         out.starts.push_back((uint32_t)out.rows.size());
     }
     return FDTD_OK;
@@ -924,7 +965,8 @@ int place_adjoint(fdtd_solver *s, const AdjointLists &l, Pool &pool, AdjointStat
     t.state_weight = g.state_weight, t.state_now = g.state_now, t.state_before = g.state_before, t.state_gain = g.state_gain;
     t.coef_b = g.coef_b, t.coef_inv = g.coef_inv;
     t.axial = s->bulk.axial;
-    t.probes = g.probes, t.probe_start = g.probe_start, t.probe_cells = g.probe_cells, t.probe_weights = g.probe_weights;
+    t.centre = s->bulk.centre;
+    for (int d = 0; d < 6; ++d) t.offset[d] = g.offset[d];
     t.corrected = (uint32_t)l.cells.size();
     int rc;
     if ((rc = place(s, pool, l.reader_start, &t.reader_start))) return rc;
@@ -934,23 +976,29 @@ int place_adjoint(fdtd_solver *s, const AdjointLists &l, Pool &pool, AdjointStat
     if ((rc = place(s, pool, l.cells, &t.corrected_cell))) return rc;
     if ((rc = place(s, pool, l.starts, &t.corrected_start))) return rc;
     if ((rc = place(s, pool, l.rows, &t.corrected_row))) return rc;
+    if ((rc = place(s, pool, l.masks, &t.corrected_mask))) return rc;
+    const uint8_t *sweep_types;
+    if ((rc = place(s, pool, l.types, &sweep_types))) return rc;
     if ((rc = place(s, pool, l.coefs, &t.corrected_coef))) return rc;
-    if ((rc = place(s, pool, l.read_cell, &t.read_cell))) return rc;
-    if ((rc = place(s, pool, l.read_start, &t.read_start))) return rc;
+    if ((rc = place(s, pool, l.special_read_start, &t.special_read_start))) return rc;
+    if ((rc = place(s, pool, l.corrected_read_start, &t.corrected_read_start))) return rc;
     if ((rc = place(s, pool, l.read_probe, &t.read_probe))) return rc;
     if ((rc = place(s, pool, l.read_weight, &t.read_weight))) return rc;
-    t.read_cells = (uint32_t)l.read_cell.size();
     for (int k = 0; k < 2; ++k) {
         if ((rc = pool.take(e * s->n_device, &a.lam[k], true))) return rc;
         if ((rc = pool.take(e * S, &a.om[k], true))) return rc;
     }
-    if ((rc = pool.take(e * K, &a.tilde, true))) return rc;
+    for (int k = 0; k < 2; ++k)
+        if ((rc = pool.take(e * K, &a.tilde[k], true))) return rc;
     if (s->bulk_blocks) {
         const CUtensorMapDataType ft = s->precision == FDTD_FP64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
         for (int k = 0; k < 2; ++k) {
             if ((rc = tensor_map(s, &a.lam_b[k], a.lam[k], ft, (uint32_t)e, kBX, kBY))) return rc;
             if ((rc = tensor_map(s, &a.lam_a[k], a.lam[k], ft, (uint32_t)e, kTX, kTY))) return rc;
         }
+        if ((rc = tensor_map(s, &a.map_t, const_cast<uint8_t *>(sweep_types), CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, kTX,
+                             kTY)))
+            return rc;
     }
     return FDTD_OK;
 }
@@ -979,27 +1027,36 @@ int set_up_adjoint(fdtd_solver *s) {
     Owned owned{s};
     if ((rc = place_adjoint(s, lists, owned, s->adjoint))) return rc;
     CUDA_TRY(s, cudaDeviceSynchronize());  // the clears (default stream) and copies (handle's stream)
+    s->adjoint_reader_row = std::move(lists.reader_row);
+    s->adjoint_reader_base = std::move(lists.reader_base);
+    s->adjoint_corrected_row = std::move(lists.rows);
+    s->adjoint_corrected_base = std::move(lists.corrected_base);
     s->adjoint_ready = true;
     return FDTD_OK;
 }
 
-// Device scratch of one fdtd_gradient call, freed at its end (the handle's stream has ended by
-// then). Each block is cleared on the handle's stream, in order with the gradient's own work.
-struct Scratch {
+// fdtd_gradient's workspace on the handle: the blocks of the last call handed out again in order
+// while the sizes match, each cleared on the handle's stream; from the first that does not, new
+// ones. (A graph of a segment's steps over these blocks, captured once and replayed, measured 8 %
+// slower than launching them on the 2.6M-cell fit room: the steps are not launch-bound there.)
+struct Kept {
     fdtd_solver *s;
-    std::vector<void *> blocks;
-    explicit Scratch(fdtd_solver *solver) : s(solver) {}
-    ~Scratch() {
-        cudaStreamSynchronize(s->stream);
-        for (void *p : blocks) cudaFree(p);
-    }
+    size_t next = 0;
     int take(size_t bytes, void **out) {
         *out = nullptr;
-        void *p = nullptr;
-        CUDA_TRY(s, cudaMalloc(&p, bytes ? bytes : 16));
-        blocks.push_back(p);
-        CUDA_TRY(s, cudaMemsetAsync(p, 0, bytes ? bytes : 16, s->stream));
-        *out = p;
+        const size_t size = bytes ? bytes : 16;
+        if (next < s->work.size() && s->work[next].bytes != size) {
+            CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+            for (size_t i = next; i < s->work.size(); ++i) cudaFree(s->work[i].p);
+            s->work.resize(next);
+        }
+        if (next == s->work.size()) {
+            void *p = nullptr;
+            CUDA_TRY(s, cudaMalloc(&p, size));
+            s->work.push_back({p, size});
+        }
+        *out = s->work[next++].p;
+        CUDA_TRY(s, cudaMemsetAsync(*out, 0, size, s->stream));
         return FDTD_OK;
     }
 };
@@ -1078,18 +1135,17 @@ int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float
         checkpoints.push_back(static_cast<char *>(p));
         if ((rc = save(checkpoints.back())) != FDTD_OK) return rc;
     }
-    // The adjoint levels beyond the end are at rest; the sums start at 0.
+    // The adjoint levels beyond the end, and their L~, are at rest; the sums start at 0.
     for (int k = 0; k < 2; ++k) {
         CUDA_TRY(s, cudaMemsetAsync(adj.lam[k], 0, level_bytes, s->stream));
         if (S) CUDA_TRY(s, cudaMemsetAsync(adj.om[k], 0, state_bytes, s->stream));
+        if (K) CUDA_TRY(s, cudaMemsetAsync(adj.tilde[k], 0, sizeof(T) * K, s->stream));
     }
     const AdjointTables &t = adj.t;
     const uint32_t row_blocks = (uint32_t)((std::max<uint64_t>(std::max<uint64_t>(K, S), 1) + kBlock - 1) / kBlock);
     const uint32_t special_blocks = (uint32_t)((K + kBlock - 1) / kBlock);
     const uint32_t corrected_blocks = (uint32_t)((t.corrected + kBlock - 1) / kBlock);
-    const uint32_t probe_blocks = (uint32_t)((t.read_cells + kBlock - 1) / kBlock);
     const uint32_t smem = Stage<T, false>::smem;
-    T *tilde = static_cast<T *>(adj.tilde);
     int x = 0;  // lam[x], om[x]: level n+1; lam[1-x], om[1-x]: level n+2, then level n
     // A segment's recomputation (the dispatch of its steps, recording the special rows), and its
     // reverse steps.
@@ -1104,26 +1160,31 @@ int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float
         for (uint64_t m = count; m-- > 0;) {
             T *lam_next = static_cast<T *>(adj.lam[xx]), *lam_out = static_cast<T *>(adj.lam[1 - xx]);
             T *om_next = static_cast<T *>(adj.om[xx]), *om_out = static_cast<T *>(adj.om[1 - xx]);
-            // L~ of level n+1; then the interior (the sweep and its corrections) on the handle's
-            // stream beside the special rows on the side stream (they write disjoint cells); then
-            // the probes' terms, which may land on either.
-            if (special_blocks) tilde_kernel<T><<<special_blocks, kBlock, 0, s->stream>>>(t, lam_next, om_next, tilde);
+            // On three streams, the sweep of the interior, the cells that special rows or probes
+            // read (correct_kernel) and the special rows (with their L~ of level n for the next
+            // step), which write disjoint cells; each step starts when all three have ended.
+            const T *tilde = static_cast<const T *>(adj.tilde[xx]);
+            T *tilde_out = static_cast<T *>(adj.tilde[1 - xx]);
             CUDA_TRY(s, cudaEventRecord(s->joined[0], s->stream));
             CUDA_TRY(s, cudaStreamWaitEvent(s->side, s->joined[0], 0));
+            CUDA_TRY(s, cudaStreamWaitEvent(s->layer_stream, s->joined[0], 0));
             if (special_blocks)
                 special_adjoint_kernel<T><<<special_blocks, kBlock, 0, s->side>>>(
-                    t, lam_next, om_next, tilde, lam_out, om_out, traj_u, traj_w, (uint32_t)m, g[1], g[0], g[2], g[3], g[4]);
+                    t, lam_next, om_next, tilde, lam_out, om_out, traj_u, traj_w, (uint32_t)m, g[1], g[0], g[2], g[3], g[4],
+                    tilde_out, seg_dloss, segment, m);
+            if (corrected_blocks)
+                correct_kernel<T><<<corrected_blocks, kBlock, 0, s->layer_stream>>>(t, lam_next, tilde, lam_out, seg_dloss,
+                                                                                    segment, m);
             CUDA_TRY(s, cudaEventRecord(s->joined[1], s->side));
+            CUDA_TRY(s, cudaEventRecord(s->joined[2], s->layer_stream));
             if (s->bulk_blocks) {
                 BulkArgs args = s->bulk;
                 args.a = lam_out;
                 bulk_kernel<T, false, false><<<s->bulk_blocks, kBlock, smem, s->stream>>>(adj.lam_b[xx], adj.lam_a[1 - xx],
-                                                                                        s->map_t, s->map_s, args);
+                                                                                        adj.map_t, s->map_s, args);
             }
-            if (corrected_blocks) correct_kernel<T><<<corrected_blocks, kBlock, 0, s->stream>>>(t, lam_next, tilde, lam_out);
             CUDA_TRY(s, cudaStreamWaitEvent(s->stream, s->joined[1], 0));
-            if (probe_blocks)
-                probe_adjoint_kernel<T><<<probe_blocks, kBlock, 0, s->stream>>>(t, seg_dloss, segment, m, lam_out);
+            CUDA_TRY(s, cudaStreamWaitEvent(s->stream, s->joined[2], 0));
             xx = 1 - xx;
         }
         CUDA_TRY(s, cudaGetLastError());
@@ -1216,9 +1277,10 @@ size_t pool_bytes(const fdtd_solver *s, const AdjointLists &l, uint64_t steps, u
     auto list = [&](size_t count, size_t unit) { total += count ? pool_round(count * unit) : 0; };
     list(l.reader_start.size(), 4), list(l.reader_index.size(), 4), list(l.reader_kind.size(), 1);
     list(l.reader_coef.size(), 8), list(l.cells.size(), 4), list(l.starts.size(), 4), list(l.rows.size(), 4);
-    list(l.coefs.size(), 8), list(l.read_cell.size(), 4), list(l.read_start.size(), 4);
+    list(l.coefs.size(), 8), list(l.special_read_start.size(), 4), list(l.corrected_read_start.size(), 4);
+    list(l.masks.size(), 1), list(l.types.size(), 1);
     list(l.read_probe.size(), 4), list(l.read_weight.size(), 8);
-    total += 2 * (pool_round(e * n) + pool_round(e * S)) + pool_round(e * K);
+    total += 2 * (pool_round(e * n) + pool_round(e * S)) + 2 * pool_round(e * K);
     if (segment == 0 || segment > steps) segment = steps;
     const uint64_t segments = (steps + segment - 1) / segment;
     total += pool_round(4 * steps) + pool_round(8 * P * steps) + pool_round(e * K * (segment + 2)) +
@@ -1472,6 +1534,44 @@ int fdtd_gradient_noalloc(fdtd_solver *s, const float *signal, uint64_t steps, c
                                      : gradient<float>(s, adj, pool, signal, steps, dloss_dy, segment, grads);
 }
 
+int fdtd_set_coefficients(fdtd_solver *s, const float *coef_b, const float *coef_inv, const float *branch_now,
+                          const float *branch_before, const float *branch_gain) {
+    if (!s) return set_global(FDTD_EINVAL, "no solver");
+    DeviceGuard guard(s->device);
+    const uint64_t K = s->specials, S = s->states;
+    for (cudaStream_t stream : {s->stream, s->side, s->layer_stream}) CUDA_TRY(s, cudaStreamSynchronize(stream));
+    Tables &g = s->tables;
+    if (coef_b && K) CUDA_TRY(s, cudaMemcpy(const_cast<float *>(g.coef_b), coef_b, 4 * K, cudaMemcpyHostToDevice));
+    if (coef_inv && K) CUDA_TRY(s, cudaMemcpy(const_cast<float *>(g.coef_inv), coef_inv, 4 * K, cudaMemcpyHostToDevice));
+    const float *branch[3] = {branch_now, branch_before, branch_gain};
+    const float *state[3] = {g.state_now, g.state_before, g.state_gain};
+    std::vector<float> gathered(S);
+    for (int c = 0; c < 3; ++c) {
+        if (!branch[c] || !S) continue;
+        for (uint64_t j = 0; j < S; ++j) gathered[j] = branch[c][s->state_branch[j]];
+        CUDA_TRY(s, cudaMemcpy(const_cast<float *>(state[c]), gathered.data(), 4 * S, cudaMemcpyHostToDevice));
+    }
+    if (coef_inv && s->adjoint_ready) {
+        // The adjoint's products with coef_inv, as its set-up forms them.
+        AdjointTables &t = s->adjoint.t;
+        std::vector<double> coef(s->adjoint_reader_row.size());
+        for (size_t e = 0; e < coef.size(); ++e) {
+            const int32_t r = s->adjoint_reader_row[e];
+            coef[e] = r >= 0 ? (double)coef_inv[r] * s->adjoint_reader_base[e] : s->adjoint_reader_base[e];
+        }
+        if (!coef.empty())
+            CUDA_TRY(s, cudaMemcpy(const_cast<double *>(t.reader_coef), coef.data(), 8 * coef.size(), cudaMemcpyHostToDevice));
+        coef.resize(s->adjoint_corrected_row.size());
+        for (size_t e = 0; e < coef.size(); ++e)
+            coef[e] = (double)coef_inv[s->adjoint_corrected_row[e]] * s->adjoint_corrected_base[e];
+        if (!coef.empty())
+            CUDA_TRY(s, cudaMemcpy(const_cast<double *>(t.corrected_coef), coef.data(), 8 * coef.size(),
+                                   cudaMemcpyHostToDevice));
+    }
+    s->tape_valid = false;
+    return FDTD_OK;
+}
+
 int fdtd_set_tape(fdtd_solver *s, uint64_t segment) {
     if (!s) return set_global(FDTD_EINVAL, "no solver");
     s->tape_segment = segment;
@@ -1514,10 +1614,10 @@ int fdtd_gradient(fdtd_solver *s, const float *signal, uint64_t steps, const dou
     int rc = set_up_adjoint(s);
     if (rc != FDTD_OK) return rc;
     double *grads[5] = {grad_coef_b, grad_coef_inv, grad_now, grad_before, grad_gain};
-    Scratch scratch(s);
+    Kept kept{s};
     return s->precision == FDTD_FP64
-               ? gradient<double>(s, s->adjoint, scratch, signal, steps, dloss_dy, segment, grads)
-               : gradient<float>(s, s->adjoint, scratch, signal, steps, dloss_dy, segment, grads);
+               ? gradient<double>(s, s->adjoint, kept, signal, steps, dloss_dy, segment, grads)
+               : gradient<float>(s, s->adjoint, kept, signal, steps, dloss_dy, segment, grads);
 }
 
 int fdtd_reset(fdtd_solver *s) {

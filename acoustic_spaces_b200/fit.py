@@ -173,8 +173,7 @@ class AdjointFit:
         ``coefficients``, also the gradient with respect to the layout's coefficients."""
         precision = precision or self.precision
         lay = self.layout(params)
-        solver = B200WaveSolver(lay, precision=precision)
-        solver.set_tape(self.segment)  # the run keeps its checkpoints for the gradient
+        solver = self._solver(lay, precision)
         t0 = time.perf_counter()
         y = solver.run(self.signal)
         self.forward_s = time.perf_counter() - t0
@@ -183,7 +182,6 @@ class AdjointFit:
         G = solver.gradient(self.signal, 2.0 * (y - self.target), segment=self.segment)
         self.gradient_s = time.perf_counter() - t0
         loss = float(np.sum((y - self.target) ** 2))
-        solver.close()
         if coefficients:
             return loss, self.chain(params, lay, G), G
         return loss, self.chain(params, lay, G)
@@ -228,6 +226,20 @@ class AdjointFit:
             measured += sign * float(np.sum((solver.run(self.signal) - self.target) ** 2))
             solver.close()
         return predicted, measured
+
+    def _solver(self, lay: dict, precision: str) -> B200WaveSolver:
+        """The fit's solver of this precision, built once and given each iteration's coefficients
+        (the geometry, the adjoint's tables and the tape's buffers stay), at rest, taping."""
+        cache = self.__dict__.setdefault("_solvers", {})
+        solver = cache.get(precision)
+        if solver is None:
+            solver = cache[precision] = B200WaveSolver(lay, precision=precision)
+            solver.set_tape(self.segment)  # the run keeps its checkpoints for the gradient
+        else:
+            solver.set_coefficients(*(lay[k] for k in ("coef_b", "coef_inv", "branch_now", "branch_before", "branch_gain")))
+            solver.set_tape(self.segment)
+            solver.reset()
+        return solver
 
     def chain(self, params: Relaxation, lay: dict, G: dict[str, np.ndarray]) -> np.ndarray:
         """dL/d(conductance, corner_hz) from dL/d of the layout's coefficients."""

@@ -108,6 +108,7 @@ class B200WaveSolver:
         info = self.info()
         self._probes = int(info.probes)
         self.shape = tuple(int(v) for v in np.asarray(layout["shape"]).reshape(-1))
+        self._branches = len(np.asarray(layout["branch_now"]).reshape(-1))
 
     @property
     def probes(self) -> int:
@@ -187,6 +188,31 @@ class B200WaveSolver:
         if status != _abi.FDTD_OK:
             _raise(self._lib, status, self._handle)
         return out
+
+    def set_coefficients(self, coef_b=None, coef_inv=None, branch_now=None, branch_before=None,
+                         branch_gain=None) -> None:  # fmt: skip
+        """Replaces the layout's material coefficients (any of them; float32, one per special row
+        for coef_b/coef_inv, one per branch for the branch terms), keeping the grid, the state and
+        the adjoint's tables: the next steps and gradients are those of a solver built with them."""
+        info = self.info()
+        lengths = {"coef_b": info.special_cells, "coef_inv": info.special_cells}
+        given = {"coef_b": coef_b, "coef_inv": coef_inv, "branch_now": branch_now,
+                 "branch_before": branch_before, "branch_gain": branch_gain}  # fmt: skip
+        arrays, pointers = [], []
+        for name, value in given.items():
+            if value is None:
+                pointers.append(None)
+                continue
+            value = np.ascontiguousarray(value, np.float32).reshape(-1)
+            if name in lengths and len(value) != int(lengths[name]):
+                raise ValueError(f"{name} has {len(value)} values, the grid has {int(lengths[name])} special rows")
+            if name.startswith("branch") and len(value) != self._branches:
+                raise ValueError(f"{name} has {len(value)} values, the grid has {self._branches} branches")
+            arrays.append(value)
+            pointers.append(value.ctypes.data_as(ctypes.POINTER(ctypes.c_float)))
+        status = self._lib.fdtd_set_coefficients(self._handle, *pointers)
+        if status != _abi.FDTD_OK:
+            _raise(self._lib, status, self._handle)
 
     def set_tape(self, segment: int) -> None:
         """With ``segment`` > 0, each :meth:`run` from rest keeps the state every ``segment`` steps

@@ -183,6 +183,18 @@ int fdtd_gradient(fdtd_solver *solver, const float *signal, uint64_t steps, cons
  */
 int fdtd_set_tape(fdtd_solver *solver, uint64_t segment);
 
+/*
+ * New material coefficients for the handle's grid (no counterpart in the reference, which builds a
+ * new solver for new materials): each non-NULL array replaces the layout's — coef_b and coef_inv
+ * one per special row (special_count), branch_now, branch_before and branch_gain one per branch
+ * (branch_count, gathered per state as fdtd_create gathers them). The geometry, the state and the
+ * adjoint's tables stay (their products with coef_inv are formed anew), so that a fit steps one
+ * handle through its iterations; stepping and gradients then equal those of a handle created with
+ * the new coefficients, to the bit. Waits for the handle's work; drops the tape.
+ */
+int fdtd_set_coefficients(fdtd_solver *solver, const float *coef_b, const float *coef_inv, const float *branch_now,
+                          const float *branch_before, const float *branch_gain);
+
 /* Bytes of the static device pool of fdtd_gradient_noalloc: 16 MiB, held on every device the
    library runs on until the process exits. */
 #define FDTD_GRADIENT_STATIC_BYTES (16ull << 20)

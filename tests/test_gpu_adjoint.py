@@ -179,3 +179,25 @@ def test_a_taped_run_gives_the_gradient_to_the_bit():
     got = taped.gradient(other, 2.0 * y2, segment=37)
     for key in expected:
         np.testing.assert_array_equal(got[key], expected[key], err_msg=key)
+
+
+def test_new_coefficients_step_and_differentiate_as_a_new_solver():
+    # fdtd_set_coefficients after a gradient (the adjoint's tables set up): the run and the
+    # gradient equal those of a solver built with the new coefficients, to the bit.
+    problem = fit.patched_room(1, size=(3.0, 2.4, 1.6), cell=0.1, steps=300, precision="fp64", segment=100)
+    f = problem.fit
+    first, second = f.layout(problem.start), f.layout(problem.truth)
+    kept = B200WaveSolver(first, precision="fp64")
+    y = kept.run(f.signal)
+    kept.reset()
+    kept.gradient(f.signal, 2.0 * y, segment=100)
+    kept.set_coefficients(*(second[k] for k in ("coef_b", "coef_inv", "branch_now", "branch_before", "branch_gain")))
+    fresh = B200WaveSolver(second, precision="fp64")
+    y2 = fresh.run(f.signal)
+    np.testing.assert_array_equal(kept.run(f.signal), y2)
+    kept.reset()
+    fresh.reset()
+    got = kept.gradient(f.signal, 2.0 * y2, segment=100)
+    expected = fresh.gradient(f.signal, 2.0 * y2, segment=100)
+    for key in expected:
+        np.testing.assert_array_equal(got[key], expected[key], err_msg=key)
