@@ -76,15 +76,13 @@ __device__ __forceinline__ double probe_terms(const AdjointTables &t, uint32_t b
     return sum;
 }
 
-// Interior cells that special rows read, or that probes read, whole: the transposed stencil of
+// An interior cell that special rows read, or that probes read, whole: the transposed stencil of
 // their interior (and solid) axial neighbours, as the sweep forms it, plus each reading row's
 // coefficient times its L~, minus the level two steps on (lam_out holds it on entry), plus the
 // probes' terms of step n. The sweep leaves these cells alone.
 template <typename T>
-__global__ void __launch_bounds__(kBlock) correct_kernel(const AdjointTables t, const T *lam_next, const T *tilde,
-                                                         T *lam_out, const double *dloss, uint64_t stride,
-                                                         uint64_t step) {
-    const uint32_t c = blockIdx.x * kBlock + threadIdx.x;
+__device__ __forceinline__ void correct_cell(const AdjointTables &t, uint32_t c, const T *lam_next, const T *tilde,
+                                             T *lam_out, const double *dloss, uint64_t stride, uint64_t step) {
     if (c >= t.corrected) return;
     const uint32_t cell = t.corrected_cell[c];
     const uint32_t special = t.corrected_mask[c];
@@ -100,20 +98,17 @@ __global__ void __launch_bounds__(kBlock) correct_kernel(const AdjointTables t, 
     lam_out[cell] = value;
 }
 
-// Special rows: the adjoint of their cells (with the probes' terms of step n) and branch states,
+// A special row: the adjoint of its cell (with the probes' terms of step n) and branch states,
 // their L~ of level n for the next reverse step (tilde_out), and the gradient of step n.
 // lam_next/om_next: level n+1 (complete), tilde its L~; lam_out/om_out: hold level n+2 on entry
 // (own row only) and level n on exit; traj levels of u_{n-1}, u_n... at l0 = n - s0, then l0 + 1,
 // l0 + 2.
 template <typename T>
-__global__ void __launch_bounds__(kBlock) special_adjoint_kernel(const AdjointTables t, const T *lam_next,
-                                                                 const T *om_next, const T *tilde, T *lam_out,
-                                                                 T *om_out, const T *traj_u, const T *traj_w,
-                                                                 uint32_t level, double *g_ci, double *g_cb,
-                                                                 double *g_now, double *g_before, double *g_gain,
-                                                                 T *tilde_out, const double *dloss, uint64_t stride,
-                                                                 uint64_t step) {
-    const uint32_t k = blockIdx.x * kBlock + threadIdx.x;
+__device__ __forceinline__ void special_adjoint_row(const AdjointTables &t, uint32_t k, const T *lam_next,
+                                                   const T *om_next, const T *tilde, T *lam_out, T *om_out,
+                                                   const T *traj_u, const T *traj_w, uint32_t level, double *g_ci,
+                                                   double *g_cb, double *g_now, double *g_before, double *g_gain,
+                                                   T *tilde_out, const double *dloss, uint64_t stride, uint64_t step) {
     if (k >= t.specials) return;
     const uint32_t i = t.special[k];
     const T ci = (T)t.coef_inv[k], cb = (T)t.coef_b[k];
@@ -155,6 +150,23 @@ __global__ void __launch_bounds__(kBlock) special_adjoint_kernel(const AdjointTa
         g_gain[j] += (double)om1 * ((double)u_next - (double)u_prev);
     }
     tilde_out[k] = next_tilde;
+}
+
+// The special rows' adjoint (blocks 0 .. special_blocks - 1) and correct_kernel's cells (the
+// blocks after) in one launch: they read the same complete level and write disjoint memory.
+template <typename T>
+__global__ void __launch_bounds__(kBlock) rows_adjoint_kernel(const AdjointTables t, uint32_t special_blocks,
+                                                              const T *lam_next, const T *om_next, const T *tilde,
+                                                              T *lam_out, T *om_out, const T *traj_u, const T *traj_w,
+                                                              uint32_t level, double *g_ci, double *g_cb, double *g_now,
+                                                              double *g_before, double *g_gain, T *tilde_out,
+                                                              const double *dloss, uint64_t stride, uint64_t step) {
+    if (blockIdx.x < special_blocks)
+        special_adjoint_row<T>(t, blockIdx.x * kBlock + threadIdx.x, lam_next, om_next, tilde, lam_out, om_out, traj_u,
+                               traj_w, level, g_ci, g_cb, g_now, g_before, g_gain, tilde_out, dloss, stride, step);
+    else
+        correct_cell<T>(t, (blockIdx.x - special_blocks) * kBlock + threadIdx.x, lam_next, tilde, lam_out, dloss, stride,
+                        step);
 }
 
 }  // namespace fdtd

@@ -372,14 +372,19 @@ int launch_steps(fdtd_solver *s, const float *d_signal, uint64_t steps, double *
         f.signal = d_signal + k;
         f.out = d_out + k;
         f.out_stride = stride;
+        if (s->record_tables) {
+            // The special rows' new values, level k + 2 of the gradient's trajectory.
+            f.traj_u = static_cast<T *>(s->record_u) + (k + 2) * s->specials;
+            f.traj_w = static_cast<T *>(s->record_w) + (k + 2) * s->states;
+        }
         if (fork) {
             if (k > 0) {
                 CUDA_TRY(s, cudaStreamWaitEvent(s->stream, s->joined[1], 0));
-                CUDA_TRY(s, cudaStreamWaitEvent(s->stream, s->joined[2], 0));
+                if (layer_blocks) CUDA_TRY(s, cudaStreamWaitEvent(s->stream, s->joined[2], 0));
             }
             CUDA_TRY(s, cudaEventRecord(s->joined[0], s->stream));
             CUDA_TRY(s, cudaStreamWaitEvent(side, s->joined[0], 0));
-            CUDA_TRY(s, cudaStreamWaitEvent(layer, s->joined[0], 0));
+            if (layer_blocks) CUDA_TRY(s, cudaStreamWaitEvent(layer, s->joined[0], 0));
         }
         cudaEvent_t *ev = nullptr;
         if (s->timing) {
@@ -429,23 +434,15 @@ int launch_steps(fdtd_solver *s, const float *d_signal, uint64_t steps, double *
         // (A recomputation for the gradient records the special rows instead of the probes.)
         if (probe_blocks && !s->record_tables) probe_kernel<T><<<probe_blocks, kBlock, 0, side>>>(g, f);
         if (ev) CUDA_TRY(s, cudaEventRecord(ev[7], side));
-        if (s->record_tables) {
-            // The special rows' new values (the special kernel's, on the same stream before).
-            const AdjointTables &t = *s->record_tables;
-            const uint32_t rows = (uint32_t)((std::max<uint32_t>(std::max(t.specials, t.states), 1u) + kBlock - 1) / kBlock);
-            record_kernel<T><<<rows, kBlock, 0, side>>>(t, f.a, f.wa,
-                                                        static_cast<T *>(s->record_u) + (k + 2) * (uint64_t)t.specials,
-                                                        static_cast<T *>(s->record_w) + (k + 2) * (uint64_t)t.states);
-        }
         if (fork) {
             CUDA_TRY(s, cudaEventRecord(s->joined[1], side));
-            CUDA_TRY(s, cudaEventRecord(s->joined[2], layer));
+            if (layer_blocks) CUDA_TRY(s, cudaEventRecord(s->joined[2], layer));
         }
     }
     // The handle's stream ends after all three.
     if (fork && steps) {
         CUDA_TRY(s, cudaStreamWaitEvent(s->stream, s->joined[1], 0));
-        CUDA_TRY(s, cudaStreamWaitEvent(s->stream, s->joined[2], 0));
+        if (layer_blocks) CUDA_TRY(s, cudaStreamWaitEvent(s->stream, s->joined[2], 0));
     }
     CUDA_TRY(s, cudaGetLastError());
     return FDTD_OK;
@@ -1160,23 +1157,19 @@ int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float
         for (uint64_t m = count; m-- > 0;) {
             T *lam_next = static_cast<T *>(adj.lam[xx]), *lam_out = static_cast<T *>(adj.lam[1 - xx]);
             T *om_next = static_cast<T *>(adj.om[xx]), *om_out = static_cast<T *>(adj.om[1 - xx]);
-            // On three streams, the sweep of the interior, the cells that special rows or probes
-            // read (correct_kernel) and the special rows (with their L~ of level n for the next
-            // step), which write disjoint cells; each step starts when all three have ended.
+            // The sweep of the interior on the handle's stream; beside it, in one launch on the side
+            // stream, the special rows (with their L~ of level n for the next step) and the cells
+            // that special rows or probes read (correct_kernel's): all write disjoint cells, and
+            // each step starts when both streams have ended the one before.
             const T *tilde = static_cast<const T *>(adj.tilde[xx]);
             T *tilde_out = static_cast<T *>(adj.tilde[1 - xx]);
             CUDA_TRY(s, cudaEventRecord(s->joined[0], s->stream));
             CUDA_TRY(s, cudaStreamWaitEvent(s->side, s->joined[0], 0));
-            CUDA_TRY(s, cudaStreamWaitEvent(s->layer_stream, s->joined[0], 0));
-            if (special_blocks)
-                special_adjoint_kernel<T><<<special_blocks, kBlock, 0, s->side>>>(
-                    t, lam_next, om_next, tilde, lam_out, om_out, traj_u, traj_w, (uint32_t)m, g[1], g[0], g[2], g[3], g[4],
-                    tilde_out, seg_dloss, segment, m);
-            if (corrected_blocks)
-                correct_kernel<T><<<corrected_blocks, kBlock, 0, s->layer_stream>>>(t, lam_next, tilde, lam_out, seg_dloss,
-                                                                                    segment, m);
+            if (special_blocks + corrected_blocks)
+                rows_adjoint_kernel<T><<<special_blocks + corrected_blocks, kBlock, 0, s->side>>>(
+                    t, special_blocks, lam_next, om_next, tilde, lam_out, om_out, traj_u, traj_w, (uint32_t)m, g[1], g[0],
+                    g[2], g[3], g[4], tilde_out, seg_dloss, segment, m);
             CUDA_TRY(s, cudaEventRecord(s->joined[1], s->side));
-            CUDA_TRY(s, cudaEventRecord(s->joined[2], s->layer_stream));
             if (s->bulk_blocks) {
                 BulkArgs args = s->bulk;
                 args.a = lam_out;
@@ -1184,7 +1177,6 @@ int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float
                                                                                         adj.map_t, s->map_s, args);
             }
             CUDA_TRY(s, cudaStreamWaitEvent(s->stream, s->joined[1], 0));
-            CUDA_TRY(s, cudaStreamWaitEvent(s->stream, s->joined[2], 0));
             xx = 1 - xx;
         }
         CUDA_TRY(s, cudaGetLastError());

@@ -311,6 +311,8 @@ struct Fields {
     const float *signal;  // the step's drive at signal[0]
     double *out;       // probe p's record at out[p * out_stride]
     uint64_t out_stride;
+    T *traj_u;         // when not null: each special row's new pressure at traj_u[k] (the gradient's
+    T *traj_w;         // recomputation), and each branch state's new velocity at traj_w[j]
 };
 
 // Special rows (fdtd.hpp:860-881), one a thread: its links, its branch states' flow, the update,
@@ -352,9 +354,12 @@ __global__ void __launch_bounds__(kBlock) special_kernel(const Tables g, const F
     const T next = ((T)g.coef_a[k] * b[i] + sum - (T)g.coef_b[k] * previous - flow +
                     (T)g.source[k] * (T)f.signal[0]) * (T)g.coef_inv[k];
     f.a[i] = next;
+    if (f.traj_u) f.traj_u[k] = next;
     for (uint32_t j = s0; j < s1; ++j) {
         const T own = (T)g.state_now[j] * f.wb[j] - (T)g.state_before[j] * f.wa[j];
-        f.wa[j] = f.wa[j] + ((next - previous) * (T)g.state_gain[j] + own);
+        const T w = f.wa[j] + ((next - previous) * (T)g.state_gain[j] + own);
+        f.wa[j] = w;
+        if (f.traj_w) f.traj_w[j] = w;
     }
 }
 
