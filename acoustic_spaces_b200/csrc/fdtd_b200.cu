@@ -131,6 +131,11 @@ struct fdtd_solver {
         size_t bytes;
     };
     std::vector<Block> work;
+    // Graphs of a full segment's recomputation and reverse steps over the kept workspace
+    // ([recompute/reverse][the levels' or adjoint levels' roles at the segment's start]), captured
+    // once and replayed while the workspace and the segment stay.
+    cudaGraphExec_t grad_graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    uint64_t graph_segment = 0;
     // While the gradient recomputes a segment: the special rows' values after each step of a
     // dispatch, recorded as level k + 2 of the trajectory after the dispatch's step k.
     const AdjointTables *record_tables = nullptr;
@@ -789,6 +794,9 @@ void release(fdtd_solver *s) {
         if (stream) cudaStreamSynchronize(stream);
     for (cudaGraphExec_t g : s->graph)
         if (g) cudaGraphExecDestroy(g);
+    for (auto &row : s->grad_graph)
+        for (cudaGraphExec_t g : row)
+            if (g) cudaGraphExecDestroy(g);
     for (const auto &b : s->work) cudaFree(b.p);
     for (cudaEvent_t e : s->timing_events) cudaEventDestroy(e);
     for (void *p : s->allocations) cudaFree(p);
@@ -1034,11 +1042,15 @@ int set_up_adjoint(fdtd_solver *s) {
 
 // fdtd_gradient's workspace on the handle: the blocks of the last call handed out again in order
 // while the sizes match, each cleared on the handle's stream; from the first that does not, new
-// ones. (A graph of a segment's steps over these blocks, captured once and replayed, measured 8 %
-// slower than launching them on the 2.6M-cell fit room: the steps are not launch-bound there.)
+// ones (the graphs over the old ones dropped).
 struct Kept {
     fdtd_solver *s;
     size_t next = 0;
+    void drop_graphs() {
+        for (auto &row : s->grad_graph)
+            for (cudaGraphExec_t &g : row)
+                if (g) cudaGraphExecDestroy(g), g = nullptr;
+    }
     int take(size_t bytes, void **out) {
         *out = nullptr;
         const size_t size = bytes ? bytes : 16;
@@ -1046,11 +1058,13 @@ struct Kept {
             CUDA_TRY(s, cudaStreamSynchronize(s->stream));
             for (size_t i = next; i < s->work.size(); ++i) cudaFree(s->work[i].p);
             s->work.resize(next);
+            drop_graphs();
         }
         if (next == s->work.size()) {
             void *p = nullptr;
             CUDA_TRY(s, cudaMalloc(&p, size));
             s->work.push_back({p, size});
+            drop_graphs();
         }
         *out = s->work[next++].p;
         CUDA_TRY(s, cudaMemsetAsync(*out, 0, size, s->stream));
@@ -1062,7 +1076,7 @@ struct Kept {
 // (scratch.take(bytes, &p): device memory cleared to 0 in order on the handle's stream).
 template <typename T, class Pool>
 int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float *signal, uint64_t steps,
-             const double *dloss, uint64_t segment, double *grads[5]) {
+             const double *dloss, uint64_t segment, double *grads[5], bool graphs) {
     const uint64_t K = s->specials, S = s->states, P = s->probes;
     const size_t e = sizeof(T);
     if (segment == 0 || segment > steps) segment = steps;
@@ -1182,6 +1196,37 @@ int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float
         CUDA_TRY(s, cudaGetLastError());
         return FDTD_OK;
     };
+    // With `graphs` (a kept workspace, whose blocks stay put), a full segment's recomputation and
+    // reverse steps are captured once as graphs and replayed: on the small grids of a fit, a step's
+    // launches and event records and waits take more host time than the step takes on the device.
+    if (graphs && s->graph_segment != segment) {
+        Kept{s}.drop_graphs();
+        s->graph_segment = segment;
+    }
+    auto run = [&](int which, int key, auto &&body, uint64_t count) -> int {
+        if (!graphs || count != segment || segments == 1) return body(count);
+        cudaGraphExec_t &exec = s->grad_graph[which][key];
+        if (!exec) {
+            const bool timing = s->timing;
+            s->timing = false;  // no timing events inside a graph
+            cudaError_t e = cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal);
+            const int r = e == cudaSuccess ? body(count) : FDTD_OK;
+            s->timing = timing;
+            if (e != cudaSuccess) return cuda_fail(s, e, "cudaStreamBeginCapture");
+            cudaGraph_t graph = nullptr;
+            e = cudaStreamEndCapture(s->stream, &graph);
+            if (r != FDTD_OK) {
+                if (graph) cudaGraphDestroy(graph);
+                return r;
+            }
+            if (e != cudaSuccess) return cuda_fail(s, e, "cudaStreamEndCapture");
+            e = cudaGraphInstantiateWithFlags(&exec, graph, cudaGraphInstantiateFlagUseNodePriority);
+            cudaGraphDestroy(graph);
+            if (e != cudaSuccess) return cuda_fail(s, e, "cudaGraphInstantiate");
+        }
+        CUDA_TRY(s, cudaGraphLaunch(exec, s->stream));
+        return FDTD_OK;
+    };
     for (uint64_t k = segments; k-- > 0;) {
         const uint64_t s0 = k * segment, s1 = std::min(steps, s0 + segment), count = s1 - s0;
         // Recompute the segment from its start, recording each level of the special rows.
@@ -1197,13 +1242,13 @@ int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float
         record_kernel<T><<<row_blocks, kBlock, 0, s->stream>>>(t, static_cast<const T *>(s->u[1]),
                                                                static_cast<const T *>(s->w[1]), traj_u + K, traj_w + S);
         CUDA_TRY(s, cudaMemcpyAsync(seg_signal, d_signal + s0, sizeof(float) * count, cudaMemcpyDeviceToDevice, s->stream));
-        if ((rc = recompute(count)) != FDTD_OK) return rc;
+        if ((rc = run(0, s->flipped ? 1 : 0, recompute, count)) != FDTD_OK) return rc;
         settle(s, count);
         // The reverse steps of the segment, with its columns of dL/dy.
         if (P)
             CUDA_TRY(s, cudaMemcpy2DAsync(seg_dloss, sizeof(double) * segment, d_dloss + s0, sizeof(double) * steps,
                                           sizeof(double) * count, P, cudaMemcpyDeviceToDevice, s->stream));
-        if ((rc = reverse(count)) != FDTD_OK) return rc;
+        if ((rc = run(1, x, reverse, count)) != FDTD_OK) return rc;
         if (count & 1) x = 1 - x;
     }
     CUDA_TRY(s, cudaStreamSynchronize(s->stream));
@@ -1522,8 +1567,9 @@ int fdtd_gradient_noalloc(fdtd_solver *s, const float *signal, uint64_t steps, c
     AdjointState adj;
     if ((rc = place_adjoint(s, lists, pool, adj)) != FDTD_OK) return rc;
     double *grads[5] = {grad_coef_b, grad_coef_inv, grad_now, grad_before, grad_gain};
-    return s->precision == FDTD_FP64 ? gradient<double>(s, adj, pool, signal, steps, dloss_dy, segment, grads)
-                                     : gradient<float>(s, adj, pool, signal, steps, dloss_dy, segment, grads);
+    // (No graphs: instantiating one allocates.)
+    return s->precision == FDTD_FP64 ? gradient<double>(s, adj, pool, signal, steps, dloss_dy, segment, grads, false)
+                                     : gradient<float>(s, adj, pool, signal, steps, dloss_dy, segment, grads, false);
 }
 
 int fdtd_set_coefficients(fdtd_solver *s, const float *coef_b, const float *coef_inv, const float *branch_now,
@@ -1608,8 +1654,8 @@ int fdtd_gradient(fdtd_solver *s, const float *signal, uint64_t steps, const dou
     double *grads[5] = {grad_coef_b, grad_coef_inv, grad_now, grad_before, grad_gain};
     Kept kept{s};
     return s->precision == FDTD_FP64
-               ? gradient<double>(s, s->adjoint, kept, signal, steps, dloss_dy, segment, grads)
-               : gradient<float>(s, s->adjoint, kept, signal, steps, dloss_dy, segment, grads);
+               ? gradient<double>(s, s->adjoint, kept, signal, steps, dloss_dy, segment, grads, true)
+               : gradient<float>(s, s->adjoint, kept, signal, steps, dloss_dy, segment, grads, true);
 }
 
 int fdtd_reset(fdtd_solver *s) {
