@@ -94,20 +94,35 @@ class Grid:
 
 
 @dataclass
+class Screen:
+    """A thin planar wall (a barrier) across axis ``axis`` at ``position`` metres, spanning
+    ``lo`` to ``hi`` along the other two axes (in their order), of ``material``: the links of the
+    cells whose centres it separates, within its span, are cut."""
+
+    axis: int
+    position: float
+    lo: tuple[float, float]
+    hi: tuple[float, float]
+    material: Material
+
+
+@dataclass
 class Room:
     """A convex room: the cells with n_f . x < d_f for every plane f. ``materials[f]`` is plane
     f's wall, or None for an open face (no wall: the air goes through). With ``patches``, the walls
     are cut into patches: ``patches(planes, points)`` gives the index into ``patch_materials`` of
-    the wall at each crossing point of a plane (arrays)."""
+    the wall at each crossing point of a plane (arrays). ``screens`` are thin walls inside."""
 
     normals: np.ndarray  # (F, 3), unit
     offsets: np.ndarray  # (F,)
     materials: list[Material | None]
     patches: object = None
     patch_materials: list[Material] | None = None
+    screens: list[Screen] = field(default_factory=list)
 
     def wall_materials(self) -> list[Material | None]:
-        return list(self.patch_materials) if self.patches is not None else list(self.materials)
+        walls = list(self.patch_materials) if self.patches is not None else list(self.materials)
+        return walls + [screen.material for screen in self.screens]
 
     @property
     def open(self) -> bool:
@@ -233,8 +248,9 @@ def cubic_cells(grid: Grid, point) -> list[tuple[int, float]]:
     return out
 
 
-def _layer_tables(size: int, layer: int, damping: float, courant: float):
-    """keep and push of the centres and the faces along an axis (fdtd.hpp:2219-2238)."""
+def _layer_tables(size: int, layer: int, damping: float, courant: float, ends=(True, True)):
+    """keep and push of the centres and the faces along an axis (fdtd.hpp:2219-2238), damped
+    toward the ends of the axis that have the layer."""
 
     def damp(from_edge: float) -> float:
         into = max(0.0, layer + 0.5 - from_edge) / layer
@@ -242,10 +258,11 @@ def _layer_tables(size: int, layer: int, damping: float, courant: float):
 
     ck, cp, fk, fp = [], [], [], []
     last = float(size - 1)
+    far = float("inf")
     for x in range(size + 1):
         c = float(x)
-        dc = damp(min(c, last - c))
-        df = damp(min(c - 0.5, last - c + 0.5))
+        dc = damp(min(c if ends[0] else far, last - c if ends[1] else far))
+        df = damp(min(c - 0.5 if ends[0] else far, last - c + 0.5 if ends[1] else far))
         ck.append((1.0 - dc) / (1.0 + dc))
         cp.append(courant / (1.0 + dc))
         fk.append((1.0 - df) / (1.0 + df))
@@ -272,21 +289,33 @@ def cell_face_layouts(
     edge_admittance: float = 1.0,
     speed: float | None = None,
     rate: float | None = None,
+    layer_sides=(True,) * 6,
+    layer_meets_walls: bool = False,
 ) -> list[Built]:
     """The layouts of one room with each of ``sources`` in turn (the same probes): the room's
-    rows are worked out once."""
+    rows are worked out once. ``layer_sides``: which faces of the grid (x-, x+, y-, y+, z-, z+)
+    have the matched layer. ``layer_meets_walls``: let walls reach the layer's cells, which then
+    take their plain layer update (a solid neighbour's pressure is zero); the reference refuses
+    such a model, and by default so does this builder."""
     nx, ny, nz = grid.shape
     n = grid.n
     sy, sz = nx, nx * ny
     inside, near = _inside(room, grid)
     inside, near = inside.reshape(-1), near.reshape(-1)
     # The grid's edge, and each cell's depth into it.
-    ix = np.arange(nx)
-    dx = np.minimum(ix, nx - 1 - ix)
-    dy = np.minimum(np.arange(ny), ny - 1 - np.arange(ny))
-    dz = np.minimum(np.arange(nz), nz - 1 - np.arange(nz))
+    def axis_depth(size, low, high):
+        i = np.arange(size)
+        big = np.full(size, np.iinfo(np.int64).max // 4)
+        return np.minimum(np.where(low, i, big), np.where(high, size - 1 - i, big))
+
+    def edge_depth(size):
+        i = np.arange(size)
+        return np.minimum(i, size - 1 - i)
+
+    dx, dy, dz = (axis_depth(size, layer_sides[2 * a], layer_sides[2 * a + 1]) for a, size in enumerate((nx, ny, nz)))
     depth = np.minimum(np.minimum(dz[:, None, None], dy[None, :, None]), dx[None, None, :]).reshape(-1)
-    edge = depth == 0
+    ex, ey, ez = edge_depth(nx), edge_depth(ny), edge_depth(nz)
+    edge = (np.minimum(np.minimum(ez[:, None, None], ey[None, :, None]), ex[None, None, :]) == 0).reshape(-1)
 
     # Air: the inside, and with an open face all but the edge (fdtd.hpp:499-519).
     air = (~edge) if room.open else (inside & ~edge)
@@ -317,13 +346,39 @@ def cell_face_layouts(
         walled = face >= 0
         blocked[k, c[walled]] = True
         material[k, c[walled]] = face[walled]
+    # Screens: the links along a screen's axis between cells on its two sides, within its span.
+    walls = len(room.wall_materials()) - len(room.screens)
+
+    def screened(screen: Screen, cells: np.ndarray, k: int) -> np.ndarray:
+        a = screen.axis
+        step = AXIAL_STEPS[k][a]
+        if step == 0:
+            return np.zeros(len(cells), bool)
+        index = (cells % nx, (cells // nx) % ny, cells // (nx * ny))
+        here = grid.centres(a)[index[a]]
+        there = here + step * grid.cell
+        others = [b for b in range(3) if b != a]
+        inside_span = np.ones(len(cells), bool)
+        for m, b in enumerate(others):
+            centre = grid.centres(b)[index[b]]
+            inside_span &= (centre >= screen.lo[m]) & (centre <= screen.hi[m])
+        return inside_span & ((here - screen.position) * (there - screen.position) < 0.0)
+
+    for si, screen in enumerate(room.screens):
+        for k in range(6):
+            hit = screened(screen, candidates, k) & ~blocked[k, candidates]
+            blocked[k, candidates[hit]] = True
+            material[k, candidates[hit]] = walls + si
     boundary = np.flatnonzero(blocked.any(axis=0) & (types == 1))
     # The matched layer's air must meet no face (fdtd.hpp:521-528).
-    for off in offsets:
-        j = layer_cells + off
-        maybe = near[layer_cells] & near[j] & ~edge[j]
-        if np.any(_first_wall(room, grid, layer_cells[maybe], j[maybe]) >= 0):
-            raise ValueError("the model reaches into the matched layer")
+    if not layer_meets_walls:
+        for k, off in enumerate(offsets):
+            j = layer_cells + off
+            maybe = near[layer_cells] & near[j] & ~edge[j]
+            if np.any(_first_wall(room, grid, layer_cells[maybe], j[maybe]) >= 0) or any(
+                np.any(screened(screen, layer_cells, k)) for screen in room.screens
+            ):
+                raise ValueError("the model reaches into the matched layer")
 
     # Materials: beta and branches.
     mats = room.wall_materials()
@@ -497,7 +552,8 @@ def cell_face_layouts(
         courant = math.sqrt(float(weights[0]))
         for a, name in enumerate("xyz"):
             if len(layer_cells):
-                ck, cp, fk, fp = _layer_tables(grid.shape[a], layer, layer_damping, courant)
+                ends = (layer_sides[2 * a], layer_sides[2 * a + 1])
+                ck, cp, fk, fp = _layer_tables(grid.shape[a], layer, layer_damping, courant, ends)
             else:
                 ck = cp = fk = fp = np.zeros(0, np.float32)
             layout[f"keep_{name}"], layout[f"push_{name}"] = ck, cp
@@ -728,6 +784,101 @@ def polyhedral_room(
         "seed": seed,
     }
     return Workload("polyhedral_room", room, built, points[0], points[1:], gaussian_drive(rate, steps), description)
+
+
+def miki_admittance(frequency_hz, flow_resistivity):
+    """Normalised surface admittance of a semi-infinite porous ground of flow resistivity
+    ``flow_resistivity`` (Pa s/m^2) by Miki's model (Miki 1990, a revision of Delany and
+    Bazley's): Z = 1 + 5.50 X^-0.632 - j 8.43 X^-0.632, X = 1000 f / sigma, time dependence
+    e^{j w t}; the reference fits its ground materials to the same model (materials/ground.py)."""
+    x = 1000.0 * np.asarray(frequency_hz, float) / flow_resistivity
+    z = 1.0 + 5.50 * x**-0.632 - 1j * 8.43 * x**-0.632
+    return 1.0 / z
+
+
+def porous_ground(flow_resistivity: float, rate: float, *, poles: int = 3, band=(20.0, 600.0)) -> Material:
+    """A ground material: Miki's admittance fitted over ``band`` Hz by a real beta and ``poles``
+    relaxation branches (conductance g_j, corner frequency f_j: Y = beta + sum g_j jw / (jw +
+    2 pi f_j)), corner frequencies log-spaced over the band and the conductances and beta by
+    non-negative least squares, so that the fit is passive."""
+    from scipy.optimize import nnls
+
+    f = np.geomspace(band[0], band[1], 200)
+    target = miki_admittance(f, flow_resistivity)
+    corners = np.geomspace(band[0], band[1], poles)
+    jw = 2j * math.pi * f
+    columns = [np.ones_like(jw)] + [jw / (jw + 2.0 * math.pi * fc) for fc in corners]
+    a = np.vstack([np.concatenate([c.real, c.imag]) for c in columns]).T
+    b = np.concatenate([target.real, target.imag])
+    coef, _ = nnls(a, b)
+    branches = [np.array([[0.0, 1.0 / g, (1.0 / g) * 2.0 * math.pi * fc / rate]])
+                for g, fc in zip(coef[1:], corners) if g > 0.0]  # fmt: skip
+    return Material(float(coef[0]), np.vstack(branches) if branches else np.zeros((0, 3)))
+
+
+def outdoor_halfspace(
+    seed: int = 0,
+    *,
+    shape=(1024, 256, 256),
+    cell: float = 0.1,
+    layer: int = 12,
+    receivers: int = 64,
+    steps: int = 8000,
+    barrier: bool = True,
+    barrier_height: float = 3.0,
+    speed_of_sound: float = 343.0,
+) -> Workload:
+    """An outdoor half-space on a grid of ``shape`` cells of ``cell`` metres: porous ground two
+    cells above the grid's floor (Miki's admittance of a flow resistivity log-uniform in 50 to
+    20,000 kPa s/m^2, fitted by three relaxation branches), air above it, a ``layer``-cell matched
+    layer (damping 0.5) on the five open sides, the ground running into it (this project's own
+    layout: the reference refuses a model that reaches its matched layer). A rigid thin barrier
+    ``barrier_height`` m high at a seeded x across y (short of the layer); the source 0.5 m above
+    the ground 5 to 15 m before the barrier (less on small grids); ``receivers`` receivers 1.5 m above the ground on a
+    line along x behind it; a 0.5 ms Gaussian drive."""
+    rng = np.random.default_rng(seed)
+    rate = speed_of_sound / (COURANT * cell)
+    nx, ny, nz = shape
+    grid = Grid(-OFFSET * cell, cell, tuple(shape))
+    ground_z = grid.origin[2] + 2.0 * cell
+    sigma = math.exp(rng.uniform(math.log(50.0), math.log(20000.0))) * 1000.0
+    ground = porous_ground(sigma, rate)
+    room = Room(np.array([[0.0, 0.0, -1.0]]), np.array([-ground_z]), [ground])
+    lo_x = grid.origin[0] + (layer + 4) * cell
+    hi_x = grid.origin[0] + (nx - layer - 4) * cell
+    lo_y = grid.origin[1] + (layer + 4) * cell
+    hi_y = grid.origin[1] + (ny - layer - 4) * cell
+    barrier_x = float(rng.uniform(0.35, 0.5) * (hi_x - lo_x) + lo_x) + 0.5 * cell * 0.37
+    y_mid = 0.5 * (lo_y + hi_y) + float(rng.uniform(-1.0, 1.0))
+    before = min(float(rng.uniform(5.0, 15.0)), 0.8 * (barrier_x - lo_x))  # (small grids: what there is)
+    source = np.array([barrier_x - before, y_mid, ground_z + 0.5])
+    xs = np.linspace(barrier_x + 2.0, hi_x - 1.0, receivers)
+    probes = np.stack([xs, np.full(receivers, y_mid), np.full(receivers, ground_z + 1.5)], 1)
+    if barrier:
+        room.screens.append(Screen(0, barrier_x, (lo_y, ground_z), (hi_y, ground_z + barrier_height), Material(0.0)))
+    built = cell_face_layout(room, grid, source, probes, layer=layer, layer_damping=LAYER_DAMPING, rate=rate,
+                             layer_sides=(True, True, True, True, False, True), layer_meets_walls=True)  # fmt: skip
+    lay = built.layout
+    description = {
+        "room": f"outdoor half-space, porous ground (Miki, sigma {sigma / 1000:.0f} kPa s/m^2, 3 relaxation branches)"
+        + (f", rigid barrier {barrier_height:g} m high at x {barrier_x:.2f} m" if barrier else ", no barrier"),
+        "grid": "x".join(str(v) for v in grid.shape),
+        "cell_m": cell,
+        "cells": grid.n,
+        "air_cells": built.air_cells,
+        "interior_cells": int(np.count_nonzero(lay["types"] == 1)),
+        "special_rows": len(lay["special"]),
+        "links": len(lay["link_direction"]),
+        "branch_states": len(lay["state_branch"]),
+        "layer_cells": len(lay["layer_cells"]),
+        "probes": receivers,
+        "steps": steps,
+        "rate_hz": rate,
+        "walls": "cell faces; the ground runs into the matched layer",
+        "stencil": 7,
+        "seed": seed,
+    }
+    return Workload("outdoor_halfspace", room, built, source, probes, gaussian_drive(rate, steps), description)
 
 
 # ---- many rooms in one grid ------------------------------------------------------------------

@@ -158,10 +158,54 @@ class Clocks:
         }
 
 
-def build_workload(args):
+def build_workload(args, barrier: bool = True):
     from acoustic_spaces_b200 import layouts
 
+    if args.workload == "outdoor_halfspace":
+        return layouts.outdoor_halfspace(args.seed, steps=max(args.steps, args.ir_steps), barrier=barrier)
     return layouts.polyhedral_room(args.seed, cell=args.cell, steps=max(args.steps, 1))
+
+
+def insertion_loss(free: np.ndarray, screened: np.ndarray, rate: float, band=(20.0, 300.0)) -> tuple[np.ndarray, np.ndarray]:
+    """Each receiver's insertion loss 20 log10 |P_free(f)| / |P_screened(f)| in dB over ``band``
+    Hz, from the spectra of the whole responses (probes, steps), and a mask of the bins where the
+    free field is within 40 dB of its receiver's peak in the band."""
+    f = np.fft.rfftfreq(free.shape[1], 1.0 / rate)
+    sel = (f >= band[0]) & (f <= band[1])
+    pf = np.abs(np.fft.rfft(free, axis=1))[:, sel]
+    ps = np.abs(np.fft.rfft(screened, axis=1))[:, sel]
+    tiny = 1e-300
+    il = 20.0 * np.log10((pf + tiny) / (ps + tiny))
+    valid = pf >= 1e-2 * pf.max(axis=1, keepdims=True)
+    return il, valid
+
+
+def outdoor_insertion_loss(args, workload, local: int) -> dict:
+    """The half-space's insertion-loss spectra (the barrier's; free field = the same ground without
+    it) from FP32 runs against those from FP64 runs on the same layouts, over the config's steps."""
+    from acoustic_spaces_b200 import B200WaveSolver
+
+    free = build_workload(args, barrier=False)
+    steps = min(len(workload.signal), args.ir_steps)
+    runs = {}
+    for name, w in (("screened", workload), ("free", free)):
+        for precision in ("fp32", "fp64"):
+            solver = B200WaveSolver(w.built.layout, precision=precision, device=local)
+            runs[name, precision] = solver.run(w.signal[:steps])
+            solver.close()
+    il32, valid = insertion_loss(runs["free", "fp32"], runs["screened", "fp32"], workload.built.rate)
+    il64, _ = insertion_loss(runs["free", "fp64"], runs["screened", "fp64"], workload.built.rate)
+    diff = np.abs(il32 - il64)[valid]
+    return {
+        "il_db_max_abs_diff": float(diff.max()),
+        "il_db_median_abs_diff": float(np.median(diff)),
+        "il_db_mean_fp64": float(np.mean(il64[valid])),
+        "band_hz": [20.0, 300.0],
+        "bins": int(valid.sum()),
+        "receivers": int(il32.shape[0]),
+        "steps": steps,
+        "vs": "the same two layouts (with and without the barrier) stepped in FP64 on the GPU",
+    }
 
 
 def cpu_reference_rate(workload, sample_steps: int) -> dict:
@@ -171,7 +215,9 @@ def cpu_reference_rate(workload, sample_steps: int) -> dict:
     from oracle import oracle
 
     threads = os.cpu_count() or 1
-    native = oracle.reference_native()
+    # (The reference lays out rooms that keep clear of the matched layer only; for the others, the
+    # oracle's C port of its stepping runs on the same layout.)
+    native = oracle.reference_native() if workload.name == "polyhedral_room" else None
     air = workload.built.air_cells
     signal = workload.signal[:sample_steps]
     if native is not None:
@@ -441,7 +487,8 @@ def main() -> None:
     parser.add_argument("--reference-repeats", type=int, default=3)
     parser.add_argument("--no-cpu-baseline", action="store_true")
     parser.add_argument("--no-e2e", action="store_true")
-    parser.add_argument("--workload", choices=["polyhedral_room", "batched_rooms", "adjoint_fit"], default="polyhedral_room")
+    parser.add_argument("--workload", choices=["polyhedral_room", "outdoor_halfspace", "batched_rooms", "adjoint_fit"],
+                        default="polyhedral_room")  # fmt: skip
     parser.add_argument("--adjoint-steps", type=int, default=3000)
     parser.add_argument("--adam-iterations", type=int, default=300)
     parser.add_argument("--rooms", type=int, default=64)
@@ -567,6 +614,7 @@ def main() -> None:
         ir_error = ir_errors(p32, p64, workload.built.rate)
         ir_error["steps"] = m
         ir_error["vs"] = "the same layout stepped in FP64 on the GPU (bit-exact with the FP64 oracle on the golden grids)"
+    insertion = outdoor_insertion_loss(args, workload, local) if args.workload == "outdoor_halfspace" else None
 
     bytes_per_step = algorithmic_bytes(desc)
     peak, peak_source = measured_peaks()
@@ -578,8 +626,8 @@ def main() -> None:
         "special": BYTES_SPECIAL * desc["special_rows"] + BYTES_LINK * desc["links"] + BYTES_STATE * desc["branch_states"],
     }
     traffic_table = {}
-    traffic_file = ROOT / "profiles" / "kernel_traffic_polyhedral_room.json"
-    if traffic_file.exists() and args.cell == 0.04:
+    traffic_file = ROOT / "profiles" / f"kernel_traffic_{args.workload}.json"
+    if traffic_file.exists() and (args.cell == 0.04 or args.workload != "polyhedral_room"):
         traffic_table = json.loads(traffic_file.read_text()).get("dram_bytes_per_launch", {})
     kernels = {}
     for kind, nbytes in per_kernel_bytes.items():
@@ -620,7 +668,7 @@ def main() -> None:
             "dtype": "f32",
             "data": "synthetic",
             "config": {
-                "workload": "polyhedral_room",
+                "workload": workload.name,
                 **desc,
                 "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                 "l2": "inputs larger than L2 (two pressure levels alone are "
@@ -649,6 +697,7 @@ def main() -> None:
             },
             "cpu_baseline": cpu,
             "ir_error_vs_fp64": ir_error,
+            "insertion_loss_vs_fp64": insertion,
             "adjoint_over_forward": None,
             "clocks": clocks.summary(),
             "finite": finite,
