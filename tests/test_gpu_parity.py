@@ -138,6 +138,19 @@ def test_gpu_steps_a_polyhedral_room_as_the_oracle_does():
         assert np.array_equal(sa[key], sb[key]), key
 
 
+def test_gpu_steps_a_larger_room_as_the_oracle_does():
+    # The benchmark's workload at 7 cm cells (286 x 214 x 143, 8.7M cells, its levels and types
+    # well beyond a small grid's, in hundreds of tiles): the probes and the whole state equal to
+    # the oracle's.
+    w = layouts.polyhedral_room(0, cell=0.07, steps=120)
+    gpu = B200WaveSolver(w.built.layout)
+    oracle = OracleSolver(w.built.layout)
+    assert np.array_equal(_pieces(gpu, w.signal, [0, 57, 120]), oracle.run(w.signal))
+    sa, sb = gpu.state(), oracle.state()
+    for key in sa:
+        assert np.array_equal(sa[key], sb[key]), key
+
+
 @pytest.fixture(scope="module")
 def full_room():
     return layouts.polyhedral_room(0, steps=600)
