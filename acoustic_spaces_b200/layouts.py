@@ -1038,6 +1038,18 @@ class Batch:
     description: dict
 
 
+def partition(cells: list[int], world: int) -> list[list[int]]:
+    """Items of sizes ``cells`` dealt to ``world`` parts, largest first, each to the part with the
+    fewest cells so far (ties to the lower part): each part's list in increasing order."""
+    parts: list[list[int]] = [[] for _ in range(world)]
+    load = [0] * world
+    for k in sorted(range(len(cells)), key=lambda k: (-cells[k], k)):
+        r = min(range(world), key=lambda r: (load[r], r))
+        parts[r].append(k)
+        load[r] += cells[k]
+    return [sorted(p) for p in parts]
+
+
 def batched_rooms(
     seed: int = 0,
     *,
@@ -1049,16 +1061,21 @@ def batched_rooms(
     receivers: int = 4,
     steps: int = 6000,
     speed_of_sound: float = 343.0,
+    part: tuple[int, int] = (0, 1),
 ) -> Batch:
     """``rooms`` seeded shoebox rooms of dims uniform in ``dims`` metres per axis on cells of
     ``cell`` metres, each wall's absorption uniform in ``absorption`` (a real admittance by Paris's
     formula), each room with ``sources`` seeded source positions (separate solves) and
     ``receivers`` receivers, all at least 0.5 m from the walls; one 0.5 ms Gaussian drive. Every
-    (room, source) is a solve of its own, and all are stacked into one grid."""
-    rng = np.random.default_rng(seed)
+    (room, source) is a solve of its own, and all are stacked into one grid. Room k is drawn from
+    its own generator (seed, k). With ``part`` = (rank, world), only the rooms of
+    :func:`partition` for that rank are built (the solves shard across GPUs with no exchange)."""
     rate = speed_of_sound / (COURANT * cell)
+    sizes = [np.random.default_rng([seed, k]).uniform(dims[0], dims[1], 3) for k in range(rooms)]
+    mine = partition([int(np.prod(room_grid(size, cell).shape)) for size in sizes], part[1])[part[0]]
     layouts, cells = [], []
-    for _ in range(rooms):
+    for k in mine:
+        rng = np.random.default_rng([seed, k])
         size = rng.uniform(dims[0], dims[1], 3)
         betas = paris_admittance(rng.uniform(absorption[0], absorption[1], 6))
         room = shoebox(size, [Material(float(b)) for b in betas])
@@ -1075,6 +1092,7 @@ def batched_rooms(
     stacked = stack(layouts)
     description = {
         "rooms": rooms,
+        "rooms_here": len(mine),
         "sources_per_room": sources,
         "solves": len(layouts),
         "cell_m": cell,

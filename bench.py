@@ -301,10 +301,17 @@ def run_batched(args, world: int, rank: int, local: int) -> None:
     (64 rooms of 3-12 m at 5 cm cells, 4 sources each: 256 solves). Beside it, a sample of the same solves stepped one after another through
     the same public API, and each solve's FP32 error against FP64."""
     import torch
+    import torch.distributed as dist
 
     from acoustic_spaces_b200 import B200WaveSolver, layouts
 
-    batch = layouts.batched_rooms(args.seed, rooms=args.rooms, sources=args.sources, steps=args.steps + args.warmup)
+    # With N ranks, the solves shard by cell count (no exchange): each rank steps its own rooms.
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=900), device_id=torch.device("cuda", local))
+    batch = layouts.batched_rooms(args.seed, rooms=args.rooms, sources=args.sources, steps=args.steps + args.warmup,
+                                  part=(rank, world))  # fmt: skip
     desc = batch.description
     solver = B200WaveSolver(batch.stacked.layout, device=local)
     air = batch.stacked.air_cells
@@ -316,19 +323,37 @@ def run_batched(args, world: int, rank: int, local: int) -> None:
     solver.synchronize()
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with Clocks(local) as clocks:
+        if world > 1:
+            dist.barrier()
         torch.cuda.synchronize()
         start.record(stream)
         solver.run_device(sig.data_ptr() + 4 * warmup, steps, out.data_ptr() + 8 * warmup, steps + warmup)
         end.record(stream)
         solver.synchronize()
         torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
     ms = start.elapsed_time(end)
-    value = air * steps / (ms / 1e3) / 1e9
-    # End to end, the whole batch through the public API.
+    total_air = air
+    if world > 1:
+        t = torch.tensor([ms, float(air)], dtype=torch.float64, device=f"cuda:{local}")
+        mx = t[:1].clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        sm = t[1:].clone()
+        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+        ms, total_air = float(mx.item()), int(sm.item())
+    value = total_air * steps / (ms / 1e3) / 1e9
+    # End to end, the whole batch through the public API (the slowest rank's time).
     solver.reset()
+    if world > 1:
+        dist.barrier()
     t0 = time.perf_counter()
     solver.run(batch.signal[:steps])
     e2e_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
     # A sample of the solves one after another (each its own grid), through the same API.
     rng = np.random.default_rng(1)
     sample = sorted(rng.choice(len(batch.layouts), size=min(args.sequential_sample, len(batch.layouts)), replace=False))
@@ -367,18 +392,22 @@ def run_batched(args, world: int, rank: int, local: int) -> None:
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": "batched_rooms", **desc, "parallelism": "single GPU"},
-        "e2e": {"value": round(air * steps / e2e_s / 1e9, 4), "unit": UNIT, "h2d_bytes_per_step": 4,
+        "config": {"workload": "batched_rooms", **desc, "air_cells_all_ranks": total_air,
+                   "parallelism": f"solves sharded over {world} GPUs by cell count" if world > 1 else "single GPU"},
+        "e2e": {"value": round(total_air * steps / e2e_s / 1e9, 4), "unit": UNIT, "h2d_bytes_per_step": 4,
                 "d2h_bytes_per_step": 8 * solver.probes},  # fmt: skip
         "sequential_solves": {"value": round(sequential, 4), "unit": UNIT, "solves_timed": len(sample),
-                              "api": "B200WaveSolver.run, one solve after another"},  # fmt: skip
-        "batched_over_sequential": round(value / sequential, 3),
+                              "api": "B200WaveSolver.run, one solve after another, on one GPU"},  # fmt: skip
+        "batched_over_sequential": round(value / world / sequential, 3),
         "per_solve_ir_rel_l2_vs_fp64": {"max": float(max(worst)), "median": float(np.median(worst)), "steps": m},
         "clocks": clocks.summary(),
         "gpu_launches": 3 * steps,  # the sweep, the special rows, the probes
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 def run_adjoint(args, world: int, rank: int, local: int) -> None:

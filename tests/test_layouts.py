@@ -155,3 +155,21 @@ def test_stacking_refuses_a_matched_layer():
 
     with pytest.raises(ValueError, match="matched layer"):
         L.stack([load_golden("resonant7")[0], load_golden("open_layer")[0]])
+
+
+def test_the_batched_solves_partition_across_ranks():
+    # Each rank builds its own rooms (balanced by cells); together they are every room, once.
+    import numpy as np
+
+    from acoustic_spaces_b200 import layouts as L
+
+    parts = L.partition([5, 3, 8, 1, 9, 2, 7], 3)
+    assert sorted(k for p in parts for k in p) == list(range(7))
+    loads = [sum([5, 3, 8, 1, 9, 2, 7][k] for k in p) for p in parts]
+    assert max(loads) - min(loads) <= 9
+    whole = L.batched_rooms(3, rooms=4, sources=1, cell=0.2, steps=10)
+    halves = [L.batched_rooms(3, rooms=4, sources=1, cell=0.2, steps=10, part=(r, 2)) for r in range(2)]
+    assert sum(h.description["air_cells"] for h in halves) == whole.description["air_cells"]
+    mine = [L.partition([int(np.prod(L.room_grid(np.random.default_rng([3, k]).uniform(3.0, 12.0, 3), 0.2).shape))
+                         for k in range(4)], 2)[r] for r in range(2)]  # fmt: skip
+    assert sorted(mine[0] + mine[1]) == [0, 1, 2, 3]
