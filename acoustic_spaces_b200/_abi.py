@@ -28,6 +28,7 @@ FDTD_ENODEV = -4
 FDTD_ENONFINITE = -5
 FDTD_FP32 = 0
 FDTD_FP64 = 1
+FDTD_FP32_COMPENSATED = 2
 
 _f32p = ctypes.POINTER(ctypes.c_float)
 _f64p = ctypes.POINTER(ctypes.c_double)
@@ -208,6 +209,7 @@ def pack_layout(layout: Mapping[str, np.ndarray]) -> tuple[FdtdLayout, dict[str,
 #: Every symbol include/fdtd_b200.h declares, with (restype, argtypes).
 SIGNATURES = {
     "fdtd_abi_version": (ctypes.c_int, []),
+    "fdtd_build_id": (ctypes.c_char_p, []),
     "fdtd_global_error": (ctypes.c_char_p, []),
     "fdtd_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
     "fdtd_device_count": (ctypes.c_int, []),
@@ -266,6 +268,14 @@ def load_library(path: str | os.PathLike | None = None) -> ctypes.CDLL:
         fn.argtypes = argtypes
     if lib.fdtd_abi_version() != 1:
         raise RuntimeError("the B200 wave stepper's library has another ABI version")
+    if path is None:
+        from acoustic_spaces_b200 import build
+
+        if lib.fdtd_build_id().decode() != build.source_id():
+            raise RuntimeError(
+                f"{where} was built from other sources than those beside it: rebuild it with "
+                "`python -m acoustic_spaces_b200.build`"
+            )
     if path is None:
         _lib = lib
     return lib

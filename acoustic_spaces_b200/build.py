@@ -9,6 +9,7 @@ linked statically.
 
 from __future__ import annotations
 
+import hashlib
 import shutil
 import subprocess
 import sys
@@ -33,14 +34,30 @@ def nvcc() -> str:
     return found
 
 
+def dependencies() -> list[Path]:
+    """Every file the library is compiled from."""
+    csrc = HERE / "csrc"
+    return sorted([*csrc.glob("*.cu"), *csrc.glob("*.cuh"), *csrc.glob("*.h"), *(ROOT / "include").glob("*.h")])
+
+
+def source_id() -> str:
+    """A digest of the sources' names and contents and of the flags: the library carries the one
+    it was built from (fdtd_build_id), so that a library built from other sources is refused."""
+    digest = hashlib.sha256(" ".join(FLAGS).encode())
+    for path in dependencies():
+        digest.update(path.name.encode() + b"\0" + path.read_bytes())
+    return digest.hexdigest()[:32]
+
+
 def build(verbose: bool = False, force: bool = False) -> Path:
     """Compiles the library unless it is newer than its sources; returns its path."""
-    deps = SOURCES + sorted((HERE / "csrc").glob("*.cuh")) + sorted((ROOT / "include").glob("*.h")) + [Path(__file__)]
+    deps = dependencies() + [Path(__file__)]
     if not force and OUTPUT.exists():
         built = OUTPUT.stat().st_mtime
         if all(p.stat().st_mtime <= built for p in deps):
             return OUTPUT
-    cmd = [nvcc(), *FLAGS, f"-I{ROOT / 'include'}", "-o", str(OUTPUT), *map(str, SOURCES)]
+    cmd = [nvcc(), *FLAGS, f'-DFDTD_BUILD_ID="{source_id()}"', f"-I{ROOT / 'include'}", "-o", str(OUTPUT),
+           *map(str, SOURCES)]  # fmt: skip
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
         print(" ".join(cmd), file=sys.stderr)

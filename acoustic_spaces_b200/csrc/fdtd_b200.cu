@@ -19,6 +19,8 @@
 #include <mutex>
 #include <new>
 #include <string>
+
+#include "fdtd_compensated.h"
 #include <unordered_map>
 #include <vector>
 
@@ -95,6 +97,7 @@ struct fdtd_solver {
     // for the branch velocities w.
     void *u[2] = {nullptr, nullptr};
     void *w[2] = {nullptr, nullptr};
+    void *increment = nullptr;              // FDTD_FP32_COMPENSATED: p_n - p_(n-1) per cell (pitched)
     void *layer_parts = nullptr;            // 3 arrays of the layer's cells: p_x, p_y, p_z
     std::vector<uint32_t> layer_cells;      // pitched, in the layout's order (for fdtd_read_state)
     const uint8_t *types_device = nullptr;  // the pitched cell types
@@ -106,6 +109,7 @@ struct fdtd_solver {
     // Tensor maps of the bulk sweep: each level as the pressure tile (with halos) and as the
     // previous-pressure tile, the cell types and the scales.
     CUtensorMap map_b[2], map_a[2], map_t, map_s;
+    CUtensorMap map_d;  // FDTD_FP32_COMPENSATED: the increments, in the previous pressure's place
     // fdtd_run's chunks: the drive and the records of kGraphSteps steps on the device, and the
     // graph of a chunk's launches for each of the levels' two roles (captured on first use).
     float *d_sig = nullptr;
@@ -335,6 +339,7 @@ Fields<T> fields_for(const fdtd_solver *s, bool flip) {
     f.a = static_cast<T *>(s->u[prev]);
     f.wb = static_cast<const T *>(s->w[cur]);
     f.wa = static_cast<T *>(s->w[prev]);
+    f.d = static_cast<T *>(s->increment);
     f.layer_parts = static_cast<T *>(s->layer_parts);
     for (int axis = 0; axis < 3; ++axis) {
         f.face_old[axis] = static_cast<const T *>(s->faces[cur][axis]);
@@ -343,12 +348,12 @@ Fields<T> fields_for(const fdtd_solver *s, bool flip) {
     return f;
 }
 
-template <typename T, bool WIDE, bool SCALED>
+template <typename T, bool WIDE, bool SCALED, bool COMP>
 int set_up_kernels(fdtd_solver *s) {
-    CUDA_TRY(s, cudaFuncSetAttribute(bulk_kernel<T, WIDE, SCALED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    CUDA_TRY(s, cudaFuncSetAttribute(bulk_kernel<T, WIDE, SCALED, COMP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)Stage<T, SCALED>::smem));
     int per_sm = 0;
-    CUDA_TRY(s, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bulk_kernel<T, WIDE, SCALED>, kBlock,
+    CUDA_TRY(s, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bulk_kernel<T, WIDE, SCALED, COMP>, kBlock,
                                                               Stage<T, SCALED>::smem));
     s->bulk_per_sm = per_sm;
     // One tile per block: measured faster than a persistent grid of the resident blocks.
@@ -356,7 +361,7 @@ int set_up_kernels(fdtd_solver *s) {
     return FDTD_OK;
 }
 
-template <typename T, bool WIDE, bool SCALED>
+template <typename T, bool WIDE, bool SCALED, bool COMP = false>
 int launch_steps(fdtd_solver *s, const float *d_signal, uint64_t steps, double *d_out, uint64_t stride) {
     const Tables &g = s->tables;
     const uint32_t special_blocks = (uint32_t)((s->specials + kBlock - 1) / kBlock);
@@ -407,9 +412,11 @@ int launch_steps(fdtd_solver *s, const float *d_signal, uint64_t steps, double *
         if (s->bulk_blocks) {
             BulkArgs args = s->bulk;
             args.a = f.a;
+            args.d = f.d;
             const int cur = flip ? 0 : 1, prev = flip ? 1 : 0;
-            bulk_kernel<T, WIDE, SCALED><<<s->bulk_blocks, kBlock, smem, s->stream>>>(
-                s->map_b[cur], s->map_a[prev], s->map_t, s->map_s, args);
+            // (Compensated: the increments stand in the previous pressure's place.)
+            bulk_kernel<T, WIDE, SCALED, COMP><<<s->bulk_blocks, kBlock, smem, s->stream>>>(
+                s->map_b[cur], COMP ? s->map_d : s->map_a[prev], s->map_t, s->map_s, args);
         }
         if (ev) CUDA_TRY(s, cudaEventRecord(ev[1], s->stream));
         if (ev) CUDA_TRY(s, cudaEventRecord(ev[2], layer));
@@ -424,15 +431,15 @@ int launch_steps(fdtd_solver *s, const float *d_signal, uint64_t steps, double *
             priority.val.priority = s->layer_priority;
             config.attrs = &priority;
             config.numAttrs = 1;
-            CUDA_TRY(s, cudaLaunchKernelEx(&config, layer_kernel<T, SCALED>, g, f));
+            CUDA_TRY(s, cudaLaunchKernelEx(&config, layer_kernel<T, SCALED, COMP>, g, f));
         }
         if (ev) CUDA_TRY(s, cudaEventRecord(ev[3], layer));
         if (ev) CUDA_TRY(s, cudaEventRecord(ev[4], side));
         if (special_blocks) {
             if (s->link_slots <= 6)
-                special_kernel<T, 6><<<special_blocks, kBlock, 0, side>>>(g, f);
+                special_kernel<T, 6, COMP><<<special_blocks, kBlock, 0, side>>>(g, f);
             else
-                special_kernel<T, 18><<<special_blocks, kBlock, 0, side>>>(g, f);
+                special_kernel<T, 18, COMP><<<special_blocks, kBlock, 0, side>>>(g, f);
         }
         if (ev) CUDA_TRY(s, cudaEventRecord(ev[5], side));
         if (ev) CUDA_TRY(s, cudaEventRecord(ev[6], side));
@@ -453,30 +460,34 @@ int launch_steps(fdtd_solver *s, const float *d_signal, uint64_t steps, double *
     return FDTD_OK;
 }
 
-template <typename T, bool W, bool S>
+template <typename T, bool W, bool S, bool C>
 int dispatch_run(fdtd_solver *s, const float *d_signal, uint64_t steps, double *d_out, uint64_t stride) {
-    return launch_steps<T, W, S>(s, d_signal, steps, d_out, stride);
+    return launch_steps<T, W, S, C>(s, d_signal, steps, d_out, stride);
 }
 
-// The instantiation for the grid: precision, stencil, speed field.
-#define FDTD_BY_KIND(CALL)                                                                          \
-    do {                                                                                            \
-        if (s->precision == FDTD_FP64) {                                                            \
-            if (!s->wide) return s->scaled ? CALL(double, false, true) : CALL(double, false, false); \
-            return s->scaled ? CALL(double, true, true) : CALL(double, true, false);                \
-        }                                                                                           \
-        if (!s->wide) return s->scaled ? CALL(float, false, true) : CALL(float, false, false);      \
-        return s->scaled ? CALL(float, true, true) : CALL(float, true, false);                      \
+// The instantiation for the grid: precision (and compensated single), stencil, speed field.
+#define FDTD_BY_KIND(CALL)                                                                                   \
+    do {                                                                                                     \
+        if (s->precision == FDTD_FP64) {                                                                     \
+            if (!s->wide) return s->scaled ? CALL(double, false, true, false) : CALL(double, false, false, false); \
+            return s->scaled ? CALL(double, true, true, false) : CALL(double, true, false, false);           \
+        }                                                                                                    \
+        if (s->precision == FDTD_FP32_COMPENSATED) {                                                         \
+            if (!s->wide) return s->scaled ? CALL(float, false, true, true) : CALL(float, false, false, true); \
+            return s->scaled ? CALL(float, true, true, true) : CALL(float, true, false, true);               \
+        }                                                                                                    \
+        if (!s->wide) return s->scaled ? CALL(float, false, true, false) : CALL(float, false, false, false); \
+        return s->scaled ? CALL(float, true, true, false) : CALL(float, true, false, false);                 \
     } while (0)
 
 int dispatch(fdtd_solver *s, const float *d_signal, uint64_t steps, double *d_out, uint64_t stride) {
-#define RUN_CALL(T, W, S) dispatch_run<T, W, S>(s, d_signal, steps, d_out, stride)
+#define RUN_CALL(T, W, S, C) dispatch_run<T, W, S, C>(s, d_signal, steps, d_out, stride)
     FDTD_BY_KIND(RUN_CALL);
 #undef RUN_CALL
 }
 
 int set_up(fdtd_solver *s) {
-#define SET_CALL(T, W, S) set_up_kernels<T, W, S>(s)
+#define SET_CALL(T, W, S, C) set_up_kernels<T, W, S, C>(s)
     FDTD_BY_KIND(SET_CALL);
 #undef SET_CALL
 }
@@ -581,6 +592,7 @@ int build(fdtd_solver *s, const fdtd_layout *L) {
         if ((rc = zeros(s, e * L->state_count, &s->w[k]))) return rc;
     }
     if ((rc = zeros(s, e * 3 * L->layer_count, &s->layer_parts))) return rc;
+    if (s->precision == FDTD_FP32_COMPENSATED && (rc = zeros(s, e * s->n_device, &s->increment))) return rc;
     if (L->layer_count)
         for (int k = 0; k < 2; ++k)
             for (int axis = 0; axis < 3; ++axis)
@@ -604,6 +616,8 @@ int build(fdtd_solver *s, const fdtd_layout *L) {
     bk.centre = L->centre;
     bk.total = L->total;
     bk.error = s->d_error;
+    std::vector<float> row_residual(L->special_count);
+    fdtd_compensated_residuals(L, &bk.residual, row_residual.data());
     if (interior) {
         bk.xa = (uint32_t)(x0 / 16 * 16);
         bk.y0 = (uint32_t)y0, bk.z0 = (uint32_t)z0;
@@ -653,6 +667,7 @@ int build(fdtd_solver *s, const fdtd_layout *L) {
             if ((rc = tensor_map(s, &s->map_b[k], s->u[k], ft, (uint32_t)e, kBX, kBY))) return rc;
             if ((rc = tensor_map(s, &s->map_a[k], s->u[k], ft, (uint32_t)e, kTX, kTY))) return rc;
         }
+        if (s->increment && (rc = tensor_map(s, &s->map_d, s->increment, ft, (uint32_t)e, kTX, kTY))) return rc;
         if ((rc = tensor_map(s, &s->map_t, const_cast<uint8_t *>(d_types), CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, kTX, kTY)))
             return rc;
         if ((rc = tensor_map(s, &s->map_s, s->scaled ? const_cast<float *>(d_scale) : s->u[0],
@@ -709,6 +724,10 @@ int build(fdtd_solver *s, const fdtd_layout *L) {
     g.coef_inv = fp;
     if ((rc = upload(s, L->source, K, &fp))) return rc;
     g.source = fp;
+    if (s->precision == FDTD_FP32_COMPENSATED) {
+        if ((rc = upload(s, row_residual.data(), K, &fp))) return rc;
+        g.row_residual = fp;
+    }
     {
         // Each state's branch coefficients gathered per state, as run() gathers them
         // (fdtd.hpp:797-805).
@@ -1349,6 +1368,11 @@ extern "C" {
 
 int fdtd_abi_version(void) { return FDTD_B200_ABI_VERSION; }
 
+#ifndef FDTD_BUILD_ID
+#define FDTD_BUILD_ID "unknown"
+#endif
+const char *fdtd_build_id(void) { return FDTD_BUILD_ID; }
+
 const char *fdtd_global_error(void) { return g_error.c_str(); }
 
 const char *fdtd_last_error(const fdtd_solver *s) { return s ? s->error.c_str() : g_error.c_str(); }
@@ -1384,8 +1408,8 @@ int fdtd_device_name(int device, char *buf, size_t size) {
 int fdtd_create(const fdtd_layout *layout, int precision, int device, fdtd_solver **out) {
     if (!out) return set_global(FDTD_EINVAL, "no place for the handle");
     *out = nullptr;
-    if (precision != FDTD_FP32 && precision != FDTD_FP64)
-        return set_global(FDTD_EINVAL, "precision is FDTD_FP32 or FDTD_FP64");
+    if (precision != FDTD_FP32 && precision != FDTD_FP64 && precision != FDTD_FP32_COMPENSATED)
+        return set_global(FDTD_EINVAL, "precision is FDTD_FP32, FDTD_FP64 or FDTD_FP32_COMPENSATED");
     std::string why;
     if (validate(layout, why) != FDTD_OK) return set_global(FDTD_EINVAL, why);
     int count = 0;
@@ -1544,6 +1568,8 @@ int fdtd_gradient_noalloc(fdtd_solver *s, const float *signal, uint64_t steps, c
                           uint64_t segment, double *grad_coef_b, double *grad_coef_inv, double *grad_now,
                           double *grad_before, double *grad_gain) {
     if (!s) return set_global(FDTD_EINVAL, "no solver");
+    if (s->precision == FDTD_FP32_COMPENSATED)
+        return fail(s, FDTD_EINVAL, "the gradient steps FDTD_FP32 or FDTD_FP64, not the compensated form");
     if (steps == 0) return fail(s, FDTD_EINVAL, "no steps to differentiate");
     if (!signal || (s->probes && !dloss_dy)) return fail(s, FDTD_EINVAL, "no signal or loss gradient");
     DeviceGuard guard(s->device);
@@ -1575,6 +1601,9 @@ int fdtd_gradient_noalloc(fdtd_solver *s, const float *signal, uint64_t steps, c
 int fdtd_set_coefficients(fdtd_solver *s, const float *coef_b, const float *coef_inv, const float *branch_now,
                           const float *branch_before, const float *branch_gain) {
     if (!s) return set_global(FDTD_EINVAL, "no solver");
+    // (The compensated form's row residuals are worked out from the coefficients at creation.)
+    if (s->precision == FDTD_FP32_COMPENSATED)
+        return fail(s, FDTD_EINVAL, "coefficients are set on FDTD_FP32 or FDTD_FP64 handles");
     DeviceGuard guard(s->device);
     const uint64_t K = s->specials, S = s->states;
     for (cudaStream_t stream : {s->stream, s->side, s->layer_stream}) CUDA_TRY(s, cudaStreamSynchronize(stream));
@@ -1612,6 +1641,7 @@ int fdtd_set_coefficients(fdtd_solver *s, const float *coef_b, const float *coef
 
 int fdtd_set_tape(fdtd_solver *s, uint64_t segment) {
     if (!s) return set_global(FDTD_EINVAL, "no solver");
+    if (segment && s->precision == FDTD_FP32_COMPENSATED) return fail(s, FDTD_EINVAL, "the gradient steps FDTD_FP32 or FDTD_FP64, not the compensated form");
     s->tape_segment = segment;
     s->tape_valid = false;
     return FDTD_OK;
@@ -1646,6 +1676,8 @@ int fdtd_get_timing(fdtd_solver *s, double ms[4], uint64_t *steps) {
 int fdtd_gradient(fdtd_solver *s, const float *signal, uint64_t steps, const double *dloss_dy, uint64_t segment,
                   double *grad_coef_b, double *grad_coef_inv, double *grad_now, double *grad_before, double *grad_gain) {
     if (!s) return set_global(FDTD_EINVAL, "no solver");
+    if (s->precision == FDTD_FP32_COMPENSATED)
+        return fail(s, FDTD_EINVAL, "the gradient steps FDTD_FP32 or FDTD_FP64, not the compensated form");
     if (steps == 0) return fail(s, FDTD_EINVAL, "no steps to differentiate");
     if (!signal || (s->probes && !dloss_dy)) return fail(s, FDTD_EINVAL, "no signal or loss gradient");
     DeviceGuard guard(s->device);
@@ -1666,6 +1698,7 @@ int fdtd_reset(fdtd_solver *s) {
         CUDA_TRY(s, cudaMemsetAsync(s->u[k], 0, e * s->n_device, s->stream));
         if (s->states) CUDA_TRY(s, cudaMemsetAsync(s->w[k], 0, e * s->states, s->stream));
     }
+    if (s->increment) CUDA_TRY(s, cudaMemsetAsync(s->increment, 0, e * s->n_device, s->stream));
     if (s->layers) {
         CUDA_TRY(s, cudaMemsetAsync(s->layer_parts, 0, e * 3 * s->layers, s->stream));
         for (int k = 0; k < 2; ++k)
@@ -1711,11 +1744,22 @@ int fdtd_read_state(const fdtd_solver *cs, void *current, void *previous, void *
     // The levels are pitched on the device: their rows of nx cells are copied out one plane of
     // rows at a time.
     void *levels[2] = {current, previous};
-    const void *sources[2] = {s->u[1], s->u[0]};
+    const void *sources[2] = {s->u[1], s->increment ? s->increment : s->u[0]};
+    std::vector<float> here;
+    if (s->increment && previous && !current) {
+        here.resize(s->n);
+        levels[0] = here.data();
+    }
     for (int k = 0; k < 2; ++k) {
         if (!levels[k]) continue;
         CUDA_TRY(s, cudaMemcpy2D(levels[k], e * s->nx, sources[k], e * s->pitch, e * s->nx, s->ny * s->nz,
                                  cudaMemcpyDeviceToHost));
+    }
+    if (s->increment && previous) {
+        // Compensated: the level before is the pressure less its increment.
+        const float *p = static_cast<const float *>(levels[0]);
+        float *q = static_cast<float *>(previous);
+        for (uint64_t i = 0; i < s->n; ++i) q[i] = p[i] - q[i];
     }
     if (branch_current && s->states) CUDA_TRY(s, cudaMemcpy(branch_current, s->w[1], e * s->states, cudaMemcpyDeviceToHost));
     if (branch_previous && s->states) CUDA_TRY(s, cudaMemcpy(branch_previous, s->w[0], e * s->states, cudaMemcpyDeviceToHost));

@@ -14,6 +14,14 @@
 // operands in the reference's order, so with T = float each operation rounds as the reference's
 // -ffp-contract=off build does, subnormal results flushed to zero as its MXCSR flush does
 // (fdtd.hpp:316-336). T = double steps the same layout with every stored coefficient promoted.
+//
+// COMP (compensated single precision, float only) steps the same scheme on the pressure p_n and
+// its increment d_n = p_n - p_(n-1), kept in place of the previous level: with p_(n-1) = p_n - d_n
+// written into the updates, every neighbour enters as a difference (p_m - p_n) and the constant
+// mode's residual (fdtd_compensated.h) times p_n; then p_(n+1) = p_n + d_(n+1). The increment is
+// rounded relative to itself, not to the pressure, so that rounding no longer drives a long run's
+// slow modes. A matched-layer cell carries its pressure on from its own rather than summing its
+// split parts, which grow far beyond the pressure under a net mass.
 #pragma once
 
 #include <cuda.h>
@@ -60,6 +68,8 @@ struct Stage {
 
 struct BulkArgs {
     void *a;  // the previous pressure, overwritten with the next (T)
+    void *d;  // COMP: each cell's increment, updated in place
+    float residual;  // COMP: the constant mode's residual (with a speed field, per unit scale)
     uint32_t pitch, ny;
     uint32_t xa, y0, z0, x1, y1, z1;  // tiles start at xa (16-aligned), y0, z0; the box ends x1, y1, z1
     // The tiles that hold interior cells: {x, y, z0, z_end} each, x 16-aligned; a tile spans
@@ -147,7 +157,7 @@ __device__ __forceinline__ TileSpan tile_span(const BulkArgs &p, uint32_t tile) 
     return TileSpan{t.x, t.y, t.z, t.w};
 }
 
-template <typename T, bool WIDE, bool SCALED>
+template <typename T, bool WIDE, bool SCALED, bool COMP = false>
 __global__ void __launch_bounds__(kBlock) bulk_kernel(const __grid_constant__ CUtensorMap map_b,
                                                       const __grid_constant__ CUtensorMap map_a,
                                                       const __grid_constant__ CUtensorMap map_t,
@@ -176,6 +186,8 @@ __global__ void __launch_bounds__(kBlock) bulk_kernel(const __grid_constant__ CU
     const int xl = threadIdx.x % kTX;
     const int r0 = (threadIdx.x / kTX) * kRowsPerThread;
     T *__restrict__ a = static_cast<T *>(p.a);
+    T *__restrict__ dd = static_cast<T *>(p.d);
+    const T residual = (T)p.residual;
     const uint64_t plane = (uint64_t)p.pitch * p.ny;
     bool ok = true, failed = false;
     int waited = 0;    // stages 0 .. waited-1 complete (this thread's view)
@@ -228,6 +240,30 @@ __global__ void __launch_bounds__(kBlock) bulk_kernel(const __grid_constant__ CU
                     if (pt[c] != kInterior) continue;
                     const int q = (yl + 1) * kBX + (xl + kHX);
                     const T here = b0[q];
+                    const uint64_t at = (uint64_t)x + (uint64_t)(t.yt + yl) * p.pitch + (uint64_t)z * plane;
+                    if (COMP) {
+                        // pa holds the increment; the neighbours as differences, in the sum's order.
+                        const T sum = (b0[q - 1] - here) + (b0[q + 1] - here) + (b0[q - kBX] - here) +
+                                      (b0[q + kBX] - here) + (bm[q] - here) + (bp[q] - here);
+                        T edges = (T)0;
+                        if (WIDE)
+                            edges = (b0[q - 1 - kBX] - here) + (b0[q + 1 - kBX] - here) + (b0[q - 1 + kBX] - here) +
+                                    (b0[q + 1 + kBX] - here) + (bm[q - 1] - here) + (bm[q + 1] - here) +
+                                    (bp[q - 1] - here) + (bp[q + 1] - here) + (bm[q - kBX] - here) +
+                                    (bm[q + kBX] - here) + (bp[q - kBX] - here) + (bp[q + kBX] - here);
+                        T step;
+                        if (SCALED) {
+                            const T sc = (T)ps[c];
+                            step = WIDE ? pa[c] + (sc * axial) * sum + (sc * diagonal) * edges + (sc * residual) * here
+                                        : pa[c] + (sc * axial) * sum + (sc * residual) * here;
+                        } else {
+                            step = WIDE ? pa[c] + axial * sum + diagonal * edges + residual * here
+                                        : pa[c] + axial * sum + residual * here;
+                        }
+                        a[at] = here + step;
+                        dd[at] = step;
+                        continue;
+                    }
                     const T sum = b0[q - 1] + b0[q + 1] + b0[q - kBX] + b0[q + kBX] + bm[q] + bp[q];
                     T next;
                     if (WIDE) {
@@ -248,7 +284,7 @@ __global__ void __launch_bounds__(kBlock) bulk_kernel(const __grid_constant__ CU
                             next = centre * here + axial * sum - pa[c];
                         }
                     }
-                    a[(uint64_t)x + (uint64_t)(t.yt + yl) * p.pitch + (uint64_t)z * plane] = next;
+                    a[at] = next;
                 }
             }
             // Every thread is done with plane z-1's stage; stop the block alike if a wait gave up.
@@ -282,6 +318,7 @@ struct Tables {
     uint32_t link_slots;
     const uint8_t *link_count, *link_direction;
     const float *link_weight, *coef_a, *coef_b, *coef_inv, *source;
+    const float *row_residual;  // COMP: each row's constant-mode residual
     const float *state_weight, *state_now, *state_before, *state_gain;
     int32_t offset[18];
     // Matched layer (fdtd.hpp:2242-2264): cells, and per axis and grid coordinate x (0..n_axis)
@@ -302,6 +339,7 @@ struct Tables {
 template <typename T>
 struct Fields {
     T *a;              // the pressure a step before, overwritten with the next
+    T *d;              // COMP: each cell's increment p_n - p_(n-1), updated in place
     const T *b;        // the current pressure
     T *wa;             // branch velocities a step before, overwritten with the next
     const T *wb;       // current branch velocities
@@ -320,7 +358,7 @@ struct Fields {
 // are coalesced; all of a row's link loads are issued before the sum, which then adds them in
 // the layout's order. A state's term now * wb - before * wa is worked out again for the
 // velocities' update rather than kept: wa has not changed in between, so it is the same value.
-template <typename T, int SLOTS>
+template <typename T, int SLOTS, bool COMP = false>
 __global__ void __launch_bounds__(kBlock) special_kernel(const Tables g, const Fields<T> f) {
     const uint32_t k = blockIdx.x * kBlock + threadIdx.x;
     const uint32_t K = g.specials;
@@ -340,18 +378,31 @@ __global__ void __launch_bounds__(kBlock) special_kernel(const Tables g, const F
             value[l] = b[(uint32_t)((int64_t)i + g.offset[g.link_direction[at]])];
         }
     }
+    const T here = b[i];
     T sum = 0;
 #pragma unroll
     for (int l = 0; l < SLOTS; ++l)
-        if ((uint32_t)l < links) sum += (T)weight[l] * value[l];
+        if ((uint32_t)l < links) sum += COMP ? (T)weight[l] * (value[l] - here) : (T)weight[l] * value[l];
     const uint32_t s0 = g.state_start[k], s1 = g.state_start[k + 1];
     T flow = 0;
     for (uint32_t j = s0; j < s1; ++j) {
         const T own = (T)g.state_now[j] * f.wb[j] - (T)g.state_before[j] * f.wa[j];
         flow += (T)g.state_weight[j] * own;
     }
+    if (COMP) {
+        const T before = f.d[i];
+        const T step = (sum + (T)g.coef_b[k] * before - flow + (T)g.source[k] * (T)f.signal[0]) * (T)g.coef_inv[k] +
+                       (T)g.row_residual[k] * here;
+        f.a[i] = here + step;
+        f.d[i] = step;
+        for (uint32_t j = s0; j < s1; ++j) {
+            const T own = (T)g.state_now[j] * f.wb[j] - (T)g.state_before[j] * f.wa[j];
+            f.wa[j] = f.wa[j] + ((step + before) * (T)g.state_gain[j] + own);
+        }
+        return;
+    }
     const T previous = f.a[i];
-    const T next = ((T)g.coef_a[k] * b[i] + sum - (T)g.coef_b[k] * previous - flow +
+    const T next = ((T)g.coef_a[k] * here + sum - (T)g.coef_b[k] * previous - flow +
                     (T)g.source[k] * (T)f.signal[0]) * (T)g.coef_inv[k];
     f.a[i] = next;
     if (f.traj_u) f.traj_u[k] = next;
@@ -374,7 +425,7 @@ __global__ void __launch_bounds__(kBlock) special_kernel(const Tables g, const F
 // that alternate with the steps: every cell reads the old values of its two faces and works both
 // out again, and writes the new value of its + face, and of its - face too where the cell below
 // is not in the layer (no one else writes that face). The pressure parts stay per cell.
-template <typename T, bool SCALED>
+template <typename T, bool SCALED, bool COMP = false>
 __global__ void __launch_bounds__(kBlock) layer_kernel(const Tables g, const Fields<T> f) {
     const uint32_t c = blockIdx.x * kBlock + threadIdx.x;
     const uint32_t L = g.layers;
@@ -400,6 +451,15 @@ __global__ void __launch_bounds__(kBlock) layer_kernel(const Tables g, const Fie
         f.face_new[axis][i] = above;
         // The cell below owns the face when it is in the layer.
         if (!(shared_below & (1u << axis))) f.face_new[axis][i - stride] = below;
+        if (COMP) {
+            // The parts' sum carried on from the pressure: p + (keep - 1) * part - flux per axis.
+            const T keep = (T)c0.x;
+            const T push = SCALED ? (T)c0.y * scale : (T)c0.y;
+            const T flux = push * (above - below);
+            total += (keep - (T)1) * part[axis] - flux;
+            part[axis] = keep * part[axis] - flux;
+            continue;
+        }
         if (SCALED) {
             part[axis] = (T)c0.x * part[axis] - ((T)c0.y * scale) * (above - below);
         } else {
@@ -409,7 +469,12 @@ __global__ void __launch_bounds__(kBlock) layer_kernel(const Tables g, const Fie
     }
 #pragma unroll
     for (int axis = 0; axis < 3; ++axis) parts[axis * L + c] = part[axis];
-    f.a[i] = total;
+    if (COMP) {
+        f.a[i] = here + total;
+        f.d[i] = total;  // (read by no update; it keeps the state's level before readable)
+    } else {
+        f.a[i] = total;
+    }
 }
 
 // Probe p's pressure before the step (fdtd.hpp:3525-3533): its cells' weighted sum in double, in

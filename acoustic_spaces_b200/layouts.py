@@ -816,6 +816,53 @@ def porous_ground(flow_resistivity: float, rate: float, *, poles: int = 3, band=
     return Material(float(coef[0]), np.vstack(branches) if branches else np.zeros((0, 3)))
 
 
+def shoebox_room(
+    seed: int = 0,
+    *,
+    size=(6.0, 4.0, 3.0),
+    cell: float = 0.05,
+    speed: float = 0.99,
+    absorption=(0.05, 0.3),
+    steps: int = 4000,
+    speed_of_sound: float = 343.0,
+) -> Workload:
+    """A closed box of ``size`` metres on cells of ``cell`` metres, laid out as the reference's
+    tests lay a box out (two cells of margin); its six walls each a real admittance from an
+    absorption uniform in ``absorption`` (Paris's formula); a uniform speed ratio ``speed`` (the
+    Courant number speed / sqrt(3)), the grid's rate such that the sound travels at
+    ``speed_of_sound``; one source and one receiver at seeded points 0.5 m from every wall; a 0.5 ms
+    Gaussian drive."""
+    rng = np.random.default_rng(seed)
+    rate = speed_of_sound / (speed * COURANT * cell)
+    betas = paris_admittance(rng.uniform(absorption[0], absorption[1], 6))
+    room = shoebox(np.asarray(size, float), [Material(float(b)) for b in betas])
+    points = inside_points(rng, room, np.asarray(size, float), 2, 0.5, apart=4 * cell)
+    grid = room_grid(np.asarray(size, float), cell)
+    built = cell_face_layout(room, grid, points[0], points[1:], speed=speed, rate=rate)
+    lay = built.layout
+    description = {
+        "room": f"box {size[0]:g}x{size[1]:g}x{size[2]:g} m, real admittance per wall from absorption U[%g, %g]"
+        % absorption,
+        "grid": "x".join(str(v) for v in grid.shape),
+        "cell_m": cell,
+        "cells": grid.n,
+        "air_cells": built.air_cells,
+        "interior_cells": int(np.count_nonzero(lay["types"] == 1)),
+        "special_rows": len(lay["special"]),
+        "links": len(lay["link_direction"]),
+        "branch_states": len(lay["state_branch"]),
+        "layer_cells": 0,
+        "probes": 1,
+        "steps": steps,
+        "rate_hz": rate,
+        "speed_ratio": speed,
+        "walls": "cell faces, real admittance",
+        "stencil": 7,
+        "seed": seed,
+    }
+    return Workload("shoebox_room", room, built, points[0], points[1:], gaussian_drive(rate, steps), description)
+
+
 def outdoor_halfspace(
     seed: int = 0,
     *,

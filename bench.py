@@ -53,14 +53,53 @@ BYTES_STATE = 28  # read/write w-, read w, its four coefficients
 BYTES_LAYER = 60  # read p, write p+, read/write three parts, read/write three faces, its index
 
 
-def algorithmic_bytes(d: dict) -> int:
-    return (
-        BYTES_INTERIOR * d["interior_cells"]
-        + BYTES_SPECIAL * d["special_rows"]
+# Compensated single precision moves each cell's increment besides its pressure: an interior cell
+# reads p and its increment and writes both (16 B); a special row reads and writes the increment
+# in place of reading and writing p- and writes p+ (+4 B); a layer cell writes its increment (+4 B).
+EXTRA_COMPENSATED = {"interior": 4, "special": 4, "layer": 4}
+
+
+def kind_bytes(d: dict, precision: str = "fp32") -> dict:
+    """Each step kernel's algorithmic bytes per launch."""
+    extra = EXTRA_COMPENSATED if precision == "fp32c" else {"interior": 0, "special": 0, "layer": 0}
+    return {
+        "bulk": (BYTES_INTERIOR + extra["interior"]) * d["interior_cells"],
+        "layer": (BYTES_LAYER + extra["layer"]) * d["layer_cells"],
+        "special": (BYTES_SPECIAL + extra["special"]) * d["special_rows"]
         + BYTES_LINK * d["links"]
-        + BYTES_STATE * d["branch_states"]
-        + BYTES_LAYER * d["layer_cells"]
-    )
+        + BYTES_STATE * d["branch_states"],
+    }
+
+
+def algorithmic_bytes(d: dict, precision: str = "fp32") -> int:
+    return sum(kind_bytes(d, precision).values())
+
+
+def decay_times(p: np.ndarray, rate: float) -> tuple[float, float]:
+    """EDT and T30 (s) of one receiver's broadband response: the backward-integrated (Schroeder)
+    decay of p^2 in dB, a least-squares line from its first sample at or below 0 dB (EDT) or -5 dB
+    (T30) to its first at or below -10 or -35 dB, -60 dB over its slope (the ranges of ISO 3382,
+    as src/acoustic_spaces/parameters.py:55 and :266-296 of the reference fit them, here without
+    its estimate of the energy past the response's end). NaN where the curve does not fall so far."""
+    e = np.cumsum((p * p)[::-1])[::-1]
+    if e[0] <= 0:
+        return float("nan"), float("nan")
+    with np.errstate(divide="ignore"):
+        level = 10.0 * np.log10(np.maximum(e, 0.0) / e[0])
+    t = np.arange(len(p)) / rate
+    out = []
+    for top, bottom in ((0.0, -10.0), (-5.0, -35.0)):
+        below = level <= bottom
+        if not below.any() or not np.isfinite(level[int(np.argmax(below))]):
+            out.append(float("nan"))
+            continue
+        start, stop = int(np.argmax(level <= top)), int(np.argmax(below))
+        if stop - start < 2:
+            out.append(float("nan"))
+            continue
+        slope = np.polyfit(t[start : stop + 1], level[start : stop + 1], 1)[0]
+        out.append(float(-60.0 / slope) if slope < 0 else float("nan"))
+    return out[0], out[1]
 
 
 def ir_errors(p32: np.ndarray, p64: np.ndarray, rate: float) -> dict:
@@ -70,6 +109,18 @@ def ir_errors(p32: np.ndarray, p64: np.ndarray, rate: float) -> dict:
     energy = np.linalg.norm(p64, axis=1)
     reached = energy > 1e-3 * energy.max()  # receivers the sound has reached
     rel = np.linalg.norm(p32 - p64, axis=1)[reached] / energy[reached]
+    # The same after removing each receiver's mean (a Gaussian drive's net mass shows as one).
+    d = p32 - p64
+    d = d - d.mean(axis=1, keepdims=True)
+    q = p64 - p64.mean(axis=1, keepdims=True)
+    rel_demeaned = np.linalg.norm(d, axis=1)[reached] / np.linalg.norm(q, axis=1)[reached]
+    edt_err, t30_err = [], []
+    for a, b in zip(p32[reached], p64[reached]):
+        (ea, ta), (eb, tb) = decay_times(a, rate), decay_times(b, rate)
+        if np.isfinite(ea) and np.isfinite(eb):
+            edt_err.append(abs(ea - eb) / eb)
+        if np.isfinite(ta) and np.isfinite(tb):
+            t30_err.append(abs(ta - tb) / tb)
     worst_db = 0.0
     for a, b in zip(p32[reached], p64[reached]):
         ea = np.cumsum((a * a)[::-1])[::-1]
@@ -82,6 +133,10 @@ def ir_errors(p32: np.ndarray, p64: np.ndarray, rate: float) -> dict:
     return {
         "ir_rel_l2_max": float(rel.max()),
         "ir_rel_l2_median": float(np.median(rel)),
+        "ir_rel_l2_demeaned_max": float(rel_demeaned.max()),
+        "edt_rel_max": float(max(edt_err)) if edt_err else None,
+        "t30_rel_max": float(max(t30_err)) if t30_err else None,
+        "t30_receivers": len(t30_err),
         "edc_db_max_abs": worst_db,
         "seconds": float(p64.shape[1] / rate),
         "receivers": int(reached.sum()),
@@ -163,7 +218,7 @@ def build_workload(args, barrier: bool = True):
 
     if args.workload == "outdoor_halfspace":
         return layouts.outdoor_halfspace(args.seed, steps=max(args.steps, args.ir_steps), barrier=barrier)
-    return layouts.polyhedral_room(args.seed, cell=args.cell, steps=max(args.steps, 1))
+    return layouts.polyhedral_room(args.seed, cell=args.cell, steps=max(args.steps, args.ir_steps, 1))
 
 
 def insertion_loss(free: np.ndarray, screened: np.ndarray, rate: float, band=(20.0, 300.0)) -> tuple[np.ndarray, np.ndarray]:
@@ -410,6 +465,88 @@ def run_batched(args, world: int, rank: int, local: int) -> None:
         dist.destroy_process_group()
 
 
+def run_shoebox(args, world: int, rank: int, local: int) -> None:
+    """The plain FP64 box (6 x 4 x 3 m at 5 cm, Courant 0.99/sqrt(3), six real walls, one source
+    and one receiver, 4000 steps): the configuration the reference runs on its CPU. The B200 steps
+    it in FP64 (device time, and end to end through the API) and must equal the FP64 oracle (its C
+    port, one core, timed) to the bit; beside them the reference's own FP32 solver on all host
+    threads."""
+    import torch
+
+    from acoustic_spaces_b200 import B200WaveSolver, layouts
+    from oracle import oracle
+
+    w = layouts.shoebox_room(args.seed, steps=args.shoebox_steps)
+    steps = len(w.signal)
+    air = w.built.air_cells
+    solver = B200WaveSolver(w.built.layout, precision="fp64", device=local)
+    sig = torch.from_numpy(np.ascontiguousarray(w.signal)).to(f"cuda:{local}")
+    out = torch.zeros((solver.probes, steps), dtype=torch.float64, device=f"cuda:{local}")
+    stream = torch.cuda.ExternalStream(solver.stream, device=f"cuda:{local}")
+    solver.run_device(sig.data_ptr(), args.warmup, out.data_ptr(), steps)
+    solver.synchronize()
+    solver.reset()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clocks:
+        torch.cuda.synchronize()
+        start.record(stream)
+        solver.run_device(sig.data_ptr(), steps, out.data_ptr(), steps)
+        end.record(stream)
+        solver.synchronize()
+    ms = start.elapsed_time(end)
+    solver.reset()
+    t0 = time.perf_counter()
+    ours = solver.run(w.signal)
+    e2e_s = time.perf_counter() - t0
+    ported = oracle.OracleSolver(w.built.layout, "fp64")
+    t0 = time.perf_counter()
+    theirs = ported.run(w.signal)
+    port_s = time.perf_counter() - t0
+    reference = None
+    native = oracle.reference_native()
+    if native is not None:
+        vertices, faces, owner = layouts.room_mesh(w.room)
+        beta = np.array([m.beta for m in w.room.materials])
+        threads = os.cpu_count() or 1
+        ref = native.WaveSolver(
+            native.Bvh(vertices, faces), owner, beta, np.zeros((0, 3)), np.zeros(0, np.int64), w.built.grid.origin,
+            w.built.grid.cell, *w.built.grid.shape, w.source, w.receivers, layer=0, layer_damping=0.0,
+            threads=threads, speed=np.full(w.built.grid.n, w.description["speed_ratio"], np.float32),
+        )  # fmt: skip
+        t0 = time.perf_counter()
+        ref_series = ref.run(w.signal)
+        ref_s = time.perf_counter() - t0
+        reference = {"value": round(air * steps / ref_s / 1e9, 4), "unit": UNIT, "cores": int(ref.threads),
+                     "kind": "reference", "precision": "FP32 (the reference's)",
+                     "sample": f"all {steps} steps", "rel_l2_vs_fp64": float(np.linalg.norm(ref_series - theirs)
+                                                                             / np.linalg.norm(theirs))}  # fmt: skip
+    line = {
+        "metric": METRIC,
+        "value": round(air * steps / (ms / 1e3) / 1e9, 4),
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(ms / steps, 5),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": "shoebox_room", **w.description, "precision": "FP64 (bit-exact with the FP64 oracle)"},
+        "e2e": {"value": round(air * steps / e2e_s / 1e9, 4), "unit": UNIT, "h2d_bytes_per_step": 4,
+                "d2h_bytes_per_step": 8 * solver.probes},  # fmt: skip
+        "bit_exact_vs_fp64_oracle": bool(np.array_equal(ours, theirs)),
+        "cpu_baseline": {"value": round(air * steps / port_s / 1e9, 4), "unit": UNIT, "cores": 1, "kind": "port",
+                         "precision": "FP64", "sample": f"all {steps} steps"},  # fmt: skip
+        "reference_cpu": reference,
+        "clocks": clocks.summary(),
+        "gpu_launches": 3 * steps,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def run_adjoint(args, world: int, rank: int, local: int) -> None:
     """The adjoint fit: a 10 x 8 x 4 m room at 5 cm cells with 8
     materials on seeded patches, a 1-pole admittance each (16 parameters); the misfit of the
@@ -516,13 +653,17 @@ def main() -> None:
     parser.add_argument("--impl", choices=["b200", "reference"], default="b200")
     parser.add_argument("--seed", type=int, default=0)
     parser.add_argument("--cell", type=float, default=0.04, help="cell size in metres (0.04: the full workload)")
+    parser.add_argument("--no-fp64-rate", action="store_true", help="skip timing the FP64 stepper alike")
+    parser.add_argument("--precision", choices=["fp32", "fp32c"], default="fp32",
+                        help="fp32: the reference's arithmetic; fp32c: compensated single precision")  # fmt: skip
     parser.add_argument("--cpu-steps", type=int, default=10, help="steps of the CPU-baseline sample")
     parser.add_argument("--reference-steps", type=int, default=10)
     parser.add_argument("--reference-repeats", type=int, default=3)
     parser.add_argument("--no-cpu-baseline", action="store_true")
     parser.add_argument("--no-e2e", action="store_true")
-    parser.add_argument("--workload", choices=["polyhedral_room", "outdoor_halfspace", "batched_rooms", "adjoint_fit"],
-                        default="polyhedral_room")  # fmt: skip
+    parser.add_argument("--workload", choices=["polyhedral_room", "outdoor_halfspace", "batched_rooms", "adjoint_fit",
+                                               "shoebox_room"], default="polyhedral_room")  # fmt: skip
+    parser.add_argument("--shoebox-steps", type=int, default=4000)
     parser.add_argument("--adjoint-steps", type=int, default=3000)
     parser.add_argument("--adam-iterations", type=int, default=300)
     parser.add_argument("--rooms", type=int, default=64)
@@ -555,6 +696,9 @@ def main() -> None:
     if args.workload == "adjoint_fit":
         run_adjoint(args, world, rank, local)
         return
+    if args.workload == "shoebox_room":
+        run_shoebox(args, world, rank, local)
+        return
     if world > 1:
         from datetime import timedelta
 
@@ -566,7 +710,7 @@ def main() -> None:
 
     workload = build_workload(args)
     desc = workload.description
-    solver = B200WaveSolver(workload.built.layout, device=local)
+    solver = B200WaveSolver(workload.built.layout, precision=args.precision, device=local)
     air = solver.air_cells
     probes = solver.probes
     steps, warmup = args.steps, args.warmup
@@ -636,6 +780,22 @@ def main() -> None:
             "api": "B200WaveSolver.run(host float32 drive) -> host float64 (probes, steps)",
         }
 
+    # The plain FP64 stepper on the same GPU and grid, timed alike: the accurate mode to beat.
+    fp64_rate = None
+    if not args.no_fp64_rate:
+        fp64 = B200WaveSolver(workload.built.layout, precision="fp64", device=local)
+        fp64.run_device(sig_dev.data_ptr(), warmup, out_dev.data_ptr(), steps + warmup)
+        fp64.synchronize()
+        s64 = torch.cuda.ExternalStream(fp64.stream, device=f"cuda:{local}")
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s64)
+        fp64.run_device(sig_dev.data_ptr() + 4 * warmup, steps, out_dev.data_ptr() + 8 * warmup, steps + warmup)
+        e1.record(s64)
+        fp64.synchronize()
+        fp64.close()
+        fp64_rate = {"value": round(air * steps / (e0.elapsed_time(e1) / 1e3) / 1e9, 4), "unit": UNIT,
+                     "what": "the same grid stepped in FP64 on the same GPU, device-timed alike"}  # fmt: skip
+
     # The IR error against FP64 on the same grid: both run from rest over the same drive.
     ir_error = None
     if not args.no_ir_error:
@@ -652,17 +812,14 @@ def main() -> None:
     if args.workload == "outdoor_halfspace" and not args.no_ir_error:
         insertion = outdoor_insertion_loss(args, workload, local)
 
-    bytes_per_step = algorithmic_bytes(desc)
+    bytes_per_step = algorithmic_bytes(desc, args.precision)
     peak, peak_source = measured_peaks()
     achieved = bytes_per_step / (ms / 1e3 / steps) / 1e9
     # Each kernel's algorithmic bytes per launch and its average launch time, live.
-    per_kernel_bytes = {
-        "bulk": BYTES_INTERIOR * desc["interior_cells"],
-        "layer": BYTES_LAYER * desc["layer_cells"],
-        "special": BYTES_SPECIAL * desc["special_rows"] + BYTES_LINK * desc["links"] + BYTES_STATE * desc["branch_states"],
-    }
+    per_kernel_bytes = kind_bytes(desc, args.precision)
     traffic_table = {}
-    traffic_file = ROOT / "profiles" / f"kernel_traffic_{args.workload}.json"
+    suffix = "" if args.precision == "fp32" else f"_{args.precision}"
+    traffic_file = ROOT / "profiles" / f"kernel_traffic_{args.workload}{suffix}.json"
     if traffic_file.exists() and (args.cell == 0.04 or args.workload != "polyhedral_room"):
         traffic_table = json.loads(traffic_file.read_text()).get("dram_bytes_per_launch", {})
     kernels = {}
@@ -709,7 +866,9 @@ def main() -> None:
                 "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                 "l2": "inputs larger than L2 (two pressure levels alone are "
                 f"{2 * 4 * desc['cells'] / 1e6:.0f} MB vs 126 MB L2), no flush",
-                "precision": "FP32, bit-exact with the reference (no FMA, subnormals flushed)",
+                "precision": "FP32, bit-exact with the reference (no FMA, subnormals flushed)"
+                if args.precision == "fp32"
+                else "FP32 compensated: each cell's pressure and its increment (not bit-equal to the reference)",
             },
             "e2e": e2e,
             "gpu_launches": launches_per_step * steps,
@@ -733,6 +892,7 @@ def main() -> None:
             },
             "cpu_baseline": cpu,
             "ir_error_vs_fp64": ir_error,
+            "fp64_same_gpu": fp64_rate,
             "insertion_loss_vs_fp64": insertion,
             "adjoint_over_forward": None,
             "clocks": clocks.summary(),

@@ -46,6 +46,18 @@ extern "C" {
 /* Arithmetic of the fields. */
 #define FDTD_FP32 0
 #define FDTD_FP64 1
+/*
+ * Compensated single precision (no counterpart in the reference): the same scheme in float,
+ * stepped on each cell's pressure and its increment p_n - p_(n-1) (kept in place of the previous
+ * level), every neighbour entering as a difference from the cell's own pressure, and the matched
+ * layer's pressure carried on from its own rather than summed from its split parts. Rounding is
+ * then relative to the increments, not to the pressures, so that long runs of rooms with a net
+ * mass or an open face into the layer stay close to FDTD_FP64, at 16 bytes of traffic per
+ * interior cell and step against FDTD_FP32's 12 and FDTD_FP64's 24. Not bit-equal to the
+ * reference; fdtd_gradient, fdtd_set_tape and fdtd_set_coefficients refuse it. fdtd_read_state's
+ * previous level is the pressure less its increment.
+ */
+#define FDTD_FP32_COMPENSATED 2
 
 /*
  * The grid's layout, named after WaveSolver::layout()'s arrays (fdtd.hpp:727-782). Counts are
@@ -110,7 +122,7 @@ typedef struct fdtd_info {
     uint64_t probes;
     uint64_t steps_done;     /* steps since creation or the last reset */
     uint64_t device_bytes;   /* device memory the handle holds */
-    int32_t precision;       /* FDTD_FP32 or FDTD_FP64 */
+    int32_t precision;       /* FDTD_FP32, FDTD_FP64 or FDTD_FP32_COMPENSATED */
     int32_t device;          /* CUDA ordinal */
 } fdtd_info;
 
@@ -118,7 +130,8 @@ typedef struct fdtd_info {
  * Replaces engine/gpu.py:GpuWaveSolver.__init__ (engine/gpu.py:449-540), which packs
  * solver.layout() into WebGPU buffers: copies `layout` to device `device` and creates a solver at
  * rest (both pressure levels, branch velocities and matched-layer state zero).
- * precision: FDTD_FP32 or FDTD_FP64. On failure *out is NULL and fdtd_global_error() says why.
+ * precision: FDTD_FP32, FDTD_FP64 or FDTD_FP32_COMPENSATED. On failure *out is NULL and
+ * fdtd_global_error() says why.
  */
 int fdtd_create(const fdtd_layout *layout, int precision, int device, fdtd_solver **out);
 
@@ -258,6 +271,10 @@ int fdtd_device_count(void);
 
 /* FDTD_B200_ABI_VERSION of the library. */
 int fdtd_abi_version(void);
+
+/* A digest of the sources and flags the library was built from (no counterpart in the
+ * reference): the Python loader refuses a library whose digest is not its sources'. */
+const char *fdtd_build_id(void);
 
 #ifdef __cplusplus
 }

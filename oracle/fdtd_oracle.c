@@ -4,6 +4,7 @@
  * naelolaiz/acoustic-spaces). Built with -ffp-contract=off so that no multiply-add is fused.
  */
 #include "fdtd_oracle.h"
+#include "../acoustic_spaces_b200/csrc/fdtd_compensated.h"
 
 #include <stdio.h>
 #include <stdlib.h>
@@ -52,6 +53,10 @@ struct oracle_solver {
     void *u0, *u1, *w0, *w1;
     void *layer_state; /* 9 per layer cell */
     void *term;        /* each state's term of the step */
+    /* ORACLE_FP32C: each cell's increment p_n - p_(n-1) (the previous level is not kept), and
+       the residuals of the constant mode (compensated_residuals) */
+    float *increment;
+    float residual, *row_residual;
 };
 
 static void *dup(const void *src, size_t bytes) {
@@ -62,7 +67,8 @@ static void *dup(const void *src, size_t bytes) {
 
 int oracle_create(const fdtd_layout *L, int precision, oracle_solver **out) {
     *out = NULL;
-    if (precision != ORACLE_FP32 && precision != ORACLE_FP64) return fail("precision is FP32 or FP64");
+    if (precision != ORACLE_FP32 && precision != ORACLE_FP64 && precision != ORACLE_FP32C)
+        return fail("precision is FP32, FP64 or FP32 compensated");
     if (L->stencil != 7 && L->stencil != 19) return fail("the stencil has 7 or 19 points");
     if (L->flow_count) return fail("moving air is stepped on the CPU only");
     oracle_solver *s = calloc(1, sizeof *s);
@@ -114,7 +120,12 @@ int oracle_create(const fdtd_layout *L, int precision, oracle_solver **out) {
     s->probe_weights = dup(L->probe_weights, 8 * pc);
     for (int k = 0; k < 18; ++k)
         s->offset[k] = kSteps[k][0] + kSteps[k][1] * (int64_t)s->sy + kSteps[k][2] * (int64_t)s->sz;
-    const size_t e = precision == ORACLE_FP32 ? 4 : 8;
+    const size_t e = precision == ORACLE_FP64 ? 8 : 4;
+    if (precision == ORACLE_FP32C) {
+        s->increment = calloc(s->n + 1, 4);
+        s->row_residual = malloc(4 * s->specials + 4);
+        fdtd_compensated_residuals(L, &s->residual, s->row_residual);
+    }
     s->u0 = calloc(s->n + 1, e);
     s->u1 = calloc(s->n + 1, e);
     s->w0 = calloc(s->states + 1, e);
@@ -219,13 +230,114 @@ int oracle_create(const fdtd_layout *L, int precision, oracle_solver **out) {
 DEFINE_STEPPER(float, step_fp32)
 DEFINE_STEPPER(double, step_fp64)
 
+/*
+ * ORACLE_FP32C: the same scheme in exact arithmetic, stepped in float on the pressure p_n and its
+ * increment d_n = p_n - p_(n-1), kept in place of the previous level. Substituting p_(n-1) =
+ * p_n - d_n into the updates above gives d_(n+1) as a sum of neighbour differences (p_m - p_n),
+ * d_n and the drive, plus the constant mode's residual times p_n (zero when the coefficients
+ * hold a constant pressure still, and worked out in double from the stored coefficients);
+ * p_(n+1) = p_n + d_(n+1). The increment, the velocity of the scheme, is then rounded relative to
+ * itself rather than to the pressure, so that rounding no longer drives the slow modes of a long
+ * run. The operation order here is the GPU's compensated kernels' (fdtd_kernels.cuh).
+ */
+static void step_fp32c(oracle_solver *s, const float *signal, uint64_t steps, double *out) {
+    float *a = (float *)s->u0, *b = (float *)s->u1, *wa = (float *)s->w0, *wb = (float *)s->w1;
+    float *term = (float *)s->term, *lstate = (float *)s->layer_state, *d = s->increment;
+    const uint64_t sy = s->sy, sz = s->sz, n = s->n;
+    const float axial = s->axial, diagonal = s->diagonal, residual = s->residual;
+    for (uint64_t step = 0; step < steps; ++step) {
+        for (uint64_t p = 0; p < s->probes; ++p) {
+            double value = 0.0;
+            for (uint64_t k = s->probe_start[p]; k < s->probe_start[p + 1]; ++k)
+                value += s->probe_weights[k] * (double)b[s->probe_cells[k]];
+            out[p * steps + step] = value;
+        }
+        for (uint64_t i = 0; i < n; ++i) {
+            if (s->types[i] != 1) continue;
+            const float here = b[i];
+            const float sum = (b[i - 1] - here) + (b[i + 1] - here) + (b[i - sy] - here) + (b[i + sy] - here) +
+                              (b[i - sz] - here) + (b[i + sz] - here);
+            float edges = 0.0f;
+            if (s->wide)
+                edges = (b[i - 1 - sy] - here) + (b[i + 1 - sy] - here) + (b[i - 1 + sy] - here) +
+                        (b[i + 1 + sy] - here) + (b[i - 1 - sz] - here) + (b[i + 1 - sz] - here) +
+                        (b[i - 1 + sz] - here) + (b[i + 1 + sz] - here) + (b[i - sy - sz] - here) +
+                        (b[i + sy - sz] - here) + (b[i - sy + sz] - here) + (b[i + sy + sz] - here);
+            float next;
+            if (s->scaled) {
+                const float sc = s->scale[i];
+                next = s->wide ? d[i] + (sc * axial) * sum + (sc * diagonal) * edges + (sc * residual) * here
+                               : d[i] + (sc * axial) * sum + (sc * residual) * here;
+            } else {
+                next = s->wide ? d[i] + axial * sum + diagonal * edges + residual * here
+                               : d[i] + axial * sum + residual * here;
+            }
+            a[i] = here + next;
+            d[i] = next;
+        }
+        const float sig = signal[step];
+        for (uint64_t k = 0; k < s->specials; ++k) {
+            const uint64_t i = (uint64_t)s->special[k];
+            const float here = b[i];
+            float sum = 0.0f;
+            for (uint64_t l = s->link_start[k]; l < s->link_start[k + 1]; ++l)
+                sum += s->link_weight[l] * (b[(int64_t)i + s->offset[s->link_direction[l]]] - here);
+            float flow = 0.0f;
+            for (uint64_t j = s->state_start[k]; j < s->state_start[k + 1]; ++j) {
+                const float own = s->state_now[j] * wb[j] - s->state_before[j] * wa[j];
+                term[j] = own;
+                flow += s->state_weight[j] * own;
+            }
+            const float before = d[i];
+            const float next = (sum + s->coef_b[k] * before - flow + s->source[k] * sig) * s->coef_inv[k] +
+                               s->row_residual[k] * here;
+            a[i] = here + next;
+            d[i] = next;
+            for (uint64_t j = s->state_start[k]; j < s->state_start[k + 1]; ++j)
+                wa[j] += (next + before) * s->state_gain[j] + term[j];
+        }
+        /* The matched layer: the parts and faces as the reference updates them, but the cell's
+           pressure carried on from its own, p + sum over axes of (keep - 1) * part - push * (above -
+           below), the parts' sum in exact arithmetic: a part along an undamped axis (keep 1) then
+           drops out, and with it the rounding of parts that grow far beyond the pressure. */
+        for (uint64_t c = 0; c < s->layers; ++c) {
+            const uint64_t i = (uint64_t)s->layer_cells[c];
+            const uint64_t at[3] = {i % s->nx, (i / s->nx) % s->ny, i / sz};
+            float *st = lstate + 9 * c;
+            const float here = b[i];
+            float change = 0.0f;
+            for (int axis = 0; axis < 3; ++axis) {
+                const uint64_t stride = axis == 0 ? 1 : (axis == 1 ? sy : sz);
+                const uint64_t x = at[axis];
+                const float *fk = s->keep[2 * axis + 1], *fp = s->push[2 * axis + 1];
+                float *below = &st[3 + 2 * axis], *above = &st[4 + 2 * axis];
+                *below = fk[x] * *below - fp[x] * (here - b[i - stride]);
+                *above = fk[x + 1] * *above - fp[x + 1] * (b[i + stride] - here);
+                float *part = &st[axis];
+                const float keep = s->keep[2 * axis][x];
+                const float push = s->scaled ? s->push[2 * axis][x] * s->layer_scale[c] : s->push[2 * axis][x];
+                const float flux = push * (*above - *below);
+                change += (keep - 1.0f) * *part - flux;
+                *part = keep * *part - flux;
+            }
+            a[i] = here + change;
+            d[i] = change;
+        }
+        float *t = a; a = b; b = t;
+        t = wa; wa = wb; wb = t;
+    }
+}
+
 int oracle_run(oracle_solver *s, const float *signal, uint64_t steps, double *out) {
-    if (s->precision == ORACLE_FP32) {
+    if (s->precision != ORACLE_FP64) {
 #ifdef ORACLE_HAS_MXCSR
         const unsigned saved = _mm_getcsr();
         _mm_setcsr(saved | 0x8040u); /* flush to zero, denormals are zero (fdtd.hpp:316-336) */
 #endif
-        step_fp32(s, signal, steps, out);
+        if (s->precision == ORACLE_FP32C)
+            step_fp32c(s, signal, steps, out);
+        else
+            step_fp32(s, signal, steps, out);
 #ifdef ORACLE_HAS_MXCSR
         _mm_setcsr(saved);
 #endif
@@ -241,7 +353,8 @@ int oracle_run(oracle_solver *s, const float *signal, uint64_t steps, double *ou
 }
 
 int oracle_reset(oracle_solver *s) {
-    const size_t e = s->precision == ORACLE_FP32 ? 4 : 8;
+    const size_t e = s->precision == ORACLE_FP64 ? 8 : 4;
+    if (s->increment) memset(s->increment, 0, 4 * s->n);
     memset(s->u0, 0, e * s->n);
     memset(s->u1, 0, e * s->n);
     memset(s->w0, 0, e * s->states);
@@ -252,9 +365,14 @@ int oracle_reset(oracle_solver *s) {
 
 int oracle_read_state(const oracle_solver *s, void *current, void *previous, void *branch_current,
                       void *branch_previous, void *layer_state) {
-    const size_t e = s->precision == ORACLE_FP32 ? 4 : 8;
+    const size_t e = s->precision == ORACLE_FP64 ? 8 : 4;
     if (current) memcpy(current, s->u1, e * s->n);
-    if (previous) memcpy(previous, s->u0, e * s->n);
+    if (previous && s->increment) {
+        /* the level before, as the pressure less its increment */
+        for (uint64_t i = 0; i < s->n; ++i) ((float *)previous)[i] = ((const float *)s->u1)[i] - s->increment[i];
+    } else if (previous) {
+        memcpy(previous, s->u0, e * s->n);
+    }
     if (branch_current) memcpy(branch_current, s->w1, e * s->states);
     if (branch_previous) memcpy(branch_previous, s->w0, e * s->states);
     if (layer_state) memcpy(layer_state, s->layer_state, e * 9 * s->layers);
@@ -267,7 +385,7 @@ void oracle_destroy(oracle_solver *s) {
                     s->probe_start, s->probe_cells, s->link_direction, s->link_weight, s->coef_a,
                     s->coef_b, s->coef_inv, s->source, s->state_weight, s->state_now,
                     s->state_before, s->state_gain, s->layer_cells, s->probe_weights, s->u0,
-                    s->u1, s->w0, s->w1, s->layer_state, s->term};
+                    s->u1, s->w0, s->w1, s->layer_state, s->term, s->increment, s->row_residual};
     for (size_t k = 0; k < sizeof ptrs / sizeof ptrs[0]; ++k) free(ptrs[k]);
     for (int k = 0; k < 6; ++k) free(s->keep[k]), free(s->push[k]);
     free(s);

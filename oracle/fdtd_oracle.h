@@ -12,7 +12,9 @@
  *   swap       fdtd.hpp:884-885, parity swap at the end fdtd.hpp:900-903
  * ORACLE_FP32 flushes subnormal results to zero as the reference does (FlushDenormals,
  * fdtd.hpp:316-336) and equals the reference bit for bit; ORACLE_FP64 steps the same layout in
- * double (every stored coefficient promoted, no flush): the FP64 oracle.
+ * double (every stored coefficient promoted, no flush): the FP64 oracle. ORACLE_FP32C is no
+ * restatement: it steps the same scheme in this project's compensated single precision
+ * (FDTD_FP32_COMPENSATED), operation for operation as the GPU does, as that mode's checker.
  * Parity of this restatement is pinned against the reference's own run() (compiled from its
  * unmodified headers, oracle/_ref) by the tests and by the golden fixtures under tests/golden.
  */
@@ -29,6 +31,7 @@ extern "C" {
 
 #define ORACLE_FP32 0
 #define ORACLE_FP64 1
+#define ORACLE_FP32C 2 /* the GPU's FDTD_FP32_COMPENSATED, its checker */
 
 typedef struct oracle_solver oracle_solver;
 

@@ -38,6 +38,8 @@ ORACLE_SO = HERE / "libfdtd_oracle.so"
 
 ORACLE_FP32 = 0
 ORACLE_FP64 = 1
+ORACLE_FP32C = 2
+PRECISIONS = {"fp32": ORACLE_FP32, "fp64": ORACLE_FP64, "fp32c": ORACLE_FP32C}
 
 
 def build(reference: bool = True) -> None:
@@ -88,7 +90,7 @@ class OracleSolver:
         packed, arrays = pack_layout(layout)
         handle = ctypes.c_void_p()
         status = lib.oracle_create(
-            ctypes.byref(packed), ORACLE_FP64 if precision == "fp64" else ORACLE_FP32, ctypes.byref(handle)
+            ctypes.byref(packed), PRECISIONS[precision], ctypes.byref(handle)
         )
         del arrays
         if status != 0:

@@ -108,6 +108,27 @@ def test_the_builder_refuses_a_probe_next_to_the_source():
         L.cell_face_layout(room, grid, points[0], points[:1] + 0.05)
 
 
+def test_the_plain_shoebox_is_laid_out_as_the_reference_lays_it():
+    # The plain box at 10 cm: six real walls, no branches, speed 0.99 in every cell; the reference's
+    # own layout array for array, and its FP32 run equal to the oracle's to the bit.
+    if not cases.available():
+        pytest.skip("the reference sources are not here")
+    w = L.shoebox_room(2, cell=0.1, steps=150)
+    native = cases.reference_native()
+    vertices, faces, owner = L.room_mesh(w.room)
+    beta = np.array([m.beta for m in w.room.materials])
+    assert np.all((beta > 0.0) & (beta < 1.0))
+    solver = native.WaveSolver(
+        native.Bvh(vertices, faces), owner, beta, np.zeros((0, 3)), np.zeros(0, np.int64), w.built.grid.origin,
+        w.built.grid.cell, *w.built.grid.shape, w.source, w.receivers, layer=0, layer_damping=0.0, threads=2,
+        speed=np.full(w.built.grid.n, 0.99, np.float32),
+    )  # fmt: skip
+    ref = solver.layout()
+    for name, value in w.built.layout.items():
+        assert np.array_equal(np.asarray(value), np.asarray(ref[name])), name
+    assert np.array_equal(solver.run(w.signal), OracleSolver(w.built.layout).run(w.signal))
+
+
 def test_the_polyhedral_workload_is_seeded():
     a = L.polyhedral_room(0, cell=0.2, steps=10)
     b = L.polyhedral_room(0, cell=0.2, steps=10)
