@@ -234,6 +234,7 @@ SIGNATURES = {
         ctypes.c_int,
         [ctypes.c_void_p, _f32p, ctypes.c_uint64, _f64p, ctypes.c_uint64, _f64p, _f64p, _f64p, _f64p, _f64p],
     ),
+    "fdtd_set_tape_budget": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
     "fdtd_set_tape": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
     "fdtd_set_coefficients": (ctypes.c_int, [ctypes.c_void_p, _f32p, _f32p, _f32p, _f32p, _f32p]),
     "fdtd_get_timing": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_uint64)]),

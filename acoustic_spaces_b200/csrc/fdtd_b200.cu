@@ -140,16 +140,29 @@ struct fdtd_solver {
     // once and replayed while the workspace and the segment stay.
     cudaGraphExec_t grad_graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
     uint64_t graph_segment = 0;
-    // While the gradient recomputes a segment: the special rows' values after each step of a
-    // dispatch, recorded as level k + 2 of the trajectory after the dispatch's step k.
-    const AdjointTables *record_tables = nullptr;
+    // While recording (the gradient's recomputation of a segment, or a taped run that keeps the
+    // trajectory): the special rows' values and branch velocities after each step k of a dispatch,
+    // written as level k + record_offset of record_u and record_w; the gradient's recomputation
+    // needs no probe records (record_probes false).
     void *record_u = nullptr, *record_w = nullptr;
-    // The tape (fdtd_set_tape): a run of fdtd_run from rest keeps the state at every multiple of
-    // tape_segment steps before its end, and its drive, for the gradient that follows.
+    uint64_t record_offset = 2;
+    bool record_probes = true;
+    // The tape (fdtd_set_tape): a run of fdtd_run from rest keeps, for the gradient that follows,
+    // its drive and either the whole trajectory of the special rows and branch velocities (levels
+    // 0 .. steps+1 of tape_u, tape_w: what the gradient otherwise recomputes), when that fits in
+    // tape_budget bytes, or else the state at every multiple of tape_segment steps before its end.
     uint64_t tape_segment = 0;
+    uint64_t tape_budget = UINT64_MAX;  // UINT64_MAX: half the device memory free at the run
     bool tape_valid = false;
+    bool tape_traj = false;  // the valid tape holds the trajectory (no checkpoints)
     std::vector<float> tape_signal;
     std::vector<void *> tape_checkpoints;
+    void *tape_u = nullptr, *tape_w = nullptr;
+    uint64_t tape_levels = 0;  // levels tape_u and tape_w have room for
+    // A taped run's chunks record into staging (kGraphSteps levels), copied onto the tape after
+    // each chunk, through graphs of their own ([the levels' roles]).
+    void *stage_u = nullptr, *stage_w = nullptr;
+    cudaGraphExec_t tape_graph[2] = {nullptr, nullptr};
     // Staging for fdtd_run's host buffers, grown on demand.
     float *stage_signal = nullptr;
     double *stage_out = nullptr;
@@ -382,10 +395,10 @@ int launch_steps(fdtd_solver *s, const float *d_signal, uint64_t steps, double *
         f.signal = d_signal + k;
         f.out = d_out + k;
         f.out_stride = stride;
-        if (s->record_tables) {
-            // The special rows' new values, level k + 2 of the gradient's trajectory.
-            f.traj_u = static_cast<T *>(s->record_u) + (k + 2) * s->specials;
-            f.traj_w = static_cast<T *>(s->record_w) + (k + 2) * s->states;
+        if (s->record_u) {
+            // The special rows' new values, level k + record_offset of the trajectory.
+            f.traj_u = static_cast<T *>(s->record_u) + (k + s->record_offset) * s->specials;
+            f.traj_w = static_cast<T *>(s->record_w) + (k + s->record_offset) * s->states;
         }
         if (fork) {
             if (k > 0) {
@@ -444,7 +457,7 @@ int launch_steps(fdtd_solver *s, const float *d_signal, uint64_t steps, double *
         if (ev) CUDA_TRY(s, cudaEventRecord(ev[5], side));
         if (ev) CUDA_TRY(s, cudaEventRecord(ev[6], side));
         // (A recomputation for the gradient records the special rows instead of the probes.)
-        if (probe_blocks && !s->record_tables) probe_kernel<T><<<probe_blocks, kBlock, 0, side>>>(g, f);
+        if (probe_blocks && s->record_probes) probe_kernel<T><<<probe_blocks, kBlock, 0, side>>>(g, f);
         if (ev) CUDA_TRY(s, cudaEventRecord(ev[7], side));
         if (fork) {
             CUDA_TRY(s, cudaEventRecord(s->joined[1], side));
@@ -813,6 +826,8 @@ void release(fdtd_solver *s) {
         if (stream) cudaStreamSynchronize(stream);
     for (cudaGraphExec_t g : s->graph)
         if (g) cudaGraphExecDestroy(g);
+    for (cudaGraphExec_t g : s->tape_graph)
+        if (g) cudaGraphExecDestroy(g);
     for (auto &row : s->grad_graph)
         for (cudaGraphExec_t g : row)
             if (g) cudaGraphExecDestroy(g);
@@ -1153,10 +1168,11 @@ int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float
     const bool taped = s->tape_valid && s->tape_signal.size() == steps &&
                        std::min<uint64_t>(s->tape_segment, steps) == segment &&
                        std::memcmp(s->tape_signal.data(), signal, sizeof(float) * steps) == 0;
+    const bool trajectory = taped && s->tape_traj;  // the tape holds every level: nothing to recompute
     std::vector<char *> checkpoints;
-    if (taped)
+    if (taped && !trajectory)
         for (uint64_t k = 0; k + 1 < segments; ++k) checkpoints.push_back(static_cast<char *>(s->tape_checkpoints[k]));
-    else if ((rc = fdtd_reset(s)) != FDTD_OK)
+    else if (!taped && (rc = fdtd_reset(s)) != FDTD_OK)
         return rc;
     for (uint64_t k = 0; !taped && k + 1 < segments; ++k) {
         if ((rc = dispatch(s, d_signal + k * segment, segment, d_out, segment)) != FDTD_OK) return rc;
@@ -1180,9 +1196,9 @@ int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float
     // A segment's recomputation (the dispatch of its steps, recording the special rows), and its
     // reverse steps.
     auto recompute = [&](uint64_t count) -> int {
-        s->record_tables = &t, s->record_u = traj_u, s->record_w = traj_w;
+        s->record_u = traj_u, s->record_w = traj_w, s->record_offset = 2, s->record_probes = false;
         const int r = dispatch(s, seg_signal, count, d_out, segment);
-        s->record_tables = nullptr, s->record_u = s->record_w = nullptr;
+        s->record_u = s->record_w = nullptr, s->record_probes = true;
         return r;
     };
     auto reverse = [&](uint64_t count) -> int {
@@ -1248,6 +1264,20 @@ int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float
     };
     for (uint64_t k = segments; k-- > 0;) {
         const uint64_t s0 = k * segment, s1 = std::min(steps, s0 + segment), count = s1 - s0;
+        if (trajectory) {
+            // The segment's levels s0 .. s1+1 from the tape, into the segment's trajectory buffers.
+            CUDA_TRY(s, cudaMemcpyAsync(traj_u, static_cast<const T *>(s->tape_u) + s0 * K, e * K * (count + 2),
+                                        cudaMemcpyDeviceToDevice, s->stream));
+            if (S)
+                CUDA_TRY(s, cudaMemcpyAsync(traj_w, static_cast<const T *>(s->tape_w) + s0 * S, e * S * (count + 2),
+                                            cudaMemcpyDeviceToDevice, s->stream));
+            if (P)
+                CUDA_TRY(s, cudaMemcpy2DAsync(seg_dloss, sizeof(double) * segment, d_dloss + s0, sizeof(double) * steps,
+                                              sizeof(double) * count, P, cudaMemcpyDeviceToDevice, s->stream));
+            if ((rc = run(1, x, reverse, count)) != FDTD_OK) return rc;
+            if (count & 1) x = 1 - x;
+            continue;
+        }
         // Recompute the segment from its start, recording each level of the special rows.
         if (k == 0) {
             if ((rc = fdtd_reset(s)) != FDTD_OK) return rc;
@@ -1491,15 +1521,59 @@ int fdtd_run(fdtd_solver *s, const float *signal, uint64_t steps, double *out) {
         CUDA_TRY(s, cudaMallocHost((void **)&s->stage_out, piece * P * sizeof(double)));
         s->stage_steps = piece;
     }
-    // A tape (fdtd_set_tape) of a run from rest: the state at every multiple of the segment before
+    // A tape (fdtd_set_tape) of a run from rest: the trajectory of the special rows and branch
+    // velocities when it fits the budget; else the state at every multiple of the segment before
     // the run's end, in the checkpoints' layout of the gradient (current level, previous level,
     // current and previous branch velocities).
     const bool taping = s->tape_segment && s->steps_done == 0;
-    const uint64_t tape_segment = taping ? std::min(s->tape_segment, steps) : 0;
+    uint64_t tape_segment = taping ? std::min(s->tape_segment, steps) : 0;
     const size_t e = s->precision == FDTD_FP64 ? 8 : 4;
     const uint64_t level_bytes = e * s->n_device, state_bytes = e * s->states;
+    const uint64_t K = s->specials, S = s->states;
+    bool keep_traj = false;
     if (taping) {
         s->tape_valid = false;
+        s->tape_traj = false;
+        uint64_t budget = s->tape_budget;
+        if (budget == UINT64_MAX) {
+            size_t free_bytes = 0, total_bytes = 0;
+            CUDA_TRY(s, cudaMemGetInfo(&free_bytes, &total_bytes));
+            budget = free_bytes / 2 + e * (K + S) * s->tape_levels;  // (what the tape holds already counts)
+        }
+        keep_traj = K + S > 0 && e * (K + S) * (steps + 2) <= budget;
+    }
+    if (keep_traj) {
+        int r;
+        if (s->tape_levels < steps + 2) {
+            // Grow the tape (freeing the old one first).
+            for (void **p : {&s->tape_u, &s->tape_w}) {
+                if (!*p) continue;
+                cudaFree(*p);
+                s->allocations.erase(std::find(s->allocations.begin(), s->allocations.end(), *p));
+                *p = nullptr;
+            }
+            s->device_bytes -= e * (K + S) * s->tape_levels;
+            s->tape_levels = 0;
+            if ((r = zeros(s, e * K * (steps + 2), &s->tape_u)) != FDTD_OK) return r;
+            if ((r = zeros(s, e * S * (steps + 2), &s->tape_w)) != FDTD_OK) return r;
+            s->tape_levels = steps + 2;
+        }
+        if (!s->stage_u) {
+            if ((r = zeros(s, e * K * kGraphSteps, &s->stage_u)) != FDTD_OK) return r;
+            if ((r = zeros(s, e * S * kGraphSteps, &s->stage_w)) != FDTD_OK) return r;
+        }
+        // Levels 0 and 1: the state at rest.
+        CUDA_TRY(s, cudaMemsetAsync(s->tape_u, 0, e * K * 2, s->stream));
+        if (S) CUDA_TRY(s, cudaMemsetAsync(s->tape_w, 0, e * S * 2, s->stream));
+        tape_segment = steps;  // no checkpoints
+    }
+    // While keeping the trajectory, every step records into the staging (restored on return).
+    struct Recording {
+        fdtd_solver *s;
+        ~Recording() { s->record_u = s->record_w = nullptr, s->record_offset = 2; }
+    } recording{s};
+    if (keep_traj) s->record_u = s->stage_u, s->record_w = s->stage_w, s->record_offset = 0, s->record_probes = true;
+    if (taping && !keep_traj) {
         const uint64_t needed = (steps + tape_segment - 1) / tape_segment - 1;
         while (s->tape_checkpoints.size() < needed) {
             void *p = nullptr;
@@ -1520,15 +1594,24 @@ int fdtd_run(fdtd_solver *s, const float *signal, uint64_t steps, double *out) {
             CUDA_TRY(s, cudaMemcpyAsync(s->d_sig, s->stage_signal + done, chunk * sizeof(float), cudaMemcpyHostToDevice,
                                         s->stream));
             if (chunk == kGraphSteps && s->n_device < kGraphCells) {
-                // A whole chunk: the captured graph of its steps for the levels' present roles.
-                cudaGraphExec_t &graph = s->graph[s->flipped ? 1 : 0];
+                // A whole chunk: the captured graph of its steps for the levels' present roles
+                // (with the trajectory's recording, a graph of its own).
+                cudaGraphExec_t &graph = keep_traj ? s->tape_graph[s->flipped ? 1 : 0] : s->graph[s->flipped ? 1 : 0];
                 if (!graph && (rc = capture(s, &graph)) != FDTD_OK) break;
                 CUDA_TRY(s, cudaGraphLaunch(graph, s->stream));
             } else if ((rc = dispatch(s, s->d_sig, chunk, s->d_rec, kGraphSteps)) != FDTD_OK) {
                 break;
             }
             settle(s, chunk);
-            if (taping && (at + chunk) % tape_segment == 0 && at + chunk < steps) {
+            if (keep_traj) {
+                // The chunk's levels at + 2 .. at + chunk + 1 onto the tape.
+                CUDA_TRY(s, cudaMemcpyAsync(static_cast<char *>(s->tape_u) + e * K * (at + 2), s->stage_u, e * K * chunk,
+                                            cudaMemcpyDeviceToDevice, s->stream));
+                if (S)
+                    CUDA_TRY(s, cudaMemcpyAsync(static_cast<char *>(s->tape_w) + e * S * (at + 2), s->stage_w,
+                                                e * S * chunk, cudaMemcpyDeviceToDevice, s->stream));
+            }
+            if (taping && !keep_traj && (at + chunk) % tape_segment == 0 && at + chunk < steps) {
                 char *c = static_cast<char *>(s->tape_checkpoints[(at + chunk) / tape_segment - 1]);
                 CUDA_TRY(s, cudaMemcpyAsync(c, s->u[1], level_bytes, cudaMemcpyDeviceToDevice, s->stream));
                 CUDA_TRY(s, cudaMemcpyAsync(c + level_bytes, s->u[0], level_bytes, cudaMemcpyDeviceToDevice, s->stream));
@@ -1557,6 +1640,7 @@ int fdtd_run(fdtd_solver *s, const float *signal, uint64_t steps, double *out) {
     if (taping) {
         s->tape_signal.assign(signal, signal + steps);
         s->tape_valid = true;
+        s->tape_traj = keep_traj;
     }
     for (uint64_t k = 0; k < s->probes * steps; ++k) {
         if (!std::isfinite(out[k])) return fail(s, FDTD_ENONFINITE, "the wave solver's run did not stay finite");
@@ -1635,6 +1719,13 @@ int fdtd_set_coefficients(fdtd_solver *s, const float *coef_b, const float *coef
             CUDA_TRY(s, cudaMemcpy(const_cast<double *>(t.corrected_coef), coef.data(), 8 * coef.size(),
                                    cudaMemcpyHostToDevice));
     }
+    s->tape_valid = false;
+    return FDTD_OK;
+}
+
+int fdtd_set_tape_budget(fdtd_solver *s, uint64_t bytes) {
+    if (!s) return set_global(FDTD_EINVAL, "no solver");
+    s->tape_budget = bytes;
     s->tape_valid = false;
     return FDTD_OK;
 }

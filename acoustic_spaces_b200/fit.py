@@ -234,7 +234,7 @@ class AdjointFit:
         solver = cache.get(precision)
         if solver is None:
             solver = cache[precision] = B200WaveSolver(lay, precision=precision)
-            solver.set_tape(self.segment)  # the run keeps its checkpoints for the gradient
+            solver.set_tape(self.segment)  # the run keeps its tape for the gradient
         else:
             solver.set_coefficients(*(lay[k] for k in ("coef_b", "coef_inv", "branch_now", "branch_before", "branch_gain")))
             solver.set_tape(self.segment)

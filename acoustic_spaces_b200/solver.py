@@ -218,10 +218,21 @@ class B200WaveSolver:
             _raise(self._lib, status, self._handle)
 
     def set_tape(self, segment: int) -> None:
-        """With ``segment`` > 0, each :meth:`run` from rest keeps the state every ``segment`` steps
-        (and its drive), so that a following :meth:`gradient` of that drive with that ``segment``
-        does not run the forward pass again; 0 turns it off."""
+        """With ``segment`` > 0, each :meth:`run` from rest keeps what a following
+        :meth:`gradient` of that drive with that ``segment`` needs, so that the gradient does not
+        run the forward pass again: the whole trajectory of the special rows and branch
+        velocities where it fits the tape's budget (:meth:`set_tape_budget`; the gradient then
+        recomputes nothing), else the state every ``segment`` steps (the gradient recomputes each
+        segment from it). 0 turns it off."""
         status = self._lib.fdtd_set_tape(self._handle, int(segment))
+        if status != _abi.FDTD_OK:
+            _raise(self._lib, status, self._handle)
+
+    def set_tape_budget(self, nbytes: int | None) -> None:
+        """The device memory the tape's trajectory may take: None for half the device memory free
+        at the run, 0 for checkpoints always."""
+        value = (1 << 64) - 1 if nbytes is None else int(nbytes)
+        status = self._lib.fdtd_set_tape_budget(self._handle, value)
         if status != _abi.FDTD_OK:
             _raise(self._lib, status, self._handle)
 

@@ -197,6 +197,15 @@ int fdtd_gradient(fdtd_solver *solver, const float *signal, uint64_t steps, cons
 int fdtd_set_tape(fdtd_solver *solver, uint64_t segment);
 
 /*
+ * The device memory a tape may take for the trajectory (no counterpart in the reference). A taped
+ * run keeps, in place of checkpoints, every level of the special rows' values and branch
+ * velocities ((steps + 2) * (special rows + branch states) elements) when that fits in `bytes`;
+ * the gradient then recomputes nothing. UINT64_MAX (the default): half the device memory free at
+ * the run. 0: always checkpoints.
+ */
+int fdtd_set_tape_budget(fdtd_solver *solver, uint64_t bytes);
+
+/*
  * New material coefficients for the handle's grid (no counterpart in the reference, which builds a
  * new solver for new materials): each non-NULL array replaces the layout's — coef_b and coef_inv
  * one per special row (special_count), branch_now, branch_before and branch_gain one per branch

@@ -158,15 +158,20 @@ def test_the_autograd_function_gives_the_material_gradient():
     np.testing.assert_allclose(ours, expected, rtol=1e-9, atol=1e-12 * np.abs(expected).max())
 
 
-def test_a_taped_run_gives_the_gradient_to_the_bit():
-    # fdtd_set_tape: the run keeps its checkpoints and the gradient starts from them; a gradient of
-    # another drive does not use them.
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("budget", [None, 0], ids=["trajectory", "checkpoints"])
+def test_a_taped_run_gives_the_gradient_to_the_bit(budget, precision):
+    # fdtd_set_tape: the run keeps the special rows' whole trajectory (within the budget; the
+    # gradient then recomputes nothing) or its checkpoints (the gradient recomputes each segment
+    # from them); either way the gradient equals an untaped one's to the bit, and a gradient of
+    # another drive does not use the tape.
     layout, signal, _ = load_golden("resonant7")
     signal = np.ascontiguousarray(signal[:300])
-    y = B200WaveSolver(layout, precision="fp64").run(signal)
+    y = B200WaveSolver(layout, precision=precision).run(signal)
     dloss = 2.0 * (y - 0.5 * y)
-    plain = B200WaveSolver(layout, precision="fp64").gradient(signal, dloss, segment=37)
-    taped = B200WaveSolver(layout, precision="fp64")
+    plain = B200WaveSolver(layout, precision=precision).gradient(signal, dloss, segment=37)
+    taped = B200WaveSolver(layout, precision=precision)
+    taped.set_tape_budget(budget)
     taped.set_tape(37)
     np.testing.assert_array_equal(taped.run(signal), y)
     taped.reset()
@@ -174,8 +179,8 @@ def test_a_taped_run_gives_the_gradient_to_the_bit():
     for key in plain:
         np.testing.assert_array_equal(got[key], plain[key], err_msg=key)
     other = signal * 0.5
-    y2 = B200WaveSolver(layout, precision="fp64").run(other)
-    expected = B200WaveSolver(layout, precision="fp64").gradient(other, 2.0 * y2, segment=37)
+    y2 = B200WaveSolver(layout, precision=precision).run(other)
+    expected = B200WaveSolver(layout, precision=precision).gradient(other, 2.0 * y2, segment=37)
     got = taped.gradient(other, 2.0 * y2, segment=37)
     for key in expected:
         np.testing.assert_array_equal(got[key], expected[key], err_msg=key)
