@@ -86,6 +86,9 @@ struct fdtd_solver {
     Tables tables{};
     BulkArgs bulk{};
     uint32_t bulk_blocks = 0;  // the persistent grid: resident blocks, at most one per tile
+    // Blocks an SM of the matched-layer and special-row kernels (0: one thread a cell), chosen by
+    // fdtd_autotune.
+    int layer_per_sm = kLayerPerSm, special_per_sm = kSpecialPerSm;
     uint32_t bulk_tiles = 0;
     int bulk_per_sm = 0;      // resident bulk blocks per multiprocessor
     uint64_t nx = 0, ny = 0, nz = 0, n = 0, pitch = 0, n_device = 0;
@@ -377,10 +380,14 @@ int set_up_kernels(fdtd_solver *s) {
 template <typename T, bool WIDE, bool SCALED, bool COMP = false>
 int launch_steps(fdtd_solver *s, const float *d_signal, uint64_t steps, double *d_out, uint64_t stride) {
     const Tables &g = s->tables;
-    const uint32_t special_blocks = (uint32_t)((s->specials + kBlock - 1) / kBlock);
+    // The layer and special kernels loop over their cells: a few blocks an SM each (the handle's
+    // layer_per_sm, special_per_sm; 0: a thread a cell), leaving the sweep's blocks their places.
+    const uint64_t special_cap = s->special_per_sm ? (uint64_t)s->sms * s->special_per_sm : UINT64_MAX;
+    const uint64_t layer_cap = s->layer_per_sm ? (uint64_t)s->sms * s->layer_per_sm : UINT64_MAX;
+    const uint32_t special_blocks = (uint32_t)std::min<uint64_t>((s->specials + kBlock - 1) / kBlock, special_cap);
     const uint32_t probe_blocks = (uint32_t)((s->probes + kProbeWarps - 1) / kProbeWarps);
     const uint32_t smem = Stage<T, SCALED>::smem;
-    const uint32_t layer_blocks = (uint32_t)((s->layers + kBlock - 1) / kBlock);
+    const uint32_t layer_blocks = (uint32_t)std::min<uint64_t>((s->layers + kBlock - 1) / kBlock, layer_cap);
     // Each step: the interior sweep on the handle's stream; beside it the matched layer on the
     // layer stream, of the highest priority (its blocks take the thread slots that the sweep's
     // shared memory leaves free on every multiprocessor), and the special rows and probes on the
@@ -1721,6 +1728,83 @@ int fdtd_set_coefficients(fdtd_solver *s, const float *coef_b, const float *coef
     }
     s->tape_valid = false;
     return FDTD_OK;
+}
+
+int fdtd_set_launch(fdtd_solver *s, int layer_per_sm, int special_per_sm) {
+    if (!s) return set_global(FDTD_EINVAL, "no solver");
+    if (layer_per_sm < 0 || special_per_sm < 0 || layer_per_sm > 64 || special_per_sm > 64)
+        return fail(s, FDTD_EINVAL, "blocks per multiprocessor are 0 (a thread a cell) to 64");
+    DeviceGuard guard(s->device);
+    for (cudaStream_t stream : {s->stream, s->side, s->layer_stream}) CUDA_TRY(s, cudaStreamSynchronize(stream));
+    s->layer_per_sm = layer_per_sm, s->special_per_sm = special_per_sm;
+    // The captured chunks and the gradient's graphs hold the old launch shapes.
+    Kept{s}.drop_graphs();
+    for (cudaGraphExec_t &g : s->graph)
+        if (g) cudaGraphExecDestroy(g), g = nullptr;
+    for (cudaGraphExec_t &g : s->tape_graph)
+        if (g) cudaGraphExecDestroy(g), g = nullptr;
+    return FDTD_OK;
+}
+
+int fdtd_autotune(fdtd_solver *s, uint64_t trial_steps, int *layer_per_sm, int *special_per_sm) {
+    if (!s) return set_global(FDTD_EINVAL, "no solver");
+    if (s->steps_done != 0) return fail(s, FDTD_EINVAL, "fdtd_autotune runs from rest (after fdtd_create or fdtd_reset)");
+    if (trial_steps == 0) trial_steps = 8;
+    DeviceGuard guard(s->device);
+    int rc = FDTD_OK;
+    // The drive (zeros) and the records of the trials, on the device; the fields' values do not
+    // change the kernels' memory traffic.
+    void *sig = nullptr, *rec = nullptr;
+    CUDA_TRY(s, cudaMalloc(&sig, sizeof(float) * trial_steps));
+    struct Free {
+        void *&a, *&b;
+        ~Free() { cudaFree(a), cudaFree(b); }
+    } release_trials{sig, rec};
+    CUDA_TRY(s, cudaMemset(sig, 0, sizeof(float) * trial_steps));
+    CUDA_TRY(s, cudaMalloc(&rec, sizeof(double) * trial_steps * std::max<uint64_t>(1, s->probes)));
+    cudaEvent_t start, end;
+    CUDA_TRY(s, cudaEventCreate(&start));
+    CUDA_TRY(s, cudaEventCreate(&end));
+    const bool timing = s->timing;
+    s->timing = false;
+    const int layers[] = {4, 8, 12, 16, 0}, specials[] = {2, 4, 8, 0};
+    float best = -1.0f;
+    int best_layer = s->layer_per_sm, best_special = s->special_per_sm;
+    for (int l : layers) {
+        if (!s->layers && l != layers[0]) continue;
+        for (int k : specials) {
+            if (!s->specials && k != specials[0]) continue;
+            s->layer_per_sm = l, s->special_per_sm = k;
+            // One untimed dispatch, then the timed one.
+            for (int pass = 0; pass < 2 && rc == FDTD_OK; ++pass) {
+                if (pass == 1) CUDA_TRY(s, cudaEventRecord(start, s->stream));
+                rc = dispatch(s, static_cast<const float *>(sig), trial_steps, static_cast<double *>(rec), trial_steps);
+                if (rc == FDTD_OK) settle(s, trial_steps);
+            }
+            if (rc != FDTD_OK) break;
+            CUDA_TRY(s, cudaEventRecord(end, s->stream));
+            CUDA_TRY(s, cudaEventSynchronize(end));
+            float ms = 0.0f;
+            CUDA_TRY(s, cudaEventElapsedTime(&ms, start, end));
+            if (best < 0.0f || ms < best) best = ms, best_layer = l, best_special = k;
+        }
+        if (rc != FDTD_OK) break;
+    }
+    s->timing = timing;
+    cudaEventDestroy(start);
+    cudaEventDestroy(end);
+    if (rc != FDTD_OK) return rc;
+    s->layer_per_sm = best_layer, s->special_per_sm = best_special;
+    // The captured chunks and the gradient's graphs hold the old launch shapes.
+    Kept{s}.drop_graphs();
+    for (cudaGraphExec_t &g : s->graph)
+        if (g) cudaGraphExecDestroy(g), g = nullptr;
+    for (cudaGraphExec_t &g : s->tape_graph)
+        if (g) cudaGraphExecDestroy(g), g = nullptr;
+    if ((rc = check_device_error(s)) != FDTD_OK) return rc;
+    if (layer_per_sm) *layer_per_sm = best_layer;
+    if (special_per_sm) *special_per_sm = best_special;
+    return fdtd_reset(s);
 }
 
 int fdtd_set_tape_budget(fdtd_solver *s, uint64_t bytes) {

@@ -44,6 +44,8 @@ constexpr int kRowsPerThread = kTX * kTY / kBlock;  // 8 rows of one column per 
 constexpr int kAhead = 2;                       // planes loaded ahead of the three in use
 constexpr int kStages = kAhead + 3;             // ring of plane stages in shared memory
 constexpr uint32_t kSpinLimit = 1u << 24;       // bounded waits: then the block gives up
+constexpr int kLayerPerSm = 8;                  // blocks an SM of the matched-layer kernel
+constexpr int kSpecialPerSm = 4;                // blocks an SM of the special rows' kernel
 
 constexpr uint32_t align128(uint32_t v) { return (v + 127u) & ~127u; }
 
@@ -358,12 +360,9 @@ struct Fields {
 // are coalesced; all of a row's link loads are issued before the sum, which then adds them in
 // the layout's order. A state's term now * wb - before * wa is worked out again for the
 // velocities' update rather than kept: wa has not changed in between, so it is the same value.
-template <typename T, int SLOTS, bool COMP = false>
-__global__ void __launch_bounds__(kBlock) special_kernel(const Tables g, const Fields<T> f) {
-    const uint32_t k = blockIdx.x * kBlock + threadIdx.x;
+template <typename T, int SLOTS, bool COMP>
+__device__ __forceinline__ void special_row(const Tables &g, const Fields<T> &f, const uint32_t k, const uint32_t i) {
     const uint32_t K = g.specials;
-    if (k >= K) return;
-    const uint32_t i = g.special[k];
     const uint32_t links = g.link_count[k];
     const T *__restrict__ b = f.b;
     T value[SLOTS];
@@ -414,6 +413,22 @@ __global__ void __launch_bounds__(kBlock) special_kernel(const Tables g, const F
     }
 }
 
+// Rows k, k + the grid's threads, ... a thread, the next row's cell index loaded while this row's
+// loads are in flight.
+template <typename T, int SLOTS, bool COMP = false>
+__global__ void __launch_bounds__(kBlock) special_kernel(const Tables g, const Fields<T> f) {
+    const uint32_t K = g.specials;
+    const uint32_t step = gridDim.x * kBlock;
+    uint32_t k = blockIdx.x * kBlock + threadIdx.x;
+    if (k >= K) return;
+    uint32_t next = g.special[k];
+    for (; k < K; k += step) {
+        const uint32_t i = next;
+        if (k + step < K) next = g.special[k + step];
+        special_row<T, SLOTS, COMP>(g, f, k, i);
+    }
+}
+
 // Matched-layer cells (fdtd.hpp:2242-2264), one a thread: per axis the cell's two face
 // velocities, then its pressure part; the cell's pressure is the parts' sum.
 //
@@ -425,55 +440,84 @@ __global__ void __launch_bounds__(kBlock) special_kernel(const Tables g, const F
 // that alternate with the steps: every cell reads the old values of its two faces and works both
 // out again, and writes the new value of its + face, and of its - face too where the cell below
 // is not in the layer (no one else writes that face). The pressure parts stay per cell.
-template <typename T, bool SCALED, bool COMP = false>
-__global__ void __launch_bounds__(kBlock) layer_kernel(const Tables g, const Fields<T> f) {
-    const uint32_t c = blockIdx.x * kBlock + threadIdx.x;
+template <typename T, bool SCALED, bool COMP>
+__device__ __forceinline__ void layer_cell(const Tables &g, const Fields<T> &f, const uint32_t c, const uint32_t i) {
     const uint32_t L = g.layers;
-    if (c >= L) return;
-    T *parts = f.layer_parts;
-    T part[3];
-#pragma unroll
-    for (int axis = 0; axis < 3; ++axis) part[axis] = parts[axis * L + c];
-    const uint32_t i = g.layer_cells[c];
-    const uint32_t at[3] = {i % g.pitch, (i / g.pitch) % g.ny, i / g.plane};
+    // Every load of the cell first — its parts, its pressure and its six neighbours', its faces'
+    // old velocities and the coefficients — so that they are in flight together; then the
+    // reference's arithmetic, axis by axis; then the stores.
+    const uint32_t z = i / g.plane, r = i - z * g.plane, y = r / g.pitch;
+    const uint32_t at[3] = {r - y * g.pitch, y, z};
     const uint32_t strides[3] = {1u, g.pitch, g.plane};
     const T *__restrict__ b = f.b;
+    T *__restrict__ parts = f.layer_parts;
+    T part[3], lo[3], hi[3], old_below[3], old_above[3];
+    float4 c0[3], c1[3];
+#pragma unroll
+    for (int axis = 0; axis < 3; ++axis) {
+        const uint32_t stride = strides[axis];
+        part[axis] = parts[axis * L + c];
+        lo[axis] = b[i - stride];
+        hi[axis] = b[i + stride];
+        old_below[axis] = __ldg(f.face_old[axis] + (i - stride));
+        old_above[axis] = __ldg(f.face_old[axis] + i);
+        c0[axis] = __ldg(g.layer_coef[axis] + at[axis]);
+        c1[axis] = __ldg(g.layer_coef[axis] + at[axis] + 1);
+    }
     const T here = b[i];
     const T scale = SCALED ? (T)g.layer_scale[c] : (T)1;
     const uint32_t shared_below = g.layer_below[c];
+    T below[3], above[3];
     T total = 0;
 #pragma unroll
     for (int axis = 0; axis < 3; ++axis) {
-        const uint32_t stride = strides[axis], x = at[axis];
-        const float4 c0 = g.layer_coef[axis][x], c1 = g.layer_coef[axis][x + 1];
-        const T below = (T)c0.z * f.face_old[axis][i - stride] - (T)c0.w * (here - b[i - stride]);
-        const T above = (T)c1.z * f.face_old[axis][i] - (T)c1.w * (b[i + stride] - here);
-        f.face_new[axis][i] = above;
-        // The cell below owns the face when it is in the layer.
-        if (!(shared_below & (1u << axis))) f.face_new[axis][i - stride] = below;
+        below[axis] = (T)c0[axis].z * old_below[axis] - (T)c0[axis].w * (here - lo[axis]);
+        above[axis] = (T)c1[axis].z * old_above[axis] - (T)c1[axis].w * (hi[axis] - here);
         if (COMP) {
             // The parts' sum carried on from the pressure: p + (keep - 1) * part - flux per axis.
-            const T keep = (T)c0.x;
-            const T push = SCALED ? (T)c0.y * scale : (T)c0.y;
-            const T flux = push * (above - below);
+            const T keep = (T)c0[axis].x;
+            const T push = SCALED ? (T)c0[axis].y * scale : (T)c0[axis].y;
+            const T flux = push * (above[axis] - below[axis]);
             total += (keep - (T)1) * part[axis] - flux;
             part[axis] = keep * part[axis] - flux;
             continue;
         }
         if (SCALED) {
-            part[axis] = (T)c0.x * part[axis] - ((T)c0.y * scale) * (above - below);
+            part[axis] = (T)c0[axis].x * part[axis] - ((T)c0[axis].y * scale) * (above[axis] - below[axis]);
         } else {
-            part[axis] = (T)c0.x * part[axis] - (T)c0.y * (above - below);
+            part[axis] = (T)c0[axis].x * part[axis] - (T)c0[axis].y * (above[axis] - below[axis]);
         }
         total += part[axis];
     }
 #pragma unroll
-    for (int axis = 0; axis < 3; ++axis) parts[axis * L + c] = part[axis];
+    for (int axis = 0; axis < 3; ++axis) {
+        f.face_new[axis][i] = above[axis];
+        // The cell below owns the face when it is in the layer.
+        if (!(shared_below & (1u << axis))) f.face_new[axis][i - strides[axis]] = below[axis];
+        parts[axis * L + c] = part[axis];
+    }
     if (COMP) {
         f.a[i] = here + total;
         f.d[i] = total;  // (read by no update; it keeps the state's level before readable)
     } else {
         f.a[i] = total;
+    }
+}
+
+// A grid of a few blocks an SM (the sweep's blocks keep their places beside it), each thread taking
+// cells c, c + the grid's threads, ...; the next cell's index is loaded while this cell's loads are
+// in flight, so that a cell costs one round trip to memory rather than two.
+template <typename T, bool SCALED, bool COMP = false>
+__global__ void __launch_bounds__(kBlock) layer_kernel(const Tables g, const Fields<T> f) {
+    const uint32_t L = g.layers;
+    const uint32_t step = gridDim.x * kBlock;
+    uint32_t c = blockIdx.x * kBlock + threadIdx.x;
+    if (c >= L) return;
+    uint32_t next = g.layer_cells[c];
+    for (; c < L; c += step) {
+        const uint32_t i = next;
+        if (c + step < L) next = g.layer_cells[c + step];
+        layer_cell<T, SCALED, COMP>(g, f, c, i);
     }
 }
 

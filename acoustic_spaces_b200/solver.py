@@ -88,9 +88,15 @@ class B200WaveSolver:
     ``precision`` ``"fp32"`` is the reference's arithmetic, bit for bit; ``"fp64"`` steps the same
     layout in double; ``"fp32c"`` steps it in compensated single precision (each cell's pressure
     and its increment, 16 bytes of traffic per interior cell against fp64's 24), which stays
-    close to fp64 over long runs where fp32's rounding drifts."""
+    close to fp64 over long runs where fp32's rounding drifts.
 
-    def __init__(self, solver, *, precision: Precision = "fp32", device: int = 0) -> None:
+    ``autotune`` chooses the matched-layer and special-row kernels' launch shapes by timing a few
+    steps of each (:meth:`autotune`); by default on grids of ``AUTOTUNE_CELLS`` cells or more,
+    where a step is long enough to time. The results do not depend on it."""
+
+    AUTOTUNE_CELLS = 1 << 22
+
+    def __init__(self, solver, *, precision: Precision = "fp32", device: int = 0, autotune: bool | None = None) -> None:
         self._lib = lib = _abi.load_library()
         layout = solver if isinstance(solver, Mapping) else solver.layout()
         if precision not in _PRECISIONS:
@@ -112,6 +118,9 @@ class B200WaveSolver:
         self._probes = int(info.probes)
         self.shape = tuple(int(v) for v in np.asarray(layout["shape"]).reshape(-1))
         self._branches = len(np.asarray(layout["branch_now"]).reshape(-1))
+        self.launch: dict[str, int] | None = None
+        if autotune or (autotune is None and int(np.prod(self.shape)) >= self.AUTOTUNE_CELLS):
+            self.launch = self.autotune()
 
     @property
     def probes(self) -> int:
@@ -227,6 +236,24 @@ class B200WaveSolver:
         status = self._lib.fdtd_set_tape(self._handle, int(segment))
         if status != _abi.FDTD_OK:
             _raise(self._lib, status, self._handle)
+
+    def autotune(self, trial_steps: int = 8) -> dict[str, int]:
+        """Chooses the matched-layer and special-row kernels' blocks per multiprocessor for this
+        grid by timing a few steps of each candidate (from rest; the state is reset after).
+        Returns the choice (0: one thread a cell)."""
+        layer, special = ctypes.c_int(), ctypes.c_int()
+        status = self._lib.fdtd_autotune(self._handle, int(trial_steps), ctypes.byref(layer), ctypes.byref(special))
+        if status != _abi.FDTD_OK:
+            _raise(self._lib, status, self._handle)
+        return {"layer_blocks_per_sm": layer.value, "special_blocks_per_sm": special.value}
+
+    def set_launch(self, layer_blocks_per_sm: int, special_blocks_per_sm: int) -> None:
+        """Sets the matched-layer and special-row kernels' blocks per multiprocessor (0: one
+        thread a cell), as :meth:`autotune` would."""
+        status = self._lib.fdtd_set_launch(self._handle, int(layer_blocks_per_sm), int(special_blocks_per_sm))
+        if status != _abi.FDTD_OK:
+            _raise(self._lib, status, self._handle)
+        self.launch = {"layer_blocks_per_sm": int(layer_blocks_per_sm), "special_blocks_per_sm": int(special_blocks_per_sm)}
 
     def set_tape_budget(self, nbytes: int | None) -> None:
         """The device memory the tape's trajectory may take: None for half the device memory free

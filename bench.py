@@ -671,6 +671,7 @@ def main() -> None:
     parser.add_argument("--seed", type=int, default=0)
     parser.add_argument("--cell", type=float, default=0.04, help="cell size in metres (0.04: the full workload)")
     parser.add_argument("--no-fp64-rate", action="store_true", help="skip timing the FP64 stepper alike")
+    parser.add_argument("--launch", default="", help="layer,special blocks per SM (skips the autotuner)")
     parser.add_argument("--precision", choices=["fp32", "fp32c"], default="fp32",
                         help="fp32: the reference's arithmetic; fp32c: compensated single precision")  # fmt: skip
     parser.add_argument("--cpu-steps", type=int, default=10, help="steps of the CPU-baseline sample")
@@ -727,7 +728,11 @@ def main() -> None:
 
     workload = build_workload(args)
     desc = workload.description
-    solver = B200WaveSolver(workload.built.layout, precision=args.precision, device=local)
+    if args.launch:
+        solver = B200WaveSolver(workload.built.layout, precision=args.precision, device=local, autotune=False)
+        solver.set_launch(*(int(v) for v in args.launch.split(",")))
+    else:
+        solver = B200WaveSolver(workload.built.layout, precision=args.precision, device=local)
     air = solver.air_cells
     probes = solver.probes
     steps, warmup = args.steps, args.warmup
@@ -883,6 +888,7 @@ def main() -> None:
                 "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                 "l2": "inputs larger than L2 (two pressure levels alone are "
                 f"{2 * 4 * desc['cells'] / 1e6:.0f} MB vs 126 MB L2), no flush",
+                "launch": solver.launch,
                 "precision": "FP32, bit-exact with the reference (no FMA, subnormals flushed)"
                 if args.precision == "fp32"
                 else "FP32 compensated: each cell's pressure and its increment (not bit-equal to the reference)",

@@ -206,6 +206,18 @@ int fdtd_set_tape(fdtd_solver *solver, uint64_t segment);
 int fdtd_set_tape_budget(fdtd_solver *solver, uint64_t bytes);
 
 /*
+ * Chooses the launch shapes of the matched-layer and special-row kernels for this grid (no
+ * counterpart in the reference): from rest, steps `trial_steps` steps (0: 8) with each candidate
+ * count of blocks per multiprocessor, keeps the fastest by CUDA events, and resets the state. The
+ * chosen counts are written to *layer_per_sm and *special_per_sm when given (0: one thread a
+ * cell). Refused after steps (fdtd_reset first).
+ */
+int fdtd_autotune(fdtd_solver *solver, uint64_t trial_steps, int *layer_per_sm, int *special_per_sm);
+
+/* Sets those launch shapes directly (0 to 64 blocks per multiprocessor; 0: one thread a cell). */
+int fdtd_set_launch(fdtd_solver *solver, int layer_per_sm, int special_per_sm);
+
+/*
  * New material coefficients for the handle's grid (no counterpart in the reference, which builds a
  * new solver for new materials): each non-NULL array replaces the layout's — coef_b and coef_inv
  * one per special row (special_count), branch_now, branch_before and branch_gain one per branch

@@ -204,3 +204,14 @@ def test_gpu_fp64_steps_the_plain_shoebox_as_the_fp64_oracle_does():
     assert np.array_equal(p64, OracleSolver(w.built.layout, "fp64").run(w.signal))
     p32 = B200WaveSolver(w.built.layout).run(w.signal)
     assert np.array_equal(p32, OracleSolver(w.built.layout).run(w.signal))
+
+
+def test_gpu_autotuned_launch_shapes_step_as_the_oracle_does():
+    # fdtd_autotune picks the layer and special kernels' blocks per SM by timing; every choice
+    # steps each cell with the same operations, so the run still equals the oracle's to the bit.
+    w = layouts.polyhedral_room(0, cell=0.2, steps=200)
+    gpu = B200WaveSolver(w.built.layout, autotune=True)
+    assert set(gpu.launch) == {"layer_blocks_per_sm", "special_blocks_per_sm"}
+    assert np.array_equal(_pieces(gpu, w.signal, [0, 64, 128, 200]), OracleSolver(w.built.layout).run(w.signal))
+    with pytest.raises(ValueError, match="from rest"):
+        gpu.autotune()
