@@ -1730,6 +1730,15 @@ int fdtd_set_coefficients(fdtd_solver *s, const float *coef_b, const float *coef
     return FDTD_OK;
 }
 
+int fdtd_level_plane(fdtd_solver *s, uint64_t z, int which, void **ptr, uint64_t *bytes) {
+    if (!s || !ptr || !bytes) return set_global(FDTD_EINVAL, "no solver or no place for the plane");
+    if (z >= s->nz || (which != 0 && which != 1)) return fail(s, FDTD_EINVAL, "no such plane or level");
+    const size_t e = s->precision == FDTD_FP64 ? 8 : 4;
+    *bytes = e * s->pitch * s->ny;
+    *ptr = static_cast<char *>(s->u[which ? 0 : 1]) + *bytes * z;
+    return FDTD_OK;
+}
+
 int fdtd_set_launch(fdtd_solver *s, int layer_per_sm, int special_per_sm) {
     if (!s) return set_global(FDTD_EINVAL, "no solver");
     if (layer_per_sm < 0 || special_per_sm < 0 || layer_per_sm > 64 || special_per_sm > 64)

@@ -114,6 +114,7 @@ class B200WaveSolver:
         if status != _abi.FDTD_OK:
             _raise(lib, status)
         self._handle = handle
+        self.device = int(device)
         info = self.info()
         self._probes = int(info.probes)
         self.shape = tuple(int(v) for v in np.asarray(layout["shape"]).reshape(-1))
@@ -246,6 +247,16 @@ class B200WaveSolver:
         if status != _abi.FDTD_OK:
             _raise(self._lib, status, self._handle)
         return {"layer_blocks_per_sm": layer.value, "special_blocks_per_sm": special.value}
+
+    def level_plane(self, z: int, previous: bool = False) -> tuple[int, int]:
+        """The device address and byte size of plane ``z`` of the current (or previous) pressure
+        level between runs: pitch x ny elements, the rows padded to 16 cells."""
+        ptr, nbytes = ctypes.c_void_p(), ctypes.c_uint64()
+        status = self._lib.fdtd_level_plane(self._handle, int(z), int(bool(previous)), ctypes.byref(ptr),
+                                            ctypes.byref(nbytes))  # fmt: skip
+        if status != _abi.FDTD_OK:
+            _raise(self._lib, status, self._handle)
+        return int(ptr.value or 0), int(nbytes.value)
 
     def set_launch(self, layer_blocks_per_sm: int, special_blocks_per_sm: int) -> None:
         """Sets the matched-layer and special-row kernels' blocks per multiprocessor (0: one

@@ -547,6 +547,82 @@ def run_shoebox(args, world: int, rank: int, local: int) -> None:
         print(json.dumps(line), flush=True)
 
 
+def run_slabs(args, world: int, rank: int, local: int) -> None:
+    """The polyhedral room as one grid split into slabs of z-planes across the ranks (strong
+    scaling): each rank steps its planes and, after every step, swaps its boundary planes with its
+    neighbours over NCCL (one plane per neighbour per step). The host orders every step. Reports the
+    whole grid's cell updates over the slowest rank's device time, and checks the gathered probes
+    against a one-rank run of the same grid where it fits."""
+    import torch
+    import torch.distributed as dist
+
+    from acoustic_spaces_b200 import B200WaveSolver, slabs
+
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+    workload = build_workload(args)
+    layout = workload.built.layout
+    bounds = slabs.partition_planes(layout, world)
+    part = slabs.slab(layout, bounds, rank)
+    solver = B200WaveSolver(part.layout, device=local)
+    planes = slabs.DevicePlanes(solver)
+    steps, warmup = args.steps, args.warmup
+    signal = np.ascontiguousarray(np.resize(workload.signal, steps + warmup), np.float32)
+    sig = torch.from_numpy(signal).to(f"cuda:{local}")
+    out = torch.zeros((max(1, len(part.probes)), steps + warmup), dtype=torch.float64, device=f"cuda:{local}")
+
+    def step(k: int) -> None:
+        solver.run_device(sig.data_ptr() + 4 * k, 1, out.data_ptr() + 8 * k, steps + warmup)
+        solver.synchronize()
+        if world > 1:
+            slabs.exchange_ghosts(planes, part, rank, world, dist)
+            torch.cuda.synchronize(local)
+
+    for k in range(warmup):
+        step(k)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(local)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clocks:
+        start.record()
+        for k in range(warmup, warmup + steps):
+            step(k)
+        end.record()
+        torch.cuda.synchronize(local)
+    ms = start.elapsed_time(end)
+    if world > 1:
+        t = torch.tensor([ms], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+        dist.destroy_process_group()
+    air = workload.built.air_cells
+    if rank == 0:
+        line = {
+            "metric": METRIC,
+            "value": round(air * steps / (ms / 1e3) / 1e9, 4),
+            "unit": UNIT,
+            "n_gpus": world,
+            "steps": steps,
+            "warmup": warmup,
+            "ms_per_step": round(ms / steps, 5),
+            "higher_is_better": True,
+            "scaling": "strong",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": workload.name, **workload.description, "parallelism": f"z-slabs x{world}",
+                       "slabs": [list(b) for b in bounds],
+                       "exchange": "one plane per neighbour per step over NCCL, the host ordering each step"},  # fmt: skip
+            "clocks": clocks.summary(),
+            "gpu_launches": 4 * steps,
+        }
+        print(json.dumps(line), flush=True)
+
+
 def run_adjoint(args, world: int, rank: int, local: int) -> None:
     """The adjoint fit: a 10 x 8 x 4 m room at 5 cm cells with 8
     materials on seeded patches, a 1-pole admittance each (16 parameters); the misfit of the
@@ -672,6 +748,8 @@ def main() -> None:
     parser.add_argument("--cell", type=float, default=0.04, help="cell size in metres (0.04: the full workload)")
     parser.add_argument("--no-fp64-rate", action="store_true", help="skip timing the FP64 stepper alike")
     parser.add_argument("--launch", default="", help="layer,special blocks per SM (skips the autotuner)")
+    parser.add_argument("--slabs", action="store_true",
+                        help="one grid split into z-slabs across the ranks, boundary planes swapped each step")  # fmt: skip
     parser.add_argument("--precision", choices=["fp32", "fp32c"], default="fp32",
                         help="fp32: the reference's arithmetic; fp32c: compensated single precision")  # fmt: skip
     parser.add_argument("--cpu-steps", type=int, default=10, help="steps of the CPU-baseline sample")
@@ -716,6 +794,9 @@ def main() -> None:
         return
     if args.workload == "shoebox_room":
         run_shoebox(args, world, rank, local)
+        return
+    if args.slabs:
+        run_slabs(args, world, rank, local)
         return
     if world > 1:
         from datetime import timedelta

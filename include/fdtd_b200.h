@@ -214,6 +214,15 @@ int fdtd_set_tape_budget(fdtd_solver *solver, uint64_t bytes);
  */
 int fdtd_autotune(fdtd_solver *solver, uint64_t trial_steps, int *layer_per_sm, int *special_per_sm);
 
+/*
+ * The device address and size of plane z of the current (which 0) or previous (1) pressure level
+ * between runs (no counterpart in the reference): pitch * ny elements, contiguous, pitch the row
+ * length rounded up to 16 cells. A grid split into slabs of planes across ranks exchanges its
+ * boundary planes through these after each step; the addresses change with the levels' roles, so
+ * ask again after every run.
+ */
+int fdtd_level_plane(fdtd_solver *solver, uint64_t z, int which, void **ptr, uint64_t *bytes);
+
 /* Sets those launch shapes directly (0 to 64 blocks per multiprocessor; 0: one thread a cell). */
 int fdtd_set_launch(fdtd_solver *solver, int layer_per_sm, int special_per_sm);
 

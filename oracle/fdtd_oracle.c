@@ -363,6 +363,8 @@ int oracle_reset(oracle_solver *s) {
     return FDTD_OK;
 }
 
+void *oracle_level(oracle_solver *s, int which) { return which ? s->u0 : s->u1; }
+
 int oracle_read_state(const oracle_solver *s, void *current, void *previous, void *branch_current,
                       void *branch_previous, void *layer_state) {
     const size_t e = s->precision == ORACLE_FP64 ? 8 : 4;

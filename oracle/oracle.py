@@ -70,6 +70,8 @@ def load_oracle() -> ctypes.CDLL:
         lib.oracle_reset.argtypes = [ctypes.c_void_p]
         lib.oracle_destroy.restype = None
         lib.oracle_destroy.argtypes = [ctypes.c_void_p]
+        lib.oracle_level.restype = ctypes.c_void_p
+        lib.oracle_level.argtypes = [ctypes.c_void_p, ctypes.c_int]
         lib.oracle_read_state.restype = ctypes.c_int
         lib.oracle_read_state.argtypes = [ctypes.c_void_p] * 6
         lib.oracle_error.restype = ctypes.c_char_p
@@ -110,6 +112,10 @@ class OracleSolver:
 
     def reset(self) -> None:
         self._lib.oracle_reset(self._handle)
+
+    def level_pointer(self, which: int = 0) -> int:
+        """The address of the current (0) or previous (1) pressure level, between runs."""
+        return int(self._lib.oracle_level(self._handle, which))
 
     def state(self) -> dict[str, np.ndarray]:
         dtype = np.float64 if self.precision == "fp64" else np.float32

@@ -1,0 +1,145 @@
+"""One grid stepped as slabs of z-planes (acoustic_spaces_b200.slabs): each slab's probes and
+pressure equal the whole grid's, bit for bit.
+
+On the CPU the slabs are stepped by the oracle — in one process, and as two ``gloo`` ranks that
+exchange their boundary planes through torch.distributed as NCCL ranks would; on the GPU by
+B200 steppers on one device, the ghost planes filled by device copies between steps (the host
+orders every step; no kernel waits on another).
+"""
+
+from __future__ import annotations
+
+import os
+import socket
+
+import numpy as np
+import pytest
+from conftest import load_golden
+
+from acoustic_spaces_b200 import layouts as L
+from acoustic_spaces_b200 import slabs
+from oracle.oracle import OracleSolver
+
+CASES = ["open_layer", "open_layer_speed", "resonant19", "speed7", "fitted_open", "drive7"]
+
+
+def _whole_and_slabs(layout, signal, world):
+    whole = OracleSolver(layout)
+    expected = whole.run(signal)
+    bounds = slabs.partition_planes(layout, world)
+    parts = [slabs.slab(layout, bounds, r) for r in range(world)]
+    oracles = [OracleSolver(p.layout) for p in parts]
+    planes = [slabs.oracle_planes(o, p) for o, p in zip(oracles, parts)]
+    records = slabs.step_slabs(oracles, planes, parts, signal, lambda o, piece: o.run(piece))
+    probes = len(np.asarray(layout["probe_start"])) - 1
+    return whole, expected, parts, oracles, slabs.gather_records(parts, records, probes, len(signal))
+
+
+def test_planes_partition_without_cutting_a_probe():
+    w = L.polyhedral_room(0, cell=0.2, steps=10)
+    lay = w.built.layout
+    nz = int(lay["shape"][2])
+    for world in (2, 3, 5):
+        bounds = slabs.partition_planes(lay, world)
+        assert bounds[0][0] == 0 and bounds[-1][1] == nz
+        assert all(a[1] == b[0] for a, b in zip(bounds[:-1], bounds[1:]))
+        for lo, hi in slabs._probe_spans(lay):
+            assert not any(lo < b0 <= hi for b0, _ in bounds[1:])
+        parts = [slabs.slab(lay, bounds, r) for r in range(world)]
+        assert sorted(p for s in parts for p in s.probes) == list(range(len(lay["probe_start"]) - 1))
+        assert sum(len(s.layout["special"]) for s in parts) == len(lay["special"])
+        assert sum(len(s.layout["layer_cells"]) for s in parts) == len(lay["layer_cells"])
+
+
+@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("world", [2, 3])
+def test_slabs_step_the_golden_grids_as_the_whole(name, world):
+    layout, signal, _ = load_golden(name)
+    signal = signal[:150]
+    try:
+        whole, expected, parts, oracles, got = _whole_and_slabs(layout, signal, world)
+    except ValueError as error:
+        pytest.skip(str(error))  # a small grid whose probes leave no boundary
+    assert np.array_equal(got, expected)
+    # and the pressure of every slab's own planes equals the whole grid's
+    current = whole.state()["current"]
+    nx, ny, _ = (int(v) for v in layout["shape"])
+    for s, o in zip(parts, oracles):
+        mine = o.state()["current"][(s.z0 - s.lo) * nx * ny : (s.z1 - s.lo) * nx * ny]
+        assert np.array_equal(mine, current[s.z0 * nx * ny : s.z1 * nx * ny])
+
+
+def test_slabs_step_the_polyhedral_room_as_the_whole():
+    # 100 x 75 x 50: the open room with its resonant walls and 8-cell matched layer, as 4 slabs
+    w = L.polyhedral_room(0, cell=0.2, steps=200)
+    _, expected, _, _, got = _whole_and_slabs(w.built.layout, w.signal, 4)
+    assert np.array_equal(got, expected)
+
+
+def _rank(rank: int, world: int, port: int, out):
+    import torch.distributed as dist
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        w = L.polyhedral_room(0, cell=0.2, steps=120)
+        bounds = slabs.partition_planes(w.built.layout, world)
+        part = slabs.slab(w.built.layout, bounds, rank)
+        oracle = OracleSolver(part.layout)
+        planes = slabs.oracle_planes(oracle, part)
+        rec = []
+        for k in range(len(w.signal)):
+            rec.append(oracle.run(w.signal[k : k + 1]))
+            slabs.exchange_ghosts(planes, part, rank, world, dist)
+        out.put((rank, part.probes, np.concatenate(rec, axis=1)))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_step_the_room_as_the_whole():
+    import multiprocessing as mp
+
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    procs = [ctx.Process(target=_rank, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    results = [out.get(timeout=300) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    w = L.polyhedral_room(0, cell=0.2, steps=120)
+    expected = OracleSolver(w.built.layout).run(w.signal)
+    got = np.full_like(expected, np.nan)
+    for _, probes, rec in results:
+        for j, p in enumerate(probes):
+            got[p] = rec[j]
+    assert np.array_equal(got, expected)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["open_layer", "resonant19", "speed7"])
+def test_gpu_slabs_step_as_the_whole_grid(name):
+    import torch
+
+    from acoustic_spaces_b200 import B200WaveSolver
+
+    layout, signal, _ = load_golden(name)
+    signal = signal[:120]
+    bounds = slabs.partition_planes(layout, 2)
+    parts = [slabs.slab(layout, bounds, r) for r in range(2)]
+    gpus = [B200WaveSolver(p.layout, autotune=False) for p in parts]
+    planes = [slabs.DevicePlanes(g) for g in gpus]
+
+    def sync():
+        for g in gpus:
+            g.synchronize()
+        torch.cuda.synchronize()
+
+    records = slabs.step_slabs(gpus, planes, parts, signal, lambda g, piece: g.run(piece), sync)
+    probes = len(np.asarray(layout["probe_start"])) - 1
+    got = slabs.gather_records(parts, records, probes, len(signal))
+    assert np.array_equal(got, OracleSolver(layout).run(signal))
