@@ -80,7 +80,9 @@ def decay_times(p: np.ndarray, rate: float) -> tuple[float, float]:
     decay of p^2 in dB, a least-squares line from its first sample at or below 0 dB (EDT) or -5 dB
     (T30) to its first at or below -10 or -35 dB, -60 dB over its slope (the ranges of ISO 3382,
     as src/acoustic_spaces/parameters.py:55 and :266-296 of the reference fit them, here without
-    its estimate of the energy past the response's end). NaN where the curve does not fall so far."""
+    its estimate of the energy past the response's end). NaN where the curve does not fall so far
+    within the first 80 % of the response: without that estimate every curve plunges at the end,
+    which is the response's truncation, not its decay (parameters.py:454-462 refuses such curves)."""
     e = np.cumsum((p * p)[::-1])[::-1]
     if e[0] <= 0:
         return float("nan"), float("nan")
@@ -94,7 +96,7 @@ def decay_times(p: np.ndarray, rate: float) -> tuple[float, float]:
             out.append(float("nan"))
             continue
         start, stop = int(np.argmax(level <= top)), int(np.argmax(below))
-        if stop - start < 2:
+        if stop - start < 2 or stop >= 0.8 * len(p):
             out.append(float("nan"))
             continue
         slope = np.polyfit(t[start : stop + 1], level[start : stop + 1], 1)[0]
