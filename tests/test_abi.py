@@ -170,3 +170,15 @@ def test_without_a_device_creation_says_so():
     assert status == _abi.FDTD_ENODEV and "no CUDA device" in error
     with pytest.raises(RuntimeError, match="CUDA device"):
         B200WaveSolver(layout)
+
+
+def test_the_loader_refuses_a_library_built_from_other_sources(monkeypatch):
+    # The library carries the digest of the sources it was built from; a stale build is refused
+    # rather than run.
+    from acoustic_spaces_b200 import build
+
+    assert _abi.load_library().fdtd_build_id().decode() == build.source_id()
+    monkeypatch.setattr(_abi, "_lib", None)
+    monkeypatch.setattr(build, "source_id", lambda: "not-these-sources")
+    with pytest.raises(RuntimeError, match="built from other sources"):
+        _abi.load_library()
