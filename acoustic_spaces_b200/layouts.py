@@ -1083,6 +1083,8 @@ class Batch:
     signal: np.ndarray
     rate: float
     description: dict
+    # each solve's scene: (room, grid, source, receivers), for the reference to lay out alike
+    scenes: list = field(default_factory=list)
 
 
 def partition(cells: list[int], world: int) -> list[list[int]]:
@@ -1120,7 +1122,7 @@ def batched_rooms(
     rate = speed_of_sound / (COURANT * cell)
     sizes = [np.random.default_rng([seed, k]).uniform(dims[0], dims[1], 3) for k in range(rooms)]
     mine = partition([int(np.prod(room_grid(size, cell).shape)) for size in sizes], part[1])[part[0]]
-    layouts, cells = [], []
+    layouts, cells, scenes = [], [], []
     for k in mine:
         rng = np.random.default_rng([seed, k])
         size = rng.uniform(dims[0], dims[1], 3)
@@ -1133,9 +1135,10 @@ def batched_rooms(
             while np.min(np.linalg.norm(src - rec[k], axis=1)) < 4 * cell:
                 rec[k] = inside_points(rng, room, size, 1, 0.5)[0]
         grid = room_grid(size, cell)
-        for built in cell_face_layouts(room, grid, list(src), rec, rate=rate):
+        for j, built in enumerate(cell_face_layouts(room, grid, list(src), rec, rate=rate)):
             layouts.append(built.layout)
             cells.append(built.air_cells)
+            scenes.append((room, grid, src[j], rec))
     stacked = stack(layouts)
     description = {
         "rooms": rooms,
@@ -1153,4 +1156,4 @@ def batched_rooms(
         "walls": "cell faces, real admittance per wall from absorption U[%g, %g]" % absorption,
         "seed": seed,
     }
-    return Batch(stacked, layouts, gaussian_drive(rate, steps), rate, description)
+    return Batch(stacked, layouts, gaussian_drive(rate, steps), rate, description, scenes)

@@ -352,6 +352,40 @@ def run_reference(args, rank: int, world: int) -> None:
     print(json.dumps(line), flush=True)
 
 
+def batch_reference_rate(batch, sample, sample_steps: int) -> dict:
+    """The reference's own solver (oracle/_ref) on two solves of ``sample``, each laid out by the
+    reference from its scene (a box with real walls, one source), every host thread, timed over
+    ``sample_steps`` steps each: cell updates per second, the rate the whole batch would run at."""
+    from acoustic_spaces_b200 import layouts
+    from oracle import oracle
+
+    native = oracle.reference_native()
+    if native is None:
+        raise RuntimeError("the reference's solver is not built")
+    threads = os.cpu_count() or 1
+    cells, seconds, used = 0, 0.0, []
+    for k in list(sample)[:2]:
+        room, grid, source, receivers = batch.scenes[k]
+        vertices, faces, owner = layouts.room_mesh(room)
+        beta = np.array([m.beta for m in room.materials])
+        solver = native.WaveSolver(
+            native.Bvh(vertices, faces), owner, beta, np.zeros((0, 3)), np.zeros(0, np.int64), grid.origin,
+            grid.cell, *grid.shape, source, receivers, layer=0, layer_damping=0.0, threads=threads,
+        )  # fmt: skip
+        air = int(solver.air_cells)
+        if air != int(np.count_nonzero(batch.layouts[k]["types"])):
+            raise RuntimeError("the reference lays a solve out otherwise than the builder")
+        solver.run(batch.signal[:2])
+        t0 = time.perf_counter()
+        solver.run(batch.signal[:sample_steps])
+        seconds += time.perf_counter() - t0
+        cells += air * sample_steps
+        used.append(k)
+        threads = int(solver.threads)
+    return {"value": round(cells / seconds / 1e9, 4), "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"solves {used} of the batch, {sample_steps} steps each, scaled as cell updates per second"}  # fmt: skip
+
+
 def run_batched(args, world: int, rank: int, local: int) -> None:
     """The batched configuration: many shoebox rooms with several sources each, every (room,
     source) a solve of its own, stacked into one grid and stepped by one launch per kind per step
@@ -426,6 +460,14 @@ def run_batched(args, world: int, rank: int, local: int) -> None:
         seq_cells += one.air_cells * steps
         one.close()
     sequential = seq_cells / seq_s / 1e9
+    # The reference's own CPU solver on two of the solves (seeded), every host thread, over a
+    # bounded sample of steps; scaled as cell updates per second.
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        try:
+            cpu = batch_reference_rate(batch, sample, args.cpu_steps)
+        except Exception as error:  # the baseline is reported, not required
+            cpu = {"value": None, "unit": UNIT, "error": str(error)[:200]}
     # Each solve's FP32 response against FP64 (the stacked grid in both).
     m = min(args.ir_steps, steps)
     solver.reset()
@@ -457,6 +499,7 @@ def run_batched(args, world: int, rank: int, local: int) -> None:
                               "api": "B200WaveSolver.run, one solve after another, on one GPU"},  # fmt: skip
         "batched_over_sequential": round(value / world / sequential, 3),
         "per_solve_ir_rel_l2_vs_fp64": {"max": float(max(worst)), "median": float(np.median(worst)), "steps": m},
+        "cpu_baseline": cpu,
         "clocks": clocks.summary(),
         "gpu_launches": 3 * steps,  # the sweep, the special rows, the probes
     }

@@ -129,6 +129,24 @@ def test_the_plain_shoebox_is_laid_out_as_the_reference_lays_it():
     assert np.array_equal(solver.run(w.signal), OracleSolver(w.built.layout).run(w.signal))
 
 
+def test_the_batched_solves_are_laid_out_as_the_reference_lays_them():
+    # Each (room, source) of the batch, from its scene, laid out by the reference: array for array.
+    if not cases.available():
+        pytest.skip("the reference sources are not here")
+    b = L.batched_rooms(2, rooms=2, sources=2, cell=0.1, dims=(2.0, 4.0), steps=10)
+    native = cases.reference_native()
+    for lay, (room, grid, source, receivers) in zip(b.layouts, b.scenes):
+        vertices, faces, owner = L.room_mesh(room)
+        beta = np.array([m.beta for m in room.materials])
+        solver = native.WaveSolver(
+            native.Bvh(vertices, faces), owner, beta, np.zeros((0, 3)), np.zeros(0, np.int64), grid.origin,
+            grid.cell, *grid.shape, source, receivers, layer=0, layer_damping=0.0, threads=2,
+        )  # fmt: skip
+        ref = solver.layout()
+        for name, value in lay.items():
+            assert np.array_equal(np.asarray(value), np.asarray(ref[name])), name
+
+
 def test_the_polyhedral_workload_is_seeded():
     a = L.polyhedral_room(0, cell=0.2, steps=10)
     b = L.polyhedral_room(0, cell=0.2, steps=10)
