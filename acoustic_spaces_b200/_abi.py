@@ -240,6 +240,7 @@ SIGNATURES = {
     "fdtd_set_launch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
     "fdtd_level_plane": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int,
                                         ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_uint64)]),
+    "fdtd_test_wait": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32]),
     "fdtd_set_tape": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
     "fdtd_set_coefficients": (ctypes.c_int, [ctypes.c_void_p, _f32p, _f32p, _f32p, _f32p, _f32p]),
     "fdtd_get_timing": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_uint64)]),

@@ -532,6 +532,9 @@ int check_device_error(fdtd_solver *s) {
     CUDA_TRY(s, cudaStreamSynchronize(s->stream));
     if (flag) {
         CUDA_TRY(s, cudaMemsetAsync(s->d_error, 0, sizeof flag, s->stream));
+        CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+        if (flag & kWaitTestBit)
+            return fail(s, FDTD_ECUDA, "a bounded wait gave up (fdtd_test_wait: the flag it waited on was never set)");
         return fail(s, FDTD_ECUDA, "a pipeline wait of the interior sweep gave up; the step's results are not valid");
     }
     return FDTD_OK;
@@ -1728,6 +1731,23 @@ int fdtd_set_coefficients(fdtd_solver *s, const float *coef_b, const float *coef
     }
     s->tape_valid = false;
     return FDTD_OK;
+}
+
+int fdtd_test_wait(fdtd_solver *s, uint32_t spins) {
+    if (!s) return set_global(FDTD_EINVAL, "no solver");
+    if (spins == 0 || spins > (1u << 24)) return fail(s, FDTD_EINVAL, "spins are 1 to 2^24");
+    DeviceGuard guard(s->device);
+    void *p = nullptr;
+    CUDA_TRY(s, cudaMalloc(&p, sizeof(unsigned int)));
+    cudaError_t e = cudaMemsetAsync(p, 0, sizeof(unsigned int), s->stream);
+    if (e == cudaSuccess) {
+        wait_test_kernel<<<1, 32, 0, s->stream>>>(static_cast<const unsigned int *>(p), spins, s->d_error);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    cudaFree(p);
+    if (e != cudaSuccess) return cuda_fail(s, e, "fdtd_test_wait");
+    return check_device_error(s);
 }
 
 int fdtd_level_plane(fdtd_solver *s, uint64_t z, int which, void **ptr, uint64_t *bytes) {

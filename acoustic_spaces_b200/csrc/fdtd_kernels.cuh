@@ -137,6 +137,20 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map
         : "memory");
 }
 
+// The error flag's bits: 1 an interior sweep's wait gave up; kWaitTestBit fdtd_test_wait's.
+constexpr unsigned int kWaitTestBit = 2u;
+
+// The failure path of a bounded wait, on its own (fdtd_test_wait): lane 0 polls a flag that
+// nothing sets, at most `spins` times, then sets the error flag and returns, as a kernel whose
+// wait gave up does; the host reads the flag as a status.
+__global__ void wait_test_kernel(const unsigned int *flag, uint32_t spins, unsigned int *error) {
+    if (threadIdx.x != 0) return;
+    const volatile unsigned int *f = flag;
+    for (uint32_t i = 0; i < spins; ++i)
+        if (*f) return;
+    atomicOr(error, kWaitTestBit);
+}
+
 // ---- interior air ------------------------------------------------------------------------------
 
 // Interior air (fdtd.hpp:242-288). The interior cells are covered by tiles of kTX x kTY cells by a

@@ -258,6 +258,13 @@ class B200WaveSolver:
             _raise(self._lib, status, self._handle)
         return int(ptr.value or 0), int(nbytes.value)
 
+    def test_wait(self, spins: int = 1 << 16) -> None:
+        """Runs the kernels' bounded-wait failure path on its own (a wait on a flag nothing sets);
+        raises RuntimeError with the status's message, as an expired wait in a step would."""
+        status = self._lib.fdtd_test_wait(self._handle, int(spins))
+        if status != _abi.FDTD_OK:
+            _raise(self._lib, status, self._handle)
+
     def set_launch(self, layer_blocks_per_sm: int, special_blocks_per_sm: int) -> None:
         """Sets the matched-layer and special-row kernels' blocks per multiprocessor (0: one
         thread a cell), as :meth:`autotune` would."""

@@ -223,6 +223,14 @@ int fdtd_autotune(fdtd_solver *solver, uint64_t trial_steps, int *layer_per_sm, 
  */
 int fdtd_level_plane(fdtd_solver *solver, uint64_t z, int which, void **ptr, uint64_t *bytes);
 
+/*
+ * The failure path of the kernels' bounded waits, on its own (no counterpart in the reference):
+ * a kernel polls a device flag that nothing sets, at most `spins` times (1 to 2^24), then reports
+ * through the error flag as a kernel whose wait gave up does; returns that status (FDTD_ECUDA
+ * and its message). The handle stays usable. No GPU is faulted or hung: the wait is bounded.
+ */
+int fdtd_test_wait(fdtd_solver *solver, uint32_t spins);
+
 /* Sets those launch shapes directly (0 to 64 blocks per multiprocessor; 0: one thread a cell). */
 int fdtd_set_launch(fdtd_solver *solver, int layer_per_sm, int special_per_sm);
 

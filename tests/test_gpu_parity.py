@@ -215,3 +215,13 @@ def test_gpu_autotuned_launch_shapes_step_as_the_oracle_does():
     assert np.array_equal(_pieces(gpu, w.signal, [0, 64, 128, 200]), OracleSolver(w.built.layout).run(w.signal))
     with pytest.raises(ValueError, match="from rest"):
         gpu.autotune()
+
+
+def test_gpu_an_expired_wait_is_a_status_and_the_handle_stays_usable():
+    # Failure detection without a fault: a bounded wait on a flag that nothing sets gives up, the
+    # error flag carries it to the host as a status, and the handle steps on as before.
+    layout, signal, reference = load_golden("resonant7")
+    gpu = B200WaveSolver(layout)
+    with pytest.raises(RuntimeError, match="bounded wait gave up"):
+        gpu.test_wait(1 << 12)
+    assert np.array_equal(gpu.run(signal), reference)
