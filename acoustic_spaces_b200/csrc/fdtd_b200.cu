@@ -211,7 +211,9 @@ int zeros(fdtd_solver *s, size_t bytes, void **out) {
     CUDA_TRY(s, cudaMalloc(&p, bytes ? bytes : 16));
     s->allocations.push_back(p);
     s->device_bytes += bytes;
-    CUDA_TRY(s, cudaMemset(p, 0, bytes ? bytes : 16));
+    // On the handle's stream, which every later use of the buffer follows (the streams are
+    // non-blocking: they do not wait for the legacy default stream).
+    CUDA_TRY(s, cudaMemsetAsync(p, 0, bytes ? bytes : 16, s->stream));
     *out = p;
     return FDTD_OK;
 }
@@ -1482,7 +1484,12 @@ int fdtd_create(const fdtd_layout *layout, int precision, int device, fdtd_solve
         delete s;
         return rc;
     }
-    const int rc = build(s, layout);
+    int rc = build(s, layout);
+    // Every upload and clearing of the set-up complete before the handle's streams use them.
+    if (rc == FDTD_OK) {
+        const cudaError_t synced = cudaDeviceSynchronize();
+        if (synced != cudaSuccess) rc = cuda_fail(s, synced, "cudaDeviceSynchronize");
+    }
     if (rc != FDTD_OK) {
         g_error = s->error;
         release(s);
@@ -1729,6 +1736,9 @@ int fdtd_set_coefficients(fdtd_solver *s, const float *coef_b, const float *coef
             CUDA_TRY(s, cudaMemcpy(const_cast<double *>(t.corrected_coef), coef.data(), 8 * coef.size(),
                                    cudaMemcpyHostToDevice));
     }
+    // (Copies from pageable memory may return before they land; the handle's streams do not wait
+    // for the default stream.)
+    CUDA_TRY(s, cudaDeviceSynchronize());
     s->tape_valid = false;
     return FDTD_OK;
 }
@@ -1789,7 +1799,7 @@ int fdtd_autotune(fdtd_solver *s, uint64_t trial_steps, int *layer_per_sm, int *
         void *&a, *&b;
         ~Free() { cudaFree(a), cudaFree(b); }
     } release_trials{sig, rec};
-    CUDA_TRY(s, cudaMemset(sig, 0, sizeof(float) * trial_steps));
+    CUDA_TRY(s, cudaMemsetAsync(sig, 0, sizeof(float) * trial_steps, s->stream));
     CUDA_TRY(s, cudaMalloc(&rec, sizeof(double) * trial_steps * std::max<uint64_t>(1, s->probes)));
     cudaEvent_t start, end;
     CUDA_TRY(s, cudaEventCreate(&start));
