@@ -404,7 +404,7 @@ def run_batched(args, world: int, rank: int, local: int) -> None:
     batch = layouts.batched_rooms(args.seed, rooms=args.rooms, sources=args.sources, steps=args.steps + args.warmup,
                                   part=(rank, world))  # fmt: skip
     desc = batch.description
-    solver = B200WaveSolver(batch.stacked.layout, device=local)
+    solver = B200WaveSolver(batch.stacked.layout, precision=args.precision, device=local)
     air = batch.stacked.air_cells
     steps, warmup = args.steps, args.warmup
     sig = torch.from_numpy(np.ascontiguousarray(batch.signal)).to(f"cuda:{local}")
@@ -450,7 +450,7 @@ def run_batched(args, world: int, rank: int, local: int) -> None:
     sample = sorted(rng.choice(len(batch.layouts), size=min(args.sequential_sample, len(batch.layouts)), replace=False))
     seq_cells, seq_s = 0, 0.0
     for k in sample:
-        one = B200WaveSolver(batch.layouts[k], device=local)
+        one = B200WaveSolver(batch.layouts[k], precision=args.precision, device=local)
         one.run(batch.signal[: max(warmup, 130)])  # both of its step graphs captured before timing
         one.reset()
         torch.cuda.synchronize()
@@ -492,7 +492,9 @@ def run_batched(args, world: int, rank: int, local: int) -> None:
         "dtype": "f32",
         "data": "synthetic",
         "config": {"workload": "batched_rooms", **desc, "air_cells_all_ranks": total_air,
-                   "parallelism": f"solves sharded over {world} GPUs by cell count" if world > 1 else "single GPU"},
+                   "parallelism": f"solves sharded over {world} GPUs by cell count" if world > 1 else "single GPU",
+                   "precision": "FP32, bit-exact with the reference" if args.precision == "fp32"
+                   else "FP32 compensated: each cell's pressure and its increment"},
         "e2e": {"value": round(total_air * steps / e2e_s / 1e9, 4), "unit": UNIT, "h2d_bytes_per_step": 4,
                 "d2h_bytes_per_step": 8 * solver.probes},  # fmt: skip
         "sequential_solves": {"value": round(sequential, 4), "unit": UNIT, "solves_timed": len(sample),
