@@ -271,6 +271,30 @@ def _layer_tables(size: int, layer: int, damping: float, courant: float, ends=(T
     return f32(ck), f32(cp), f32(fk), f32(fp)
 
 
+def layer_tables_tangent(size: int, layer: int, damping: float, courant: float, ends=(True, True)):
+    """The derivatives in ``damping`` of :func:`_layer_tables`'s keep and push of the centres and
+    the faces (float64): with d = damping * into^2 (into the layer's depth fraction),
+    keep = (1 - d) / (1 + d) and push = courant / (1 + d) give d keep = -2 into^2 / (1 + d)^2 and
+    d push = -courant into^2 / (1 + d)^2 — the chain from a gradient in the tables to one in the
+    layer's damping."""
+
+    def into2(from_edge: float) -> float:
+        into = max(0.0, layer + 0.5 - from_edge) / layer
+        return into * into
+
+    last, far = float(size - 1), float("inf")
+    out = {"keep": [], "push": [], "keep_face": [], "push_face": []}
+    for x in range(size + 1):
+        c = float(x)
+        for kind, edge in (("", min(c if ends[0] else far, last - c if ends[1] else far)),
+                           ("_face", min(c - 0.5 if ends[0] else far, last - c + 0.5 if ends[1] else far))):  # fmt: skip
+            i2 = into2(edge)
+            d = damping * i2
+            out["keep" + kind].append(-2.0 * i2 / (1.0 + d) ** 2)
+            out["push" + kind].append(-courant * i2 / (1.0 + d) ** 2)
+    return {k: np.array(v, np.float64) for k, v in out.items()}
+
+
 def cell_face_layout(room: Room, grid: Grid, source, probes, **options) -> Built:
     """The reference's layout of ``room`` on ``grid`` with walls on cell faces, the 7-point
     stencil, a uniform speed ratio ``speed`` (None: the grid's), the source at ``source`` and

@@ -5,13 +5,21 @@ This is the checker of the CUDA reverse-time stepper. It differentiates the forw
 reference steps it (special rows fdtd.hpp:860-881, interior cells fdtd.hpp:242-288 for the
 7-point stencil, probes fdtd.hpp:3525-3533), written here with whole-array torch operations, and
 shares no derivation with the hand-written transposed operator of the CUDA library. Grids of the
-7-point stencil without a matched layer or a speed field only, the case the CUDA adjoint covers.
+7-point stencil without a speed field. With a matched layer it also steps the layer as the
+reference does (fdtd.hpp:2242-2264: each cell its own copy of both faces on every axis) and gives
+the gradient in the layer's twelve coefficient tables (keep and push of the centres and the faces
+per axis, fdtd.hpp:2219-2238) — the checker of a gradient in the layer's parameters, which the
+CUDA adjoint does not compute yet (it refuses grids with a matched layer).
 """
 
 from __future__ import annotations
 
 import numpy as np
 import torch
+
+#: The layer's tables: per axis the centres' keep, the faces' keep (and the same for push).
+KEEP = ("keep_x", "keep_face_x", "keep_y", "keep_face_y", "keep_z", "keep_face_z")
+PUSH = ("push_x", "push_face_x", "push_y", "push_face_y", "push_z", "push_face_z")
 
 # The link directions of fdtd.hpp:924-927: six axial, then the twelve edge neighbours.
 _DIRECTIONS = (
@@ -24,12 +32,12 @@ _DIRECTIONS = (
 class AutogradStepper:
     """The forward scheme of one layout in float64 torch, differentiable in the special rows'
     coef_b, coef_inv and the branch states' now, before, gain (one leaf per state, as the CUDA
-    gradient reports them)."""
+    gradient reports them), and with a matched layer in its twelve tables (KEEP, PUSH)."""
 
     def __init__(self, layout) -> None:
         nx, ny, nz = (int(v) for v in layout["shape"])
-        if len(layout.get("layer_cells", ())) or len(np.asarray(layout.get("scale", ()))):
-            raise ValueError("the autograd stepper covers grids without a matched layer or speed field")
+        if len(np.asarray(layout.get("scale", ()))):
+            raise ValueError("the autograd stepper covers grids without a speed field")
         if int(np.asarray(layout["stencil"]).reshape(-1)[0]) != 7:
             raise ValueError("the autograd stepper covers the 7-point stencil")
         sy, sz = nx, nx * ny
@@ -61,6 +69,14 @@ class AutogradStepper:
             "before": torch.tensor(np.asarray(layout["branch_before"], np.float64)[branch], dtype=d, requires_grad=True),
             "gain": torch.tensor(np.asarray(layout["branch_gain"], np.float64)[branch], dtype=d, requires_grad=True),
         }
+        # The matched layer: its cells, their coordinates and strides per axis, and the tables.
+        self.layer = torch.as_tensor(np.asarray(layout.get("layer_cells", np.zeros(0)), np.int64))
+        self.strides = (1, sy, sz)
+        if len(self.layer):
+            cells = self.layer
+            self.coords = (cells % nx, (cells // sy) % ny, cells // sz)
+            for name in KEEP + PUSH:
+                self.params[name] = torch.tensor(np.asarray(layout[name], np.float64), dtype=d, requires_grad=True)
         probe_start = np.asarray(layout["probe_start"], np.int64)
         self.probes = len(probe_start) - 1
         self.probe_row = torch.as_tensor(np.repeat(np.arange(self.probes), np.diff(probe_start)))
@@ -68,7 +84,6 @@ class AutogradStepper:
         self.probe_weights = torch.as_tensor(np.asarray(layout["probe_weights"], np.float64))
 
     def run(self, signal) -> torch.Tensor:
-        """The probe series (probes, steps) from a zero state, differentiable in the parameters."""
         p = self.params
         specials = len(self.special)
         states = len(self.state_row)
@@ -76,6 +91,19 @@ class AutogradStepper:
         b = torch.zeros(self.n, dtype=torch.float64)
         wa = torch.zeros(states, dtype=torch.float64)
         wb = torch.zeros(states, dtype=torch.float64)
+        cells = len(self.layer)
+        # The layer's nine values per cell: the parts, and per axis the - face and the + face.
+        parts = [torch.zeros(cells, dtype=torch.float64) for _ in range(3)]
+        below = [torch.zeros(cells, dtype=torch.float64) for _ in range(3)]
+        above = [torch.zeros(cells, dtype=torch.float64) for _ in range(3)]
+        # Each layer cell's coefficients, gathered from the tables once (one gather node each,
+        # whose gradient the steps accumulate).
+        coef = []
+        for axis in range(3) if cells else ():
+            x = self.coords[axis]
+            keep, keep_face = p[KEEP[2 * axis]], p[KEEP[2 * axis + 1]]
+            push, push_face = p[PUSH[2 * axis]], p[PUSH[2 * axis + 1]]
+            coef.append((keep[x], push[x], keep_face[x], push_face[x], keep_face[x + 1], push_face[x + 1]))
         series = []
         for s in np.asarray(signal, np.float64):
             series.append(torch.zeros(self.probes, dtype=torch.float64).index_add(
@@ -89,14 +117,44 @@ class AutogradStepper:
             rows = (self.coef_a * b[self.special] + links - p["coef_b"] * previous - flow + self.source * s) * p["coef_inv"]
             w_next = wa + (rows - previous)[self.state_row] * p["gain"] + own
             new = a.index_put((self.interior,), interior).index_put((self.special,), rows)
+            if cells:
+                here = b[self.layer]
+                total = torch.zeros(cells, dtype=torch.float64)
+                for axis in range(3):
+                    st = self.strides[axis]
+                    keep, push, keep_lo, push_lo, keep_hi, push_hi = coef[axis]
+                    below[axis] = keep_lo * below[axis] - push_lo * (here - b[self.layer - st])
+                    above[axis] = keep_hi * above[axis] - push_hi * (b[self.layer + st] - here)
+                    parts[axis] = keep * parts[axis] - push * (above[axis] - below[axis])
+                    total = total + parts[axis]
+                new = new.index_put((self.layer,), total)
             a, b, wa, wb = b, new, wb, w_next
         return torch.stack(series, 1)
 
 
+class _Flushed:
+    """Subnormal results flush to zero while the checker runs, forward and backward: values below
+    1e-308 (ahead of the wavefront, where the stencil's reach leaves vanishing values) would slow
+    the CPU's arithmetic a hundredfold; the FP64 oracle keeps them, which changes nothing at the
+    checks' tolerances."""
+
+    def __enter__(self):
+        # (The flag is the calling thread's: torch's operations run on that thread alone meanwhile.)
+        self.threads = torch.get_num_threads()
+        torch.set_num_threads(1)
+        self.set = torch.set_flush_denormal(True)
+
+    def __exit__(self, *exc):
+        if self.set:
+            torch.set_flush_denormal(False)
+        torch.set_num_threads(self.threads)
+
+
 def gradient(layout, signal, dloss_dy) -> dict[str, np.ndarray]:
-    """dL/d(coef_b, coef_inv per special row; now, before, gain per branch state) for a loss whose
-    derivative by the probe series is dloss_dy (probes, steps): the vector-Jacobian product."""
-    with torch.enable_grad():  # also when called from inside another backward pass
+    """dL/d(coef_b, coef_inv per special row; now, before, gain per branch state; with a matched
+    layer, every entry of its twelve tables) for a loss whose derivative by the probe series is
+    dloss_dy (probes, steps): the vector-Jacobian product."""
+    with torch.enable_grad(), _Flushed():  # also when called from inside another backward pass
         stepper = AutogradStepper(layout)
         y = stepper.run(signal)
         y.backward(torch.as_tensor(np.asarray(dloss_dy, np.float64)))
@@ -104,5 +162,5 @@ def gradient(layout, signal, dloss_dy) -> dict[str, np.ndarray]:
 
 
 def series(layout, signal) -> np.ndarray:
-    with torch.no_grad():
+    with torch.no_grad(), _Flushed():
         return AutogradStepper(layout).run(signal).numpy()

@@ -100,3 +100,75 @@ def test_central_difference_of_the_material_parameters(monkeypatch):
             t = (cu[name] - cd[name]) / (2 * h)
             tangent += float(np.sum(G[key][:B] * t) if name.startswith("coef") else np.sum(G[key] * t[branch]))
         assert abs(grad[index] - tangent) <= 1e-5 * np.max(np.abs(grad)), (index, grad[index], tangent)
+
+
+# ---- the matched layer's parameters --------------------------------------------------------------
+
+_TABLES = adjoint_reference.KEEP + adjoint_reference.PUSH
+
+
+@pytest.mark.parametrize("name", ["open_layer", "fitted_open"])
+def test_the_autograd_stepper_steps_a_matched_layer_as_the_oracle(name):
+    layout, signal, _ = load_golden(name)
+    ours = adjoint_reference.series(layout, signal[:200])
+    oracle = OracleSolver(layout, "fp64").run(signal[:200])
+    assert np.max(np.abs(ours - oracle)) <= 1e-12 * np.max(np.abs(oracle))
+
+
+def test_the_layer_tables_gradient_matches_symmetric_central_differences():
+    # Every entry of the twelve tables stepped by a whole number of float32 units at once: the
+    # directional derivative from the gradient against the loss's central difference.
+    layout, signal, _ = load_golden("open_layer")
+    signal = signal[:150]
+    y, target = _misfit(layout, signal)
+    grad = adjoint_reference.gradient(layout, signal, 2.0 * (y - target))
+    rng = np.random.default_rng(2)
+    plus, minus, predicted = dict(layout), dict(layout), 0.0
+    for name in _TABLES:
+        c0 = np.asarray(layout[name], np.float32)
+        unit = np.spacing(np.abs(c0)).astype(np.float64)
+        d = np.round(1e-5 * np.abs(c0.astype(np.float64)) * rng.uniform(-1, 1, len(c0)) / unit) * unit
+        plus[name] = (c0.astype(np.float64) + d).astype(np.float32)
+        minus[name] = (c0.astype(np.float64) - d).astype(np.float32)
+        assert np.array_equal(plus[name].astype(np.float64) - c0, d)
+        predicted += float(np.sum(grad[name] * d))
+    loss = lambda lay: float(np.sum((OracleSolver(lay, "fp64").run(signal) - target) ** 2))  # noqa: E731
+    measured = 0.5 * (loss(plus) - loss(minus))
+    assert abs(measured) > 0.0
+    assert abs(predicted - measured) <= 1e-4 * abs(measured), (predicted, measured)
+
+
+def test_the_layer_damping_gradient_by_the_chain_rule():
+    # dL/d(layer damping) = the tables' gradient times their tangent in the damping
+    # (layouts.layer_tables_tangent), against a central difference of the loss in the damping with
+    # the room laid out again at damping -+ h: a 4 x 3 x 2.4 m convex room at 10 cm, open through
+    # one face into a 4-cell matched layer.
+    from acoustic_spaces_b200 import layouts as L
+
+    cell, box, layer, damping = 0.1, (4.0, 3.0, 2.4), 4, 0.5
+    rng = np.random.default_rng(3)
+    rate = 343.0 / (L.COURANT * cell)
+    room = L.convex_room(rng, box, faces=14, margin=cell * (layer + 3), open_face=1,
+                         material=lambda r: L.Material(float(r.uniform(0.02, 0.1))))  # fmt: skip
+    points = L.inside_points(rng, room, box, 5, 0.35, apart=0.35)
+    grid = L.Grid(-L.OFFSET * cell, cell, tuple(int(round(b / cell)) for b in box))
+    signal = L.gaussian_drive(rate, 150)
+
+    def built(value):
+        return L.cell_face_layout(room, grid, points[0], points[1:], layer=layer, layer_damping=value).layout
+
+    lay = built(damping)
+    y, target = _misfit(lay, signal)
+    grad = adjoint_reference.gradient(lay, signal, 2.0 * (y - target))
+    courant = float(np.sqrt(np.float64(np.asarray(lay["weights"], np.float32)[0])))
+    predicted = 0.0
+    for a, axis in enumerate("xyz"):
+        t = L.layer_tables_tangent(int(grid.shape[a]), layer, damping, courant)
+        for table, kind in ((f"keep_{axis}", "keep"), (f"push_{axis}", "push"), (f"keep_face_{axis}", "keep_face"),
+                            (f"push_face_{axis}", "push_face")):  # fmt: skip
+            predicted += float(np.sum(grad[table] * t[kind]))
+    h = 0.01 * damping
+    loss = lambda value: float(np.sum((OracleSolver(built(value), "fp64").run(signal) - target) ** 2))  # noqa: E731
+    measured = (loss(damping + h) - loss(damping - h)) / (2.0 * h)
+    assert abs(measured) > 0.0
+    assert abs(predicted - measured) <= 2e-3 * abs(measured), (predicted, measured)
