@@ -172,3 +172,51 @@ def test_the_layer_damping_gradient_by_the_chain_rule():
     measured = (loss(damping + h) - loss(damping - h)) / (2.0 * h)
     assert abs(measured) > 0.0
     assert abs(predicted - measured) <= 2e-3 * abs(measured), (predicted, measured)
+
+
+def test_the_layer_reverse_step_formulas():
+    # The reverse step of one matched-layer update, as the GPU adjoint of the layer is to form it
+    # (per axis: Q += P; H~ = H - p Q, L~ = L + p Q; the old q takes k Q, the old faces kf H~ and
+    # kf L~; the pressures b_(i+s), b_(i-s), b_i take -pf H~, pf L~, pf H~ - pf L~; the tables
+    # dk += Q q, dp -= Q (hi' - lo'), dkf += H~ hi, dpf -= H~ (b_(i+s) - b_i), and the same for the
+    # - face), against autograd's vector-Jacobian product through the forward update.
+    import torch
+
+    rng = np.random.default_rng(4)
+    n = 50  # cells along each axis of one line, the layer's cells at 1 .. n-2
+    cells = np.arange(1, n - 1)
+    tabs = {k: torch.tensor(rng.uniform(0.2, 1.0, n + 1), dtype=torch.float64, requires_grad=True)
+            for k in ("k", "p", "kf", "pf")}  # fmt: skip
+    b = torch.tensor(rng.standard_normal(n), dtype=torch.float64, requires_grad=True)
+    lo, hi, q = (torch.tensor(rng.standard_normal(len(cells)), dtype=torch.float64, requires_grad=True) for _ in range(3))
+    x = torch.as_tensor(cells)
+    lo1 = tabs["kf"][x] * lo - tabs["pf"][x] * (b[x] - b[x - 1])
+    hi1 = tabs["kf"][x + 1] * hi - tabs["pf"][x + 1] * (b[x + 1] - b[x])
+    q1 = tabs["k"][x] * q - tabs["p"][x] * (hi1 - lo1)
+    P, L, H, Q = (rng.standard_normal(len(cells)) for _ in range(4))  # adjoints of p', lo', hi', q'
+    (q1 * torch.as_tensor(P + Q) + lo1 * torch.as_tensor(L) + hi1 * torch.as_tensor(H)).sum().backward()
+    # the formulas, in numpy
+    k, p, kf, pf = (tabs[name].detach().numpy() for name in ("k", "p", "kf", "pf"))
+    bn, lon, hin, qn = (v.detach().numpy() for v in (b, lo, hi, q))
+    lo1n, hi1n = lo1.detach().numpy(), hi1.detach().numpy()
+    Qt = Q + P
+    Ht = H - p[cells] * Qt
+    Lt = L + p[cells] * Qt
+    gb = np.zeros(n)
+    np.add.at(gb, cells + 1, -pf[cells + 1] * Ht)
+    np.add.at(gb, cells - 1, pf[cells] * Lt)
+    np.add.at(gb, cells, pf[cells + 1] * Ht - pf[cells] * Lt)
+    gk, gp, gkf, gpf = (np.zeros(n + 1) for _ in range(4))
+    np.add.at(gk, cells, Qt * qn)
+    np.add.at(gp, cells, -Qt * (hi1n - lo1n))
+    np.add.at(gkf, cells + 1, Ht * hin)
+    np.add.at(gpf, cells + 1, -Ht * (bn[cells + 1] - bn[cells]))
+    np.add.at(gkf, cells, Lt * lon)
+    np.add.at(gpf, cells, -Lt * (bn[cells] - bn[cells - 1]))
+    close = lambda a, b_: np.testing.assert_allclose(a, b_, rtol=1e-12, atol=1e-12)  # noqa: E731
+    close(q.grad.numpy(), k[cells] * Qt)
+    close(hi.grad.numpy(), kf[cells + 1] * Ht)
+    close(lo.grad.numpy(), kf[cells] * Lt)
+    close(b.grad.numpy(), gb)
+    for name, g in (("k", gk), ("p", gp), ("kf", gkf), ("pf", gpf)):
+        close(tabs[name].grad.numpy(), g)
