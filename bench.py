@@ -18,8 +18,11 @@ public API (``B200WaveSolver.run`` on a host drive, its probe series back on the
 ``roofline`` relates the step kernel's algorithmic bytes per launch to the measured HBM peak;
 ``cpu_baseline`` is the reference's own CPU solver (oracle/_ref, the reference's unmodified C++)
 timed on the host's cores on a bounded sample of the same workload. Under torchrun each rank steps
-its own replica of the room (a single grid does not shard without a halo exchange: replicas only).
-``--impl reference`` times the reference's CPU solver alone and prints its line.
+its own replica of the room (weak scaling); ``--slabs`` splits the one grid into z-slabs across the
+ranks instead, one plane swapped with each neighbour per step (strong scaling), and the batched
+rooms shard their solves by cell count. ``--impl reference`` times the reference's CPU solver alone
+and prints its line. ``--workload`` picks the other configurations (the plain FP64 box, the outdoor
+half-space, the batched rooms, the adjoint fit).
 """
 
 from __future__ import annotations
@@ -264,9 +267,18 @@ def outdoor_insertion_loss(args, workload, local: int) -> dict:
     }
 
 
+def oracle_cores(layout) -> int:
+    """The host threads the oracle's C port steps a grid of this layout on."""
+    from oracle import oracle
+
+    cells = int(np.prod(np.asarray(layout["shape"], np.int64)))
+    return int(oracle.load_oracle().oracle_threads()) if cells >= oracle.PARALLEL_CELLS else 1
+
+
 def cpu_reference_rate(workload, sample_steps: int) -> dict:
     """The reference's own CPU solver (its unmodified C++, oracle/_ref) on the same room, timed
-    over ``sample_steps`` steps with every host thread; else the oracle's C port, one thread."""
+    over ``sample_steps`` steps with every host thread; else the oracle's C port, on every host
+    thread too where the grid is large."""
     from acoustic_spaces_b200 import layouts
     from oracle import oracle
 
@@ -306,7 +318,7 @@ def cpu_reference_rate(workload, sample_steps: int) -> dict:
         t0 = time.perf_counter()
         ported.run(signal)
         seconds = time.perf_counter() - t0
-        kind, cores, extra = "port", 1, {}
+        kind, cores, extra = "port", oracle_cores(workload.built.layout), {}
     value = air * len(signal) / seconds / 1e9
     return {
         "value": round(value, 4),
@@ -583,7 +595,8 @@ def run_shoebox(args, world: int, rank: int, local: int) -> None:
         "e2e": {"value": round(air * steps / e2e_s / 1e9, 4), "unit": UNIT, "h2d_bytes_per_step": 4,
                 "d2h_bytes_per_step": 8 * solver.probes},  # fmt: skip
         "bit_exact_vs_fp64_oracle": bool(np.array_equal(ours, theirs)),
-        "cpu_baseline": {"value": round(air * steps / port_s / 1e9, 4), "unit": UNIT, "cores": 1, "kind": "port",
+        "cpu_baseline": {"value": round(air * steps / port_s / 1e9, 4), "unit": UNIT,
+                         "cores": oracle_cores(w.built.layout), "kind": "port",
                          "precision": "FP64", "sample": f"all {steps} steps"},  # fmt: skip
         "reference_cpu": reference,
         "clocks": clocks.summary(),

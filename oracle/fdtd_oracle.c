@@ -3,17 +3,74 @@
  * written for reading, of WaveSolver::run (cpp/include/acoustic_spaces/fdtd.hpp:786-904 of
  * naelolaiz/acoustic-spaces). Built with -ffp-contract=off so that no multiply-add is fused.
  */
+#define _POSIX_C_SOURCE 200809L
 #include "fdtd_oracle.h"
 #include "../acoustic_spaces_b200/csrc/fdtd_compensated.h"
 
+#include <pthread.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <unistd.h>
 
 #if defined(__SSE__) || defined(__x86_64__)
 #include <xmmintrin.h>
 #define ORACLE_HAS_MXCSR 1
 #endif
+
+/*
+ * Threads. Within a step every write is to the next level (or a cell's own branch and layer
+ * state) and every read of a neighbour is of the current level, so the cells, rows and layer
+ * cells split across threads in contiguous ranges with one barrier per step, and no result
+ * changes. Grids of ORACLE_PARALLEL_CELLS cells or more use oracle_threads() threads.
+ */
+#define ORACLE_PARALLEL_CELLS (1u << 16)
+
+int oracle_threads(void) {
+    const char *env = getenv("ORACLE_THREADS");
+    long t = env ? atol(env) : sysconf(_SC_NPROCESSORS_ONLN);
+    return (int)(t < 1 ? 1 : (t > 64 ? 64 : t));
+}
+
+typedef struct oracle_job {
+    oracle_solver *s;
+    const float *signal;
+    uint64_t steps;
+    double *out;
+    int tid, threads;
+    pthread_barrier_t *barrier;
+} oracle_job;
+
+/* This thread's share [*lo, *hi) of count items. */
+static void share(const oracle_job *j, uint64_t count, uint64_t *lo, uint64_t *hi) {
+    *lo = count * (uint64_t)j->tid / (uint64_t)j->threads;
+    *hi = count * (uint64_t)(j->tid + 1) / (uint64_t)j->threads;
+}
+
+static void step_barrier(const oracle_job *j) {
+    if (j->threads > 1) pthread_barrier_wait(j->barrier);
+}
+
+/* The reference's flush of subnormal single-precision results (fdtd.hpp:316-336) is a per-thread
+   flag: every thread that steps float sets it for itself. */
+static unsigned flush_enter(int flush) {
+#ifdef ORACLE_HAS_MXCSR
+    const unsigned saved = _mm_getcsr();
+    if (flush) _mm_setcsr(saved | 0x8040u);
+    return saved;
+#else
+    (void)flush;
+    return 0;
+#endif
+}
+
+static void flush_leave(int flush, unsigned saved) {
+#ifdef ORACLE_HAS_MXCSR
+    if (flush) _mm_setcsr(saved);
+#else
+    (void)flush, (void)saved;
+#endif
+}
 
 static char g_error[512];
 
@@ -59,7 +116,7 @@ struct oracle_solver {
     float residual, *row_residual;
 };
 
-static void *dup(const void *src, size_t bytes) {
+static void *copy_of(const void *src, size_t bytes) {
     void *p = malloc(bytes ? bytes : 1);
     if (p && src && bytes) memcpy(p, src, bytes);
     return p;
@@ -84,19 +141,19 @@ int oracle_create(const fdtd_layout *L, int precision, oracle_solver **out) {
     s->scaled = L->scaled != 0;
     s->specials = L->special_count, s->links = L->link_count, s->states = L->state_count;
     s->branches = L->branch_count, s->layers = L->layer_count, s->probes = L->probe_count;
-    s->types = dup(L->types, s->n);
-    s->scale = s->scaled ? dup(L->scale, 4 * s->n) : NULL;
-    s->layer_scale = s->scaled ? dup(L->layer_scale, 4 * s->layers) : NULL;
-    s->special = dup(L->special, 8 * s->specials);
-    s->link_start = dup(L->link_start, 8 * (s->specials + 1));
-    s->state_start = dup(L->state_start, 8 * (s->specials + 1));
-    s->link_direction = dup(L->link_direction, s->links);
-    s->link_weight = dup(L->link_weight, 4 * s->links);
-    s->coef_a = dup(L->coef_a, 4 * s->specials);
-    s->coef_b = dup(L->coef_b, 4 * s->specials);
-    s->coef_inv = dup(L->coef_inv, 4 * s->specials);
-    s->source = dup(L->source, 4 * s->specials);
-    s->state_weight = dup(L->state_weight, 4 * s->states);
+    s->types = copy_of(L->types, s->n);
+    s->scale = s->scaled ? copy_of(L->scale, 4 * s->n) : NULL;
+    s->layer_scale = s->scaled ? copy_of(L->layer_scale, 4 * s->layers) : NULL;
+    s->special = copy_of(L->special, 8 * s->specials);
+    s->link_start = copy_of(L->link_start, 8 * (s->specials + 1));
+    s->state_start = copy_of(L->state_start, 8 * (s->specials + 1));
+    s->link_direction = copy_of(L->link_direction, s->links);
+    s->link_weight = copy_of(L->link_weight, 4 * s->links);
+    s->coef_a = copy_of(L->coef_a, 4 * s->specials);
+    s->coef_b = copy_of(L->coef_b, 4 * s->specials);
+    s->coef_inv = copy_of(L->coef_inv, 4 * s->specials);
+    s->source = copy_of(L->source, 4 * s->specials);
+    s->state_weight = copy_of(L->state_weight, 4 * s->states);
     s->state_now = malloc(4 * s->states + 4);
     s->state_before = malloc(4 * s->states + 4);
     s->state_gain = malloc(4 * s->states + 4);
@@ -107,17 +164,17 @@ int oracle_create(const fdtd_layout *L, int precision, oracle_solver **out) {
         s->state_before[j] = L->branch_before[b];
         s->state_gain[j] = L->branch_gain[b];
     }
-    s->layer_cells = dup(L->layer_cells, 8 * s->layers);
+    s->layer_cells = copy_of(L->layer_cells, 8 * s->layers);
     s->axis_len[0] = s->nx, s->axis_len[1] = s->ny, s->axis_len[2] = s->nz;
     for (int k = 0; k < 6; ++k) {
         const uint64_t len = s->axis_len[k / 2] + 1;
-        s->keep[k] = s->layers ? dup(L->keep[k], 4 * len) : NULL;
-        s->push[k] = s->layers ? dup(L->push[k], 4 * len) : NULL;
+        s->keep[k] = s->layers ? copy_of(L->keep[k], 4 * len) : NULL;
+        s->push[k] = s->layers ? copy_of(L->push[k], 4 * len) : NULL;
     }
-    s->probe_start = dup(L->probe_start, 8 * (s->probes + 1));
+    s->probe_start = copy_of(L->probe_start, 8 * (s->probes + 1));
     const uint64_t pc = s->probe_start[s->probes];
-    s->probe_cells = dup(L->probe_cells, 8 * pc);
-    s->probe_weights = dup(L->probe_weights, 8 * pc);
+    s->probe_cells = copy_of(L->probe_cells, 8 * pc);
+    s->probe_weights = copy_of(L->probe_weights, 8 * pc);
     for (int k = 0; k < 18; ++k)
         s->offset[k] = kSteps[k][0] + kSteps[k][1] * (int64_t)s->sy + kSteps[k][2] * (int64_t)s->sz;
     const size_t e = precision == ORACLE_FP64 ? 8 : 4;
@@ -141,23 +198,34 @@ int oracle_create(const fdtd_layout *L, int precision, oracle_solver **out) {
  * One instantiation per arithmetic type T. Each expression keeps the reference's operands in the
  * reference's order; with T float every operation rounds to float as the reference's does.
  */
-#define DEFINE_STEPPER(T, NAME)                                                                   \
-    static void NAME(oracle_solver *s, const float *signal, uint64_t steps, double *out) {       \
-        T *a = (T *)s->u0, *b = (T *)s->u1, *wa = (T *)s->w0, *wb = (T *)s->w1;                  \
+#define DEFINE_STEPPER(T, NAME, FLUSH)                                                            \
+    static void NAME(const oracle_job *job) {                                                    \
+        oracle_solver *s = job->s;                                                               \
+        const float *signal = job->signal;                                                       \
+        const uint64_t steps = job->steps;                                                       \
+        double *out = job->out;                                                                  \
         T *term = (T *)s->term, *lstate = (T *)s->layer_state;                                   \
-        const uint64_t sy = s->sy, sz = s->sz, n = s->n;                                         \
+        const uint64_t sy = s->sy, sz = s->sz;                                                   \
         const T axial = (T)s->axial, diagonal = (T)s->diagonal, centre = (T)s->centre;           \
         const T total = (T)s->total;                                                             \
+        uint64_t i0, i1, k0, k1, c0, c1;                                                         \
+        share(job, s->n, &i0, &i1);                                                              \
+        share(job, s->specials, &k0, &k1);                                                       \
+        share(job, s->layers, &c0, &c1);                                                         \
+        const unsigned csr = flush_enter(FLUSH);                                                 \
         for (uint64_t step = 0; step < steps; ++step) {                                          \
+            /* the levels' roles by the step's parity (the swap of fdtd.hpp:884-885) */          \
+            T *a = (T *)(step & 1 ? s->u1 : s->u0), *b = (T *)(step & 1 ? s->u0 : s->u1);        \
+            T *wa = (T *)(step & 1 ? s->w1 : s->w0), *wb = (T *)(step & 1 ? s->w0 : s->w1);      \
             /* record (fdtd.hpp:3525-3533) */                                                    \
-            for (uint64_t p = 0; p < s->probes; ++p) {                                           \
+            for (uint64_t p = 0; job->tid == 0 && p < s->probes; ++p) {                          \
                 double value = 0.0;                                                              \
                 for (uint64_t k = s->probe_start[p]; k < s->probe_start[p + 1]; ++k)             \
                     value += s->probe_weights[k] * (double)b[s->probe_cells[k]];                 \
                 out[p * steps + step] = value;                                                   \
             }                                                                                    \
             /* interior (fdtd.hpp:242-288) */                                                    \
-            for (uint64_t i = 0; i < n; ++i) {                                                   \
+            for (uint64_t i = i0; i < i1; ++i) {                                                 \
                 if (s->types[i] != 1) continue;                                                  \
                 const T sum = b[i - 1] + b[i + 1] + b[i - sy] + b[i + sy] + b[i - sz] + b[i + sz]; \
                 T edges = 0;                                                                     \
@@ -180,7 +248,7 @@ int oracle_create(const fdtd_layout *L, int precision, oracle_solver **out) {
             }                                                                                    \
             /* special cells (fdtd.hpp:860-881) */                                               \
             const T sig = (T)signal[step];                                                       \
-            for (uint64_t k = 0; k < s->specials; ++k) {                                         \
+            for (uint64_t k = k0; k < k1; ++k) {                                                 \
                 const uint64_t i = (uint64_t)s->special[k];                                      \
                 T sum = 0;                                                                       \
                 for (uint64_t l = s->link_start[k]; l < s->link_start[k + 1]; ++l)               \
@@ -199,7 +267,7 @@ int oracle_create(const fdtd_layout *L, int precision, oracle_solver **out) {
                     wa[j] += (next - previous) * (T)s->state_gain[j] + term[j];                  \
             }                                                                                    \
             /* matched layer (fdtd.hpp:2242-2264) */                                             \
-            for (uint64_t c = 0; c < s->layers; ++c) {                                           \
+            for (uint64_t c = c0; c < c1; ++c) {                                                 \
                 const uint64_t i = (uint64_t)s->layer_cells[c];                                  \
                 const uint64_t at[3] = {i % s->nx, (i / s->nx) % s->ny, i / sz};                 \
                 T *st = lstate + 9 * c;                                                          \
@@ -222,13 +290,13 @@ int oracle_create(const fdtd_layout *L, int precision, oracle_solver **out) {
                 }                                                                                \
                 a[i] = tot;                                                                      \
             }                                                                                    \
-            T *t = a; a = b; b = t;                                                              \
-            t = wa; wa = wb; wb = t;                                                             \
+            step_barrier(job);                                                                   \
         }                                                                                        \
+        flush_leave(FLUSH, csr);                                                                 \
     }
 
-DEFINE_STEPPER(float, step_fp32)
-DEFINE_STEPPER(double, step_fp64)
+DEFINE_STEPPER(float, step_fp32, 1)
+DEFINE_STEPPER(double, step_fp64, 0)
 
 /*
  * ORACLE_FP32C: the same scheme in exact arithmetic, stepped in float on the pressure p_n and its
@@ -240,19 +308,29 @@ DEFINE_STEPPER(double, step_fp64)
  * itself rather than to the pressure, so that rounding no longer drives the slow modes of a long
  * run. The operation order here is the GPU's compensated kernels' (fdtd_kernels.cuh).
  */
-static void step_fp32c(oracle_solver *s, const float *signal, uint64_t steps, double *out) {
-    float *a = (float *)s->u0, *b = (float *)s->u1, *wa = (float *)s->w0, *wb = (float *)s->w1;
+static void step_fp32c(const oracle_job *job) {
+    oracle_solver *s = job->s;
+    const float *signal = job->signal;
+    const uint64_t steps = job->steps;
+    double *out = job->out;
     float *term = (float *)s->term, *lstate = (float *)s->layer_state, *d = s->increment;
-    const uint64_t sy = s->sy, sz = s->sz, n = s->n;
+    const uint64_t sy = s->sy, sz = s->sz;
     const float axial = s->axial, diagonal = s->diagonal, residual = s->residual;
+    uint64_t i0, i1, k0, k1, c0, c1;
+    share(job, s->n, &i0, &i1);
+    share(job, s->specials, &k0, &k1);
+    share(job, s->layers, &c0, &c1);
+    const unsigned csr = flush_enter(1);
     for (uint64_t step = 0; step < steps; ++step) {
-        for (uint64_t p = 0; p < s->probes; ++p) {
+        float *a = (float *)(step & 1 ? s->u1 : s->u0), *b = (float *)(step & 1 ? s->u0 : s->u1);
+        float *wa = (float *)(step & 1 ? s->w1 : s->w0), *wb = (float *)(step & 1 ? s->w0 : s->w1);
+        for (uint64_t p = 0; job->tid == 0 && p < s->probes; ++p) {
             double value = 0.0;
             for (uint64_t k = s->probe_start[p]; k < s->probe_start[p + 1]; ++k)
                 value += s->probe_weights[k] * (double)b[s->probe_cells[k]];
             out[p * steps + step] = value;
         }
-        for (uint64_t i = 0; i < n; ++i) {
+        for (uint64_t i = i0; i < i1; ++i) {
             if (s->types[i] != 1) continue;
             const float here = b[i];
             const float sum = (b[i - 1] - here) + (b[i + 1] - here) + (b[i - sy] - here) + (b[i + sy] - here) +
@@ -276,7 +354,7 @@ static void step_fp32c(oracle_solver *s, const float *signal, uint64_t steps, do
             d[i] = next;
         }
         const float sig = signal[step];
-        for (uint64_t k = 0; k < s->specials; ++k) {
+        for (uint64_t k = k0; k < k1; ++k) {
             const uint64_t i = (uint64_t)s->special[k];
             const float here = b[i];
             float sum = 0.0f;
@@ -300,7 +378,7 @@ static void step_fp32c(oracle_solver *s, const float *signal, uint64_t steps, do
            pressure carried on from its own, p + sum over axes of (keep - 1) * part - push * (above -
            below), the parts' sum in exact arithmetic: a part along an undamped axis (keep 1) then
            drops out, and with it the rounding of parts that grow far beyond the pressure. */
-        for (uint64_t c = 0; c < s->layers; ++c) {
+        for (uint64_t c = c0; c < c1; ++c) {
             const uint64_t i = (uint64_t)s->layer_cells[c];
             const uint64_t at[3] = {i % s->nx, (i / s->nx) % s->ny, i / sz};
             float *st = lstate + 9 * c;
@@ -323,27 +401,65 @@ static void step_fp32c(oracle_solver *s, const float *signal, uint64_t steps, do
             a[i] = here + change;
             d[i] = change;
         }
-        float *t = a; a = b; b = t;
-        t = wa; wa = wb; wb = t;
+        step_barrier(job);
     }
+    flush_leave(1, csr);
+}
+
+static void step_job(const oracle_job *job) {
+    if (job->s->precision == ORACLE_FP32C)
+        step_fp32c(job);
+    else if (job->s->precision == ORACLE_FP32)
+        step_fp32(job);
+    else
+        step_fp64(job);
+}
+
+/* Workers start when every one of them exists (go), or return at once (abort). */
+typedef struct start_gate {
+    pthread_mutex_t mutex;
+    pthread_cond_t cond;
+    int state; /* 0 waiting, 1 go, -1 abort */
+} start_gate;
+
+typedef struct worker {
+    oracle_job job;
+    start_gate *gate;
+} worker;
+
+static void *run_worker(void *arg) {
+    worker *w = (worker *)arg;
+    pthread_mutex_lock(&w->gate->mutex);
+    while (w->gate->state == 0) pthread_cond_wait(&w->gate->cond, &w->gate->mutex);
+    const int state = w->gate->state;
+    pthread_mutex_unlock(&w->gate->mutex);
+    if (state > 0) step_job(&w->job);
+    return NULL;
 }
 
 int oracle_run(oracle_solver *s, const float *signal, uint64_t steps, double *out) {
-    if (s->precision != ORACLE_FP64) {
-#ifdef ORACLE_HAS_MXCSR
-        const unsigned saved = _mm_getcsr();
-        _mm_setcsr(saved | 0x8040u); /* flush to zero, denormals are zero (fdtd.hpp:316-336) */
-#endif
-        if (s->precision == ORACLE_FP32C)
-            step_fp32c(s, signal, steps, out);
-        else
-            step_fp32(s, signal, steps, out);
-#ifdef ORACLE_HAS_MXCSR
-        _mm_setcsr(saved);
-#endif
-    } else {
-        step_fp64(s, signal, steps, out);
+    int threads = s->n >= ORACLE_PARALLEL_CELLS ? oracle_threads() : 1;
+    worker workers[64];
+    pthread_t ids[64];
+    pthread_barrier_t barrier;
+    start_gate gate = {PTHREAD_MUTEX_INITIALIZER, PTHREAD_COND_INITIALIZER, 0};
+    int started = 1;
+    for (; started < threads; ++started) {
+        workers[started].job = (oracle_job){s, signal, steps, out, started, threads, &barrier};
+        workers[started].gate = &gate;
+        if (pthread_create(&ids[started], NULL, run_worker, &workers[started]) != 0) break;
     }
+    int go = started == threads && (threads == 1 || pthread_barrier_init(&barrier, NULL, (unsigned)threads) == 0);
+    pthread_mutex_lock(&gate.mutex);
+    gate.state = go ? 1 : -1;
+    pthread_cond_broadcast(&gate.cond);
+    pthread_mutex_unlock(&gate.mutex);
+    /* (without all of them, the workers return and this thread steps alone) */
+    const oracle_job mine = go ? (oracle_job){s, signal, steps, out, 0, threads, &barrier}
+                               : (oracle_job){s, signal, steps, out, 0, 1, NULL};
+    step_job(&mine);
+    for (int t = 1; t < started; ++t) pthread_join(ids[t], NULL);
+    if (go && threads > 1) pthread_barrier_destroy(&barrier);
     /* the parity swap (fdtd.hpp:900-903): u1 stays the current level between runs */
     if (steps % 2 == 1) {
         void *t = s->u0; s->u0 = s->u1; s->u1 = t;

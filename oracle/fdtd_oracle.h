@@ -43,6 +43,8 @@ void oracle_destroy(oracle_solver *solver);
 int oracle_read_state(const oracle_solver *solver, void *current, void *previous,
                       void *branch_current, void *branch_previous, void *layer_state);
 const char *oracle_error(void);
+/* The host threads a run of a large grid steps on (the host's cores, or ORACLE_THREADS). */
+int oracle_threads(void);
 /* The current (which 0) or previous (1) pressure level between runs, nx*ny*nz elements: the
    slab tests read and write its planes. */
 void *oracle_level(oracle_solver *solver, int which);

@@ -39,6 +39,8 @@ ORACLE_SO = HERE / "libfdtd_oracle.so"
 ORACLE_FP32 = 0
 ORACLE_FP64 = 1
 ORACLE_FP32C = 2
+#: Grids of this many cells or more step on oracle_threads() host threads (ORACLE_PARALLEL_CELLS).
+PARALLEL_CELLS = 1 << 16
 PRECISIONS = {"fp32": ORACLE_FP32, "fp64": ORACLE_FP64, "fp32c": ORACLE_FP32C}
 
 
@@ -70,6 +72,8 @@ def load_oracle() -> ctypes.CDLL:
         lib.oracle_reset.argtypes = [ctypes.c_void_p]
         lib.oracle_destroy.restype = None
         lib.oracle_destroy.argtypes = [ctypes.c_void_p]
+        lib.oracle_threads.restype = ctypes.c_int
+        lib.oracle_threads.argtypes = []
         lib.oracle_level.restype = ctypes.c_void_p
         lib.oracle_level.argtypes = [ctypes.c_void_p, ctypes.c_int]
         lib.oracle_read_state.restype = ctypes.c_int

@@ -103,3 +103,21 @@ def test_oracle_matches_the_reference_live_on_new_drives(name):
     oracle = OracleSolver(layout)
     reference = np.concatenate([solver.run(signal[:101]), solver.run(signal[101:])], axis=1)
     assert np.array_equal(oracle.run(signal), reference)
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64", "fp32c"])
+def test_the_oracle_steps_alike_on_one_thread_and_on_many(precision, monkeypatch):
+    # Large grids split their cells, rows and layer cells across host threads with one barrier a
+    # step: the probes and the whole state equal a single thread's, bit for bit.
+    from acoustic_spaces_b200 import layouts as L
+
+    w = L.polyhedral_room(0, cell=0.2, steps=150)
+    runs = {}
+    for threads in ("1", "5"):
+        monkeypatch.setenv("ORACLE_THREADS", threads)
+        solver = OracleSolver(w.built.layout, precision)
+        runs[threads] = (solver.run(w.signal[:77]), solver.run(w.signal[77:]), solver.state())
+    one, many = runs["1"], runs["5"]
+    assert np.array_equal(one[0], many[0]) and np.array_equal(one[1], many[1])
+    for key in one[2]:
+        assert np.array_equal(one[2][key], many[2][key]), key
