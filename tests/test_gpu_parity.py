@@ -225,3 +225,27 @@ def test_gpu_an_expired_wait_is_a_status_and_the_handle_stays_usable():
     with pytest.raises(RuntimeError, match="bounded wait gave up"):
         gpu.test_wait(1 << 12)
     assert np.array_equal(gpu.run(signal), reference)
+
+
+def test_gpu_an_empty_run_changes_nothing():
+    # A drive of no steps records nothing and leaves the state as it was: the run that follows is
+    # the reference's run from rest.
+    layout, signal, reference = load_golden("resonant7")
+    gpu = B200WaveSolver(layout)
+    assert gpu.run(signal[:0]).shape == (gpu.probes, 0)
+    assert np.array_equal(gpu.run(signal), reference)
+
+
+def test_gpu_steps_a_layout_without_probes_as_the_oracle_does():
+    # No probes at all: nothing is recorded, and the whole state equals the oracle's.
+    layout, signal, _ = load_golden("open_layer")
+    layout = dict(layout)
+    layout.update(probe_start=np.zeros(1, np.uint64), probe_cells=np.zeros(0, np.uint64),
+                  probe_weights=np.zeros(0, np.float64))  # fmt: skip
+    gpu, oracle = B200WaveSolver(layout), OracleSolver(layout)
+    assert gpu.probes == 0
+    assert gpu.run(signal).shape == (0, len(signal))
+    oracle.run(signal)
+    sa, sb = gpu.state(), oracle.state()
+    for key in sa:
+        assert np.array_equal(sa[key], sb[key]), key
