@@ -275,7 +275,7 @@ def oracle_cores(layout) -> int:
     return int(oracle.load_oracle().oracle_threads()) if cells >= oracle.PARALLEL_CELLS else 1
 
 
-def cpu_reference_rate(workload, sample_steps: int) -> dict:
+def cpu_reference_rate(workload, sample_steps: int, warmup: int = 3) -> dict:
     """The reference's own CPU solver (its unmodified C++, oracle/_ref) on the same room, timed
     over ``sample_steps`` steps with every host thread; else the oracle's C port, on every host
     thread too where the grid is large."""
@@ -304,7 +304,8 @@ def cpu_reference_rate(workload, sample_steps: int) -> dict:
             workload.receivers, layer=8, layer_damping=0.5, threads=threads,
         )  # fmt: skip
         setup = time.perf_counter() - t0
-        solver.run(signal[:2])  # threads spun up once
+        solver.run(workload.signal[:warmup])  # its threads spun up, untimed
+        solver.reset()
         t0 = time.perf_counter()
         solver.run(signal)
         seconds = time.perf_counter() - t0
@@ -314,7 +315,8 @@ def cpu_reference_rate(workload, sample_steps: int) -> dict:
         extra = {"setup_s": round(setup, 2)}
     else:
         ported = oracle.OracleSolver(workload.built.layout)
-        ported.run(signal[:2])
+        ported.run(workload.signal[:warmup])
+        ported.reset()
         t0 = time.perf_counter()
         ported.run(signal)
         seconds = time.perf_counter() - t0
@@ -326,7 +328,7 @@ def cpu_reference_rate(workload, sample_steps: int) -> dict:
         "cores": cores,
         "kind": kind,
         "sample": f"{len(signal)} steps of the full {workload.description['grid']} grid "
-        f"({air} air cells), after 2 warm-up steps",
+        f"({air} air cells), after {warmup} warm-up steps",
         **extra,
     }
 
@@ -336,10 +338,11 @@ def run_reference(args, rank: int, world: int) -> None:
         return
     workload = build_workload(args)
     steps = max(1, min(args.steps, args.reference_steps))
+    warmup = max(3, args.warmup)
     times = []
     base = None
     for _ in range(max(1, args.reference_repeats)):
-        base = cpu_reference_rate(workload, steps)
+        base = cpu_reference_rate(workload, steps, warmup)
         times.append(base["value"])
     value = statistics.median(times)
     base["value"] = round(value, 4)
@@ -350,7 +353,7 @@ def run_reference(args, rank: int, world: int) -> None:
         "unit": UNIT,
         "n_gpus": world,
         "steps": steps,
-        "warmup": 2,
+        "warmup": warmup,
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,

@@ -45,3 +45,28 @@ def test_kind_bytes_count_the_compensated_increment():
     assert plain["bulk"] == 120 and comp["bulk"] == 160
     assert comp["layer"] - plain["layer"] == 16 and comp["special"] - plain["special"] == 8
     assert bench.algorithmic_bytes(d) == sum(plain.values())
+
+
+def test_the_reference_arm_prints_the_contracts_line():
+    # bench.py --impl reference: the reference's own CPU solver on the benchmark's room (here at
+    # 20 cm cells), one JSON line with the metric, a cpu_baseline describing the run and a zero-copy
+    # e2e, after at least 3 warm-up steps.
+    import json
+    import subprocess
+    import sys
+
+    from conftest import ROOT
+    from oracle.oracle import reference_native
+
+    if reference_native() is None:
+        import pytest
+
+        pytest.skip("the reference's solver is not built")
+    out = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--cell", "0.2", "--steps", "2",
+                          "--warmup", "3"], capture_output=True, text=True, timeout=600, check=True).stdout  # fmt: skip
+    line = json.loads(out.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["unit"] == bench.UNIT and line["metric"] == bench.METRIC
+    assert line["value"] > 0 and line["warmup"] >= 3 and line["higher_is_better"] is True
+    cpu = line["cpu_baseline"]
+    assert cpu["kind"] == "reference" and cpu["cores"] >= 1 and cpu["value"] == line["value"] and cpu["sample"]
+    assert line["e2e"] == {"value": line["value"], "unit": line["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
