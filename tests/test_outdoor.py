@@ -59,6 +59,57 @@ def test_the_layer_has_no_floor_and_the_ground_runs_into_it():
     assert kz[nz - 2] < kz[nz // 2]
 
 
+def test_the_reference_lays_the_outdoor_pieces_out_alike_where_they_stop_short_of_the_layer():
+    # The reference refuses the half-space itself (its ground runs into the matched layer), so its
+    # pieces are checked on a grid it accepts: a floating porous ground panel (Miki's admittance,
+    # three relaxation branches) and the rigid barrier, both short of a 4-cell layer on all six
+    # sides, air all round. Handed to the reference as four triangles, the same scene gives the
+    # same layout, array for array, and the reference's run equals the oracle's to the bit.
+    from oracle.oracle import reference_native
+
+    native = reference_native()
+    if native is None:
+        pytest.skip("the reference sources are not here")
+    cell, layer, shape = 0.1, 4, (80, 40, 40)
+    rate = 343.0 / (layouts.COURANT * cell)
+    grid = layouts.Grid(-layouts.OFFSET * cell, cell, shape)
+    ground_z = grid.origin[2] + 12.37 * cell
+    ground = layouts.porous_ground(200e3, rate)
+    lo = (grid.origin[0] + (layer + 4) * cell, grid.origin[1] + (layer + 4.21) * cell)
+    hi = (grid.origin[0] + (shape[0] - layer - 4) * cell, grid.origin[1] + (shape[1] - layer - 3.79) * cell)
+    barrier_x = grid.origin[0] + 40.37 * cell
+    room = layouts.Room(np.zeros((0, 3)), np.zeros(0), [])
+    room.screens.append(layouts.Screen(2, ground_z, lo, hi, ground))
+    room.screens.append(layouts.Screen(0, barrier_x, (lo[1], ground_z), (hi[1], ground_z + 1.0), layouts.Material(0.0)))
+    y = 0.5 * (lo[1] + hi[1])
+    source = np.array([barrier_x - 1.0, y, ground_z + 0.5])
+    probes = np.array([[barrier_x + 1.0, y, ground_z + 1.0], [barrier_x + 2.0, y + 0.3, ground_z + 1.2]])
+    built = layouts.cell_face_layout(room, grid, source, probes, layer=layer, layer_damping=0.5, rate=rate,
+                                     layer_meets_walls=False)  # fmt: skip
+    vertices, faces, owner = [], [], []
+    for k, screen in enumerate(room.screens):
+        others = [b for b in range(3) if b != screen.axis]
+        for u, v in ((screen.lo[0], screen.lo[1]), (screen.hi[0], screen.lo[1]), (screen.hi[0], screen.hi[1]),
+                     (screen.lo[0], screen.hi[1])):  # fmt: skip
+            p = np.zeros(3)
+            p[screen.axis], p[others[0]], p[others[1]] = screen.position, u, v
+            vertices.append(p)
+        faces += [[4 * k, 4 * k + 1, 4 * k + 2], [4 * k, 4 * k + 2, 4 * k + 3]]
+        owner += [k, k]
+    branches = np.ascontiguousarray(np.asarray(ground.branches, float).reshape(-1, 3))
+    solver = native.WaveSolver(
+        native.Bvh(np.array(vertices), np.array(faces, np.int64)), np.array(owner, np.int64),
+        np.array([ground.beta, 0.0]), branches, np.zeros(len(branches), np.int64), grid.origin, grid.cell, *grid.shape,
+        source, probes, layer=layer, layer_damping=0.5, threads=2,
+    )  # fmt: skip
+    ref = solver.layout()
+    assert len(built.layout["state_branch"]) > 0 and len(built.layout["layer_cells"]) > 0
+    for name, value in built.layout.items():
+        assert np.array_equal(np.asarray(value), np.asarray(ref[name])), name
+    signal = layouts.gaussian_drive(rate, 200)
+    assert np.array_equal(solver.run(signal), OracleSolver(built.layout).run(signal))
+
+
 def test_the_oracle_steps_it():
     w = layouts.outdoor_halfspace(0, **SMALL)
     y = OracleSolver(w.built.layout, "fp32").run(w.signal)
