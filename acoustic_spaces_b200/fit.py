@@ -21,7 +21,7 @@ from __future__ import annotations
 
 import math
 import time
-from dataclasses import dataclass
+from dataclasses import dataclass, field
 
 import numpy as np
 
@@ -283,6 +283,9 @@ class FitProblem:
     truth: Relaxation
     start: Relaxation
     description: dict
+    # the room as built (room, grid, source, receivers, and the patches' cuts and materials), for
+    # handing the same scene to the reference's own solver
+    scene: dict = field(default_factory=dict)
 
 
 def patched_room(seed: int = 0, *, size=(10.0, 8.0, 4.0), cell: float = 0.05, receivers: int = 4,
@@ -343,7 +346,9 @@ def patched_room(seed: int = 0, *, size=(10.0, 8.0, 4.0), cell: float = 0.05, re
         "checkpoint_every": segment,
         "seed": seed,
     }
-    return FitProblem(fit, truth, start, description)
+    scene = {"room": room, "grid": grid, "source": points[0], "receivers": points[1:], "x_cut": x_cut,
+             "y_cut": y_cut, "order": order, "split": split, "materials": mats}  # fmt: skip
+    return FitProblem(fit, truth, start, description, scene)
 
 
 def adam(problem: FitProblem, *, iterations: int = 300, rate: float = 0.05, final_rate: float | None = None,

@@ -7,8 +7,10 @@ from __future__ import annotations
 import math
 
 import numpy as np
+import pytest
 
 from acoustic_spaces_b200 import fit, layouts
+from oracle.oracle import OracleSolver
 
 
 def _small_problem():
@@ -68,3 +70,67 @@ def test_the_chain_rule_matches_finite_differences():
         down[i] -= h
         fd = (synthetic(fit.Relaxation.from_vector(truth.beta, up)) - synthetic(fit.Relaxation.from_vector(truth.beta, down))) / (2 * h)
         assert math.isclose(grad[i], fd, rel_tol=1e-6, abs_tol=1e-9 * abs(fd) + 1e-12), (i, grad[i], fd)
+
+
+def test_the_fit_room_is_laid_out_as_the_reference_lays_it(monkeypatch):
+    # The adjoint fit's room (a box, the floor and the ceiling each cut in two patches, 8 materials
+    # of one relaxation branch each) handed to the reference as triangles with a material each: the
+    # reference's own layout, array for array, and its run equal to the oracle's to the bit.
+    from oracle.oracle import reference_native
+
+    native = reference_native()
+    if native is None:
+        pytest.skip("the reference sources are not here")
+
+    class _Oracle:
+        def __init__(self, layout, precision="fp32"):
+            self._solver = OracleSolver(layout, precision)
+
+        def run(self, signal):
+            return self._solver.run(signal)
+
+        def close(self):
+            pass
+
+    monkeypatch.setattr(fit, "B200WaveSolver", _Oracle)
+    X, Y, Z = 3.0, 2.4, 1.6
+    problem = fit.patched_room(1, size=(X, Y, Z), cell=0.1, steps=150)
+    sc = problem.scene
+    xc, yc, order = sc["x_cut"], sc["y_cut"], sc["order"]
+
+    def rect(normal, corners):  # corners ordered round their centroid, as layouts.room_mesh orders them
+        pts = np.array(corners, float)
+        c = pts.mean(0)
+        e1 = (pts[0] - c) / np.linalg.norm(pts[0] - c)
+        e2 = np.cross(normal, e1)
+        return pts[np.argsort(np.arctan2((pts - c) @ e2, (pts - c) @ e1))]
+
+    walls = [
+        (rect([-1, 0, 0], [[0, 0, 0], [0, Y, 0], [0, Y, Z], [0, 0, Z]]), order[4]),
+        (rect([1, 0, 0], [[X, 0, 0], [X, Y, 0], [X, Y, Z], [X, 0, Z]]), order[5]),
+        (rect([0, -1, 0], [[0, 0, 0], [X, 0, 0], [X, 0, Z], [0, 0, Z]]), order[6]),
+        (rect([0, 1, 0], [[0, Y, 0], [X, Y, 0], [X, Y, Z], [0, Y, Z]]), order[7]),
+        (rect([0, 0, -1], [[0, 0, 0], [xc, 0, 0], [xc, Y, 0], [0, Y, 0]]), order[0]),
+        (rect([0, 0, -1], [[xc, 0, 0], [X, 0, 0], [X, Y, 0], [xc, Y, 0]]), order[1]),
+        (rect([0, 0, 1], [[0, 0, Z], [X, 0, Z], [X, yc, Z], [0, yc, Z]]), order[2]),
+        (rect([0, 0, 1], [[0, yc, Z], [X, yc, Z], [X, Y, Z], [0, Y, Z]]), order[3]),
+    ]
+    vertices, triangles, owner = [], [], []
+    for pts, material in walls:
+        base = len(vertices)
+        vertices.extend(pts)
+        triangles += [(base, base + k, base + k + 1) for k in range(1, len(pts) - 1)]
+        owner += [int(material)] * (len(pts) - 2)
+    mats = sc["materials"]
+    rows = [np.asarray(m.branches, float).reshape(-1, 3) for m in mats]
+    grid = sc["grid"]
+    solver = native.WaveSolver(
+        native.Bvh(np.array(vertices), np.array(triangles, np.int64)), np.array(owner, np.int64),
+        np.array([m.beta for m in mats]), np.ascontiguousarray(np.vstack(rows)),
+        np.concatenate([np.full(len(r), k, np.int64) for k, r in enumerate(rows)]), grid.origin, grid.cell,
+        *grid.shape, sc["source"], sc["receivers"], layer=0, layer_damping=0.0, threads=2,
+    )  # fmt: skip
+    ref, lay = solver.layout(), problem.fit.built.layout
+    for name, value in lay.items():
+        assert np.array_equal(np.asarray(value), np.asarray(ref[name])), name
+    assert np.array_equal(solver.run(problem.fit.signal), OracleSolver(lay).run(problem.fit.signal))
