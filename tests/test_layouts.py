@@ -145,6 +145,7 @@ def test_the_batched_solves_are_laid_out_as_the_reference_lays_them():
         ref = solver.layout()
         for name, value in lay.items():
             assert np.array_equal(np.asarray(value), np.asarray(ref[name])), name
+        assert np.array_equal(solver.run(b.signal), OracleSolver(lay).run(b.signal))
 
 
 def test_the_polyhedral_workload_is_seeded():
