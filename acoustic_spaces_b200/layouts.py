@@ -439,8 +439,9 @@ def cell_face_layouts(
     mat = material[:, boundary]
     open_link = ~blk
     beta_sum = np.zeros(B)
+    padded = np.concatenate([betas, [0.0]])  # (a room of no walls: only the grid's edge is met)
     for k in range(6):
-        term = np.where(mat[k] == -2, BOUNDARY * edge_admittance, BOUNDARY * betas[np.maximum(mat[k], 0)])
+        term = np.where(mat[k] == -2, BOUNDARY * edge_admittance, BOUNDARY * padded[np.maximum(mat[k], 0)])
         beta_sum = beta_sum + np.where(blk[k], term, 0.0)
     # The materials met, in order of first meeting, and the weight of each one's cut links.
     kinds = np.full((6, B), -1, np.int64)
