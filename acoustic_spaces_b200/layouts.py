@@ -679,10 +679,15 @@ def inside_points(
     rng: np.random.Generator, room: Room, box, count: int, clearance: float, apart: float = 0.0
 ) -> np.ndarray:
     """``count`` seeded points inside ``room`` at least ``clearance`` from each of its planes,
-    the others at least ``apart`` from the first (a source and its receivers)."""
+    the others at least ``apart`` from the first (a source and its receivers). Raises ValueError
+    when 200,000 draws find none (a room too small for the clearance)."""
     box = np.asarray(box, float)
     out: list[np.ndarray] = []
+    draws = 0
     while len(out) < count:
+        draws += 1
+        if draws > 200_000:
+            raise ValueError(f"no point {clearance} m inside every wall of the room: is it too small?")
         p = rng.uniform(0.0, box)
         if not np.all(room.normals @ p - room.offsets < -clearance):
             continue

@@ -213,3 +213,9 @@ def test_the_batched_solves_partition_across_ranks():
     mine = [L.partition([int(np.prod(L.room_grid(np.random.default_rng([3, k]).uniform(3.0, 12.0, 3), 0.2).shape))
                          for k in range(4)], 2)[r] for r in range(2)]  # fmt: skip
     assert sorted(mine[0] + mine[1]) == [0, 1, 2, 3]
+
+
+def test_inside_points_refuses_a_room_too_small_for_the_clearance():
+    room = L.shoebox(np.array([1.0, 1.0, 0.5]), [L.Material(0.1)] * 6)
+    with pytest.raises(ValueError, match="too small"):
+        L.inside_points(np.random.default_rng(0), room, (1.0, 1.0, 0.5), 2, 0.3)

@@ -94,3 +94,80 @@ def test_gpu_the_matched_layer_absorbs_a_pulse():
     from acoustic_spaces_b200 import B200WaveSolver
 
     _layer_against_edge(lambda layout, signal: B200WaveSolver(layout).run(signal))
+
+
+def _speed_runs(run):
+    # An open convex room with resonant walls and a 4-cell matched layer, laid out with a speed
+    # ratio of exactly 1 in every cell and with none.
+    rng = np.random.default_rng(7)
+    cell, box = 0.1, (4.0, 3.0, 2.4)
+    rate = C / (L.COURANT * cell)
+
+    def material(r):
+        return L.Material(float(r.uniform(0.02, 0.1)),
+                          L.resonant_branch(r.uniform(0.005, 0.5), r.uniform(0.5, 10.0), r.uniform(30.0, 300.0), rate))  # fmt: skip
+
+    room = L.convex_room(rng, box, faces=12, margin=cell * (4 + 3), open_face=1, material=material)
+    points = L.inside_points(rng, room, box, 3, 0.35, apart=0.35)
+    grid = L.Grid(-L.OFFSET * cell, cell, tuple(int(round(b / cell)) for b in box))
+    signal = L.gaussian_drive(rate, 400)
+    out = []
+    for speed in (1.0, None):
+        built = L.cell_face_layout(room, grid, points[0], points[1:], layer=4, layer_damping=0.5, speed=speed, rate=rate)
+        out.append(run(built.layout, signal))
+    return out
+
+
+def test_one_speed_everywhere_changes_nothing():
+    # As the reference's tests/test_wave.py:2545 checks its own solver: the scaled update with every
+    # cell at the grid's speed is the unscaled one, to the bit, walls and layer included.
+    scaled, plain = _speed_runs(lambda layout, signal: OracleSolver(layout).run(signal))
+    assert np.array_equal(scaled, plain)
+
+
+@pytest.mark.gpu
+def test_gpu_one_speed_everywhere_changes_nothing():
+    from acoustic_spaces_b200 import B200WaveSolver
+
+    scaled, plain = _speed_runs(lambda layout, signal: B200WaveSolver(layout).run(signal))
+    assert np.array_equal(scaled, plain)
+
+
+@pytest.mark.parametrize("stencil", [7, 19])
+def test_the_update_keeps_its_highest_modes_inside_the_stability_limit(stencil):
+    # The layout's constants (the reference's tests/test_wave.py:400-439): on a mode alternating
+    # along some axes (signs c = +-1) the update is p+ = A p - p-; the weights are the exact ones
+    # lowered by 2^-18, so that A stays 2^-16 inside -2, and in single precision a kicked
+    # checkerboard swings within about 1 / (2 sqrt(2^-18)) = 256 times its kick rather than growing.
+    import itertools
+
+    from conftest import load_golden
+
+    if stencil == 7:
+        layout = _rigid_box()[0].layout
+    else:
+        layout = load_golden("resonant19")[0]
+    axial = float(np.asarray(layout["weights"])[0])
+    diagonal = float(np.asarray(layout["weights"])[6]) if stencil == 19 else 0.0
+    centre = float(np.asarray(layout["centre"])[0])
+    margin = 2.0**-18
+    exact = (1 / 3, 0.0) if stencil == 7 else (0.25, 0.125)
+    np.testing.assert_allclose([axial, diagonal], np.multiply(exact, 1 - margin), rtol=2**-22)
+    c = np.array(list(itertools.product([1.0, -1.0], repeat=3)))
+    pairs = c[:, 0] * c[:, 1] + c[:, 0] * c[:, 2] + c[:, 1] * c[:, 2]
+    factors = centre + 2 * axial * c.sum(axis=1) + 4 * diagonal * pairs
+    assert factors[0] == 2.0 and factors.min() >= -2 + 4 * margin
+    f32 = np.float32
+    kicks = np.random.default_rng(1).uniform(0.5, 2.0, 32).astype(f32)
+    previous, current, peak = np.zeros_like(kicks), kicks.copy(), np.zeros_like(kicks)
+    a, d, centre32 = f32(axial), f32(diagonal), f32(centre)
+    for _ in range(20_000):
+        p, q = current, -current
+        if stencil == 7:
+            following = centre32 * p + a * (q + q + q + q + q + q) - previous
+        else:
+            edges = q + q + q + q + q + q + q + q + p + p + p + p
+            following = centre32 * p + a * (p + p + q + q + q + q) + d * edges - previous
+        previous, current = current, following
+        np.maximum(peak, np.abs(current), out=peak)
+    assert np.max(peak / kicks) < 1.1 * 256
