@@ -171,3 +171,32 @@ def test_the_update_keeps_its_highest_modes_inside_the_stability_limit(stencil):
         previous, current = current, following
         np.maximum(peak, np.abs(current), out=peak)
     assert np.max(peak / kicks) < 1.1 * 256
+
+
+@pytest.mark.parametrize("beta", [0.0, 0.1, 0.5, 1.0])
+def test_a_duct_end_reflects_as_its_admittance_says(beta):
+    # As the reference's tests/test_wave.py:538-568: a plane wave down an 80 m duct whose near end
+    # absorbs (admittance 1) reflects off the far end, of admittance beta, by (1 - beta) / (1 + beta)
+    # at normal incidence — the incident and reflected waves, 40-200 Hz, gated by Hann windows.
+    size = np.array([80.0, 0.6, 0.6])
+    cell = 0.1
+    rate = C / (L.COURANT * cell)
+    betas = [1.0, beta, 0.0, 0.0, 0.0, 0.0]  # -x (near), +x (far), then the duct's sides
+    room = L.shoebox(size, [L.Material(b) for b in betas])
+    built = L.cell_face_layout(room, L.room_grid(size, cell), (10.0, 0.3, 0.3), [(30.0, 0.3, 0.3)], rate=rate)
+    steps = int(0.45 * rate)
+    pressure = OracleSolver(built.layout, "fp64").run(L.gaussian_drive(rate, steps))[0]
+    delay = 6 * 0.5e-3 * rate  # the pulse's centre
+    n_fft = 1 << 14
+    f = np.fft.rfftfreq(n_fft, 1.0 / rate)
+    gain = np.clip((f - 40) / 20, 0, 1) * np.clip((200 - f) / 50, 0, 1)
+    pressure = np.fft.irfft(np.fft.rfft(pressure, n_fft) * gain, n_fft)[:steps]
+    t = (np.arange(steps) - delay) / rate
+
+    def gated(path: float) -> float:
+        x = t - path / C
+        window = np.where(np.abs(x) < 0.04, 0.5 + 0.5 * np.cos(np.pi * x / 0.04), 0.0)
+        return float(np.sum((pressure * window) ** 2))
+
+    reflection = math.sqrt(gated(120.0) / gated(20.0))
+    assert reflection == pytest.approx((1 - beta) / (1 + beta), abs=0.005 if beta < 1 else 0.05)
