@@ -353,7 +353,9 @@ def cell_face_layouts(
     # Cut links: between inside and outside cells, leaving through a wall (not the open face).
     offsets = [s[0] + s[1] * sy + s[2] * sz for s in AXIAL_STEPS]
     blocked = np.zeros((6, n), bool)
-    material = np.full((6, n), -1, np.int64)
+    if len(room.wall_materials()) >= np.iinfo(np.int16).max:
+        raise ValueError("a room of 32,767 materials or more")
+    material = np.full((6, n), -1, np.int16)  # a wall, screen or patch index; -1 none, -2 the edge
     candidates = np.flatnonzero(air & (types == 1))
     for k, off in enumerate(offsets):
         j = candidates + off
