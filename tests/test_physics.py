@@ -200,3 +200,30 @@ def test_a_duct_end_reflects_as_its_admittance_says(beta):
 
     reflection = math.sqrt(gated(120.0) / gated(20.0))
     assert reflection == pytest.approx((1 - beta) / (1 + beta), abs=0.005 if beta < 1 else 0.05)
+
+
+def test_a_tubes_modes_sit_at_the_schemes_own_frequencies():
+    # The axial modes of a rigid 6 m tube at 10 cm (cross-section 0.4 m, its first cross mode at
+    # 429 Hz, above those tested) at 20, 16 and 12 cells per wavelength: each at the frequency the
+    # 7-point leapfrog gives a plane wave along an axis, sin(w dt / 2) = sqrt(a) sin(k h / 2) with a
+    # the layout's (lowered) axial weight, to 2e-5 (the reference's tests/test_wave.py:287-317 measures
+    # its solver's dispersion the same way), and below the tube's own by that much.
+    size, h = np.array([6.0, 0.4, 0.4]), 0.1
+    rate = C / (L.COURANT * h)
+    room = L.shoebox(size, [L.Material(0.0)] * 6)
+    built = L.cell_face_layout(room, L.room_grid(size, h), (0.27, 0.2, 0.2), [(5.73, 0.2, 0.2)], rate=rate)
+    a = float(np.asarray(built.layout["weights"], np.float32)[0])
+    steps = int(3 * rate)
+    pressure = OracleSolver(built.layout, "fp64").run(L.ricker_drive(rate, steps, sigma_s=0.25e-3))[0]
+    n_fft = 1 << 20
+    spectrum = np.abs(np.fft.rfft(pressure * np.hanning(len(pressure)), n_fft))
+    f = np.fft.rfftfreq(n_fft, 1.0 / rate)
+    spacing = C / (2 * size[0])
+    for per_wavelength in (20, 16, 12):
+        m = round(2 * size[0] / (per_wavelength * h))
+        k = math.pi * m / size[0]
+        scheme = rate / math.pi * math.asin(math.sqrt(a) * math.sin(k * h / 2))
+        near = np.abs(f - scheme) < 0.4 * spacing
+        peak = f[near][np.argmax(spectrum[near])]
+        assert peak == pytest.approx(scheme, rel=2e-5), (per_wavelength, peak, scheme)
+        assert scheme < m * spacing
