@@ -869,13 +869,19 @@ def main() -> None:
         if world > 1:
             dist.barrier()
 
+    # Set-up, outside the metric and reported apart: the layout on the host, then the handle (its
+    # uploads, and the autotuner's trial steps).
+    t_setup = time.perf_counter()
     workload = build_workload(args)
+    layout_s = time.perf_counter() - t_setup
     desc = workload.description
+    t_setup = time.perf_counter()
     if args.launch:
         solver = B200WaveSolver(workload.built.layout, precision=args.precision, device=local, autotune=False)
         solver.set_launch(*(int(v) for v in args.launch.split(",")))
     else:
         solver = B200WaveSolver(workload.built.layout, precision=args.precision, device=local)
+    handle_s = time.perf_counter() - t_setup
     air = solver.air_cells
     probes = solver.probes
     steps, warmup = args.steps, args.warmup
@@ -1032,6 +1038,7 @@ def main() -> None:
                 "l2": "inputs larger than L2 (two pressure levels alone are "
                 f"{2 * 4 * desc['cells'] / 1e6:.0f} MB vs 126 MB L2), no flush",
                 "launch": solver.launch,
+                "setup_s": {"layout_on_host": round(layout_s, 2), "create_and_autotune": round(handle_s, 2)},
                 "precision": "FP32, bit-exact with the reference (no FMA, subnormals flushed)"
                 if args.precision == "fp32"
                 else "FP32 compensated: each cell's pressure and its increment (not bit-equal to the reference)",
