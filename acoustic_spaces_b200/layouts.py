@@ -142,30 +142,45 @@ class Built:
     sensitivity: dict | None = None
 
 
-def _signed(room: Room, grid: Grid, f: int, zs: slice | None = None) -> np.ndarray:
-    """n_f . centre - d_f of every cell (nz, ny, nx), or of the planes zs."""
-    nrm, d = room.normals[f], room.offsets[f]
-    x = nrm[0] * grid.centres(0)
-    y = nrm[1] * grid.centres(1)
-    z = nrm[2] * grid.centres(2)
-    if zs is not None:
-        z = z[zs]
-    return (z[:, None, None] + y[None, :, None]) + x[None, None, :] - d
-
-
 def _inside(room: Room, grid: Grid) -> tuple[np.ndarray, np.ndarray]:
     """Each cell's centre inside the room, and within a cell's reach of it (every plane's
-    signed distance below one cell), as (nz, ny, nx) masks."""
+    signed distance below one cell), as (nz, ny, nx) masks.
+
+    The signed distance of a cell's centre (x, y, z) to plane f is worked out in double as
+    (n_z z + n_y y) + n_x x - d_f; along a row of fixed y and z it never decreases in x where n_x > 0 (the
+    float sums are monotone) and never increases where n_x < 0, so the cells on the inner side of
+    the plane are a prefix or a suffix of the row. Its end is found by bisection on that same
+    expression, row by row, and each mask is the intersection of the planes' intervals."""
     nx, ny, nz = grid.shape
-    inside = np.ones((nz, ny, nx), bool)
-    near = np.ones((nz, ny, nx), bool)
+    xs, ys, zs = grid.centres(0), grid.centres(1), grid.centres(2)
+    limits = {"inside": 0.0, "near": 1.01 * grid.cell}
+    spans = {key: (np.zeros((nz, ny), np.int64), np.full((nz, ny), nx, np.int64)) for key in limits}
     for f in range(len(room.offsets)):
-        for z0 in range(0, nz, 64):
-            zs = slice(z0, min(nz, z0 + 64))
-            signed = _signed(room, grid, f, zs)
-            inside[zs] &= signed < 0.0
-            near[zs] &= signed < 1.01 * grid.cell
-    return inside, near
+        nrm, d = room.normals[f], room.offsets[f]
+        x = nrm[0] * xs
+        zy = (nrm[2] * zs)[:, None] + (nrm[1] * ys)[None, :]
+        for key, limit in limits.items():
+            lo, hi = spans[key]
+            if nrm[0] == 0.0:
+                lo[~(((zy + x[0]) - d) < limit)] = nx  # the whole row on one side
+                continue
+            # a: the count of leading cells on the inner side (n_x > 0), or of leading cells on
+            # the outer side, the first inner one (n_x < 0)
+            a, b = np.zeros((nz, ny), np.int64), np.full((nz, ny), nx, np.int64)
+            while np.any(a < b):
+                mid = (a + b) // 2
+                value = (zy + x[np.minimum(mid, nx - 1)]) - d
+                goes = (value < limit) if nrm[0] > 0 else ~(value < limit)
+                open_ = a < b
+                a = np.where(open_ & goes, mid + 1, a)
+                b = np.where(open_ & ~goes, mid, b)
+            if nrm[0] > 0:
+                np.minimum(hi, a, out=hi)
+            else:
+                np.maximum(lo, a, out=lo)
+    column = np.arange(nx)[None, None, :]
+    masks = [(column >= lo[:, :, None]) & (column < hi[:, :, None]) for lo, hi in spans.values()]
+    return masks[0], masks[1]
 
 
 def _first_wall(room: Room, grid: Grid, start: np.ndarray, end: np.ndarray) -> np.ndarray:
