@@ -371,18 +371,30 @@ def cell_face_layouts(
     if len(room.wall_materials()) >= np.iinfo(np.int16).max:
         raise ValueError("a room of 32,767 materials or more")
     material = np.full((6, n), -1, np.int16)  # a wall, screen or patch index; -1 none, -2 the edge
-    candidates = np.flatnonzero(air & (types == 1))
+    is_candidate = air & (types == 1)
+    candidates = np.flatnonzero(is_candidate)
+
+    def ahead(mask: np.ndarray, off: int) -> np.ndarray:
+        """mask[i + off] at every cell i (False where that leaves the grid: never a candidate's)."""
+        out = np.zeros_like(mask)
+        if off > 0:
+            out[:-off] = mask[off:]
+        else:
+            out[-off:] = mask[:off]
+        return out
+
     for k, off in enumerate(offsets):
-        j = candidates + off
-        edge_link = edge[j]
-        blocked[k, candidates[edge_link]] = True
-        material[k, candidates[edge_link]] = -2  # the grid's edge
+        edge_ahead = ahead(edge, off)
+        edge_link = is_candidate & edge_ahead
+        blocked[k, edge_link] = True
+        material[k, edge_link] = -2  # the grid's edge
         # Links that may meet a wall: an end inside and one out, or both within a cell's reach
         # of the room (a link can clip an edge or corner of it).
-        maybe = ~edge_link & near[candidates] & near[j] & ~(inside[candidates] & inside[j])
+        maybe = is_candidate & ~edge_ahead & near & ahead(near, off) & ~(inside & ahead(inside, off))
         if not np.any(maybe):
             continue
-        c, jj = candidates[maybe], j[maybe]
+        c = np.flatnonzero(maybe)
+        jj = c + off
         face = _first_wall(room, grid, c, jj)
         walled = face >= 0
         blocked[k, c[walled]] = True
