@@ -20,7 +20,6 @@ filled exactly, every rank's cells step as the whole grid's do: bit for bit.
 
 from __future__ import annotations
 
-import ctypes
 from dataclasses import dataclass
 from typing import Callable, Mapping, Sequence
 
@@ -279,25 +278,3 @@ def gather_records(slabs: Sequence[Slab], records: Sequence[np.ndarray], probes:
         for j, p in enumerate(s.probes):
             out[p] = rec[j]
     return out
-
-
-def oracle_planes(oracle, slab: Slab):
-    """Planes of an oracle instance (test infrastructure: the oracle steps the slabs on the CPU)."""
-
-    class _OraclePlanes(Planes):
-        def __init__(self) -> None:
-            nx, ny, _ = _planes(slab.layout)
-            self.plane = nx * ny
-
-        def _level(self) -> np.ndarray:
-            ptr = oracle.level_pointer()
-            n = self.plane * (slab.hi - slab.lo)
-            return np.ctypeslib.as_array(ctypes.cast(ptr, ctypes.POINTER(ctypes.c_float)), shape=(n,))
-
-        def get(self, q: int) -> np.ndarray:
-            return self._level()[q * self.plane : (q + 1) * self.plane].copy()
-
-        def put(self, q: int, values) -> None:
-            self._level()[q * self.plane : (q + 1) * self.plane] = np.asarray(values, np.float32)
-
-    return _OraclePlanes()

@@ -23,13 +23,36 @@ from oracle.oracle import OracleSolver
 CASES = ["open_layer", "open_layer_speed", "resonant19", "speed7", "fitted_open", "drive7"]
 
 
-def _whole_and_slabs(layout, signal, world):
-    whole = OracleSolver(layout)
+def oracle_planes(oracle, part: slabs.Slab) -> slabs.Planes:
+    """The planes of an oracle instance's current level (its elements float or double, as its
+    precision), for stepping the slabs on the CPU."""
+    import ctypes
+
+    nx, ny, _ = (int(v) for v in part.layout["shape"])
+    plane = nx * ny
+    kind, dtype = (ctypes.c_double, np.float64) if oracle.precision == "fp64" else (ctypes.c_float, np.float32)
+
+    class _Planes(slabs.Planes):
+        def _level(self) -> np.ndarray:
+            pointer = ctypes.cast(oracle.level_pointer(), ctypes.POINTER(kind))
+            return np.ctypeslib.as_array(pointer, shape=(plane * (part.hi - part.lo),))
+
+        def get(self, q: int) -> np.ndarray:
+            return self._level()[q * plane : (q + 1) * plane].copy()
+
+        def put(self, q: int, values) -> None:
+            self._level()[q * plane : (q + 1) * plane] = np.asarray(values, dtype)
+
+    return _Planes()
+
+
+def _whole_and_slabs(layout, signal, world, precision="fp32"):
+    whole = OracleSolver(layout, precision)
     expected = whole.run(signal)
     bounds = slabs.partition_planes(layout, world)
     parts = [slabs.slab(layout, bounds, r) for r in range(world)]
-    oracles = [OracleSolver(p.layout) for p in parts]
-    planes = [slabs.oracle_planes(o, p) for o, p in zip(oracles, parts)]
+    oracles = [OracleSolver(p.layout, precision) for p in parts]
+    planes = [oracle_planes(o, p) for o, p in zip(oracles, parts)]
     records = slabs.step_slabs(oracles, planes, parts, signal, lambda o, piece: o.run(piece))
     probes = len(np.asarray(layout["probe_start"])) - 1
     return whole, expected, parts, oracles, slabs.gather_records(parts, records, probes, len(signal))
@@ -69,10 +92,12 @@ def test_slabs_step_the_golden_grids_as_the_whole(name, world):
         assert np.array_equal(mine, current[s.z0 * nx * ny : s.z1 * nx * ny])
 
 
-def test_slabs_step_the_polyhedral_room_as_the_whole():
-    # 100 x 75 x 50: the open room with its resonant walls and 8-cell matched layer, as 4 slabs
+@pytest.mark.parametrize("precision", ["fp32", "fp64", "fp32c"])
+def test_slabs_step_the_polyhedral_room_as_the_whole(precision):
+    # 100 x 75 x 50: the open room with its resonant walls and 8-cell matched layer, as 4 slabs; in
+    # the compensated form too (the ghost planes carry the pressure; a cell's increment is its own)
     w = L.polyhedral_room(0, cell=0.2, steps=200)
-    _, expected, _, _, got = _whole_and_slabs(w.built.layout, w.signal, 4)
+    _, expected, _, _, got = _whole_and_slabs(w.built.layout, w.signal, 4, precision)
     assert np.array_equal(got, expected)
 
 
@@ -86,7 +111,7 @@ def _rank(rank: int, world: int, port: int, out):
         bounds = slabs.partition_planes(w.built.layout, world)
         part = slabs.slab(w.built.layout, bounds, rank)
         oracle = OracleSolver(part.layout)
-        planes = slabs.oracle_planes(oracle, part)
+        planes = oracle_planes(oracle, part)
         rec = []
         for k in range(len(w.signal)):
             rec.append(oracle.run(w.signal[k : k + 1]))
