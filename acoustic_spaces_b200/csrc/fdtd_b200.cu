@@ -235,6 +235,17 @@ int validate(const fdtd_layout *L, std::string &why) {
         return refuse("the layout's weights do not match its stencil");
     if (!L->types) return refuse("the layout has no cell types");
     if (L->scaled && !L->scale) return refuse("a scaled layout needs each cell's scale");
+    if (L->scaled) {
+        // A cell's scale is its speed ratio squared; the reference refuses a ratio outside (0, 1]
+        // (fdtd.hpp:415-425), so no scale lies outside it either.
+        const uint64_t n = L->nx * L->ny * L->nz;
+        for (uint64_t i = 0; i < n; ++i)
+            if (!(L->scale[i] > 0.0f && L->scale[i] <= 1.0f))
+                return refuse("each cell's speed of sound over the grid's lies in (0, 1]");
+        for (uint64_t c = 0; c < L->layer_count; ++c)
+            if (L->layer_scale && !(L->layer_scale[c] > 0.0f && L->layer_scale[c] <= 1.0f))
+                return refuse("each cell's speed of sound over the grid's lies in (0, 1]");
+    }
     const uint64_t nx = L->nx, ny = L->ny, nz = L->nz, sz = nx * ny;
     auto inner = [&](uint64_t i) {
         const uint64_t x = i % nx, y = (i / nx) % ny, z = i / sz;

@@ -182,3 +182,14 @@ def test_the_loader_refuses_a_library_built_from_other_sources(monkeypatch):
     monkeypatch.setattr(build, "source_id", lambda: "not-these-sources")
     with pytest.raises(RuntimeError, match="built from other sources"):
         _abi.load_library()
+
+
+@pytest.mark.parametrize("bad", [0.0, 1.5, float("nan")])
+def test_a_speed_outside_its_range_is_refused(bad):
+    # A cell's scale is its speed ratio squared, the ratio in (0, 1] (fdtd.hpp:415-425).
+    layout, _, _ = load_golden("speed7")
+    scale = np.asarray(layout["scale"], np.float32).copy()
+    scale[len(scale) // 2] = bad
+    status, error = _create(dict(layout, scale=scale))
+    assert status == _abi.FDTD_EINVAL and "lies in (0, 1]" in error
+    assert _create(layout)[0] != _abi.FDTD_EINVAL  # the golden layout itself passes the check
