@@ -124,3 +124,22 @@ def test_gpu_steps_the_half_space_as_the_oracle(barrier):
         ours = B200WaveSolver(w.built.layout, precision=precision).run(w.signal)
         oracle = OracleSolver(w.built.layout, precision).run(w.signal)
         np.testing.assert_array_equal(ours, oracle, err_msg=precision)
+
+
+@pytest.mark.parametrize("sigma", [50e3, 1e6, 20e6])
+def test_the_ground_fit_follows_mikis_admittance(sigma):
+    # A real beta and up to three relaxation branches (g jw / (jw + 2 pi fc), fc log-spaced over the
+    # band, non-negative least squares: passive) against Miki's admittance, 20-600 Hz: within 15 %
+    # rms and 30 % at worst over the flow resistivities of the half-space (the fit's bound, not the
+    # model's: its corners are fixed).
+    import math
+
+    rate = 343.0 / (layouts.COURANT * 0.1)
+    ground = layouts.porous_ground(sigma, rate)
+    assert ground.beta >= 0.0 and np.all(np.asarray(ground.branches) >= 0.0)
+    f = np.geomspace(20.0, 600.0, 400)
+    jw = 2j * math.pi * f
+    fitted = ground.beta + sum((1.0 / r) * jw / (jw + q * rate / r) for _, r, q in np.asarray(ground.branches))
+    miki = layouts.miki_admittance(f, sigma)
+    rel = np.abs(fitted - miki) / np.abs(miki)
+    assert np.sqrt(np.mean(rel**2)) < 0.15 and rel.max() < 0.30, (np.sqrt(np.mean(rel**2)), rel.max())
