@@ -1,13 +1,14 @@
-"""Known answers of the scheme itself, independent of the reference's code: a rigid box rings at
-its room modes (the reference's tests/test_wave.py:263-284 checks its own solver the same way), and
-the matched layer takes a pulse's energy out of an open grid far better than the grid's edge alone.
+"""Known answers of the scheme itself, independent of the reference's code: room modes, the
+scheme's own dispersion, a wall's reflection, the stability margin of the update's constants, what
+the matched layer takes out of a pulse, and a speed field of ones.
 
-On the oracle (CPU) and on the B200 (gpu): both step the builder's layouts, so the answers pin the
-layouts as well as the stepping.
+On the oracle (CPU) and, where marked, on the B200: both step the builder's layouts, so the answers
+pin the layouts as well as the stepping.
 """
 
 from __future__ import annotations
 
+import itertools
 import math
 
 import numpy as np
@@ -17,41 +18,173 @@ from acoustic_spaces_b200 import layouts as L
 from oracle.oracle import OracleSolver
 
 C = 343.0
-SIZE = (2.0, 1.5, 1.0)
-MODES = ((1, 0, 0), (0, 1, 0), (1, 1, 0))
+
+
+def _peak(series: np.ndarray, rate: float, around: float, half_width: float) -> float:
+    """The frequency of the strongest spectral line of ``series`` within ``half_width`` Hz of
+    ``around``: a Blackman-windowed, zero-padded transform, its largest bin there refined by the
+    parabola through the log magnitudes of that bin and its two neighbours."""
+    n = 1 << max(18, int(math.ceil(math.log2(len(series)))) + 3)
+    spectrum = np.abs(np.fft.rfft(series * np.blackman(len(series)), n))
+    step = rate / n
+    lo, hi = int((around - half_width) / step), int((around + half_width) / step) + 1
+    k = lo + int(np.argmax(spectrum[lo:hi]))
+    a, b, c = np.log(spectrum[k - 1 : k + 2] + 1e-300)
+    return (k + 0.5 * (a - c) / (a - 2 * b + c)) * step
+
+
+# ---- a rigid box's modes ---------------------------------------------------------------------
+
+BOX = (2.0, 1.5, 1.0)
 
 
 def _rigid_box(cell: float = 0.1):
     rate = C / (L.COURANT * cell)
-    room = L.shoebox(np.asarray(SIZE), [L.Material(0.0)] * 6)
-    built = L.cell_face_layout(room, L.room_grid(np.asarray(SIZE), cell), (0.33, 0.27, 0.33), [(1.67, 1.21, 0.67)],
+    room = L.shoebox(np.asarray(BOX), [L.Material(0.0)] * 6)
+    built = L.cell_face_layout(room, L.room_grid(np.asarray(BOX), cell), (0.33, 0.27, 0.33), [(1.67, 1.21, 0.67)],
                                rate=rate)  # fmt: skip
     return built, rate
 
 
-def _mode_peaks(pressure: np.ndarray, rate: float) -> list[tuple[float, float]]:
-    n_fft = 1 << 18
-    spectrum = np.abs(np.fft.rfft(pressure, n_fft))
-    f = np.fft.rfftfreq(n_fft, 1.0 / rate)
-    out = []
-    for mode in MODES:
-        expected = C / 2 * math.hypot(*(m / s for m, s in zip(mode, SIZE)))
-        near = (f > expected - 4) & (f < expected + 4)
-        out.append((float(f[near][np.argmax(spectrum[near])]), expected))
-    return out
+def _lowest_modes(count: int) -> list[tuple[tuple[int, int, int], float]]:
+    """The box's lowest ``count`` modes above 0 Hz: C/2 sqrt((l/X)^2 + (m/Y)^2 + (n/Z)^2)."""
+    modes = [(lmn, C / 2 * math.sqrt(sum((q / s) ** 2 for q, s in zip(lmn, BOX))))
+             for lmn in itertools.product(range(4), repeat=3) if any(lmn)]  # fmt: skip
+    return sorted(modes, key=lambda m: m[1])[:count]
 
 
-def _check(run):
+def _check_modes(run):
     built, rate = _rigid_box()
     assert built.air_cells == 20 * 15 * 10
-    steps = int(4 * rate)
-    pressure = run(built.layout, L.ricker_drive(rate, steps))[0]
-    for peak, expected in _mode_peaks(pressure, rate):
-        assert peak == pytest.approx(expected, abs=0.6), (peak, expected)
+    response = run(built.layout, L.ricker_drive(rate, int(4 * rate)))[0]
+    modes = _lowest_modes(3)
+    assert [m[0] for m in modes] == [(1, 0, 0), (0, 1, 0), (1, 1, 0)]
+    for lmn, expected in modes:
+        # (the 10 cm grid's dispersion puts them a tenth of a hertz low)
+        assert abs(_peak(response, rate, expected, 3.0) - expected) < 0.5, lmn
 
 
 def test_a_rigid_box_rings_at_its_modes():
-    _check(lambda layout, signal: OracleSolver(layout).run(signal))
+    _check_modes(lambda layout, signal: OracleSolver(layout).run(signal))
+
+
+@pytest.mark.gpu
+def test_gpu_a_rigid_box_rings_at_its_modes():
+    from acoustic_spaces_b200 import B200WaveSolver
+
+    _check_modes(lambda layout, signal: B200WaveSolver(layout).run(signal))
+
+
+# ---- the scheme's own dispersion -------------------------------------------------------------
+
+
+def test_a_tubes_modes_sit_at_the_schemes_own_frequencies():
+    # The axial modes of a rigid 6 m tube at 10 cm (cross-section 0.4 m, its first cross mode at
+    # 429 Hz, above those tested) at 20, 16 and 12 cells per wavelength: each where the 7-point
+    # leapfrog puts a plane wave along an axis, sin(w dt / 2) = sqrt(a) sin(k h / 2) with a the
+    # layout's (lowered) axial weight, to 1e-6; below the tube's continuous mode by 0.3-0.8 %.
+    size, h = np.array([6.0, 0.4, 0.4]), 0.1
+    rate = C / (L.COURANT * h)
+    room = L.shoebox(size, [L.Material(0.0)] * 6)
+    built = L.cell_face_layout(room, L.room_grid(size, h), (0.27, 0.2, 0.2), [(5.73, 0.2, 0.2)], rate=rate)
+    a = float(np.asarray(built.layout["weights"], np.float32)[0])
+    response = OracleSolver(built.layout, "fp64").run(L.ricker_drive(rate, int(3 * rate), sigma_s=0.25e-3))[0]
+    spacing = C / (2 * size[0])
+    for per_wavelength in (20, 16, 12):
+        m = round(2 * size[0] / (per_wavelength * h))
+        scheme = rate / math.pi * math.asin(math.sqrt(a) * math.sin(math.pi * m * h / (2 * size[0])))
+        assert _peak(response, rate, scheme, 0.3 * spacing) == pytest.approx(scheme, rel=1e-6), per_wavelength
+        assert 0.002 < 1 - scheme / (m * spacing) < 0.01
+
+
+# ---- a wall's reflection -----------------------------------------------------------------------
+
+
+@pytest.mark.parametrize("beta", [0.0, 0.1, 0.3, 0.5, 1.0])
+def test_a_duct_end_reflects_as_its_admittance_says(beta):
+    # A plane wave down an 80 m duct whose near end absorbs (admittance 1): the pulse that comes
+    # back from the far end, of admittance beta, against the one that passed, each cut out of the
+    # response by a Tukey gate round its arrival. Below the duct's cross modes the ratio of their
+    # spectra is the grid's reflection factor: (1 - beta) / (1 + beta), normal incidence on a
+    # locally reacting wall, plus a discretisation term that grows with frequency (at 10 cm, 0.08
+    # at 180 Hz for an absorbing end). A quadratic through the ratio over 40-200 Hz meets the
+    # continuous factor at 0 Hz to 1e-3; a rigid end reflects all of it at every frequency (to 1e-4,
+    # what the gates leave).
+    from scipy.signal.windows import tukey
+
+    size, cell = np.array([80.0, 0.6, 0.6]), 0.1
+    rate = C / (L.COURANT * cell)
+    room = L.shoebox(size, [L.Material(b) for b in (1.0, beta, 0.0, 0.0, 0.0, 0.0)])  # -x near, +x far
+    source, receiver = (10.0, 0.3, 0.3), (30.0, 0.3, 0.3)
+    built = L.cell_face_layout(room, L.room_grid(size, cell), source, [receiver], rate=rate)
+    steps, sigma = int(0.45 * rate), 1.5e-3
+    # (a Ricker drive: a Gaussian's pressure would leave a plateau behind the passing front that
+    # the reflected pulse's gate cuts into)
+    response = OracleSolver(built.layout, "fp64").run(L.ricker_drive(rate, steps, sigma_s=sigma))[0]
+    n = 1 << 14
+    f = np.fft.rfftfreq(n, 1.0 / rate)
+    band = (f >= 40.0) & (f <= 200.0)
+
+    def spectrum(path: float) -> np.ndarray:
+        centre = int(round((6 * sigma + path / C) * rate))
+        width = int(0.06 * rate)
+        gate = np.zeros(steps)
+        gate[centre - width // 2 : centre - width // 2 + width] = tukey(width, 0.5)
+        return np.abs(np.fft.rfft(response * gate, n))[band]
+
+    ratio = spectrum((size[0] - source[0]) + (size[0] - receiver[0])) / spectrum(receiver[0] - source[0])
+    expected = (1 - beta) / (1 + beta)
+    assert np.polyfit(f[band], ratio, 2)[-1] == pytest.approx(expected, abs=1e-3)
+    assert np.all(np.abs(ratio - expected) < (1e-4 if beta == 0 else 0.1))
+
+
+# ---- the update's stability margin -------------------------------------------------------------
+
+
+@pytest.mark.parametrize("stencil", [7, 19])
+def test_the_update_keeps_its_highest_modes_inside_the_stability_limit(stencil):
+    # On a mode that alternates in sign along some axes (s_a = -1) and is constant along the rest
+    # (s_a = 1), the update is the two-step recurrence p+ = A p - p-, A = centre + 2 axial sum_a s_a
+    # + 4 diagonal sum_{a<b} s_a s_b, whose roots stay on the unit circle while |A| <= 2. The
+    # layout's weights are the exact ones times (1 - 2^-18): A is 2 for a constant pressure and at
+    # least -2 + 2^-16 elsewhere. Stepped in single precision, a kicked mode then swings within
+    # 1 / sin(acos(A / 2)) of its kick (256 at the margin) instead of growing.
+    from conftest import load_golden
+
+    layout = _rigid_box()[0].layout if stencil == 7 else load_golden("resonant19")[0]
+    w = np.asarray(layout["weights"], np.float64)
+    axial, diagonal = float(w[0]), (float(w[6]) if stencil == 19 else 0.0)
+    centre = float(np.asarray(layout["centre"])[0])
+    exact = (1.0 / 3.0, 0.0) if stencil == 7 else (0.25, 0.125)
+    assert axial == pytest.approx(exact[0] * (1 - 2.0**-18), rel=2**-22)
+    assert diagonal == pytest.approx(exact[1] * (1 - 2.0**-18), rel=2**-22)
+    patterns = np.array(list(itertools.product((1.0, -1.0), repeat=3)))
+    pair_sum = np.array([s[0] * s[1] + s[0] * s[2] + s[1] * s[2] for s in patterns])
+    A = centre + 2 * axial * patterns.sum(axis=1) + 4 * diagonal * pair_sum
+    assert A.max() == 2.0 and A.min() >= -2 + 2.0**-16
+    # the kicked recurrence in float32, every sign pattern at once: six face neighbours, twelve
+    # edge neighbours
+    f32 = np.float32
+    c32, a32, d32 = f32(centre), f32(axial), f32(diagonal)
+    kick = np.random.default_rng(3).uniform(0.5, 2.0, len(patterns)).astype(f32)
+    s = patterns.astype(f32)
+    before, now = np.zeros_like(kick), kick.copy()
+    worst = np.zeros_like(kick)
+    for _ in range(20_000):
+        axial_sum = np.zeros_like(now)
+        for sign in (s[:, 0], s[:, 0], s[:, 1], s[:, 1], s[:, 2], s[:, 2]):
+            axial_sum = axial_sum + sign * now
+        edge_sum = np.zeros_like(now)
+        for sign in [s[:, 0] * s[:, 1]] * 4 + [s[:, 0] * s[:, 2]] * 4 + [s[:, 1] * s[:, 2]] * 4:
+            edge_sum = edge_sum + sign * now
+        before, now = now, c32 * now + a32 * axial_sum + d32 * edge_sum - before
+        np.maximum(worst, np.abs(now), out=worst)
+    bound = 1.0 / np.sqrt(np.maximum(1e-12, 1.0 - (np.clip(A, -2, 2) / 2) ** 2))
+    oscillating = np.abs(A) < 2.0
+    assert np.all(worst[oscillating] / kick[oscillating] <= 1.1 * bound[oscillating])
+
+
+# ---- the matched layer, and a speed field of ones ---------------------------------------------
 
 
 def _open_pulse_energy(run, layer: int = 8) -> tuple[float, float]:
@@ -80,13 +213,6 @@ def _layer_against_edge(run):
 
 def test_the_matched_layer_absorbs_a_pulse():
     _layer_against_edge(lambda layout, signal: OracleSolver(layout).run(signal))
-
-
-@pytest.mark.gpu
-def test_gpu_a_rigid_box_rings_at_its_modes():
-    from acoustic_spaces_b200 import B200WaveSolver
-
-    _check(lambda layout, signal: B200WaveSolver(layout).run(signal))
 
 
 @pytest.mark.gpu
@@ -131,99 +257,3 @@ def test_gpu_one_speed_everywhere_changes_nothing():
 
     scaled, plain = _speed_runs(lambda layout, signal: B200WaveSolver(layout).run(signal))
     assert np.array_equal(scaled, plain)
-
-
-@pytest.mark.parametrize("stencil", [7, 19])
-def test_the_update_keeps_its_highest_modes_inside_the_stability_limit(stencil):
-    # The layout's constants (the reference's tests/test_wave.py:400-439): on a mode alternating
-    # along some axes (signs c = +-1) the update is p+ = A p - p-; the weights are the exact ones
-    # lowered by 2^-18, so that A stays 2^-16 inside -2, and in single precision a kicked
-    # checkerboard swings within about 1 / (2 sqrt(2^-18)) = 256 times its kick rather than growing.
-    import itertools
-
-    from conftest import load_golden
-
-    if stencil == 7:
-        layout = _rigid_box()[0].layout
-    else:
-        layout = load_golden("resonant19")[0]
-    axial = float(np.asarray(layout["weights"])[0])
-    diagonal = float(np.asarray(layout["weights"])[6]) if stencil == 19 else 0.0
-    centre = float(np.asarray(layout["centre"])[0])
-    margin = 2.0**-18
-    exact = (1 / 3, 0.0) if stencil == 7 else (0.25, 0.125)
-    np.testing.assert_allclose([axial, diagonal], np.multiply(exact, 1 - margin), rtol=2**-22)
-    c = np.array(list(itertools.product([1.0, -1.0], repeat=3)))
-    pairs = c[:, 0] * c[:, 1] + c[:, 0] * c[:, 2] + c[:, 1] * c[:, 2]
-    factors = centre + 2 * axial * c.sum(axis=1) + 4 * diagonal * pairs
-    assert factors[0] == 2.0 and factors.min() >= -2 + 4 * margin
-    f32 = np.float32
-    kicks = np.random.default_rng(1).uniform(0.5, 2.0, 32).astype(f32)
-    previous, current, peak = np.zeros_like(kicks), kicks.copy(), np.zeros_like(kicks)
-    a, d, centre32 = f32(axial), f32(diagonal), f32(centre)
-    for _ in range(20_000):
-        p, q = current, -current
-        if stencil == 7:
-            following = centre32 * p + a * (q + q + q + q + q + q) - previous
-        else:
-            edges = q + q + q + q + q + q + q + q + p + p + p + p
-            following = centre32 * p + a * (p + p + q + q + q + q) + d * edges - previous
-        previous, current = current, following
-        np.maximum(peak, np.abs(current), out=peak)
-    assert np.max(peak / kicks) < 1.1 * 256
-
-
-@pytest.mark.parametrize("beta", [0.0, 0.1, 0.5, 1.0])
-def test_a_duct_end_reflects_as_its_admittance_says(beta):
-    # As the reference's tests/test_wave.py:538-568: a plane wave down an 80 m duct whose near end
-    # absorbs (admittance 1) reflects off the far end, of admittance beta, by (1 - beta) / (1 + beta)
-    # at normal incidence — the incident and reflected waves, 40-200 Hz, gated by Hann windows.
-    size = np.array([80.0, 0.6, 0.6])
-    cell = 0.1
-    rate = C / (L.COURANT * cell)
-    betas = [1.0, beta, 0.0, 0.0, 0.0, 0.0]  # -x (near), +x (far), then the duct's sides
-    room = L.shoebox(size, [L.Material(b) for b in betas])
-    built = L.cell_face_layout(room, L.room_grid(size, cell), (10.0, 0.3, 0.3), [(30.0, 0.3, 0.3)], rate=rate)
-    steps = int(0.45 * rate)
-    pressure = OracleSolver(built.layout, "fp64").run(L.gaussian_drive(rate, steps))[0]
-    delay = 6 * 0.5e-3 * rate  # the pulse's centre
-    n_fft = 1 << 14
-    f = np.fft.rfftfreq(n_fft, 1.0 / rate)
-    gain = np.clip((f - 40) / 20, 0, 1) * np.clip((200 - f) / 50, 0, 1)
-    pressure = np.fft.irfft(np.fft.rfft(pressure, n_fft) * gain, n_fft)[:steps]
-    t = (np.arange(steps) - delay) / rate
-
-    def gated(path: float) -> float:
-        x = t - path / C
-        window = np.where(np.abs(x) < 0.04, 0.5 + 0.5 * np.cos(np.pi * x / 0.04), 0.0)
-        return float(np.sum((pressure * window) ** 2))
-
-    reflection = math.sqrt(gated(120.0) / gated(20.0))
-    assert reflection == pytest.approx((1 - beta) / (1 + beta), abs=0.005 if beta < 1 else 0.05)
-
-
-def test_a_tubes_modes_sit_at_the_schemes_own_frequencies():
-    # The axial modes of a rigid 6 m tube at 10 cm (cross-section 0.4 m, its first cross mode at
-    # 429 Hz, above those tested) at 20, 16 and 12 cells per wavelength: each at the frequency the
-    # 7-point leapfrog gives a plane wave along an axis, sin(w dt / 2) = sqrt(a) sin(k h / 2) with a
-    # the layout's (lowered) axial weight, to 2e-5 (the reference's tests/test_wave.py:287-317 measures
-    # its solver's dispersion the same way), and below the tube's own by that much.
-    size, h = np.array([6.0, 0.4, 0.4]), 0.1
-    rate = C / (L.COURANT * h)
-    room = L.shoebox(size, [L.Material(0.0)] * 6)
-    built = L.cell_face_layout(room, L.room_grid(size, h), (0.27, 0.2, 0.2), [(5.73, 0.2, 0.2)], rate=rate)
-    a = float(np.asarray(built.layout["weights"], np.float32)[0])
-    steps = int(3 * rate)
-    pressure = OracleSolver(built.layout, "fp64").run(L.ricker_drive(rate, steps, sigma_s=0.25e-3))[0]
-    n_fft = 1 << 20
-    spectrum = np.abs(np.fft.rfft(pressure * np.hanning(len(pressure)), n_fft))
-    f = np.fft.rfftfreq(n_fft, 1.0 / rate)
-    spacing = C / (2 * size[0])
-    for per_wavelength in (20, 16, 12):
-        m = round(2 * size[0] / (per_wavelength * h))
-        k = math.pi * m / size[0]
-        scheme = rate / math.pi * math.asin(math.sqrt(a) * math.sin(k * h / 2))
-        near = np.abs(f - scheme) < 0.4 * spacing
-        peak = f[near][np.argmax(spectrum[near])]
-        assert peak == pytest.approx(scheme, rel=2e-5), (per_wavelength, peak, scheme)
-        assert scheme < m * spacing
