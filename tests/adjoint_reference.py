@@ -2,14 +2,16 @@
 coefficients, by PyTorch autograd through a float64 restatement of the forward step.
 
 This is the checker of the CUDA reverse-time stepper. It differentiates the forward scheme as the
-reference steps it (special rows fdtd.hpp:860-881, interior cells fdtd.hpp:242-288 for the
-7-point stencil, probes fdtd.hpp:3525-3533), written here with whole-array torch operations, and
-shares no derivation with the hand-written transposed operator of the CUDA library. Grids of the
-7-point stencil without a speed field. With a matched layer it also steps the layer as the
-reference does (fdtd.hpp:2242-2264: each cell its own copy of both faces on every axis) and gives
-the gradient in the layer's twelve coefficient tables (keep and push of the centres and the faces
-per axis, fdtd.hpp:2219-2238) — the checker of a gradient in the layer's parameters, which the
-CUDA adjoint does not compute yet (it refuses grids with a matched layer).
+reference steps it (special rows fdtd.hpp:860-881, interior cells fdtd.hpp:242-288, probes
+fdtd.hpp:3525-3533), written here with whole-array torch operations, and shares no derivation with
+the hand-written transposed operator of the CUDA library. Both stencils (7 and 19 points), with
+or without a speed field (each interior cell's update scaled by its speed of sound over the
+grid's, squared, as fdtd.hpp:250-262 scales it). With a matched layer it also steps the layer as
+the reference does (fdtd.hpp:2242-2264: each cell its own copy of both faces on every axis; with a
+speed field each cell's push scaled by its own factor) and gives the gradient in the layer's
+twelve coefficient tables (keep and push of the centres and the faces per axis,
+fdtd.hpp:2219-2238). The CUDA adjoint covers the 7-point stencil without a speed field or a
+matched layer so far; the rest of this checker is the bar for what comes next.
 """
 
 from __future__ import annotations
@@ -36,10 +38,9 @@ class AutogradStepper:
 
     def __init__(self, layout) -> None:
         nx, ny, nz = (int(v) for v in layout["shape"])
-        if len(np.asarray(layout.get("scale", ()))):
-            raise ValueError("the autograd stepper covers grids without a speed field")
-        if int(np.asarray(layout["stencil"]).reshape(-1)[0]) != 7:
-            raise ValueError("the autograd stepper covers the 7-point stencil")
+        stencil = int(np.asarray(layout["stencil"]).reshape(-1)[0])
+        if stencil not in (7, 19):
+            raise ValueError("the stencil has 7 or 19 points")
         sy, sz = nx, nx * ny
         self.n = nx * ny * nz
         offsets = torch.tensor([x + y * sy + z * sz for x, y, z in _DIRECTIONS], dtype=torch.int64)
@@ -47,8 +48,16 @@ class AutogradStepper:
         types = torch.as_tensor(np.asarray(layout["types"]))
         self.interior = torch.nonzero(types == 1).flatten()
         self.neighbours = self.interior[:, None] + offsets[None, :6]
+        self.edges = self.interior[:, None] + offsets[None, 6:] if stencil == 19 else None
+        weights = np.asarray(layout["weights"], np.float64)
         self.centre = float(np.asarray(layout["centre"])[0])
-        self.axial = float(np.asarray(layout["weights"])[0])
+        self.total = float(np.asarray(layout["total"])[0])
+        self.axial = float(weights[0])
+        self.diagonal = float(weights[6]) if stencil == 19 else 0.0
+        # A speed field: each interior cell's factor, and each layer cell's (its push's).
+        scale = np.asarray(layout.get("scale", ()), np.float64)
+        self.scale = torch.as_tensor(scale[self.interior.numpy()]) if len(scale) else None
+        self.layer_scale = torch.as_tensor(np.asarray(layout["layer_scale"], np.float64)) if len(scale) else None
         self.special = torch.as_tensor(np.asarray(layout["special"], np.int64))
         link_start = np.asarray(layout["link_start"], np.int64)
         state_start = np.asarray(layout["state_start"], np.int64)
@@ -103,12 +112,22 @@ class AutogradStepper:
             x = self.coords[axis]
             keep, keep_face = p[KEEP[2 * axis]], p[KEEP[2 * axis + 1]]
             push, push_face = p[PUSH[2 * axis]], p[PUSH[2 * axis + 1]]
-            coef.append((keep[x], push[x], keep_face[x], push_face[x], keep_face[x + 1], push_face[x + 1]))
+            pushed = push[x] if self.layer_scale is None else push[x] * self.layer_scale
+            coef.append((keep[x], pushed, keep_face[x], push_face[x], keep_face[x + 1], push_face[x + 1]))
         series = []
         for s in np.asarray(signal, np.float64):
             series.append(torch.zeros(self.probes, dtype=torch.float64).index_add(
                 0, self.probe_row, self.probe_weights * b[self.probe_cells]))
-            interior = self.centre * b[self.interior] + self.axial * b[self.neighbours].sum(1) - a[self.interior]
+            here, sums = b[self.interior], b[self.neighbours].sum(1)
+            if self.scale is None:
+                interior = self.centre * here + self.axial * sums - a[self.interior]
+                if self.edges is not None:
+                    interior = interior + self.diagonal * b[self.edges].sum(1)
+            else:
+                sc = self.scale
+                interior = (2.0 - self.total * sc) * here + (sc * self.axial) * sums - a[self.interior]
+                if self.edges is not None:
+                    interior = interior + (sc * self.diagonal) * b[self.edges].sum(1)
             links = torch.zeros(specials, dtype=torch.float64).index_add(
                 0, self.link_row, self.link_weight * b[self.link_cell])
             own = p["now"] * wb - p["before"] * wa
