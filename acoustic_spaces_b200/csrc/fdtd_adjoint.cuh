@@ -1,6 +1,6 @@
 // Device code of the reverse-time (adjoint) stepper: the gradient of a loss of the probes'
 // series with respect to the special rows' coefficients, for grids of the 7-point stencil without
-// a matched layer or a speed field.
+// a matched layer (with or without a speed field).
 //
 // A forward step maps the levels (u_n, u_{n-1}) and branch velocities (w_n, w_{n-1}) to u_{n+1},
 // w_{n+1}: z_{n+1} = G z_n - H z_{n-1} (+ the source), z = (u, w). For a special row (cell i,
@@ -16,6 +16,10 @@
 // (an interior cell's L~ is its lam). Interior cells take the forward bulk sweep on the adjoint
 // levels (their readers are interior and axial), except the cells that special rows read, which
 // correct_kernel forms whole; special rows a gather over their readers (a transposed list).
+// With a speed field an interior cell's adjoint is carried as s lam (s its scale): the forward
+// scaled sweep steps it, and a corrected cell forms it with its own scale (the host folds s into
+// its rows' coefficients and probe weights; a special row's gather takes axial x s lam from an
+// interior reader, which is its coefficient a s times lam).
 // The gradient of step n, with U = L~_{n+1}[i] and own~_j = om_{n+1}[j] - W_j ci U:
 //   dL/dci += U x,  dL/dcb += -U ci u_{n-1}[i],  dL/dnow_j += own~_j w_n[j],
 //   dL/dbefore_j += -own~_j w_{n-1}[j],  dL/dgain_j += om_{n+1}[j] (u_{n+1}[i] - u_{n-1}[i])
@@ -47,7 +51,8 @@ struct AdjointTables {
     const uint32_t *corrected_cell, *corrected_start, *corrected_row;
     const uint8_t *corrected_mask;
     const double *corrected_coef;
-    float axial, centre;
+    const float *corrected_scale;  // with a speed field: each corrected cell's scale (else null)
+    float axial, centre, total;
     int32_t offset[6];
     // The probes' terms dL/dy_p x weight on the cells they read, by cell: a special row's at
     // special_read_start[k] .. [k + 1], a corrected cell's at corrected_read_start[c] .. [c + 1], of
@@ -90,7 +95,13 @@ __device__ __forceinline__ void correct_cell(const AdjointTables &t, uint32_t c,
 #pragma unroll
     for (int d = 0; d < 6; ++d)
         if (!(special & (1u << d))) sum += lam_next[(uint32_t)((int64_t)cell + t.offset[d])];
-    T value = (T)t.centre * lam_next[cell] + (T)t.axial * sum - lam_out[cell];
+    T centre = (T)t.centre, axial = (T)t.axial;
+    if (t.corrected_scale) {  // as the forward scaled sweep forms its cells
+        const T sc = (T)t.corrected_scale[c];
+        centre = (T)2 - (T)t.total * sc;
+        axial = sc * (T)t.axial;
+    }
+    T value = centre * lam_next[cell] + axial * sum - lam_out[cell];
     for (uint32_t e = t.corrected_start[c], end = t.corrected_start[c + 1]; e < end; ++e)
         value += (T)t.corrected_coef[e] * tilde[t.corrected_row[e]];
     const double probed = probe_terms(t, t.corrected_read_start[c], t.corrected_read_start[c + 1], dloss, stride, step);

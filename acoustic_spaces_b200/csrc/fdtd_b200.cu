@@ -104,6 +104,7 @@ struct fdtd_solver {
     void *layer_parts = nullptr;            // 3 arrays of the layer's cells: p_x, p_y, p_z
     std::vector<uint32_t> layer_cells;      // pitched, in the layout's order (for fdtd_read_state)
     const uint8_t *types_device = nullptr;  // the pitched cell types
+    const float *scale_device = nullptr;    // with a speed field: each pitched cell's scale
     // Per axis, the velocity on each cell's + face (pitched, only the layer's faces used), in two
     // buffers: faces[1] holds the latest values between runs, as u[1] does.
     void *faces[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
@@ -621,6 +622,7 @@ int build(fdtd_solver *s, const fdtd_layout *L) {
     s->types_device = d_types;
     const float *d_scale = nullptr;
     if (s->scaled && (rc = upload(s, scale.data(), scale.size(), &d_scale))) return rc;
+    s->scale_device = d_scale;
 
     // The state, at rest; the error flag.
     for (int k = 0; k < 2; ++k) {
@@ -882,6 +884,7 @@ int download(fdtd_solver *s, const V *device, size_t count, std::vector<V> &host
 struct AdjointLists {
     std::vector<uint32_t> reader_start, reader_index, cells, starts, rows;
     std::vector<uint8_t> masks, types;  // each corrected cell's special axial neighbours; the sweep's types
+    std::vector<float> scales;          // with a speed field: each corrected cell's scale
     std::vector<uint32_t> special_read_start, corrected_read_start, read_probe;  // the probes' terms by cell
     std::vector<double> read_weight;
     // Each reader's and correction's coefficient as coef_inv[row] x base (row -1: the base alone),
@@ -893,10 +896,17 @@ struct AdjointLists {
 };
 
 // The lists from the handle's own device tables.
+//
+// With a speed field the interior update scales each row by its own cell's factor s_i, so the
+// operator is no longer symmetric: its transpose takes s_j of every reader j. The adjoint of an
+// interior cell is then carried as v = s lam, whose reverse step is the forward scaled sweep
+// itself: v_i = (2 - total s_i) V_i + s_i axial sum V_j - v+_i, V the level after. What reads or
+// feeds an interior cell's adjoint follows from that: a special row gathers axial x v_j from an
+// interior reader j (its coefficient a s_j times lam_j), and a corrected cell's terms from special
+// rows and probes enter times its own s. Special rows and branch states keep their plain adjoints.
 int adjoint_lists(fdtd_solver *s, AdjointLists &out) {
-    if (s->wide || s->scaled || s->layers)
-        return fail(s, FDTD_EINVAL,
-                    "the adjoint takes the 7-point stencil without a matched layer or a speed of sound per cell");
+    if (s->wide || s->layers)
+        return fail(s, FDTD_EINVAL, "the adjoint takes the 7-point stencil without a matched layer");
     const Tables &g = s->tables;
     const uint64_t K = s->specials;
     std::vector<uint32_t> special;
@@ -910,6 +920,8 @@ int adjoint_lists(fdtd_solver *s, AdjointLists &out) {
     if ((rc = download(s, g.coef_a, K, coef_a))) return rc;
     if ((rc = download(s, g.coef_inv, K, coef_inv))) return rc;
     if ((rc = download(s, s->types_device, s->n_device, types))) return rc;
+    std::vector<float> scale;
+    if (s->scaled && (rc = download(s, s->scale_device, s->n_device, scale))) return rc;
     const double axial = (double)s->bulk.axial;
     std::unordered_map<uint32_t, uint32_t> row_of;
     row_of.reserve(K * 2);
@@ -972,20 +984,22 @@ int adjoint_lists(fdtd_solver *s, AdjointLists &out) {
             if (row_of.count(cell) || types[cell] == kInterior) probed[cell].push_back({p, probe_weights[e]});
             if (types[cell] == kInterior) corrected[cell];
         }
-    auto read_terms = [&](uint32_t cell) {
+    auto read_terms = [&](uint32_t cell, double factor) {
         auto it = probed.find(cell);
         if (it != probed.end())
-            for (const auto &[p, w] : it->second) out.read_probe.push_back(p), out.read_weight.push_back(w);
+            for (const auto &[p, w] : it->second) out.read_probe.push_back(p), out.read_weight.push_back(w * factor);
         return (uint32_t)out.read_probe.size();
     };
     out.special_read_start.assign(1, 0);
-    for (uint64_t k = 0; k < K; ++k) out.special_read_start.push_back(read_terms(special[k]));
+    for (uint64_t k = 0; k < K; ++k) out.special_read_start.push_back(read_terms(special[k], 1.0));
     out.corrected_read_start.assign(1, out.special_read_start.back());
     out.starts.assign(1, 0);
     out.types = types;
     for (auto &[cell, list] : corrected) {
+        const double factor = s->scaled ? (double)scale[cell] : 1.0;
         out.cells.push_back(cell);
-        out.corrected_read_start.push_back(read_terms(cell));
+        if (s->scaled) out.scales.push_back(scale[cell]);
+        out.corrected_read_start.push_back(read_terms(cell, factor));
         out.types[cell] = kSpecial;  // left to correct_kernel
         uint8_t mask = 0;
         for (int d = 0; d < 6; ++d)
@@ -993,8 +1007,8 @@ int adjoint_lists(fdtd_solver *s, AdjointLists &out) {
         out.masks.push_back(mask);
         for (const auto &[r, base] : list) {
             out.rows.push_back(r);
-            out.corrected_base.push_back(base);
-            out.coefs.push_back((double)coef_inv[r] * base);
+            out.corrected_base.push_back(base * factor);
+            out.coefs.push_back((double)coef_inv[r] * (base * factor));
         }
         out.starts.push_back((uint32_t)out.rows.size());
     }
@@ -1028,6 +1042,7 @@ int place_adjoint(fdtd_solver *s, const AdjointLists &l, Pool &pool, AdjointStat
     t.coef_b = g.coef_b, t.coef_inv = g.coef_inv;
     t.axial = s->bulk.axial;
     t.centre = s->bulk.centre;
+    t.total = s->bulk.total;
     for (int d = 0; d < 6; ++d) t.offset[d] = g.offset[d];
     t.corrected = (uint32_t)l.cells.size();
     int rc;
@@ -1039,6 +1054,7 @@ int place_adjoint(fdtd_solver *s, const AdjointLists &l, Pool &pool, AdjointStat
     if ((rc = place(s, pool, l.starts, &t.corrected_start))) return rc;
     if ((rc = place(s, pool, l.rows, &t.corrected_row))) return rc;
     if ((rc = place(s, pool, l.masks, &t.corrected_mask))) return rc;
+    if ((rc = place(s, pool, l.scales, &t.corrected_scale))) return rc;
     const uint8_t *sweep_types;
     if ((rc = place(s, pool, l.types, &sweep_types))) return rc;
     if ((rc = place(s, pool, l.coefs, &t.corrected_coef))) return rc;
@@ -1214,7 +1230,7 @@ int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float
     const uint32_t row_blocks = (uint32_t)((std::max<uint64_t>(std::max<uint64_t>(K, S), 1) + kBlock - 1) / kBlock);
     const uint32_t special_blocks = (uint32_t)((K + kBlock - 1) / kBlock);
     const uint32_t corrected_blocks = (uint32_t)((t.corrected + kBlock - 1) / kBlock);
-    const uint32_t smem = Stage<T, false>::smem;
+    const uint32_t smem = s->scaled ? Stage<T, true>::smem : Stage<T, false>::smem;
     int x = 0;  // lam[x], om[x]: level n+1; lam[1-x], om[1-x]: level n+2, then level n
     // A segment's recomputation (the dispatch of its steps, recording the special rows), and its
     // reverse steps.
@@ -1243,10 +1259,15 @@ int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float
                     g[2], g[3], g[4], tilde_out, seg_dloss, segment, m);
             CUDA_TRY(s, cudaEventRecord(s->joined[1], s->side));
             if (s->bulk_blocks) {
+                // (With a speed field the sweep steps v = s lam: the forward scaled sweep.)
                 BulkArgs args = s->bulk;
                 args.a = lam_out;
-                bulk_kernel<T, false, false><<<s->bulk_blocks, kBlock, smem, s->stream>>>(adj.lam_b[xx], adj.lam_a[1 - xx],
-                                                                                        adj.map_t, s->map_s, args);
+                if (s->scaled)
+                    bulk_kernel<T, false, true><<<s->bulk_blocks, kBlock, smem, s->stream>>>(
+                        adj.lam_b[xx], adj.lam_a[1 - xx], adj.map_t, s->map_s, args);
+                else
+                    bulk_kernel<T, false, false><<<s->bulk_blocks, kBlock, smem, s->stream>>>(
+                        adj.lam_b[xx], adj.lam_a[1 - xx], adj.map_t, s->map_s, args);
             }
             CUDA_TRY(s, cudaStreamWaitEvent(s->stream, s->joined[1], 0));
             xx = 1 - xx;
@@ -1387,7 +1408,7 @@ size_t pool_bytes(const fdtd_solver *s, const AdjointLists &l, uint64_t steps, u
     list(l.reader_start.size(), 4), list(l.reader_index.size(), 4), list(l.reader_kind.size(), 1);
     list(l.reader_coef.size(), 8), list(l.cells.size(), 4), list(l.starts.size(), 4), list(l.rows.size(), 4);
     list(l.coefs.size(), 8), list(l.special_read_start.size(), 4), list(l.corrected_read_start.size(), 4);
-    list(l.masks.size(), 1), list(l.types.size(), 1);
+    list(l.masks.size(), 1), list(l.scales.size(), 4), list(l.types.size(), 1);
     list(l.read_probe.size(), 4), list(l.read_weight.size(), 8);
     total += 2 * (pool_round(e * n) + pool_round(e * S)) + 2 * pool_round(e * K);
     if (segment == 0 || segment > steps) segment = steps;

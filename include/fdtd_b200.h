@@ -178,8 +178,8 @@ int fdtd_get_timing(fdtd_solver *solver, double ms[4], uint64_t *steps);
  * over the run in double; any output may be NULL. The forward pass is recomputed in segments of
  * `segment` steps from checkpoints of the whole state kept at each segment's start (0: one
  * segment), recording each step's values at the special rows; the adjoint then steps back
- * through each segment. Grids of the 7-point stencil without a matched layer or a speed field
- * only (FDTD_EINVAL otherwise). The solver is left at rest.
+ * through each segment. Grids of the 7-point stencil without a matched layer (a speed field or
+ * none) only (FDTD_EINVAL otherwise). The solver is left at rest.
  */
 int fdtd_gradient(fdtd_solver *solver, const float *signal, uint64_t steps, const double *dloss_dy,
                   uint64_t segment, double *grad_coef_b, double *grad_coef_inv, double *grad_now,
