@@ -10,7 +10,7 @@ gradient with respect to the parameters comes from torch's own chain rule.
 
 The coefficients are float32 in the layout (the reference's type); the values given are rounded to
 float32 before the run, and the gradient returned is the gradient at those rounded values. Grids of
-the 7-point stencil without a matched layer, with or without a speed field.
+either stencil without a matched layer, with or without a speed field.
 """
 
 from __future__ import annotations

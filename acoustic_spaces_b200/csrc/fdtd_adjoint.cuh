@@ -1,13 +1,14 @@
 // Device code of the reverse-time (adjoint) stepper: the gradient of a loss of the probes'
-// series with respect to the special rows' coefficients, for grids of the 7-point stencil without
-// a matched layer (with or without a speed field).
+// series with respect to the special rows' coefficients, for grids without a matched layer (either
+// stencil, with or without a speed field).
 //
 // A forward step maps the levels (u_n, u_{n-1}) and branch velocities (w_n, w_{n-1}) to u_{n+1},
 // w_{n+1}: z_{n+1} = G z_n - H z_{n-1} (+ the source), z = (u, w). For a special row (cell i,
 // states j; fdtd.hpp:860-881):
 //   x = ca u_n[i] + sum_l wl u_n[i + o_l] - cb u_{n-1}[i] - sum_j W_j (now_j w_n[j] - before_j w_{n-1}[j]) + src s
 //   u_{n+1}[i] = ci x,   w_{n+1}[j] = w_{n-1}[j] + gain_j (u_{n+1}[i] - u_{n-1}[i]) + now_j w_n[j] - before_j w_{n-1}[j]
-// and interior cells have G = centre on the diagonal and axial to each neighbour, H = 1.
+// and interior cells have G = centre on the diagonal, axial to each face neighbour and (19 points)
+// diagonal to each edge neighbour, H = 1.
 // The adjoint z~_n = dL/dz_n obeys z~_n = G^T z~_{n+1} - H^T z~_{n+2} + P_n (P_n the probes'
 // terms), a leapfrog run backwards in time with the transposed operator. With a row's effective
 // adjoint L~ = lam[i] + sum_j gain_j om[j] (lam, om: the adjoints of u and w):
@@ -44,16 +45,17 @@ struct AdjointTables {
     const uint8_t *reader_kind;
     const double *reader_coef;
     // Interior cells that special rows read: corrected_start .. per cell, entries (special row,
-    // its coefficient on the cell), and which of the cell's six axial neighbours are special rows
-    // (bit d, in the order of the stencil's directions). The adjoint sweep leaves these cells to
-    // correct_kernel.
+    // its coefficient on the cell), and which of the cell's neighbours (6, or 18 with the wide
+    // stencil) are special rows (bit d, in the order of the stencil's directions). The adjoint
+    // sweep leaves these cells to correct_kernel.
     uint32_t corrected;
     const uint32_t *corrected_cell, *corrected_start, *corrected_row;
-    const uint8_t *corrected_mask;
+    const uint32_t *corrected_mask;
     const double *corrected_coef;
     const float *corrected_scale;  // with a speed field: each corrected cell's scale (else null)
-    float axial, centre, total;
-    int32_t offset[6];
+    float axial, diagonal, centre, total;
+    uint32_t wide;  // 1: the 19-point stencil
+    int32_t offset[18];
     // The probes' terms dL/dy_p x weight on the cells they read, by cell: a special row's at
     // special_read_start[k] .. [k + 1], a corrected cell's at corrected_read_start[c] .. [c + 1], of
     // (read_probe, read_weight). (Probes read no other cells that the adjoint carries: a solid
@@ -82,7 +84,7 @@ __device__ __forceinline__ double probe_terms(const AdjointTables &t, uint32_t b
 }
 
 // An interior cell that special rows read, or that probes read, whole: the transposed stencil of
-// their interior (and solid) axial neighbours, as the sweep forms it, plus each reading row's
+// its interior (and solid) neighbours, as the sweep forms it, plus each reading row's
 // coefficient times its L~, minus the level two steps on (lam_out holds it on entry), plus the
 // probes' terms of step n. The sweep leaves these cells alone.
 template <typename T>
@@ -91,17 +93,23 @@ __device__ __forceinline__ void correct_cell(const AdjointTables &t, uint32_t c,
     if (c >= t.corrected) return;
     const uint32_t cell = t.corrected_cell[c];
     const uint32_t special = t.corrected_mask[c];
-    T sum = 0;
+    T sum = 0, edges = 0;
 #pragma unroll
     for (int d = 0; d < 6; ++d)
         if (!(special & (1u << d))) sum += lam_next[(uint32_t)((int64_t)cell + t.offset[d])];
-    T centre = (T)t.centre, axial = (T)t.axial;
+    if (t.wide) {
+#pragma unroll
+        for (int d = 6; d < 18; ++d)
+            if (!(special & (1u << d))) edges += lam_next[(uint32_t)((int64_t)cell + t.offset[d])];
+    }
+    T centre = (T)t.centre, axial = (T)t.axial, diagonal = (T)t.diagonal;
     if (t.corrected_scale) {  // as the forward scaled sweep forms its cells
         const T sc = (T)t.corrected_scale[c];
         centre = (T)2 - (T)t.total * sc;
         axial = sc * (T)t.axial;
+        diagonal = sc * (T)t.diagonal;
     }
-    T value = centre * lam_next[cell] + axial * sum - lam_out[cell];
+    T value = centre * lam_next[cell] + axial * sum + diagonal * edges - lam_out[cell];
     for (uint32_t e = t.corrected_start[c], end = t.corrected_start[c + 1]; e < end; ++e)
         value += (T)t.corrected_coef[e] * tilde[t.corrected_row[e]];
     const double probed = probe_terms(t, t.corrected_read_start[c], t.corrected_read_start[c + 1], dloss, stride, step);

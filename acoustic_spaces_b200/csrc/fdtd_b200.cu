@@ -883,7 +883,8 @@ int download(fdtd_solver *s, const V *device, size_t count, std::vector<V> &host
 // and the interior cells next to special rows with their corrections.
 struct AdjointLists {
     std::vector<uint32_t> reader_start, reader_index, cells, starts, rows;
-    std::vector<uint8_t> masks, types;  // each corrected cell's special axial neighbours; the sweep's types
+    std::vector<uint32_t> masks;        // each corrected cell's special neighbours (bit d: direction d)
+    std::vector<uint8_t> types;         // the sweep's cell types
     std::vector<float> scales;          // with a speed field: each corrected cell's scale
     std::vector<uint32_t> special_read_start, corrected_read_start, read_probe;  // the probes' terms by cell
     std::vector<double> read_weight;
@@ -904,9 +905,10 @@ struct AdjointLists {
 // feeds an interior cell's adjoint follows from that: a special row gathers axial x v_j from an
 // interior reader j (its coefficient a s_j times lam_j), and a corrected cell's terms from special
 // rows and probes enter times its own s. Special rows and branch states keep their plain adjoints.
+// The 19-point operator is symmetric as the 7-point one is: its readers and corrections reach the
+// twelve edge neighbours too, with the diagonal weight.
 int adjoint_lists(fdtd_solver *s, AdjointLists &out) {
-    if (s->wide || s->layers)
-        return fail(s, FDTD_EINVAL, "the adjoint takes the 7-point stencil without a matched layer");
+    if (s->layers) return fail(s, FDTD_EINVAL, "the adjoint takes grids without a matched layer");
     const Tables &g = s->tables;
     const uint64_t K = s->specials;
     std::vector<uint32_t> special;
@@ -922,7 +924,17 @@ int adjoint_lists(fdtd_solver *s, AdjointLists &out) {
     if ((rc = download(s, s->types_device, s->n_device, types))) return rc;
     std::vector<float> scale;
     if (s->scaled && (rc = download(s, s->scale_device, s->n_device, scale))) return rc;
-    const double axial = (double)s->bulk.axial;
+    const double axial = (double)s->bulk.axial, diagonal = (double)s->bulk.diagonal;
+    const int directions = s->wide ? 18 : 6;
+    // The pitched cell one step from cell i along direction d, if it lies in the grid.
+    auto neighbour = [&](uint32_t i, int d, uint32_t *j) {
+        const int64_t x = (int64_t)(i % s->pitch) + kSteps[d][0];
+        const int64_t y = (int64_t)((i / s->pitch) % s->ny) + kSteps[d][1];
+        const int64_t z = (int64_t)(i / (s->pitch * s->ny)) + kSteps[d][2];
+        if (x < 0 || y < 0 || z < 0 || x >= (int64_t)s->nx || y >= (int64_t)s->ny || z >= (int64_t)s->nz) return false;
+        *j = (uint32_t)((int64_t)i + g.offset[d]);
+        return true;
+    };
     std::unordered_map<uint32_t, uint32_t> row_of;
     row_of.reserve(K * 2);
     for (uint64_t k = 0; k < K; ++k) row_of[special[k]] = (uint32_t)k;
@@ -939,10 +951,10 @@ int adjoint_lists(fdtd_solver *s, AdjointLists &out) {
     for (uint64_t k = 0; k < K; ++k) {
         const uint32_t i = special[k];
         readers[k].push_back({kind_bit | k, (int32_t)k, (double)coef_a[k]});
-        for (int d = 0; d < 6; ++d) {
-            const uint32_t j = (uint32_t)((int64_t)i + g.offset[d]);
-            if (types[j] == kInterior) {
-                readers[k].push_back({j, -1, axial});
+        for (int d = 0; d < directions; ++d) {
+            uint32_t j;
+            if (neighbour(i, d, &j) && types[j] == kInterior) {
+                readers[k].push_back({j, -1, d < 6 ? axial : diagonal});
                 corrected[j];  // an interior cell next to a special row: formed by correct_kernel
             }
         }
@@ -1001,9 +1013,9 @@ int adjoint_lists(fdtd_solver *s, AdjointLists &out) {
         if (s->scaled) out.scales.push_back(scale[cell]);
         out.corrected_read_start.push_back(read_terms(cell, factor));
         out.types[cell] = kSpecial;  // left to correct_kernel
-        uint8_t mask = 0;
-        for (int d = 0; d < 6; ++d)
-            if (row_of.count((uint32_t)((int64_t)cell + g.offset[d]))) mask |= (uint8_t)(1u << d);
+        uint32_t mask = 0;  // (an interior cell's neighbours all lie in the grid)
+        for (int d = 0; d < directions; ++d)
+            if (row_of.count((uint32_t)((int64_t)cell + g.offset[d]))) mask |= 1u << d;
         out.masks.push_back(mask);
         for (const auto &[r, base] : list) {
             out.rows.push_back(r);
@@ -1043,7 +1055,9 @@ int place_adjoint(fdtd_solver *s, const AdjointLists &l, Pool &pool, AdjointStat
     t.axial = s->bulk.axial;
     t.centre = s->bulk.centre;
     t.total = s->bulk.total;
-    for (int d = 0; d < 6; ++d) t.offset[d] = g.offset[d];
+    t.diagonal = s->wide ? s->bulk.diagonal : 0.0f;
+    t.wide = s->wide ? 1 : 0;
+    for (int d = 0; d < 18; ++d) t.offset[d] = g.offset[d];
     t.corrected = (uint32_t)l.cells.size();
     int rc;
     if ((rc = place(s, pool, l.reader_start, &t.reader_start))) return rc;
@@ -1259,15 +1273,18 @@ int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float
                     g[2], g[3], g[4], tilde_out, seg_dloss, segment, m);
             CUDA_TRY(s, cudaEventRecord(s->joined[1], s->side));
             if (s->bulk_blocks) {
-                // (With a speed field the sweep steps v = s lam: the forward scaled sweep.)
+                // The forward sweep of the grid's own kind (with a speed field it steps v = s lam).
                 BulkArgs args = s->bulk;
                 args.a = lam_out;
-                if (s->scaled)
-                    bulk_kernel<T, false, true><<<s->bulk_blocks, kBlock, smem, s->stream>>>(
-                        adj.lam_b[xx], adj.lam_a[1 - xx], adj.map_t, s->map_s, args);
+                const CUtensorMap &mb = adj.lam_b[xx], &ma = adj.lam_a[1 - xx];
+                if (s->wide && s->scaled)
+                    bulk_kernel<T, true, true><<<s->bulk_blocks, kBlock, smem, s->stream>>>(mb, ma, adj.map_t, s->map_s, args);
+                else if (s->wide)
+                    bulk_kernel<T, true, false><<<s->bulk_blocks, kBlock, smem, s->stream>>>(mb, ma, adj.map_t, s->map_s, args);
+                else if (s->scaled)
+                    bulk_kernel<T, false, true><<<s->bulk_blocks, kBlock, smem, s->stream>>>(mb, ma, adj.map_t, s->map_s, args);
                 else
-                    bulk_kernel<T, false, false><<<s->bulk_blocks, kBlock, smem, s->stream>>>(
-                        adj.lam_b[xx], adj.lam_a[1 - xx], adj.map_t, s->map_s, args);
+                    bulk_kernel<T, false, false><<<s->bulk_blocks, kBlock, smem, s->stream>>>(mb, ma, adj.map_t, s->map_s, args);
             }
             CUDA_TRY(s, cudaStreamWaitEvent(s->stream, s->joined[1], 0));
             xx = 1 - xx;
@@ -1408,7 +1425,7 @@ size_t pool_bytes(const fdtd_solver *s, const AdjointLists &l, uint64_t steps, u
     list(l.reader_start.size(), 4), list(l.reader_index.size(), 4), list(l.reader_kind.size(), 1);
     list(l.reader_coef.size(), 8), list(l.cells.size(), 4), list(l.starts.size(), 4), list(l.rows.size(), 4);
     list(l.coefs.size(), 8), list(l.special_read_start.size(), 4), list(l.corrected_read_start.size(), 4);
-    list(l.masks.size(), 1), list(l.scales.size(), 4), list(l.types.size(), 1);
+    list(l.masks.size(), 4), list(l.scales.size(), 4), list(l.types.size(), 1);
     list(l.read_probe.size(), 4), list(l.read_weight.size(), 8);
     total += 2 * (pool_round(e * n) + pool_round(e * S)) + 2 * pool_round(e * K);
     if (segment == 0 || segment > steps) segment = steps;

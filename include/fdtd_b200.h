@@ -178,7 +178,7 @@ int fdtd_get_timing(fdtd_solver *solver, double ms[4], uint64_t *steps);
  * over the run in double; any output may be NULL. The forward pass is recomputed in segments of
  * `segment` steps from checkpoints of the whole state kept at each segment's start (0: one
  * segment), recording each step's values at the special rows; the adjoint then steps back
- * through each segment. Grids of the 7-point stencil without a matched layer (a speed field or
+ * through each segment. Grids without a matched layer (either stencil, a speed field or
  * none) only (FDTD_EINVAL otherwise). The solver is left at rest.
  */
 int fdtd_gradient(fdtd_solver *solver, const float *signal, uint64_t steps, const double *dloss_dy,

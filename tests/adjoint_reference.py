@@ -10,8 +10,8 @@ grid's, squared, as fdtd.hpp:250-262 scales it). With a matched layer it also st
 the reference does (fdtd.hpp:2242-2264: each cell its own copy of both faces on every axis; with a
 speed field each cell's push scaled by its own factor) and gives the gradient in the layer's
 twelve coefficient tables (keep and push of the centres and the faces per axis,
-fdtd.hpp:2219-2238). The CUDA adjoint covers the 7-point stencil without a speed field or a
-matched layer so far; the rest of this checker is the bar for what comes next.
+fdtd.hpp:2219-2238). The CUDA adjoint covers grids without a matched layer so far; the layer's
+part of this checker is the bar for what comes next.
 """
 
 from __future__ import annotations

@@ -54,8 +54,12 @@ def _assert_equal_gradients(ours, checker, rtol):
         np.testing.assert_allclose(ours[key], checker[key], rtol=0, atol=rtol * scale, err_msg=key)
 
 
-# (speed7, uniform099: a speed field, whose interior adjoint the sweep carries as s lam)
-@pytest.mark.parametrize("name", ["resonant7", "drive7", "fitted_closed", "speed7", "uniform099"])
+# (speed7, uniform099, speed19: a speed field, whose interior adjoint the sweep carries as s lam;
+# resonant19, speed19: the 19-point stencil)
+_GRIDS = ["resonant7", "drive7", "fitted_closed", "speed7", "uniform099", "resonant19", "speed19"]
+
+
+@pytest.mark.parametrize("name", _GRIDS)
 def test_fp64_gradient_is_the_autograd_gradient(name):
     layout, signal, _ = load_golden(name)
     signal = signal[:300]
@@ -63,7 +67,7 @@ def test_fp64_gradient_is_the_autograd_gradient(name):
     _assert_equal_gradients(_gradient(layout, signal, target, "fp64"), checker, 1e-9)
 
 
-@pytest.mark.parametrize("name", ["resonant7", "drive7", "fitted_closed", "speed7", "uniform099"])
+@pytest.mark.parametrize("name", _GRIDS)
 def test_fp32_gradient_matches_the_autograd_gradient(name):
     layout, signal, _ = load_golden(name)
     signal = signal[:300]
