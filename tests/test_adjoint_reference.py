@@ -264,3 +264,38 @@ def test_a_speed_fields_reverse_step_is_its_forward_sweep_on_scaled_adjoints(ste
     v = scale * lam
     swept = update(scale * Lam, scale) * interior
     np.testing.assert_allclose(v, swept, rtol=1e-12, atol=1e-12)
+
+
+@pytest.mark.parametrize(
+    "name", ["resonant7", "drive7", "fitted_closed", "speed19", "uniform099", "open_layer", "fitted_open", "open_layer_speed"]
+)
+def test_the_adjoint_decomposition_gives_the_autograd_gradient(name):
+    # The CUDA adjoint's decomposition by kind of cell (tests/adjoint_decomposition.py: the sweep,
+    # corrected cells, special rows, and the matched layer's part to come) against autograd, which
+    # differentiates the forward scheme whole.
+    import adjoint_decomposition
+
+    layout, signal, _ = load_golden(name)
+    signal = signal[:150]
+    y, target = _misfit(layout, signal)
+    ours = adjoint_decomposition.gradient(layout, signal, 2.0 * (y - target))
+    checker = adjoint_reference.gradient(layout, signal, 2.0 * (y - target))
+    for key, value in ours.items():
+        scale = np.abs(checker[key]).max() if checker[key].size else 0.0
+        np.testing.assert_allclose(value, checker[key], rtol=0, atol=1e-12 * scale, err_msg=key)
+
+
+@pytest.mark.parametrize("name", ["fitted_open", "open_layer_speed"])
+def test_the_adjoint_decomposition_gives_the_layer_tables_gradient(name):
+    # The twelve tables' gradient from the layer's adjoints of each step's new states and the
+    # states before and after it, against autograd (with a speed field, each cell's push scaled).
+    import adjoint_decomposition
+
+    layout, signal, _ = load_golden(name)
+    signal = signal[:60]
+    y, target = _misfit(layout, signal)
+    ours = adjoint_decomposition.gradient(layout, signal, 2.0 * (y - target), tables=True)
+    checker = adjoint_reference.gradient(layout, signal, 2.0 * (y - target))
+    assert set(_TABLES) <= set(ours)
+    for key in _TABLES:
+        np.testing.assert_allclose(ours[key], checker[key], rtol=0, atol=1e-12 * np.abs(checker[key]).max(), err_msg=key)
