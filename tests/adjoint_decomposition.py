@@ -100,7 +100,8 @@ def gradient(layout, signal, dloss_dy, tables: bool = False) -> dict[str, np.nda
             new[inner] = centre * b[inner] + a * faces + dg * edges - prev[inner]
         own = now * wb - before * wa
         links = np.bincount(link_row, link_w * b[link_cell], K)
-        rows = (ca * b[special] + links - cb * prev[special] - np.bincount(state_row, sw * own, K) + src * signal[m]) * ci
+        flow = np.bincount(state_row, sw * own, K)
+        rows = (ca * b[special] + links - cb * prev[special] - flow + src * signal[m]) * ci
         new[special] = rows
         w[m + 2] = wa + (rows - prev[special])[state_row] * gain + own
         if C:
@@ -218,7 +219,8 @@ def gradient(layout, signal, dloss_dy, tables: bool = False) -> dict[str, np.nda
             for o in off[:6]:
                 j = layer + o
                 own += np.where(interior[j], a * lam_next[j], 0.0)
-            np.add.at(from_rows, link_cell[to_layer], link_w[to_layer] * ci[link_row[to_layer]] * til[link_row[to_layer]])
+            by = link_row[to_layer]
+            np.add.at(from_rows, link_cell[to_layer], link_w[to_layer] * ci[by] * til[by])
             out[layer] = own + from_rows[layer] + terms[layer] + probed[layer]
         # special rows and their branch states
         gathered = np.bincount(r_row, r_coef * np.where(r_kind, til[np.minimum(r_idx, K - 1)] if K else 0.0,

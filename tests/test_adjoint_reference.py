@@ -28,7 +28,10 @@ def _misfit(layout, signal, seed=0):
     return base, target
 
 
-@pytest.mark.parametrize("name", ["resonant7", "drive7", "fitted_closed", "resonant19", "speed7", "speed19", "uniform099"])
+_PLAIN_KINDS = ["resonant7", "drive7", "fitted_closed", "resonant19", "speed7", "speed19", "uniform099"]
+
+
+@pytest.mark.parametrize("name", _PLAIN_KINDS)
 def test_the_autograd_stepper_steps_as_the_oracle(name):
     layout, signal, _ = load_golden(name)
     ours = adjoint_reference.series(layout, signal[:200])
@@ -267,8 +270,9 @@ def test_a_speed_fields_reverse_step_is_its_forward_sweep_on_scaled_adjoints(ste
 
 
 @pytest.mark.parametrize(
-    "name", ["resonant7", "drive7", "fitted_closed", "speed19", "uniform099", "open_layer", "fitted_open", "open_layer_speed"]
-)
+    "name", ["resonant7", "drive7", "fitted_closed", "speed19", "uniform099", "open_layer", "fitted_open",
+             "open_layer_speed"],
+)  # fmt: skip
 def test_the_adjoint_decomposition_gives_the_autograd_gradient(name):
     # The CUDA adjoint's decomposition by kind of cell (tests/adjoint_decomposition.py: the sweep,
     # corrected cells, special rows, and the matched layer's part to come) against autograd, which
@@ -298,4 +302,5 @@ def test_the_adjoint_decomposition_gives_the_layer_tables_gradient(name):
     checker = adjoint_reference.gradient(layout, signal, 2.0 * (y - target))
     assert set(_TABLES) <= set(ours)
     for key in _TABLES:
-        np.testing.assert_allclose(ours[key], checker[key], rtol=0, atol=1e-12 * np.abs(checker[key]).max(), err_msg=key)
+        scale = np.abs(checker[key]).max()
+        np.testing.assert_allclose(ours[key], checker[key], rtol=0, atol=1e-12 * scale, err_msg=key)
