@@ -70,3 +70,17 @@ def test_the_reference_arm_prints_the_contracts_line():
     cpu = line["cpu_baseline"]
     assert cpu["kind"] == "reference" and cpu["cores"] >= 1 and cpu["value"] == line["value"] and cpu["sample"]
     assert line["e2e"] == {"value": line["value"], "unit": line["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+
+
+def test_the_reference_arm_leaves_the_other_ranks_idle():
+    # Under torchrun every rank but 0 exits at once, with nothing printed and no process group.
+    import os
+    import subprocess
+    import sys
+
+    from conftest import ROOT
+
+    env = dict(os.environ, RANK="1", LOCAL_RANK="1", WORLD_SIZE="2", MASTER_ADDR="127.0.0.1", MASTER_PORT="1")
+    done = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--gpus", "2"],
+                          capture_output=True, text=True, timeout=120, env=env)  # fmt: skip
+    assert done.returncode == 0 and done.stdout.strip() == ""
