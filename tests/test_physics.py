@@ -1,5 +1,5 @@
 """Known answers of the scheme itself, independent of the reference's code: room modes, the
-scheme's own dispersion, a wall's reflection, the stability margin of the update's constants, what
+scheme's own dispersion (both stencils), a wall's reflection, the stability margin of the update's constants, what
 the matched layer takes out of a pulse, and a speed field of ones.
 
 On the oracle (CPU) and, where marked, on the B200: both step the builder's layouts, so the answers
@@ -95,6 +95,40 @@ def test_a_tubes_modes_sit_at_the_schemes_own_frequencies():
         scheme = rate / math.pi * math.asin(math.sqrt(a) * math.sin(math.pi * m * h / (2 * size[0])))
         assert _peak(response, rate, scheme, 0.3 * spacing) == pytest.approx(scheme, rel=1e-6), per_wavelength
         assert 0.002 < 1 - scheme / (m * spacing) < 0.01
+
+
+def test_the_19_point_stencils_tube_modes_sit_at_its_own_frequencies():
+    # The same rigid 6 m tube laid out by the reference itself (a box of twelve triangles) with the
+    # 19-point stencil, stepped by the FP64 oracle: a plane wave along an axis sees
+    # sin(w dt / 2) = sqrt(a + 4 d) sin(k h / 2), a and d the layout's face and edge weights (the
+    # faces across the wave add 4 a and its edges 8 d cos(k h) + 4 d), so each axial mode sits there
+    # to 1e-6 (measured: 3e-9), in cycles a step; the 7-point layout of the same tube, likewise
+    # with d = 0.
+    from oracle.oracle import reference_native
+
+    native = reference_native()
+    if native is None:
+        pytest.skip("the reference's solver is not built")
+    size, h = np.array([6.0, 0.4, 0.4]), 0.1
+    grid = L.room_grid(size, h)
+    corners = np.array([[x, y, z] for z in (0, size[2]) for y in (0, size[1]) for x in (0, size[0])], float)
+    quads = [(0, 2, 3, 1), (4, 5, 7, 6), (0, 1, 5, 4), (2, 6, 7, 3), (0, 4, 6, 2), (1, 3, 7, 5)]
+    triangles = np.array([t for a, b, c, d in quads for t in ([a, b, c], [a, c, d])], np.int64)
+    for stencil in (7, 19):
+        solver = native.WaveSolver(
+            native.Bvh(corners, triangles), np.zeros(12, np.int64), np.array([0.0]), np.zeros((0, 3)),
+            np.zeros(0, np.int64), grid.origin, grid.cell, *grid.shape, np.array([0.27, 0.2, 0.2]),
+            np.array([[5.73, 0.2, 0.2]]), threads=2, stencil=stencil,
+        )  # fmt: skip
+        layout = solver.layout()
+        w = np.asarray(layout["weights"], np.float64)
+        a, d = float(w[0]), (float(w[6]) if stencil == 19 else 0.0)
+        response = OracleSolver(layout, "fp64").run(L.ricker_drive(1.0, 20000, sigma_s=1.2))[0]
+        for per_wavelength in (20, 16, 12):
+            m = round(2 * size[0] / (per_wavelength * h))
+            scheme = math.asin(math.sqrt(a + 4 * d) * math.sin(math.pi * m * h / (2 * size[0]))) / math.pi
+            got = _peak(response, 1.0, scheme, 0.3 * scheme / m)
+            assert got == pytest.approx(scheme, rel=1e-6), (stencil, per_wavelength)
 
 
 # ---- a wall's reflection -----------------------------------------------------------------------
