@@ -16,7 +16,6 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
-#include <mutex>
 #include <new>
 #include <string>
 
@@ -1159,6 +1158,14 @@ struct Kept {
     }
 };
 
+// Whether the handle holds the tape of a run of this drive with these segments: gradient<T> then
+// takes the tape's checkpoints or trajectory and recomputes no forward pass of its own.
+bool holds_tape(const fdtd_solver *s, const float *signal, uint64_t steps, uint64_t segment) {
+    if (segment == 0 || segment > steps) segment = steps;
+    return s->tape_valid && s->tape_signal.size() == steps && std::min<uint64_t>(s->tape_segment, steps) == segment &&
+           std::memcmp(s->tape_signal.data(), signal, sizeof(float) * steps) == 0;
+}
+
 // The gradient (fdtd_gradient) with the adjoint state `adj` and scratch from `scratch`
 // (scratch.take(bytes, &p): device memory cleared to 0 in order on the handle's stream).
 template <typename T, class Pool>
@@ -1218,9 +1225,7 @@ int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float
     };
     // The forward pass from rest, keeping checkpoints[m] = the state at the start of segment m+1;
     // or, when the handle holds the tape of a run of this drive with these segments, its states.
-    const bool taped = s->tape_valid && s->tape_signal.size() == steps &&
-                       std::min<uint64_t>(s->tape_segment, steps) == segment &&
-                       std::memcmp(s->tape_signal.data(), signal, sizeof(float) * steps) == 0;
+    const bool taped = holds_tape(s, signal, steps, segment);
     const bool trajectory = taped && s->tape_traj;  // the tape holds every level: nothing to recompute
     std::vector<char *> checkpoints;
     if (taped && !trajectory)
@@ -1379,22 +1384,16 @@ static __device__ __align__(256) unsigned char g_gradient_pool[kPoolBytes];
 
 constexpr size_t pool_round(size_t bytes) { return ((bytes ? bytes : 16) + kPoolAlign - 1) / kPoolAlign * kPoolAlign; }
 
-// The pool's address on each device, looked up once per device with that device current.
-constexpr int kPoolDevices = 64;
-std::mutex g_pool_mutex;
-void *g_pool_address[kPoolDevices] = {};
-
+// The pool's address on the current device. Looked up on every call, not cached: the address
+// belongs to the context that loaded the module, and a caller that destroys and recreates the
+// device's primary context (cudaDeviceReset) gets the module loaded again, possibly elsewhere.
+// Once the module is loaded the lookup is a table read.
 int pool_address(fdtd_solver *s, void **out) {
     *out = nullptr;
-    if (s->device < 0 || s->device >= kPoolDevices) return fail(s, FDTD_EINVAL, "the static pool serves devices 0 to 63");
-    std::lock_guard<std::mutex> lock(g_pool_mutex);
-    if (!g_pool_address[s->device]) {
-        void *p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_gradient_pool);
-        if (e != cudaSuccess) return cuda_fail(s, e, "cudaGetSymbolAddress of the gradient's static pool");
-        g_pool_address[s->device] = p;
-    }
-    *out = g_pool_address[s->device];
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_gradient_pool);
+    if (e != cudaSuccess) return cuda_fail(s, e, "cudaGetSymbolAddress of the gradient's static pool");
+    *out = p;
     return FDTD_OK;
 }
 
@@ -1416,8 +1415,9 @@ struct StaticPool {
     int take(size_t bytes, void **out) { return take(bytes, out, true); }  // gradient<T>'s scratch
 };
 
-// The pool's bytes for one gradient: the blocks place_adjoint and then gradient<T> take, in order.
-size_t pool_bytes(const fdtd_solver *s, const AdjointLists &l, uint64_t steps, uint64_t segment) {
+// The pool's bytes for one gradient: the blocks place_adjoint and then gradient<T> take, in order
+// (the checkpoints only where no tape supplies the segments' states).
+size_t pool_bytes(const fdtd_solver *s, const AdjointLists &l, uint64_t steps, uint64_t segment, bool taped) {
     const size_t e = s->precision == FDTD_FP64 ? 8 : 4;
     const uint64_t K = s->specials, S = s->states, P = std::max<uint64_t>(1, s->probes), n = s->n_device;
     size_t total = 0;
@@ -1434,7 +1434,7 @@ size_t pool_bytes(const fdtd_solver *s, const AdjointLists &l, uint64_t steps, u
              pool_round(e * S * (segment + 2)) + pool_round(8 * P * segment) + pool_round(4 * segment) +
              pool_round(8 * P * segment);
     total += 2 * pool_round(8 * K) + 3 * pool_round(8 * S);
-    total += (segments - 1) * pool_round(2 * e * n + 2 * e * S);
+    if (!taped) total += (segments - 1) * pool_round(2 * e * n + 2 * e * S);
     return total;
 }
 
@@ -1728,7 +1728,7 @@ int fdtd_gradient_noalloc(fdtd_solver *s, const float *signal, uint64_t steps, c
     if ((rc = pool_address(s, &base)) != FDTD_OK) return rc;
     AdjointLists lists;
     if ((rc = adjoint_lists(s, lists)) != FDTD_OK) return rc;
-    const size_t need = pool_bytes(s, lists, steps, segment);
+    const size_t need = pool_bytes(s, lists, steps, segment, holds_tape(s, signal, steps, segment));
     if (need > kPoolBytes) {
         char message[200];
         std::snprintf(message, sizeof message,

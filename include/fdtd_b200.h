@@ -261,9 +261,11 @@ int fdtd_set_coefficients(fdtd_solver *solver, const float *coef_b, const float 
  * kernels), and a process whose device memory belongs to a caching allocator (PyTorch's) may have
  * none left to give. A run whose buffers do not fit the pool is refused with FDTD_EINVAL before any
  * device work, the message giving the bytes it needs (take fewer steps, a longer `segment`, or
- * fdtd_gradient). The first call on a device looks up the pool's device address
- * (cudaGetSymbolAddress) with that device current; make that first call before any stream capture
- * on the device. There is one pool per device, shared by every handle and kept between calls:
+ * fdtd_gradient). Every call looks up the pool's device address (cudaGetSymbolAddress) with the
+ * handle's device current, so a context destroyed and made again (cudaDeviceReset) leaves no stale
+ * address behind; make the first call on a device before any stream capture on it, since that
+ * lookup loads the library's device code there. A tape kept by fdtd_set_tape supplies the
+ * checkpoints, which then take no room in the pool. There is one pool per device, shared by every handle and kept between calls:
  * what must start at zero is cleared by each call, but calls whose work overlaps on a device — from
  * two threads, or on two handles — race on the pool and give wrong results. A call returns only
  * when its work has ended, so calls made one after another are safe. Arguments, results and

@@ -32,7 +32,9 @@ from pathlib import Path
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
-REFERENCE = Path(os.environ.get("ACOUSTIC_SPACES_REFERENCE", "/root/reference"))
+#: The reference's sources: ACOUSTIC_SPACES_REFERENCE, else a checkout named "reference" beside
+#: this repository.
+REFERENCE = Path(os.environ.get("ACOUSTIC_SPACES_REFERENCE", HERE.parent.parent / "reference")).resolve()
 REF_SO = HERE / "_ref" / f"_native{sysconfig.get_config_var('EXT_SUFFIX')}"
 ORACLE_SO = HERE / "libfdtd_oracle.so"
 

@@ -45,9 +45,12 @@ def test_the_static_pool_gives_fdtd_gradients_result_twice(name, precision, rtol
     dloss = 2.0 * (y - 0.7 * y)
     solver.reset()
     expected = solver.gradient(signal, dloss, segment=64)
+    held = solver.info().device_bytes
     for _ in range(2):
         status, got = _noalloc(solver, signal, dloss, 64)
         assert status == _abi.FDTD_OK, _abi.load_library().fdtd_last_error(solver._handle)
+        # the handle took no device memory for it, and kept none
+        assert solver.info().device_bytes == held
         for key in expected:
             scale = np.max(np.abs(expected[key])) if expected[key].size else 0.0
             np.testing.assert_allclose(got[key], expected[key], rtol=rtol, atol=rtol * scale, err_msg=key)
@@ -55,12 +58,20 @@ def test_the_static_pool_gives_fdtd_gradients_result_twice(name, precision, rtol
 
 
 def test_a_run_beyond_the_pool_is_refused_before_any_work():
-    layout, _, _ = load_golden("resonant7")
+    layout, signal, _ = load_golden("resonant7")
     solver = B200WaveSolver(layout, precision="fp64")
+    # a state a gradient would change: a gradient resets the grid and steps it from rest
+    solver.run(signal[:37])
+    before = solver.state()
+    held = solver.info().device_bytes
     steps = 1_000_000  # dL/dy alone takes probes x 8 MB, beyond the 16 MiB pool
     status, _ = _noalloc(solver, np.zeros(steps, np.float32), np.zeros((solver.probes, steps)), 0)
     assert status == _abi.FDTD_EINVAL
     message = _abi.load_library().fdtd_last_error(solver._handle).decode()
     assert "static pool holds 16777216" in message
-    assert solver.info().steps_done == 0
+    after = solver.state()
+    for key in before:
+        np.testing.assert_array_equal(after[key], before[key], err_msg=key)
+    assert solver.info().steps_done == 37
+    assert solver.info().device_bytes == held
     solver.close()
