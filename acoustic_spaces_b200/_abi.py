@@ -103,6 +103,50 @@ class FdtdInfo(ctypes.Structure):
     ]
 
 
+class FdtdTiles(ctypes.Structure):
+    """``struct fdtd_tiles`` (include/fdtd_b200.h)."""
+
+    _fields_ = [
+        ("shape", ctypes.c_int32),
+        ("tile_x", ctypes.c_int32),
+        ("tile_y", ctypes.c_int32),
+        ("stages", ctypes.c_int32),
+        ("planes", ctypes.c_uint64),
+        ("tiles", ctypes.c_uint32),
+        ("blocks_per_sm", ctypes.c_int32),
+    ]
+
+
+class FdtdCutRoom(ctypes.Structure):
+    """``struct fdtd_cut_room`` (include/fdtd_b200.h)."""
+
+    _fields_ = [
+        ("normals", _f64p),
+        ("offsets", _f64p),
+        ("open", _u8p),
+        ("planes", ctypes.c_uint32),
+        ("origin", ctypes.c_double * 3),
+        ("cell", ctypes.c_double),
+        ("nx", ctypes.c_uint64),
+        ("ny", ctypes.c_uint64),
+        ("nz", ctypes.c_uint64),
+    ]
+
+
+class FdtdCutCells(ctypes.Structure):
+    """``struct fdtd_cut_cells`` (include/fdtd_b200.h)."""
+
+    _fields_ = [
+        ("cells", ctypes.c_uint64),
+        ("planes", ctypes.c_uint32),
+        ("cell", _u64p),
+        ("volume", _f64p),
+        ("face_area", _f64p),
+        ("cap", _f64p),
+        ("bare", _f64p),
+    ]
+
+
 #: The axis tables of the matched layer, in the order of fdtd_layout.keep / .push.
 KEEP = ("keep_x", "keep_face_x", "keep_y", "keep_face_y", "keep_z", "keep_face_z")
 PUSH = ("push_x", "push_face_x", "push_y", "push_face_y", "push_z", "push_face_z")
@@ -234,16 +278,22 @@ SIGNATURES = {
         ctypes.c_int,
         [ctypes.c_void_p, _f32p, ctypes.c_uint64, _f64p, ctypes.c_uint64, _f64p, _f64p, _f64p, _f64p, _f64p],
     ),
+    "fdtd_layer_gradient": (ctypes.c_int, [ctypes.c_void_p, _f64p]),
     "fdtd_set_tape_budget": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
     "fdtd_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_int),
                                      ctypes.POINTER(ctypes.c_int)]),
     "fdtd_set_launch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    "fdtd_set_tiles": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_uint64]),
+    "fdtd_get_tiles": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(FdtdTiles)]),
     "fdtd_level_plane": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int,
                                         ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_uint64)]),
     "fdtd_test_wait": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32]),
     "fdtd_set_tape": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
     "fdtd_set_coefficients": (ctypes.c_int, [ctypes.c_void_p, _f32p, _f32p, _f32p, _f32p, _f32p]),
     "fdtd_get_timing": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_uint64)]),
+    "fdtd_cut_convex": (ctypes.c_int, [ctypes.POINTER(FdtdCutRoom), ctypes.c_int, ctypes.POINTER(FdtdCutCells)]),
+    "fdtd_cut_free": (None, [ctypes.POINTER(FdtdCutCells)]),
+    "fdtd_cut_error": (ctypes.c_char_p, []),
     "fdtd_reset": (ctypes.c_int, [ctypes.c_void_p]),
     "fdtd_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "fdtd_get_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(FdtdInfo)]),

@@ -1,6 +1,6 @@
 // Device code of the reverse-time (adjoint) stepper: the gradient of a loss of the probes'
-// series with respect to the special rows' coefficients, for grids without a matched layer (either
-// stencil, with or without a speed field).
+// series with respect to the special rows' coefficients and the matched layer's tables (either
+// stencil, with or without a speed field; a matched layer comes with the 7-point stencil).
 //
 // A forward step maps the levels (u_n, u_{n-1}) and branch velocities (w_n, w_{n-1}) to u_{n+1},
 // w_{n+1}: z_{n+1} = G z_n - H z_{n-1} (+ the source), z = (u, w). For a special row (cell i,
@@ -62,6 +62,24 @@ struct AdjointTables {
     // cell's pressure never changes.)
     const uint32_t *special_read_start, *corrected_read_start, *read_probe;
     const double *read_weight;
+    // The matched layer (fdtd.hpp:2242-2264): its cells (pitched), the packed per-axis tables
+    // {keep, push, keep_face, push_face} by grid coordinate, each cell's scale with a speed field.
+    uint32_t layers;
+    const uint32_t *layer_cells;
+    const float4 *layer_coef[3];
+    const float *layer_scale;
+    uint32_t pitch, plane;
+    uint64_t cells;  // pitched cells of a level (the stride of the hat arrays)
+    // Rows linking to each layer cell (layer_from_start[c] .. [c + 1] of row and coefficient), the
+    // probes' terms of each layer cell (layer_read_start[c] .. [c + 1] into read_probe, read_weight),
+    // and which of each layer cell's axial neighbours are interior (bit d, direction d).
+    const uint32_t *layer_from_start, *layer_from_row, *layer_read_start;
+    const double *layer_from_coef;
+    const uint8_t *layer_interior;
+    // The layer's terms on a cell's adjoint (layer_terms): bit 2a, the cell below along axis a is a
+    // layer cell; bit 2a + 1, the cell above; bit 6, the cell itself. Per special row, per
+    // corrected cell (0 where no layer cell is near) and per layer cell.
+    const uint8_t *special_layer_mask, *corrected_layer_mask, *layer_mask;
 };
 
 // The trajectory of a run: level l of the special rows' pressure at traj_u[l * specials + k] and
@@ -88,8 +106,12 @@ __device__ __forceinline__ double probe_terms(const AdjointTables &t, uint32_t b
 // coefficient times its L~, minus the level two steps on (lam_out holds it on entry), plus the
 // probes' terms of step n. The sweep leaves these cells alone.
 template <typename T>
+__device__ __forceinline__ T layer_terms(const AdjointTables &t, const T *hat, uint32_t j, uint32_t mask);
+
+template <typename T>
 __device__ __forceinline__ void correct_cell(const AdjointTables &t, uint32_t c, const T *lam_next, const T *tilde,
-                                             T *lam_out, const double *dloss, uint64_t stride, uint64_t step) {
+                                             const T *hat, T *lam_out, const double *dloss, uint64_t stride,
+                                             uint64_t step) {
     if (c >= t.corrected) return;
     const uint32_t cell = t.corrected_cell[c];
     const uint32_t special = t.corrected_mask[c];
@@ -102,9 +124,9 @@ __device__ __forceinline__ void correct_cell(const AdjointTables &t, uint32_t c,
         for (int d = 6; d < 18; ++d)
             if (!(special & (1u << d))) edges += lam_next[(uint32_t)((int64_t)cell + t.offset[d])];
     }
-    T centre = (T)t.centre, axial = (T)t.axial, diagonal = (T)t.diagonal;
+    T centre = (T)t.centre, axial = (T)t.axial, diagonal = (T)t.diagonal, sc = (T)1;
     if (t.corrected_scale) {  // as the forward scaled sweep forms its cells
-        const T sc = (T)t.corrected_scale[c];
+        sc = (T)t.corrected_scale[c];
         centre = (T)2 - (T)t.total * sc;
         axial = sc * (T)t.axial;
         diagonal = sc * (T)t.diagonal;
@@ -112,6 +134,8 @@ __device__ __forceinline__ void correct_cell(const AdjointTables &t, uint32_t c,
     T value = centre * lam_next[cell] + axial * sum + diagonal * edges - lam_out[cell];
     for (uint32_t e = t.corrected_start[c], end = t.corrected_start[c + 1]; e < end; ++e)
         value += (T)t.corrected_coef[e] * tilde[t.corrected_row[e]];
+    // the matched layer's terms, times the cell's own scale as the rows' are
+    if (t.layers && t.corrected_layer_mask[c]) value += sc * layer_terms<T>(t, hat, cell, t.corrected_layer_mask[c]);
     const double probed = probe_terms(t, t.corrected_read_start[c], t.corrected_read_start[c + 1], dloss, stride, step);
     if (probed != 0.0) value += (T)probed;
     lam_out[cell] = value;
@@ -124,7 +148,7 @@ __device__ __forceinline__ void correct_cell(const AdjointTables &t, uint32_t c,
 // l0 + 2.
 template <typename T>
 __device__ __forceinline__ void special_adjoint_row(const AdjointTables &t, uint32_t k, const T *lam_next,
-                                                   const T *om_next, const T *tilde, T *lam_out, T *om_out,
+                                                   const T *om_next, const T *tilde, const T *hat, T *lam_out, T *om_out,
                                                    const T *traj_u, const T *traj_w, uint32_t level, double *g_ci,
                                                    double *g_cb, double *g_now, double *g_before, double *g_gain,
                                                    T *tilde_out, const double *dloss, uint64_t stride, uint64_t step) {
@@ -145,6 +169,7 @@ __device__ __forceinline__ void special_adjoint_row(const AdjointTables &t, uint
         gain_om2 += term;
     }
     const T U = tilde[k];
+    if (t.layers && t.special_layer_mask[k]) gathered += layer_terms<T>(t, hat, i, t.special_layer_mask[k]);
     T lam = gathered - (ci * cb * tilde2 + gain_om2);
     const double probed = probe_terms(t, t.special_read_start[k], t.special_read_start[k + 1], dloss, stride, step);
     if (probed != 0.0) lam += (T)probed;
@@ -171,21 +196,128 @@ __device__ __forceinline__ void special_adjoint_row(const AdjointTables &t, uint
     tilde_out[k] = next_tilde;
 }
 
-// The special rows' adjoint (blocks 0 .. special_blocks - 1) and correct_kernel's cells (the
-// blocks after) in one launch: they read the same complete level and write disjoint memory.
+// ---- the matched layer ------------------------------------------------------------------------
+//
+// Per layer cell and axis the forward step is (fdtd.hpp:2242-2264; s the cell's speed scale, 1
+// without a speed field)
+//   lo' = kf[x] lo - pf[x] (b_i - b_(i-st)),  hi' = kf[x+1] hi - pf[x+1] (b_(i+st) - b_i),
+//   q' = k[x] q - p[x] s (hi' - lo'),  b'_i = sum over axes of q'.
+// Going back, the adjoints of step n's new states, from the level after and the values carried
+// from the step after (primed):
+//   Q^ = lam_(n+1)[i] + k Q^',  H^ = -p s Q^ + kf[x+1] H^',  L^ = p s Q^ + kf[x] L^'.
+// Their terms on the pressures the states read: -pf[x+1] H^ on b_(i+st), pf[x] L^ on b_(i-st), and
+// pf[x+1] H^ - pf[x] L^ on b_i; the cells those land on gather them (layer_terms). The tables'
+// gradient, from the forward's factors of step n (layer_cell records them):
+//   dk[x] += Q^ q,  dp[x] -= Q^ s (hi' - lo'),  dkf[x+1] += H^ hi,  dpf[x+1] -= H^ (b_(i+st) - b_i),
+//   dkf[x] += L^ lo,  dpf[x] -= L^ (b_i - b_(i-st)).
+
+// The six factors per axis a layer cell records per forward step, at factor f of cell c:
+// traj[f * layers + c]: q, hi' - lo', hi, b_(i+st) - b_i, lo, b_i - b_(i-st) for axis 0, then 1, 2.
+constexpr int kLayerFactors = 18;
+
+// The carried values (9 per cell: Q^' x3, L^' x3, H^' x3, at carried[v * layers + c]) are
+// updated in place; hat[(2a) * cells + i] = pf[x] L^ and hat[(2a + 1) * cells + i] = pf[x+1] H^ are
+// the terms' factors its neighbours gather; g[(6a + f) * layers + c] sums the gradient's products of
+// the cell in double.
+template <typename T>
+__global__ void __launch_bounds__(kBlock) layer_hat_kernel(const AdjointTables t, const T *lam_next, T *carried,
+                                                           T *hat, const T *traj, double *g) {
+    const uint32_t c = blockIdx.x * kBlock + threadIdx.x;
+    const uint32_t L = t.layers;
+    if (c >= L) return;
+    const uint32_t i = t.layer_cells[c];
+    const uint32_t z = i / t.plane, r = i - z * t.plane, y = r / t.pitch;
+    const uint32_t at[3] = {r - y * t.pitch, y, z};
+    const T s = t.layer_scale ? (T)t.layer_scale[c] : (T)1;
+    const T lam = lam_next[i];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float4 c0 = __ldg(t.layer_coef[a] + at[a]), c1 = __ldg(t.layer_coef[a] + at[a] + 1);
+        const T ps = t.layer_scale ? (T)c0.y * s : (T)c0.y;
+        const T q_hat = lam + carried[(uint64_t)a * L + c];
+        const T lo_hat = ps * q_hat + carried[(uint64_t)(3 + a) * L + c];
+        const T hi_hat = -ps * q_hat + carried[(uint64_t)(6 + a) * L + c];
+        carried[(uint64_t)a * L + c] = (T)c0.x * q_hat;
+        carried[(uint64_t)(3 + a) * L + c] = (T)c0.z * lo_hat;
+        carried[(uint64_t)(6 + a) * L + c] = (T)c1.z * hi_hat;
+        hat[(uint64_t)(2 * a) * t.cells + i] = (T)c0.w * lo_hat;
+        hat[(uint64_t)(2 * a + 1) * t.cells + i] = (T)c1.w * hi_hat;
+        if (g) {
+            const T *f = traj + (uint64_t)(6 * a) * L + c;
+            double *gg = g + (uint64_t)(6 * a) * L + c;
+            gg[0] += (double)q_hat * (double)f[0];
+            gg[(uint64_t)1 * L] += -(double)q_hat * (double)s * (double)f[(uint64_t)1 * L];
+            gg[(uint64_t)2 * L] += (double)hi_hat * (double)f[(uint64_t)2 * L];
+            gg[(uint64_t)3 * L] += -(double)hi_hat * (double)f[(uint64_t)3 * L];
+            gg[(uint64_t)4 * L] += (double)lo_hat * (double)f[(uint64_t)4 * L];
+            gg[(uint64_t)5 * L] += -(double)lo_hat * (double)f[(uint64_t)5 * L];
+        }
+    }
+}
+
+// The layer's terms on the adjoint of cell j, from the hats of its layer neighbours and its own
+// (mask as AdjointTables' layer masks).
+template <typename T>
+__device__ __forceinline__ T layer_terms(const AdjointTables &t, const T *hat, uint32_t j, uint32_t mask) {
+    T sum = 0;
+    if (!mask) return sum;
+    const uint32_t strides[3] = {1u, t.pitch, t.plane};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        if (mask & (1u << (2 * a))) sum -= hat[(uint64_t)(2 * a + 1) * t.cells + (j - strides[a])];
+        if (mask & (1u << (2 * a + 1))) sum += hat[(uint64_t)(2 * a) * t.cells + (j + strides[a])];
+    }
+    if (mask & 64u) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) sum += hat[(uint64_t)(2 * a + 1) * t.cells + j] - hat[(uint64_t)(2 * a) * t.cells + j];
+    }
+    return sum;
+}
+
+// A layer cell's adjoint: its interior neighbours' axial x lam (with a speed field their stored
+// s lam), the rows linking to it, the layer's terms and the probes' terms (a layer cell's update
+// reads no level before the last, so no level two steps on enters).
+template <typename T>
+__device__ __forceinline__ void layer_adjoint_cell(const AdjointTables &t, uint32_t c, const T *lam_next, const T *tilde,
+                                                   const T *hat, T *lam_out, const double *dloss, uint64_t stride,
+                                                   uint64_t step) {
+    if (c >= t.layers) return;
+    const uint32_t i = t.layer_cells[c];
+    const uint32_t inner = t.layer_interior[c];
+    T sum = 0;
+#pragma unroll
+    for (int d = 0; d < 6; ++d)
+        if (inner & (1u << d)) sum += lam_next[(uint32_t)((int64_t)i + t.offset[d])];
+    T value = (T)t.axial * sum;
+    for (uint32_t e = t.layer_from_start[c], end = t.layer_from_start[c + 1]; e < end; ++e)
+        value += (T)t.layer_from_coef[e] * tilde[t.layer_from_row[e]];
+    value += layer_terms<T>(t, hat, i, t.layer_mask[c]);
+    const double probed = probe_terms(t, t.layer_read_start[c], t.layer_read_start[c + 1], dloss, stride, step);
+    if (probed != 0.0) value += (T)probed;
+    lam_out[i] = value;
+}
+
+// The special rows' adjoint (blocks 0 .. special_blocks - 1), correct_kernel's cells (the next
+// corrected_blocks) and the matched layer's cells (the blocks after) in one launch: they read the
+// same complete level (and the layer's hats of the step) and write disjoint memory.
 template <typename T>
 __global__ void __launch_bounds__(kBlock) rows_adjoint_kernel(const AdjointTables t, uint32_t special_blocks,
-                                                              const T *lam_next, const T *om_next, const T *tilde,
-                                                              T *lam_out, T *om_out, const T *traj_u, const T *traj_w,
+                                                              uint32_t corrected_blocks, const T *lam_next,
+                                                              const T *om_next, const T *tilde, const T *hat, T *lam_out,
+                                                              T *om_out, const T *traj_u, const T *traj_w,
                                                               uint32_t level, double *g_ci, double *g_cb, double *g_now,
                                                               double *g_before, double *g_gain, T *tilde_out,
                                                               const double *dloss, uint64_t stride, uint64_t step) {
     if (blockIdx.x < special_blocks)
-        special_adjoint_row<T>(t, blockIdx.x * kBlock + threadIdx.x, lam_next, om_next, tilde, lam_out, om_out, traj_u,
-                               traj_w, level, g_ci, g_cb, g_now, g_before, g_gain, tilde_out, dloss, stride, step);
+        special_adjoint_row<T>(t, blockIdx.x * kBlock + threadIdx.x, lam_next, om_next, tilde, hat, lam_out, om_out,
+                               traj_u, traj_w, level, g_ci, g_cb, g_now, g_before, g_gain, tilde_out, dloss, stride,
+                               step);
+    else if (blockIdx.x < special_blocks + corrected_blocks)
+        correct_cell<T>(t, (blockIdx.x - special_blocks) * kBlock + threadIdx.x, lam_next, tilde, hat, lam_out, dloss,
+                        stride, step);
     else
-        correct_cell<T>(t, (blockIdx.x - special_blocks) * kBlock + threadIdx.x, lam_next, tilde, lam_out, dloss, stride,
-                        step);
+        layer_adjoint_cell<T>(t, (blockIdx.x - special_blocks - corrected_blocks) * kBlock + threadIdx.x, lam_next,
+                              tilde, hat, lam_out, dloss, stride, step);
 }
 
 }  // namespace fdtd

@@ -62,10 +62,13 @@ using EncodeTiled = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t,
 struct AdjointState {
     AdjointTables t{};
     CUtensorMap map_t;  // the cell types of the adjoint sweep: the cells special rows read left out
+    CUtensorMap map_s;  // with a speed field, the scales in the adjoint sweep's boxes
     void *lam[2] = {nullptr, nullptr};
     void *om[2] = {nullptr, nullptr};
     void *tilde[2] = {nullptr, nullptr};  // L~ of the level at hand, and of the next (alternating)
     CUtensorMap lam_b[2], lam_a[2];
+    void *carried = nullptr;  // the matched layer's carried values (9 per cell)
+    void *hat = nullptr;      // the matched layer's terms' factors (6 pitched levels)
 };
 
 }  // namespace
@@ -89,7 +92,18 @@ struct fdtd_solver {
     // fdtd_autotune.
     int layer_per_sm = kLayerPerSm, special_per_sm = kSpecialPerSm;
     uint32_t bulk_tiles = 0;
-    int bulk_per_sm = 0;      // resident bulk blocks per multiprocessor
+    int bulk_per_sm = 0;      // resident bulk blocks per multiprocessor (shape 0)
+    int shape_per_sm[kShapes] = {0, 0, 0, 0};  // the same, each shape
+    // The sweep's tile shape (an index of kShapeInfo) and planes a tile, chosen by fdtd_autotune
+    // or fdtd_set_tiles; the pitched cell types kept on the host to lay the tiles out again; the
+    // forward list's device copy (replaced with the shape), and the adjoint's list (shape 0, no
+    // full tiles).
+    int bulk_shape = 0;
+    uint64_t bulk_chunk = 32;
+    std::vector<uint8_t> host_types;
+    void *tiles_device = nullptr;
+    const int4 *plain_tiles = nullptr;
+    uint32_t plain_count = 0;
     uint64_t nx = 0, ny = 0, nz = 0, n = 0, pitch = 0, n_device = 0;
     uint64_t air = 0, interior = 0, links = 0, states = 0, layers = 0, probes = 0, specials = 0;
     uint64_t steps_done = 0;
@@ -129,7 +143,11 @@ struct fdtd_solver {
     std::vector<int32_t> adjoint_reader_row;  // of the kept adjoint (fdtd_set_coefficients)
     std::vector<uint32_t> adjoint_corrected_row;
     std::vector<double> adjoint_reader_base, adjoint_corrected_base;
+    std::vector<uint32_t> adjoint_layer_row;  // rows linking to layer cells, and their bases
+    std::vector<double> adjoint_layer_base;
     std::vector<int32_t> state_branch;  // each branch state's branch
+    // The last gradient's part in the matched layer's tables (fdtd_layer_gradient), empty without.
+    std::vector<double> layer_gradient;
     uint64_t branches = 0;
     // fdtd_gradient's device workspace, kept and handed out again in the same order while the
     // sizes asked for stay the same (a fit's iterations then allocate nothing).
@@ -148,6 +166,7 @@ struct fdtd_solver {
     // written as level k + record_offset of record_u and record_w; the gradient's recomputation
     // needs no probe records (record_probes false).
     void *record_u = nullptr, *record_w = nullptr;
+    void *record_layer = nullptr;  // the layer's factors of each step (kLayerFactors x layers a step)
     uint64_t record_offset = 2;
     bool record_probes = true;
     // The tape (fdtd_set_tape): a run of fdtd_run from rest keeps, for the gradient that follows,
@@ -359,6 +378,113 @@ int tensor_map(fdtd_solver *s, CUtensorMap *map, void *base, CUtensorMapDataType
     return FDTD_OK;
 }
 
+// Planes a tile by default: at most 64, halved while there would be fewer than 8 tiles a
+// multiprocessor (at least 8 planes).
+uint64_t default_chunk(const fdtd_solver *s) {
+    const BulkArgs &bk = s->bulk;
+    const uint64_t cols = ((bk.x1 - bk.xa + 63) / 64) * ((bk.y1 - bk.y0 + 15) / 16);
+    const uint64_t planes = cols * (bk.z1 - bk.z0);
+    uint64_t chunk = 64;
+    while (chunk > 8 && planes / chunk < (uint64_t)s->sms * 8) chunk /= 2;
+    return chunk;
+}
+
+// The sweep's tile list for shape `shape`: the columns of TX x TY cells over the interior cells'
+// box (x from its 16-aligned start), and in each the runs of planes that hold interior cells, cut
+// into chunks of at most `chunk` planes. Grids of many rooms (stacked along z) skip the planes
+// between the rooms. With `flags`, a tile whose cells are all interior in all of its planes is
+// marked kFullTile.
+int tile_list(fdtd_solver *s, int shape, uint64_t chunk, bool flags, std::vector<int4> &list) {
+    const BulkArgs &bk = s->bulk;
+    const uint64_t TX = (uint64_t)kShapeInfo[shape].tx, TY = (uint64_t)kShapeInfo[shape].ty;
+    const uint64_t nz = s->nz, nx = s->nx, ny = s->ny, pitch = s->pitch;
+    const uint64_t tiles_x = (bk.x1 - bk.xa + TX - 1) / TX, tiles_y = (bk.y1 - bk.y0 + TY - 1) / TY;
+    const uint64_t columns = tiles_x * tiles_y;
+    // Per column and plane: interior cells it holds.
+    std::vector<uint32_t> count(columns * nz, 0);
+    for (uint64_t z = bk.z0; z < bk.z1; ++z)
+        for (uint64_t y = bk.y0; y < bk.y1; ++y) {
+            const uint8_t *row = &s->host_types[pitch * (y + ny * z)];
+            const uint64_t base = ((y - bk.y0) / TY * tiles_x) * nz + z;
+            for (uint64_t x = bk.xa; x < bk.x1; ++x)
+                if (row[x] == kInterior) ++count[base + (x - bk.xa) / TX * nz];
+        }
+    list.clear();
+    for (uint64_t c = 0; c < columns; ++c) {
+        const uint64_t xt = bk.xa + (c % tiles_x) * TX, yt = bk.y0 + (c / tiles_x) * TY;
+        // A plane of the column is full when all its TX x TY cells lie in the grid and are interior.
+        const bool inside = xt + TX <= nx && yt + TY <= ny;
+        for (uint64_t z = 0; z < nz;) {
+            if (!count[c * nz + z]) {
+                ++z;
+                continue;
+            }
+            uint64_t end = z;
+            bool full = flags && inside;
+            while (end < nz && count[c * nz + end] && end - z < chunk) {
+                full = full && count[c * nz + end] == TX * TY;
+                ++end;
+            }
+            list.push_back(make_int4((int)xt, (int)yt, (int)z, (int)end | (full ? kFullTile : 0)));
+            z = end;
+        }
+    }
+    if (list.size() >= (1ull << 31)) return fail(s, FDTD_EINVAL, "the wave grid is too large for one launch");
+    return FDTD_OK;
+}
+
+// Lays the sweep's tiles out for shape `shape` and `chunk` planes a tile: its list on the device
+// (the previous one freed) and the tensor maps with the shape's boxes.
+int use_shape(fdtd_solver *s, int shape, uint64_t chunk) {
+    if (shape < 0 || shape >= kShapes) return fail(s, FDTD_EINVAL, "no such tile shape");
+    if (chunk < 1 || chunk > 1024) return fail(s, FDTD_EINVAL, "planes a tile out of 1 to 1024");
+    std::vector<int4> list;
+    int rc;
+    if ((rc = tile_list(s, shape, chunk, true, list))) return rc;
+    // The previous list is no longer read once the handle's work has ended.
+    CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+    if (s->tiles_device) {
+        auto it = std::find(s->allocations.begin(), s->allocations.end(), s->tiles_device);
+        if (it != s->allocations.end()) s->allocations.erase(it);
+        s->device_bytes -= sizeof(int4) * s->bulk_tiles;
+        cudaFree(s->tiles_device);
+        s->tiles_device = nullptr;
+    }
+    const int4 *d_list;
+    if ((rc = upload(s, list.data(), list.size(), &d_list))) return rc;
+    s->tiles_device = const_cast<int4 *>(d_list);
+    s->bulk_tiles = (uint32_t)list.size();
+    s->bulk.tiles = s->bulk_tiles;
+    s->bulk.tile_list = d_list;
+    s->bulk_blocks = s->bulk_tiles;  // one tile a block
+    s->bulk_shape = shape;
+    s->bulk_chunk = chunk;
+    const uint32_t TX = (uint32_t)kShapeInfo[shape].tx, TY = (uint32_t)kShapeInfo[shape].ty;
+    const uint32_t BX = TX + 2 * kHX, BY = TY + 2;
+    const size_t e = s->precision == FDTD_FP64 ? 8 : 4;
+    const CUtensorMapDataType ft = e == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    // The levels' roles at this moment (u[1] current): map_b/map_a[k] follow u[k].
+    for (int k = 0; k < 2; ++k) {
+        if ((rc = tensor_map(s, &s->map_b[k], s->u[k], ft, (uint32_t)e, BX, BY))) return rc;
+        if ((rc = tensor_map(s, &s->map_a[k], s->u[k], ft, (uint32_t)e, TX, TY))) return rc;
+    }
+    if (s->increment && (rc = tensor_map(s, &s->map_d, s->increment, ft, (uint32_t)e, TX, TY))) return rc;
+    if ((rc = tensor_map(s, &s->map_t, const_cast<uint8_t *>(s->types_device), CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, TX, TY)))
+        return rc;
+    if ((rc = tensor_map(s, &s->map_s, s->scaled ? const_cast<float *>(s->scale_device) : s->u[0],
+                         CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, TX, TY)))
+        return rc;
+    // Captured chunks hold the old list and maps.
+    for (cudaGraphExec_t &g : s->graph)
+        if (g) cudaGraphExecDestroy(g), g = nullptr;
+    for (cudaGraphExec_t &g : s->tape_graph)
+        if (g) cudaGraphExecDestroy(g), g = nullptr;
+    for (auto &row : s->grad_graph)
+        for (cudaGraphExec_t &g : row)
+            if (g) cudaGraphExecDestroy(g), g = nullptr;
+    return FDTD_OK;
+}
+
 template <typename T>
 Fields<T> fields_for(const fdtd_solver *s, bool flip) {
     // flip = false: b is u[1] (current), a is u[0]; flip = true after an odd number of steps.
@@ -377,17 +503,40 @@ Fields<T> fields_for(const fdtd_solver *s, bool flip) {
     return f;
 }
 
+template <typename T, bool WIDE, bool SCALED, bool COMP, class SH>
+int set_up_shape(fdtd_solver *s, int *per_sm) {
+    CUDA_TRY(s, cudaFuncSetAttribute(bulk_kernel<T, WIDE, SCALED, COMP, SH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)Stage<T, SCALED, SH>::smem));
+    CUDA_TRY(s, cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, bulk_kernel<T, WIDE, SCALED, COMP, SH>, kBlock,
+                                                              Stage<T, SCALED, SH>::smem));
+    return FDTD_OK;
+}
+
+// Every shape's shared memory set up; the resident blocks an SM of each kept.
 template <typename T, bool WIDE, bool SCALED, bool COMP>
 int set_up_kernels(fdtd_solver *s) {
-    CUDA_TRY(s, cudaFuncSetAttribute(bulk_kernel<T, WIDE, SCALED, COMP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)Stage<T, SCALED>::smem));
-    int per_sm = 0;
-    CUDA_TRY(s, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bulk_kernel<T, WIDE, SCALED, COMP>, kBlock,
-                                                              Stage<T, SCALED>::smem));
-    s->bulk_per_sm = per_sm;
-    // One tile per block: measured faster than a persistent grid of the resident blocks.
-    s->bulk_blocks = s->bulk_tiles;
+    int rc;
+    if ((rc = set_up_shape<T, WIDE, SCALED, COMP, Shape0>(s, &s->shape_per_sm[0]))) return rc;
+    if ((rc = set_up_shape<T, WIDE, SCALED, COMP, Shape1>(s, &s->shape_per_sm[1]))) return rc;
+    if ((rc = set_up_shape<T, WIDE, SCALED, COMP, Shape2>(s, &s->shape_per_sm[2]))) return rc;
+    if ((rc = set_up_shape<T, WIDE, SCALED, COMP, Shape3>(s, &s->shape_per_sm[3]))) return rc;
+    s->bulk_per_sm = s->shape_per_sm[0];
     return FDTD_OK;
+}
+
+// One launch of the sweep in the handle's shape.
+template <typename T, bool WIDE, bool SCALED, bool COMP>
+void launch_bulk(const fdtd_solver *s, const CUtensorMap &mb, const CUtensorMap &ma, const BulkArgs &args) {
+#define FDTD_BULK(SH)                                                                          \
+    bulk_kernel<T, WIDE, SCALED, COMP, SH><<<s->bulk_blocks, kBlock, Stage<T, SCALED, SH>::smem, s->stream>>>( \
+        mb, ma, s->map_t, s->map_s, args)
+    switch (s->bulk_shape) {
+        case 1: FDTD_BULK(Shape1); break;
+        case 2: FDTD_BULK(Shape2); break;
+        case 3: FDTD_BULK(Shape3); break;
+        default: FDTD_BULK(Shape0); break;
+    }
+#undef FDTD_BULK
 }
 
 template <typename T, bool WIDE, bool SCALED, bool COMP = false>
@@ -399,7 +548,6 @@ int launch_steps(fdtd_solver *s, const float *d_signal, uint64_t steps, double *
     const uint64_t layer_cap = s->layer_per_sm ? (uint64_t)s->sms * s->layer_per_sm : UINT64_MAX;
     const uint32_t special_blocks = (uint32_t)std::min<uint64_t>((s->specials + kBlock - 1) / kBlock, special_cap);
     const uint32_t probe_blocks = (uint32_t)((s->probes + kProbeWarps - 1) / kProbeWarps);
-    const uint32_t smem = Stage<T, SCALED>::smem;
     const uint32_t layer_blocks = (uint32_t)std::min<uint64_t>((s->layers + kBlock - 1) / kBlock, layer_cap);
     // Each step: the interior sweep on the handle's stream; beside it the matched layer on the
     // layer stream, of the highest priority (its blocks take the thread slots that the sweep's
@@ -420,6 +568,8 @@ int launch_steps(fdtd_solver *s, const float *d_signal, uint64_t steps, double *
             f.traj_u = static_cast<T *>(s->record_u) + (k + s->record_offset) * s->specials;
             f.traj_w = static_cast<T *>(s->record_w) + (k + s->record_offset) * s->states;
         }
+        // The matched layer's factors of step k (the gradient's recomputation).
+        if (s->record_layer) f.traj_layer = static_cast<T *>(s->record_layer) + k * kLayerFactors * s->layers;
         if (fork) {
             if (k > 0) {
                 CUDA_TRY(s, cudaStreamWaitEvent(s->stream, s->joined[1], 0));
@@ -448,8 +598,7 @@ int launch_steps(fdtd_solver *s, const float *d_signal, uint64_t steps, double *
             args.d = f.d;
             const int cur = flip ? 0 : 1, prev = flip ? 1 : 0;
             // (Compensated: the increments stand in the previous pressure's place.)
-            bulk_kernel<T, WIDE, SCALED, COMP><<<s->bulk_blocks, kBlock, smem, s->stream>>>(
-                s->map_b[cur], COMP ? s->map_d : s->map_a[prev], s->map_t, s->map_s, args);
+            launch_bulk<T, WIDE, SCALED, COMP>(s, s->map_b[cur], COMP ? s->map_d : s->map_a[prev], args);
         }
         if (ev) CUDA_TRY(s, cudaEventRecord(ev[1], s->stream));
         if (ev) CUDA_TRY(s, cudaEventRecord(ev[2], layer));
@@ -659,58 +808,18 @@ int build(fdtd_solver *s, const fdtd_layout *L) {
         bk.xa = (uint32_t)(x0 / 16 * 16);
         bk.y0 = (uint32_t)y0, bk.z0 = (uint32_t)z0;
         bk.x1 = (uint32_t)x1, bk.y1 = (uint32_t)y1, bk.z1 = (uint32_t)z1;
-        // The tile list: the columns of kTX x kTY cells over the box, and in each the runs of
-        // planes that hold interior cells, cut into chunks of at most `chunk` planes, so that
-        // there are blocks enough for every multiprocessor several times over. Grids of many
-        // rooms (stacked along z) skip the planes between the rooms.
-        const uint64_t tiles_x = (x1 - bk.xa + kTX - 1) / kTX, tiles_y = (y1 - y0 + kTY - 1) / kTY;
-        const uint64_t columns = tiles_x * tiles_y;
-        std::vector<uint8_t> occupied(columns * nz, 0);
-        uint64_t planes = 0;
-        for (uint64_t z = z0; z < z1; ++z)
-            for (uint64_t y = y0; y < y1; ++y) {
-                const uint8_t *row = &L->types[nx * (y + ny * z)];
-                for (uint64_t x = x0; x < x1; ++x) {
-                    if (row[x] != kInterior) continue;
-                    uint8_t &o = occupied[((y - y0) / kTY * tiles_x + (x - bk.xa) / kTX) * nz + z];
-                    planes += o == 0;
-                    o = 1;
-                }
-            }
-        uint64_t chunk = 64;
-        while (chunk > 8 && planes / chunk < (uint64_t)s->sms * 8) chunk /= 2;
-        std::vector<int4> list;
-        for (uint64_t c = 0; c < columns; ++c) {
-            const int xt = (int)(bk.xa + (c % tiles_x) * kTX), yt = (int)(y0 + (c / tiles_x) * kTY);
-            for (uint64_t z = 0; z < nz;) {
-                if (!occupied[c * nz + z]) {
-                    ++z;
-                    continue;
-                }
-                uint64_t end = z;
-                while (end < nz && occupied[c * nz + end] && end - z < chunk) ++end;
-                list.push_back(make_int4(xt, yt, (int)z, (int)end));
-                z = end;
-            }
-        }
-        if (list.size() >= (1ull << 31)) return fail(s, FDTD_EINVAL, "the wave grid is too large for one launch");
-        s->bulk_tiles = (uint32_t)list.size();
-        bk.tiles = s->bulk_tiles;
-        const int4 *d_list;
-        if ((rc = upload(s, list.data(), list.size(), &d_list))) return rc;
-        bk.tile_list = d_list;
-        const CUtensorMapDataType ft = s->precision == FDTD_FP64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
-        for (int k = 0; k < 2; ++k) {
-            if ((rc = tensor_map(s, &s->map_b[k], s->u[k], ft, (uint32_t)e, kBX, kBY))) return rc;
-            if ((rc = tensor_map(s, &s->map_a[k], s->u[k], ft, (uint32_t)e, kTX, kTY))) return rc;
-        }
-        if (s->increment && (rc = tensor_map(s, &s->map_d, s->increment, ft, (uint32_t)e, kTX, kTY))) return rc;
-        if ((rc = tensor_map(s, &s->map_t, const_cast<uint8_t *>(d_types), CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, kTX, kTY)))
-            return rc;
-        if ((rc = tensor_map(s, &s->map_s, s->scaled ? const_cast<float *>(d_scale) : s->u[0],
-                             CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, kTX, kTY)))
-            return rc;
+        s->host_types = std::move(types);
+        s->bulk_chunk = default_chunk(s);
+        // The adjoint's sweep: the default shape and chunk, every tile checking its cell types
+        // (the adjoint's types leave out cells that a full tile of the forward sweep holds).
+        std::vector<int4> plain;
+        if ((rc = tile_list(s, 0, s->bulk_chunk, false, plain))) return rc;
+        const int4 *d_plain;
+        if ((rc = upload(s, plain.data(), plain.size(), &d_plain))) return rc;
+        s->plain_tiles = d_plain;
+        s->plain_count = (uint32_t)plain.size();
         if ((rc = set_up(s))) return rc;
+        if ((rc = use_shape(s, 0, s->bulk_chunk))) return rc;
     }
 
     // Special rows with 32-bit pitched indices.
@@ -893,6 +1002,12 @@ struct AdjointLists {
     std::vector<double> reader_base, corrected_base;
     std::vector<uint8_t> reader_kind;
     std::vector<double> reader_coef, coefs;
+    // The matched layer: rows linking to each layer cell (start, row, coefficient and its base),
+    // the probes' terms of each layer cell, each layer cell's interior axial neighbours, and the
+    // layer-term masks of the special rows, corrected cells and layer cells (AdjointTables).
+    std::vector<uint32_t> layer_from_start, layer_from_row, layer_read_start;
+    std::vector<double> layer_from_coef, layer_from_base;
+    std::vector<uint8_t> layer_interior, special_layer_mask, corrected_layer_mask, layer_mask;
 };
 
 // The lists from the handle's own device tables.
@@ -907,7 +1022,6 @@ struct AdjointLists {
 // The 19-point operator is symmetric as the 7-point one is: its readers and corrections reach the
 // twelve edge neighbours too, with the diagonal weight.
 int adjoint_lists(fdtd_solver *s, AdjointLists &out) {
-    if (s->layers) return fail(s, FDTD_EINVAL, "the adjoint takes grids without a matched layer");
     const Tables &g = s->tables;
     const uint64_t K = s->specials;
     std::vector<uint32_t> special;
@@ -947,6 +1061,27 @@ int adjoint_lists(fdtd_solver *s, AdjointLists &out) {
     std::vector<std::vector<Reader>> readers(K);
     std::unordered_map<uint32_t, std::vector<std::pair<uint32_t, double>>> corrected;  // (row, base)
     const uint64_t kind_bit = 1ull << 63;
+    // The matched layer's cells by pitched index, and the rows linking to each.
+    const uint64_t Lc = s->layers;
+    std::unordered_map<uint32_t, uint32_t> layer_of;
+    layer_of.reserve(Lc * 2);
+    for (uint64_t c = 0; c < Lc; ++c) layer_of[s->layer_cells[c]] = (uint32_t)c;
+    std::vector<std::vector<std::pair<uint32_t, double>>> layer_from(Lc);  // (row, base)
+    // A cell's layer-term mask: bit d for an axial neighbour d in the layer, bit 6 for itself.
+    auto layer_mask = [&](uint32_t i) {
+        uint32_t mask = types[i] == kLayer ? 64u : 0u;
+        for (int d = 0; d < 6; ++d) {
+            uint32_t j;
+            if (neighbour(i, d, &j) && types[j] == kLayer) mask |= 1u << d;
+        }
+        return (uint8_t)mask;
+    };
+    // Interior cells next to the layer read its terms: formed whole by correct_kernel.
+    for (uint64_t c = 0; c < Lc; ++c)
+        for (int d = 0; d < 6; ++d) {
+            uint32_t j;
+            if (neighbour(s->layer_cells[c], d, &j) && types[j] == kInterior) corrected[j];
+        }
     for (uint64_t k = 0; k < K; ++k) {
         const uint32_t i = special[k];
         readers[k].push_back({kind_bit | k, (int32_t)k, (double)coef_a[k]});
@@ -965,8 +1100,10 @@ int adjoint_lists(fdtd_solver *s, AdjointLists &out) {
                 readers[it->second].push_back({kind_bit | k, (int32_t)k, (double)weight[at]});
             } else if (types[j] == kInterior) {
                 corrected[j].push_back({(uint32_t)k, (double)weight[at]});
+            } else if (types[j] == kLayer) {
+                layer_from[layer_of.at(j)].push_back({(uint32_t)k, (double)weight[at]});
             } else {
-                return fail(s, FDTD_EINVAL, "a special row links to a cell that is neither interior nor special");
+                return fail(s, FDTD_EINVAL, "a special row links to a cell that holds no air");
             }
         }
     }
@@ -992,7 +1129,8 @@ int adjoint_lists(fdtd_solver *s, AdjointLists &out) {
     for (uint32_t p = 0; p < g.probes; ++p)
         for (uint32_t e = probe_start[p]; e < probe_start[p + 1]; ++e) {
             const uint32_t cell = probe_cells[e];
-            if (row_of.count(cell) || types[cell] == kInterior) probed[cell].push_back({p, probe_weights[e]});
+            if (row_of.count(cell) || types[cell] == kInterior || types[cell] == kLayer)
+                probed[cell].push_back({p, probe_weights[e]});
             if (types[cell] == kInterior) corrected[cell];
         }
     auto read_terms = [&](uint32_t cell, double factor) {
@@ -1003,6 +1141,8 @@ int adjoint_lists(fdtd_solver *s, AdjointLists &out) {
     };
     out.special_read_start.assign(1, 0);
     for (uint64_t k = 0; k < K; ++k) out.special_read_start.push_back(read_terms(special[k], 1.0));
+    out.special_layer_mask.resize(K);
+    for (uint64_t k = 0; k < K; ++k) out.special_layer_mask[k] = Lc ? layer_mask(special[k]) : 0;
     out.corrected_read_start.assign(1, out.special_read_start.back());
     out.starts.assign(1, 0);
     out.types = types;
@@ -1012,16 +1152,43 @@ int adjoint_lists(fdtd_solver *s, AdjointLists &out) {
         if (s->scaled) out.scales.push_back(scale[cell]);
         out.corrected_read_start.push_back(read_terms(cell, factor));
         out.types[cell] = kSpecial;  // left to correct_kernel
-        uint32_t mask = 0;  // (an interior cell's neighbours all lie in the grid)
-        for (int d = 0; d < directions; ++d)
-            if (row_of.count((uint32_t)((int64_t)cell + g.offset[d]))) mask |= 1u << d;
+        // The neighbours left out of its stencil: special rows, and layer cells (whose updates read
+        // it through their faces: the layer's terms). (An interior cell's neighbours all lie in
+        // the grid.)
+        uint32_t mask = 0;
+        for (int d = 0; d < directions; ++d) {
+            const uint32_t j = (uint32_t)((int64_t)cell + g.offset[d]);
+            if (row_of.count(j) || types[j] == kLayer) mask |= 1u << d;
+        }
         out.masks.push_back(mask);
+        out.corrected_layer_mask.push_back(Lc ? layer_mask(cell) : 0);
         for (const auto &[r, base] : list) {
             out.rows.push_back(r);
             out.corrected_base.push_back(base * factor);
             out.coefs.push_back((double)coef_inv[r] * (base * factor));
         }
         out.starts.push_back((uint32_t)out.rows.size());
+    }
+    // The layer cells: the rows linking to each, the probes' terms, the interior neighbours whose
+    // adjoints they read, and their layer-term masks.
+    out.layer_from_start.assign(1, 0);
+    out.layer_read_start.assign(1, out.corrected_read_start.back());
+    for (uint64_t c = 0; c < Lc; ++c) {
+        const uint32_t i = s->layer_cells[c];
+        for (const auto &[r, base] : layer_from[c]) {
+            out.layer_from_row.push_back(r);
+            out.layer_from_base.push_back(base);
+            out.layer_from_coef.push_back((double)coef_inv[r] * base);
+        }
+        out.layer_from_start.push_back((uint32_t)out.layer_from_row.size());
+        out.layer_read_start.push_back(read_terms(i, 1.0));
+        uint8_t inner = 0;
+        for (int d = 0; d < 6; ++d) {
+            uint32_t j;
+            if (neighbour(i, d, &j) && types[j] == kInterior) inner |= (uint8_t)(1u << d);
+        }
+        out.layer_interior.push_back(inner);
+        out.layer_mask.push_back(layer_mask(i));
     }
     return FDTD_OK;
 }
@@ -1075,6 +1242,26 @@ int place_adjoint(fdtd_solver *s, const AdjointLists &l, Pool &pool, AdjointStat
     if ((rc = place(s, pool, l.corrected_read_start, &t.corrected_read_start))) return rc;
     if ((rc = place(s, pool, l.read_probe, &t.read_probe))) return rc;
     if ((rc = place(s, pool, l.read_weight, &t.read_weight))) return rc;
+    // The matched layer: the forward's cells and tables, the lists, the masks; its carried values
+    // and the hats (six pitched levels) are the adjoint's own.
+    t.layers = (uint32_t)s->layers;
+    t.layer_cells = g.layer_cells;
+    for (int axis = 0; axis < 3; ++axis) t.layer_coef[axis] = g.layer_coef[axis];
+    t.layer_scale = g.layer_scale;
+    t.pitch = g.pitch, t.plane = g.plane;
+    t.cells = s->n_device;
+    if ((rc = place(s, pool, l.special_layer_mask, &t.special_layer_mask))) return rc;
+    if ((rc = place(s, pool, l.corrected_layer_mask, &t.corrected_layer_mask))) return rc;
+    if ((rc = place(s, pool, l.layer_mask, &t.layer_mask))) return rc;
+    if ((rc = place(s, pool, l.layer_from_start, &t.layer_from_start))) return rc;
+    if ((rc = place(s, pool, l.layer_from_row, &t.layer_from_row))) return rc;
+    if ((rc = place(s, pool, l.layer_from_coef, &t.layer_from_coef))) return rc;
+    if ((rc = place(s, pool, l.layer_read_start, &t.layer_read_start))) return rc;
+    if ((rc = place(s, pool, l.layer_interior, &t.layer_interior))) return rc;
+    if (s->layers) {
+        if ((rc = pool.take(e * 9 * s->layers, &a.carried, true))) return rc;
+        if ((rc = pool.take(e * 6 * s->n_device, &a.hat, true))) return rc;
+    }
     for (int k = 0; k < 2; ++k) {
         if ((rc = pool.take(e * s->n_device, &a.lam[k], true))) return rc;
         if ((rc = pool.take(e * S, &a.om[k], true))) return rc;
@@ -1089,6 +1276,9 @@ int place_adjoint(fdtd_solver *s, const AdjointLists &l, Pool &pool, AdjointStat
         }
         if ((rc = tensor_map(s, &a.map_t, const_cast<uint8_t *>(sweep_types), CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, kTX,
                              kTY)))
+            return rc;
+        if ((rc = tensor_map(s, &a.map_s, s->scaled ? const_cast<float *>(s->scale_device) : a.lam[0],
+                             CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, kTX, kTY)))
             return rc;
     }
     return FDTD_OK;
@@ -1122,6 +1312,8 @@ int set_up_adjoint(fdtd_solver *s) {
     s->adjoint_reader_base = std::move(lists.reader_base);
     s->adjoint_corrected_row = std::move(lists.rows);
     s->adjoint_corrected_base = std::move(lists.corrected_base);
+    s->adjoint_layer_row = std::move(lists.layer_from_row);
+    s->adjoint_layer_base = std::move(lists.layer_from_base);
     s->adjoint_ready = true;
     return FDTD_OK;
 }
@@ -1157,6 +1349,54 @@ struct Kept {
         return FDTD_OK;
     }
 };
+
+// A checkpoint of the state between runs: the current and the previous level, the current and
+// the previous branch velocities, and with a matched layer its pressure parts and the current
+// faces (faces[1]).
+uint64_t checkpoint_bytes(const fdtd_solver *s) {
+    const uint64_t e = s->precision == FDTD_FP64 ? 8 : 4;
+    uint64_t bytes = 2 * e * s->n_device + 2 * e * s->states;
+    if (s->layers) bytes += 3 * e * s->layers + 3 * e * s->n_device;
+    return bytes;
+}
+
+int save_checkpoint(fdtd_solver *s, char *c) {
+    const uint64_t e = s->precision == FDTD_FP64 ? 8 : 4, level = e * s->n_device, states = e * s->states;
+    CUDA_TRY(s, cudaMemcpyAsync(c, s->u[1], level, cudaMemcpyDeviceToDevice, s->stream));
+    CUDA_TRY(s, cudaMemcpyAsync(c + level, s->u[0], level, cudaMemcpyDeviceToDevice, s->stream));
+    c += 2 * level;
+    if (states) {
+        CUDA_TRY(s, cudaMemcpyAsync(c, s->w[1], states, cudaMemcpyDeviceToDevice, s->stream));
+        CUDA_TRY(s, cudaMemcpyAsync(c + states, s->w[0], states, cudaMemcpyDeviceToDevice, s->stream));
+    }
+    c += 2 * states;
+    if (s->layers) {
+        CUDA_TRY(s, cudaMemcpyAsync(c, s->layer_parts, 3 * e * s->layers, cudaMemcpyDeviceToDevice, s->stream));
+        c += 3 * e * s->layers;
+        for (int axis = 0; axis < 3; ++axis, c += level)
+            CUDA_TRY(s, cudaMemcpyAsync(c, s->faces[1][axis], level, cudaMemcpyDeviceToDevice, s->stream));
+    }
+    return FDTD_OK;
+}
+
+int restore_checkpoint(fdtd_solver *s, const char *c) {
+    const uint64_t e = s->precision == FDTD_FP64 ? 8 : 4, level = e * s->n_device, states = e * s->states;
+    CUDA_TRY(s, cudaMemcpyAsync(s->u[1], c, level, cudaMemcpyDeviceToDevice, s->stream));
+    CUDA_TRY(s, cudaMemcpyAsync(s->u[0], c + level, level, cudaMemcpyDeviceToDevice, s->stream));
+    c += 2 * level;
+    if (states) {
+        CUDA_TRY(s, cudaMemcpyAsync(s->w[1], c, states, cudaMemcpyDeviceToDevice, s->stream));
+        CUDA_TRY(s, cudaMemcpyAsync(s->w[0], c + states, states, cudaMemcpyDeviceToDevice, s->stream));
+    }
+    c += 2 * states;
+    if (s->layers) {
+        CUDA_TRY(s, cudaMemcpyAsync(s->layer_parts, c, 3 * e * s->layers, cudaMemcpyDeviceToDevice, s->stream));
+        c += 3 * e * s->layers;
+        for (int axis = 0; axis < 3; ++axis, c += level)
+            CUDA_TRY(s, cudaMemcpyAsync(s->faces[1][axis], c, level, cudaMemcpyDeviceToDevice, s->stream));
+    }
+    return FDTD_OK;
+}
 
 // Whether the handle holds the tape of a run of this drive with these segments: gradient<T> then
 // takes the tape's checkpoints or trajectory and recomputes no forward pass of its own.
@@ -1203,26 +1443,16 @@ int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float
         g[k] = static_cast<double *>(p);
     }
     const uint64_t level_bytes = e * s->n_device, state_bytes = e * S;
-    auto save = [&](char *c) -> int {
-        CUDA_TRY(s, cudaMemcpyAsync(c, s->u[1], level_bytes, cudaMemcpyDeviceToDevice, s->stream));
-        CUDA_TRY(s, cudaMemcpyAsync(c + level_bytes, s->u[0], level_bytes, cudaMemcpyDeviceToDevice, s->stream));
-        if (S) {
-            CUDA_TRY(s, cudaMemcpyAsync(c + 2 * level_bytes, s->w[1], state_bytes, cudaMemcpyDeviceToDevice, s->stream));
-            CUDA_TRY(s, cudaMemcpyAsync(c + 2 * level_bytes + state_bytes, s->w[0], state_bytes,
-                                        cudaMemcpyDeviceToDevice, s->stream));
-        }
-        return FDTD_OK;
-    };
-    auto restore = [&](const char *c) -> int {
-        CUDA_TRY(s, cudaMemcpyAsync(s->u[1], c, level_bytes, cudaMemcpyDeviceToDevice, s->stream));
-        CUDA_TRY(s, cudaMemcpyAsync(s->u[0], c + level_bytes, level_bytes, cudaMemcpyDeviceToDevice, s->stream));
-        if (S) {
-            CUDA_TRY(s, cudaMemcpyAsync(s->w[1], c + 2 * level_bytes, state_bytes, cudaMemcpyDeviceToDevice, s->stream));
-            CUDA_TRY(s, cudaMemcpyAsync(s->w[0], c + 2 * level_bytes + state_bytes, state_bytes,
-                                        cudaMemcpyDeviceToDevice, s->stream));
-        }
-        return FDTD_OK;
-    };
+    // The matched layer: its factors of each step of a segment, and its gradient's sums per cell.
+    const uint64_t Lc = s->layers;
+    T *traj_layer = nullptr;
+    double *g_layer = nullptr;
+    if (Lc) {
+        if ((rc = scratch.take(e * kLayerFactors * Lc * segment, &p))) return rc;
+        traj_layer = static_cast<T *>(p);
+        if ((rc = scratch.take(sizeof(double) * kLayerFactors * Lc, &p))) return rc;
+        g_layer = static_cast<double *>(p);
+    }
     // The forward pass from rest, keeping checkpoints[m] = the state at the start of segment m+1;
     // or, when the handle holds the tape of a run of this drive with these segments, its states.
     const bool taped = holds_tape(s, signal, steps, segment);
@@ -1235,9 +1465,9 @@ int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float
     for (uint64_t k = 0; !taped && k + 1 < segments; ++k) {
         if ((rc = dispatch(s, d_signal + k * segment, segment, d_out, segment)) != FDTD_OK) return rc;
         settle(s, segment);
-        if ((rc = scratch.take(2 * level_bytes + 2 * state_bytes, &p))) return rc;
+        if ((rc = scratch.take(checkpoint_bytes(s), &p))) return rc;
         checkpoints.push_back(static_cast<char *>(p));
-        if ((rc = save(checkpoints.back())) != FDTD_OK) return rc;
+        if ((rc = save_checkpoint(s, checkpoints.back())) != FDTD_OK) return rc;
     }
     // The adjoint levels beyond the end, and their L~, are at rest; the sums start at 0.
     for (int k = 0; k < 2; ++k) {
@@ -1245,18 +1475,21 @@ int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float
         if (S) CUDA_TRY(s, cudaMemsetAsync(adj.om[k], 0, state_bytes, s->stream));
         if (K) CUDA_TRY(s, cudaMemsetAsync(adj.tilde[k], 0, sizeof(T) * K, s->stream));
     }
+    if (Lc) CUDA_TRY(s, cudaMemsetAsync(adj.carried, 0, e * 9 * Lc, s->stream));
     const AdjointTables &t = adj.t;
     const uint32_t row_blocks = (uint32_t)((std::max<uint64_t>(std::max<uint64_t>(K, S), 1) + kBlock - 1) / kBlock);
     const uint32_t special_blocks = (uint32_t)((K + kBlock - 1) / kBlock);
     const uint32_t corrected_blocks = (uint32_t)((t.corrected + kBlock - 1) / kBlock);
+    const uint32_t layer_blocks = (uint32_t)((Lc + kBlock - 1) / kBlock);
     const uint32_t smem = s->scaled ? Stage<T, true>::smem : Stage<T, false>::smem;
     int x = 0;  // lam[x], om[x]: level n+1; lam[1-x], om[1-x]: level n+2, then level n
     // A segment's recomputation (the dispatch of its steps, recording the special rows), and its
     // reverse steps.
     auto recompute = [&](uint64_t count) -> int {
         s->record_u = traj_u, s->record_w = traj_w, s->record_offset = 2, s->record_probes = false;
+        s->record_layer = traj_layer;
         const int r = dispatch(s, seg_signal, count, d_out, segment);
-        s->record_u = s->record_w = nullptr, s->record_probes = true;
+        s->record_u = s->record_w = s->record_layer = nullptr, s->record_probes = true;
         return r;
     };
     auto reverse = [&](uint64_t count) -> int {
@@ -1272,24 +1505,32 @@ int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float
             T *tilde_out = static_cast<T *>(adj.tilde[1 - xx]);
             CUDA_TRY(s, cudaEventRecord(s->joined[0], s->stream));
             CUDA_TRY(s, cudaStreamWaitEvent(s->side, s->joined[0], 0));
-            if (special_blocks + corrected_blocks)
-                rows_adjoint_kernel<T><<<special_blocks + corrected_blocks, kBlock, 0, s->side>>>(
-                    t, special_blocks, lam_next, om_next, tilde, lam_out, om_out, traj_u, traj_w, (uint32_t)m, g[1], g[0],
-                    g[2], g[3], g[4], tilde_out, seg_dloss, segment, m);
+            T *hat = static_cast<T *>(adj.hat);
+            // The matched layer's hats of step m first (the gathers below read them).
+            if (layer_blocks)
+                layer_hat_kernel<T><<<layer_blocks, kBlock, 0, s->side>>>(
+                    t, lam_next, static_cast<T *>(adj.carried), hat, traj_layer + m * kLayerFactors * Lc, g_layer);
+            if (special_blocks + corrected_blocks + layer_blocks)
+                rows_adjoint_kernel<T><<<special_blocks + corrected_blocks + layer_blocks, kBlock, 0, s->side>>>(
+                    t, special_blocks, corrected_blocks, lam_next, om_next, tilde, hat, lam_out, om_out, traj_u, traj_w,
+                    (uint32_t)m, g[1], g[0], g[2], g[3], g[4], tilde_out, seg_dloss, segment, m);
             CUDA_TRY(s, cudaEventRecord(s->joined[1], s->side));
             if (s->bulk_blocks) {
                 // The forward sweep of the grid's own kind (with a speed field it steps v = s lam).
                 BulkArgs args = s->bulk;
                 args.a = lam_out;
+                args.tile_list = s->plain_tiles;
+                args.tiles = s->plain_count;
+                const uint32_t blocks = s->plain_count;
                 const CUtensorMap &mb = adj.lam_b[xx], &ma = adj.lam_a[1 - xx];
                 if (s->wide && s->scaled)
-                    bulk_kernel<T, true, true><<<s->bulk_blocks, kBlock, smem, s->stream>>>(mb, ma, adj.map_t, s->map_s, args);
+                    bulk_kernel<T, true, true><<<blocks, kBlock, smem, s->stream>>>(mb, ma, adj.map_t, adj.map_s, args);
                 else if (s->wide)
-                    bulk_kernel<T, true, false><<<s->bulk_blocks, kBlock, smem, s->stream>>>(mb, ma, adj.map_t, s->map_s, args);
+                    bulk_kernel<T, true, false><<<blocks, kBlock, smem, s->stream>>>(mb, ma, adj.map_t, adj.map_s, args);
                 else if (s->scaled)
-                    bulk_kernel<T, false, true><<<s->bulk_blocks, kBlock, smem, s->stream>>>(mb, ma, adj.map_t, s->map_s, args);
+                    bulk_kernel<T, false, true><<<blocks, kBlock, smem, s->stream>>>(mb, ma, adj.map_t, adj.map_s, args);
                 else
-                    bulk_kernel<T, false, false><<<s->bulk_blocks, kBlock, smem, s->stream>>>(mb, ma, adj.map_t, s->map_s, args);
+                    bulk_kernel<T, false, false><<<blocks, kBlock, smem, s->stream>>>(mb, ma, adj.map_t, adj.map_s, args);
             }
             CUDA_TRY(s, cudaStreamWaitEvent(s->stream, s->joined[1], 0));
             xx = 1 - xx;
@@ -1347,7 +1588,7 @@ int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float
         // Recompute the segment from its start, recording each level of the special rows.
         if (k == 0) {
             if ((rc = fdtd_reset(s)) != FDTD_OK) return rc;
-        } else if ((rc = restore(checkpoints[k - 1])) != FDTD_OK) {
+        } else if ((rc = restore_checkpoint(s, checkpoints[k - 1])) != FDTD_OK) {
             return rc;
         }
         // Level 0 is the segment's previous level, level 1 its current one, level l + 1 the one
@@ -1370,6 +1611,32 @@ int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float
     if ((rc = check_device_error(s)) != FDTD_OK) return rc;
     for (int k = 0; k < 5; ++k)
         if (grads[k] && g_len[k]) CUDA_TRY(s, cudaMemcpy(grads[k], g[k], sizeof(double) * g_len[k], cudaMemcpyDeviceToHost));
+    if (Lc) {
+        // The layer tables' gradient: each cell's sums added into its coordinates' entries.
+        std::vector<double> cell(kLayerFactors * Lc);
+        CUDA_TRY(s, cudaMemcpy(cell.data(), g_layer, sizeof(double) * cell.size(), cudaMemcpyDeviceToHost));
+        const uint64_t len[3] = {s->nx + 1, s->ny + 1, s->nz + 1};
+        uint64_t keep_at[6], push_at[6], at = 0;  // offsets of keep/keep_face (x, y, z), then push/push_face
+        for (int a = 0; a < 3; ++a) keep_at[2 * a] = at, at += len[a], keep_at[2 * a + 1] = at, at += len[a];
+        for (int a = 0; a < 3; ++a) push_at[2 * a] = at, at += len[a], push_at[2 * a + 1] = at, at += len[a];
+        s->layer_gradient.assign(at, 0.0);
+        double *out = s->layer_gradient.data();
+        for (uint64_t c = 0; c < Lc; ++c) {
+            const uint64_t i = s->layer_cells[c], z = i / (s->pitch * s->ny), r = i - z * s->pitch * s->ny;
+            const uint64_t y = r / s->pitch, coord[3] = {r - y * s->pitch, y, z};
+            for (int a = 0; a < 3; ++a) {
+                const double *f = cell.data() + (uint64_t)(6 * a) * Lc + c;
+                out[keep_at[2 * a] + coord[a]] += f[0];
+                out[push_at[2 * a] + coord[a]] += f[1 * Lc];
+                out[keep_at[2 * a + 1] + coord[a] + 1] += f[2 * Lc];
+                out[push_at[2 * a + 1] + coord[a] + 1] += f[3 * Lc];
+                out[keep_at[2 * a + 1] + coord[a]] += f[4 * Lc];
+                out[push_at[2 * a + 1] + coord[a]] += f[5 * Lc];
+            }
+        }
+    } else {
+        s->layer_gradient.clear();
+    }
     return fdtd_reset(s);
 }
 
@@ -1427,6 +1694,11 @@ size_t pool_bytes(const fdtd_solver *s, const AdjointLists &l, uint64_t steps, u
     list(l.coefs.size(), 8), list(l.special_read_start.size(), 4), list(l.corrected_read_start.size(), 4);
     list(l.masks.size(), 4), list(l.scales.size(), 4), list(l.types.size(), 1);
     list(l.read_probe.size(), 4), list(l.read_weight.size(), 8);
+    list(l.special_layer_mask.size(), 1), list(l.corrected_layer_mask.size(), 1), list(l.layer_mask.size(), 1);
+    list(l.layer_from_start.size(), 4), list(l.layer_from_row.size(), 4), list(l.layer_from_coef.size(), 8);
+    list(l.layer_read_start.size(), 4), list(l.layer_interior.size(), 1);
+    const uint64_t Lc = s->layers;
+    if (Lc) total += pool_round(e * 9 * Lc) + pool_round(e * 6 * n);
     total += 2 * (pool_round(e * n) + pool_round(e * S)) + 2 * pool_round(e * K);
     if (segment == 0 || segment > steps) segment = steps;
     const uint64_t segments = (steps + segment - 1) / segment;
@@ -1434,7 +1706,8 @@ size_t pool_bytes(const fdtd_solver *s, const AdjointLists &l, uint64_t steps, u
              pool_round(e * S * (segment + 2)) + pool_round(8 * P * segment) + pool_round(4 * segment) +
              pool_round(8 * P * segment);
     total += 2 * pool_round(8 * K) + 3 * pool_round(8 * S);
-    if (!taped) total += (segments - 1) * pool_round(2 * e * n + 2 * e * S);
+    if (Lc) total += pool_round(e * kLayerFactors * Lc * segment) + pool_round(8 * kLayerFactors * Lc);
+    if (!taped) total += (segments - 1) * pool_round(checkpoint_bytes(s));
     return total;
 }
 
@@ -1594,7 +1867,6 @@ int fdtd_run(fdtd_solver *s, const float *signal, uint64_t steps, double *out) {
     const bool taping = s->tape_segment && s->steps_done == 0;
     uint64_t tape_segment = taping ? std::min(s->tape_segment, steps) : 0;
     const size_t e = s->precision == FDTD_FP64 ? 8 : 4;
-    const uint64_t level_bytes = e * s->n_device, state_bytes = e * s->states;
     const uint64_t K = s->specials, S = s->states;
     bool keep_traj = false;
     if (taping) {
@@ -1606,7 +1878,9 @@ int fdtd_run(fdtd_solver *s, const float *signal, uint64_t steps, double *out) {
             CUDA_TRY(s, cudaMemGetInfo(&free_bytes, &total_bytes));
             budget = free_bytes / 2 + e * (K + S) * s->tape_levels;  // (what the tape holds already counts)
         }
-        keep_traj = K + S > 0 && e * (K + S) * (steps + 2) <= budget;
+        // (A grid with a matched layer keeps checkpoints: its gradient recomputes the layer's
+        // factors a segment at a time.)
+        keep_traj = K + S > 0 && !s->layers && e * (K + S) * (steps + 2) <= budget;
     }
     if (keep_traj) {
         int r;
@@ -1643,9 +1917,9 @@ int fdtd_run(fdtd_solver *s, const float *signal, uint64_t steps, double *out) {
         const uint64_t needed = (steps + tape_segment - 1) / tape_segment - 1;
         while (s->tape_checkpoints.size() < needed) {
             void *p = nullptr;
-            CUDA_TRY(s, cudaMalloc(&p, 2 * level_bytes + 2 * state_bytes));
+            CUDA_TRY(s, cudaMalloc(&p, checkpoint_bytes(s)));
             s->allocations.push_back(p);
-            s->device_bytes += 2 * level_bytes + 2 * state_bytes;
+            s->device_bytes += checkpoint_bytes(s);
             s->tape_checkpoints.push_back(p);
         }
     }
@@ -1679,14 +1953,7 @@ int fdtd_run(fdtd_solver *s, const float *signal, uint64_t steps, double *out) {
             }
             if (taping && !keep_traj && (at + chunk) % tape_segment == 0 && at + chunk < steps) {
                 char *c = static_cast<char *>(s->tape_checkpoints[(at + chunk) / tape_segment - 1]);
-                CUDA_TRY(s, cudaMemcpyAsync(c, s->u[1], level_bytes, cudaMemcpyDeviceToDevice, s->stream));
-                CUDA_TRY(s, cudaMemcpyAsync(c + level_bytes, s->u[0], level_bytes, cudaMemcpyDeviceToDevice, s->stream));
-                if (s->states) {
-                    CUDA_TRY(s, cudaMemcpyAsync(c + 2 * level_bytes, s->w[1], state_bytes, cudaMemcpyDeviceToDevice,
-                                                s->stream));
-                    CUDA_TRY(s, cudaMemcpyAsync(c + 2 * level_bytes + state_bytes, s->w[0], state_bytes,
-                                                cudaMemcpyDeviceToDevice, s->stream));
-                }
+                if ((rc = save_checkpoint(s, c)) != FDTD_OK) break;
             }
             if (s->probes) {
                 CUDA_TRY(s, cudaMemcpy2DAsync(s->stage_out + done, count * sizeof(double), s->d_rec,
@@ -1784,6 +2051,12 @@ int fdtd_set_coefficients(fdtd_solver *s, const float *coef_b, const float *coef
         if (!coef.empty())
             CUDA_TRY(s, cudaMemcpy(const_cast<double *>(t.corrected_coef), coef.data(), 8 * coef.size(),
                                    cudaMemcpyHostToDevice));
+        coef.resize(s->adjoint_layer_row.size());
+        for (size_t e = 0; e < coef.size(); ++e)
+            coef[e] = (double)coef_inv[s->adjoint_layer_row[e]] * s->adjoint_layer_base[e];
+        if (!coef.empty())
+            CUDA_TRY(s, cudaMemcpy(const_cast<double *>(t.layer_from_coef), coef.data(), 8 * coef.size(),
+                                   cudaMemcpyHostToDevice));
     }
     // (Copies from pageable memory may return before they land; the handle's streams do not wait
     // for the default stream.)
@@ -1834,6 +2107,30 @@ int fdtd_set_launch(fdtd_solver *s, int layer_per_sm, int special_per_sm) {
     return FDTD_OK;
 }
 
+int fdtd_set_tiles(fdtd_solver *s, int shape, uint64_t planes) {
+    if (!s) return set_global(FDTD_EINVAL, "no solver");
+    if (shape < 0 || shape >= kShapes) return fail(s, FDTD_EINVAL, "the tile shape is an index 0 to 3");
+    if (planes < 1 || planes > 1024) return fail(s, FDTD_EINVAL, "planes a tile are 1 to 1024");
+    if (!s->bulk_tiles) return FDTD_OK;  // no interior cells: no sweep
+    if (s->shape_per_sm[shape] < 1) return fail(s, FDTD_EINVAL, "the tile shape does not fit a multiprocessor here");
+    DeviceGuard guard(s->device);
+    for (cudaStream_t stream : {s->stream, s->side, s->layer_stream}) CUDA_TRY(s, cudaStreamSynchronize(stream));
+    Kept{s}.drop_graphs();
+    return use_shape(s, shape, planes);
+}
+
+int fdtd_get_tiles(const fdtd_solver *s, fdtd_tiles *out) {
+    if (!s || !out) return set_global(FDTD_EINVAL, "no solver or no output");
+    out->shape = s->bulk_shape;
+    out->tile_x = kShapeInfo[s->bulk_shape].tx;
+    out->tile_y = kShapeInfo[s->bulk_shape].ty;
+    out->stages = kShapeInfo[s->bulk_shape].stages;
+    out->planes = s->bulk_chunk;
+    out->tiles = s->bulk_tiles;
+    out->blocks_per_sm = s->shape_per_sm[s->bulk_shape];
+    return FDTD_OK;
+}
+
 int fdtd_autotune(fdtd_solver *s, uint64_t trial_steps, int *layer_per_sm, int *special_per_sm) {
     if (!s) return set_global(FDTD_EINVAL, "no solver");
     if (s->steps_done != 0) return fail(s, FDTD_EINVAL, "fdtd_autotune runs from rest (after fdtd_create or fdtd_reset)");
@@ -1855,25 +2152,51 @@ int fdtd_autotune(fdtd_solver *s, uint64_t trial_steps, int *layer_per_sm, int *
     CUDA_TRY(s, cudaEventCreate(&end));
     const bool timing = s->timing;
     s->timing = false;
+    // Times trial_steps steps of the handle's present choice (one untimed dispatch first); ms < 0
+    // when it could not run.
+    auto trial = [&](float &ms) -> int {
+        ms = -1.0f;
+        for (int pass = 0; pass < 2; ++pass) {
+            if (pass == 1) CUDA_TRY(s, cudaEventRecord(start, s->stream));
+            const int r = dispatch(s, static_cast<const float *>(sig), trial_steps, static_cast<double *>(rec), trial_steps);
+            if (r != FDTD_OK) return r;
+            settle(s, trial_steps);
+        }
+        CUDA_TRY(s, cudaEventRecord(end, s->stream));
+        CUDA_TRY(s, cudaEventSynchronize(end));
+        CUDA_TRY(s, cudaEventElapsedTime(&ms, start, end));
+        return FDTD_OK;
+    };
+    // First the sweep's tile shape and planes a tile (the default chunk, half and twice it, within
+    // 8 to 64), with the layer and special launches as they are; then those given the best tiles.
+    if (s->bulk_tiles) {
+        const uint64_t base = default_chunk(s);
+        float best_tiles = -1.0f;
+        int best_shape = s->bulk_shape;
+        uint64_t best_chunk = s->bulk_chunk;
+        for (int shape = 0; shape < kShapes && rc == FDTD_OK; ++shape) {
+            if (s->shape_per_sm[shape] < 1) continue;  // does not fit an SM in this precision
+            for (uint64_t chunk : {base / 2, base, base * 2}) {
+                if (chunk < 8 || chunk > 64) continue;
+                if ((rc = use_shape(s, shape, chunk)) != FDTD_OK) break;
+                float ms;
+                if ((rc = trial(ms)) != FDTD_OK) break;
+                if (best_tiles < 0.0f || ms < best_tiles) best_tiles = ms, best_shape = shape, best_chunk = chunk;
+            }
+        }
+        if (rc == FDTD_OK) rc = use_shape(s, best_shape, best_chunk);
+    }
     const int layers[] = {4, 8, 12, 16, 0}, specials[] = {2, 4, 8, 0};
     float best = -1.0f;
     int best_layer = s->layer_per_sm, best_special = s->special_per_sm;
     for (int l : layers) {
+        if (rc != FDTD_OK) break;
         if (!s->layers && l != layers[0]) continue;
         for (int k : specials) {
             if (!s->specials && k != specials[0]) continue;
             s->layer_per_sm = l, s->special_per_sm = k;
-            // One untimed dispatch, then the timed one.
-            for (int pass = 0; pass < 2 && rc == FDTD_OK; ++pass) {
-                if (pass == 1) CUDA_TRY(s, cudaEventRecord(start, s->stream));
-                rc = dispatch(s, static_cast<const float *>(sig), trial_steps, static_cast<double *>(rec), trial_steps);
-                if (rc == FDTD_OK) settle(s, trial_steps);
-            }
-            if (rc != FDTD_OK) break;
-            CUDA_TRY(s, cudaEventRecord(end, s->stream));
-            CUDA_TRY(s, cudaEventSynchronize(end));
-            float ms = 0.0f;
-            CUDA_TRY(s, cudaEventElapsedTime(&ms, start, end));
+            float ms;
+            if ((rc = trial(ms)) != FDTD_OK) break;
             if (best < 0.0f || ms < best) best = ms, best_layer = l, best_special = k;
         }
         if (rc != FDTD_OK) break;
@@ -1951,6 +2274,16 @@ int fdtd_gradient(fdtd_solver *s, const float *signal, uint64_t steps, const dou
     return s->precision == FDTD_FP64
                ? gradient<double>(s, s->adjoint, kept, signal, steps, dloss_dy, segment, grads, true)
                : gradient<float>(s, s->adjoint, kept, signal, steps, dloss_dy, segment, grads, true);
+}
+
+int fdtd_layer_gradient(const fdtd_solver *s, double *tables) {
+    if (!s) return set_global(FDTD_EINVAL, "no solver");
+    if (!tables) return set_global(FDTD_EINVAL, "no output");
+    if (s->layer_gradient.empty())
+        return set_global(FDTD_EINVAL, "no gradient of the matched layer's tables: the grid has no layer, or no "
+                                       "gradient was taken since the handle was made");
+    std::memcpy(tables, s->layer_gradient.data(), sizeof(double) * s->layer_gradient.size());
+    return FDTD_OK;
 }
 
 int fdtd_reset(fdtd_solver *s) {

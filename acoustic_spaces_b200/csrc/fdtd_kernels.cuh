@@ -35,38 +35,67 @@ constexpr int kSolid = 0, kInterior = 1, kSpecial = 2, kLayer = 3;
 constexpr int kBlock = 128;  // threads per block of every kernel
 
 // ---- the bulk sweep's tiles ------------------------------------------------------------------
-constexpr int kTX = 64;                         // cells of a tile along x
-constexpr int kTY = 16;                         // rows of a tile along y
 constexpr int kHX = 4;                          // x halo of the pressure tile: 16 bytes of floats
-constexpr int kBX = kTX + 2 * kHX;              // 72: pressure tile width
-constexpr int kBY = kTY + 2;                    // 18: pressure tile rows (one halo row each side)
-constexpr int kRowsPerThread = kTX * kTY / kBlock;  // 8 rows of one column per thread
-constexpr int kAhead = 2;                       // planes loaded ahead of the three in use
-constexpr int kStages = kAhead + 3;             // ring of plane stages in shared memory
 constexpr uint32_t kSpinLimit = 1u << 24;       // bounded waits: then the block gives up
 constexpr int kLayerPerSm = 8;                  // blocks an SM of the matched-layer kernel
 constexpr int kSpecialPerSm = 4;                // blocks an SM of the special rows' kernel
+
+// A tile shape of the bulk sweep: TX x TY cells a plane, a ring of STAGES plane stages (the three
+// in use and STAGES - 3 loaded ahead). Each of the block's threads updates ROWS rows of one column.
+template <int TX_, int TY_, int STAGES_>
+struct Shape {
+    static constexpr int TX = TX_, TY = TY_, STAGES = STAGES_;
+    static constexpr int BX = TX + 2 * kHX;  // pressure tile width (x halo each side)
+    static constexpr int BY = TY + 2;        // pressure tile rows (one halo row each side)
+    static constexpr int ROWS = TX * TY / kBlock;
+    static constexpr int AHEAD = STAGES - 3;
+    static_assert(TX % 16 == 0 && kBlock % TX == 0 && (TX * TY) % kBlock == 0 && STAGES >= 4, "tile shape");
+};
+
+// The shapes the library is built with (fdtd_autotune picks one per grid; shape 0 by default):
+// 64 x 16 with 5 stages (4 blocks of 52 KB an SM in FP32), 128 x 16 and 64 x 32 with 4 stages (2
+// blocks of 80 KB: fewer halo cells a cell, 1.19x against 1.27x), and 32 x 32 with 5 (4 blocks).
+using Shape0 = Shape<64, 16, 5>;
+using Shape1 = Shape<128, 16, 4>;
+using Shape2 = Shape<64, 32, 4>;
+using Shape3 = Shape<32, 32, 5>;
+constexpr int kShapes = 4;
+struct ShapeInfo {
+    int tx, ty, stages;
+};
+constexpr ShapeInfo kShapeInfo[kShapes] = {{Shape0::TX, Shape0::TY, Shape0::STAGES},
+                                           {Shape1::TX, Shape1::TY, Shape1::STAGES},
+                                           {Shape2::TX, Shape2::TY, Shape2::STAGES},
+                                           {Shape3::TX, Shape3::TY, Shape3::STAGES}};
+// The default shape's sizes (the adjoint's sweep keeps them).
+constexpr int kTX = Shape0::TX, kTY = Shape0::TY, kBX = Shape0::BX, kBY = Shape0::BY;
 
 constexpr uint32_t align128(uint32_t v) { return (v + 127u) & ~127u; }
 
 // One stage of the ring: plane k's pressure tile with halos, and its previous pressure, cell
 // types and (with a speed field) scales over the tile's own cells.
-template <typename T, bool SCALED>
+template <typename T, bool SCALED, class SH = Shape0>
 struct Stage {
-    static constexpr uint32_t b_bytes = align128(kBY * kBX * sizeof(T));
-    static constexpr uint32_t a_bytes = align128(kTY * kTX * sizeof(T));
-    static constexpr uint32_t t_bytes = align128(kTY * kTX);
-    static constexpr uint32_t s_bytes = SCALED ? align128(kTY * kTX * 4) : 0;
+    static constexpr uint32_t b_bytes = align128(SH::BY * SH::BX * sizeof(T));
+    static constexpr uint32_t a_bytes = align128(SH::TY * SH::TX * sizeof(T));
+    static constexpr uint32_t t_bytes = align128(SH::TY * SH::TX);
+    static constexpr uint32_t s_bytes = SCALED ? align128(SH::TY * SH::TX * 4) : 0;
     static constexpr uint32_t b_off = 0;
     static constexpr uint32_t a_off = b_off + b_bytes;
     static constexpr uint32_t t_off = a_off + a_bytes;
     static constexpr uint32_t s_off = t_off + t_bytes;
     static constexpr uint32_t bytes = s_off + s_bytes;
-    // What the four copies of a stage write (the boxes, zero-filled where they leave the grid).
+    // What the copies of a stage write (the boxes, zero-filled where they leave the grid); a tile
+    // whose cells are all interior loads no types (kFullTile).
     static constexpr uint32_t tx_bytes =
-        kBY * kBX * sizeof(T) + kTY * kTX * sizeof(T) + kTY * kTX + (SCALED ? kTY * kTX * 4 : 0);
-    static constexpr uint32_t smem = kStages * bytes + 8 * kStages;  // + the stages' mbarriers
+        SH::BY * SH::BX * sizeof(T) + SH::TY * SH::TX * sizeof(T) + SH::TY * SH::TX + (SCALED ? SH::TY * SH::TX * 4 : 0);
+    static constexpr uint32_t tx_bytes_full = tx_bytes - SH::TY * SH::TX;
+    static constexpr uint32_t smem = SH::STAGES * bytes + 8 * SH::STAGES;  // + the stages' mbarriers
 };
+
+// A tile list entry's w holds z_end, with this bit set when every cell of the tile, in every one
+// of its planes, is interior: its planes' stages then carry no cell types.
+constexpr int kFullTile = 1 << 30;
 
 struct BulkArgs {
     void *a;  // the previous pressure, overwritten with the next (T)
@@ -74,8 +103,8 @@ struct BulkArgs {
     float residual;  // COMP: the constant mode's residual (with a speed field, per unit scale)
     uint32_t pitch, ny;
     uint32_t xa, y0, z0, x1, y1, z1;  // tiles start at xa (16-aligned), y0, z0; the box ends x1, y1, z1
-    // The tiles that hold interior cells: {x, y, z0, z_end} each, x 16-aligned; a tile spans
-    // kTX x kTY cells from (x, y) and the planes z0 .. z_end-1.
+    // The tiles that hold interior cells: {x, y, z0, z_end | kFullTile if all interior} each, x
+    // 16-aligned; a tile spans the shape's TX x TY cells from (x, y) and the planes z0 .. z_end-1.
     const int4 *tile_list;
     uint32_t tiles;
     float axial, diagonal, centre, total;
@@ -153,33 +182,36 @@ __global__ void wait_test_kernel(const unsigned int *flag, uint32_t spins, unsig
 
 // ---- interior air ------------------------------------------------------------------------------
 
-// Interior air (fdtd.hpp:242-288). The interior cells are covered by tiles of kTX x kTY cells by a
-// chunk of planes along z (a list, only tiles that hold interior cells); each block takes tiles
+// Interior air (fdtd.hpp:242-288). The interior cells are covered by tiles of SH::TX x SH::TY cells
+// by a chunk of planes along z (a list, only tiles that hold interior cells); each block takes tiles
 // blockIdx.x, + gridDim.x, ... and marches each along z. Its planes' stages — plane k's pressure
 // tile with halos, previous pressure, types and scales — form one sequence over all its tiles:
-// tile m's stages are planes z0-1 .. z_end. Thread 0 issues the sequence with TMA, kAhead stages
-// ahead of the three in use (across tile boundaries too), into a ring of kStages slots in shared
+// tile m's stages are planes z0-1 .. z_end. Thread 0 issues the sequence with TMA, SH::AHEAD stages
+// ahead of the three in use (across tile boundaries too), into a ring of SH::STAGES slots in shared
 // memory, each completed on its slot's mbarrier; the block updates plane z from the stages of
-// planes z-1, z and z+1, each thread 8 rows of one column, and stores the new pressure of the
-// interior cells. Every wait is bounded: a block that gives up sets the error flag, lets its
-// copies in flight land, and stops.
+// planes z-1, z and z+1, each thread SH::ROWS rows of one column, and stores the new pressure of the
+// interior cells. A tile whose cells are all interior (kFullTile) loads no cell types and checks
+// none. Every wait is bounded: a block that gives up sets the error flag, lets its copies in flight
+// land, and stops.
 // The reference's sums in its order: x-1, x+1, y-1, y+1, z-1, z+1, then the twelve edges.
 struct TileSpan {
     int xt, yt, z0, z_end;  // the tile's corner and its planes z0 .. z_end-1
+    bool full;              // every cell of the tile interior
 };
 
 __device__ __forceinline__ TileSpan tile_span(const BulkArgs &p, uint32_t tile) {
     const int4 t = p.tile_list[tile];
-    return TileSpan{t.x, t.y, t.z, t.w};
+    return TileSpan{t.x, t.y, t.z, t.w & (kFullTile - 1), (t.w & kFullTile) != 0};
 }
 
-template <typename T, bool WIDE, bool SCALED, bool COMP = false>
+template <typename T, bool WIDE, bool SCALED, bool COMP = false, class SH = Shape0>
 __global__ void __launch_bounds__(kBlock) bulk_kernel(const __grid_constant__ CUtensorMap map_b,
                                                       const __grid_constant__ CUtensorMap map_a,
                                                       const __grid_constant__ CUtensorMap map_t,
                                                       const __grid_constant__ CUtensorMap map_s,
                                                       const BulkArgs p) {
-    using S = Stage<T, SCALED>;
+    using S = Stage<T, SCALED, SH>;
+    constexpr int kStages = SH::STAGES, TX = SH::TX, BX = SH::BX;
     extern __shared__ __align__(128) unsigned char smem[];
     const uint32_t base = smem_address(smem);
     const uint32_t bars = base + kStages * S::bytes;
@@ -199,8 +231,8 @@ __global__ void __launch_bounds__(kBlock) bulk_kernel(const __grid_constant__ CU
     int p_k = p_span.z0 - 1;
     int issued = 0;
     const T axial = (T)p.axial, centre = (T)p.centre, diagonal = (T)p.diagonal, total = (T)p.total;
-    const int xl = threadIdx.x % kTX;
-    const int r0 = (threadIdx.x / kTX) * kRowsPerThread;
+    const int xl = threadIdx.x % TX;
+    const int r0 = (threadIdx.x / TX) * SH::ROWS;
     T *__restrict__ a = static_cast<T *>(p.a);
     T *__restrict__ dd = static_cast<T *>(p.d);
     const T residual = (T)p.residual;
@@ -215,17 +247,17 @@ __global__ void __launch_bounds__(kBlock) bulk_kernel(const __grid_constant__ CU
         for (int z = t.z0; z < t.z_end; ++z) {
             const int centre_at = position + (z - t.z0 + 1);  // plane z's stage
             // Refill the slots whose stages are over (up to plane z-2's) with the stages up to
-            // kAhead beyond plane z+1's.
+            // SH::AHEAD beyond plane z+1's.
             if (threadIdx.x == 0) {
                 fence_proxy_async();
-                const int target = centre_at + 2 + kAhead;  // issue stages .. target-1
+                const int target = centre_at + 2 + SH::AHEAD;  // issue stages .. target-1
                 while (issued < target && p_tile < tiles) {
                     const int slot = issued % kStages;
                     const uint32_t stage = base + slot * S::bytes, bar = bars + 8 * slot;
-                    mbar_expect_tx(bar, S::tx_bytes);
+                    mbar_expect_tx(bar, p_span.full ? S::tx_bytes_full : S::tx_bytes);
                     tma_load_3d(stage + S::b_off, &map_b, p_span.xt - kHX, p_span.yt - 1, p_k, bar);
                     tma_load_3d(stage + S::a_off, &map_a, p_span.xt, p_span.yt, p_k, bar);
-                    tma_load_3d(stage + S::t_off, &map_t, p_span.xt, p_span.yt, p_k, bar);
+                    if (!p_span.full) tma_load_3d(stage + S::t_off, &map_t, p_span.xt, p_span.yt, p_k, bar);
                     if (SCALED) tma_load_3d(stage + S::s_off, &map_s, p_span.xt, p_span.yt, p_k, bar);
                     ++issued;
                     if (++p_k > p_span.z_end) {
@@ -248,25 +280,25 @@ __global__ void __launch_bounds__(kBlock) bulk_kernel(const __grid_constant__ CU
                 const uint8_t *pt = reinterpret_cast<const uint8_t *>(s0 + S::t_off);
                 const float *ps = reinterpret_cast<const float *>(s0 + S::s_off);
 #pragma unroll
-                for (int r = 0; r < kRowsPerThread; ++r) {
+                for (int r = 0; r < SH::ROWS; ++r) {
                     const int yl = r0 + r;
-                    const int c = yl * kTX + xl;
+                    const int c = yl * TX + xl;
                     // Outside the interior cells' box, and outside the grid (zero fill), no cell
                     // is interior.
-                    if (pt[c] != kInterior) continue;
-                    const int q = (yl + 1) * kBX + (xl + kHX);
+                    if (!t.full && pt[c] != kInterior) continue;
+                    const int q = (yl + 1) * BX + (xl + kHX);
                     const T here = b0[q];
                     const uint64_t at = (uint64_t)x + (uint64_t)(t.yt + yl) * p.pitch + (uint64_t)z * plane;
                     if (COMP) {
                         // pa holds the increment; the neighbours as differences, in the sum's order.
-                        const T sum = (b0[q - 1] - here) + (b0[q + 1] - here) + (b0[q - kBX] - here) +
-                                      (b0[q + kBX] - here) + (bm[q] - here) + (bp[q] - here);
+                        const T sum = (b0[q - 1] - here) + (b0[q + 1] - here) + (b0[q - BX] - here) +
+                                      (b0[q + BX] - here) + (bm[q] - here) + (bp[q] - here);
                         T edges = (T)0;
                         if (WIDE)
-                            edges = (b0[q - 1 - kBX] - here) + (b0[q + 1 - kBX] - here) + (b0[q - 1 + kBX] - here) +
-                                    (b0[q + 1 + kBX] - here) + (bm[q - 1] - here) + (bm[q + 1] - here) +
-                                    (bp[q - 1] - here) + (bp[q + 1] - here) + (bm[q - kBX] - here) +
-                                    (bm[q + kBX] - here) + (bp[q - kBX] - here) + (bp[q + kBX] - here);
+                            edges = (b0[q - 1 - BX] - here) + (b0[q + 1 - BX] - here) + (b0[q - 1 + BX] - here) +
+                                    (b0[q + 1 + BX] - here) + (bm[q - 1] - here) + (bm[q + 1] - here) +
+                                    (bp[q - 1] - here) + (bp[q + 1] - here) + (bm[q - BX] - here) +
+                                    (bm[q + BX] - here) + (bp[q - BX] - here) + (bp[q + BX] - here);
                         T step;
                         if (SCALED) {
                             const T sc = (T)ps[c];
@@ -280,12 +312,12 @@ __global__ void __launch_bounds__(kBlock) bulk_kernel(const __grid_constant__ CU
                         dd[at] = step;
                         continue;
                     }
-                    const T sum = b0[q - 1] + b0[q + 1] + b0[q - kBX] + b0[q + kBX] + bm[q] + bp[q];
+                    const T sum = b0[q - 1] + b0[q + 1] + b0[q - BX] + b0[q + BX] + bm[q] + bp[q];
                     T next;
                     if (WIDE) {
-                        const T edges = b0[q - 1 - kBX] + b0[q + 1 - kBX] + b0[q - 1 + kBX] + b0[q + 1 + kBX] +
+                        const T edges = b0[q - 1 - BX] + b0[q + 1 - BX] + b0[q - 1 + BX] + b0[q + 1 + BX] +
                                         bm[q - 1] + bm[q + 1] + bp[q - 1] + bp[q + 1] +
-                                        bm[q - kBX] + bm[q + kBX] + bp[q - kBX] + bp[q + kBX];
+                                        bm[q - BX] + bm[q + BX] + bp[q - BX] + bp[q + BX];
                         if (SCALED) {
                             const T sc = (T)ps[c];
                             next = ((T)2 - total * sc) * here + (sc * axial) * sum + (sc * diagonal) * edges - pa[c];
@@ -367,6 +399,10 @@ struct Fields {
     uint64_t out_stride;
     T *traj_u;         // when not null: each special row's new pressure at traj_u[k] (the gradient's
     T *traj_w;         // recomputation), and each branch state's new velocity at traj_w[j]
+    // When not null (the gradient's recomputation of a grid with a matched layer): each layer
+    // cell's six factors per axis of the tables' gradient, at traj_layer[f * layers + c]
+    // (fdtd_adjoint.cuh: q, hi' - lo', hi, b_(i+st) - b_i, lo, b_i - b_(i-st) per axis).
+    T *traj_layer;
 };
 
 // Special rows (fdtd.hpp:860-881), one a thread: its links, its branch states' flow, the update,
@@ -495,6 +531,15 @@ __device__ __forceinline__ void layer_cell(const Tables &g, const Fields<T> &f, 
             total += (keep - (T)1) * part[axis] - flux;
             part[axis] = keep * part[axis] - flux;
             continue;
+        }
+        if (f.traj_layer) {
+            T *o = f.traj_layer + (uint64_t)(6 * axis) * L + c;
+            o[0] = part[axis];
+            o[(uint64_t)1 * L] = above[axis] - below[axis];
+            o[(uint64_t)2 * L] = old_above[axis];
+            o[(uint64_t)3 * L] = hi[axis] - here;
+            o[(uint64_t)4 * L] = old_below[axis];
+            o[(uint64_t)5 * L] = here - lo[axis];
         }
         if (SCALED) {
             part[axis] = (T)c0[axis].x * part[axis] - ((T)c0[axis].y * scale) * (above[axis] - below[axis]);

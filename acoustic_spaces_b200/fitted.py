@@ -1,0 +1,758 @@
+"""Fitted (cut-cell) walls: the fit of a convex room on the GPU, and the grid's layout from a fit.
+
+The reference lays fitted walls out in two stages (cpp/include/acoustic_spaces/fdtd.hpp:929-1264
+of naelolaiz/acoustic-spaces): the fit (cut_cells.hpp, CutCells) measures, for every row — an air
+cell that owns cut air — its air volume V, its open area towards each of its 18 neighbours A_k,
+its wall area per material W_m and the thickness of the slivers of air it owns through each face;
+then set_up_fitted turns those into special rows: link weights lowered(g A_k / V), the wall term
+(L/2) sum_m W_m (beta_m + sum_j 1 / (2 a_j)) / V with one branch state per branch, the sliver rule
+that scales the link opposite a sliver by w(1 + f) = 3 l / ((l + 1/2)(l + 1)), l = 1 + f, and the
+clamp V >= (g/2) sum_k A_k.
+
+* :func:`set_up_fitted` restates the second stage over any fit: fed the reference's own fit (its
+  CutFit) it gives the reference's layout array for array (tests/test_fitted.py).
+* :func:`convex_fit` is this library's first stage for convex rooms of planar walls, one face of
+  which may be open: the cut of every cell by the walls in double precision on the GPU
+  (``fdtd_cut_convex``), then on the host each cut cell's air on each side of the walls as a
+  region, the reference's owner rule (a region holding an air cell's centre is that cell's; each
+  other region, round by round, goes to the air cell whose regions it shares the most open area
+  with, ties to the lowest cell) and the rows' sums. Its regions are the cell's air inside and
+  outside the room — where the reference's exact fit splits a cell at a room's edge along each
+  wall plane into further convex pieces, this fit keeps the air outside the room as one region —
+  so its rows agree with the reference's away from the room's edges and corners, and differ in
+  those cells (the measured agreement: tests/test_fitted.py).
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import layouts as L
+
+#: The directions of fdtd.hpp:924-927: six axial, then the twelve edge neighbours.
+STEPS = np.array(
+    [(-1, 0, 0), (1, 0, 0), (0, -1, 0), (0, 1, 0), (0, 0, -1), (0, 0, 1), (-1, -1, 0), (1, -1, 0), (-1, 1, 0),
+     (1, 1, 0), (-1, 0, -1), (1, 0, -1), (-1, 0, 1), (1, 0, 1), (0, -1, -1), (0, 1, -1), (0, -1, 1), (0, 1, 1)],
+    np.int64,
+)  # fmt: skip
+#: The fit's kinds of cell (cut_cells.hpp:1042).
+SOLID, AIR, LAYER = 0, 1, 2
+
+
+def opposite(k: int) -> int:
+    """The direction opposite k (fdtd.hpp:929)."""
+    return k ^ 1 if k < 6 else 6 + 4 * ((k - 6) // 4) + 3 - (k - 6) % 4
+
+
+def sliver_factor(f):
+    """The sliver rule's factor for a sliver f cells thick (fdtd.hpp:950-954)."""
+    lam = 1.0 + np.asarray(f, np.float64)
+    return 3.0 * lam / ((lam + 0.5) * (lam + 1.0))
+
+
+@dataclass
+class Fit:
+    """What a fit gives, as the reference's CutFit names it: the rows (ascending cells), each
+    row's ``air_volume`` (cells^3), ``open_area`` (rows, 18), ``wall_area`` (rows, materials + 1;
+    the last column the grid's edge) and ``sliver`` (rows, 6); every cell's kind ``air``
+    (SOLID, AIR, LAYER); and each cell's ``widths`` per axis on the fit's lattice (cells)."""
+
+    cell: np.ndarray
+    air_volume: np.ndarray
+    open_area: np.ndarray
+    wall_area: np.ndarray
+    sliver: np.ndarray
+    air: np.ndarray
+    widths: tuple[np.ndarray, np.ndarray, np.ndarray]
+
+
+def set_up_fitted(
+    fit: Fit,
+    grid: L.Grid,
+    materials: list[L.Material | None],
+    source_cells: list[tuple[int, float]],
+    probe_cells: list[list[tuple[int, float]]],
+    *,
+    layer: int = 0,
+    layer_damping: float = 0.0,
+    edge_admittance: float = 1.0,
+) -> dict[str, np.ndarray]:
+    """The layout of the grid from ``fit`` with the reference's rules for fitted walls
+    (set_up_fitted, fdtd.hpp:970-1217; add_special_fitted, fdtd.hpp:1219-1264), the 7-point
+    stencil and no speed field (as the reference's fitted walls take them): ``materials`` in the
+    fit's columns (None: a material of no admittance), the source's and the probes' cells with
+    their weights. Vectorised over the rows."""
+    nx, ny, nz = grid.shape
+    n = nx * ny * nz
+    sy, sz = nx, nx * ny
+    offsets = STEPS[:, 0] + STEPS[:, 1] * sy + STEPS[:, 2] * sz
+    idx = np.arange(n, dtype=np.int64)
+    x, y, z = idx % nx, (idx // nx) % ny, idx // sz
+
+    # The cells' kinds (fdtd.hpp:976-995).
+    types = np.zeros(n, np.uint8)
+    types[fit.air == AIR] = 1
+    types[fit.air == LAYER] = 3
+    layer_cells = np.flatnonzero(types == 3).astype(np.int64)
+    edge = (x == 0) | (y == 0) | (z == 0) | (x == nx - 1) | (y == ny - 1) | (z == nz - 1)
+
+    # The stencil (set_up_stencil, fdtd.hpp:1649-1670).
+    exact = 1.0 / 3.0
+    plane = exact / (2.0 * math.sqrt(exact))  # L/2: a whole cell face's boundary weight
+    half_g = exact / 2.0
+    weight_plain = np.float32(L.lowered(exact))
+    total_plain = 0.0
+    for _ in range(6):
+        total_plain += float(weight_plain)
+    centre = np.float32(2.0 - total_plain)
+
+    # Materials and branches (fdtd.hpp:392-411).
+    M = fit.wall_area.shape[1] - 1
+    betas = np.zeros(M)
+    branch_rows, branch_owner = [], []
+    for m in range(M):
+        mat = materials[m] if m < len(materials) else None
+        if mat is None:
+            continue
+        betas[m] = mat.beta
+        for row in np.asarray(mat.branches, float).reshape(-1, 3):
+            branch_rows.append(row)
+            branch_owner.append(m)
+    branch_rows = np.array(branch_rows, np.float64).reshape(-1, 3)
+    branch_owner = np.array(branch_owner, np.int64)
+    branch_a = branch_rows[:, 0] + 0.5 * branch_rows[:, 1] + 0.5 * branch_rows[:, 2]
+    if len(branch_a) and not np.all((branch_rows >= 0) & (branch_a[:, None] > 0)):
+        raise ValueError("a branch needs mass, resistance and stiffness >= 0")
+    material_branches = [np.flatnonzero(branch_owner == m) for m in range(M)]
+
+    rows = np.asarray(fit.cell, np.int64)
+    R = len(rows)
+
+    def row_of(cells):
+        cells = np.asarray(cells, np.int64)
+        at = np.searchsorted(rows, cells)
+        at_c = np.minimum(at, max(R - 1, 0))
+        hit = (at < R) & (rows[at_c] == cells) if R else np.zeros(len(cells), bool)
+        return np.where(hit, at_c, -1)
+
+    wx, wy, wz = (np.asarray(w, np.float64) for w in fit.widths)
+
+    def width(cells, a):
+        return (wx[cells % nx], wy[(cells // nx) % ny], wz[cells // sz])[a]
+
+    def cell_volume(cells):
+        return width(cells, 0) * width(cells, 1) * width(cells, 2)
+
+    def face_area(cells, a):
+        return width(cells, (a + 1) % 3) * width(cells, (a + 2) % 3)
+
+    # The sliver rule (fdtd.hpp:1019-1075): per row o and face k with a sliver of f > 0, the link
+    # between o and its neighbour m across the opposite face, scaled on both sides; where both
+    # cells' rules touch a link, the product of their factors (in ascending order of factor).
+    keys, facs = [], []
+    for k in range(6):
+        f = fit.sliver[:, k]
+        has = f > 0.0
+        o = rows[has]
+        m = o + offsets[opposite(k)]
+        ok = ~edge[m] & (types[m] != 0) & (types[m] != 3)
+        o, m, fk = o[ok], m[ok], f[has][ok]
+        keys.append(3 * np.minimum(o, m) + k // 2)
+        facs.append(sliver_factor(fk))
+    keys = np.concatenate(keys) if keys else np.zeros(0, np.int64)
+    facs = np.concatenate(facs) if facs else np.zeros(0)
+    order = np.lexsort((facs, keys))
+    keys, facs = keys[order], facs[order]
+    factor_keys, first = np.unique(keys, return_index=True)
+    factor_values = np.ones(len(factor_keys))
+    # products in sorted order, one factor at a time (each key has a handful)
+    counts = np.diff(np.concatenate([first, [len(keys)]]))
+    for step in range(int(counts.max()) if len(counts) else 0):
+        has = counts > step
+        factor_values[has] = factor_values[has] * facs[first[has] + step]
+    lower = factor_keys // 3
+    upper = lower + np.array([1, sy, sz], np.int64)[factor_keys % 3]
+    far = np.unique(np.concatenate([lower, upper]))
+    far = far[row_of(far) < 0]
+
+    def factor_of(i, j, axis):
+        key = 3 * np.minimum(i, j) + axis
+        at = np.searchsorted(factor_keys, key)
+        at_c = np.minimum(at, max(len(factor_keys) - 1, 0))
+        hit = (at < len(factor_keys)) & (factor_keys[at_c] == key) if len(factor_keys) else np.zeros(len(key), bool)
+        return np.where(hit, factor_values[at_c] if len(factor_keys) else 1.0, 1.0)
+
+    # The candidates in ascending order: the rows and the plain cells the sliver rule reaches.
+    cand = np.union1d(rows, far).astype(np.int64)
+    r_of = row_of(cand)
+    is_row = r_of >= 0
+    rc = np.maximum(r_of, 0)
+    room = (types == 1) | (types == 2)
+
+    # Each candidate's open area towards each direction (area_towards, fdtd.hpp:1087-1100).
+    area = np.zeros((len(cand), 18))
+    for k in range(18):
+        j = cand + offsets[k]
+        a = np.where(is_row, fit.open_area[rc, k] if R else 0.0, 0.0)
+        if k < 6:
+            plain = ~is_row & (types[cand] != 0) & ~edge[j] & (types[j] != 0)
+            a = np.where(plain, face_area(cand, k // 2), a)
+            touched = (a > 0.0) & room[cand] & room[j]
+            a = np.where(touched, a * factor_of(cand, j, k // 2), a)
+        area[:, k] = a
+    air_volume = np.where(is_row, fit.air_volume[rc] if R else 0.0, cell_volume(cand))
+
+    # The wall term and the branch states (fdtd.hpp:1106-1128), in material order.
+    wall = np.zeros(len(cand))
+    st_cand, st_branch, st_weight = [], [], []
+    for m in range(M):
+        W = np.where(is_row, fit.wall_area[rc, m] if R else 0.0, 0.0)
+        has = W > 0.0
+        weight = plane * W
+        wall = np.where(has, wall + weight * betas[m], wall)
+        for j in material_branches[m]:
+            wall = np.where(has, wall + weight * (0.5 / branch_a[j]), wall)
+            st_cand.append(np.flatnonzero(has))
+            st_branch.append(np.full(int(has.sum()), j, np.int64))
+            st_weight.append(weight[has])
+    edge_wall = np.where(is_row, fit.wall_area[rc, M] if R else 0.0, 0.0)
+    wall = np.where(edge_wall > 0.0, wall + plane * edge_wall * edge_admittance, wall)
+    total = np.zeros(len(cand))
+    for k in range(18):
+        total = total + area[:, k]
+    volume = np.maximum(air_volume, half_g * total)
+
+    # add_special_fitted (fdtd.hpp:1219-1264), s = 1, r = 1 / V.
+    r = 1.0 / volume
+    lw = np.zeros((len(cand), 18), np.float32)
+    link_total = np.zeros(len(cand))
+    for k in range(18):
+        has = area[:, k] > 0.0
+        w = L.lowered(exact * area[:, k] / volume)
+        lw[:, k] = np.where(has, w, np.float32(0.0))
+        link_total = link_total + np.where(has, lw[:, k].astype(np.float64), 0.0)
+    centre_d = 2.0 - link_total
+    coef_a = centre_d.astype(np.float32)
+    over = coef_a.astype(np.float64) > centre_d
+    coef_a = np.where(over, np.nextafter(coef_a, np.float32(-np.inf)), coef_a).astype(np.float32)
+    coef_b = (1.0 - r * wall).astype(np.float32)
+    coef_inv = (1.0 / (1.0 + r * wall)).astype(np.float32)
+    n_states = np.zeros(len(cand), np.int64)
+    for c in st_cand:
+        n_states += np.bincount(c, minlength=len(cand))
+    plain_links = np.all(lw[:, :6] == weight_plain, axis=1) & np.all(lw[:, 6:] == 0.0, axis=1)
+    spared = (n_states == 0) & (coef_a == centre) & (coef_b == 1.0) & (coef_inv == 1.0) & plain_links
+    kept = ~spared
+
+    special = cand[kept]
+    K = len(special)
+    volumes = list(volume[kept])
+    has_link = area[kept] > 0.0
+    link_direction = np.tile(np.arange(18, dtype=np.uint8), (K, 1))[has_link]
+    link_weight = lw[kept][has_link]
+    link_start = np.concatenate([[0], np.cumsum(has_link.sum(axis=1))]).astype(np.uint64)
+    # Branch states in row order, each row's in material then branch order.
+    if st_cand:
+        sc = np.concatenate(st_cand)
+        order = np.argsort(sc, kind="stable")
+        sc = sc[order]
+        sb = np.concatenate(st_branch)[order]
+        sw = np.concatenate(st_weight)[order]
+        keep_state = kept[sc]
+        sc, sb, sw = sc[keep_state], sb[keep_state], sw[keep_state]
+        state_weight = (r[sc] * sw).astype(np.float32)
+        per_row = np.bincount(np.searchsorted(np.flatnonzero(kept), sc), minlength=K)
+    else:
+        sb = np.zeros(0, np.int64)
+        state_weight = np.zeros(0, np.float32)
+        per_row = np.zeros(K, np.int64)
+    state_start = np.concatenate([[0], np.cumsum(per_row)]).astype(np.uint64)
+    types[special] = 2
+
+    # The source's cells (fdtd.hpp:1141-1163): a cell not yet special becomes special (a row that
+    # stayed plain with its own coefficients, any other cell with the interior's), each fed w / V.
+    special_list = list(special)
+    coef_a_l, coef_b_l, coef_inv_l = list(coef_a[kept]), list(coef_b[kept]), list(coef_inv[kept])
+    link_dir_l, link_w_l = [link_direction], [link_weight]
+    link_counts = list(has_link.sum(axis=1))
+    source = [np.float32(0.0)] * K
+    added: dict[int, int] = {}
+    for i, w in source_cells:
+        i = int(i)
+        k = int(np.searchsorted(special, i))
+        if not (k < K and special[k] == i):
+            k = added.get(i, -1)
+        if k < 0:
+            at = int(np.searchsorted(cand, i))
+            if at < len(cand) and cand[at] == i and is_row[at]:
+                # a row that stayed plain: its own coefficients (add_special_fitted, no spare)
+                hl = area[at] > 0.0
+                link_dir_l.append(np.arange(18, dtype=np.uint8)[hl])
+                link_w_l.append(lw[at][hl])
+                link_counts.append(int(hl.sum()))
+                coef_a_l.append(coef_a[at]), coef_b_l.append(coef_b[at]), coef_inv_l.append(coef_inv[at])
+                volumes.append(volume[at])
+            else:
+                # add_special(i, exact, 0): the interior's links and coefficients
+                link_dir_l.append(np.arange(6, dtype=np.uint8))
+                link_w_l.append(np.full(6, weight_plain, np.float32))
+                link_counts.append(6)
+                tot = 0.0
+                for _ in range(6):
+                    tot += exact
+                coef_a_l.append(np.float32(2.0 - tot * (1.0 - L.MARGIN)))
+                coef_b_l.append(np.float32(1.0)), coef_inv_l.append(np.float32(1.0))
+                volumes.append(float(cell_volume(np.array([i]))[0]))
+            types[i] = 2
+            k = len(special_list)
+            special_list.append(i)
+            source.append(np.float32(0.0))
+            added[i] = k
+        source[k] = np.float32(source[k] + np.float32(w / volumes[k]))
+    E = len(special_list) - K
+    state_start = np.concatenate([state_start, np.full(E, state_start[-1], np.uint64)])
+    link_start = np.concatenate([[0], np.cumsum(link_counts)]).astype(np.uint64)
+
+    layout: dict[str, np.ndarray] = {}
+    layout["shape"] = np.array(grid.shape, np.uint64)
+    layout["stencil"] = np.array([7], np.uint64)
+    layout["weights"] = np.full(6, weight_plain, np.float32)
+    layout["centre"] = np.array([centre], np.float32)
+    layout["total"] = np.array([total_plain], np.float32)
+    layout["scaled"] = np.array([0], np.uint64)
+    layout["scale"] = np.zeros(0, np.float32)
+    layout["layer_scale"] = np.zeros(0, np.float32)
+    layout["types"] = types
+    layout["special"] = np.array(special_list, np.int64)
+    layout["link_start"] = link_start
+    layout["link_direction"] = np.concatenate(link_dir_l).astype(np.uint8)
+    layout["link_weight"] = np.concatenate(link_w_l).astype(np.float32)
+    layout["coef_a"] = np.array(coef_a_l, np.float32)
+    layout["coef_b"] = np.array(coef_b_l, np.float32)
+    layout["coef_inv"] = np.array(coef_inv_l, np.float32)
+    layout["source"] = np.array(source, np.float32)
+    layout["state_start"] = state_start
+    layout["state_branch"] = sb.astype(np.int32)
+    layout["state_weight"] = state_weight
+    layout["branch_now"] = (2.0 * branch_rows[:, 0] / branch_a).astype(np.float32)
+    layout["branch_before"] = ((2.0 * branch_rows[:, 0] + branch_rows[:, 2]) / branch_a).astype(np.float32)
+    layout["branch_gain"] = (0.5 / branch_a).astype(np.float32)
+    layout["layer_cells"] = layer_cells
+    courant = math.sqrt(float(weight_plain))
+    for a, name in enumerate("xyz"):
+        if len(layer_cells):
+            ck, cp, fk, fp = L._layer_tables(grid.shape[a], layer, layer_damping, courant)
+        else:
+            ck = cp = fk = fp = np.zeros(0, np.float32)
+        layout[f"keep_{name}"], layout[f"push_{name}"] = ck, cp
+        layout[f"keep_face_{name}"], layout[f"push_face_{name}"] = fk, fp
+    starts, cells, weights = [0], [], []
+    for probe in probe_cells:
+        for i, w in probe:
+            cells.append(int(i))
+            weights.append(float(w))
+        starts.append(len(cells))
+    layout["probe_start"] = np.array(starts, np.uint64)
+    layout["probe_cells"] = np.array(cells, np.uint64)
+    layout["probe_weights"] = np.array(weights, np.float64)
+    layout["flow_mask"] = np.zeros(0, np.uint8)
+    return layout
+
+
+# ---- this library's fit of a convex room --------------------------------------------------------
+
+
+@dataclass
+class Cut:
+    """The cells the walls' planes cut (fdtd_cut_convex), ascending: each cell's air inside the
+    walls (cells^3), its faces' areas on that side (cells, 6), each plane's wall area in it, and
+    the area of the walls' planes between its two sides that no wall covers."""
+
+    cell: np.ndarray
+    volume: np.ndarray
+    face_area: np.ndarray
+    cap: np.ndarray
+    bare: np.ndarray
+
+
+def cut_room(room: L.Room, grid: L.Grid) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+    """The room's planes as the fit takes them: unit normals, offsets, and which are open."""
+    normals = np.ascontiguousarray(room.normals, np.float64)
+    offsets = np.ascontiguousarray(room.offsets, np.float64)
+    open_ = np.array([m is None for m in room.materials], np.uint8)
+    return normals, offsets, open_
+
+
+def cut_convex(room: L.Room, grid: L.Grid, device: int = 0) -> Cut:
+    """The FP64 cut of ``room``'s walls by ``grid``'s cells on the GPU (fdtd_cut_convex)."""
+    from . import _abi
+
+    lib = _abi.load_library()
+    normals, offsets, open_ = cut_room(room, grid)
+    r = _abi.FdtdCutRoom()
+    r.normals = normals.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    r.offsets = offsets.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    r.open = open_.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))
+    r.planes = len(offsets)
+    for a in range(3):
+        r.origin[a] = float(grid.origin[a])
+    r.cell = float(grid.cell)
+    r.nx, r.ny, r.nz = (int(v) for v in grid.shape)
+    out = _abi.FdtdCutCells()
+    status = lib.fdtd_cut_convex(ctypes.byref(r), int(device), ctypes.byref(out))
+    if status != _abi.FDTD_OK:
+        message = lib.fdtd_cut_error().decode()
+        if status == _abi.FDTD_EINVAL:
+            raise ValueError(message)
+        raise RuntimeError(message)
+    try:
+        return cut_from(out)
+    finally:
+        lib.fdtd_cut_free(ctypes.byref(out))
+
+
+def cut_from(out) -> Cut:
+    """A Cut from a filled ``fdtd_cut_cells`` (copied; ascending cells)."""
+    n, P = int(out.cells), int(out.planes)
+    cell = np.ctypeslib.as_array(out.cell, (max(n, 1),))[:n].copy()
+    volume = np.ctypeslib.as_array(out.volume, (max(n, 1),))[:n].copy()
+    face = np.ctypeslib.as_array(out.face_area, (max(n, 1) * 6,))[: 6 * n].reshape(n, 6).copy()
+    cap = np.ctypeslib.as_array(out.cap, (max(n, 1) * P,))[: P * n].reshape(n, P).copy()
+    bare = np.ctypeslib.as_array(out.bare, (max(n, 1),))[:n].copy()
+    order = np.argsort(cell, kind="stable")
+    return Cut(cell[order].astype(np.int64), volume[order], face[order], cap[order], bare[order])
+
+
+#: A cell's wall counts as cut where its area there exceeds this (in cell faces), a region as air
+#: where its volume does (in cells^3): FP64 noise lies far below both.
+TINY = 1e-12
+
+
+def _direction_table():
+    table = np.full(27, -1, np.int64)
+    for k, (dx, dy, dz) in enumerate(STEPS):
+        table[(dx + 1) + 3 * (dy + 1) + 9 * (dz + 1)] = k
+    return table
+
+
+_DIRECTION = _direction_table()
+
+
+def _direction(grid: L.Grid, a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    """The direction k of the step from cell a to cell b (-1 unless one of the 18 neighbours)."""
+    nx, ny, _ = grid.shape
+    sz = nx * ny
+    d = [(b % nx) - (a % nx), ((b // nx) % ny) - ((a // nx) % ny), (b // sz) - (a // sz)]
+    near = (np.abs(d[0]) <= 1) & (np.abs(d[1]) <= 1) & (np.abs(d[2]) <= 1)
+    key = np.where(near, (d[0] + 1) + 3 * (d[1] + 1) + 9 * (d[2] + 1), 13)
+    return np.where(near, _DIRECTION[key], -1)
+
+
+def lattice_widths(room: L.Room, grid: L.Grid) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+    """Each cell's width per axis (cells) as the reference's fit measures it on its lattice
+    (cut_cells.hpp:2031-2122): the frame E is the largest half-extent of the room's triangles that
+    reach the grid's box grown by 2h and of the grid's box, grown by 2h; p = the exponent of E plus
+    one, s = 61 - p; the middle X0 per axis rounded to a multiple of 2^(p - 2); a face's double x
+    becomes round(x 2^s) - X0 2^s (ties to even); a cell's width is the difference of its faces'
+    quanta over h 2^s. Uncut cells hold these widths' product of air (1 within about 1e-15)."""
+    vertices, faces, _ = L.room_mesh(room)
+    h = float(grid.cell)
+    face_at = [grid.origin[a] + np.arange(grid.shape[a] + 1, dtype=np.float64) * h for a in range(3)]
+    glo = [float(face_at[a][0]) - 2.0 * h for a in range(3)]
+    ghi = [float(face_at[a][-1]) + 2.0 * h for a in range(3)]
+    lo, hi = [1e300] * 3, [-1e300] * 3
+    tri = vertices[faces]  # (T, 3 corners, 3)
+    mn, mx = tri.min(axis=1), tri.max(axis=1)
+    meets = np.all((mx >= np.array(glo)) & (mn <= np.array(ghi)), axis=1)
+    for a in range(3):
+        if np.any(meets):
+            lo[a] = min(lo[a], float(mn[meets, a].min()))
+            hi[a] = max(hi[a], float(mx[meets, a].max()))
+        lo[a] = min(lo[a], float(face_at[a][0]))
+        hi[a] = max(hi[a], float(face_at[a][-1]))
+    E = max((hi[a] - lo[a]) / 2.0 for a in range(3)) + 2.0 * h
+    m, e = math.frexp(E)
+    p = (e if m > 0.5 else e - 1) + 1
+    shift = 61 - p
+    S = math.ldexp(h, shift)
+    widths = []
+    for a in range(3):
+        x0 = math.ldexp(float(np.rint(math.ldexp((lo[a] + hi[a]) / 2.0, -(p - 2)))), p - 2)
+        q0 = int(math.ldexp(x0, shift))
+
+        def quantize(x: float) -> int:
+            y = math.ldexp(float(x), shift)  # exact
+            fl = math.floor(y)
+            fr = y - fl
+            t = int(fl) - q0
+            if fr > 0.5 or (fr == 0.5 and t & 1):
+                t += 1
+            return t
+
+        g = [quantize(v) for v in face_at[a]]
+        widths.append(np.array([float(g[i + 1] - g[i]) / S for i in range(grid.shape[a])]))
+    return tuple(widths)
+
+
+def fit_from_cut(cut: Cut, room: L.Room, grid: L.Grid, *, layer: int = 0) -> Fit:
+    """The rows of a convex room from its cut (:func:`cut_convex`), by the reference's rules for
+    what a row owns and sums (cut_cells.hpp: the owner rule, sum_up): each cut cell holds up to
+    two regions, its air inside the walls' planes and outside them; a region holding an air cell's
+    centre is that cell's, and the uncut cells next to a cut one own themselves; then, round by
+    round, each region without an owner goes to the air cell (not of the matched layer) whose
+    regions it shares the most open area with across the squares between cells, within 1e-12 the
+    lowest cell. A row's air volume, walls, open areas towards its 18 neighbours (between regions
+    of two owners, by the direction from one owner to the other) and slivers (the volume it owns in
+    a face neighbour's cell over the open area through which it owns it) are the sums of what it
+    owns."""
+    nx, ny, nz = grid.shape
+    n = nx * ny * nz
+    sy, sz = nx, nx * ny
+    idx = np.arange(n, dtype=np.int64)
+    x, y, z = idx % nx, (idx // nx) % ny, idx // sz
+    edge = (x == 0) | (y == 0) | (z == 0) | (x == nx - 1) | (y == ny - 1) | (z == nz - 1)
+    depth = np.minimum.reduce([x, y, z, nx - 1 - x, ny - 1 - y, nz - 1 - z])
+    normals, offsets, open_ = cut_room(room, grid)
+    walls = np.flatnonzero(open_ == 0)
+    # The air: with an open face every cell but the grid's edge; closed, the cells whose centre
+    # lies inside the walls. Cells within `layer` of the edge form the matched layer.
+    centres = np.stack([grid.centres(0)[x], grid.centres(1)[y], grid.centres(2)[z]], axis=1) if not room.open else None
+    if room.open:
+        air_mask = ~edge
+    else:
+        air_mask = ~edge & np.all(centres @ normals[walls].T - offsets[walls] < 0.0, axis=1)
+    air = np.where(air_mask, AIR, SOLID).astype(np.uint8)
+    if layer > 0:
+        air[air_mask & (depth <= layer)] = LAYER
+
+    # The cut cells: those a wall reaches with positive area.
+    is_cut = np.any(cut.cap[:, walls] > TINY, axis=1) if len(walls) else np.zeros(len(cut.cell), bool)
+    cc = cut.cell[is_cut]
+    C = len(cc)
+    wx, wy, wz = lattice_widths(room, grid)
+
+    def cell_volume(cells):
+        return wx[cells % nx] * wy[(cells // nx) % ny] * wz[cells // sz]
+
+    def face_area(cells, a):
+        """The area of each cell's face across axis a (a scalar or one axis per cell)."""
+        w3 = np.stack([wx[cells % nx], wy[(cells // nx) % ny], wz[cells // sz]])
+        a = np.broadcast_to(np.asarray(a), np.shape(cells))
+        cols = np.arange(np.size(cells))
+        return w3[(a + 1) % 3, cols] * w3[(a + 2) % 3, cols]
+
+    v_in = np.clip(cut.volume[is_cut], 0.0, 1.0)
+    v_out = np.maximum(cell_volume(cc) - v_in, 0.0)
+    # Where the walls' planes leave part of the boundary between the two sides bare (past a face
+    # left open), the sides meet: one region, as the reference joins leaves across a bare facet.
+    joined = cut.bare[is_cut] > TINY
+    v_in = np.where(joined, cell_volume(cc), v_in)
+    v_out = np.where(joined, 0.0, v_out)
+    faces = cut.face_area[is_cut]
+    caps = cut.cap[is_cut]
+    # Which side holds each cut cell's centre: inside every wall plane that cuts it (a joined
+    # cell's one region holds it).
+    cx = np.stack([grid.centres(0)[cc % nx], grid.centres(1)[(cc // nx) % ny], grid.centres(2)[cc // sz]], axis=1)
+    centre_in = np.all(cx @ normals[walls].T - offsets[walls] < 0.0, axis=1) | joined
+
+    # Regions: 2c the inside of cut cell c, 2c + 1 its outside; whole cells after them.
+    has_in = v_in > TINY
+    has_out = v_out > TINY
+    cut_index = np.full(n, -1, np.int64)
+    cut_index[cc] = np.arange(C)
+    offsets6 = np.array([-1, 1, -sy, sy, -sz, sz], np.int64)
+    neigh = cc[:, None] + offsets6[None, :]
+    whole = np.unique(neigh[(cut_index[neigh] < 0) & ~edge[neigh]])
+    W = len(whole)
+    whole_index = np.full(n, -1, np.int64)
+    whole_index[whole] = 2 * C + np.arange(W)
+    G = 2 * C + W
+    reg_cell = np.concatenate([np.repeat(cc, 2), whole])
+    reg_volume = np.concatenate([np.stack([v_in, v_out], axis=1).reshape(-1), cell_volume(whole)])
+    reg_valid = np.concatenate([np.stack([has_in, has_out], axis=1).reshape(-1), np.ones(W, bool)])
+    in_air = reg_valid & (air[reg_cell] != SOLID)
+    if not room.open:  # the air outside a closed room's walls is not the source's
+        in_air[1 : 2 * C : 2] = False
+
+    # The squares of the cut cells: (lower cell, axis), each once; each gives an inside piece and
+    # an outside piece, joining the regions on its two sides.
+    lower = np.concatenate([cc[:, None] + np.zeros(3, np.int64)[None, :], neigh[:, [0, 2, 4]]], axis=0).reshape(-1)
+    axis = np.concatenate([np.tile(np.arange(3), (C, 1)), np.tile(np.arange(3), (C, 1))], axis=0).reshape(-1)
+    key = np.unique(3 * lower + axis)
+    lower, axis = key // 3, key % 3
+    upper = lower + np.array([1, sy, sz], np.int64)[axis]
+    ok = ~edge[lower] & ~edge[upper]
+    lower, upper, axis = lower[ok], upper[ok], axis[ok]
+    la, ua = cut_index[lower], cut_index[upper]
+    # The inside part of the square: from the lower cell's + face where it is cut, else the upper's - face.
+    a_in = np.where(la >= 0, faces[np.maximum(la, 0), 2 * axis + 1], faces[np.maximum(ua, 0), 2 * axis])
+    a_in = np.clip(a_in, 0.0, 1.0)
+
+    def region(cell_cut, cell, side):
+        # (a joined cell's pieces on both sides meet its one region)
+        side = np.where(joined[np.maximum(cell_cut, 0)], 0, side)
+        return np.where(cell_cut >= 0, 2 * np.maximum(cell_cut, 0) + side, whole_index[cell])
+
+    p_low = np.concatenate([region(la, lower, 0), region(la, lower, 1)])
+    p_high = np.concatenate([region(ua, upper, 0), region(ua, upper, 1)])
+    p_area = np.concatenate([a_in, np.maximum(face_area(lower, axis) - a_in, 0.0)])
+    keep = (p_area > TINY) & (p_low >= 0) & (p_high >= 0)
+    keep[keep] &= reg_valid[p_low[keep]] & reg_valid[p_high[keep]]
+    p_low, p_high, p_area = p_low[keep], p_high[keep], p_area[keep]
+
+    # Owners (cut_cells.hpp:4641-4711).
+    owner = np.full(G, -1, np.int64)
+    centre_region = 2 * np.arange(C) + np.where(centre_in, 0, 1)
+    own_centre = air[cc] == AIR
+    owner[centre_region[own_centre]] = cc[own_centre]
+    owner[2 * C :] = np.where(air[whole] != SOLID, whole, -1)
+    owner[~reg_valid] = -2  # no region
+    for _ in range(64):
+        offer_r, offer_o, offer_a = [], [], []
+        for to, by in ((p_low, p_high), (p_high, p_low)):
+            ob = owner[by]
+            ok = (owner[to] == -1) & in_air[to] & (ob >= 0)
+            ok[ok] &= air[ob[ok]] == AIR
+            offer_r.append(to[ok]), offer_o.append(ob[ok]), offer_a.append(np.maximum(p_area[ok], 0.0))
+        r_ = np.concatenate(offer_r)
+        if len(r_) == 0:
+            break
+        o_, a_ = np.concatenate(offer_o), np.concatenate(offer_a)
+        order = np.lexsort((o_, r_))
+        r_, o_, a_ = r_[order], o_[order], a_[order]
+        pair = np.flatnonzero(np.r_[True, (r_[1:] != r_[:-1]) | (o_[1:] != o_[:-1])])
+        sums = np.add.reduceat(a_, pair)
+        pr, po = r_[pair], o_[pair]
+        start = np.flatnonzero(np.r_[True, pr[1:] != pr[:-1]])
+        count = np.diff(np.r_[start, len(pr)])
+        best, most = po[start].copy(), sums[start].copy()
+        for step in range(1, int(count.max())):
+            has = count > step
+            cand_a = sums[start[has] + step]
+            better = cand_a > most[has] + 1e-12
+            sel = np.flatnonzero(has)[better]
+            best[sel] = po[start[sel] + step]
+            most[sel] = cand_a[better]
+        owner[pr[start]] = best
+    owner[owner == -2] = -1
+
+    # The rows and their sums (sum_up, cut_cells.hpp:4846-4960).
+    is_row_cell = np.zeros(n, bool)
+    owned = owner >= 0
+    is_row_cell[owner[owned]] = air[owner[owned]] == AIR
+    rows = np.flatnonzero(is_row_cell)
+    row_index = np.full(n, -1, np.int64)
+    row_index[rows] = np.arange(len(rows))
+    R = len(rows)
+    M = len(room.materials)
+    air_volume = np.zeros(R)
+    open_area = np.zeros((R, 18))
+    wall_area = np.zeros((R, M + 1))
+    sliver = np.zeros((R, 6))
+    sliver_area = np.zeros((R, 6))
+    g_ok = owned & np.zeros(G, bool)
+    g_ok[owned] = is_row_cell[owner[owned]]
+    gr = np.flatnonzero(g_ok)
+    ro = row_index[owner[gr]]
+    np.add.at(air_volume, ro, reg_volume[gr])
+    # walls: both sides of a wall see it (a cut cell's inside and outside regions)
+    cut_g = gr[gr < 2 * C]
+    both_sides = np.where(joined[cut_g // 2], 2.0, 1.0)  # a joined region sees each wall's two sides
+    for f in walls:
+        np.add.at(wall_area[:, f], row_index[owner[cut_g]], both_sides * caps[cut_g // 2, f])
+    k = _direction(grid, owner[gr], reg_cell[gr])
+    ax = (k >= 0) & (k < 6)
+    np.add.at(sliver, (ro[ax], k[ax]), reg_volume[gr][ax])
+    oa, ob = owner[p_low], owner[p_high]
+    rowa = (oa >= 0) & is_row_cell[np.maximum(oa, 0)]
+    rowb = (ob >= 0) & is_row_cell[np.maximum(ob, 0)]
+    same = (oa == ob) & (oa >= 0)
+    ca, cb = reg_cell[p_low], reg_cell[p_high]
+    sl = same & rowa & ((ca == oa) != (cb == oa))
+    other = np.where(ca == oa, cb, ca)
+    ks = _direction(grid, oa, other)
+    sl &= (ks >= 0) & (ks < 6)
+    np.add.at(sliver_area, (row_index[oa[sl]], ks[sl]), p_area[sl])
+    diff = ~same & (oa >= 0) & (ob >= 0)
+    kd = _direction(grid, oa, ob)
+    both = rowa & rowb
+    link = diff & (kd >= 0) & ((kd < 6) | both)
+    ka = link & rowa
+    np.add.at(open_area, (row_index[oa[ka]], kd[ka]), p_area[ka])
+    kb = link & rowb
+    opp = np.array([opposite(k) for k in range(18)], np.int64)
+    np.add.at(open_area, (row_index[ob[kb]], opp[kd[kb]]), p_area[kb])
+    # A row's faces that no square was cut for: whole (its cell and the one across both uncut).
+    uncut_rows = rows[cut_index[rows] < 0]
+    for k6 in range(6):
+        j = uncut_rows + offsets6[k6]
+        whole_face = cut_index[j] < 0
+        to_edge = whole_face & edge[j]
+        to_air = whole_face & ~edge[j] & (air[j] != SOLID)
+        np.add.at(wall_area[:, M], row_index[uncut_rows[to_edge]], face_area(uncut_rows[to_edge], k6 // 2))
+        np.add.at(open_area[:, k6], row_index[uncut_rows[to_air]], face_area(uncut_rows[to_air], k6 // 2))
+    sliver = np.where(sliver_area > 1e-9, sliver / np.where(sliver_area > 1e-9, sliver_area, 1.0), 0.0)
+    return Fit(rows.astype(np.int64), air_volume, open_area, wall_area, sliver, air, (wx, wy, wz))
+
+
+def fitted_cubic(grid: L.Grid, point) -> list[tuple[int, float]]:
+    """The 4 x 4 x 4 cells round ``point`` with the fitted path's cubic weights, z then y then x
+    (reading_cells_fitted, fdtd.hpp:1518-1605, for a point whose cells are all air in sight of
+    it): along each axis, with lo the point's place between the centres below and above it, the
+    weight of cell k of the four is prod over m != k of (lo - (m - 1)) / (k - m)."""
+    nx, ny, _ = grid.shape
+    start, weight = [], []
+    for a in range(3):
+        centres = grid.centres(a)
+        p = float(np.asarray(point, float)[a])
+        j = int(np.searchsorted(centres, p, side="right")) - 1
+        if not (1 <= j < grid.shape[a] - 3):
+            raise ValueError("the point is too near the grid's edge for its cubic stencil")
+        lo = (p - centres[j]) / (centres[j + 1] - centres[j])
+        ws = []
+        for k in range(4):
+            w = 1.0
+            for m in range(4):
+                if m != k:
+                    w *= (lo - float(m - 1)) / float(k - m)
+            ws.append(w)
+        start.append(j - 1)
+        weight.append(ws)
+    out = []
+    for z in range(4):
+        for y in range(4):
+            for x in range(4):
+                w = weight[0][x] * weight[1][y] * weight[2][z]
+                if w != 0.0:
+                    out.append((int(start[0] + x + (start[1] + y) * nx + (start[2] + z) * nx * ny), w))
+    return out
+
+
+def convex_fit(room: L.Room, grid: L.Grid, *, layer: int = 0, device: int = 0) -> Fit:
+    """This library's fit of a convex room: the cut on the GPU, then the rows on the host."""
+    return fit_from_cut(cut_convex(room, grid, device), room, grid, layer=layer)
+
+
+def fitted_layout(room: L.Room, grid: L.Grid, source, probes, *, layer: int = 0, layer_damping: float = 0.0,
+                  edge_admittance: float = 1.0, device: int = 0, fit: Fit | None = None) -> dict[str, np.ndarray]:
+    """The layout of ``room`` with fitted walls: this library's fit (or ``fit``), then the
+    reference's rules for its rows, with the source and the probes on the fitted cubic stencil
+    (each must lie where its 64 cells are air clear of every wall)."""
+    if fit is None:
+        fit = convex_fit(room, grid, layer=layer, device=device)
+    source_cells = fitted_cubic(grid, source)
+    probe_cells = [fitted_cubic(grid, p) for p in np.asarray(probes, float).reshape(-1, 3)]
+    rows = set(int(i) for i in fit.cell)
+    for cells in [source_cells, *probe_cells]:
+        for i, _ in cells:
+            if fit.air[i] != AIR:
+                raise ValueError("a point's cubic stencil reaches a cell outside the air or in the matched layer")
+    for cells in probe_cells:
+        if any(int(i) in rows for i, _ in cells):
+            raise ValueError("a probe's cubic stencil reaches a cut cell: keep the probes clear of the walls")
+    return set_up_fitted(fit, grid, room.materials, source_cells, probe_cells, layer=layer,
+                         layer_damping=layer_damping, edge_admittance=edge_admittance)  # fmt: skip

@@ -800,6 +800,8 @@ def polyhedral_room(
     receivers: int = 16,
     steps: int = 12000,
     speed_of_sound: float = 343.0,
+    walls: str = "faces",
+    device: int = 0,
 ) -> Workload:
     """A seeded convex polyhedral room of 12 to 20 planar faces inscribed in ``box`` metres, open
     through its +x face into the air round it, on a grid of ``cell`` metres spanning the box with
@@ -807,7 +809,11 @@ def polyhedral_room(
     admittance: a real beta in [0.02, 0.1] and one passive resonant branch of seeded resonance
     (30 to 300 Hz), quality (0.5 to 10) and conductance (0.005 to 0.5). One source and
     ``receivers`` receivers at seeded points at least 0.5 m from every plane; the drive a 0.5 ms
-    Gaussian pulse. Walls on cell faces, 7-point stencil, at its Courant limit."""
+    Gaussian pulse. 7-point stencil at its Courant limit. ``walls``: "faces" for walls on cell
+    faces (the reference's default path), "fitted" for fitted (cut-cell) walls by this library's
+    FP64 fit on the GPU (``fitted.fitted_layout``; ``device`` runs it)."""
+    if walls not in ("faces", "fitted"):
+        raise ValueError("walls are 'faces' or 'fitted'")
     rng = np.random.default_rng(seed)
     rate = speed_of_sound / (COURANT * cell)
     faces = int(rng.integers(12, 21))
@@ -822,7 +828,15 @@ def polyhedral_room(
     room = convex_room(rng, box, faces=faces, margin=margin, open_face=1, material=material)
     points = inside_points(rng, room, box, 1 + receivers, max(0.5, 3 * cell), apart=max(0.5, 4 * cell))
     grid = Grid(-OFFSET * cell, cell, tuple(int(round(b / cell)) for b in box))
-    built = cell_face_layout(room, grid, points[0], points[1:], layer=layer, layer_damping=LAYER_DAMPING, rate=rate)
+    if walls == "fitted":
+        from . import fitted
+
+        lay = fitted.fitted_layout(room, grid, points[0], points[1:], layer=layer, layer_damping=LAYER_DAMPING,
+                                   device=device)  # fmt: skip
+        built = Built(lay, grid, int(np.count_nonzero(lay["types"])), len(lay["special"]), 0, rate)
+    else:
+        built = cell_face_layout(room, grid, points[0], points[1:], layer=layer, layer_damping=LAYER_DAMPING,
+                                 rate=rate)  # fmt: skip
     lay = built.layout
     description = {
         "room": f"convex polyhedron, {faces} planes in {box[0]:g}x{box[1]:g}x{box[2]:g} m, +x face open",
@@ -838,7 +852,8 @@ def polyhedral_room(
         "probes": receivers,
         "steps": steps,
         "rate_hz": rate,
-        "walls": "cell faces, 2-pole admittance per wall",
+        "walls": ("fitted cut cells (this library's FP64 GPU fit of the convex room), 2-pole admittance per wall"
+                  if walls == "fitted" else "cell faces, 2-pole admittance per wall"),  # fmt: skip
         "stencil": 7,
         "seed": seed,
     }

@@ -175,9 +175,10 @@ class B200WaveSolver:
         """The gradient of a loss L of the probes' series with respect to the layout's
         coefficients, by the reverse-time stepper: the run from rest on ``signal`` gives the
         series y (probes, steps); ``dloss_dy`` is dL/dy. Returns dL/d ``coef_b``, ``coef_inv``
-        (one per special row) and dL/d ``now``, ``before``, ``gain`` (one per branch state). The
-        forward pass is recomputed in segments of ``segment`` steps from checkpoints. The solver
-        is left at rest."""
+        (one per special row) and dL/d ``now``, ``before``, ``gain`` (one per branch state); on a
+        grid with a matched layer also dL/d of its twelve tables (``keep_x``, ``keep_face_x``, ...,
+        ``push_face_z``, the layout's names, fdtd.hpp:2219-2238). The forward pass is recomputed in
+        segments of ``segment`` steps from checkpoints. The solver is left at rest."""
         signal = np.ascontiguousarray(signal, np.float32).reshape(-1)
         steps = len(signal)
         dloss = np.ascontiguousarray(dloss_dy, np.float64).reshape(self._probes, steps)
@@ -200,6 +201,22 @@ class B200WaveSolver:
         )
         if status != _abi.FDTD_OK:
             _raise(self._lib, status, self._handle)
+        if int(info.layer_cells):
+            out.update(self.layer_gradient())
+        return out
+
+    def layer_gradient(self) -> dict[str, np.ndarray]:
+        """The last gradient's part in the matched layer's twelve tables, by the layout's names."""
+        nx, ny, nz = self.shape
+        lengths = [nx + 1, nx + 1, ny + 1, ny + 1, nz + 1, nz + 1]
+        flat = np.zeros(2 * sum(lengths))
+        status = self._lib.fdtd_layer_gradient(self._handle, flat.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        if status != _abi.FDTD_OK:
+            _raise(self._lib, status, self._handle)
+        out, at = {}, 0
+        for name, n in zip(_abi.KEEP + _abi.PUSH, lengths + lengths):
+            out[name] = flat[at : at + n].copy()
+            at += n
         return out
 
     def set_coefficients(self, coef_b=None, coef_inv=None, branch_now=None, branch_before=None,
@@ -239,14 +256,33 @@ class B200WaveSolver:
             _raise(self._lib, status, self._handle)
 
     def autotune(self, trial_steps: int = 8) -> dict[str, int]:
-        """Chooses the matched-layer and special-row kernels' blocks per multiprocessor for this
-        grid by timing a few steps of each candidate (from rest; the state is reset after).
-        Returns the choice (0: one thread a cell)."""
+        """Chooses the launch shapes for this grid by timing a few steps of each candidate (from
+        rest; the state is reset after): the interior sweep's tile shape and planes a tile, then
+        the matched-layer and special-row kernels' blocks per multiprocessor. Returns the choice
+        (blocks 0: one thread a cell; the tiles as :meth:`tiles` gives them)."""
         layer, special = ctypes.c_int(), ctypes.c_int()
         status = self._lib.fdtd_autotune(self._handle, int(trial_steps), ctypes.byref(layer), ctypes.byref(special))
         if status != _abi.FDTD_OK:
             _raise(self._lib, status, self._handle)
-        return {"layer_blocks_per_sm": layer.value, "special_blocks_per_sm": special.value}
+        return {"layer_blocks_per_sm": layer.value, "special_blocks_per_sm": special.value, **self.tiles()}
+
+    def tiles(self) -> dict[str, int]:
+        """The interior sweep's tiles: shape index, cells a tile along x and y, ring stages,
+        planes a tile, tiles, and resident blocks a multiprocessor."""
+        t = _abi.FdtdTiles()
+        status = self._lib.fdtd_get_tiles(self._handle, ctypes.byref(t))
+        if status != _abi.FDTD_OK:
+            _raise(self._lib, status, self._handle)
+        return {"tile_shape": t.shape, "tile_x": t.tile_x, "tile_y": t.tile_y, "tile_stages": t.stages,
+                "tile_planes": int(t.planes), "tiles": int(t.tiles), "tile_blocks_per_sm": t.blocks_per_sm}  # fmt: skip
+
+    def set_tiles(self, shape: int, planes: int) -> None:
+        """Sets the interior sweep's tile shape (0: 64 x 16, 1: 128 x 16, 2: 64 x 32, 3: 32 x 32)
+        and planes a tile, as :meth:`autotune` would; results are the same to the bit."""
+        status = self._lib.fdtd_set_tiles(self._handle, int(shape), int(planes))
+        if status != _abi.FDTD_OK:
+            _raise(self._lib, status, self._handle)
+        self.launch = {**getattr(self, "launch", {}), **self.tiles()}
 
     def level_plane(self, z: int, previous: bool = False) -> tuple[int, int]:
         """The device address and byte size of plane ``z`` of the current (or previous) pressure

@@ -31,7 +31,6 @@ import argparse
 import json
 import os
 import statistics
-import subprocess
 import sys
 import threading
 import time
@@ -155,65 +154,74 @@ def measured_peaks() -> tuple[float, str]:
 
 
 class Clocks:
-    """nvidia-smi samples of SM clock and throttle reasons while it runs."""
+    """The SM clock and throttle reasons sampled through NVML while the timed region runs: a thread
+    polls as fast as NVML answers (about every half millisecond), since the timed region can be
+    a few milliseconds, shorter than nvidia-smi's sampling period. Nothing is set, only read."""
 
-    QUERY = (
-        "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-        "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-        "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
-    )
+    # NVML's clocks-event reason bits (nvml.h): the four the timing rules name.
+    REASONS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40}
 
     def __init__(self, device: int):
         self.device = device
-        self.proc = None
-        self.lines: list[str] = []
+        self.samples: list[tuple[float, int]] = []
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._thread = None
+        self._nvml = None
+
+    def _handle(self, nvml):
+        try:
+            import torch
+
+            props = torch.cuda.get_device_properties(self.device)
+            bus = f"{props.pci_domain_id:08x}:{props.pci_bus_id:02x}:{props.pci_device_id:02x}.0"
+            return nvml.nvmlDeviceGetHandleByPciBusId(bus.encode())
+        except Exception:
+            return nvml.nvmlDeviceGetHandleByIndex(self.device)
+
+    def _poll(self, nvml, handle):
+        while not self._stop.is_set():
+            try:
+                mhz = nvml.nvmlDeviceGetClockInfo(handle, nvml.NVML_CLOCK_SM)
+                reasons = nvml.nvmlDeviceGetCurrentClocksEventReasons(handle)
+            except Exception:
+                return
+            self.samples.append((float(mhz), int(reasons)))
+            time.sleep(0.0002)
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits", "-lms", "100"],
-                stdout=subprocess.PIPE,
-                stderr=subprocess.DEVNULL,
-                text=True,
-            )
-            self.thread = threading.Thread(target=self._read, daemon=True)
-            self.thread.start()
-        except (OSError, FileNotFoundError):
-            self.proc = None
+            import pynvml as nvml
+
+            nvml.nvmlInit()
+            self._nvml = nvml
+            handle = self._handle(nvml)
+            self.max_mhz = float(nvml.nvmlDeviceGetMaxClockInfo(handle, nvml.NVML_CLOCK_SM))
+            self._thread = threading.Thread(target=self._poll, args=(nvml, handle), daemon=True)
+            self._thread.start()
+        except Exception:
+            self._thread = None
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
-
     def __exit__(self, *exc):
-        if self.proc is not None:
-            self.proc.terminate()
+        self._stop.set()
+        if self._thread is not None:
+            self._thread.join(timeout=5)
+        if self._nvml is not None:
             try:
-                self.proc.wait(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
+                self._nvml.nvmlShutdown()
+            except Exception:
+                pass
 
     def summary(self) -> dict:
-        sm, max_sm, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                sm.append(float(parts[1]))
-                max_sm = float(parts[2])
-            except ValueError:
-                continue
-            for name, flag in zip(names, parts[5:9]):
-                if flag.lower().startswith("active"):
-                    reasons.add(name)
+        sm = [mhz for mhz, _ in self.samples]
+        reasons = sorted(name for name, bit in self.REASONS.items() if any(r & bit for _, r in self.samples))
         return {
             "sm_mhz": statistics.median(sm) if sm else None,
-            "sm_max_mhz": max_sm,
-            "reasons": sorted(reasons),
+            "sm_max_mhz": self.max_mhz,
+            "reasons": reasons,
             "samples": len(sm),
+            "source": "NVML, polled through the timed region",
         }
 
 

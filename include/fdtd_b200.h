@@ -177,13 +177,26 @@ int fdtd_get_timing(fdtd_solver *solver, double ms[4], uint64_t *steps);
  * before and gain coefficients (state_count each; the state's branch's, fdtd.hpp:797-805), summed
  * over the run in double; any output may be NULL. The forward pass is recomputed in segments of
  * `segment` steps from checkpoints of the whole state kept at each segment's start (0: one
- * segment), recording each step's values at the special rows; the adjoint then steps back
- * through each segment. Grids without a matched layer (either stencil, a speed field or
- * none) only (FDTD_EINVAL otherwise). The solver is left at rest.
+ * segment), recording each step's values at the special rows (and, with a matched layer, each
+ * layer cell's eighteen factors of the layer's update: kLayerFactors x layer_count values a step of
+ * the segment); the adjoint then steps back through each segment. Either stencil, with or without
+ * a speed field, with or without a matched layer (fdtd.hpp:2219-2264); on a grid with a layer
+ * the gradient in its twelve tables follows from fdtd_layer_gradient. The solver is left at rest.
  */
 int fdtd_gradient(fdtd_solver *solver, const float *signal, uint64_t steps, const double *dloss_dy,
                   uint64_t segment, double *grad_coef_b, double *grad_coef_inv, double *grad_now,
                   double *grad_before, double *grad_gain);
+
+/*
+ * The last fdtd_gradient's (or fdtd_gradient_noalloc's) dL/d of the matched layer's twelve tables
+ * (no counterpart in the reference; the tables are layer_coefficients', fdtd.hpp:2219-2238), into
+ * `tables`: keep_x, keep_face_x, keep_y, keep_face_y, keep_z, keep_face_z, then push_x,
+ * push_face_x, ..., push_face_z, the order of fdtd_layout.keep and .push, each of nx + 1, nx + 1,
+ * ny + 1, ny + 1, nz + 1, nz + 1 values (4 (nx + ny + nz + 3) in all). The gradient in the layer's
+ * damping follows by the chain rule through the tables (their derivative in the damping).
+ * FDTD_EINVAL on a grid without a layer or before a gradient.
+ */
+int fdtd_layer_gradient(const fdtd_solver *solver, double *tables);
 
 /*
  * The tape of a run for a gradient that follows (no counterpart in the reference). With `segment`
@@ -192,7 +205,9 @@ int fdtd_gradient(fdtd_solver *solver, const float *signal, uint64_t steps, cons
  * drive and steps with the same `segment` starts from those states instead of running the forward
  * pass again, so that a fit's forward run and its gradient together step the grid twice rather
  * than three times. The result is the same to the bit. 0 turns the tape off. The states take
- * (steps / segment - 1) x (2 levels + 2 branch-velocity sets) of device memory, kept by the handle.
+ * (steps / segment - 1) x (2 levels + 2 branch-velocity sets, and with a matched layer its parts
+ * and a level of faces per axis) of device memory, kept by the handle; a grid with a matched layer
+ * always keeps states, never the trajectory.
  */
 int fdtd_set_tape(fdtd_solver *solver, uint64_t segment);
 
@@ -206,13 +221,37 @@ int fdtd_set_tape(fdtd_solver *solver, uint64_t segment);
 int fdtd_set_tape_budget(fdtd_solver *solver, uint64_t bytes);
 
 /*
- * Chooses the launch shapes of the matched-layer and special-row kernels for this grid (no
- * counterpart in the reference): from rest, steps `trial_steps` steps (0: 8) with each candidate
- * count of blocks per multiprocessor, keeps the fastest by CUDA events, and resets the state. The
- * chosen counts are written to *layer_per_sm and *special_per_sm when given (0: one thread a
- * cell). Refused after steps (fdtd_reset first).
+ * Chooses the launch shapes for this grid (no counterpart in the reference): from rest, steps
+ * `trial_steps` steps (0: 8) with each candidate and keeps the fastest by CUDA events — first the
+ * interior sweep's tile shape (each of the four shapes of fdtd_tiles that fits a multiprocessor,
+ * each with 1/2, 1 and 2 times the default planes a tile, within 8 to 64), then, with the best
+ * tiles, the count of blocks per multiprocessor of the matched-layer and special-row kernels — and
+ * resets the state. The chosen counts are written to *layer_per_sm and *special_per_sm when given
+ * (0: one thread a cell); fdtd_get_tiles gives the chosen tiles. Results do not depend on any of
+ * these choices. Refused after steps (fdtd_reset first).
  */
 int fdtd_autotune(fdtd_solver *solver, uint64_t trial_steps, int *layer_per_sm, int *special_per_sm);
+
+/* The interior sweep's tiles (no counterpart in the reference). */
+typedef struct fdtd_tiles {
+    int shape;          /* 0: 64 x 16 cells, 5 stages; 1: 128 x 16, 4; 2: 64 x 32, 4; 3: 32 x 32, 5 */
+    int tile_x, tile_y; /* cells of a tile along x and y */
+    int stages;         /* plane stages in a block's shared-memory ring */
+    uint64_t planes;    /* planes of a tile, at most (a tile marches them along z) */
+    uint32_t tiles;     /* tiles, one block each */
+    int blocks_per_sm;  /* resident blocks of the sweep a multiprocessor */
+} fdtd_tiles;
+
+/*
+ * Sets the interior sweep's tile shape (an index of fdtd_tiles.shape) and planes a tile (1 to
+ * 1024), as fdtd_autotune would choose them; the state is kept and results are unchanged, to the
+ * bit. FDTD_EINVAL for a shape out of range or one whose shared memory does not fit a
+ * multiprocessor in the handle's precision. Waits for the handle's work.
+ */
+int fdtd_set_tiles(fdtd_solver *solver, int shape, uint64_t planes);
+
+/* The interior sweep's present tiles. */
+int fdtd_get_tiles(const fdtd_solver *solver, fdtd_tiles *out);
 
 /*
  * The device address and size of plane z of the current (which 0) or previous (1) pressure level
@@ -308,6 +347,58 @@ int fdtd_device_name(int device, char *buf, size_t size);
 
 /* CUDA devices of compute capability 10.x visible to the process (0 when none). */
 int fdtd_device_count(void);
+
+/* ---- fitted walls: the cut of a convex room by the grid (set-up, not stepping) ---- */
+
+/* Planes of a convex room, at most. */
+#define FDTD_CUT_MAX_PLANES 64
+
+/* A convex room P = {x : normals[f] . x <= offsets[f] for every plane f} (unit normals, pointing
+ * out of the room; metres), on a grid of nx x ny x nz cells of `cell` metres whose first cell's
+ * corner is `origin` (cell (i, j, k) spans origin + (i, j, k) cell .. + cell, the doubles of the
+ * reference's cut_grid, fdtd.hpp:1620-1634). */
+typedef struct fdtd_cut_room {
+    const double *normals; /* planes x 3 */
+    const double *offsets; /* planes */
+    const uint8_t *open;   /* planes: nonzero for a face left open (no wall), NULL for none */
+    uint32_t planes;
+    double origin[3];
+    double cell;
+    uint64_t nx, ny, nz;
+} fdtd_cut_room;
+
+/* The cells the walls' planes cut, in no particular order (the library allocates the arrays;
+ * fdtd_cut_free releases them): each cell's index (x fastest); the volume of its air inside every
+ * wall's plane (in cells^3; the rest of the cell is its air outside them), the area of each of its
+ * faces (-x, +x, -y, +y, -z, +z; in cell faces, 6 a cell) on that inner side, each wall's area
+ * in the cell (`planes` a cell; 0 for an open plane), and the area of the walls' planes between
+ * the inner and the outer air that no wall covers (beyond a face left open: the two sides of the
+ * cell's air meet there). */
+typedef struct fdtd_cut_cells {
+    uint64_t cells;
+    uint32_t planes;
+    uint64_t *cell;
+    double *volume;
+    double *face_area;
+    double *cap;
+    double *bare;
+} fdtd_cut_cells;
+
+/*
+ * The FP64 fractions of fitted (cut-cell) walls for a convex room, on the GPU (no counterpart
+ * for this kind of room in the reference, whose exact fit of a triangle mesh runs on the host:
+ * cut_cells.hpp, CutCells, measured per cell in set_up_fitted, fdtd.hpp:970-1217). One thread a
+ * cell: each cell that a wall's plane cuts is clipped by every plane that cuts it (a wall's plane
+ * splits the cell, an open plane only bounds the walls' faces). Returns FDTD_OK with
+ * *out filled, or a status with fdtd_cut_error's message (no device: FDTD_ENODEV).
+ */
+int fdtd_cut_convex(const fdtd_cut_room *room, int device, fdtd_cut_cells *out);
+
+/* Releases the arrays of a fdtd_cut_cells (NULL and a zeroed struct are accepted). */
+void fdtd_cut_free(fdtd_cut_cells *cells);
+
+/* The message of the calling thread's last failed fdtd_cut_convex. */
+const char *fdtd_cut_error(void);
 
 /* FDTD_B200_ABI_VERSION of the library. */
 int fdtd_abi_version(void);

@@ -8,6 +8,7 @@
 //   Bvh(vertices, faces, split="sah")                     cpp/bindings/native_module.cpp:1422-1435
 //   WaveSolver(bvh, face_material, beta, branches, ...)   cpp/bindings/native_module.cpp:1238-1283,
 //                                                         1564-1707
+//   CutFit(vertices, faces, face_material, materials, ...) cpp/bindings/native_module.cpp:1465-1559
 // so that `acoustic_spaces._native` can be replaced by it under the reference's Python sources.
 // Its compiled form lives in oracle/_ref/ (built by oracle/Makefile from the reference headers
 // where they lie; no reference source is copied into this repository).
@@ -139,6 +140,65 @@ std::shared_ptr<SolverHolder> make_solver(
     return h;
 }
 
+// The fit alone (the reference's CutCells on the wave solver's grid; its own binding is CutFit,
+// cpp/bindings/native_module.cpp:1465-1559): the vertices and faces are kept for the fit's life.
+struct FitHolder {
+    std::vector<double> vertices;
+    std::vector<std::int64_t> faces;
+    std::unique_ptr<as::CutCells> cut;
+};
+
+std::shared_ptr<FitHolder> make_fit(const CArray<double> &vertices, const CArray<std::int64_t> &faces,
+                                    const CArray<std::int64_t> &face_material, std::size_t materials,
+                                    const CArray<double> &origin, double cell, std::size_t nx, std::size_t ny,
+                                    std::size_t nz, const CArray<double> &source, std::size_t layer,
+                                    std::size_t threads) {
+    if (vertices.ndim() != 2 || vertices.shape(1) != 3) throw std::invalid_argument("CutFit: vertices (n, 3)");
+    if (faces.ndim() != 2 || faces.shape(1) != 3) throw std::invalid_argument("CutFit: faces (m, 3)");
+    if (face_material.size() != faces.shape(0)) throw std::invalid_argument("CutFit: one material per face");
+    auto h = std::make_shared<FitHolder>();
+    h->vertices.assign(vertices.data(), vertices.data() + vertices.size());
+    h->faces.assign(faces.data(), faces.data() + faces.size());
+    for (std::int64_t f : h->faces)
+        if (f < 0 || static_cast<std::size_t>(f) >= h->vertices.size() / 3)
+            throw std::invalid_argument("CutFit: a face refers to a missing vertex");
+    for (py::ssize_t f = 0; f < face_material.size(); ++f)
+        if (face_material.data()[f] < 0 || static_cast<std::size_t>(face_material.data()[f]) >= materials)
+            throw std::invalid_argument("CutFit: a face's material is not below materials");
+    as::CutCells::Mesh mesh;
+    mesh.vertices = h->vertices.data();
+    mesh.vertex_count = h->vertices.size() / 3;
+    mesh.faces = h->faces.data();
+    mesh.face_count = h->faces.size() / 3;
+    const as::Vec3 o = vec_of(origin, "origin"), src = vec_of(source, "source");
+    {
+        py::gil_scoped_release release;
+        h->cut = std::make_unique<as::CutCells>(mesh, face_material.data(), materials,
+                                                as::WaveSolver::cut_grid(o, cell, nx, ny, nz, layer), src, threads);
+    }
+    if (h->cut->refused()) throw std::invalid_argument(h->cut->refusal());
+    return h;
+}
+
+template <typename T>
+py::array shaped(const std::vector<T> &values, std::size_t rows, std::size_t cols) {
+    py::array_t<T> out({static_cast<py::ssize_t>(rows), static_cast<py::ssize_t>(cols)});
+    std::copy(values.begin(), values.end(), out.mutable_data());
+    return out;
+}
+
+py::dict fit_cells(const FitHolder &h) {
+    const as::CutCells &cut = *h.cut;
+    const std::size_t n = cut.cells().size(), w = cut.materials() + 1;
+    py::dict out;
+    out["cell"] = to_numpy(cut.cells());
+    out["air_volume"] = to_numpy(cut.air_volume());
+    out["open_area"] = shaped(cut.open_area(), n, 18);
+    out["wall_area"] = shaped(cut.wall_area(), n, w);
+    out["sliver"] = shaped(cut.sliver(), n, 6);
+    return out;
+}
+
 py::array run(SolverHolder &h, const CArray<float> &signal) {
     if (signal.ndim() != 1) throw std::invalid_argument("run: the signal is 1-D");
     const std::size_t steps = static_cast<std::size_t>(signal.shape(0));
@@ -224,4 +284,52 @@ PYBIND11_MODULE(_native, m) {
         .def("run", &run, py::arg("signal"))
         .def("reset", [](SolverHolder &h) { h.solver->reset(); })
         .def("layout", &layout);
+
+    py::class_<FitHolder, std::shared_ptr<FitHolder>>(m, "CutFit")
+        .def(py::init(&make_fit), py::arg("vertices"), py::arg("faces"), py::arg("face_material"),
+             py::arg("materials"), py::arg("origin"), py::arg("cell"), py::arg("nx"), py::arg("ny"), py::arg("nz"),
+             py::arg("source"), py::arg("layer") = 0, py::arg("threads") = 0)
+        .def("cut_cells", &fit_cells)
+        .def("cut_air", [](const FitHolder &h) { return to_numpy(h.cut->air()); })
+        .def("cut_widths",
+             [](const FitHolder &h) {
+                 return py::make_tuple(to_numpy(h.cut->widths(0)), to_numpy(h.cut->widths(1)), to_numpy(h.cut->widths(2)));
+             })
+        .def_property_readonly("cut_stats",
+                               [](const FitHolder &h) {
+                                   const auto &st = h.cut->stats();
+                                   py::dict d;
+                                   d["cubes"] = st.cubes;
+                                   d["regions"] = st.regions;
+                                   d["squares"] = st.squares;
+                                   d["ties"] = st.ties;
+                                   d["dropped_area"] = st.dropped_area;
+                                   d["diagonal_area"] = st.diagonal_area;
+                                   d["far_volume"] = st.far_volume;
+                                   d["farthest"] = st.farthest;
+                                   d["air_cells"] = st.air_cells;
+                                   d["seconds"] = st.seconds;
+                                   return d;
+                               })
+        .def(
+            "cut_points",
+            [](const FitHolder &h, const CArray<double> &source, const CArray<double> &probes, std::size_t per_listener) {
+                const std::vector<as::Vec3> src = points_of(source, "source"), ps = points_of(probes, "probes");
+                if (src.size() != 1) throw std::invalid_argument("one source point");
+                const auto &n = h.cut->shape();
+                const auto fp = as::WaveSolver::FittedStencil(*h.cut, n[0], n[1], n[2], h.cut->cell())
+                                    .points(src[0], ps, per_listener);
+                auto cells = [](const std::vector<std::pair<std::size_t, double>> &v) {
+                    py::list l;
+                    for (const auto &[i, w] : v) l.append(py::make_tuple(i, w));
+                    return l;
+                };
+                py::dict out;
+                out["source"] = cells(fp.source);
+                py::list pl;
+                for (const auto &p : fp.probes) pl.append(cells(p));
+                out["probes"] = pl;
+                return out;
+            },
+            py::arg("source"), py::arg("probes"), py::arg("probes_per_listener") = 1);
 }

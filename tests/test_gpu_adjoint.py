@@ -87,11 +87,7 @@ def test_checkpointed_segments_give_the_same_gradient():
         np.testing.assert_allclose(pieces[key], whole[key], rtol=1e-10, atol=1e-14 * np.abs(whole[key]).max())
 
 
-def test_the_adjoint_refuses_a_matched_layer():
-    layout, signal, _ = load_golden("open_layer")
-    solver = B200WaveSolver(layout)
-    with pytest.raises(ValueError, match="matched layer"):
-        solver.gradient(signal[:10], np.zeros((solver.probes, 10)))
+# (grids with a matched layer: tests/test_layer_gradient.py)
 
 
 def test_gradient_of_a_builder_room_is_the_autograd_gradient():

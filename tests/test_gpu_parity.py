@@ -211,10 +211,42 @@ def test_gpu_autotuned_launch_shapes_step_as_the_oracle_does():
     # steps each cell with the same operations, so the run still equals the oracle's to the bit.
     w = layouts.polyhedral_room(0, cell=0.2, steps=200)
     gpu = B200WaveSolver(w.built.layout, autotune=True)
-    assert set(gpu.launch) == {"layer_blocks_per_sm", "special_blocks_per_sm"}
+    assert {"layer_blocks_per_sm", "special_blocks_per_sm", "tile_shape", "tile_planes"} <= set(gpu.launch)
     assert np.array_equal(_pieces(gpu, w.signal, [0, 64, 128, 200]), OracleSolver(w.built.layout).run(w.signal))
     with pytest.raises(ValueError, match="from rest"):
         gpu.autotune()
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64", "fp32c"])
+def test_gpu_every_tile_shape_steps_as_the_oracle_does(precision):
+    # The sweep's four tile shapes, each with a few planes a tile, on a room large enough for
+    # tiles whose cells are all interior (they load and check no cell types): every choice equals
+    # the oracle to the bit, whole state included, also when the shape changes between runs.
+    w = layouts.polyhedral_room(0, box=(4.0, 3.0, 2.0), cell=0.04, steps=90)
+    oracle = OracleSolver(w.built.layout, precision)
+    expected = oracle.run(w.signal)
+    state = oracle.state()
+    for shape, planes in [(0, 8), (1, 16), (2, 32), (3, 5), (1, 64)]:
+        gpu = B200WaveSolver(w.built.layout, precision=precision, autotune=False)
+        gpu.set_tiles(shape, planes)
+        t = gpu.tiles()
+        assert (t["tile_shape"], t["tile_planes"]) == (shape, planes)
+        assert t["tile_blocks_per_sm"] >= 1
+        got = np.concatenate([gpu.run(w.signal[:31]), gpu.run(w.signal[31:])], axis=1)
+        assert np.array_equal(got, expected), (shape, planes)
+        got_state = gpu.state()
+        for key in state:
+            assert np.array_equal(got_state[key], state[key]), (shape, planes, key)
+        gpu.close()
+    # changed mid-run, between pieces of odd length
+    gpu = B200WaveSolver(w.built.layout, precision=precision, autotune=False)
+    pieces = []
+    for (a, b), shape in zip([(0, 17), (17, 50), (50, 90)], [3, 1, 2]):
+        gpu.set_tiles(shape, 12)
+        pieces.append(gpu.run(w.signal[a:b]))
+    assert np.array_equal(np.concatenate(pieces, axis=1), expected)
+    with pytest.raises(ValueError, match="tile shape"):
+        gpu.set_tiles(4, 8)
 
 
 def test_gpu_an_expired_wait_is_a_status_and_the_handle_stays_usable():

@@ -1,0 +1,125 @@
+"""The reverse-time stepper through a matched layer against the autograd checker (needs a B200).
+
+On grids with a matched layer the B200 gradient carries the layer's own adjoint (its split-field
+states' adjoints, carried from step to step, and their terms on the pressures the states read)
+and gives, beside the rows' and branch states' coefficients, dL/d of the layer's twelve tables
+(keep and push of the centres and the faces per axis, fdtd.hpp:2219-2238). The checker steps the
+layer as the reference does (each cell its own copy of both faces) in float64 torch and
+differentiates it by autograd (tests/adjoint_reference.py, pinned on the CPU to the oracle and to
+exactly symmetric central differences). FP64 must equal it to 1e-9 of each array's largest value;
+FP32 its directional derivative to 1e-3. The damping's gradient, by the chain rule through the
+tables, must match a central difference of the loss with the room laid out again.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+from conftest import load_golden
+
+import adjoint_reference
+from acoustic_spaces_b200 import B200WaveSolver
+from acoustic_spaces_b200 import layouts as L
+from oracle.oracle import OracleSolver
+
+pytestmark = pytest.mark.gpu
+
+_TABLES = adjoint_reference.KEEP + adjoint_reference.PUSH
+_LAYER_GRIDS = ["open_layer", "fitted_open", "open_layer_speed"]
+
+
+def _problem(layout, signal, seed=0):
+    rng = np.random.default_rng(seed)
+    base = B200WaveSolver(layout, precision="fp64").run(signal)
+    target = 0.8 * base + 0.01 * np.abs(base).max() * rng.standard_normal(base.shape)
+    return target, adjoint_reference.gradient(layout, signal, 2.0 * (base - target))
+
+
+def _gradient(layout, signal, target, precision, segment=0, tape=0):
+    solver = B200WaveSolver(layout, precision=precision)
+    if tape:
+        solver.set_tape(tape)
+    y = solver.run(signal)
+    if not tape:
+        solver.reset()
+    return solver.gradient(signal, 2.0 * (y - target), segment=segment)
+
+
+def _keys(checker):
+    return [k for k in ("coef_b", "coef_inv", "now", "before", "gain", *_TABLES) if k in checker]
+
+
+@pytest.mark.parametrize("name", _LAYER_GRIDS)
+def test_fp64_layer_gradient_is_the_autograd_gradient(name):
+    layout, signal, _ = load_golden(name)
+    signal = signal[:240]
+    target, checker = _problem(layout, signal)
+    ours = _gradient(layout, signal, target, "fp64")
+    assert set(_TABLES) <= set(ours)
+    for key in _keys(checker):
+        scale = np.max(np.abs(checker[key])) if checker[key].size else 0.0
+        np.testing.assert_allclose(ours[key], checker[key], rtol=0, atol=1e-9 * scale, err_msg=key)
+
+
+@pytest.mark.parametrize("name", _LAYER_GRIDS)
+def test_fp32_layer_gradient_matches_the_autograd_gradient(name):
+    layout, signal, _ = load_golden(name)
+    signal = signal[:240]
+    target, checker = _problem(layout, signal)
+    ours = _gradient(layout, signal, target, "fp32")
+    rng = np.random.default_rng(7)
+    predicted = exact = 0.0
+    for key in _keys(checker):
+        direction = rng.uniform(-1.0, 1.0, len(checker[key]))
+        predicted += float(np.sum(ours[key] * direction))
+        exact += float(np.sum(checker[key] * direction))
+    assert abs(predicted - exact) <= 1e-3 * abs(exact), (predicted, exact)
+
+
+def test_layer_gradient_in_segments_and_from_a_tape_is_one_segments():
+    layout, signal, _ = load_golden("fitted_open")
+    signal = signal[:200]
+    target, _ = _problem(layout, signal)
+    whole = _gradient(layout, signal, target, "fp64", segment=0)
+    pieces = _gradient(layout, signal, target, "fp64", segment=37)
+    taped = _gradient(layout, signal, target, "fp64", segment=37, tape=37)
+    for key in whole:
+        scale = np.abs(whole[key]).max() if whole[key].size else 0.0
+        np.testing.assert_allclose(pieces[key], whole[key], rtol=1e-10, atol=1e-14 * scale, err_msg=key)
+        np.testing.assert_array_equal(taped[key], pieces[key], err_msg=key)
+
+
+def test_the_layer_damping_gradient_on_the_gpu_matches_central_differences():
+    # dL/d(layer damping) = the B200's tables' gradient times the tables' tangent in the damping
+    # (layouts.layer_tables_tangent), against a central difference of the loss (the FP64 oracle)
+    # with the room laid out again at damping -+ h: a 4 x 3 x 2.4 m convex room at 10 cm, open
+    # through one face into a 4-cell matched layer.
+    cell, box, layer, damping = 0.1, (4.0, 3.0, 2.4), 4, 0.5
+    rng = np.random.default_rng(3)
+    rate = 343.0 / (L.COURANT * cell)
+    room = L.convex_room(rng, box, faces=14, margin=cell * (layer + 3), open_face=1,
+                         material=lambda r: L.Material(float(r.uniform(0.02, 0.1))))  # fmt: skip
+    points = L.inside_points(rng, room, box, 5, 0.35, apart=0.35)
+    grid = L.Grid(-L.OFFSET * cell, cell, tuple(int(round(b / cell)) for b in box))
+    signal = L.gaussian_drive(rate, 150)
+
+    def built(value):
+        return L.cell_face_layout(room, grid, points[0], points[1:], layer=layer, layer_damping=value).layout
+
+    lay = built(damping)
+    y = OracleSolver(lay, "fp64").run(signal)
+    target = 0.7 * y
+    solver = B200WaveSolver(lay, precision="fp64")
+    grad = solver.gradient(signal, 2.0 * (y - target), segment=50)
+    courant = float(np.sqrt(np.float64(np.asarray(lay["weights"], np.float32)[0])))
+    predicted = 0.0
+    for a, axis in enumerate("xyz"):
+        t = L.layer_tables_tangent(int(grid.shape[a]), layer, damping, courant)
+        for table, kind in ((f"keep_{axis}", "keep"), (f"push_{axis}", "push"), (f"keep_face_{axis}", "keep_face"),
+                            (f"push_face_{axis}", "push_face")):  # fmt: skip
+            predicted += float(np.sum(grad[table] * t[kind]))
+    h = 0.01 * damping
+    loss = lambda value: float(np.sum((OracleSolver(built(value), "fp64").run(signal) - target) ** 2))  # noqa: E731
+    measured = (loss(damping + h) - loss(damping - h)) / (2.0 * h)
+    assert abs(measured) > 0.0
+    assert abs(predicted - measured) <= 2e-3 * abs(measured), (predicted, measured)
