@@ -696,6 +696,79 @@ def fit_from_cut(cut: Cut, room: L.Room, grid: L.Grid, *, layer: int = 0) -> Fit
         np.add.at(wall_area[:, M], row_index[uncut_rows[to_edge]], face_area(uncut_rows[to_edge], k6 // 2))
         np.add.at(open_area[:, k6], row_index[uncut_rows[to_air]], face_area(uncut_rows[to_air], k6 // 2))
     sliver = np.where(sliver_area > 1e-9, sliver / np.where(sliver_area > 1e-9, sliver_area, 1.0), 0.0)
+
+    # The conduit rule (thin_conduits, cut_cells.hpp:5190-5360): a region of the air outside its
+    # owner's cube (round a convex edge of the walls whose faces lie just inside the grid's
+    # planes, a thin L of air) has its open area to an edge-diagonal neighbour n of its owner o
+    # scaled by phi = 2 V / (A_s A_p) (V its volume, A_s its open area to o's own cube, A_p its
+    # open area through the link) where that is below 1 - 1e-12, and a share
+    # (1 - phi) A_p / (A_s + the sum of its A_p) of its walls moves from o's row to n's.
+    diag = ~same & rowa & rowb & (kd >= 6)
+    if np.any(diag):
+        pl, ph, pa_, da, db_, kk = p_low[diag], p_high[diag], p_area[diag], oa[diag], ob[diag], kd[diag]
+        ca_, cb_ = reg_cell[pl] != da, reg_cell[ph] != db_
+        link_g = np.concatenate([pl[ca_], ph[cb_]])
+        link_k = np.concatenate([kk[ca_], opp[kk[cb_]]])
+        link_a = np.concatenate([pa_[ca_], pa_[cb_]])
+        lkey = link_g * 18 + link_k
+        keys_u, inv = np.unique(lkey, return_inverse=True)
+        through = np.zeros(len(keys_u))
+        np.add.at(through, inv, link_a)
+        lg, lk = keys_u // 18, keys_u % 18
+        conduits = np.unique(lg)
+        # A_s: each conduit's open area to the regions of its owner's own cube.
+        contact = np.zeros(len(conduits))
+        sm = same & (oa >= 0)
+        ia_, ib_ = reg_cell[p_low] == oa, reg_cell[p_high] == oa
+        one = sm & (ia_ != ib_)
+        gg = np.where(ia_, p_high, p_low)[one]
+        at = np.searchsorted(conduits, gg)
+        hit = (at < len(conduits)) & (conduits[np.minimum(at, len(conduits) - 1)] == gg)
+        np.add.at(contact, at[hit], p_area[one][hit])
+        ci_ = np.searchsorted(conduits, lg)
+        a_s = contact[ci_]
+        kc = _direction(grid, owner[lg], reg_cell[lg])
+        ok_link = (kc >= 0) & (kc < 6) & (a_s > 0.0) & (through > 0.0)
+        ratio = np.where(ok_link, 2.0 * reg_volume[lg] / np.where(ok_link, a_s * through, 1.0), 1.0)
+        phi = np.where(ok_link & (ratio < 1.0 - 1e-12), ratio, 1.0)
+        if np.any(phi < 1.0):
+            def phi_of(g, k):
+                key_ = g * 18 + k
+                at_ = np.searchsorted(keys_u, key_)
+                return phi[np.minimum(at_, len(keys_u) - 1)]
+
+            f = np.ones(len(pl))
+            f = np.where(ca_, f * phi_of(pl, kk), f)
+            f = np.where(cb_, f * phi_of(ph, opp[kk]), f)
+            ra, rb = row_index[da], row_index[db_]
+            marked = np.zeros((R, 18), bool)
+            marked[ra[f < 1.0], kk[f < 1.0]] = True
+            marked[rb[f < 1.0], opp[kk[f < 1.0]]] = True
+            plain = np.zeros((R, 18))
+            scaled = np.zeros((R, 18))
+            for rr, kq in ((ra, kk), (rb, opp[kk])):
+                m_ = marked[rr, kq]
+                np.add.at(plain, (rr[m_], kq[m_]), pa_[m_])
+                np.add.at(scaled, (rr[m_], kq[m_]), pa_[m_] * f[m_])
+            open_area = np.where(marked, scaled, open_area)
+            # The walls: each link's share of its conduit's walls, to the diagonal neighbour's row.
+            spans = contact.copy()
+            np.add.at(spans, ci_, through)
+            share = (1.0 - phi) * through / spans[ci_]
+            o_ = owner[lg]
+            across = o_ + np.array([int(d[0] + d[1] * sy + d[2] * sz) for d in STEPS], np.int64)[lk]
+            moving = (share > 0.0) & is_row_cell[across]
+            for link in np.flatnonzero(moving):
+                g = int(lg[link])
+                if g >= 2 * C:
+                    continue  # a whole cell has no walls
+                ro_, rn_ = row_index[o_[link]], row_index[across[link]]
+                sides = 2.0 if joined[g // 2] else 1.0
+                for wf in walls:
+                    a_ = sides * caps[g // 2, wf]
+                    if a_ > 0.0:
+                        wall_area[ro_, wf] -= share[link] * a_
+                        wall_area[rn_, wf] += share[link] * a_
     return Fit(rows.astype(np.int64), air_volume, open_area, wall_area, sliver, air, (wx, wy, wz))
 
 

@@ -230,7 +230,8 @@ def build_workload(args, barrier: bool = True):
 
     if args.workload == "outdoor_halfspace":
         return layouts.outdoor_halfspace(args.seed, steps=max(args.steps, args.ir_steps), barrier=barrier)
-    return layouts.polyhedral_room(args.seed, cell=args.cell, steps=max(args.steps, args.ir_steps, 1))
+    return layouts.polyhedral_room(args.seed, cell=args.cell, steps=max(args.steps, args.ir_steps, 1), walls=args.walls,
+                                   device=int(os.environ.get("LOCAL_RANK", "0")))  # fmt: skip
 
 
 def insertion_loss(free: np.ndarray, screened: np.ndarray, rate: float, band=(20.0, 300.0)) -> tuple[np.ndarray, np.ndarray]:
@@ -283,7 +284,7 @@ def oracle_cores(layout) -> int:
     return int(oracle.load_oracle().oracle_threads()) if cells >= oracle.PARALLEL_CELLS else 1
 
 
-def cpu_reference_rate(workload, sample_steps: int, warmup: int = 3) -> dict:
+def cpu_reference_rate(workload, sample_steps: int, warmup: int = 3, fitted_walls: bool = False) -> dict:
     """The reference's own CPU solver (its unmodified C++, oracle/_ref) on the same room, timed
     over ``sample_steps`` steps with every host thread; else the oracle's C port, on every host
     thread too where the grid is large."""
@@ -309,7 +310,8 @@ def cpu_reference_rate(workload, sample_steps: int, warmup: int = 3) -> dict:
         solver = native.WaveSolver(
             native.Bvh(vertices, faces), owner, beta, np.ascontiguousarray(np.vstack(rows)),
             np.concatenate(owners), grid.origin, grid.cell, *grid.shape, workload.source,
-            workload.receivers, layer=8, layer_damping=0.5, threads=threads,
+            workload.receivers, layer=8, layer_damping=0.5, threads=threads, fitted_walls=fitted_walls,
+            vertices=np.ascontiguousarray(vertices), faces=np.ascontiguousarray(faces),
         )  # fmt: skip
         setup = time.perf_counter() - t0
         solver.run(workload.signal[:warmup])  # its threads spun up, untimed
@@ -320,7 +322,8 @@ def cpu_reference_rate(workload, sample_steps: int, warmup: int = 3) -> dict:
         kind, cores, ref_air = "reference", int(solver.threads), int(solver.air_cells)
         if ref_air != air:
             raise RuntimeError(f"the reference lays the room out with {ref_air} air cells, the builder {air}")
-        extra = {"setup_s": round(setup, 2)}
+        extra = {"setup_s": round(setup, 2), "walls": "the reference's own fitted walls (its exact fit) of the same room"
+                 if fitted_walls else "cell faces"}  # fmt: skip
     else:
         ported = oracle.OracleSolver(workload.built.layout)
         ported.run(workload.signal[:warmup])
@@ -344,13 +347,23 @@ def cpu_reference_rate(workload, sample_steps: int, warmup: int = 3) -> dict:
 def run_reference(args, rank: int, world: int) -> None:
     if rank != 0:
         return
+    # The room as the host lays it out (no GPU on this arm): the reference builds its own layout of
+    # it, with its own fitted walls where those are asked for, and is checked to hold the same air.
+    fitted_walls = args.walls == "fitted" and args.workload == "polyhedral_room"
+    walls = args.walls
+    args.walls = "faces"
     workload = build_workload(args)
+    args.walls = walls
+    if fitted_walls:
+        workload.description["walls"] = "fitted cut cells (the reference's own exact fit), 2-pole admittance per wall"
+        for key in ("special_rows", "links", "branch_states", "interior_cells"):
+            workload.description.pop(key, None)
     steps = max(1, min(args.steps, args.reference_steps))
     warmup = max(3, args.warmup)
     times = []
     base = None
     for _ in range(max(1, args.reference_repeats)):
-        base = cpu_reference_rate(workload, steps, warmup)
+        base = cpu_reference_rate(workload, steps, warmup, fitted_walls)
         times.append(base["value"])
     value = statistics.median(times)
     base["value"] = round(value, 4)
@@ -816,6 +829,12 @@ def main() -> None:
     parser.add_argument("--impl", choices=["b200", "reference"], default="b200")
     parser.add_argument("--seed", type=int, default=0)
     parser.add_argument("--cell", type=float, default=0.04, help="cell size in metres (0.04: the full workload)")
+    parser.add_argument("--walls", choices=["fitted", "faces"], default="fitted",
+                        help="the polyhedral room's walls: fitted cut cells (the configuration's) or on cell faces")  # fmt: skip
+    parser.add_argument("--no-compensated", action="store_true", help="skip the compensated-precision leg")
+    parser.add_argument("--gradient-steps", type=int, default=200,
+                        help="steps of the forward + adjoint timing on the polyhedral room (0: skip)")  # fmt: skip
+    parser.add_argument("--gradient-segment", type=int, default=50)
     parser.add_argument("--no-fp64-rate", action="store_true", help="skip timing the FP64 stepper alike")
     parser.add_argument("--launch", default="", help="layer,special blocks per SM (skips the autotuner)")
     parser.add_argument("--slabs", action="store_true",
@@ -837,7 +856,8 @@ def main() -> None:
     parser.add_argument("--sequential-sample", type=int, default=16)
     parser.add_argument("--no-ir-error", action="store_true")
     parser.add_argument("--kernel-steps", type=int, default=200, help="steps of the per-kernel timing pass")
-    parser.add_argument("--ir-steps", type=int, default=2000, help="steps of the FP32-vs-FP64 comparison")
+    parser.add_argument("--ir-steps", type=int, default=12000,
+                        help="steps of the FP32-vs-FP64 comparison (12000: the configuration's full length)")  # fmt: skip
     args = parser.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -977,6 +997,7 @@ def main() -> None:
 
     # The IR error against FP64 on the same grid: both run from rest over the same drive.
     ir_error = None
+    p64 = None
     if not args.no_ir_error:
         fp64 = B200WaveSolver(workload.built.layout, precision="fp64", device=local)
         m = min(args.ir_steps, len(signal))
@@ -987,6 +1008,72 @@ def main() -> None:
         ir_error = ir_errors(p32, p64, workload.built.rate)
         ir_error["steps"] = m
         ir_error["vs"] = "the same layout stepped in FP64 on the GPU (bit-exact with the FP64 oracle on the golden grids)"
+
+    # The compensated single precision on the same grid, device-timed alike, with its IR error
+    # over the same steps: the mode that meets the 1e-4 bar over the configuration's full length.
+    compensated = None
+    if args.precision == "fp32" and not args.no_compensated:
+        comp = B200WaveSolver(workload.built.layout, precision="fp32c", device=local)
+        comp.run_device(sig_dev.data_ptr(), warmup, out_dev.data_ptr(), steps + warmup)
+        comp.synchronize()
+        sc = torch.cuda.ExternalStream(comp.stream, device=f"cuda:{local}")
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(sc)
+        comp.run_device(sig_dev.data_ptr() + 4 * warmup, steps, out_dev.data_ptr() + 8 * warmup, steps + warmup)
+        e1.record(sc)
+        comp.synchronize()
+        comp_ms = e0.elapsed_time(e1)
+        compensated = {
+            "value": round(air * steps / (comp_ms / 1e3) / 1e9, 4),
+            "unit": UNIT,
+            "ms_per_step": round(comp_ms / steps, 5),
+            "what": "the same grid in compensated FP32 (each cell's pressure and its increment), device-timed alike",
+        }
+        if p64 is not None:
+            comp.reset()
+            pc = comp.run(signal[: p64.shape[1]])
+            compensated["ir_error_vs_fp64"] = {**ir_errors(pc, p64, workload.built.rate), "steps": int(p64.shape[1])}
+        comp.close()
+
+    # Forward + adjoint against forward on the same grid (the gradient in the walls' coefficients
+    # and, with a matched layer, its tables), checkpoints every `gradient_segment` steps: a taped
+    # forward run keeps them, the gradient recomputes each segment from them and steps back.
+    adjoint = None
+    if args.gradient_steps > 0 and workload.name == "polyhedral_room":
+        try:
+            g_steps = min(args.gradient_steps, len(signal))
+            grad_solver = B200WaveSolver(workload.built.layout, device=local, autotune=False)
+            grad_solver.launch = solver.launch
+            head = np.ascontiguousarray(signal[:g_steps])
+            y = grad_solver.run(head)
+            dloss = 2.0 * (y - 0.9 * y)
+            grad_solver.reset()
+            grad_solver.gradient(head, dloss, segment=args.gradient_segment)  # set-up of the adjoint, untimed
+            grad_solver.reset()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            grad_solver.run(head)
+            forward_s = time.perf_counter() - t0
+            grad_solver.reset()
+            grad_solver.set_tape(args.gradient_segment)
+            t0 = time.perf_counter()
+            grad_solver.run(head)
+            grads = grad_solver.gradient(head, dloss, segment=args.gradient_segment)
+            both_s = time.perf_counter() - t0
+            adjoint = {
+                "ratio": round(both_s / forward_s, 3),
+                "steps": g_steps,
+                "segment": args.gradient_segment,
+                "forward_s": round(forward_s, 4),
+                "forward_and_adjoint_s": round(both_s, 4),
+                "finite": bool(all(np.isfinite(v).all() for v in grads.values())),
+                "layer_tables": bool(any(k.startswith("keep") for k in grads)),
+                "what": "taped forward (checkpoints) + gradient over the same steps, against a plain forward run; wall "
+                        "clock through B200WaveSolver",
+            }  # fmt: skip
+            grad_solver.close()
+        except Exception as error:  # reported, not required
+            adjoint = {"ratio": None, "error": str(error)[:300]}
     insertion = None
     if args.workload == "outdoor_halfspace" and not args.no_ir_error:
         insertion = outdoor_insertion_loss(args, workload, local)
@@ -1023,7 +1110,7 @@ def main() -> None:
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
             try:
-                cpu = cpu_reference_rate(workload, args.cpu_steps)
+                cpu = cpu_reference_rate(workload, args.cpu_steps, fitted_walls=args.walls == "fitted")
             except Exception as error:  # the baseline is reported, not required
                 cpu = {"value": None, "unit": UNIT, "error": str(error)[:200]}
         line = {
@@ -1075,7 +1162,8 @@ def main() -> None:
             "ir_error_vs_fp64": ir_error,
             "fp64_same_gpu": fp64_rate,
             "insertion_loss_vs_fp64": insertion,
-            "adjoint_over_forward": None,
+            "adjoint_over_forward": adjoint,
+            "compensated": compensated,
             "clocks": clocks.summary(),
             "finite": finite,
         }
