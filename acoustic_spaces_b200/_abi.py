@@ -147,6 +147,17 @@ class FdtdCutCells(ctypes.Structure):
     ]
 
 
+class FdtdPlaneLink(ctypes.Structure):
+    """``struct fdtd_plane_link`` (include/fdtd_b200.h)."""
+
+    _fields_ = [
+        ("from_", ctypes.c_uint32),
+        ("to", ctypes.c_uint32),
+        ("from_plane", ctypes.c_uint64),
+        ("to_plane", ctypes.c_uint64),
+    ]
+
+
 #: The axis tables of the matched layer, in the order of fdtd_layout.keep / .push.
 KEEP = ("keep_x", "keep_face_x", "keep_y", "keep_face_y", "keep_z", "keep_face_z")
 PUSH = ("push_x", "push_face_x", "push_y", "push_face_y", "push_z", "push_face_z")
@@ -283,6 +294,11 @@ SIGNATURES = {
     "fdtd_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_int),
                                      ctypes.POINTER(ctypes.c_int)]),
     "fdtd_set_launch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    "fdtd_run_linked": (
+        ctypes.c_int,
+        [ctypes.POINTER(ctypes.c_void_p), ctypes.c_uint32, ctypes.POINTER(FdtdPlaneLink), ctypes.c_uint32,
+         ctypes.POINTER(ctypes.c_void_p), ctypes.c_uint64, ctypes.POINTER(ctypes.c_void_p), ctypes.c_uint64],
+    ),
     "fdtd_set_tiles": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_uint64]),
     "fdtd_get_tiles": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(FdtdTiles)]),
     "fdtd_level_plane": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int,

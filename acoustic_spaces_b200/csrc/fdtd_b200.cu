@@ -2091,6 +2091,109 @@ int fdtd_level_plane(fdtd_solver *s, uint64_t z, int which, void **ptr, uint64_t
     return FDTD_OK;
 }
 
+int fdtd_run_linked(fdtd_solver *const *solvers, uint32_t count, const fdtd_plane_link *links, uint32_t link_count,
+                    const float *const *d_signals, uint64_t steps, double *const *d_outs, uint64_t out_stride) {
+    if (!solvers || count == 0) return set_global(FDTD_EINVAL, "no solvers to run");
+    if (link_count && !links) return set_global(FDTD_EINVAL, "no links");
+    if (!d_signals) return set_global(FDTD_EINVAL, "no signals");
+    for (uint32_t h = 0; h < count; ++h) {
+        fdtd_solver *s = solvers[h];
+        if (!s) return set_global(FDTD_EINVAL, "a null solver in the group");
+        if (!d_signals[h]) return fail(s, FDTD_EINVAL, "no signal for a solver of the group");
+        if (s->probes && (!d_outs || !d_outs[h])) return fail(s, FDTD_EINVAL, "no output buffer for a solver of the group");
+        if (s->probes && out_stride < steps) return fail(s, FDTD_EINVAL, "the output's stride is shorter than the run");
+        if (s->precision != solvers[0]->precision)
+            return set_global(FDTD_EINVAL, "the group's solvers step in one precision");
+        for (uint32_t g = 0; g < h; ++g)
+            if (solvers[g] == s) return set_global(FDTD_EINVAL, "a solver appears twice in the group");
+    }
+    const size_t e = solvers[0]->precision == FDTD_FP64 ? 8 : 4;
+    for (uint32_t l = 0; l < link_count; ++l) {
+        const fdtd_plane_link &k = links[l];
+        if (k.from >= count || k.to >= count || k.from == k.to) return set_global(FDTD_EINVAL, "a link joins no two solvers of the group");
+        const fdtd_solver *a = solvers[k.from], *b = solvers[k.to];
+        if (k.from_plane >= a->nz || k.to_plane >= b->nz) return set_global(FDTD_EINVAL, "a link's plane lies outside its grid");
+        if (a->pitch != b->pitch || a->ny != b->ny) return set_global(FDTD_EINVAL, "linked grids have planes of different sizes");
+        // Only a plane of solid cells (nothing of its own steps it) may be filled from another grid.
+        for (uint64_t y = 0; y < b->ny; ++y)
+            for (uint64_t x = 0; x < b->nx; ++x)
+                if (b->host_types.size() && b->host_types[x + b->pitch * (y + b->ny * k.to_plane)] != kSolid)
+                    return set_global(FDTD_EINVAL, "a link fills a plane that holds air of its own grid");
+    }
+    if (steps == 0) return FDTD_OK;
+    // Peer access between the devices the links join (a no-op where it is already on).
+    for (uint32_t l = 0; l < link_count; ++l) {
+        const int da = solvers[links[l].from]->device, db = solvers[links[l].to]->device;
+        if (da == db) continue;
+        int can = 0;
+        cudaDeviceCanAccessPeer(&can, da, db);
+        if (can) {
+            DeviceGuard guard(da);
+            const cudaError_t pe = cudaDeviceEnablePeerAccess(db, 0);
+            if (pe != cudaSuccess && pe != cudaErrorPeerAccessAlreadyEnabled) return cuda_fail(solvers[0], pe, "cudaDeviceEnablePeerAccess");
+            cudaGetLastError();
+        }
+    }
+    // Per solver, the event after its step and the copies out of it (its neighbours' next step
+    // waits for it).
+    std::vector<cudaEvent_t> copied(count, nullptr);
+    auto release_events = [&]() {
+        for (cudaEvent_t ev : copied)
+            if (ev) cudaEventDestroy(ev);
+    };
+    for (uint32_t h = 0; h < count; ++h) {
+        DeviceGuard guard(solvers[h]->device);
+        const cudaError_t ce = cudaEventCreateWithFlags(&copied[h], cudaEventDisableTiming);
+        if (ce != cudaSuccess) {
+            release_events();
+            return cuda_fail(solvers[h], ce, "cudaEventCreate");
+        }
+    }
+    int rc = FDTD_OK;
+    for (uint64_t k = 0; k < steps && rc == FDTD_OK; ++k) {
+        // Each solver's step k, after the planes its neighbours sent it at step k - 1.
+        for (uint32_t h = 0; h < count && rc == FDTD_OK; ++h) {
+            fdtd_solver *s = solvers[h];
+            DeviceGuard guard(s->device);
+            if (k > 0)
+                for (uint32_t l = 0; l < link_count; ++l)
+                    if (links[l].to == h) {
+                        const cudaError_t we = cudaStreamWaitEvent(s->stream, copied[links[l].from], 0);
+                        if (we != cudaSuccess) rc = cuda_fail(s, we, "cudaStreamWaitEvent");
+                    }
+            if (rc == FDTD_OK) rc = dispatch(s, d_signals[h] + k, 1, d_outs ? d_outs[h] + k : nullptr, out_stride);
+            if (rc == FDTD_OK) settle(s, 1);
+        }
+        // Then the planes of the new levels, each on its source's stream after its step.
+        for (uint32_t l = 0; l < link_count && rc == FDTD_OK; ++l) {
+            fdtd_solver *a = solvers[links[l].from], *b = solvers[links[l].to];
+            DeviceGuard guard(a->device);
+            const uint64_t plane = e * a->pitch * a->ny;
+            const char *src = static_cast<const char *>(a->u[1]) + plane * links[l].from_plane;
+            char *dst = static_cast<char *>(b->u[1]) + plane * links[l].to_plane;
+            const cudaError_t me = a->device == b->device
+                                       ? cudaMemcpyAsync(dst, src, plane, cudaMemcpyDeviceToDevice, a->stream)
+                                       : cudaMemcpyPeerAsync(dst, b->device, src, a->device, plane, a->stream);
+            if (me != cudaSuccess) rc = cuda_fail(a, me, "the plane's copy");
+        }
+        for (uint32_t h = 0; h < count && rc == FDTD_OK; ++h) {
+            DeviceGuard guard(solvers[h]->device);
+            const cudaError_t re = cudaEventRecord(copied[h], solvers[h]->stream);
+            if (re != cudaSuccess) rc = cuda_fail(solvers[h], re, "cudaEventRecord");
+        }
+    }
+    // Every solver's stream ends after the copies into its grid (its level is then complete).
+    for (uint32_t l = 0; l < link_count && rc == FDTD_OK; ++l) {
+        fdtd_solver *b = solvers[links[l].to];
+        DeviceGuard guard(b->device);
+        const cudaError_t we = cudaStreamWaitEvent(b->stream, copied[links[l].from], 0);
+        if (we != cudaSuccess) rc = cuda_fail(b, we, "cudaStreamWaitEvent");
+    }
+    // (Destroying an event whose work is pending is allowed: it is released when it completes.)
+    release_events();
+    return rc;
+}
+
 int fdtd_set_launch(fdtd_solver *s, int layer_per_sm, int special_per_sm) {
     if (!s) return set_global(FDTD_EINVAL, "no solver");
     if (layer_per_sm < 0 || special_per_sm < 0 || layer_per_sm > 64 || special_per_sm > 64)

@@ -43,6 +43,21 @@ STEPS = np.array(
 SOLID, AIR, LAYER = 0, 1, 2
 
 
+def _edge(grid: L.Grid) -> np.ndarray:
+    """Whether each cell lies on the grid's edge (x fastest)."""
+    nx, ny, nz = grid.shape
+    e = [np.zeros(m, bool) for m in (nx, ny, nz)]
+    for a in e:
+        a[0] = a[-1] = True
+    return (e[2][:, None, None] | e[1][None, :, None] | e[0][None, None, :]).reshape(-1)
+
+
+def _accumulate(target: np.ndarray, index: np.ndarray, values) -> None:
+    """target[index] += values for repeated indices (a flat view of target), by bincount."""
+    flat = target.reshape(-1)
+    flat += np.bincount(np.asarray(index, np.int64), np.broadcast_to(values, np.shape(index)), minlength=flat.size)
+
+
 def opposite(k: int) -> int:
     """The direction opposite k (fdtd.hpp:929)."""
     return k ^ 1 if k < 6 else 6 + 4 * ((k - 6) // 4) + 3 - (k - 6) % 4
@@ -90,15 +105,13 @@ def set_up_fitted(
     n = nx * ny * nz
     sy, sz = nx, nx * ny
     offsets = STEPS[:, 0] + STEPS[:, 1] * sy + STEPS[:, 2] * sz
-    idx = np.arange(n, dtype=np.int64)
-    x, y, z = idx % nx, (idx // nx) % ny, idx // sz
 
     # The cells' kinds (fdtd.hpp:976-995).
     types = np.zeros(n, np.uint8)
     types[fit.air == AIR] = 1
     types[fit.air == LAYER] = 3
     layer_cells = np.flatnonzero(types == 3).astype(np.int64)
-    edge = (x == 0) | (y == 0) | (z == 0) | (x == nx - 1) | (y == ny - 1) | (z == nz - 1)
+    edge = _edge(grid)
 
     # The stencil (set_up_stencil, fdtd.hpp:1649-1670).
     exact = 1.0 / 3.0
@@ -512,19 +525,23 @@ def fit_from_cut(cut: Cut, room: L.Room, grid: L.Grid, *, layer: int = 0) -> Fit
     nx, ny, nz = grid.shape
     n = nx * ny * nz
     sy, sz = nx, nx * ny
-    idx = np.arange(n, dtype=np.int64)
-    x, y, z = idx % nx, (idx // nx) % ny, idx // sz
-    edge = (x == 0) | (y == 0) | (z == 0) | (x == nx - 1) | (y == ny - 1) | (z == nz - 1)
-    depth = np.minimum.reduce([x, y, z, nx - 1 - x, ny - 1 - y, nz - 1 - z])
+    edge = _edge(grid)
+    ax_depth = [np.minimum(np.arange(m), m - 1 - np.arange(m)).astype(np.int32) for m in (nx, ny, nz)]
+    depth = np.minimum(np.minimum(ax_depth[2][:, None, None], ax_depth[1][None, :, None]),
+                       ax_depth[0][None, None, :]).reshape(-1)  # fmt: skip
     normals, offsets, open_ = cut_room(room, grid)
     walls = np.flatnonzero(open_ == 0)
     # The air: with an open face every cell but the grid's edge; closed, the cells whose centre
     # lies inside the walls. Cells within `layer` of the edge form the matched layer.
-    centres = np.stack([grid.centres(0)[x], grid.centres(1)[y], grid.centres(2)[z]], axis=1) if not room.open else None
     if room.open:
         air_mask = ~edge
     else:
-        air_mask = ~edge & np.all(centres @ normals[walls].T - offsets[walls] < 0.0, axis=1)
+        inside = np.ones((nz, ny, nx), bool)
+        cz, cy, cx_ = (grid.centres(a) for a in (2, 1, 0))
+        for f in walls:
+            nf = normals[f]
+            inside &= (nf[0] * cx_[None, None, :] + nf[1] * cy[None, :, None] + nf[2] * cz[:, None, None]) - offsets[f] < 0.0
+        air_mask = ~edge & inside.reshape(-1)
     air = np.where(air_mask, AIR, SOLID).astype(np.uint8)
     if layer > 0:
         air[air_mask & (depth <= layer)] = LAYER
@@ -658,15 +675,15 @@ def fit_from_cut(cut: Cut, room: L.Room, grid: L.Grid, *, layer: int = 0) -> Fit
     g_ok[owned] = is_row_cell[owner[owned]]
     gr = np.flatnonzero(g_ok)
     ro = row_index[owner[gr]]
-    np.add.at(air_volume, ro, reg_volume[gr])
+    _accumulate(air_volume, ro, reg_volume[gr])
     # walls: both sides of a wall see it (a cut cell's inside and outside regions)
     cut_g = gr[gr < 2 * C]
     both_sides = np.where(joined[cut_g // 2], 2.0, 1.0)  # a joined region sees each wall's two sides
     for f in walls:
-        np.add.at(wall_area[:, f], row_index[owner[cut_g]], both_sides * caps[cut_g // 2, f])
+        _accumulate(wall_area, row_index[owner[cut_g]] * (M + 1) + f, both_sides * caps[cut_g // 2, f])
     k = _direction(grid, owner[gr], reg_cell[gr])
     ax = (k >= 0) & (k < 6)
-    np.add.at(sliver, (ro[ax], k[ax]), reg_volume[gr][ax])
+    _accumulate(sliver, ro[ax] * 6 + k[ax], reg_volume[gr][ax])
     oa, ob = owner[p_low], owner[p_high]
     rowa = (oa >= 0) & is_row_cell[np.maximum(oa, 0)]
     rowb = (ob >= 0) & is_row_cell[np.maximum(ob, 0)]
@@ -676,16 +693,16 @@ def fit_from_cut(cut: Cut, room: L.Room, grid: L.Grid, *, layer: int = 0) -> Fit
     other = np.where(ca == oa, cb, ca)
     ks = _direction(grid, oa, other)
     sl &= (ks >= 0) & (ks < 6)
-    np.add.at(sliver_area, (row_index[oa[sl]], ks[sl]), p_area[sl])
+    _accumulate(sliver_area, row_index[oa[sl]] * 6 + ks[sl], p_area[sl])
     diff = ~same & (oa >= 0) & (ob >= 0)
     kd = _direction(grid, oa, ob)
     both = rowa & rowb
     link = diff & (kd >= 0) & ((kd < 6) | both)
     ka = link & rowa
-    np.add.at(open_area, (row_index[oa[ka]], kd[ka]), p_area[ka])
+    _accumulate(open_area, row_index[oa[ka]] * 18 + kd[ka], p_area[ka])
     kb = link & rowb
     opp = np.array([opposite(k) for k in range(18)], np.int64)
-    np.add.at(open_area, (row_index[ob[kb]], opp[kd[kb]]), p_area[kb])
+    _accumulate(open_area, row_index[ob[kb]] * 18 + opp[kd[kb]], p_area[kb])
     # A row's faces that no square was cut for: whole (its cell and the one across both uncut).
     uncut_rows = rows[cut_index[rows] < 0]
     for k6 in range(6):
@@ -693,8 +710,8 @@ def fit_from_cut(cut: Cut, room: L.Room, grid: L.Grid, *, layer: int = 0) -> Fit
         whole_face = cut_index[j] < 0
         to_edge = whole_face & edge[j]
         to_air = whole_face & ~edge[j] & (air[j] != SOLID)
-        np.add.at(wall_area[:, M], row_index[uncut_rows[to_edge]], face_area(uncut_rows[to_edge], k6 // 2))
-        np.add.at(open_area[:, k6], row_index[uncut_rows[to_air]], face_area(uncut_rows[to_air], k6 // 2))
+        _accumulate(wall_area, row_index[uncut_rows[to_edge]] * (M + 1) + M, face_area(uncut_rows[to_edge], k6 // 2))
+        _accumulate(open_area, row_index[uncut_rows[to_air]] * 18 + k6, face_area(uncut_rows[to_air], k6 // 2))
     sliver = np.where(sliver_area > 1e-9, sliver / np.where(sliver_area > 1e-9, sliver_area, 1.0), 0.0)
 
     # The conduit rule (thin_conduits, cut_cells.hpp:5190-5360): a region of the air outside its
@@ -757,18 +774,16 @@ def fit_from_cut(cut: Cut, room: L.Room, grid: L.Grid, *, layer: int = 0) -> Fit
             share = (1.0 - phi) * through / spans[ci_]
             o_ = owner[lg]
             across = o_ + np.array([int(d[0] + d[1] * sy + d[2] * sz) for d in STEPS], np.int64)[lk]
-            moving = (share > 0.0) & is_row_cell[across]
-            for link in np.flatnonzero(moving):
-                g = int(lg[link])
-                if g >= 2 * C:
-                    continue  # a whole cell has no walls
-                ro_, rn_ = row_index[o_[link]], row_index[across[link]]
-                sides = 2.0 if joined[g // 2] else 1.0
-                for wf in walls:
-                    a_ = sides * caps[g // 2, wf]
-                    if a_ > 0.0:
-                        wall_area[ro_, wf] -= share[link] * a_
-                        wall_area[rn_, wf] += share[link] * a_
+            # (in the order of the links, conduit by conduit; a whole cell has no walls)
+            moving = np.flatnonzero((share > 0.0) & is_row_cell[across] & (lg < 2 * C))
+            ro_, rn_ = row_index[o_[moving]], row_index[across[moving]]
+            gl = lg[moving] // 2
+            sides = np.where(joined[gl], 2.0, 1.0)
+            for wf in walls:
+                a_ = sides * caps[gl, wf]
+                has = a_ > 0.0
+                np.subtract.at(wall_area[:, wf], ro_[has], share[moving][has] * a_[has])
+                np.add.at(wall_area[:, wf], rn_[has], share[moving][has] * a_[has])
     return Fit(rows.astype(np.int64), air_volume, open_area, wall_area, sliver, air, (wx, wy, wz))
 
 

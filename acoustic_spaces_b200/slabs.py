@@ -278,3 +278,51 @@ def gather_records(slabs: Sequence[Slab], records: Sequence[np.ndarray], probes:
         for j, p in enumerate(s.probes):
             out[p] = rec[j]
     return out
+
+
+def links(slabs: Sequence[Slab]) -> list[tuple[int, int, int, int]]:
+    """The plane copies after each step, (from slab, to slab, its plane, their plane): each slab's
+    first and last planes into its neighbours' ghost planes."""
+    out = []
+    for r in range(len(slabs) - 1):
+        lower, upper = slabs[r], slabs[r + 1]
+        out.append((r, r + 1, lower.z1 - 1 - lower.lo, 0))
+        out.append((r + 1, r, upper.z0 - upper.lo, lower.hi - 1 - lower.lo))
+    return out
+
+
+def run_linked(solvers: Sequence, slabs: Sequence[Slab], signal: np.ndarray, *, device_buffers=None) -> list[np.ndarray]:
+    """Steps every slab of one grid together in the library (fdtd_run_linked): the ghost planes
+    are filled on the devices after each step, the host enqueues the whole run and waits once.
+    Returns each slab's probe records (its probes, steps). ``device_buffers``: optional
+    ``(signals, outs, stride)`` already on the devices (each solver's drive and records), for
+    timing without host copies."""
+    import ctypes
+
+    import torch
+
+    from . import _abi
+
+    lib = _abi.load_library()
+    steps = len(signal)
+    if device_buffers is None:
+        signals = [torch.from_numpy(np.ascontiguousarray(signal, np.float32)).to(f"cuda:{s.device}") for s in solvers]
+        outs = [torch.zeros((max(1, s.probes), max(1, steps)), dtype=torch.float64, device=f"cuda:{s.device}")
+                for s in solvers]  # fmt: skip
+        stride = max(1, steps)
+    else:
+        signals, outs, stride = device_buffers
+    joined = links(slabs)
+    link_array = (_abi.FdtdPlaneLink * max(1, len(joined)))()
+    for k, (a, b, pa, pb) in enumerate(joined):
+        link_array[k].from_, link_array[k].to, link_array[k].from_plane, link_array[k].to_plane = a, b, pa, pb
+    handles = (ctypes.c_void_p * len(solvers))(*[s._handle for s in solvers])
+    sig_ptrs = (ctypes.c_void_p * len(solvers))(*[t.data_ptr() for t in signals])
+    out_ptrs = (ctypes.c_void_p * len(solvers))(*[t.data_ptr() for t in outs])
+    status = lib.fdtd_run_linked(handles, len(solvers), link_array, len(joined), sig_ptrs, steps, out_ptrs, stride)
+    if status != _abi.FDTD_OK:
+        message = (lib.fdtd_last_error(solvers[0]._handle) or lib.fdtd_global_error()).decode()
+        raise RuntimeError(message or f"fdtd_run_linked failed ({status})")
+    for s in solvers:
+        s.synchronize()
+    return [o[: s.probes, :steps].cpu().numpy() for o, s in zip(outs, solvers)]

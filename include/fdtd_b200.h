@@ -262,6 +262,29 @@ int fdtd_get_tiles(const fdtd_solver *solver, fdtd_tiles *out);
  */
 int fdtd_level_plane(fdtd_solver *solver, uint64_t z, int which, void **ptr, uint64_t *bytes);
 
+/* A plane of one grid of a group copied, after each step, into a plane of another (fdtd_run_linked). */
+typedef struct fdtd_plane_link {
+    uint32_t from, to;     /* indices of the solvers in the group */
+    uint64_t from_plane;   /* plane z of the source's grid (one of its own planes) */
+    uint64_t to_plane;     /* plane z of the destination's grid: solid there (a ghost plane) */
+} fdtd_plane_link;
+
+/*
+ * Steps a group of grids together, `steps` steps, each the z-slab of one larger grid (no
+ * counterpart in the reference, whose solver holds one grid on one machine): after every step,
+ * each link copies the source's plane of the new pressure into the destination's plane — a slab's
+ * first and last planes into its neighbours' ghost planes. The ordering lives on the devices: a
+ * solver's step waits for the planes its neighbours sent it, each copy runs on its source's stream
+ * after the source's step (cudaMemcpyPeerAsync between devices, with peer access enabled), and the
+ * host enqueues the whole run without waiting, so no step costs a round trip to the host. Each
+ * solver takes its drive from d_signals[h] and records its probes into d_outs[h] (device memory,
+ * as fdtd_run_device; out_stride between probes). The grids' planes must be of one size, a link's
+ * destination plane solid, the solvers distinct and of one precision. Returns when the work is
+ * enqueued; each solver's stream ends with the run (fdtd_synchronize, or fdtd_stream).
+ */
+int fdtd_run_linked(fdtd_solver *const *solvers, uint32_t count, const fdtd_plane_link *links, uint32_t link_count,
+                    const float *const *d_signals, uint64_t steps, double *const *d_outs, uint64_t out_stride);
+
 /*
  * The failure path of the kernels' bounded waits, on its own (no counterpart in the reference):
  * a kernel polls a device flag that nothing sets, at most `spins` times (1 to 2^24), then reports

@@ -168,3 +168,24 @@ def test_gpu_slabs_step_as_the_whole_grid(name):
     probes = len(np.asarray(layout["probe_start"])) - 1
     got = slabs.gather_records(parts, records, probes, len(signal))
     assert np.array_equal(got, OracleSolver(layout).run(signal))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,count", [("open_layer", 2), ("resonant19", 3), ("speed7", 2), ("fitted_open", 4)])
+def test_gpu_linked_slabs_step_as_the_whole_grid(name, count):
+    # The slabs stepped together inside the library (fdtd_run_linked): the ghost planes filled on
+    # the device after each step, no host round trip; equal to the whole grid to the bit, and a
+    # second run continues from the first.
+    from acoustic_spaces_b200 import B200WaveSolver
+
+    layout, signal, _ = load_golden(name)
+    signal = signal[:150]
+    bounds = slabs.partition_planes(layout, count)
+    parts = [slabs.slab(layout, bounds, r) for r in range(count)]
+    gpus = [B200WaveSolver(p.layout, autotune=False) for p in parts]
+    first = slabs.run_linked(gpus, parts, signal[:61])
+    second = slabs.run_linked(gpus, parts, signal[61:])
+    records = [np.concatenate([a, b], axis=1) for a, b in zip(first, second)]
+    probes = len(np.asarray(layout["probe_start"])) - 1
+    got = slabs.gather_records(parts, records, probes, len(signal))
+    assert np.array_equal(got, OracleSolver(layout).run(signal))
