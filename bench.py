@@ -631,11 +631,13 @@ def run_shoebox(args, world: int, rank: int, local: int) -> None:
 
 
 def run_slabs(args, world: int, rank: int, local: int) -> None:
-    """The polyhedral room as one grid split into slabs of z-planes across the ranks (strong
-    scaling): each rank steps its planes and, after every step, swaps its boundary planes with its
-    neighbours over NCCL (one plane per neighbour per step). The host orders every step. Reports the
-    whole grid's cell updates over the slowest rank's device time, and checks the gathered probes
-    against a one-rank run of the same grid where it fits."""
+    """The polyhedral room as one grid split into slabs of z-planes (strong scaling), one plane per
+    neighbour exchanged after every step. Across ranks (one GPU each): each rank steps its slab and
+    swaps its boundary planes with its neighbours over NCCL, everything enqueued on the solver's
+    stream (torch's NCCL streams wait for it and it for them) so the host never waits between
+    steps. In one process (``--slab-count`` S > 1 on one GPU): the S slabs stepped together inside
+    the library (fdtd_run_linked), the planes copied on the device. Reports the whole grid's cell
+    updates over the slowest rank's device time."""
     import torch
     import torch.distributed as dist
 
@@ -647,35 +649,57 @@ def run_slabs(args, world: int, rank: int, local: int) -> None:
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
     workload = build_workload(args)
     layout = workload.built.layout
-    bounds = slabs.partition_planes(layout, world)
-    part = slabs.slab(layout, bounds, rank)
-    solver = B200WaveSolver(part.layout, device=local)
-    planes = slabs.DevicePlanes(solver)
+    count = args.slab_count if (world == 1 and args.slab_count > 1) else world
+    bounds = slabs.partition_planes(layout, count)
     steps, warmup = args.steps, args.warmup
     signal = np.ascontiguousarray(np.resize(workload.signal, steps + warmup), np.float32)
     sig = torch.from_numpy(signal).to(f"cuda:{local}")
-    out = torch.zeros((max(1, len(part.probes)), steps + warmup), dtype=torch.float64, device=f"cuda:{local}")
-
-    def step(k: int) -> None:
-        solver.run_device(sig.data_ptr() + 4 * k, 1, out.data_ptr() + 8 * k, steps + warmup)
-        solver.synchronize()
-        if world > 1:
-            slabs.exchange_ghosts(planes, part, rank, world, dist)
-            torch.cuda.synchronize(local)
-
-    for k in range(warmup):
-        step(k)
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize(local)
-    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with Clocks(local) as clocks:
-        start.record()
-        for k in range(warmup, warmup + steps):
-            step(k)
-        end.record()
+    if world == 1 and count > 1:
+        parts = [slabs.slab(layout, bounds, r) for r in range(count)]
+        solvers = [B200WaveSolver(p.layout, device=local) for p in parts]
+        outs = [torch.zeros((max(1, s.probes), steps + warmup), dtype=torch.float64, device=f"cuda:{local}")
+                for s in solvers]  # fmt: skip
+        slabs.run_linked(solvers, parts, signal[:warmup], device_buffers=([sig] * count, outs, steps + warmup))
         torch.cuda.synchronize(local)
-    ms = start.elapsed_time(end)
+        stream = torch.cuda.ExternalStream(solvers[0].stream, device=f"cuda:{local}")
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with Clocks(local) as clocks:
+            start.record(stream)
+            shifted = [torch.narrow(sig, 0, warmup, steps)] * count
+            outs_k = [o[:, warmup:] for o in outs]
+            slabs.run_linked(solvers, parts, signal[warmup:], device_buffers=(shifted, outs_k, steps + warmup))
+            end.record(stream)
+            torch.cuda.synchronize(local)
+        ms = start.elapsed_time(end)
+        exchange = "one plane per neighbour per step, copied on the device inside the library (fdtd_run_linked)"
+    else:
+        part = slabs.slab(layout, bounds, rank)
+        solver = B200WaveSolver(part.layout, device=local)
+        planes = slabs.DevicePlanes(solver)
+        out = torch.zeros((max(1, len(part.probes)), steps + warmup), dtype=torch.float64, device=f"cuda:{local}")
+        stream = torch.cuda.ExternalStream(solver.stream, device=f"cuda:{local}")
+
+        def step(k: int) -> None:
+            solver.run_device(sig.data_ptr() + 4 * k, 1, out.data_ptr() + 8 * k, steps + warmup)
+            if world > 1:
+                with torch.cuda.stream(stream):
+                    slabs.exchange_ghosts(planes, part, rank, world, dist)
+
+        for k in range(warmup):
+            step(k)
+        torch.cuda.synchronize(local)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(local)
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with Clocks(local) as clocks:
+            start.record(stream)
+            for k in range(warmup, warmup + steps):
+                step(k)
+            end.record(stream)
+            torch.cuda.synchronize(local)
+        ms = start.elapsed_time(end)
+        exchange = "one plane per neighbour per step over NCCL, enqueued on the solver's stream (no host wait between steps)"
     if world > 1:
         t = torch.tensor([ms], device=f"cuda:{local}")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -697,11 +721,10 @@ def run_slabs(args, world: int, rank: int, local: int) -> None:
             "vs_baseline": None,
             "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": workload.name, **workload.description, "parallelism": f"z-slabs x{world}",
-                       "slabs": [list(b) for b in bounds],
-                       "exchange": "one plane per neighbour per step over NCCL, the host ordering each step"},  # fmt: skip
+            "config": {"workload": workload.name, **workload.description, "parallelism": f"z-slabs x{count}",
+                       "slabs": [list(b) for b in bounds], "exchange": exchange},  # fmt: skip
             "clocks": clocks.summary(),
-            "gpu_launches": 4 * steps,
+            "gpu_launches": 4 * steps * count // max(1, world),
         }
         print(json.dumps(line), flush=True)
 
@@ -837,6 +860,8 @@ def main() -> None:
     parser.add_argument("--gradient-segment", type=int, default=50)
     parser.add_argument("--no-fp64-rate", action="store_true", help="skip timing the FP64 stepper alike")
     parser.add_argument("--launch", default="", help="layer,special blocks per SM (skips the autotuner)")
+    parser.add_argument("--slab-count", type=int, default=0,
+                        help="with --slabs on one GPU: this many slabs stepped together in one process")  # fmt: skip
     parser.add_argument("--slabs", action="store_true",
                         help="one grid split into z-slabs across the ranks, boundary planes swapped each step")  # fmt: skip
     parser.add_argument("--precision", choices=["fp32", "fp32c"], default="fp32",
