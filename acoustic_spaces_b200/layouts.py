@@ -1062,11 +1062,15 @@ class Stacked:
         return sum(part[2] for part in self.parts)
 
 
-def stack(layouts: list[dict[str, np.ndarray]]) -> Stacked:
-    """One layout of many grids without matched layers: grid k's cells at its own (x, y) of a
-    plane of the largest nx x ny, its planes after grid k-1's. Each grid's outermost layer of cells
-    is never air, so no link joins two grids, and each grid is stepped exactly as on its own:
-    every row keeps its coefficients, every link its neighbour."""
+def stack(layouts: list[dict[str, np.ndarray]], across: int = 1) -> Stacked:
+    """One layout of many grids without matched layers. The grids go in groups of ``across``
+    consecutive ones: a group's grids side by side along x (each after the one before), the group
+    at y = 0 of a plane as wide as the widest group and as deep as the deepest grid, its planes
+    after the group before's (as many as its tallest grid has). Grids of one room with several
+    sources, side by side, fill the interior sweep's tiles where one alone would leave most of a
+    tile empty. Each grid's outermost layer of cells is never air, so no link joins two grids, and
+    each grid is stepped exactly as on its own: every row keeps its coefficients, every link its
+    neighbour."""
     first = layouts[0]
     for lay in layouts:
         if int(lay["stencil"][0]) != int(first["stencil"][0]) or not np.array_equal(lay["weights"], first["weights"]):
@@ -1079,14 +1083,24 @@ def stack(layouts: list[dict[str, np.ndarray]]) -> Stacked:
             raise ValueError("grids with a matched layer cannot be stacked (its tables are the grid's own)")
         if len(lay.get("flow_mask", [])):
             raise ValueError("moving air cannot be stacked")
+    if across < 1:
+        raise ValueError("at least one grid a group")
     shapes = [tuple(int(v) for v in lay["shape"]) for lay in layouts]
-    NX = max(s[0] for s in shapes)
+    groups = [list(range(g, min(g + across, len(shapes)))) for g in range(0, len(shapes), across)]
+    # Each grid's offset: x after the grids before it in its group, z after the groups before.
+    x_at, z_at, z = [0] * len(shapes), [0] * len(shapes), 0
+    for group in groups:
+        x = 0
+        for k in group:
+            x_at[k], z_at[k] = x, z
+            x += shapes[k][0]
+        z += max(shapes[k][2] for k in group)
+    NX = max(sum(shapes[k][0] for k in group) for group in groups)
     NY = max(s[1] for s in shapes)
-    NZ = sum(s[2] for s in shapes)
+    NZ = z
     scaled = int(first["scaled"][0]) == 1
     types = np.zeros((NZ, NY, NX), np.uint8)
     scale = np.ones((NZ, NY, NX), np.float32) if scaled else None
-    z0 = 0
     out = {k: [] for k in ("special", "link_direction", "link_weight", "coef_a", "coef_b", "coef_inv", "source",
                            "state_branch", "state_weight", "branch_now", "branch_before", "branch_gain",
                            "probe_cells", "probe_weights")}  # fmt: skip
@@ -1094,23 +1108,24 @@ def stack(layouts: list[dict[str, np.ndarray]]) -> Stacked:
     links = states = branches = probes = reads = 0
     parts = []
 
-    def mapped(index, shape, z_first):
+    def mapped(index, shape, x_first, z_first):
         nx, ny, _ = shape
         i = np.asarray(index, np.int64)
-        return (i % nx) + NX * ((i // nx) % ny + NY * (i // (nx * ny) + z_first))
+        return (i % nx + x_first) + NX * ((i // nx) % ny + NY * (i // (nx * ny) + z_first))
 
-    for lay, shape in zip(layouts, shapes):
+    for k, (lay, shape) in enumerate(zip(layouts, shapes)):
         nx, ny, nz = shape
+        x0, z0 = x_at[k], z_at[k]
         t = np.asarray(lay["types"]).reshape(nz, ny, nx)
-        types[z0 : z0 + nz, :ny, :nx] = t
+        types[z0 : z0 + nz, :ny, x0 : x0 + nx] = t
         if scaled:
-            scale[z0 : z0 + nz, :ny, :nx] = np.asarray(lay["scale"]).reshape(nz, ny, nx)
-        out["special"].append(mapped(lay["special"], shape, z0))
+            scale[z0 : z0 + nz, :ny, x0 : x0 + nx] = np.asarray(lay["scale"]).reshape(nz, ny, nx)
+        out["special"].append(mapped(lay["special"], shape, x0, z0))
         for name in ("link_direction", "link_weight", "coef_a", "coef_b", "coef_inv", "source", "state_weight",
                      "branch_now", "branch_before", "branch_gain", "probe_weights"):  # fmt: skip
             out[name].append(np.asarray(lay[name]))
         out["state_branch"].append(np.asarray(lay["state_branch"], np.int64) + branches)
-        out["probe_cells"].append(mapped(lay["probe_cells"], shape, z0).astype(np.uint64))
+        out["probe_cells"].append(mapped(lay["probe_cells"], shape, x0, z0).astype(np.uint64))
         link_start.append(np.asarray(lay["link_start"], np.uint64)[1:] + np.uint64(links))
         state_start.append(np.asarray(lay["state_start"], np.uint64)[1:] + np.uint64(states))
         probe_start.append(np.asarray(lay["probe_start"], np.uint64)[1:] + np.uint64(reads))
@@ -1121,7 +1136,6 @@ def stack(layouts: list[dict[str, np.ndarray]]) -> Stacked:
         branches += len(lay["branch_now"])
         probes += p
         reads += len(lay["probe_cells"])
-        z0 += nz
     layout = {
         "shape": np.array([NX, NY, NZ], np.uint64),
         "stencil": np.asarray(first["stencil"]).copy(),
@@ -1213,7 +1227,7 @@ def batched_rooms(
             layouts.append(built.layout)
             cells.append(built.air_cells)
             scenes.append((room, grid, src[j], rec))
-    stacked = stack(layouts)
+    stacked = stack(layouts, across=sources)  # a room's solves side by side
     description = {
         "rooms": rooms,
         "rooms_here": len(mine),

@@ -177,13 +177,15 @@ def test_a_stack_steps_each_grid_as_it_steps_alone():
         assert air == np.count_nonzero(lay["types"])
 
 
-def test_golden_grids_stack_with_their_own_runs():
+@pytest.mark.parametrize("across", [1, 2, 3])
+def test_golden_grids_stack_with_their_own_runs(across):
+    # (across > 1: grids of different shapes side by side along x in one group of planes)
     from conftest import golden_names, load_golden
 
     names = [n for n in golden_names() if len(load_golden(n)[0]["layer_cells"]) == 0 and load_golden(n)[0]["scaled"][0] == 0]
     layouts = [load_golden(n)[0] for n in names]
     sevens = [lay for lay in layouts if int(lay["stencil"][0]) == 7]
-    stacked = L.stack(sevens)
+    stacked = L.stack(sevens, across=across)
     signal = np.random.default_rng(2).standard_normal(150).astype(np.float32)
     together = OracleSolver(stacked.layout).run(signal)
     for lay, (p0, p1, _, _) in zip(sevens, stacked.parts):
