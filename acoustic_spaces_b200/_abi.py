@@ -81,6 +81,11 @@ class FdtdLayout(ctypes.Structure):
         ("probe_cells", _u64p),
         ("probe_weights", _f64p),
         ("flow_count", ctypes.c_uint64),
+        ("flow_x", _f32p),
+        ("flow_y", _f32p),
+        ("flow_mask", _u8p),
+        ("wind", _f32p * 3),
+        ("loop", _f32p * 3),
     ]
 
 
@@ -114,6 +119,7 @@ class FdtdTiles(ctypes.Structure):
         ("planes", ctypes.c_uint64),
         ("tiles", ctypes.c_uint32),
         ("blocks_per_sm", ctypes.c_int32),
+        ("concurrent", ctypes.c_int32),
     ]
 
 
@@ -187,6 +193,10 @@ ARRAYS = {
     "probe_cells": np.uint64,
     "probe_weights": np.float64,
     **{name: np.float32 for name in KEEP + PUSH},
+    "flow_x": np.float32,
+    "flow_y": np.float32,
+    "flow_mask": np.uint8,
+    **{f"{kind}_{axis}": np.float32 for kind in ("wind", "loop") for axis in "xyz"},
 }
 
 
@@ -216,7 +226,6 @@ def pack_layout(layout: Mapping[str, np.ndarray]) -> tuple[FdtdLayout, dict[str,
         raise ValueError("link_start and state_start have one entry more than special")
     if len(keep["probe_start"]) == 0:
         keep["probe_start"] = np.zeros(1, np.uint64)
-    flow = layout.get("flow_mask")
     s = FdtdLayout()
     s.nx, s.ny, s.nz = shape
     s.stencil = int(np.asarray(layout["stencil"]).reshape(-1)[0])
@@ -257,7 +266,13 @@ def pack_layout(layout: Mapping[str, np.ndarray]) -> tuple[FdtdLayout, dict[str,
     s.probe_start = _ptr(keep["probe_start"], _u64p)
     s.probe_cells = _ptr(keep["probe_cells"], _u64p)
     s.probe_weights = _ptr(keep["probe_weights"], _f64p)
-    s.flow_count = 0 if flow is None else len(flow)
+    s.flow_count = len(keep["flow_mask"])
+    s.flow_x = _ptr(keep["flow_x"], _f32p)
+    s.flow_y = _ptr(keep["flow_y"], _f32p)
+    s.flow_mask = _ptr(keep["flow_mask"], _u8p)
+    for a, axis in enumerate("xyz"):
+        s.wind[a] = _ptr(keep[f"wind_{axis}"], _f32p)
+        s.loop[a] = _ptr(keep[f"loop_{axis}"], _f32p)
     return s, keep
 
 
@@ -290,6 +305,7 @@ SIGNATURES = {
         [ctypes.c_void_p, _f32p, ctypes.c_uint64, _f64p, ctypes.c_uint64, _f64p, _f64p, _f64p, _f64p, _f64p],
     ),
     "fdtd_layer_gradient": (ctypes.c_int, [ctypes.c_void_p, _f64p]),
+    "fdtd_set_gradient_tables": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "fdtd_set_tape_budget": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
     "fdtd_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_int),
                                      ctypes.POINTER(ctypes.c_int)]),
@@ -301,6 +317,7 @@ SIGNATURES = {
     ),
     "fdtd_set_tiles": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_uint64]),
     "fdtd_get_tiles": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(FdtdTiles)]),
+    "fdtd_set_streams": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "fdtd_level_plane": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int,
                                         ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_uint64)]),
     "fdtd_test_wait": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32]),
@@ -339,7 +356,7 @@ def load_library(path: str | os.PathLike | None = None) -> ctypes.CDLL:
         fn = getattr(lib, name)
         fn.restype = restype
         fn.argtypes = argtypes
-    if lib.fdtd_abi_version() != 1:
+    if lib.fdtd_abi_version() != 2:
         raise RuntimeError("the B200 wave stepper's library has another ABI version")
     if path is None:
         from acoustic_spaces_b200 import build

@@ -255,6 +255,36 @@ __global__ void __launch_bounds__(kBlock) layer_hat_kernel(const AdjointTables t
     }
 }
 
+// The tables' gradient per coordinate, in a fixed order: block b sums the six products of the
+// layer cells whose coordinate along its axis is its own (cells by_coord[start[b]] ..
+// by_coord[start[b + 1]] - 1, the cells sorted by that coordinate), each thread a strided share in
+// order, then the shares in a fixed tree; out[6 b + f] takes sum f. Blocks 0 .. of axis 0's
+// coordinates first, then axis 1's, then axis 2's (axis_block[a] the first block of axis a).
+__global__ void __launch_bounds__(kBlock) layer_table_sums_kernel(const double *g, uint32_t layers,
+                                                                  const uint32_t *by_coord, const uint32_t *start,
+                                                                  uint32_t axis1_block, uint32_t axis2_block,
+                                                                  double *out) {
+    __shared__ double part[6][kBlock];
+    const uint32_t b = blockIdx.x;
+    const int a = b >= axis2_block ? 2 : (b >= axis1_block ? 1 : 0);
+    double sum[6] = {0, 0, 0, 0, 0, 0};
+    for (uint32_t e = start[b] + threadIdx.x; e < start[b + 1]; e += kBlock) {
+        const uint32_t c = by_coord[e];
+#pragma unroll
+        for (int f = 0; f < 6; ++f) sum[f] += g[(uint64_t)(6 * a + f) * layers + c];
+    }
+#pragma unroll
+    for (int f = 0; f < 6; ++f) part[f][threadIdx.x] = sum[f];
+    __syncthreads();
+    for (int half = kBlock / 2; half > 0; half /= 2) {
+        if ((int)threadIdx.x < half)
+#pragma unroll
+            for (int f = 0; f < 6; ++f) part[f][threadIdx.x] += part[f][threadIdx.x + half];
+        __syncthreads();
+    }
+    if (threadIdx.x < 6) out[6 * (uint64_t)b + threadIdx.x] = part[threadIdx.x][0];
+}
+
 // The layer's terms on the adjoint of cell j, from the hats of its layer neighbours and its own
 // (mask as AdjointTables' layer masks).
 template <typename T>

@@ -69,6 +69,9 @@ struct AdjointState {
     CUtensorMap lam_b[2], lam_a[2];
     void *carried = nullptr;  // the matched layer's carried values (9 per cell)
     void *hat = nullptr;      // the matched layer's terms' factors (6 pitched levels)
+    // The layer cells sorted by their coordinate along each axis in turn (x, then y, then z; each
+    // a permutation of the cells) and each coordinate's first entry: the tables' sums by coordinate.
+    const uint32_t *by_coord = nullptr, *coord_start = nullptr;
 };
 
 }  // namespace
@@ -91,6 +94,10 @@ struct fdtd_solver {
     // Blocks an SM of the matched-layer and special-row kernels (0: one thread a cell), chosen by
     // fdtd_autotune.
     int layer_per_sm = kLayerPerSm, special_per_sm = kSpecialPerSm;
+    // Whether a step's kernels run beside one another on the three streams (1) or one after
+    // another on the handle's stream (0): where the special rows are many, running them beside
+    // the sweep can cost the sweep more than it saves (fdtd_autotune times both).
+    int concurrent = 1;
     uint32_t bulk_tiles = 0;
     int bulk_per_sm = 0;      // resident bulk blocks per multiprocessor (shape 0)
     int shape_per_sm[kShapes] = {0, 0, 0, 0};  // the same, each shape
@@ -148,6 +155,7 @@ struct fdtd_solver {
     std::vector<int32_t> state_branch;  // each branch state's branch
     // The last gradient's part in the matched layer's tables (fdtd_layer_gradient), empty without.
     std::vector<double> layer_gradient;
+    bool gradient_tables = true;  // whether gradients also give the layer tables' (fdtd_set_gradient_tables)
     uint64_t branches = 0;
     // fdtd_gradient's device workspace, kept and handed out again in the same order while the
     // sizes asked for stay the same (a fit's iterations then allocate nothing).
@@ -555,7 +563,7 @@ int launch_steps(fdtd_solver *s, const float *d_signal, uint64_t steps, double *
     // side stream. The three write disjoint memory; each step starts when all three have ended the
     // step before. While timing, all run one after another on the handle's stream, so that each
     // kernel's events bracket that kernel alone.
-    const bool fork = !s->timing;
+    const bool fork = !s->timing && s->concurrent;
     cudaStream_t side = fork ? s->side : s->stream, layer = fork ? s->layer_stream : s->stream;
     for (uint64_t k = 0; k < steps; ++k) {
         const bool flip = (k & 1) != 0;
@@ -1008,6 +1016,7 @@ struct AdjointLists {
     std::vector<uint32_t> layer_from_start, layer_from_row, layer_read_start;
     std::vector<double> layer_from_coef, layer_from_base;
     std::vector<uint8_t> layer_interior, special_layer_mask, corrected_layer_mask, layer_mask;
+    std::vector<uint32_t> by_coord, coord_start;  // the layer cells by coordinate, per axis
 };
 
 // The lists from the handle's own device tables.
@@ -1190,6 +1199,28 @@ int adjoint_lists(fdtd_solver *s, AdjointLists &out) {
         out.layer_interior.push_back(inner);
         out.layer_mask.push_back(layer_mask(i));
     }
+    // Per axis, the layer cells sorted by their coordinate along it (counting sort, stable), and
+    // where each coordinate's cells begin: coordinates 0 .. n_a - 1 of axis a follow axis a - 1's.
+    if (Lc) {
+        const uint64_t len[3] = {s->nx, s->ny, s->nz};
+        out.coord_start.assign(1, 0);
+        for (int a = 0; a < 3; ++a) {
+            std::vector<uint32_t> count(len[a] + 1, 0);
+            std::vector<uint32_t> coord(Lc);
+            for (uint64_t c = 0; c < Lc; ++c) {
+                const uint64_t i = s->layer_cells[c], z = i / (s->pitch * s->ny), r = i - z * s->pitch * s->ny;
+                const uint64_t y = r / s->pitch, at[3] = {r - y * s->pitch, y, z};
+                coord[c] = (uint32_t)at[a];
+                ++count[at[a] + 1];
+            }
+            for (uint64_t x = 0; x < len[a]; ++x) count[x + 1] += count[x];
+            const size_t base = out.by_coord.size();
+            out.by_coord.resize(base + Lc);
+            std::vector<uint32_t> next(count.begin(), count.end() - 1);
+            for (uint64_t c = 0; c < Lc; ++c) out.by_coord[base + next[coord[c]]++] = (uint32_t)c;
+            for (uint64_t x = 0; x < len[a]; ++x) out.coord_start.push_back((uint32_t)(base + count[x + 1]));
+        }
+    }
     return FDTD_OK;
 }
 
@@ -1261,6 +1292,8 @@ int place_adjoint(fdtd_solver *s, const AdjointLists &l, Pool &pool, AdjointStat
     if (s->layers) {
         if ((rc = pool.take(e * 9 * s->layers, &a.carried, true))) return rc;
         if ((rc = pool.take(e * 6 * s->n_device, &a.hat, true))) return rc;
+        if ((rc = place(s, pool, l.by_coord, &a.by_coord))) return rc;
+        if ((rc = place(s, pool, l.coord_start, &a.coord_start))) return rc;
     }
     for (int k = 0; k < 2; ++k) {
         if ((rc = pool.take(e * s->n_device, &a.lam[k], true))) return rc;
@@ -1445,13 +1478,17 @@ int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float
     const uint64_t level_bytes = e * s->n_device, state_bytes = e * S;
     // The matched layer: its factors of each step of a segment, and its gradient's sums per cell.
     const uint64_t Lc = s->layers;
+    const bool tables = Lc && s->gradient_tables;
     T *traj_layer = nullptr;
-    double *g_layer = nullptr;
-    if (Lc) {
+    double *g_layer = nullptr, *table_sums = nullptr;
+    const uint64_t coords = s->nx + s->ny + s->nz;
+    if (tables) {
         if ((rc = scratch.take(e * kLayerFactors * Lc * segment, &p))) return rc;
         traj_layer = static_cast<T *>(p);
         if ((rc = scratch.take(sizeof(double) * kLayerFactors * Lc, &p))) return rc;
         g_layer = static_cast<double *>(p);
+        if ((rc = scratch.take(sizeof(double) * 6 * coords, &p))) return rc;
+        table_sums = static_cast<double *>(p);
     }
     // The forward pass from rest, keeping checkpoints[m] = the state at the start of segment m+1;
     // or, when the handle holds the tape of a run of this drive with these segments, its states.
@@ -1487,7 +1524,7 @@ int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float
     // reverse steps.
     auto recompute = [&](uint64_t count) -> int {
         s->record_u = traj_u, s->record_w = traj_w, s->record_offset = 2, s->record_probes = false;
-        s->record_layer = traj_layer;
+        s->record_layer = tables ? traj_layer : nullptr;
         const int r = dispatch(s, seg_signal, count, d_out, segment);
         s->record_u = s->record_w = s->record_layer = nullptr, s->record_probes = true;
         return r;
@@ -1509,7 +1546,8 @@ int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float
             // The matched layer's hats of step m first (the gathers below read them).
             if (layer_blocks)
                 layer_hat_kernel<T><<<layer_blocks, kBlock, 0, s->side>>>(
-                    t, lam_next, static_cast<T *>(adj.carried), hat, traj_layer + m * kLayerFactors * Lc, g_layer);
+                    t, lam_next, static_cast<T *>(adj.carried), hat,
+                    tables ? traj_layer + m * kLayerFactors * Lc : nullptr, g_layer);
             if (special_blocks + corrected_blocks + layer_blocks)
                 rows_adjoint_kernel<T><<<special_blocks + corrected_blocks + layer_blocks, kBlock, 0, s->side>>>(
                     t, special_blocks, corrected_blocks, lam_next, om_next, tilde, hat, lam_out, om_out, traj_u, traj_w,
@@ -1611,29 +1649,33 @@ int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float
     if ((rc = check_device_error(s)) != FDTD_OK) return rc;
     for (int k = 0; k < 5; ++k)
         if (grads[k] && g_len[k]) CUDA_TRY(s, cudaMemcpy(grads[k], g[k], sizeof(double) * g_len[k], cudaMemcpyDeviceToHost));
-    if (Lc) {
-        // The layer tables' gradient: each cell's sums added into its coordinates' entries.
-        std::vector<double> cell(kLayerFactors * Lc);
-        CUDA_TRY(s, cudaMemcpy(cell.data(), g_layer, sizeof(double) * cell.size(), cudaMemcpyDeviceToHost));
+    if (tables) {
+        // The layer tables' gradient: the cells' sums by coordinate on the device, in a fixed
+        // order, then each coordinate's six sums into its tables' entries (a product of the cells
+        // at coordinate x goes to the face entries x + 1 or x).
+        layer_table_sums_kernel<<<(uint32_t)coords, kBlock, 0, s->stream>>>(
+            g_layer, (uint32_t)Lc, adj.by_coord, adj.coord_start, (uint32_t)s->nx, (uint32_t)(s->nx + s->ny), table_sums);
+        CUDA_TRY(s, cudaGetLastError());
+        std::vector<double> sums(6 * coords);
+        CUDA_TRY(s, cudaMemcpyAsync(sums.data(), table_sums, sizeof(double) * sums.size(), cudaMemcpyDeviceToHost, s->stream));
+        CUDA_TRY(s, cudaStreamSynchronize(s->stream));
         const uint64_t len[3] = {s->nx + 1, s->ny + 1, s->nz + 1};
         uint64_t keep_at[6], push_at[6], at = 0;  // offsets of keep/keep_face (x, y, z), then push/push_face
         for (int a = 0; a < 3; ++a) keep_at[2 * a] = at, at += len[a], keep_at[2 * a + 1] = at, at += len[a];
         for (int a = 0; a < 3; ++a) push_at[2 * a] = at, at += len[a], push_at[2 * a + 1] = at, at += len[a];
         s->layer_gradient.assign(at, 0.0);
         double *out = s->layer_gradient.data();
-        for (uint64_t c = 0; c < Lc; ++c) {
-            const uint64_t i = s->layer_cells[c], z = i / (s->pitch * s->ny), r = i - z * s->pitch * s->ny;
-            const uint64_t y = r / s->pitch, coord[3] = {r - y * s->pitch, y, z};
-            for (int a = 0; a < 3; ++a) {
-                const double *f = cell.data() + (uint64_t)(6 * a) * Lc + c;
-                out[keep_at[2 * a] + coord[a]] += f[0];
-                out[push_at[2 * a] + coord[a]] += f[1 * Lc];
-                out[keep_at[2 * a + 1] + coord[a] + 1] += f[2 * Lc];
-                out[push_at[2 * a + 1] + coord[a] + 1] += f[3 * Lc];
-                out[keep_at[2 * a + 1] + coord[a]] += f[4 * Lc];
-                out[push_at[2 * a + 1] + coord[a]] += f[5 * Lc];
+        uint64_t block = 0;
+        for (int a = 0; a < 3; ++a)
+            for (uint64_t x = 0; x + 1 < len[a]; ++x, ++block) {
+                const double *f = sums.data() + 6 * block;
+                out[keep_at[2 * a] + x] += f[0];
+                out[push_at[2 * a] + x] += f[1];
+                out[keep_at[2 * a + 1] + x + 1] += f[2];
+                out[push_at[2 * a + 1] + x + 1] += f[3];
+                out[keep_at[2 * a + 1] + x] += f[4];
+                out[push_at[2 * a + 1] + x] += f[5];
             }
-        }
     } else {
         s->layer_gradient.clear();
     }
@@ -1706,7 +1748,10 @@ size_t pool_bytes(const fdtd_solver *s, const AdjointLists &l, uint64_t steps, u
              pool_round(e * S * (segment + 2)) + pool_round(8 * P * segment) + pool_round(4 * segment) +
              pool_round(8 * P * segment);
     total += 2 * pool_round(8 * K) + 3 * pool_round(8 * S);
-    if (Lc) total += pool_round(e * kLayerFactors * Lc * segment) + pool_round(8 * kLayerFactors * Lc);
+    if (Lc) total += pool_round(4 * l.by_coord.size()) + pool_round(4 * l.coord_start.size());
+    if (Lc && s->gradient_tables)
+        total += pool_round(e * kLayerFactors * Lc * segment) + pool_round(8 * kLayerFactors * Lc) +
+                 pool_round(8 * 6 * (s->nx + s->ny + s->nz));
     if (!taped) total += (segments - 1) * pool_round(checkpoint_bytes(s));
     return total;
 }
@@ -2231,6 +2276,21 @@ int fdtd_get_tiles(const fdtd_solver *s, fdtd_tiles *out) {
     out->planes = s->bulk_chunk;
     out->tiles = s->bulk_tiles;
     out->blocks_per_sm = s->shape_per_sm[s->bulk_shape];
+    out->concurrent = s->concurrent;
+    return FDTD_OK;
+}
+
+int fdtd_set_streams(fdtd_solver *s, int concurrent) {
+    if (!s) return set_global(FDTD_EINVAL, "no solver");
+    DeviceGuard guard(s->device);
+    for (cudaStream_t stream : {s->stream, s->side, s->layer_stream}) CUDA_TRY(s, cudaStreamSynchronize(stream));
+    s->concurrent = concurrent ? 1 : 0;
+    // The captured chunks and the gradient's graphs hold the old streams' order.
+    Kept{s}.drop_graphs();
+    for (cudaGraphExec_t &g : s->graph)
+        if (g) cudaGraphExecDestroy(g), g = nullptr;
+    for (cudaGraphExec_t &g : s->tape_graph)
+        if (g) cudaGraphExecDestroy(g), g = nullptr;
     return FDTD_OK;
 }
 
@@ -2279,7 +2339,7 @@ int fdtd_autotune(fdtd_solver *s, uint64_t trial_steps, int *layer_per_sm, int *
         uint64_t best_chunk = s->bulk_chunk;
         for (int shape = 0; shape < kShapes && rc == FDTD_OK; ++shape) {
             if (s->shape_per_sm[shape] < 1) continue;  // does not fit an SM in this precision
-            for (uint64_t chunk : {base / 2, base, base * 2}) {
+            for (uint64_t chunk : {base / 4, base / 2, base, base * 2}) {
                 if (chunk < 8 || chunk > 64) continue;
                 if ((rc = use_shape(s, shape, chunk)) != FDTD_OK) break;
                 float ms;
@@ -2291,19 +2351,23 @@ int fdtd_autotune(fdtd_solver *s, uint64_t trial_steps, int *layer_per_sm, int *
     }
     const int layers[] = {4, 8, 12, 16, 0}, specials[] = {2, 4, 8, 0};
     float best = -1.0f;
-    int best_layer = s->layer_per_sm, best_special = s->special_per_sm;
-    for (int l : layers) {
-        if (rc != FDTD_OK) break;
-        if (!s->layers && l != layers[0]) continue;
-        for (int k : specials) {
-            if (!s->specials && k != specials[0]) continue;
-            s->layer_per_sm = l, s->special_per_sm = k;
-            float ms;
-            if ((rc = trial(ms)) != FDTD_OK) break;
-            if (best < 0.0f || ms < best) best = ms, best_layer = l, best_special = k;
+    int best_layer = s->layer_per_sm, best_special = s->special_per_sm, best_concurrent = s->concurrent;
+    for (int c : {1, 0}) {
+        s->concurrent = c;
+        for (int l : layers) {
+            if (rc != FDTD_OK) break;
+            if (!s->layers && l != layers[0]) continue;
+            for (int k : specials) {
+                if (!s->specials && k != specials[0]) continue;
+                s->layer_per_sm = l, s->special_per_sm = k;
+                float ms;
+                if ((rc = trial(ms)) != FDTD_OK) break;
+                if (best < 0.0f || ms < best) best = ms, best_layer = l, best_special = k, best_concurrent = c;
+            }
+            if (rc != FDTD_OK) break;
         }
-        if (rc != FDTD_OK) break;
     }
+    s->concurrent = best_concurrent;
     s->timing = timing;
     cudaEventDestroy(start);
     cudaEventDestroy(end);
@@ -2377,6 +2441,13 @@ int fdtd_gradient(fdtd_solver *s, const float *signal, uint64_t steps, const dou
     return s->precision == FDTD_FP64
                ? gradient<double>(s, s->adjoint, kept, signal, steps, dloss_dy, segment, grads, true)
                : gradient<float>(s, s->adjoint, kept, signal, steps, dloss_dy, segment, grads, true);
+}
+
+int fdtd_set_gradient_tables(fdtd_solver *s, int enable) {
+    if (!s) return set_global(FDTD_EINVAL, "no solver");
+    s->gradient_tables = enable != 0;
+    s->layer_gradient.clear();
+    return FDTD_OK;
 }
 
 int fdtd_layer_gradient(const fdtd_solver *s, double *tables) {

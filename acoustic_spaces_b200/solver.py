@@ -171,14 +171,17 @@ class B200WaveSolver:
         """The address of the solver's CUDA stream (for events and ordering)."""
         return int(self._lib.fdtd_stream(self._handle) or 0)
 
-    def gradient(self, signal: np.ndarray, dloss_dy: np.ndarray, segment: int = 250) -> dict[str, np.ndarray]:
+    def gradient(self, signal: np.ndarray, dloss_dy: np.ndarray, segment: int = 250,
+                 layer_tables: bool = True) -> dict[str, np.ndarray]:  # fmt: skip
         """The gradient of a loss L of the probes' series with respect to the layout's
         coefficients, by the reverse-time stepper: the run from rest on ``signal`` gives the
         series y (probes, steps); ``dloss_dy`` is dL/dy. Returns dL/d ``coef_b``, ``coef_inv``
         (one per special row) and dL/d ``now``, ``before``, ``gain`` (one per branch state); on a
         grid with a matched layer also dL/d of its twelve tables (``keep_x``, ``keep_face_x``, ...,
-        ``push_face_z``, the layout's names, fdtd.hpp:2219-2238). The forward pass is recomputed in
-        segments of ``segment`` steps from checkpoints. The solver is left at rest."""
+        ``push_face_z``, the layout's names, fdtd.hpp:2219-2238), unless ``layer_tables`` is False
+        (then the walls' gradient alone, without recording the layer's factors). The forward pass
+        is recomputed in segments of ``segment`` steps from checkpoints. The solver is left at
+        rest."""
         signal = np.ascontiguousarray(signal, np.float32).reshape(-1)
         steps = len(signal)
         dloss = np.ascontiguousarray(dloss_dy, np.float64).reshape(self._probes, steps)
@@ -191,6 +194,8 @@ class B200WaveSolver:
             "gain": np.zeros(int(info.branch_states)),
         }
         f64 = ctypes.POINTER(ctypes.c_double)
+        if int(info.layer_cells):
+            self._lib.fdtd_set_gradient_tables(self._handle, int(bool(layer_tables)))
         status = self._lib.fdtd_gradient(
             self._handle,
             signal.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
@@ -201,7 +206,7 @@ class B200WaveSolver:
         )
         if status != _abi.FDTD_OK:
             _raise(self._lib, status, self._handle)
-        if int(info.layer_cells):
+        if int(info.layer_cells) and layer_tables:
             out.update(self.layer_gradient())
         return out
 
@@ -274,7 +279,16 @@ class B200WaveSolver:
         if status != _abi.FDTD_OK:
             _raise(self._lib, status, self._handle)
         return {"tile_shape": t.shape, "tile_x": t.tile_x, "tile_y": t.tile_y, "tile_stages": t.stages,
-                "tile_planes": int(t.planes), "tiles": int(t.tiles), "tile_blocks_per_sm": t.blocks_per_sm}  # fmt: skip
+                "tile_planes": int(t.planes), "tiles": int(t.tiles), "tile_blocks_per_sm": t.blocks_per_sm,
+                "concurrent": t.concurrent}  # fmt: skip
+
+    def set_streams(self, concurrent: bool) -> None:
+        """A step's kernels beside one another on three streams (True) or in turn on one (False), as
+        :meth:`autotune` may choose; results are the same to the bit."""
+        status = self._lib.fdtd_set_streams(self._handle, int(bool(concurrent)))
+        if status != _abi.FDTD_OK:
+            _raise(self._lib, status, self._handle)
+        self.launch = {**(getattr(self, "launch", None) or {}), **self.tiles()}
 
     def set_tiles(self, shape: int, planes: int) -> None:
         """Sets the interior sweep's tile shape (0: 64 x 16, 1: 128 x 16, 2: 64 x 32, 3: 32 x 32)
@@ -282,7 +296,7 @@ class B200WaveSolver:
         status = self._lib.fdtd_set_tiles(self._handle, int(shape), int(planes))
         if status != _abi.FDTD_OK:
             _raise(self._lib, status, self._handle)
-        self.launch = {**getattr(self, "launch", {}), **self.tiles()}
+        self.launch = {**(getattr(self, "launch", None) or {}), **self.tiles()}
 
     def level_plane(self, z: int, previous: bool = False) -> tuple[int, int]:
         """The device address and byte size of plane ``z`` of the current (or previous) pressure

@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define FDTD_B200_ABI_VERSION 1
+#define FDTD_B200_ABI_VERSION 2
 
 /* Status codes. */
 #define FDTD_OK 0
@@ -61,10 +61,12 @@ extern "C" {
 
 /*
  * The grid's layout, named after WaveSolver::layout()'s arrays (fdtd.hpp:727-782). Counts are
- * given explicitly; the arrays are borrowed only during fdtd_create(). Moving-air arrays
- * (flow_x, flow_y, flow_mask, wind_*, loop_*) have no place here: the reference steps moving
- * air on the CPU only (engine/wave.py:1158-1160), and so does this library — a layout with
- * flow_count > 0 is refused.
+ * given explicitly; the arrays are borrowed only during fdtd_create(). Moving air
+ * (fdtd.hpp:1672-2119), which the reference steps on its CPU only (engine/wave.py:1158-1160):
+ * with flow_count = nx*ny*nz, each step first carries both pressure levels along with the air
+ * (three-stage strong-stability-preserving Runge-Kutta), either the plain way (flow_x, flow_y and
+ * the neighbour bits of flow_mask) or, where wind[0] is not NULL, round the solids (wind and
+ * loop per axis, flow_mask 1 for a moving cell and 2 at the border of the moving air).
  */
 typedef struct fdtd_layout {
     uint64_t nx, ny, nz;          /* "shape": x fastest, sy = nx, sz = nx * ny */
@@ -105,7 +107,11 @@ typedef struct fdtd_layout {
     const uint64_t *probe_start;  /* "probe_start": probe_count + 1 */
     const uint64_t *probe_cells;  /* "probe_cells" */
     const double *probe_weights;  /* "probe_weights" */
-    uint64_t flow_count;          /* length of "flow_mask": must be 0 */
+    uint64_t flow_count;          /* length of "flow_mask": 0 (still air) or nx*ny*nz */
+    const float *flow_x, *flow_y; /* "flow_x", "flow_y": the plain form's shifts (cells a step) */
+    const uint8_t *flow_mask;     /* "flow_mask" */
+    const float *wind[3];         /* "wind_x", "wind_y", "wind_z": the round form's face winds, or NULL */
+    const float *loop[3];         /* "loop_x", "loop_y", "loop_z" */
 } fdtd_layout;
 
 typedef struct fdtd_solver fdtd_solver;
@@ -194,9 +200,19 @@ int fdtd_gradient(fdtd_solver *solver, const float *signal, uint64_t steps, cons
  * push_face_x, ..., push_face_z, the order of fdtd_layout.keep and .push, each of nx + 1, nx + 1,
  * ny + 1, ny + 1, nz + 1, nz + 1 values (4 (nx + ny + nz + 3) in all). The gradient in the layer's
  * damping follows by the chain rule through the tables (their derivative in the damping).
- * FDTD_EINVAL on a grid without a layer or before a gradient.
+ * FDTD_EINVAL on a grid without a layer, before a gradient, or after gradients without the tables
+ * (fdtd_set_gradient_tables).
  */
 int fdtd_layer_gradient(const fdtd_solver *solver, double *tables);
+
+/*
+ * Whether the handle's gradients also give the matched layer's tables' gradient (1, the default)
+ * or the rows' and branch states' only (0; no counterpart in the reference). Without the tables a
+ * gradient records none of the layer's per-step factors (18 values a layer cell a step of the
+ * segment) and steps back through the layer on its carried values alone: the walls' gradient is
+ * the same, to the bit, at the cost of the layer's adjoint only.
+ */
+int fdtd_set_gradient_tables(fdtd_solver *solver, int enable);
 
 /*
  * The tape of a run for a gradient that follows (no counterpart in the reference). With `segment`
@@ -224,9 +240,9 @@ int fdtd_set_tape_budget(fdtd_solver *solver, uint64_t bytes);
  * Chooses the launch shapes for this grid (no counterpart in the reference): from rest, steps
  * `trial_steps` steps (0: 8) with each candidate and keeps the fastest by CUDA events — first the
  * interior sweep's tile shape (each of the four shapes of fdtd_tiles that fits a multiprocessor,
- * each with 1/2, 1 and 2 times the default planes a tile, within 8 to 64), then, with the best
- * tiles, the count of blocks per multiprocessor of the matched-layer and special-row kernels — and
- * resets the state. The chosen counts are written to *layer_per_sm and *special_per_sm when given
+ * each with 1/4, 1/2, 1 and 2 times the default planes a tile, within 8 to 64), then, with the best
+ * tiles, the count of blocks per multiprocessor of the matched-layer and special-row kernels, the
+ * step's kernels beside one another and in turn (fdtd_set_streams) — and resets the state. The chosen counts are written to *layer_per_sm and *special_per_sm when given
  * (0: one thread a cell); fdtd_get_tiles gives the chosen tiles. Results do not depend on any of
  * these choices. Refused after steps (fdtd_reset first).
  */
@@ -240,6 +256,7 @@ typedef struct fdtd_tiles {
     uint64_t planes;    /* planes of a tile, at most (a tile marches them along z) */
     uint32_t tiles;     /* tiles, one block each */
     int blocks_per_sm;  /* resident blocks of the sweep a multiprocessor */
+    int concurrent;     /* 1: a step's kernels beside one another on three streams; 0: in turn */
 } fdtd_tiles;
 
 /*
@@ -252,6 +269,14 @@ int fdtd_set_tiles(fdtd_solver *solver, int shape, uint64_t planes);
 
 /* The interior sweep's present tiles. */
 int fdtd_get_tiles(const fdtd_solver *solver, fdtd_tiles *out);
+
+/*
+ * Whether a step's kernels run beside one another — the interior sweep on the handle's stream,
+ * the matched layer and the special rows on streams of their own (concurrent 1, the default) — or
+ * one after another on the handle's stream (0), as fdtd_autotune may choose (no counterpart in
+ * the reference). Results are the same to the bit. Waits for the handle's work.
+ */
+int fdtd_set_streams(fdtd_solver *solver, int concurrent);
 
 /*
  * The device address and size of plane z of the current (which 0) or previous (1) pressure level

@@ -114,6 +114,12 @@ struct oracle_solver {
        the residuals of the constant mode (compensated_residuals) */
     float *increment;
     float residual, *row_residual;
+    /* moving air (fdtd.hpp:1672-2119): the plain form's shifts and neighbour bits, or the round
+       form's face winds and loops (round); the carry's two stage fields (T, zero where solid) */
+    int flowing, round;
+    float *flow_x, *flow_y, *wind[3], *loop[3];
+    uint8_t *flow_mask;
+    void *t1, *t2;
 };
 
 static void *copy_of(const void *src, size_t bytes) {
@@ -127,7 +133,8 @@ int oracle_create(const fdtd_layout *L, int precision, oracle_solver **out) {
     if (precision != ORACLE_FP32 && precision != ORACLE_FP64 && precision != ORACLE_FP32C)
         return fail("precision is FP32, FP64 or FP32 compensated");
     if (L->stencil != 7 && L->stencil != 19) return fail("the stencil has 7 or 19 points");
-    if (L->flow_count) return fail("moving air is stepped on the CPU only");
+    if (L->flow_count && L->flow_count != L->nx * L->ny * L->nz) return fail("moving air needs one mask per cell");
+    if (L->flow_count && precision == ORACLE_FP32C) return fail("the compensated form steps still air only");
     oracle_solver *s = calloc(1, sizeof *s);
     if (!s) return FDTD_ENOMEM;
     s->precision = precision;
@@ -183,6 +190,22 @@ int oracle_create(const fdtd_layout *L, int precision, oracle_solver **out) {
         s->row_residual = malloc(4 * s->specials + 4);
         fdtd_compensated_residuals(L, &s->residual, s->row_residual);
     }
+    if (L->flow_count) {
+        s->flowing = 1;
+        s->round = L->wind[0] != NULL;
+        s->flow_mask = copy_of(L->flow_mask, s->n);
+        if (s->round) {
+            for (int d = 0; d < 3; ++d) {
+                s->wind[d] = copy_of(L->wind[d], 4 * s->n);
+                s->loop[d] = copy_of(L->loop[d], 4 * s->n);
+            }
+        } else {
+            s->flow_x = copy_of(L->flow_x, 4 * s->n);
+            s->flow_y = copy_of(L->flow_y, 4 * s->n);
+        }
+        s->t1 = calloc(s->n + 1, e);
+        s->t2 = calloc(s->n + 1, e);
+    }
     s->u0 = calloc(s->n + 1, e);
     s->u1 = calloc(s->n + 1, e);
     s->w0 = calloc(s->states + 1, e);
@@ -195,10 +218,108 @@ int oracle_create(const fdtd_layout *L, int precision, oracle_solver **out) {
 }
 
 /*
+ * Moving air (fdtd.hpp:1946-2119): -v . grad q of cell i over a step, and the three stages of the
+ * strong-stability-preserving Runge-Kutta method. T float rounds as the reference's float code
+ * (its constants 1/12 and 2/3 formed in float); T double promotes them.
+ */
+#define DEFINE_CARRY(T, SUFFIX)                                                                   \
+    /* gradient, fdtd.hpp:1946-1967: along an axis of stride st, the mask's four bits m */       \
+    static T gradient_##SUFFIX(const T *q, uint64_t i, uint64_t st, unsigned m, float shift) {   \
+        if ((m & 15u) == 15u)                                                                     \
+            return ((T)8 * (q[i + st] - q[i - st]) - (q[i + 2 * st] - q[i - 2 * st])) *          \
+                   ((T)1 / (T)12);                                                                \
+        const int below = (m & 1u) != 0, above = (m & 2u) != 0;                                   \
+        const T c = q[i];                                                                         \
+        T faces = 0, loops = 0;                                                                   \
+        if (above) {                                                                              \
+            faces += (T)0.5 * (q[i + st] - c);                                                    \
+            if (m & 8u) loops += q[i + st] - q[i + 2 * st];                                       \
+        } else if (shift < 0.0f) {                                                                \
+            faces -= c;                                                                           \
+        }                                                                                         \
+        if (below) {                                                                              \
+            faces += (T)0.5 * (c - q[i - st]);                                                    \
+            if (m & 4u) loops += q[i - 2 * st] - q[i - st];                                       \
+        } else if (shift > 0.0f) {                                                                \
+            faces += c;                                                                           \
+        }                                                                                         \
+        if (below && above) loops += q[i + st] - q[i - st];                                       \
+        return faces + loops * ((T)1 / (T)12);                                                    \
+    }                                                                                             \
+    /* carried, fdtd.hpp:1970-1974: the plain way */                                             \
+    static T carried_##SUFFIX(const oracle_solver *s, const T *q, uint64_t i) {                  \
+        const float sx = s->flow_x[i], sy = s->flow_y[i];                                        \
+        const unsigned m = s->flow_mask[i];                                                       \
+        return -((T)sx * gradient_##SUFFIX(q, i, 1, m & 15u, sx) +                                \
+                 (T)sy * gradient_##SUFFIX(q, i, s->sy, m >> 4, sy));                             \
+    }                                                                                             \
+    /* carried_round, fdtd.hpp:1978-1991; carried_border, fdtd.hpp:1996-2020 */                  \
+    static T carried_round_##SUFFIX(const oracle_solver *s, const T *q, uint64_t i) {            \
+        const uint64_t stride[3] = {1, s->sy, s->sz};                                             \
+        const int border = s->flow_mask[i] == 2;                                                  \
+        const T c = q[i];                                                                         \
+        T sum = 0;                                                                                \
+        for (int d = 0; d < 3; ++d) {                                                             \
+            const uint64_t st = stride[d];                                                        \
+            const float *w = s->wind[d], *l = s->loop[d];                                         \
+            const T above = q[i + st], below = q[i - st];                                         \
+            if (!border) {                                                                        \
+                sum += (T)0.5 * ((T)w[i] * (above - c) + (T)w[i - st] * (c - below)) +            \
+                       (T)l[i] * (above - q[i + 2 * st]) + (T)l[i - st] * (above - below) +       \
+                       (T)l[i - 2 * st] * (q[i - 2 * st] - below);                                \
+                continue;                                                                         \
+            }                                                                                     \
+            if (s->flow_mask[i + st]) {                                                           \
+                sum += (T)0.5 * (T)w[i] * (above - c);                                            \
+            } else if (w[i] < 0.0f) {                                                             \
+                sum -= (T)w[i] * c;                                                               \
+            }                                                                                     \
+            if (s->flow_mask[i - st]) {                                                           \
+                sum += (T)0.5 * (T)w[i - st] * (c - below);                                       \
+            } else if (w[i - st] > 0.0f) {                                                        \
+                sum += (T)w[i - st] * c;                                                          \
+            }                                                                                     \
+            sum += (T)l[i] * (above - q[i + 2 * st]) + (T)l[i - st] * (above - below) +           \
+                   (T)l[i - 2 * st] * (q[i - 2 * st] - below);                                    \
+        }                                                                                         \
+        return -sum;                                                                              \
+    }                                                                                             \
+    static int still_##SUFFIX(const oracle_solver *s, uint64_t i) {                               \
+        return s->round ? s->flow_mask[i] == 0 : (s->flow_x[i] == 0.0f && s->flow_y[i] == 0.0f);  \
+    }                                                                                             \
+    static T moved_##SUFFIX(const oracle_solver *s, const T *q, uint64_t i) {                     \
+        return s->round ? carried_round_##SUFFIX(s, q, i) : carried_##SUFFIX(s, q, i);            \
+    }                                                                                             \
+    /* carry, fdtd.hpp:2049-2097: the three stages over this thread's cells [i0, i1) */          \
+    static void carry_##SUFFIX(const oracle_job *job, T *q, uint64_t i0, uint64_t i1) {          \
+        const oracle_solver *s = job->s;                                                          \
+        T *t1 = (T *)s->t1, *t2 = (T *)s->t2;                                                     \
+        for (uint64_t i = i0; i < i1; ++i) {                                                      \
+            if (s->types[i] == 0) continue;                                                       \
+            t1[i] = still_##SUFFIX(s, i) ? q[i] : q[i] + moved_##SUFFIX(s, q, i);                  \
+        }                                                                                         \
+        step_barrier(job);                                                                        \
+        for (uint64_t i = i0; i < i1; ++i) {                                                      \
+            if (s->types[i] == 0) continue;                                                       \
+            t2[i] = still_##SUFFIX(s, i) ? q[i]                                                   \
+                                         : (T)0.75 * q[i] + (T)0.25 * (t1[i] + moved_##SUFFIX(s, t1, i)); \
+        }                                                                                         \
+        step_barrier(job);                                                                        \
+        for (uint64_t i = i0; i < i1; ++i) {                                                      \
+            if (s->types[i] == 0 || still_##SUFFIX(s, i)) continue;                               \
+            q[i] = q[i] + ((T)2 / (T)3) * ((t2[i] + moved_##SUFFIX(s, t2, i)) - q[i]);            \
+        }                                                                                         \
+        step_barrier(job);                                                                        \
+    }
+
+DEFINE_CARRY(float, f32)
+DEFINE_CARRY(double, f64)
+
+/*
  * One instantiation per arithmetic type T. Each expression keeps the reference's operands in the
  * reference's order; with T float every operation rounds to float as the reference's does.
  */
-#define DEFINE_STEPPER(T, NAME, FLUSH)                                                            \
+#define DEFINE_STEPPER(T, NAME, FLUSH, SUFFIX)                                                    \
     static void NAME(const oracle_job *job) {                                                    \
         oracle_solver *s = job->s;                                                               \
         const float *signal = job->signal;                                                       \
@@ -223,6 +344,11 @@ int oracle_create(const fdtd_layout *L, int precision, oracle_solver **out) {
                 for (uint64_t k = s->probe_start[p]; k < s->probe_start[p + 1]; ++k)             \
                     value += s->probe_weights[k] * (double)b[s->probe_cells[k]];                 \
                 out[p * steps + step] = value;                                                   \
+            }                                                                                    \
+            /* moving air: both levels carried along (fdtd.hpp:833-840) */                       \
+            if (s->flowing) {                                                                    \
+                carry_##SUFFIX(job, b, i0, i1);                                                  \
+                carry_##SUFFIX(job, a, i0, i1);                                                  \
             }                                                                                    \
             /* interior (fdtd.hpp:242-288) */                                                    \
             for (uint64_t i = i0; i < i1; ++i) {                                                 \
@@ -295,8 +421,8 @@ int oracle_create(const fdtd_layout *L, int precision, oracle_solver **out) {
         flush_leave(FLUSH, csr);                                                                 \
     }
 
-DEFINE_STEPPER(float, step_fp32, 1)
-DEFINE_STEPPER(double, step_fp64, 0)
+DEFINE_STEPPER(float, step_fp32, 1, f32)
+DEFINE_STEPPER(double, step_fp64, 0, f64)
 
 /*
  * ORACLE_FP32C: the same scheme in exact arithmetic, stepped in float on the pressure p_n and its

@@ -100,12 +100,19 @@ def box_solver(size, cell, stencil, *, branches=True, speed=None, probes=24, bet
     return solver, rate
 
 
-def open_ground(h=0.3, speed=None, probes=6):
+def open_ground(h=0.3, speed=None, probes=6, flow=None, screen=False):
     """A 5 m x 4 m ground in the open, its grid ringed by the matched layer (8 cells, damping
-    0.5): tests/test_gpu.py:87-110."""
+    0.5): tests/test_gpu.py:87-110. ``flow(centres)`` gives the air's motion (cells per step along
+    x and y, tests/test_wave.py:123-133); ``screen`` stands a 1.5 m wall across y at x = 2.6 m on
+    the ground, which the wind must go round."""
     native, _, wave, _ = _modules()
     vertices = np.array([[0, 0, 0], [5, 0, 0], [5, 4, 0], [0, 4, 0]], float)
-    bvh = native.Bvh(vertices, np.array([[0, 1, 2], [0, 2, 3]], np.int64))
+    faces = np.array([[0, 1, 2], [0, 2, 3]], np.int64)
+    if screen:
+        wall = np.array([[2.6, 1.0, 0.0], [2.6, 3.0, 0.0], [2.6, 3.0, 1.5], [2.6, 1.0, 1.5]], float)
+        faces = np.vstack([faces, np.array([[4, 5, 6], [4, 6, 7]], np.int64)])
+        vertices = np.vstack([vertices, wall])
+    bvh = native.Bvh(vertices, faces)
     source = np.array([2.0, 2.0, 1.5])
     listeners = np.vstack(
         [np.array([[4.0, 3.0, 1.2], [1.0, 1.0, 0.6]]), spread_points([0.5, 0.5, 0.3], [4.5, 3.5, 2.0], probes - 2, 11)]
@@ -121,9 +128,15 @@ def open_ground(h=0.3, speed=None, probes=6):
         zz, yy, xx = np.meshgrid(z, y, x, indexing="ij")
         centres = np.column_stack([xx.reshape(-1), yy.reshape(-1), zz.reshape(-1)])
         speeds = np.ascontiguousarray(speed(centres), dtype=np.float32)
+    flows = {}
+    if flow is not None:
+        x, y, z = (origin[a] + (np.arange(shape[a]) + 0.5) * h for a in range(3))
+        zz, yy, xx = np.meshgrid(z, y, x, indexing="ij")
+        fx, fy = flow(np.column_stack([xx.reshape(-1), yy.reshape(-1), zz.reshape(-1)]))
+        flows = {"flow_x": np.ascontiguousarray(fx, np.float32), "flow_y": np.ascontiguousarray(fy, np.float32)}
     solver = native.WaveSolver(
         bvh,
-        np.zeros(2, np.int64),
+        np.zeros(len(faces), np.int64),
         np.array([0.05]),
         np.zeros((0, 3)),
         np.zeros(0, np.int64),
@@ -136,8 +149,20 @@ def open_ground(h=0.3, speed=None, probes=6):
         layer_damping=wave.LAYER_DAMPING,
         threads=1,
         speed=speeds,
+        **flows,
     )
     return solver, C / (wave.COURANT * h)
+
+
+def _wind(centres):
+    """A wind along +x and a little along -y, stronger with height: 0.12 + 0.04 z cells a step along x,
+    -0.03 along y (each below half a cell a step)."""
+    z = np.maximum(centres[:, 2], 0.0)
+    return 0.12 + 0.04 * np.minimum(z, 2.0), np.full(len(centres), -0.03)
+
+
+def _uniform_wind(centres):
+    return np.full(len(centres), 0.2), np.full(len(centres), 0.07)
 
 
 # ---- the L-room of tests/test_fitted_walls.py:280-300, with fitted walls ----------------------
@@ -257,6 +282,8 @@ CASES = {
     "open_layer_speed": (lambda: open_ground(speed=_gradient), 500, "noise"),
     "fitted_closed": (fitted_closed, 400, "drive"),
     "fitted_open": (fitted_open, 400, "noise"),
+    "wind_plain": (lambda: open_ground(flow=_uniform_wind), 400, "drive"),
+    "wind_round": (lambda: open_ground(flow=_wind, screen=True), 400, "noise"),
 }
 
 

@@ -29,6 +29,11 @@ def golden_names() -> list[str]:
     return list(json.loads((GOLDEN / "manifest.json").read_text()))
 
 
+def still_names() -> list[str]:
+    """The golden grids without moving air: the ones the compensated form and stacking take."""
+    return [n for n in golden_names() if not n.startswith("wind_")]
+
+
 def load_golden(name: str):
     """(layout, signal, reference) of a golden fixture: the reference's layout arrays, the drive,
     and the reference's own probe series (probes, steps)."""

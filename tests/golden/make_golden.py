@@ -1,4 +1,5 @@
-"""Writes the golden fixtures of the wave solver's time stepping: ``python tests/golden/make_golden.py``.
+"""Writes the golden fixtures of the wave solver's time stepping: ``python tests/golden/make_golden.py
+[case ...]`` (every case when none is named).
 
 For each case of ``tests/cases.py`` (small grids laid out by the reference's own C++ solver,
 naelolaiz/acoustic-spaces cpp/include/acoustic_spaces/fdtd.hpp, compiled unmodified by
@@ -35,19 +36,22 @@ KEEP = (
     "source", "state_start", "state_branch", "state_weight", "branch_now", "branch_before",
     "branch_gain", "layer_cells", "keep_x", "keep_face_x", "keep_y", "keep_face_y", "keep_z",
     "keep_face_z", "push_x", "push_face_x", "push_y", "push_face_y", "push_z", "push_face_z",
-    "probe_start", "probe_cells", "probe_weights", "flow_mask",
+    "probe_start", "probe_cells", "probe_weights", "flow_mask", "flow_x", "flow_y", "wind_x", "wind_y", "wind_z",
+    "loop_x", "loop_y", "loop_z",
 )  # fmt: skip
 
 
-def main() -> None:
+def main(names: list[str]) -> None:
+    """Writes the fixtures of ``names`` (every case when empty), keeping the others' entries."""
     if not cases.available():
         raise SystemExit("the reference sources are needed to make the golden fixtures")
-    manifest = {}
-    for name in cases.CASES:
+    path = HERE / "manifest.json"
+    manifest = json.loads(path.read_text()) if path.exists() else {}
+    for name in names or cases.CASES:
         solver, signal = cases.build_case(name)
         layout = solver.layout()
         reference = solver.run(signal)
-        arrays = {f"layout/{k}": np.asarray(layout[k]) for k in KEEP}
+        arrays = {f"layout/{k}": np.asarray(layout[k]) for k in KEEP if k in layout}
         arrays["signal"] = signal
         arrays["reference"] = reference
         np.savez_compressed(HERE / f"{name}.npz", **arrays)
@@ -65,8 +69,9 @@ def main() -> None:
             "reference_sha256": hashlib.sha256(reference.tobytes()).hexdigest(),
         }
         print(name, manifest[name]["shape"], manifest[name]["reference_sha256"][:12])
-    (HERE / "manifest.json").write_text(json.dumps(manifest, indent=1) + "\n")
+    manifest = {name: manifest[name] for name in cases.CASES if name in manifest}
+    path.write_text(json.dumps(manifest, indent=1) + "\n")
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

@@ -13,7 +13,7 @@ from __future__ import annotations
 
 import numpy as np
 import pytest
-from conftest import golden_names, load_golden
+from conftest import load_golden, still_names
 
 from acoustic_spaces_b200 import layouts as L
 from oracle.oracle import OracleSolver
@@ -56,7 +56,7 @@ def test_compensated_holds_a_closed_rooms_net_mass():
     assert e32c < 1e-5, e32c
 
 
-@pytest.mark.parametrize("name", golden_names())
+@pytest.mark.parametrize("name", still_names())
 def test_compensated_is_no_worse_than_fp32_on_the_golden_grids(name):
     layout, signal, reference = load_golden(name)
     p64 = OracleSolver(layout, "fp64").run(signal)
@@ -93,7 +93,7 @@ def test_compensated_reset_and_pieces_repeat_the_run():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", golden_names())
+@pytest.mark.parametrize("name", still_names())
 def test_gpu_compensated_equals_its_oracle_on_the_golden_grids(name):
     from acoustic_spaces_b200 import B200WaveSolver
 

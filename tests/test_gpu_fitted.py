@@ -98,5 +98,9 @@ def test_gpu_full_size_fitted_room_in_pieces_is_one_run():
     got = np.concatenate([pieces.run(w.signal[a:b]) for a, b in [(0, 77), (77, 300), (300, 600)]], axis=1)
     assert np.array_equal(got, one)
     p64 = B200WaveSolver(layout, precision="fp64").run(w.signal)
-    rel = np.linalg.norm(one - p64, axis=1) / np.linalg.norm(p64, axis=1)
+    # (over the receivers the sound has reached in these 600 steps)
+    energy = np.linalg.norm(p64, axis=1)
+    reached = energy > 1e-3 * energy.max()
+    assert reached.sum() >= 4
+    rel = np.linalg.norm(one - p64, axis=1)[reached] / energy[reached]
     assert rel.max() <= 1e-4, rel.max()

@@ -180,9 +180,9 @@ def test_a_stack_steps_each_grid_as_it_steps_alone():
 @pytest.mark.parametrize("across", [1, 2, 3])
 def test_golden_grids_stack_with_their_own_runs(across):
     # (across > 1: grids of different shapes side by side along x in one group of planes)
-    from conftest import golden_names, load_golden
+    from conftest import load_golden, still_names
 
-    names = [n for n in golden_names() if len(load_golden(n)[0]["layer_cells"]) == 0 and load_golden(n)[0]["scaled"][0] == 0]
+    names = [n for n in still_names() if len(load_golden(n)[0]["layer_cells"]) == 0 and load_golden(n)[0]["scaled"][0] == 0]
     layouts = [load_golden(n)[0] for n in names]
     sevens = [lay for lay in layouts if int(lay["stencil"][0]) == 7]
     stacked = L.stack(sevens, across=across)
