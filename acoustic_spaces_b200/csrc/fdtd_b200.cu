@@ -25,6 +25,7 @@
 
 #include "fdtd_adjoint.cuh"
 #include "fdtd_b200.h"
+#include "fdtd_flow.cuh"
 #include "fdtd_kernels.cuh"
 
 using namespace fdtd;
@@ -129,6 +130,11 @@ struct fdtd_solver {
     // buffers: faces[1] holds the latest values between runs, as u[1] does.
     void *faces[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
     uint32_t link_slots = 0;  // the most links of a special row (6 or 18 kernels)
+    // Moving air (fdtd_flow.cuh): whether the grid's air moves, which form carries it, the carry's
+    // cell lists, fields and stage buffers, and its launches' blocks.
+    bool flowing = false, flow_round = false;
+    Flow flow{};
+    uint32_t flow_blocks = 0;
     unsigned int *d_error = nullptr;  // set by a kernel whose wait gave up
     // Tensor maps of the bulk sweep: each level as the pressure tile (with halos) and as the
     // previous-pressure tile, the cell types and the scales.
@@ -245,6 +251,60 @@ int zeros(fdtd_solver *s, size_t bytes, void **out) {
     return FDTD_OK;
 }
 
+// Whether cell i's air moves: the plain form's shifts, or the round form's mask (fdtd.hpp:2049-2097
+// skips the others, whose levels stand still through the carry).
+bool moves(const fdtd_layout *L, uint64_t i) {
+    if (L->types[i] == kSolid) return false;
+    return L->wind[0] ? L->flow_mask[i] != 0 : (L->flow_x[i] != 0.0f || L->flow_y[i] != 0.0f);
+}
+
+// The cells the carry of moving cell (x, y, z) reads, as (axis, step) pairs: the plain form's x
+// and y neighbours as its mask's bits allow them (fdtd.hpp:1946-1967), the round form's two
+// neighbours either side along every axis (fdtd.hpp:1978-2020).
+template <class Visit>
+void flow_reads(const fdtd_layout *L, uint64_t i, Visit visit) {
+    if (L->wind[0]) {
+        for (int a = 0; a < 3; ++a)
+            for (int step : {-2, -1, 1, 2}) visit(a, step);
+        return;
+    }
+    for (int a = 0; a < 2; ++a) {
+        const unsigned m = a == 0 ? (L->flow_mask[i] & 15u) : (L->flow_mask[i] >> 4);
+        if (m == 15u) {
+            for (int step : {-2, -1, 1, 2}) visit(a, step);
+            continue;
+        }
+        if (m & 1u) visit(a, -1);
+        if (m & 2u) visit(a, 1);
+        if (m & 4u) visit(a, -2);
+        if (m & 8u) visit(a, 2);
+    }
+}
+
+// The moving air's arrays present, and every cell a moving cell's carry reads inside the grid
+// (the reference leaves two cells of still air or wall round it).
+std::string flow_check(const fdtd_layout *L) {
+    const uint64_t n = L->nx * L->ny * L->nz;
+    if (L->flow_count != n) return "moving air needs one mask per cell";
+    if (!L->flow_mask) return "moving air needs its mask";
+    const bool round = L->wind[0] != nullptr;
+    for (int d = 0; d < 3; ++d)
+        if (round && (!L->wind[d] || !L->loop[d])) return "the round form needs each axis's winds and loops";
+    if (!round && (!L->flow_x || !L->flow_y)) return "the plain form needs the shifts along x and y";
+    const uint64_t len[3] = {L->nx, L->ny, L->nz};
+    for (uint64_t i = 0; i < n; ++i) {
+        if (!moves(L, i)) continue;
+        const uint64_t at[3] = {i % L->nx, (i / L->nx) % L->ny, i / (L->nx * L->ny)};
+        bool inside = true;
+        flow_reads(L, i, [&](int a, int step) {
+            const int64_t c = (int64_t)at[a] + step;
+            if (c < 0 || c >= (int64_t)len[a]) inside = false;
+        });
+        if (!inside) return "a moving cell's carry reads outside the grid";
+    }
+    return "";
+}
+
 int validate(const fdtd_layout *L, std::string &why) {
     auto refuse = [&](const std::string &m) {
         why = m;
@@ -252,8 +312,11 @@ int validate(const fdtd_layout *L, std::string &why) {
     };
     if (!L) return refuse("no layout");
     if (L->stencil != 7 && L->stencil != 19) return refuse("the stencil has 7 or 19 points");
-    if (L->flow_count) return refuse("the GPU steps still air only: moving air stays on the CPU");
     if (L->nx < 3 || L->ny < 3 || L->nz < 3) return refuse("the grid is too small");
+    if (L->flow_count) {
+        const std::string bad = flow_check(L);
+        if (!bad.empty()) return refuse(bad);
+    }
     const uint64_t n = L->nx * L->ny * L->nz;
     if (L->nx > (1ull << 31) || L->ny > (1ull << 31) || L->nz > (1ull << 31) || n >= (1ull << 32) ||
         n / L->nx / L->ny != L->nz)
@@ -547,6 +610,23 @@ void launch_bulk(const fdtd_solver *s, const CUtensorMap &mb, const CUtensorMap 
 #undef FDTD_BULK
 }
 
+// The carry of both levels (b, the current, and a), before a step's updates.
+template <typename T>
+int launch_carry(fdtd_solver *s, const Fields<T> &f, cudaStream_t stream) {
+    T *b = const_cast<T *>(f.b), *a = f.a;
+    const dim3 grid(s->flow_blocks, 2);
+    if (s->flow_round) {
+        carry_kernel<T, true, 1><<<grid, kBlock, 0, stream>>>(s->flow, b, a);
+        carry_kernel<T, true, 2><<<grid, kBlock, 0, stream>>>(s->flow, b, a);
+        carry_kernel<T, true, 3><<<grid, kBlock, 0, stream>>>(s->flow, b, a);
+    } else {
+        carry_kernel<T, false, 1><<<grid, kBlock, 0, stream>>>(s->flow, b, a);
+        carry_kernel<T, false, 2><<<grid, kBlock, 0, stream>>>(s->flow, b, a);
+        carry_kernel<T, false, 3><<<grid, kBlock, 0, stream>>>(s->flow, b, a);
+    }
+    return FDTD_OK;
+}
+
 template <typename T, bool WIDE, bool SCALED, bool COMP = false>
 int launch_steps(fdtd_solver *s, const float *d_signal, uint64_t steps, double *d_out, uint64_t stride) {
     const Tables &g = s->tables;
@@ -583,6 +663,14 @@ int launch_steps(fdtd_solver *s, const float *d_signal, uint64_t steps, double *
                 CUDA_TRY(s, cudaStreamWaitEvent(s->stream, s->joined[1], 0));
                 if (layer_blocks) CUDA_TRY(s, cudaStreamWaitEvent(s->stream, s->joined[2], 0));
             }
+        }
+        // Moving air: the probes read the levels before the carry moves them (fdtd.hpp:833-840
+        // after the record of fdtd.hpp:3525-3533); the step's updates follow the carry.
+        if (s->flowing) {
+            if (probe_blocks && s->record_probes) probe_kernel<T><<<probe_blocks, kBlock, 0, s->stream>>>(g, f);
+            launch_carry<T>(s, f, s->stream);
+        }
+        if (fork) {
             CUDA_TRY(s, cudaEventRecord(s->joined[0], s->stream));
             CUDA_TRY(s, cudaStreamWaitEvent(side, s->joined[0], 0));
             if (layer_blocks) CUDA_TRY(s, cudaStreamWaitEvent(layer, s->joined[0], 0));
@@ -634,7 +722,7 @@ int launch_steps(fdtd_solver *s, const float *d_signal, uint64_t steps, double *
         if (ev) CUDA_TRY(s, cudaEventRecord(ev[5], side));
         if (ev) CUDA_TRY(s, cudaEventRecord(ev[6], side));
         // (A recomputation for the gradient records the special rows instead of the probes.)
-        if (probe_blocks && s->record_probes) probe_kernel<T><<<probe_blocks, kBlock, 0, side>>>(g, f);
+        if (probe_blocks && s->record_probes && !s->flowing) probe_kernel<T><<<probe_blocks, kBlock, 0, side>>>(g, f);
         if (ev) CUDA_TRY(s, cudaEventRecord(ev[7], side));
         if (fork) {
             CUDA_TRY(s, cudaEventRecord(s->joined[1], side));
@@ -732,6 +820,61 @@ int capture(fdtd_solver *s, cudaGraphExec_t *out) {
     return FDTD_OK;
 }
 
+// Moving air on the device: the moving cells and the still air cells their carry reads (pitched),
+// the form's fields pitched, and two stage buffers for each level (zero, as the cells never
+// written stay: walls and padding read as still, silent air).
+int set_up_flow(fdtd_solver *s, const fdtd_layout *L) {
+    s->flowing = true;
+    s->flow_round = L->wind[0] != nullptr;
+    const uint64_t n = s->n, nx = s->nx, ny = s->ny;
+    std::vector<uint32_t> cells, halo;
+    std::vector<uint8_t> seen(n, 0);
+    for (uint64_t i = 0; i < n; ++i)
+        if (moves(L, i)) cells.push_back(pitched(s, i)), seen[i] = 1;
+    const int64_t stride[3] = {1, (int64_t)nx, (int64_t)(nx * ny)};
+    for (uint64_t i = 0; i < n; ++i) {
+        if (!moves(L, i)) continue;
+        flow_reads(L, i, [&](int a, int step) {
+            const uint64_t j = (uint64_t)((int64_t)i + step * stride[a]);
+            if (L->types[j] != kSolid && !seen[j]) seen[j] = 1, halo.push_back(pitched(s, j));
+        });
+    }
+    std::sort(halo.begin(), halo.end());
+    Flow &f = s->flow;
+    f.moving = (uint32_t)cells.size();
+    cells.insert(cells.end(), halo.begin(), halo.end());
+    f.count = (uint32_t)cells.size();
+    f.sy = (uint32_t)s->pitch;
+    f.sz = (uint32_t)(s->pitch * ny);
+    int rc;
+    if ((rc = upload(s, cells.data(), cells.size(), &f.cells))) return rc;
+    auto pitch_up = [&](const auto *host, auto **out) {
+        using V = std::remove_const_t<std::remove_pointer_t<decltype(host)>>;
+        std::vector<V> a(s->n_device, V(0));
+        for (uint64_t z = 0; z < s->nz; ++z)
+            for (uint64_t y = 0; y < ny; ++y)
+                std::memcpy(&a[s->pitch * (y + ny * z)], &host[nx * (y + ny * z)], nx * sizeof(V));
+        return upload(s, a.data(), a.size(), out);
+    };
+    if ((rc = pitch_up(L->flow_mask, &f.mask))) return rc;
+    if (s->flow_round) {
+        for (int d = 0; d < 3; ++d) {
+            if ((rc = pitch_up(L->wind[d], &f.wind[d]))) return rc;
+            if ((rc = pitch_up(L->loop[d], &f.loop[d]))) return rc;
+        }
+    } else {
+        if ((rc = pitch_up(L->flow_x, &f.shift_x))) return rc;
+        if ((rc = pitch_up(L->flow_y, &f.shift_y))) return rc;
+    }
+    const size_t e = s->precision == FDTD_FP64 ? 8 : 4;
+    for (int k = 0; k < 2; ++k) {
+        if ((rc = zeros(s, e * s->n_device, &f.t1[k]))) return rc;
+        if ((rc = zeros(s, e * s->n_device, &f.t2[k]))) return rc;
+    }
+    s->flow_blocks = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((f.count + kBlock - 1) / kBlock, 4ull * s->sms));
+    return FDTD_OK;
+}
+
 int build(fdtd_solver *s, const fdtd_layout *L) {
     const uint64_t nx = L->nx, ny = L->ny, nz = L->nz, n = nx * ny * nz;
     s->nx = nx, s->ny = ny, s->nz = nz, s->n = n;
@@ -799,6 +942,7 @@ int build(fdtd_solver *s, const fdtd_layout *L) {
     s->d_sig = static_cast<float *>(chunk);
     if ((rc = zeros(s, sizeof(double) * kGraphSteps * std::max<uint64_t>(1, L->probe_count), &chunk))) return rc;
     s->d_rec = static_cast<double *>(chunk);
+    if (L->flow_count && (rc = set_up_flow(s, L))) return rc;
 
     // The bulk sweep: tiles of kTX x kTY over the box, x from a 16-aligned start; chunks of planes
     // enough for every multiprocessor several times over.
@@ -1821,6 +1965,8 @@ int fdtd_create(const fdtd_layout *layout, int precision, int device, fdtd_solve
         return set_global(FDTD_EINVAL, "precision is FDTD_FP32, FDTD_FP64 or FDTD_FP32_COMPENSATED");
     std::string why;
     if (validate(layout, why) != FDTD_OK) return set_global(FDTD_EINVAL, why);
+    if (layout->flow_count && precision == FDTD_FP32_COMPENSATED)
+        return set_global(FDTD_EINVAL, "the compensated form steps still air only");
     int count = 0;
     if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0 || device < 0 || device >= count) {
         cudaGetLastError();
@@ -2033,6 +2179,7 @@ int fdtd_gradient_noalloc(fdtd_solver *s, const float *signal, uint64_t steps, c
     if (s->precision == FDTD_FP32_COMPENSATED)
         return fail(s, FDTD_EINVAL, "the gradient steps FDTD_FP32 or FDTD_FP64, not the compensated form");
     if (steps == 0) return fail(s, FDTD_EINVAL, "no steps to differentiate");
+    if (s->flowing) return fail(s, FDTD_EINVAL, "the gradient steps still air only");
     if (!signal || (s->probes && !dloss_dy)) return fail(s, FDTD_EINVAL, "no signal or loss gradient");
     DeviceGuard guard(s->device);
     void *base;
@@ -2149,6 +2296,7 @@ int fdtd_run_linked(fdtd_solver *const *solvers, uint32_t count, const fdtd_plan
         if (s->probes && out_stride < steps) return fail(s, FDTD_EINVAL, "the output's stride is shorter than the run");
         if (s->precision != solvers[0]->precision)
             return set_global(FDTD_EINVAL, "the group's solvers step in one precision");
+        if (s->flowing) return fail(s, FDTD_EINVAL, "linked slabs step still air only");
         for (uint32_t g = 0; g < h; ++g)
             if (solvers[g] == s) return set_global(FDTD_EINVAL, "a solver appears twice in the group");
     }
@@ -2395,6 +2543,7 @@ int fdtd_set_tape_budget(fdtd_solver *s, uint64_t bytes) {
 int fdtd_set_tape(fdtd_solver *s, uint64_t segment) {
     if (!s) return set_global(FDTD_EINVAL, "no solver");
     if (segment && s->precision == FDTD_FP32_COMPENSATED) return fail(s, FDTD_EINVAL, "the gradient steps FDTD_FP32 or FDTD_FP64, not the compensated form");
+    if (segment && s->flowing) return fail(s, FDTD_EINVAL, "the gradient steps still air only");
     s->tape_segment = segment;
     s->tape_valid = false;
     return FDTD_OK;
@@ -2432,6 +2581,7 @@ int fdtd_gradient(fdtd_solver *s, const float *signal, uint64_t steps, const dou
     if (s->precision == FDTD_FP32_COMPENSATED)
         return fail(s, FDTD_EINVAL, "the gradient steps FDTD_FP32 or FDTD_FP64, not the compensated form");
     if (steps == 0) return fail(s, FDTD_EINVAL, "no steps to differentiate");
+    if (s->flowing) return fail(s, FDTD_EINVAL, "the gradient steps still air only");
     if (!signal || (s->probes && !dloss_dy)) return fail(s, FDTD_EINVAL, "no signal or loss gradient");
     DeviceGuard guard(s->device);
     int rc = set_up_adjoint(s);

@@ -53,7 +53,7 @@ def _bad(**changes):
     "changes, message",
     [
         ({"stencil": np.array([9], np.uint64)}, "the stencil has 7 or 19 points"),
-        ({"flow_mask": np.ones(4, np.uint8)}, "moving air stays on the CPU"),
+        ({"flow_mask": np.ones(4, np.uint8)}, "one mask per cell"),
         ({"shape": np.array([2, 14, 12], np.uint64)}, "the grid is too small"),
         ({"shape": np.array([70000, 70000, 12], np.uint64)}, "32-bit indices"),
     ],
@@ -193,3 +193,28 @@ def test_a_speed_outside_its_range_is_refused(bad):
     status, error = _create(dict(layout, scale=scale))
     assert status == _abi.FDTD_EINVAL and "lies in (0, 1]" in error
     assert _create(layout)[0] != _abi.FDTD_EINVAL  # the golden layout itself passes the check
+
+
+@pytest.mark.parametrize("name", ["wind_plain", "wind_round"])
+def test_moving_air_is_checked_before_the_device(name):
+    # The reference's wind grids pass; the compensated form refuses moving air; a moving cell
+    # whose carry would read beyond the grid's edge is refused (the round form reads two cells
+    # either side along every axis).
+    layout, _, _ = load_golden(name)
+    assert _create(layout)[0] != _abi.FDTD_EINVAL
+    status, error = _create(layout, _abi.FDTD_FP32_COMPENSATED)
+    assert status == _abi.FDTD_EINVAL and "still air only" in error
+    nx, ny, _ = (int(v) for v in layout["shape"])
+    types = np.asarray(layout["types"])
+    edge = [i for i in np.flatnonzero(types) if i % nx == 1][0]
+    mask = np.asarray(layout["flow_mask"]).copy()
+    changed = dict(layout, flow_mask=mask)
+    if name == "wind_round":
+        mask[edge] = 1
+    else:
+        mask[edge] = 15  # x's four bits: two cells either side along x
+        fx = np.asarray(layout["flow_x"], np.float32).copy()
+        fx[edge] = 0.1
+        changed["flow_x"] = fx
+    status, error = _create(changed)
+    assert status == _abi.FDTD_EINVAL and "reads outside the grid" in error

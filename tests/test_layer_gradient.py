@@ -89,6 +89,27 @@ def test_layer_gradient_in_segments_and_from_a_tape_is_one_segments():
         np.testing.assert_array_equal(taped[key], pieces[key], err_msg=key)
 
 
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+def test_the_walls_gradient_without_the_tables_is_the_same(precision):
+    # Without the tables no layer factor is recorded: the walls' gradient is the same to the bit,
+    # and a second gradient with the tables gives them again, summed in the same fixed order.
+    layout, signal, _ = load_golden("fitted_open")
+    signal = signal[:150]
+    target, _ = _problem(layout, signal)
+    solver = B200WaveSolver(layout, precision=precision)
+    y = solver.run(signal)
+    solver.reset()
+    dloss = 2.0 * (y - target)
+    with_tables = solver.gradient(signal, dloss, segment=40)
+    walls = solver.gradient(signal, dloss, segment=40, layer_tables=False)
+    again = solver.gradient(signal, dloss, segment=40)
+    assert set(walls) | set(_TABLES) == set(with_tables) and not set(walls) & set(_TABLES)
+    for key in walls:
+        np.testing.assert_array_equal(walls[key], with_tables[key], err_msg=key)
+    for key in with_tables:
+        np.testing.assert_array_equal(again[key], with_tables[key], err_msg=key)
+
+
 def test_the_layer_damping_gradient_on_the_gpu_matches_central_differences():
     # dL/d(layer damping) = the B200's tables' gradient times the tables' tangent in the damping
     # (layouts.layer_tables_tangent), against a central difference of the loss (the FP64 oracle)
