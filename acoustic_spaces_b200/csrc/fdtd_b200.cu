@@ -1577,8 +1577,10 @@ int restore_checkpoint(fdtd_solver *s, const char *c) {
 
 // Whether the handle holds the tape of a run of this drive with these segments: gradient<T> then
 // takes the tape's checkpoints or trajectory and recomputes no forward pass of its own.
+// (A trajectory holds no matched layer's factors: a gradient in the layer's tables recomputes.)
 bool holds_tape(const fdtd_solver *s, const float *signal, uint64_t steps, uint64_t segment) {
     if (segment == 0 || segment > steps) segment = steps;
+    if (s->tape_traj && s->layers && s->gradient_tables) return false;
     return s->tape_valid && s->tape_signal.size() == steps && std::min<uint64_t>(s->tape_segment, steps) == segment &&
            std::memcmp(s->tape_signal.data(), signal, sizeof(float) * steps) == 0;
 }
@@ -2069,9 +2071,10 @@ int fdtd_run(fdtd_solver *s, const float *signal, uint64_t steps, double *out) {
             CUDA_TRY(s, cudaMemGetInfo(&free_bytes, &total_bytes));
             budget = free_bytes / 2 + e * (K + S) * s->tape_levels;  // (what the tape holds already counts)
         }
-        // (A grid with a matched layer keeps checkpoints: its gradient recomputes the layer's
-        // factors a segment at a time.)
-        keep_traj = K + S > 0 && !s->layers && e * (K + S) * (steps + 2) <= budget;
+        // (A grid with a matched layer whose gradients give its tables keeps checkpoints: the
+        // gradient recomputes the layer's factors a segment at a time. Without the tables the
+        // layer steps back on its carried values alone, and the rows' trajectory is all it needs.)
+        keep_traj = K + S > 0 && (!s->layers || !s->gradient_tables) && e * (K + S) * (steps + 2) <= budget;
     }
     if (keep_traj) {
         int r;
@@ -2596,6 +2599,8 @@ int fdtd_gradient(fdtd_solver *s, const float *signal, uint64_t steps, const dou
 int fdtd_set_gradient_tables(fdtd_solver *s, int enable) {
     if (!s) return set_global(FDTD_EINVAL, "no solver");
     s->gradient_tables = enable != 0;
+    // (A tape taken without the tables may hold the rows' trajectory alone: it serves no
+    // gradient in the tables, which then runs the forward pass again.)
     s->layer_gradient.clear();
     return FDTD_OK;
 }

@@ -90,6 +90,9 @@ struct Stage {
     static constexpr uint32_t tx_bytes =
         SH::BY * SH::BX * sizeof(T) + SH::TY * SH::TX * sizeof(T) + SH::TY * SH::TX + (SCALED ? SH::TY * SH::TX * 4 : 0);
     static constexpr uint32_t tx_bytes_full = tx_bytes - SH::TY * SH::TX;
+    // A tile's first and last stages (planes z0 - 1 and z_end) serve only as the pressure above or
+    // below: they carry the pressure tile alone.
+    static constexpr uint32_t tx_bytes_halo = SH::BY * SH::BX * sizeof(T);
     static constexpr uint32_t smem = SH::STAGES * bytes + 8 * SH::STAGES;  // + the stages' mbarriers
 };
 
@@ -254,11 +257,14 @@ __global__ void __launch_bounds__(kBlock) bulk_kernel(const __grid_constant__ CU
                 while (issued < target && p_tile < tiles) {
                     const int slot = issued % kStages;
                     const uint32_t stage = base + slot * S::bytes, bar = bars + 8 * slot;
-                    mbar_expect_tx(bar, p_span.full ? S::tx_bytes_full : S::tx_bytes);
+                    const bool halo = p_k < p_span.z0 || p_k >= p_span.z_end;
+                    mbar_expect_tx(bar, halo ? S::tx_bytes_halo : (p_span.full ? S::tx_bytes_full : S::tx_bytes));
                     tma_load_3d(stage + S::b_off, &map_b, p_span.xt - kHX, p_span.yt - 1, p_k, bar);
-                    tma_load_3d(stage + S::a_off, &map_a, p_span.xt, p_span.yt, p_k, bar);
-                    if (!p_span.full) tma_load_3d(stage + S::t_off, &map_t, p_span.xt, p_span.yt, p_k, bar);
-                    if (SCALED) tma_load_3d(stage + S::s_off, &map_s, p_span.xt, p_span.yt, p_k, bar);
+                    if (!halo) {
+                        tma_load_3d(stage + S::a_off, &map_a, p_span.xt, p_span.yt, p_k, bar);
+                        if (!p_span.full) tma_load_3d(stage + S::t_off, &map_t, p_span.xt, p_span.yt, p_k, bar);
+                        if (SCALED) tma_load_3d(stage + S::s_off, &map_s, p_span.xt, p_span.yt, p_k, bar);
+                    }
                     ++issued;
                     if (++p_k > p_span.z_end) {
                         p_tile += gridDim.x;

@@ -249,13 +249,16 @@ class B200WaveSolver:
         if status != _abi.FDTD_OK:
             _raise(self._lib, status, self._handle)
 
-    def set_tape(self, segment: int) -> None:
+    def set_tape(self, segment: int, layer_tables: bool = True) -> None:
         """With ``segment`` > 0, each :meth:`run` from rest keeps what a following
         :meth:`gradient` of that drive with that ``segment`` needs, so that the gradient does not
         run the forward pass again: the whole trajectory of the special rows and branch
         velocities where it fits the tape's budget (:meth:`set_tape_budget`; the gradient then
         recomputes nothing), else the state every ``segment`` steps (the gradient recomputes each
-        segment from it). 0 turns it off."""
+        segment from it). 0 turns it off. On a grid with a matched layer the trajectory serves
+        only gradients without the layer's tables (``layer_tables`` False, as the following
+        :meth:`gradient` must then be asked); with them the tape keeps checkpoints."""
+        self._lib.fdtd_set_gradient_tables(self._handle, int(bool(layer_tables)))
         status = self._lib.fdtd_set_tape(self._handle, int(segment))
         if status != _abi.FDTD_OK:
             _raise(self._lib, status, self._handle)

@@ -210,7 +210,9 @@ int fdtd_layer_gradient(const fdtd_solver *solver, double *tables);
  * or the rows' and branch states' only (0; no counterpart in the reference). Without the tables a
  * gradient records none of the layer's per-step factors (18 values a layer cell a step of the
  * segment) and steps back through the layer on its carried values alone: the walls' gradient is
- * the same, to the bit, at the cost of the layer's adjoint only.
+ * the same, to the bit, at the cost of the layer's adjoint only. It also decides a following
+ * taped run's kind (fdtd_set_tape): without the tables, a grid with a matched layer keeps the
+ * rows' trajectory where it fits, as grids without one do, and its gradient recomputes nothing.
  */
 int fdtd_set_gradient_tables(fdtd_solver *solver, int enable);
 

@@ -110,6 +110,31 @@ def test_the_walls_gradient_without_the_tables_is_the_same(precision):
         np.testing.assert_array_equal(again[key], with_tables[key], err_msg=key)
 
 
+def test_a_walls_only_tape_keeps_the_trajectory_and_gives_the_same_gradient():
+    # Taped without the tables, a grid with a matched layer keeps the rows' trajectory (no
+    # checkpoints, nothing recomputed); its walls' gradient equals the untaped one to the bit. A
+    # gradient that asks for the tables after such a tape runs the forward pass again and gives
+    # the untaped tables too.
+    layout, signal, _ = load_golden("open_layer")
+    signal = signal[:120]
+    target, _ = _problem(layout, signal)
+    solver = B200WaveSolver(layout, precision="fp64")
+    y = solver.run(signal)
+    solver.reset()
+    dloss = 2.0 * (y - target)
+    plain = solver.gradient(signal, dloss, segment=30, layer_tables=False)
+    full = solver.gradient(signal, dloss, segment=30)
+    solver.set_tape(30, layer_tables=False)
+    solver.run(signal)
+    taped = solver.gradient(signal, dloss, segment=30, layer_tables=False)
+    for key in plain:
+        np.testing.assert_array_equal(taped[key], plain[key], err_msg=key)
+    solver.run(signal)
+    retaped = solver.gradient(signal, dloss, segment=30)
+    for key in full:
+        np.testing.assert_array_equal(retaped[key], full[key], err_msg=key)
+
+
 def test_the_layer_damping_gradient_on_the_gpu_matches_central_differences():
     # dL/d(layer damping) = the B200's tables' gradient times the tables' tangent in the damping
     # (layouts.layer_tables_tangent), against a central difference of the loss (the FP64 oracle)
