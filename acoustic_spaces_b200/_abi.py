@@ -35,6 +35,7 @@ _f64p = ctypes.POINTER(ctypes.c_double)
 _u8p = ctypes.POINTER(ctypes.c_uint8)
 _i32p = ctypes.POINTER(ctypes.c_int32)
 _i64p = ctypes.POINTER(ctypes.c_int64)
+_u32p = ctypes.POINTER(ctypes.c_uint32)
 _u64p = ctypes.POINTER(ctypes.c_uint64)
 
 
@@ -136,6 +137,10 @@ class FdtdCutRoom(ctypes.Structure):
         ("nx", ctypes.c_uint64),
         ("ny", ctypes.c_uint64),
         ("nz", ctypes.c_uint64),
+        ("pieces", ctypes.c_uint32),
+        ("piece_plane", _u32p),
+        ("piece_start", _u32p),
+        ("piece_edges", _f64p),
     ]
 
 
@@ -356,7 +361,7 @@ def load_library(path: str | os.PathLike | None = None) -> ctypes.CDLL:
         fn = getattr(lib, name)
         fn.restype = restype
         fn.argtypes = argtypes
-    if lib.fdtd_abi_version() != 2:
+    if lib.fdtd_abi_version() != 3:
         raise RuntimeError("the B200 wave stepper's library has another ABI version")
     if path is None:
         from acoustic_spaces_b200 import build

@@ -34,6 +34,8 @@ namespace {
 
 constexpr int kBlockFit = 128;
 constexpr int kMaxPlanes = FDTD_CUT_MAX_PLANES;
+constexpr int kMaxPieces = FDTD_CUT_MAX_PIECES;
+constexpr int kMaxColumns = kMaxPieces > kMaxPlanes ? kMaxPieces : kMaxPlanes;
 constexpr int kMaxCut = 16;    // planes cutting one cell, at most
 constexpr int kMaxPoly = 32;   // vertices of a clipped polygon, at most
 
@@ -133,6 +135,12 @@ struct CutArgs {
     const double *offsets;  // planes
     const uint8_t *open;    // planes (null: every plane a wall)
     uint32_t planes;
+    // The walls in pieces (pieces 0: one a plane): piece k on plane piece_plane[k], inside the
+    // half-spaces piece_edges[4 e ..] for e in piece_start[k] .. piece_start[k + 1] - 1.
+    uint32_t pieces;
+    const uint32_t *piece_plane, *piece_start;
+    const double *piece_edges;
+    uint32_t columns;  // caps a cell: pieces, else planes
     double origin[3], cell;
     uint64_t nx, ny, nz;
     // Outputs (capacity cells): each cut cell's index, the volume inside the room (cells^3), the
@@ -195,7 +203,7 @@ __host__ __device__ inline bool cut_cell(const CutArgs &g, uint64_t i, double *v
     // Each wall plane's section inside the other walls (for the volume, by the divergence
     // theorem) and inside the open planes too (the wall's own area in the cell).
     double volume = face_out[1] + face_out[3] + face_out[5], bare = 0.0;
-    for (uint32_t f = 0; f < g.planes; ++f) cap_out[f] = 0.0;
+    for (uint32_t f = 0; f < g.columns; ++f) cap_out[f] = 0.0;
     for (int q = 0; q < cuts; ++q) {
         if (open[q]) continue;
         double p[kMaxPoly][3];
@@ -206,9 +214,28 @@ __host__ __device__ inline bool cut_cell(const CutArgs &g, uint64_t i, double *v
         volume += e[q] * facet;
         for (int r = 0; r < cuts && m > 0; ++r)
             if (open[r]) m = clip3(p, m, g.normals + 3 * cut[r], e[r]);
-        cap_out[cut[q]] = m >= 3 ? area3(p, m) : 0.0;
+        double covered = 0.0;
+        if (!g.pieces) {
+            covered = cap_out[cut[q]] = m >= 3 ? area3(p, m) : 0.0;
+        } else {
+            // each piece of the wall: the wall's part in the cell clipped by the piece's edges
+            for (uint32_t k = 0; k < g.pieces && m >= 3; ++k) {
+                if (g.piece_plane[k] != (uint32_t)cut[q]) continue;
+                double w[kMaxPoly][3];
+                for (int v = 0; v < m; ++v) w[v][0] = p[v][0], w[v][1] = p[v][1], w[v][2] = p[v][2];
+                int wm = m;
+                for (uint32_t h = g.piece_start[k]; h < g.piece_start[k + 1] && wm > 0; ++h) {
+                    const double *edge = g.piece_edges + 4 * h;
+                    const double eh =
+                        (edge[3] - (edge[0] * corner[0] + edge[1] * corner[1] + edge[2] * corner[2])) / g.cell;
+                    wm = clip3(w, wm, edge, eh);
+                }
+                cap_out[k] = wm >= 3 ? area3(w, wm) : 0.0;
+                covered += cap_out[k];
+            }
+        }
         // the part of the facet no wall covers (beyond the open face): the air meets across it
-        bare += facet - cap_out[cut[q]];
+        bare += facet - covered;
     }
     *volume_out = volume / 3.0;
     *bare_out = bare;
@@ -218,7 +245,7 @@ __host__ __device__ inline bool cut_cell(const CutArgs &g, uint64_t i, double *v
 __global__ void __launch_bounds__(kBlockFit) cut_kernel(const CutArgs g) {
     const uint64_t n = g.nx * g.ny * g.nz;
     for (uint64_t i = blockIdx.x * (uint64_t)kBlockFit + threadIdx.x; i < n; i += (uint64_t)gridDim.x * kBlockFit) {
-        double volume, face[6], cap[kMaxPlanes], bare;
+        double volume, face[6], cap[kMaxColumns], bare;
         if (!cut_cell(g, i, &volume, face, cap, &bare)) continue;
         const unsigned long long slot = atomicAdd(g.count, 1ull);
         if (slot >= g.capacity) continue;  // the host sees the count and grows the buffers
@@ -226,7 +253,7 @@ __global__ void __launch_bounds__(kBlockFit) cut_kernel(const CutArgs g) {
         g.volume[slot] = volume;
         g.bare[slot] = bare;
         for (int k = 0; k < 6; ++k) g.face_area[slot * 6 + k] = face[k];
-        for (uint32_t f = 0; f < g.planes; ++f) g.cap[slot * g.planes + f] = cap[f];
+        for (uint32_t f = 0; f < g.columns; ++f) g.cap[slot * g.columns + f] = cap[f];
     }
 }
 
@@ -255,6 +282,24 @@ int fdtd_cut_convex(const fdtd_cut_room *room, int device, fdtd_cut_cells *out) 
         const double l = nf[0] * nf[0] + nf[1] * nf[1] + nf[2] * nf[2];
         if (!(std::abs(l - 1.0) < 1e-9)) return fit_fail(FDTD_EINVAL, "each plane's normal is a unit vector");
     }
+    const uint32_t K = room->pieces;
+    std::vector<uint32_t> piece_start;
+    if (K) {
+        if (K > (uint32_t)kMaxPieces)
+            return fit_fail(FDTD_EINVAL, "the walls have 1 to " + std::to_string(kMaxPieces) + " pieces");
+        if (!room->piece_plane || !room->piece_start || !room->piece_edges)
+            return fit_fail(FDTD_EINVAL, "the walls' pieces miss their planes, starts or edges");
+        if (room->piece_start[0] != 0) return fit_fail(FDTD_EINVAL, "piece_start does not start at 0");
+        for (uint32_t k = 0; k < K; ++k) {
+            if (room->piece_plane[k] >= room->planes) return fit_fail(FDTD_EINVAL, "a piece lies on no plane of the room");
+            if (room->open && room->open[room->piece_plane[k]])
+                return fit_fail(FDTD_EINVAL, "a piece of wall lies on an open plane");
+            if (room->piece_start[k + 1] < room->piece_start[k] || room->piece_start[k + 1] - room->piece_start[k] > 64)
+                return fit_fail(FDTD_EINVAL, "a piece has 0 to 64 edges, in order");
+        }
+        piece_start.assign(room->piece_start, room->piece_start + K + 1);
+    }
+    const uint32_t edges = K ? piece_start[K] : 0;
     int count = 0;
     if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) {
         cudaGetLastError();
@@ -264,7 +309,7 @@ int fdtd_cut_convex(const fdtd_cut_room *room, int device, fdtd_cut_cells *out) 
     cudaGetDevice(&previous);
     cudaSetDevice(device);
     const uint64_t n = room->nx * room->ny * room->nz;
-    const uint32_t P = room->planes;
+    const uint32_t P = room->planes, columns = K ? K : P;
     // Capacity from the planes' area: a cut cell lies within a cell of a plane; start from a
     // generous guess and grow once if it fell short.
     uint64_t capacity = std::min<uint64_t>(n, 1u << 20);
@@ -298,9 +343,24 @@ int fdtd_cut_convex(const fdtd_cut_room *room, int device, fdtd_cut_cells *out) 
     if (room->open)
         for (uint32_t f = 0; f < P; ++f) open[f] = room->open[f] ? 1 : 0;
     cudaMemcpy(d_open, open.data(), P, cudaMemcpyHostToDevice);
+    uint32_t *d_piece_plane = nullptr, *d_piece_start = nullptr;
+    double *d_piece_edges = nullptr;
+    if (K) {
+        if ((rc = check(cudaMalloc(&d_piece_plane, 4 * K), "cudaMalloc"))) return release(), rc;
+        held.push_back(d_piece_plane);
+        if ((rc = check(cudaMalloc(&d_piece_start, 4 * (K + 1)), "cudaMalloc"))) return release(), rc;
+        held.push_back(d_piece_start);
+        if ((rc = check(cudaMalloc(&d_piece_edges, 32 * std::max<uint32_t>(1, edges)), "cudaMalloc"))) return release(), rc;
+        held.push_back(d_piece_edges);
+        cudaMemcpy(d_piece_plane, room->piece_plane, 4 * K, cudaMemcpyHostToDevice);
+        cudaMemcpy(d_piece_start, piece_start.data(), 4 * (K + 1), cudaMemcpyHostToDevice);
+        if (edges) cudaMemcpy(d_piece_edges, room->piece_edges, 32 * edges, cudaMemcpyHostToDevice);
+    }
     for (int attempt = 0; attempt < 2; ++attempt) {
         CutArgs g{};
         g.normals = d_normals, g.offsets = d_offsets, g.open = d_open, g.planes = P;
+        g.pieces = K, g.piece_plane = d_piece_plane, g.piece_start = d_piece_start, g.piece_edges = d_piece_edges;
+        g.columns = columns;
         for (int a = 0; a < 3; ++a) g.origin[a] = room->origin[a];
         g.cell = room->cell, g.nx = room->nx, g.ny = room->ny, g.nz = room->nz;
         g.count = d_count, g.capacity = capacity;
@@ -312,7 +372,7 @@ int fdtd_cut_convex(const fdtd_cut_room *room, int device, fdtd_cut_cells *out) 
         held.push_back(d_volume);
         if ((rc = check(cudaMalloc(&d_face, 48 * capacity), "cudaMalloc"))) return release(), rc;
         held.push_back(d_face);
-        if ((rc = check(cudaMalloc(&d_cap, 8 * P * capacity), "cudaMalloc"))) return release(), rc;
+        if ((rc = check(cudaMalloc(&d_cap, 8 * (uint64_t)columns * capacity), "cudaMalloc"))) return release(), rc;
         held.push_back(d_cap);
         if ((rc = check(cudaMalloc(&d_bare, 8 * capacity), "cudaMalloc"))) return release(), rc;
         held.push_back(d_bare);
@@ -332,11 +392,11 @@ int fdtd_cut_convex(const fdtd_cut_room *room, int device, fdtd_cut_cells *out) 
             continue;
         }
         out->cells = found;
-        out->planes = P;
+        out->planes = columns;
         out->cell = static_cast<uint64_t *>(std::malloc(8 * std::max<uint64_t>(1, found)));
         out->volume = static_cast<double *>(std::malloc(8 * std::max<uint64_t>(1, found)));
         out->face_area = static_cast<double *>(std::malloc(48 * std::max<uint64_t>(1, found)));
-        out->cap = static_cast<double *>(std::malloc(8 * P * std::max<uint64_t>(1, found)));
+        out->cap = static_cast<double *>(std::malloc(8 * (uint64_t)columns * std::max<uint64_t>(1, found)));
         out->bare = static_cast<double *>(std::malloc(8 * std::max<uint64_t>(1, found)));
         if (!out->cell || !out->volume || !out->face_area || !out->cap || !out->bare) {
             fdtd_cut_free(out);
@@ -347,7 +407,7 @@ int fdtd_cut_convex(const fdtd_cut_room *room, int device, fdtd_cut_cells *out) 
         cudaMemcpy(out->volume, d_volume, 8 * found, cudaMemcpyDeviceToHost);
         cudaMemcpy(out->face_area, d_face, 48 * found, cudaMemcpyDeviceToHost);
         cudaMemcpy(out->bare, d_bare, 8 * found, cudaMemcpyDeviceToHost);
-        rc = check(cudaMemcpy(out->cap, d_cap, 8 * P * found, cudaMemcpyDeviceToHost), "cudaMemcpy");
+        rc = check(cudaMemcpy(out->cap, d_cap, 8 * (uint64_t)columns * found, cudaMemcpyDeviceToHost), "cudaMemcpy");
         release();
         if (rc) fdtd_cut_free(out);
         return rc;

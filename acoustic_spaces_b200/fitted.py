@@ -27,7 +27,7 @@ from __future__ import annotations
 
 import ctypes
 import math
-from dataclasses import dataclass
+from dataclasses import dataclass, field
 
 import numpy as np
 
@@ -392,27 +392,148 @@ class Cut:
     bare: np.ndarray
 
 
-def cut_room(room: L.Room, grid: L.Grid) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
-    """The room's planes as the fit takes them: unit normals, offsets, and which are open."""
+@dataclass
+class Walls:
+    """A convex room's walls as the fit takes them: its planes (unit normals out of the room,
+    offsets, and which are open: no wall), the count of materials, and the columns of the cut's
+    wall areas with the material of each (one a plane, the plane's own index; or one a piece of
+    wall, the walls cut into pieces of their own materials as a mesh's triangles carry them), and
+    the walls as triangles (the fit's lattice frame takes their extent). Offsets (and the pieces'
+    edges' offsets) are taken from ``anchor``."""
+
+    normals: np.ndarray
+    offsets: np.ndarray
+    open_: np.ndarray
+    materials: int
+    column_material: np.ndarray
+    vertices: np.ndarray
+    faces: np.ndarray
+    piece_plane: np.ndarray | None = None
+    piece_start: np.ndarray | None = None
+    piece_edges: np.ndarray | None = None
+    # The point the offsets are taken from (planes n . (x - anchor) <= offset).
+    anchor: np.ndarray = field(default_factory=lambda: np.zeros(3))
+
+    @property
+    def open(self) -> bool:
+        return bool(np.any(self.open_))
+
+    @property
+    def wall_planes(self) -> np.ndarray:
+        return np.flatnonzero(self.open_ == 0)
+
+
+def walls_of(room) -> Walls:
+    """The walls of a :class:`layouts.Room` (each plane its own material index), or ``room``
+    itself when it is a :class:`Walls` already."""
+    if isinstance(room, Walls):
+        return room
     normals = np.ascontiguousarray(room.normals, np.float64)
     offsets = np.ascontiguousarray(room.offsets, np.float64)
     open_ = np.array([m is None for m in room.materials], np.uint8)
-    return normals, offsets, open_
+    vertices, faces, _ = L.room_mesh(room)
+    return Walls(normals, offsets, open_, len(room.materials), np.arange(len(offsets), dtype=np.int64),
+                 np.asarray(vertices, np.float64), np.asarray(faces, np.int64))  # fmt: skip
 
 
-def cut_convex(room: L.Room, grid: L.Grid, device: int = 0) -> Cut:
-    """The FP64 cut of ``room``'s walls by ``grid``'s cells on the GPU (fdtd_cut_convex)."""
+def mesh_walls(vertices, faces, materials, count: int, *, tolerance: float = 1e-9, convexity: float = 1e-7) -> Walls:
+    """The walls of a convex room given as a triangle mesh, each triangle with its material (as
+    the reference's WaveSolver and CutFit take a room, native_module.cpp:1465-1559): the planes of
+    its triangles (coplanar ones merged), each triangle a piece of wall on its plane bounded by
+    its three edges, and the faces of the vertices' convex hull on which no triangle lies left
+    open. Triangles within ``tolerance`` (of the room's size) of one plane share it; a face folded
+    by less than ``convexity`` (a vertex that far outside a triangle's plane) is taken as the two
+    planes of its triangles. The planes are taken relative to the first vertex (``anchor``), so
+    that a room far from the origin keeps its digits. Raises ValueError where vertices lie farther
+    on both sides of a triangle's plane (the room is not convex)."""
+    from scipy.spatial import ConvexHull
+
+    v = np.asarray(vertices, np.float64)
+    f = np.asarray(faces, np.int64)
+    mat = np.asarray(materials, np.int64)
+    anchor = v[0].copy()
+    w = v - anchor  # (exact where the coordinates are alike, as a room's are)
+    size = max(float(np.abs(w).max()), 1e-300)
+    # (a room far from the origin has its vertices rounded to the doubles there: its faces are
+    # planar to a few of their steps only)
+    rounding = 8.0 * float(np.spacing(np.abs(v).max())) / size
+    tolerance, convexity = max(tolerance, rounding), max(convexity, rounding)
+    planes: list[tuple[np.ndarray, float]] = []
+
+    def plane_of(n, d, tol):
+        for k, (m, e) in enumerate(planes):
+            if np.abs(n - m).max() < tol and abs(d - e) < tol * size:
+                return k
+        return -1
+
+    piece_plane, piece_start, edges = [], [0], []
+    for tri in f:
+        a, b, c = w[tri]
+        n = np.cross(b - a, c - a)
+        if np.linalg.norm(n) == 0.0:
+            raise ValueError("a triangle of the room has no area")
+        n /= np.linalg.norm(n)
+        d = float(n @ a)
+        side = w @ n - d
+        if side.max() > convexity * size:  # (the triangle faces into the room: turn it out)
+            if side.min() < -convexity * size:
+                raise ValueError("vertices lie on both sides of a triangle's plane: the room is not convex")
+            n, d = -n, -d
+        k = plane_of(n, d, tolerance)
+        if k < 0:
+            planes.append((n, d))
+            k = len(planes) - 1
+        m = planes[k][0]
+        for p, q, r in ((a, b, c), (b, c, a), (c, a, b)):
+            h = np.cross(q - p, m)
+            h /= np.linalg.norm(h)
+            if h @ (r - p) > 0.0:
+                h = -h
+            edges.append((*h, float(h @ p)))
+        piece_plane.append(k)
+        piece_start.append(len(edges))
+    walls = len(planes)
+    # the hull's faces that no triangle covers: open (no wall, the air goes through)
+    for eq in ConvexHull(w).equations:  # n . x + c <= 0 inside
+        norm = np.linalg.norm(eq[:3])
+        n, d = eq[:3] / norm, float(-eq[3] / norm)
+        if plane_of(n, d, 1e-6) < 0:
+            planes.append((n, d))
+    normals = np.array([n for n, _ in planes], np.float64)
+    offsets = np.array([d for _, d in planes], np.float64)
+    open_ = np.r_[np.zeros(walls, np.uint8), np.ones(len(planes) - walls, np.uint8)]
+    # piece edges relative to the anchor too (their offsets were taken in its frame)
+    return Walls(normals, offsets, open_, int(count), mat.copy(), v, f,
+                 np.array(piece_plane, np.uint32), np.array(piece_start, np.uint32),
+                 np.ascontiguousarray(np.array(edges, np.float64).reshape(-1)), anchor)  # fmt: skip
+
+
+def cut_room(room, grid: L.Grid) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+    """The room's planes as the fit takes them: unit normals, offsets, and which are open."""
+    w = walls_of(room)
+    return w.normals, w.offsets, w.open_
+
+
+def cut_convex(room, grid: L.Grid, device: int = 0) -> Cut:
+    """The FP64 cut of ``room``'s walls (a :class:`layouts.Room` or :class:`Walls`) by ``grid``'s
+    cells on the GPU (fdtd_cut_convex)."""
     from . import _abi
 
     lib = _abi.load_library()
-    normals, offsets, open_ = cut_room(room, grid)
+    w = walls_of(room)
+    normals, offsets, open_ = w.normals, w.offsets, w.open_
     r = _abi.FdtdCutRoom()
     r.normals = normals.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
     r.offsets = offsets.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
     r.open = open_.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))
     r.planes = len(offsets)
+    if w.piece_plane is not None:
+        r.pieces = len(w.piece_plane)
+        r.piece_plane = w.piece_plane.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32))
+        r.piece_start = w.piece_start.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32))
+        r.piece_edges = w.piece_edges.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
     for a in range(3):
-        r.origin[a] = float(grid.origin[a])
+        r.origin[a] = float(grid.origin[a] - w.anchor[a])
     r.cell = float(grid.cell)
     r.nx, r.ny, r.nz = (int(v) for v in grid.shape)
     out = _abi.FdtdCutCells()
@@ -465,14 +586,15 @@ def _direction(grid: L.Grid, a: np.ndarray, b: np.ndarray) -> np.ndarray:
     return np.where(near, _DIRECTION[key], -1)
 
 
-def lattice_widths(room: L.Room, grid: L.Grid) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+def lattice_widths(room, grid: L.Grid) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
     """Each cell's width per axis (cells) as the reference's fit measures it on its lattice
     (cut_cells.hpp:2031-2122): the frame E is the largest half-extent of the room's triangles that
     reach the grid's box grown by 2h and of the grid's box, grown by 2h; p = the exponent of E plus
     one, s = 61 - p; the middle X0 per axis rounded to a multiple of 2^(p - 2); a face's double x
     becomes round(x 2^s) - X0 2^s (ties to even); a cell's width is the difference of its faces'
     quanta over h 2^s. Uncut cells hold these widths' product of air (1 within about 1e-15)."""
-    vertices, faces, _ = L.room_mesh(room)
+    w = walls_of(room)
+    vertices, faces = w.vertices, w.faces
     h = float(grid.cell)
     face_at = [grid.origin[a] + np.arange(grid.shape[a] + 1, dtype=np.float64) * h for a in range(3)]
     glo = [float(face_at[a][0]) - 2.0 * h for a in range(3)]
@@ -511,7 +633,7 @@ def lattice_widths(room: L.Room, grid: L.Grid) -> tuple[np.ndarray, np.ndarray, 
     return tuple(widths)
 
 
-def fit_from_cut(cut: Cut, room: L.Room, grid: L.Grid, *, layer: int = 0) -> Fit:
+def fit_from_cut(cut: Cut, room, grid: L.Grid, *, layer: int = 0) -> Fit:
     """The rows of a convex room from its cut (:func:`cut_convex`), by the reference's rules for
     what a row owns and sums (cut_cells.hpp: the owner rule, sum_up): each cut cell holds up to
     two regions, its air inside the walls' planes and outside them; a region holding an air cell's
@@ -529,15 +651,18 @@ def fit_from_cut(cut: Cut, room: L.Room, grid: L.Grid, *, layer: int = 0) -> Fit
     ax_depth = [np.minimum(np.arange(m), m - 1 - np.arange(m)).astype(np.int32) for m in (nx, ny, nz)]
     depth = np.minimum(np.minimum(ax_depth[2][:, None, None], ax_depth[1][None, :, None]),
                        ax_depth[0][None, None, :]).reshape(-1)  # fmt: skip
-    normals, offsets, open_ = cut_room(room, grid)
-    walls = np.flatnonzero(open_ == 0)
+    room = walls_of(room)
+    normals, offsets = room.normals, room.offsets
+    walls = room.wall_planes
+    # The cut's columns of wall area, each with its material's column of the rows' sums.
+    columns = [(c, int(m)) for c, m in enumerate(room.column_material) if m >= 0 and c < cut.cap.shape[1]]
     # The air: with an open face every cell but the grid's edge; closed, the cells whose centre
     # lies inside the walls. Cells within `layer` of the edge form the matched layer.
     if room.open:
         air_mask = ~edge
     else:
         inside = np.ones((nz, ny, nx), bool)
-        cz, cy, cx_ = (grid.centres(a) for a in (2, 1, 0))
+        cz, cy, cx_ = (grid.centres(a) - room.anchor[a] for a in (2, 1, 0))
         for f in walls:
             nf = normals[f]
             inside &= (nf[0] * cx_[None, None, :] + nf[1] * cy[None, :, None] + nf[2] * cz[:, None, None]) - offsets[f] < 0.0
@@ -547,7 +672,7 @@ def fit_from_cut(cut: Cut, room: L.Room, grid: L.Grid, *, layer: int = 0) -> Fit
         air[air_mask & (depth <= layer)] = LAYER
 
     # The cut cells: those a wall reaches with positive area.
-    is_cut = np.any(cut.cap[:, walls] > TINY, axis=1) if len(walls) else np.zeros(len(cut.cell), bool)
+    is_cut = np.any(cut.cap > TINY, axis=1) if len(walls) else np.zeros(len(cut.cell), bool)
     cc = cut.cell[is_cut]
     C = len(cc)
     wx, wy, wz = lattice_widths(room, grid)
@@ -574,6 +699,7 @@ def fit_from_cut(cut: Cut, room: L.Room, grid: L.Grid, *, layer: int = 0) -> Fit
     # Which side holds each cut cell's centre: inside every wall plane that cuts it (a joined
     # cell's one region holds it).
     cx = np.stack([grid.centres(0)[cc % nx], grid.centres(1)[(cc // nx) % ny], grid.centres(2)[cc // sz]], axis=1)
+    cx = cx - room.anchor
     centre_in = np.all(cx @ normals[walls].T - offsets[walls] < 0.0, axis=1) | joined
 
     # Regions: 2c the inside of cut cell c, 2c + 1 its outside; whole cells after them.
@@ -665,7 +791,7 @@ def fit_from_cut(cut: Cut, room: L.Room, grid: L.Grid, *, layer: int = 0) -> Fit
     row_index = np.full(n, -1, np.int64)
     row_index[rows] = np.arange(len(rows))
     R = len(rows)
-    M = len(room.materials)
+    M = room.materials
     air_volume = np.zeros(R)
     open_area = np.zeros((R, 18))
     wall_area = np.zeros((R, M + 1))
@@ -679,8 +805,8 @@ def fit_from_cut(cut: Cut, room: L.Room, grid: L.Grid, *, layer: int = 0) -> Fit
     # walls: both sides of a wall see it (a cut cell's inside and outside regions)
     cut_g = gr[gr < 2 * C]
     both_sides = np.where(joined[cut_g // 2], 2.0, 1.0)  # a joined region sees each wall's two sides
-    for f in walls:
-        _accumulate(wall_area, row_index[owner[cut_g]] * (M + 1) + f, both_sides * caps[cut_g // 2, f])
+    for col, mat in columns:
+        _accumulate(wall_area, row_index[owner[cut_g]] * (M + 1) + mat, both_sides * caps[cut_g // 2, col])
     k = _direction(grid, owner[gr], reg_cell[gr])
     ax = (k >= 0) & (k < 6)
     _accumulate(sliver, ro[ax] * 6 + k[ax], reg_volume[gr][ax])
@@ -779,11 +905,11 @@ def fit_from_cut(cut: Cut, room: L.Room, grid: L.Grid, *, layer: int = 0) -> Fit
             ro_, rn_ = row_index[o_[moving]], row_index[across[moving]]
             gl = lg[moving] // 2
             sides = np.where(joined[gl], 2.0, 1.0)
-            for wf in walls:
-                a_ = sides * caps[gl, wf]
+            for col, mat in columns:
+                a_ = sides * caps[gl, col]
                 has = a_ > 0.0
-                np.subtract.at(wall_area[:, wf], ro_[has], share[moving][has] * a_[has])
-                np.add.at(wall_area[:, wf], rn_[has], share[moving][has] * a_[has])
+                np.subtract.at(wall_area[:, mat], ro_[has], share[moving][has] * a_[has])
+                np.add.at(wall_area[:, mat], rn_[has], share[moving][has] * a_[has])
     return Fit(rows.astype(np.int64), air_volume, open_area, wall_area, sliver, air, (wx, wy, wz))
 
 
@@ -820,8 +946,9 @@ def fitted_cubic(grid: L.Grid, point) -> list[tuple[int, float]]:
     return out
 
 
-def convex_fit(room: L.Room, grid: L.Grid, *, layer: int = 0, device: int = 0) -> Fit:
-    """This library's fit of a convex room: the cut on the GPU, then the rows on the host."""
+def convex_fit(room, grid: L.Grid, *, layer: int = 0, device: int = 0) -> Fit:
+    """This library's fit of a convex room (a :class:`layouts.Room` or :class:`Walls`): the cut
+    on the GPU, then the rows on the host."""
     return fit_from_cut(cut_convex(room, grid, device), room, grid, layer=layer)
 
 

@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define FDTD_B200_ABI_VERSION 2
+#define FDTD_B200_ABI_VERSION 3
 
 /* Status codes. */
 #define FDTD_OK 0
@@ -400,8 +400,9 @@ int fdtd_device_count(void);
 
 /* ---- fitted walls: the cut of a convex room by the grid (set-up, not stepping) ---- */
 
-/* Planes of a convex room, at most. */
+/* Planes of a convex room, and pieces of its walls, at most. */
 #define FDTD_CUT_MAX_PLANES 64
+#define FDTD_CUT_MAX_PIECES 256
 
 /* A convex room P = {x : normals[f] . x <= offsets[f] for every plane f} (unit normals, pointing
  * out of the room; metres), on a grid of nx x ny x nz cells of `cell` metres whose first cell's
@@ -415,13 +416,23 @@ typedef struct fdtd_cut_room {
     double origin[3];
     double cell;
     uint64_t nx, ny, nz;
+    /* Optional (pieces 0: each wall one piece, its plane's): the walls cut into pieces, as the
+     * triangles of a mesh carry materials of their own. Piece k lies on the wall plane
+     * piece_plane[k] and is the part of it inside the half-spaces piece_edges[4 e .. 4 e + 3]
+     * (normal, offset: n . x <= d) for e in piece_start[k] .. piece_start[k + 1] - 1; the pieces
+     * of a plane cover its wall face without overlapping. */
+    uint32_t pieces;
+    const uint32_t *piece_plane;  /* pieces */
+    const uint32_t *piece_start;  /* pieces + 1 */
+    const double *piece_edges;    /* 4 per edge */
 } fdtd_cut_room;
 
 /* The cells the walls' planes cut, in no particular order (the library allocates the arrays;
  * fdtd_cut_free releases them): each cell's index (x fastest); the volume of its air inside every
  * wall's plane (in cells^3; the rest of the cell is its air outside them), the area of each of its
  * faces (-x, +x, -y, +y, -z, +z; in cell faces, 6 a cell) on that inner side, each wall's area
- * in the cell (`planes` a cell; 0 for an open plane), and the area of the walls' planes between
+ * in the cell (`planes` values a cell: one a plane, 0 for an open plane; or, for a room given in
+ * pieces, one a piece, `planes` then the count of pieces), and the area of the walls' planes between
  * the inner and the outer air that no wall covers (beyond a face left open: the two sides of the
  * cell's air meet there). */
 typedef struct fdtd_cut_cells {

@@ -29,7 +29,7 @@ def test_the_library_exports_every_declared_function(name):
 
 
 def test_the_abi_version():
-    assert _abi.load_library().fdtd_abi_version() == 2
+    assert _abi.load_library().fdtd_abi_version() == 3
 
 
 def _create(layout, precision=_abi.FDTD_FP32):
