@@ -121,6 +121,8 @@ class FdtdTiles(ctypes.Structure):
         ("tiles", ctypes.c_uint32),
         ("blocks_per_sm", ctypes.c_int32),
         ("concurrent", ctypes.c_int32),
+        ("threads", ctypes.c_int32),
+        ("cols", ctypes.c_int32),
     ]
 
 

@@ -101,7 +101,7 @@ struct fdtd_solver {
     int concurrent = 1;
     uint32_t bulk_tiles = 0;
     int bulk_per_sm = 0;      // resident bulk blocks per multiprocessor (shape 0)
-    int shape_per_sm[kShapes] = {0, 0, 0, 0};  // the same, each shape
+    int shape_per_sm[kShapes] = {};  // the same, each shape
     // The sweep's tile shape (an index of kShapeInfo) and planes a tile, chosen by fdtd_autotune
     // or fdtd_set_tiles; the pitched cell types kept on the host to lay the tiles out again; the
     // forward list's device copy (replaced with the shape), and the adjoint's list (shape 0, no
@@ -578,7 +578,7 @@ template <typename T, bool WIDE, bool SCALED, bool COMP, class SH>
 int set_up_shape(fdtd_solver *s, int *per_sm) {
     CUDA_TRY(s, cudaFuncSetAttribute(bulk_kernel<T, WIDE, SCALED, COMP, SH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)Stage<T, SCALED, SH>::smem));
-    CUDA_TRY(s, cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, bulk_kernel<T, WIDE, SCALED, COMP, SH>, kBlock,
+    CUDA_TRY(s, cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, bulk_kernel<T, WIDE, SCALED, COMP, SH>, SH::THREADS,
                                                               Stage<T, SCALED, SH>::smem));
     return FDTD_OK;
 }
@@ -591,6 +591,12 @@ int set_up_kernels(fdtd_solver *s) {
     if ((rc = set_up_shape<T, WIDE, SCALED, COMP, Shape1>(s, &s->shape_per_sm[1]))) return rc;
     if ((rc = set_up_shape<T, WIDE, SCALED, COMP, Shape2>(s, &s->shape_per_sm[2]))) return rc;
     if ((rc = set_up_shape<T, WIDE, SCALED, COMP, Shape3>(s, &s->shape_per_sm[3]))) return rc;
+    if ((rc = set_up_shape<T, WIDE, SCALED, COMP, Shape4>(s, &s->shape_per_sm[4]))) return rc;
+    if ((rc = set_up_shape<T, WIDE, SCALED, COMP, Shape5>(s, &s->shape_per_sm[5]))) return rc;
+    if ((rc = set_up_shape<T, WIDE, SCALED, COMP, Shape6>(s, &s->shape_per_sm[6]))) return rc;
+    if ((rc = set_up_shape<T, WIDE, SCALED, COMP, Shape7>(s, &s->shape_per_sm[7]))) return rc;
+    if ((rc = set_up_shape<T, WIDE, SCALED, COMP, Shape8>(s, &s->shape_per_sm[8]))) return rc;
+    if ((rc = set_up_shape<T, WIDE, SCALED, COMP, Shape9>(s, &s->shape_per_sm[9]))) return rc;
     s->bulk_per_sm = s->shape_per_sm[0];
     return FDTD_OK;
 }
@@ -599,12 +605,18 @@ int set_up_kernels(fdtd_solver *s) {
 template <typename T, bool WIDE, bool SCALED, bool COMP>
 void launch_bulk(const fdtd_solver *s, const CUtensorMap &mb, const CUtensorMap &ma, const BulkArgs &args) {
 #define FDTD_BULK(SH)                                                                          \
-    bulk_kernel<T, WIDE, SCALED, COMP, SH><<<s->bulk_blocks, kBlock, Stage<T, SCALED, SH>::smem, s->stream>>>( \
+    bulk_kernel<T, WIDE, SCALED, COMP, SH><<<s->bulk_blocks, SH::THREADS, Stage<T, SCALED, SH>::smem, s->stream>>>( \
         mb, ma, s->map_t, s->map_s, args)
     switch (s->bulk_shape) {
         case 1: FDTD_BULK(Shape1); break;
         case 2: FDTD_BULK(Shape2); break;
         case 3: FDTD_BULK(Shape3); break;
+        case 4: FDTD_BULK(Shape4); break;
+        case 5: FDTD_BULK(Shape5); break;
+        case 6: FDTD_BULK(Shape6); break;
+        case 7: FDTD_BULK(Shape7); break;
+        case 8: FDTD_BULK(Shape8); break;
+        case 9: FDTD_BULK(Shape9); break;
         default: FDTD_BULK(Shape0); break;
     }
 #undef FDTD_BULK
@@ -2408,7 +2420,8 @@ int fdtd_set_launch(fdtd_solver *s, int layer_per_sm, int special_per_sm) {
 
 int fdtd_set_tiles(fdtd_solver *s, int shape, uint64_t planes) {
     if (!s) return set_global(FDTD_EINVAL, "no solver");
-    if (shape < 0 || shape >= kShapes) return fail(s, FDTD_EINVAL, "the tile shape is an index 0 to 3");
+    if (shape < 0 || shape >= kShapes)
+        return fail(s, FDTD_EINVAL, "the tile shape is an index 0 to " + std::to_string(kShapes - 1));
     if (planes < 1 || planes > 1024) return fail(s, FDTD_EINVAL, "planes a tile are 1 to 1024");
     if (!s->bulk_tiles) return FDTD_OK;  // no interior cells: no sweep
     if (s->shape_per_sm[shape] < 1) return fail(s, FDTD_EINVAL, "the tile shape does not fit a multiprocessor here");
@@ -2428,6 +2441,8 @@ int fdtd_get_tiles(const fdtd_solver *s, fdtd_tiles *out) {
     out->tiles = s->bulk_tiles;
     out->blocks_per_sm = s->shape_per_sm[s->bulk_shape];
     out->concurrent = s->concurrent;
+    out->threads = kShapeInfo[s->bulk_shape].threads;
+    out->cols = kShapeInfo[s->bulk_shape].cols;
     return FDTD_OK;
 }
 
@@ -2481,44 +2496,53 @@ int fdtd_autotune(fdtd_solver *s, uint64_t trial_steps, int *layer_per_sm, int *
         CUDA_TRY(s, cudaEventElapsedTime(&ms, start, end));
         return FDTD_OK;
     };
-    // First the sweep's tile shape and planes a tile (the default chunk, half and twice it, within
-    // 8 to 64), with the layer and special launches as they are; then those given the best tiles.
-    if (s->bulk_tiles) {
+    // The sweep's tile shape and planes a tile (the default chunk, a quarter, half and twice it,
+    // within 8 to 64) with the layer and special launches as they are; then those launches (the
+    // streams beside one another or in turn, the layer's and the special rows' blocks an SM) given
+    // the tiles; then the tiles once more given the launches, as the kernels share the SMs.
+    auto tune_tiles = [&]() -> int {
+        if (!s->bulk_tiles) return FDTD_OK;
         const uint64_t base = default_chunk(s);
         float best_tiles = -1.0f;
-        int best_shape = s->bulk_shape;
+        int best_shape = s->bulk_shape, r = FDTD_OK;
         uint64_t best_chunk = s->bulk_chunk;
-        for (int shape = 0; shape < kShapes && rc == FDTD_OK; ++shape) {
+        for (int shape = 0; shape < kShapes && r == FDTD_OK; ++shape) {
             if (s->shape_per_sm[shape] < 1) continue;  // does not fit an SM in this precision
             for (uint64_t chunk : {base / 4, base / 2, base, base * 2}) {
                 if (chunk < 8 || chunk > 64) continue;
-                if ((rc = use_shape(s, shape, chunk)) != FDTD_OK) break;
+                if ((r = use_shape(s, shape, chunk)) != FDTD_OK) break;
                 float ms;
-                if ((rc = trial(ms)) != FDTD_OK) break;
+                if ((r = trial(ms)) != FDTD_OK) break;
                 if (best_tiles < 0.0f || ms < best_tiles) best_tiles = ms, best_shape = shape, best_chunk = chunk;
             }
         }
-        if (rc == FDTD_OK) rc = use_shape(s, best_shape, best_chunk);
-    }
+        return r == FDTD_OK ? use_shape(s, best_shape, best_chunk) : r;
+    };
     const int layers[] = {4, 8, 12, 16, 0}, specials[] = {2, 4, 8, 0};
-    float best = -1.0f;
     int best_layer = s->layer_per_sm, best_special = s->special_per_sm, best_concurrent = s->concurrent;
-    for (int c : {1, 0}) {
-        s->concurrent = c;
-        for (int l : layers) {
-            if (rc != FDTD_OK) break;
-            if (!s->layers && l != layers[0]) continue;
-            for (int k : specials) {
-                if (!s->specials && k != specials[0]) continue;
-                s->layer_per_sm = l, s->special_per_sm = k;
-                float ms;
-                if ((rc = trial(ms)) != FDTD_OK) break;
-                if (best < 0.0f || ms < best) best = ms, best_layer = l, best_special = k, best_concurrent = c;
+    auto tune_launch = [&]() -> int {
+        float best = -1.0f;
+        int r = FDTD_OK;
+        for (int c : {1, 0}) {
+            s->concurrent = c;
+            for (int l : layers) {
+                if (r != FDTD_OK) break;
+                if (!s->layers && l != layers[0]) continue;
+                for (int k : specials) {
+                    if (!s->specials && k != specials[0]) continue;
+                    s->layer_per_sm = l, s->special_per_sm = k;
+                    float ms;
+                    if ((r = trial(ms)) != FDTD_OK) break;
+                    if (best < 0.0f || ms < best) best = ms, best_layer = l, best_special = k, best_concurrent = c;
+                }
             }
-            if (rc != FDTD_OK) break;
         }
-    }
-    s->concurrent = best_concurrent;
+        s->concurrent = best_concurrent, s->layer_per_sm = best_layer, s->special_per_sm = best_special;
+        return r;
+    };
+    if (rc == FDTD_OK) rc = tune_tiles();
+    if (rc == FDTD_OK) rc = tune_launch();
+    if (rc == FDTD_OK) rc = tune_tiles();
     s->timing = timing;
     cudaEventDestroy(start);
     cudaEventDestroy(end);

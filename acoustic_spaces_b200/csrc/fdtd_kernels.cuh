@@ -41,36 +41,65 @@ constexpr int kLayerPerSm = 8;                  // blocks an SM of the matched-l
 constexpr int kSpecialPerSm = 4;                // blocks an SM of the special rows' kernel
 
 // A tile shape of the bulk sweep: TX x TY cells a plane, a ring of STAGES plane stages (the three
-// in use and STAGES - 3 loaded ahead). Each of the block's threads updates ROWS rows of one column.
-template <int TX_, int TY_, int STAGES_>
+// in use and STAGES - 3 loaded ahead), THREADS threads a block. Each thread updates ROWS rows of
+// one column.
+template <int TX_, int TY_, int STAGES_, int THREADS_ = kBlock, int COLS_ = 1>
 struct Shape {
-    static constexpr int TX = TX_, TY = TY_, STAGES = STAGES_;
+    static constexpr int TX = TX_, TY = TY_, STAGES = STAGES_, THREADS = THREADS_;
+    static constexpr int COLS = COLS_;       // adjacent columns a thread (2: pairs of cells, vector loads)
+    static constexpr int XT = TX / COLS;     // threads across a row
     static constexpr int BX = TX + 2 * kHX;  // pressure tile width (x halo each side)
     static constexpr int BY = TY + 2;        // pressure tile rows (one halo row each side)
-    static constexpr int ROWS = TX * TY / kBlock;
+    static constexpr int ROWS = TX * TY / (THREADS * COLS);
     static constexpr int AHEAD = STAGES - 3;
-    static_assert(TX % 16 == 0 && kBlock % TX == 0 && (TX * TY) % kBlock == 0 && STAGES >= 4, "tile shape");
+    static_assert(TX % 16 == 0 && (COLS == 1 || COLS == 2) && THREADS % XT == 0 && THREADS % 32 == 0 &&
+                      (TX * TY) % (THREADS * COLS) == 0 && STAGES >= 4,
+                  "tile shape");
 };
 
 // The shapes the library is built with (fdtd_autotune picks one per grid; shape 0 by default):
 // 64 x 16 with 5 stages (4 blocks of 52 KB an SM in FP32), 128 x 16 and 64 x 32 with 4 stages (2
-// blocks of 80 KB: fewer halo cells a cell, 1.19x against 1.27x), and 32 x 32 with 5 (4 blocks).
+// blocks of 80 KB: fewer halo cells a cell, 1.19x against 1.27x), and 32 x 32 with 5 (4 blocks);
+// then the first three again with 256 threads a block (4 rows a thread, or 8), twice the warps an
+// SM in the same shared memory, for a sweep whose issue waits on its own latencies.
 using Shape0 = Shape<64, 16, 5>;
 using Shape1 = Shape<128, 16, 4>;
 using Shape2 = Shape<64, 32, 4>;
 using Shape3 = Shape<32, 32, 5>;
-constexpr int kShapes = 4;
+using Shape4 = Shape<64, 16, 5, 256>;
+using Shape5 = Shape<128, 16, 4, 256>;
+using Shape6 = Shape<64, 32, 4, 256>;
+// Pairs of cells a thread (the 7-point stencil's loads and stores two cells wide): 64 x 16 with 128
+// threads, 128 x 16 with 256, 64 x 16 with 256.
+using Shape7 = Shape<64, 16, 5, 128, 2>;
+using Shape8 = Shape<128, 16, 4, 256, 2>;
+using Shape9 = Shape<64, 16, 5, 256, 2>;
+constexpr int kShapes = 10;
 struct ShapeInfo {
-    int tx, ty, stages;
+    int tx, ty, stages, threads, cols;
 };
-constexpr ShapeInfo kShapeInfo[kShapes] = {{Shape0::TX, Shape0::TY, Shape0::STAGES},
-                                           {Shape1::TX, Shape1::TY, Shape1::STAGES},
-                                           {Shape2::TX, Shape2::TY, Shape2::STAGES},
-                                           {Shape3::TX, Shape3::TY, Shape3::STAGES}};
+#define FDTD_SHAPE_INFO(SH) {SH::TX, SH::TY, SH::STAGES, SH::THREADS, SH::COLS}
+constexpr ShapeInfo kShapeInfo[kShapes] = {FDTD_SHAPE_INFO(Shape0), FDTD_SHAPE_INFO(Shape1), FDTD_SHAPE_INFO(Shape2),
+                                           FDTD_SHAPE_INFO(Shape3), FDTD_SHAPE_INFO(Shape4), FDTD_SHAPE_INFO(Shape5),
+                                           FDTD_SHAPE_INFO(Shape6), FDTD_SHAPE_INFO(Shape7), FDTD_SHAPE_INFO(Shape8),
+                                           FDTD_SHAPE_INFO(Shape9)};
+#undef FDTD_SHAPE_INFO
 // The default shape's sizes (the adjoint's sweep keeps them).
 constexpr int kTX = Shape0::TX, kTY = Shape0::TY, kBX = Shape0::BX, kBY = Shape0::BY;
 
 constexpr uint32_t align128(uint32_t v) { return (v + 127u) & ~127u; }
+
+// Two adjacent values of T as one vector (8 bytes of float, 16 of double).
+template <typename T>
+struct Pair;
+template <>
+struct Pair<float> {
+    using type = float2;
+};
+template <>
+struct Pair<double> {
+    using type = double2;
+};
 
 // One stage of the ring: plane k's pressure tile with halos, and its previous pressure, cell
 // types and (with a speed field) scales over the tile's own cells.
@@ -208,7 +237,7 @@ __device__ __forceinline__ TileSpan tile_span(const BulkArgs &p, uint32_t tile) 
 }
 
 template <typename T, bool WIDE, bool SCALED, bool COMP = false, class SH = Shape0>
-__global__ void __launch_bounds__(kBlock) bulk_kernel(const __grid_constant__ CUtensorMap map_b,
+__global__ void __launch_bounds__(SH::THREADS) bulk_kernel(const __grid_constant__ CUtensorMap map_b,
                                                       const __grid_constant__ CUtensorMap map_a,
                                                       const __grid_constant__ CUtensorMap map_t,
                                                       const __grid_constant__ CUtensorMap map_s,
@@ -234,8 +263,8 @@ __global__ void __launch_bounds__(kBlock) bulk_kernel(const __grid_constant__ CU
     int p_k = p_span.z0 - 1;
     int issued = 0;
     const T axial = (T)p.axial, centre = (T)p.centre, diagonal = (T)p.diagonal, total = (T)p.total;
-    const int xl = threadIdx.x % TX;
-    const int r0 = (threadIdx.x / TX) * SH::ROWS;
+    const int xl = (threadIdx.x % SH::XT) * SH::COLS;
+    const int r0 = (threadIdx.x / SH::XT) * SH::ROWS;
     T *__restrict__ a = static_cast<T *>(p.a);
     T *__restrict__ dd = static_cast<T *>(p.d);
     const T residual = (T)p.residual;
@@ -285,60 +314,106 @@ __global__ void __launch_bounds__(kBlock) bulk_kernel(const __grid_constant__ CU
                 const T *pa = reinterpret_cast<const T *>(s0 + S::a_off);
                 const uint8_t *pt = reinterpret_cast<const uint8_t *>(s0 + S::t_off);
                 const float *ps = reinterpret_cast<const float *>(s0 + S::s_off);
+                // (the thread's first row in the level; row r lies r pitches on)
+                const uint64_t row0 = (uint64_t)x + (uint64_t)(t.yt + r0) * p.pitch + (uint64_t)z * plane;
 #pragma unroll
                 for (int r = 0; r < SH::ROWS; ++r) {
                     const int yl = r0 + r;
-                    const int c = yl * TX + xl;
-                    // Outside the interior cells' box, and outside the grid (zero fill), no cell
-                    // is interior.
-                    if (!t.full && pt[c] != kInterior) continue;
-                    const int q = (yl + 1) * BX + (xl + kHX);
-                    const T here = b0[q];
-                    const uint64_t at = (uint64_t)x + (uint64_t)(t.yt + yl) * p.pitch + (uint64_t)z * plane;
-                    if (COMP) {
-                        // pa holds the increment; the neighbours as differences, in the sum's order.
-                        const T sum = (b0[q - 1] - here) + (b0[q + 1] - here) + (b0[q - BX] - here) +
-                                      (b0[q + BX] - here) + (bm[q] - here) + (bp[q] - here);
-                        T edges = (T)0;
-                        if (WIDE)
-                            edges = (b0[q - 1 - BX] - here) + (b0[q + 1 - BX] - here) + (b0[q - 1 + BX] - here) +
-                                    (b0[q + 1 + BX] - here) + (bm[q - 1] - here) + (bm[q + 1] - here) +
-                                    (bp[q - 1] - here) + (bp[q + 1] - here) + (bm[q - BX] - here) +
-                                    (bm[q + BX] - here) + (bp[q - BX] - here) + (bp[q + BX] - here);
-                        T step;
+                    if constexpr (SH::COLS == 2 && !WIDE && !COMP) {
+                        // Two cells side by side: the pair's pressures, previous pressures, scales
+                        // and neighbours above, below, z-1 and z+1 each as one vector load (even
+                        // offsets: the tile's x start, the halo and the pitch are even), and the
+                        // pair's new pressures as one vector store where both are interior.
+                        using V2 = typename Pair<T>::type;
+                        const int c = yl * TX + xl;
+                        const bool in0 = t.full || pt[c] == kInterior, in1 = t.full || pt[c + 1] == kInterior;
+                        if (!in0 && !in1) continue;
+                        const int q = (yl + 1) * BX + (xl + kHX);
+                        const V2 h = *reinterpret_cast<const V2 *>(b0 + q);
+                        const T left = b0[q - 1], right = b0[q + 2];
+                        const V2 up = *reinterpret_cast<const V2 *>(b0 + q - BX);
+                        const V2 dn = *reinterpret_cast<const V2 *>(b0 + q + BX);
+                        const V2 zm = *reinterpret_cast<const V2 *>(bm + q);
+                        const V2 zp = *reinterpret_cast<const V2 *>(bp + q);
+                        const V2 pv = *reinterpret_cast<const V2 *>(pa + c);
+                        const T sum0 = left + h.y + up.x + dn.x + zm.x + zp.x;
+                        const T sum1 = h.x + right + up.y + dn.y + zm.y + zp.y;
+                        T n0, n1;
                         if (SCALED) {
-                            const T sc = (T)ps[c];
-                            step = WIDE ? pa[c] + (sc * axial) * sum + (sc * diagonal) * edges + (sc * residual) * here
-                                        : pa[c] + (sc * axial) * sum + (sc * residual) * here;
+                            const float2 sv = *reinterpret_cast<const float2 *>(ps + c);
+                            const T s0 = (T)sv.x, s1 = (T)sv.y;
+                            n0 = ((T)2 - total * s0) * h.x + (s0 * axial) * sum0 - pv.x;
+                            n1 = ((T)2 - total * s1) * h.y + (s1 * axial) * sum1 - pv.y;
                         } else {
-                            step = WIDE ? pa[c] + axial * sum + diagonal * edges + residual * here
-                                        : pa[c] + axial * sum + residual * here;
+                            n0 = centre * h.x + axial * sum0 - pv.x;
+                            n1 = centre * h.y + axial * sum1 - pv.y;
                         }
-                        a[at] = here + step;
-                        dd[at] = step;
-                        continue;
-                    }
-                    const T sum = b0[q - 1] + b0[q + 1] + b0[q - BX] + b0[q + BX] + bm[q] + bp[q];
-                    T next;
-                    if (WIDE) {
-                        const T edges = b0[q - 1 - BX] + b0[q + 1 - BX] + b0[q - 1 + BX] + b0[q + 1 + BX] +
-                                        bm[q - 1] + bm[q + 1] + bp[q - 1] + bp[q + 1] +
-                                        bm[q - BX] + bm[q + BX] + bp[q - BX] + bp[q + BX];
-                        if (SCALED) {
-                            const T sc = (T)ps[c];
-                            next = ((T)2 - total * sc) * here + (sc * axial) * sum + (sc * diagonal) * edges - pa[c];
+                        T *out = a + (row0 + (uint32_t)r * p.pitch);
+                        if (in0 && in1) {
+                            V2 v;
+                            v.x = n0, v.y = n1;
+                            *reinterpret_cast<V2 *>(out) = v;
+                        } else if (in0) {
+                            out[0] = n0;
                         } else {
-                            next = centre * here + axial * sum + diagonal * edges - pa[c];
+                            out[1] = n1;
                         }
                     } else {
-                        if (SCALED) {
-                            const T sc = (T)ps[c];
-                            next = ((T)2 - total * sc) * here + (sc * axial) * sum - pa[c];
-                        } else {
-                            next = centre * here + axial * sum - pa[c];
+#pragma unroll
+                    for (int k = 0; k < SH::COLS; ++k) {
+                        const int c = yl * TX + xl + k;
+                        // Outside the interior cells' box, and outside the grid (zero fill), no cell
+                        // is interior.
+                        if (!t.full && pt[c] != kInterior) continue;
+                        const int q = (yl + 1) * BX + (xl + k + kHX);
+                        const T here = b0[q];
+                        const uint64_t at = row0 + (uint32_t)r * p.pitch + k;
+                        if (COMP) {
+                            // pa holds the increment; the neighbours as differences, in the sum's order.
+                            const T sum = (b0[q - 1] - here) + (b0[q + 1] - here) + (b0[q - BX] - here) +
+                                          (b0[q + BX] - here) + (bm[q] - here) + (bp[q] - here);
+                            T edges = (T)0;
+                            if (WIDE)
+                                edges = (b0[q - 1 - BX] - here) + (b0[q + 1 - BX] - here) + (b0[q - 1 + BX] - here) +
+                                        (b0[q + 1 + BX] - here) + (bm[q - 1] - here) + (bm[q + 1] - here) +
+                                        (bp[q - 1] - here) + (bp[q + 1] - here) + (bm[q - BX] - here) +
+                                        (bm[q + BX] - here) + (bp[q - BX] - here) + (bp[q + BX] - here);
+                            T step;
+                            if (SCALED) {
+                                const T sc = (T)ps[c];
+                                step = WIDE ? pa[c] + (sc * axial) * sum + (sc * diagonal) * edges + (sc * residual) * here
+                                            : pa[c] + (sc * axial) * sum + (sc * residual) * here;
+                            } else {
+                                step = WIDE ? pa[c] + axial * sum + diagonal * edges + residual * here
+                                            : pa[c] + axial * sum + residual * here;
+                            }
+                            a[at] = here + step;
+                            dd[at] = step;
+                            continue;
                         }
+                        const T sum = b0[q - 1] + b0[q + 1] + b0[q - BX] + b0[q + BX] + bm[q] + bp[q];
+                        T next;
+                        if (WIDE) {
+                            const T edges = b0[q - 1 - BX] + b0[q + 1 - BX] + b0[q - 1 + BX] + b0[q + 1 + BX] +
+                                            bm[q - 1] + bm[q + 1] + bp[q - 1] + bp[q + 1] +
+                                            bm[q - BX] + bm[q + BX] + bp[q - BX] + bp[q + BX];
+                            if (SCALED) {
+                                const T sc = (T)ps[c];
+                                next = ((T)2 - total * sc) * here + (sc * axial) * sum + (sc * diagonal) * edges - pa[c];
+                            } else {
+                                next = centre * here + axial * sum + diagonal * edges - pa[c];
+                            }
+                        } else {
+                            if (SCALED) {
+                                const T sc = (T)ps[c];
+                                next = ((T)2 - total * sc) * here + (sc * axial) * sum - pa[c];
+                            } else {
+                                next = centre * here + axial * sum - pa[c];
+                            }
+                        }
+                        a[at] = next;
                     }
-                    a[at] = next;
+                    }
                 }
             }
             // Every thread is done with plane z-1's stage; stop the block alike if a wait gave up.

@@ -276,14 +276,14 @@ class B200WaveSolver:
 
     def tiles(self) -> dict[str, int]:
         """The interior sweep's tiles: shape index, cells a tile along x and y, ring stages,
-        planes a tile, tiles, and resident blocks a multiprocessor."""
+        planes a tile, tiles, resident blocks a multiprocessor and threads a block."""
         t = _abi.FdtdTiles()
         status = self._lib.fdtd_get_tiles(self._handle, ctypes.byref(t))
         if status != _abi.FDTD_OK:
             _raise(self._lib, status, self._handle)
         return {"tile_shape": t.shape, "tile_x": t.tile_x, "tile_y": t.tile_y, "tile_stages": t.stages,
                 "tile_planes": int(t.planes), "tiles": int(t.tiles), "tile_blocks_per_sm": t.blocks_per_sm,
-                "concurrent": t.concurrent}  # fmt: skip
+                "tile_threads": t.threads, "tile_cols": t.cols, "concurrent": t.concurrent}  # fmt: skip
 
     def set_streams(self, concurrent: bool) -> None:
         """A step's kernels beside one another on three streams (True) or in turn on one (False), as

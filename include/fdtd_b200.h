@@ -252,13 +252,18 @@ int fdtd_autotune(fdtd_solver *solver, uint64_t trial_steps, int *layer_per_sm, 
 
 /* The interior sweep's tiles (no counterpart in the reference). */
 typedef struct fdtd_tiles {
-    int shape;          /* 0: 64 x 16 cells, 5 stages; 1: 128 x 16, 4; 2: 64 x 32, 4; 3: 32 x 32, 5 */
+    int shape;          /* 0: 64 x 16 cells, 5 stages; 1: 128 x 16, 4; 2: 64 x 32, 4; 3: 32 x 32, 5 (128
+                         * threads a block, a column a thread); 4, 5, 6: shapes 0, 1, 2 with 256
+                         * threads a block; 7: shape 0 with a pair of columns a thread; 8: 128 x 16,
+                         * 4 stages, 256 threads, pairs; 9: 64 x 16, 5 stages, 256 threads, pairs */
     int tile_x, tile_y; /* cells of a tile along x and y */
     int stages;         /* plane stages in a block's shared-memory ring */
     uint64_t planes;    /* planes of a tile, at most (a tile marches them along z) */
     uint32_t tiles;     /* tiles, one block each */
     int blocks_per_sm;  /* resident blocks of the sweep a multiprocessor */
     int concurrent;     /* 1: a step's kernels beside one another on three streams; 0: in turn */
+    int threads;        /* threads a block of the sweep */
+    int cols;           /* adjacent columns a thread (1, or 2: the 7-point stencil a pair at a time) */
 } fdtd_tiles;
 
 /*

@@ -226,7 +226,7 @@ def test_gpu_every_tile_shape_steps_as_the_oracle_does(precision):
     oracle = OracleSolver(w.built.layout, precision)
     expected = oracle.run(w.signal)
     state = oracle.state()
-    for shape, planes in [(0, 8), (1, 16), (2, 32), (3, 5), (1, 64)]:
+    for shape, planes in [(0, 8), (1, 16), (2, 32), (3, 5), (1, 64), (4, 16), (5, 8), (6, 24), (7, 16), (8, 9), (9, 32)]:
         gpu = B200WaveSolver(w.built.layout, precision=precision, autotune=False)
         gpu.set_tiles(shape, planes)
         t = gpu.tiles()
@@ -241,12 +241,12 @@ def test_gpu_every_tile_shape_steps_as_the_oracle_does(precision):
     # changed mid-run, between pieces of odd length
     gpu = B200WaveSolver(w.built.layout, precision=precision, autotune=False)
     pieces = []
-    for (a, b), shape in zip([(0, 17), (17, 50), (50, 90)], [3, 1, 2]):
+    for (a, b), shape in zip([(0, 17), (17, 50), (50, 90)], [7, 4, 9]):
         gpu.set_tiles(shape, 12)
         pieces.append(gpu.run(w.signal[a:b]))
     assert np.array_equal(np.concatenate(pieces, axis=1), expected)
     with pytest.raises(ValueError, match="tile shape"):
-        gpu.set_tiles(4, 8)
+        gpu.set_tiles(10, 8)
 
 
 def test_gpu_an_expired_wait_is_a_status_and_the_handle_stays_usable():
