@@ -80,6 +80,11 @@ struct AdjointTables {
     // layer cell; bit 2a + 1, the cell above; bit 6, the cell itself. Per special row, per
     // corrected cell (0 where no layer cell is near) and per layer cell.
     const uint8_t *special_layer_mask, *corrected_layer_mask, *layer_mask;
+    // The special rows and the corrected cells in an order that puts first those whose update
+    // gathers none of the layer's terms (special_far of the rows, corrected_far of the cells):
+    // those step back beside the layer's kernels, the others after the layer's hats.
+    const uint32_t *special_order, *corrected_order;
+    uint32_t special_far, corrected_far;
 };
 
 // The trajectory of a run: level l of the special rows' pressure at traj_u[l * specials + k] and
@@ -327,27 +332,39 @@ __device__ __forceinline__ void layer_adjoint_cell(const AdjointTables &t, uint3
     lam_out[i] = value;
 }
 
-// The special rows' adjoint (blocks 0 .. special_blocks - 1), correct_kernel's cells (the next
-// corrected_blocks) and the matched layer's cells (the blocks after) in one launch: they read the
-// same complete level (and the layer's hats of the step) and write disjoint memory.
+// One launch of the special rows' adjoint (the rows special_order[begin .. end), on the first
+// blocks), of correct_kernel's cells (corrected_order[begin .. end), the next blocks) and, with
+// `layer`, of the matched layer's cells (the blocks after): they read the same complete level (and
+// the layer's hats of the step) and write disjoint memory. The rows and cells far from the layer
+// take one launch beside the layer's hat kernel, the rest and the layer's cells one after it.
+struct RowsPart {
+    uint32_t special_begin, special_end, special_blocks;
+    uint32_t corrected_begin, corrected_end, corrected_blocks;
+    bool layer;
+};
+
 template <typename T>
-__global__ void __launch_bounds__(kBlock) rows_adjoint_kernel(const AdjointTables t, uint32_t special_blocks,
-                                                              uint32_t corrected_blocks, const T *lam_next,
-                                                              const T *om_next, const T *tilde, const T *hat, T *lam_out,
-                                                              T *om_out, const T *traj_u, const T *traj_w,
-                                                              uint32_t level, double *g_ci, double *g_cb, double *g_now,
-                                                              double *g_before, double *g_gain, T *tilde_out,
-                                                              const double *dloss, uint64_t stride, uint64_t step) {
-    if (blockIdx.x < special_blocks)
-        special_adjoint_row<T>(t, blockIdx.x * kBlock + threadIdx.x, lam_next, om_next, tilde, hat, lam_out, om_out,
-                               traj_u, traj_w, level, g_ci, g_cb, g_now, g_before, g_gain, tilde_out, dloss, stride,
-                               step);
-    else if (blockIdx.x < special_blocks + corrected_blocks)
-        correct_cell<T>(t, (blockIdx.x - special_blocks) * kBlock + threadIdx.x, lam_next, tilde, hat, lam_out, dloss,
-                        stride, step);
-    else
-        layer_adjoint_cell<T>(t, (blockIdx.x - special_blocks - corrected_blocks) * kBlock + threadIdx.x, lam_next,
+__global__ void __launch_bounds__(kBlock) rows_adjoint_kernel(const AdjointTables t, const RowsPart part,
+                                                              const T *lam_next, const T *om_next, const T *tilde,
+                                                              const T *hat, T *lam_out, T *om_out, const T *traj_u,
+                                                              const T *traj_w, uint32_t level, double *g_ci,
+                                                              double *g_cb, double *g_now, double *g_before,
+                                                              double *g_gain, T *tilde_out, const double *dloss,
+                                                              uint64_t stride, uint64_t step) {
+    const uint32_t b = blockIdx.x;
+    if (b < part.special_blocks) {
+        const uint32_t e = part.special_begin + b * kBlock + threadIdx.x;
+        if (e < part.special_end)
+            special_adjoint_row<T>(t, t.special_order[e], lam_next, om_next, tilde, hat, lam_out, om_out, traj_u,
+                                   traj_w, level, g_ci, g_cb, g_now, g_before, g_gain, tilde_out, dloss, stride, step);
+    } else if (b < part.special_blocks + part.corrected_blocks) {
+        const uint32_t e = part.corrected_begin + (b - part.special_blocks) * kBlock + threadIdx.x;
+        if (e < part.corrected_end)
+            correct_cell<T>(t, t.corrected_order[e], lam_next, tilde, hat, lam_out, dloss, stride, step);
+    } else if (part.layer) {
+        layer_adjoint_cell<T>(t, (b - part.special_blocks - part.corrected_blocks) * kBlock + threadIdx.x, lam_next,
                               tilde, hat, lam_out, dloss, stride, step);
+    }
 }
 
 }  // namespace fdtd

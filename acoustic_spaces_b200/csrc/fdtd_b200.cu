@@ -1173,6 +1173,9 @@ struct AdjointLists {
     std::vector<double> layer_from_coef, layer_from_base;
     std::vector<uint8_t> layer_interior, special_layer_mask, corrected_layer_mask, layer_mask;
     std::vector<uint32_t> by_coord, coord_start;  // the layer cells by coordinate, per axis
+    // The rows and corrected cells, those that gather no layer terms first (AdjointTables).
+    std::vector<uint32_t> special_order, corrected_order;
+    uint32_t special_far = 0, corrected_far = 0;
 };
 
 // The lists from the handle's own device tables.
@@ -1355,6 +1358,15 @@ int adjoint_lists(fdtd_solver *s, AdjointLists &out) {
         out.layer_interior.push_back(inner);
         out.layer_mask.push_back(layer_mask(i));
     }
+    // The rows and the corrected cells, those whose updates gather none of the layer's terms
+    // first, each part in its own order.
+    for (int near = 0; near < 2; ++near) {
+        for (uint64_t k = 0; k < K; ++k)
+            if ((out.special_layer_mask[k] != 0) == (near != 0)) out.special_order.push_back((uint32_t)k);
+        for (uint64_t c = 0; c < out.cells.size(); ++c)
+            if ((out.corrected_layer_mask[c] != 0) == (near != 0)) out.corrected_order.push_back((uint32_t)c);
+        if (!near) out.special_far = (uint32_t)out.special_order.size(), out.corrected_far = (uint32_t)out.corrected_order.size();
+    }
     // Per axis, the layer cells sorted by their coordinate along it (counting sort, stable), and
     // where each coordinate's cells begin: coordinates 0 .. n_a - 1 of axis a follow axis a - 1's.
     if (Lc) {
@@ -1445,6 +1457,9 @@ int place_adjoint(fdtd_solver *s, const AdjointLists &l, Pool &pool, AdjointStat
     if ((rc = place(s, pool, l.layer_from_coef, &t.layer_from_coef))) return rc;
     if ((rc = place(s, pool, l.layer_read_start, &t.layer_read_start))) return rc;
     if ((rc = place(s, pool, l.layer_interior, &t.layer_interior))) return rc;
+    if ((rc = place(s, pool, l.special_order, &t.special_order))) return rc;
+    if ((rc = place(s, pool, l.corrected_order, &t.corrected_order))) return rc;
+    t.special_far = l.special_far, t.corrected_far = l.corrected_far;
     if (s->layers) {
         if ((rc = pool.take(e * 9 * s->layers, &a.carried, true))) return rc;
         if ((rc = pool.take(e * 6 * s->n_device, &a.hat, true))) return rc;
@@ -1673,9 +1688,12 @@ int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float
     if (Lc) CUDA_TRY(s, cudaMemsetAsync(adj.carried, 0, e * 9 * Lc, s->stream));
     const AdjointTables &t = adj.t;
     const uint32_t row_blocks = (uint32_t)((std::max<uint64_t>(std::max<uint64_t>(K, S), 1) + kBlock - 1) / kBlock);
-    const uint32_t special_blocks = (uint32_t)((K + kBlock - 1) / kBlock);
-    const uint32_t corrected_blocks = (uint32_t)((t.corrected + kBlock - 1) / kBlock);
     const uint32_t layer_blocks = (uint32_t)((Lc + kBlock - 1) / kBlock);
+    auto blocks_of = [](uint32_t count) { return (count + kBlock - 1) / kBlock; };
+    // (Without a layer every row and cell is far from it.)
+    const RowsPart far{0, t.special_far, blocks_of(t.special_far), 0, t.corrected_far, blocks_of(t.corrected_far), false};
+    const RowsPart near{t.special_far, (uint32_t)K, blocks_of((uint32_t)K - t.special_far),
+                        t.corrected_far, t.corrected, blocks_of(t.corrected - t.corrected_far), true};
     const uint32_t smem = s->scaled ? Stage<T, true>::smem : Stage<T, false>::smem;
     int x = 0;  // lam[x], om[x]: level n+1; lam[1-x], om[1-x]: level n+2, then level n
     // A segment's recomputation (the dispatch of its steps, recording the special rows), and its
@@ -1700,16 +1718,25 @@ int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float
             T *tilde_out = static_cast<T *>(adj.tilde[1 - xx]);
             CUDA_TRY(s, cudaEventRecord(s->joined[0], s->stream));
             CUDA_TRY(s, cudaStreamWaitEvent(s->side, s->joined[0], 0));
+            if (layer_blocks) CUDA_TRY(s, cudaStreamWaitEvent(s->layer_stream, s->joined[0], 0));
             T *hat = static_cast<T *>(adj.hat);
-            // The matched layer's hats of step m first (the gathers below read them).
-            if (layer_blocks)
-                layer_hat_kernel<T><<<layer_blocks, kBlock, 0, s->side>>>(
+            // The rows and corrected cells far from the layer on the side stream; on the layer's
+            // stream (the highest priority) the layer's hats of step m, then the rows and cells
+            // that gather them and the layer's own cells.
+            if (far.special_blocks + far.corrected_blocks)
+                rows_adjoint_kernel<T><<<far.special_blocks + far.corrected_blocks, kBlock, 0, s->side>>>(
+                    t, far, lam_next, om_next, tilde, hat, lam_out, om_out, traj_u, traj_w, (uint32_t)m, g[1], g[0],
+                    g[2], g[3], g[4], tilde_out, seg_dloss, segment, m);
+            if (layer_blocks) {
+                layer_hat_kernel<T><<<layer_blocks, kBlock, 0, s->layer_stream>>>(
                     t, lam_next, static_cast<T *>(adj.carried), hat,
                     tables ? traj_layer + m * kLayerFactors * Lc : nullptr, g_layer);
-            if (special_blocks + corrected_blocks + layer_blocks)
-                rows_adjoint_kernel<T><<<special_blocks + corrected_blocks + layer_blocks, kBlock, 0, s->side>>>(
-                    t, special_blocks, corrected_blocks, lam_next, om_next, tilde, hat, lam_out, om_out, traj_u, traj_w,
-                    (uint32_t)m, g[1], g[0], g[2], g[3], g[4], tilde_out, seg_dloss, segment, m);
+                rows_adjoint_kernel<T><<<near.special_blocks + near.corrected_blocks + layer_blocks, kBlock, 0,
+                                         s->layer_stream>>>(t, near, lam_next, om_next, tilde, hat, lam_out, om_out,
+                                                            traj_u, traj_w, (uint32_t)m, g[1], g[0], g[2], g[3], g[4],
+                                                            tilde_out, seg_dloss, segment, m);
+                CUDA_TRY(s, cudaEventRecord(s->joined[2], s->layer_stream));
+            }
             CUDA_TRY(s, cudaEventRecord(s->joined[1], s->side));
             if (s->bulk_blocks) {
                 // The forward sweep of the grid's own kind (with a speed field it steps v = s lam).
@@ -1729,6 +1756,7 @@ int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float
                     bulk_kernel<T, false, false><<<blocks, kBlock, smem, s->stream>>>(mb, ma, adj.map_t, adj.map_s, args);
             }
             CUDA_TRY(s, cudaStreamWaitEvent(s->stream, s->joined[1], 0));
+            if (layer_blocks) CUDA_TRY(s, cudaStreamWaitEvent(s->stream, s->joined[2], 0));
             xx = 1 - xx;
         }
         CUDA_TRY(s, cudaGetLastError());
@@ -1897,6 +1925,7 @@ size_t pool_bytes(const fdtd_solver *s, const AdjointLists &l, uint64_t steps, u
     list(l.special_layer_mask.size(), 1), list(l.corrected_layer_mask.size(), 1), list(l.layer_mask.size(), 1);
     list(l.layer_from_start.size(), 4), list(l.layer_from_row.size(), 4), list(l.layer_from_coef.size(), 8);
     list(l.layer_read_start.size(), 4), list(l.layer_interior.size(), 1);
+    list(l.special_order.size(), 4), list(l.corrected_order.size(), 4);
     const uint64_t Lc = s->layers;
     if (Lc) total += pool_round(e * 9 * Lc) + pool_round(e * 6 * n);
     total += 2 * (pool_round(e * n) + pool_round(e * S)) + 2 * pool_round(e * K);
