@@ -214,9 +214,10 @@ __host__ __device__ inline bool cut_cell(const CutArgs &g, uint64_t i, double *v
         volume += e[q] * facet;
         for (int r = 0; r < cuts && m > 0; ++r)
             if (open[r]) m = clip3(p, m, g.normals + 3 * cut[r], e[r]);
-        double covered = 0.0;
+        // (the wall's area in the cell: the pieces split it by material, a rounding apart)
+        const double covered = m >= 3 ? area3(p, m) : 0.0;
         if (!g.pieces) {
-            covered = cap_out[cut[q]] = m >= 3 ? area3(p, m) : 0.0;
+            cap_out[cut[q]] = covered;
         } else {
             // each piece of the wall: the wall's part in the cell clipped by the piece's edges
             for (uint32_t k = 0; k < g.pieces && m >= 3; ++k) {
@@ -231,7 +232,6 @@ __host__ __device__ inline bool cut_cell(const CutArgs &g, uint64_t i, double *v
                     wm = clip3(w, wm, edge, eh);
                 }
                 cap_out[k] = wm >= 3 ? area3(w, wm) : 0.0;
-                covered += cap_out[k];
             }
         }
         // the part of the facet no wall covers (beyond the open face): the air meets across it

@@ -436,14 +436,14 @@ def walls_of(room) -> Walls:
                  np.asarray(vertices, np.float64), np.asarray(faces, np.int64))  # fmt: skip
 
 
-def mesh_walls(vertices, faces, materials, count: int, *, tolerance: float = 1e-9, convexity: float = 1e-7) -> Walls:
+def mesh_walls(vertices, faces, materials, count: int, *, tolerance: float = 1e-7, convexity: float = 1e-7) -> Walls:
     """The walls of a convex room given as a triangle mesh, each triangle with its material (as
     the reference's WaveSolver and CutFit take a room, native_module.cpp:1465-1559): the planes of
     its triangles (coplanar ones merged), each triangle a piece of wall on its plane bounded by
     its three edges, and the faces of the vertices' convex hull on which no triangle lies left
-    open. Triangles within ``tolerance`` (of the room's size) of one plane share it; a face folded
-    by less than ``convexity`` (a vertex that far outside a triangle's plane) is taken as the two
-    planes of its triangles. The planes are taken relative to the first vertex (``anchor``), so
+    open. Triangles within ``tolerance`` (of the room's size) of one plane share it (the first's):
+    a face folded by less, either way, is taken as flat, since a fit of the walls' half-spaces
+    cannot follow a fold into the room. The planes are taken relative to the first vertex (``anchor``), so
     that a room far from the origin keeps its digits. Raises ValueError where vertices lie farther
     on both sides of a triangle's plane (the room is not convex)."""
     from scipy.spatial import ConvexHull
@@ -718,6 +718,9 @@ def fit_from_cut(cut: Cut, room, grid: L.Grid, *, layer: int = 0) -> Fit:
     reg_volume = np.concatenate([np.stack([v_in, v_out], axis=1).reshape(-1), cell_volume(whole)])
     reg_valid = np.concatenate([np.stack([has_in, has_out], axis=1).reshape(-1), np.ones(W, bool)])
     in_air = reg_valid & (air[reg_cell] != SOLID)
+    # A cut cell's air inside the walls is the room's whether or not the cell's centre is: where
+    # the centre lies outside, the owner rule gives that region to a neighbour.
+    in_air[0 : 2 * C : 2] |= reg_valid[0 : 2 * C : 2] & ~edge[cc]
     if not room.open:  # the air outside a closed room's walls is not the source's
         in_air[1 : 2 * C : 2] = False
 
