@@ -69,6 +69,7 @@ struct AdjointTables {
     const float4 *layer_coef[3];
     const float *layer_scale;
     uint32_t pitch, plane;
+    FastDiv by_plane, by_pitch;
     uint64_t cells;  // pitched cells of a level (the stride of the hat arrays)
     // Rows linking to each layer cell (layer_from_start[c] .. [c + 1] of row and coefficient), the
     // probes' terms of each layer cell (layer_read_start[c] .. [c + 1] into read_probe, read_weight),
@@ -231,7 +232,7 @@ __global__ void __launch_bounds__(kBlock) layer_hat_kernel(const AdjointTables t
     const uint32_t L = t.layers;
     if (c >= L) return;
     const uint32_t i = t.layer_cells[c];
-    const uint32_t z = i / t.plane, r = i - z * t.plane, y = r / t.pitch;
+    const uint32_t z = t.by_plane(i), r = i - z * t.plane, y = t.by_pitch(r);
     const uint32_t at[3] = {r - y * t.pitch, y, z};
     const T s = t.layer_scale ? (T)t.layer_scale[c] : (T)1;
     const T lam = lam_next[i];

@@ -122,7 +122,7 @@ struct fdtd_solver {
     void *u[2] = {nullptr, nullptr};
     void *w[2] = {nullptr, nullptr};
     void *increment = nullptr;              // FDTD_FP32_COMPENSATED: p_n - p_(n-1) per cell (pitched)
-    void *layer_parts = nullptr;            // 3 arrays of the layer's cells: p_x, p_y, p_z
+    void *layer_parts = nullptr;            // the layer's cells' parts p_x, p_y, p_z, kPartStride a cell
     std::vector<uint32_t> layer_cells;      // pitched, in the layout's order (for fdtd_read_state)
     const uint8_t *types_device = nullptr;  // the pitched cell types
     const float *scale_device = nullptr;    // with a speed field: each pitched cell's scale
@@ -903,6 +903,8 @@ int build(fdtd_solver *s, const fdtd_layout *L) {
     g.nz = (uint32_t)nz;
     g.sz = (uint32_t)(s->pitch * ny);
     g.plane = (uint32_t)(s->pitch * ny);
+    g.by_plane = FastDiv(g.plane);
+    g.by_pitch = FastDiv(g.pitch);
     for (int k = 0; k < 18; ++k)
         g.offset[k] = (int32_t)(kSteps[k][0] + kSteps[k][1] * (int64_t)s->pitch + kSteps[k][2] * (int64_t)(s->pitch * ny));
 
@@ -940,7 +942,7 @@ int build(fdtd_solver *s, const fdtd_layout *L) {
         if ((rc = zeros(s, e * s->n_device, &s->u[k]))) return rc;
         if ((rc = zeros(s, e * L->state_count, &s->w[k]))) return rc;
     }
-    if ((rc = zeros(s, e * 3 * L->layer_count, &s->layer_parts))) return rc;
+    if ((rc = zeros(s, e * kPartStride * L->layer_count, &s->layer_parts))) return rc;
     if (s->precision == FDTD_FP32_COMPENSATED && (rc = zeros(s, e * s->n_device, &s->increment))) return rc;
     if (L->layer_count)
         for (int k = 0; k < 2; ++k)
@@ -1448,6 +1450,7 @@ int place_adjoint(fdtd_solver *s, const AdjointLists &l, Pool &pool, AdjointStat
     for (int axis = 0; axis < 3; ++axis) t.layer_coef[axis] = g.layer_coef[axis];
     t.layer_scale = g.layer_scale;
     t.pitch = g.pitch, t.plane = g.plane;
+    t.by_plane = g.by_plane, t.by_pitch = g.by_pitch;
     t.cells = s->n_device;
     if ((rc = place(s, pool, l.special_layer_mask, &t.special_layer_mask))) return rc;
     if ((rc = place(s, pool, l.corrected_layer_mask, &t.corrected_layer_mask))) return rc;
@@ -1560,7 +1563,7 @@ struct Kept {
 uint64_t checkpoint_bytes(const fdtd_solver *s) {
     const uint64_t e = s->precision == FDTD_FP64 ? 8 : 4;
     uint64_t bytes = 2 * e * s->n_device + 2 * e * s->states;
-    if (s->layers) bytes += 3 * e * s->layers + 3 * e * s->n_device;
+    if (s->layers) bytes += kPartStride * e * s->layers + 3 * e * s->n_device;
     return bytes;
 }
 
@@ -1575,8 +1578,8 @@ int save_checkpoint(fdtd_solver *s, char *c) {
     }
     c += 2 * states;
     if (s->layers) {
-        CUDA_TRY(s, cudaMemcpyAsync(c, s->layer_parts, 3 * e * s->layers, cudaMemcpyDeviceToDevice, s->stream));
-        c += 3 * e * s->layers;
+        CUDA_TRY(s, cudaMemcpyAsync(c, s->layer_parts, kPartStride * e * s->layers, cudaMemcpyDeviceToDevice, s->stream));
+        c += kPartStride * e * s->layers;
         for (int axis = 0; axis < 3; ++axis, c += level)
             CUDA_TRY(s, cudaMemcpyAsync(c, s->faces[1][axis], level, cudaMemcpyDeviceToDevice, s->stream));
     }
@@ -1594,8 +1597,8 @@ int restore_checkpoint(fdtd_solver *s, const char *c) {
     }
     c += 2 * states;
     if (s->layers) {
-        CUDA_TRY(s, cudaMemcpyAsync(s->layer_parts, c, 3 * e * s->layers, cudaMemcpyDeviceToDevice, s->stream));
-        c += 3 * e * s->layers;
+        CUDA_TRY(s, cudaMemcpyAsync(s->layer_parts, c, kPartStride * e * s->layers, cudaMemcpyDeviceToDevice, s->stream));
+        c += kPartStride * e * s->layers;
         for (int axis = 0; axis < 3; ++axis, c += level)
             CUDA_TRY(s, cudaMemcpyAsync(s->faces[1][axis], c, level, cudaMemcpyDeviceToDevice, s->stream));
     }
@@ -2678,7 +2681,7 @@ int fdtd_reset(fdtd_solver *s) {
     }
     if (s->increment) CUDA_TRY(s, cudaMemsetAsync(s->increment, 0, e * s->n_device, s->stream));
     if (s->layers) {
-        CUDA_TRY(s, cudaMemsetAsync(s->layer_parts, 0, e * 3 * s->layers, s->stream));
+        CUDA_TRY(s, cudaMemsetAsync(s->layer_parts, 0, e * kPartStride * s->layers, s->stream));
         for (int k = 0; k < 2; ++k)
             for (int axis = 0; axis < 3; ++axis)
                 CUDA_TRY(s, cudaMemsetAsync(s->faces[k][axis], 0, e * s->n_device, s->stream));
@@ -2745,11 +2748,11 @@ int fdtd_read_state(const fdtd_solver *cs, void *current, void *previous, void *
         // The reference's nine values per cell (fdtd.hpp:2245): the parts, then per axis the
         // velocity of the - face (the + face of the cell below) and of the + face.
         const std::vector<uint32_t> &cells = s->layer_cells;
-        std::vector<char> parts(e * 3 * s->layers);
+        std::vector<char> parts(e * kPartStride * s->layers);
         CUDA_TRY(s, cudaMemcpy(parts.data(), s->layer_parts, parts.size(), cudaMemcpyDeviceToHost));
         char *dst = static_cast<char *>(layer_state);
         for (uint64_t c = 0; c < s->layers; ++c)
-            for (int k = 0; k < 3; ++k) std::memcpy(dst + e * (9 * c + k), parts.data() + e * (k * s->layers + c), e);
+            for (int k = 0; k < 3; ++k) std::memcpy(dst + e * (9 * c + k), parts.data() + e * (kPartStride * c + k), e);
         std::vector<char> face(e * s->n_device);
         const uint64_t strides[3] = {1, s->pitch, s->pitch * s->ny};
         for (int axis = 0; axis < 3; ++axis) {

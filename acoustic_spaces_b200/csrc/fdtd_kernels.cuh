@@ -33,6 +33,9 @@ namespace fdtd {
 
 constexpr int kSolid = 0, kInterior = 1, kSpecial = 2, kLayer = 3;
 constexpr int kBlock = 128;  // threads per block of every kernel
+// A matched-layer cell's three pressure parts sit together, padded to four (one 16-byte load and
+// store a cell in FP32, two in FP64): one stream of memory for the parts, not three.
+constexpr int kPartStride = 4;
 
 // ---- the bulk sweep's tiles ------------------------------------------------------------------
 constexpr int kHX = 4;                          // x halo of the pressure tile: 16 bytes of floats
@@ -437,6 +440,30 @@ __global__ void __launch_bounds__(SH::THREADS) bulk_kernel(const __grid_constant
 
 // ---- special rows, matched layer, probes -------------------------------------------------------
 
+// Division of 32-bit indices by a divisor fixed at set-up (a row's pitch, a plane's cells) by one
+// multiply-high and two shifts, Granlund and Montgomery's method for run-time invariant unsigned
+// divisors ("Division by invariant integers using multiplication", 1994, figure 4.1): with
+// l = ceil(log2 d) and m = floor(2^32 (2^l - d) / d) + 1, t = mulhi(m, n) gives
+// n / d = (t + ((n - t) >> 1)) >> (l - 1) for every 32-bit n (d >= 2).
+struct FastDiv {
+    uint32_t m = 0, shift = 0;
+    FastDiv() = default;
+    explicit FastDiv(uint32_t d) {
+        uint32_t l = 0;
+        while ((1ull << l) < d) ++l;
+        m = (uint32_t)(((1ull << 32) * ((1ull << l) - d)) / d + 1);
+        shift = l - 1;
+    }
+    __host__ __device__ __forceinline__ uint32_t operator()(uint32_t n) const {
+#ifdef __CUDA_ARCH__
+        const uint32_t t = __umulhi(m, n);
+#else
+        const uint32_t t = (uint32_t)(((uint64_t)m * n) >> 32);
+#endif
+        return (t + ((n - t) >> 1)) >> shift;
+    }
+};
+
 struct Tables {
     uint32_t pitch, ny, nz, sz;
     // Special rows (fdtd.hpp:860-881), as structure of arrays.
@@ -459,6 +486,7 @@ struct Tables {
     const float4 *layer_coef[3];
     const uint8_t *layer_below;  // bit a: the cell below along axis a is in the layer too
     uint32_t plane;  // pitch * ny
+    FastDiv by_plane, by_pitch;  // a pitched index's plane, and its row within the plane
     // Probes (fdtd.hpp:3525-3533).
     uint32_t probes;
     const uint32_t *probe_start, *probe_cells;
@@ -472,7 +500,7 @@ struct Fields {
     const T *b;        // the current pressure
     T *wa;             // branch velocities a step before, overwritten with the next
     const T *wb;       // current branch velocities
-    T *layer_parts;    // 3 arrays of `layers`: the pressure parts p_x, p_y, p_z
+    T *layer_parts;    // per layer cell c, its pressure parts p_x, p_y, p_z at kPartStride c + axis
     const T *face_old[3];  // per axis, the velocity on each cell's + face (pitched), a step before
     T *face_new[3];        // the same, this step
     const float *signal;  // the step's drive at signal[0]
@@ -577,17 +605,22 @@ __device__ __forceinline__ void layer_cell(const Tables &g, const Fields<T> &f, 
     // Every load of the cell first — its parts, its pressure and its six neighbours', its faces'
     // old velocities and the coefficients — so that they are in flight together; then the
     // reference's arithmetic, axis by axis; then the stores.
-    const uint32_t z = i / g.plane, r = i - z * g.plane, y = r / g.pitch;
+    const uint32_t z = g.by_plane(i), r = i - z * g.plane, y = g.by_pitch(r);
     const uint32_t at[3] = {r - y * g.pitch, y, z};
     const uint32_t strides[3] = {1u, g.pitch, g.plane};
     const T *__restrict__ b = f.b;
     T *__restrict__ parts = f.layer_parts;
     T part[3], lo[3], hi[3], old_below[3], old_above[3];
     float4 c0[3], c1[3];
+    {
+        using V2 = typename Pair<T>::type;
+        const V2 *own = reinterpret_cast<const V2 *>(parts + (uint64_t)kPartStride * c);
+        const V2 p01 = own[0], p2 = own[1];
+        part[0] = p01.x, part[1] = p01.y, part[2] = p2.x;
+    }
 #pragma unroll
     for (int axis = 0; axis < 3; ++axis) {
         const uint32_t stride = strides[axis];
-        part[axis] = parts[axis * L + c];
         lo[axis] = b[i - stride];
         hi[axis] = b[i + stride];
         old_below[axis] = __ldg(f.face_old[axis] + (i - stride));
@@ -634,7 +667,13 @@ __device__ __forceinline__ void layer_cell(const Tables &g, const Fields<T> &f, 
         f.face_new[axis][i] = above[axis];
         // The cell below owns the face when it is in the layer.
         if (!(shared_below & (1u << axis))) f.face_new[axis][i - strides[axis]] = below[axis];
-        parts[axis * L + c] = part[axis];
+    }
+    {
+        using V2 = typename Pair<T>::type;
+        V2 *own = reinterpret_cast<V2 *>(parts + (uint64_t)kPartStride * c);
+        V2 p01, p2;
+        p01.x = part[0], p01.y = part[1], p2.x = part[2], p2.y = (T)0;
+        own[0] = p01, own[1] = p2;
     }
     if (COMP) {
         f.a[i] = here + total;
