@@ -223,19 +223,20 @@ constexpr int kLayerFactors = 18;
 
 // The carried values (9 per cell: Q^' x3, L^' x3, H^' x3, at carried[v * layers + c]) are
 // updated in place; hat[(2a) * cells + i] = pf[x] L^ and hat[(2a + 1) * cells + i] = pf[x+1] H^ are
-// the terms' factors its neighbours gather; g[(6a + f) * layers + c] sums the gradient's products of
-// the cell in double.
+// the terms' factors its neighbours gather. A cell's hats of step n depend only on its own adjoint
+// of level n + 1 and its carried values, so the thread that forms that adjoint (the layer cell's
+// reverse step n + 1, layer_adjoint_cell) forms the hats of step n right after, into the other of
+// two hat buffers: the layer takes one launch a reverse step, not two. The tables' gradient sums
+// g[(6a + f) * layers + c] the products of Q^, H^, L^ with the forward's factors of step n (`traj`,
+// layer_cell's records); where step n's factors are not recorded yet (step n ends the segment
+// before, recomputed later), Q^, L^, H^ wait in `pending` (9 per cell) for layer_pending_kernel.
 template <typename T>
-__global__ void __launch_bounds__(kBlock) layer_hat_kernel(const AdjointTables t, const T *lam_next, T *carried,
-                                                           T *hat, const T *traj, double *g) {
-    const uint32_t c = blockIdx.x * kBlock + threadIdx.x;
+__device__ __forceinline__ void layer_hat_cell(const AdjointTables &t, uint32_t c, uint32_t i, T lam, T *carried, T *hat,
+                                               const T *traj, double *g, T *pending) {
     const uint32_t L = t.layers;
-    if (c >= L) return;
-    const uint32_t i = t.layer_cells[c];
     const uint32_t z = t.by_plane(i), r = i - z * t.plane, y = t.by_pitch(r);
     const uint32_t at[3] = {r - y * t.pitch, y, z};
     const T s = t.layer_scale ? (T)t.layer_scale[c] : (T)1;
-    const T lam = lam_next[i];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         const float4 c0 = __ldg(t.layer_coef[a] + at[a]), c1 = __ldg(t.layer_coef[a] + at[a] + 1);
@@ -248,7 +249,7 @@ __global__ void __launch_bounds__(kBlock) layer_hat_kernel(const AdjointTables t
         carried[(uint64_t)(6 + a) * L + c] = (T)c1.z * hi_hat;
         hat[(uint64_t)(2 * a) * t.cells + i] = (T)c0.w * lo_hat;
         hat[(uint64_t)(2 * a + 1) * t.cells + i] = (T)c1.w * hi_hat;
-        if (g) {
+        if (g && traj) {
             const T *f = traj + (uint64_t)(6 * a) * L + c;
             double *gg = g + (uint64_t)(6 * a) * L + c;
             gg[0] += (double)q_hat * (double)f[0];
@@ -257,7 +258,35 @@ __global__ void __launch_bounds__(kBlock) layer_hat_kernel(const AdjointTables t
             gg[(uint64_t)3 * L] += -(double)hi_hat * (double)f[(uint64_t)3 * L];
             gg[(uint64_t)4 * L] += (double)lo_hat * (double)f[(uint64_t)4 * L];
             gg[(uint64_t)5 * L] += -(double)lo_hat * (double)f[(uint64_t)5 * L];
+        } else if (pending) {
+            pending[(uint64_t)(3 * a) * L + c] = q_hat;
+            pending[(uint64_t)(3 * a + 1) * L + c] = lo_hat;
+            pending[(uint64_t)(3 * a + 2) * L + c] = hi_hat;
         }
+    }
+}
+
+// The tables' products of a step whose Q^, L^, H^ waited in `pending` (layer_hat_cell), once its
+// forward factors are recorded.
+template <typename T>
+__global__ void __launch_bounds__(kBlock) layer_pending_kernel(const AdjointTables t, const T *pending, const T *traj,
+                                                               double *g) {
+    const uint32_t c = blockIdx.x * kBlock + threadIdx.x;
+    const uint32_t L = t.layers;
+    if (c >= L) return;
+    const T s = t.layer_scale ? (T)t.layer_scale[c] : (T)1;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const T q_hat = pending[(uint64_t)(3 * a) * L + c], lo_hat = pending[(uint64_t)(3 * a + 1) * L + c];
+        const T hi_hat = pending[(uint64_t)(3 * a + 2) * L + c];
+        const T *f = traj + (uint64_t)(6 * a) * L + c;
+        double *gg = g + (uint64_t)(6 * a) * L + c;
+        gg[0] += (double)q_hat * (double)f[0];
+        gg[(uint64_t)1 * L] += -(double)q_hat * (double)s * (double)f[(uint64_t)1 * L];
+        gg[(uint64_t)2 * L] += (double)hi_hat * (double)f[(uint64_t)2 * L];
+        gg[(uint64_t)3 * L] += -(double)hi_hat * (double)f[(uint64_t)3 * L];
+        gg[(uint64_t)4 * L] += (double)lo_hat * (double)f[(uint64_t)4 * L];
+        gg[(uint64_t)5 * L] += -(double)lo_hat * (double)f[(uint64_t)5 * L];
     }
 }
 
@@ -310,13 +339,24 @@ __device__ __forceinline__ T layer_terms(const AdjointTables &t, const T *hat, u
     return sum;
 }
 
+// The layer's part of a reverse step: where its hats of the step before go (`next`, the other hat
+// buffer), its carried values, and the tables' sums with the factors of that step (`traj`, or null
+// with `pending` where they are not recorded yet; both null for a gradient without the tables).
+template <typename T>
+struct LayerNext {
+    T *hat, *carried, *pending;
+    const T *traj;
+    double *g;
+};
+
 // A layer cell's adjoint: its interior neighbours' axial x lam (with a speed field their stored
 // s lam), the rows linking to it, the layer's terms and the probes' terms (a layer cell's update
-// reads no level before the last, so no level two steps on enters).
+// reads no level before the last, so no level two steps on enters); then, from it, the cell's hats
+// of the step before (layer_hat_cell).
 template <typename T>
 __device__ __forceinline__ void layer_adjoint_cell(const AdjointTables &t, uint32_t c, const T *lam_next, const T *tilde,
                                                    const T *hat, T *lam_out, const double *dloss, uint64_t stride,
-                                                   uint64_t step) {
+                                                   uint64_t step, const LayerNext<T> &next) {
     if (c >= t.layers) return;
     const uint32_t i = t.layer_cells[c];
     const uint32_t inner = t.layer_interior[c];
@@ -331,13 +371,14 @@ __device__ __forceinline__ void layer_adjoint_cell(const AdjointTables &t, uint3
     const double probed = probe_terms(t, t.layer_read_start[c], t.layer_read_start[c + 1], dloss, stride, step);
     if (probed != 0.0) value += (T)probed;
     lam_out[i] = value;
+    layer_hat_cell<T>(t, c, i, value, next.carried, next.hat, next.traj, next.g, next.pending);
 }
 
 // One launch of the special rows' adjoint (the rows special_order[begin .. end), on the first
 // blocks), of correct_kernel's cells (corrected_order[begin .. end), the next blocks) and, with
 // `layer`, of the matched layer's cells (the blocks after): they read the same complete level (and
 // the layer's hats of the step) and write disjoint memory. The rows and cells far from the layer
-// take one launch beside the layer's hat kernel, the rest and the layer's cells one after it.
+// take one launch, the rest and the layer's cells another, beside it on a stream of its own.
 struct RowsPart {
     uint32_t special_begin, special_end, special_blocks;
     uint32_t corrected_begin, corrected_end, corrected_blocks;
@@ -351,7 +392,7 @@ __global__ void __launch_bounds__(kBlock) rows_adjoint_kernel(const AdjointTable
                                                               const T *traj_w, uint32_t level, double *g_ci,
                                                               double *g_cb, double *g_now, double *g_before,
                                                               double *g_gain, T *tilde_out, const double *dloss,
-                                                              uint64_t stride, uint64_t step) {
+                                                              uint64_t stride, uint64_t step, const LayerNext<T> next) {
     const uint32_t b = blockIdx.x;
     if (b < part.special_blocks) {
         const uint32_t e = part.special_begin + b * kBlock + threadIdx.x;
@@ -364,7 +405,7 @@ __global__ void __launch_bounds__(kBlock) rows_adjoint_kernel(const AdjointTable
             correct_cell<T>(t, t.corrected_order[e], lam_next, tilde, hat, lam_out, dloss, stride, step);
     } else if (part.layer) {
         layer_adjoint_cell<T>(t, (b - part.special_blocks - part.corrected_blocks) * kBlock + threadIdx.x, lam_next,
-                              tilde, hat, lam_out, dloss, stride, step);
+                              tilde, hat, lam_out, dloss, stride, step, next);
     }
 }
 

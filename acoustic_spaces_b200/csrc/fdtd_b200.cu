@@ -69,7 +69,8 @@ struct AdjointState {
     void *tilde[2] = {nullptr, nullptr};  // L~ of the level at hand, and of the next (alternating)
     CUtensorMap lam_b[2], lam_a[2];
     void *carried = nullptr;  // the matched layer's carried values (9 per cell)
-    void *hat = nullptr;      // the matched layer's terms' factors (6 pitched levels)
+    void *hat[2] = {nullptr, nullptr};  // the matched layer's terms' factors (6 pitched levels), a step's and the next's
+    void *pending = nullptr;  // the layer's Q^, L^, H^ of a step whose factors come with the next segment
     // The layer cells sorted by their coordinate along each axis in turn (x, then y, then z; each
     // a permutation of the cells) and each coordinate's first entry: the tables' sums by coordinate.
     const uint32_t *by_coord = nullptr, *coord_start = nullptr;
@@ -1465,7 +1466,9 @@ int place_adjoint(fdtd_solver *s, const AdjointLists &l, Pool &pool, AdjointStat
     t.special_far = l.special_far, t.corrected_far = l.corrected_far;
     if (s->layers) {
         if ((rc = pool.take(e * 9 * s->layers, &a.carried, true))) return rc;
-        if ((rc = pool.take(e * 6 * s->n_device, &a.hat, true))) return rc;
+        for (int k = 0; k < 2; ++k)
+            if ((rc = pool.take(e * 6 * s->n_device, &a.hat[k], true))) return rc;
+        if ((rc = pool.take(e * 9 * s->layers, &a.pending, true))) return rc;
         if ((rc = place(s, pool, l.by_coord, &a.by_coord))) return rc;
         if ((rc = place(s, pool, l.coord_start, &a.coord_start))) return rc;
     }
@@ -1688,7 +1691,11 @@ int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float
         if (S) CUDA_TRY(s, cudaMemsetAsync(adj.om[k], 0, state_bytes, s->stream));
         if (K) CUDA_TRY(s, cudaMemsetAsync(adj.tilde[k], 0, sizeof(T) * K, s->stream));
     }
-    if (Lc) CUDA_TRY(s, cudaMemsetAsync(adj.carried, 0, e * 9 * Lc, s->stream));
+    // (The layer's hats of the first reverse step are those of rest: zero.)
+    if (Lc) {
+        CUDA_TRY(s, cudaMemsetAsync(adj.carried, 0, e * 9 * Lc, s->stream));
+        for (int k = 0; k < 2; ++k) CUDA_TRY(s, cudaMemsetAsync(adj.hat[k], 0, e * 6 * s->n_device, s->stream));
+    }
     const AdjointTables &t = adj.t;
     const uint32_t row_blocks = (uint32_t)((std::max<uint64_t>(std::max<uint64_t>(K, S), 1) + kBlock - 1) / kBlock);
     const uint32_t layer_blocks = (uint32_t)((Lc + kBlock - 1) / kBlock);
@@ -1722,22 +1729,28 @@ int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float
             CUDA_TRY(s, cudaEventRecord(s->joined[0], s->stream));
             CUDA_TRY(s, cudaStreamWaitEvent(s->side, s->joined[0], 0));
             if (layer_blocks) CUDA_TRY(s, cudaStreamWaitEvent(s->layer_stream, s->joined[0], 0));
-            T *hat = static_cast<T *>(adj.hat);
+            // The layer's hats of step m (formed in the step before, or zero), and where the layer
+            // cells put those of step m - 1: the other buffer, with the tables' factors of step
+            // m - 1 of this segment, or (m = 0) the values that wait for the segment before.
+            T *hat = static_cast<T *>(adj.hat[xx]);
+            LayerNext<T> next{static_cast<T *>(adj.hat[1 - xx]), static_cast<T *>(adj.carried), nullptr, nullptr,
+                              tables ? g_layer : nullptr};
+            if (tables) {
+                if (m > 0) next.traj = traj_layer + (m - 1) * kLayerFactors * Lc;
+                else next.pending = static_cast<T *>(adj.pending);
+            }
             // The rows and corrected cells far from the layer on the side stream; on the layer's
-            // stream (the highest priority) the layer's hats of step m, then the rows and cells
-            // that gather them and the layer's own cells.
+            // stream (the highest priority) the rows and cells that gather the layer's hats and
+            // the layer's own cells.
             if (far.special_blocks + far.corrected_blocks)
                 rows_adjoint_kernel<T><<<far.special_blocks + far.corrected_blocks, kBlock, 0, s->side>>>(
                     t, far, lam_next, om_next, tilde, hat, lam_out, om_out, traj_u, traj_w, (uint32_t)m, g[1], g[0],
-                    g[2], g[3], g[4], tilde_out, seg_dloss, segment, m);
+                    g[2], g[3], g[4], tilde_out, seg_dloss, segment, m, next);
             if (layer_blocks) {
-                layer_hat_kernel<T><<<layer_blocks, kBlock, 0, s->layer_stream>>>(
-                    t, lam_next, static_cast<T *>(adj.carried), hat,
-                    tables ? traj_layer + m * kLayerFactors * Lc : nullptr, g_layer);
                 rows_adjoint_kernel<T><<<near.special_blocks + near.corrected_blocks + layer_blocks, kBlock, 0,
                                          s->layer_stream>>>(t, near, lam_next, om_next, tilde, hat, lam_out, om_out,
                                                             traj_u, traj_w, (uint32_t)m, g[1], g[0], g[2], g[3], g[4],
-                                                            tilde_out, seg_dloss, segment, m);
+                                                            tilde_out, seg_dloss, segment, m, next);
                 CUDA_TRY(s, cudaEventRecord(s->joined[2], s->layer_stream));
             }
             CUDA_TRY(s, cudaEventRecord(s->joined[1], s->side));
@@ -1831,6 +1844,13 @@ int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float
         if (P)
             CUDA_TRY(s, cudaMemcpy2DAsync(seg_dloss, sizeof(double) * segment, d_dloss + s0, sizeof(double) * steps,
                                           sizeof(double) * count, P, cudaMemcpyDeviceToDevice, s->stream));
+        // The layer's products of this segment's last step, whose Q^, L^, H^ the segment after
+        // left waiting: its factors are recorded now.
+        if (tables && k + 1 < segments) {
+            layer_pending_kernel<T><<<layer_blocks, kBlock, 0, s->stream>>>(
+                t, static_cast<const T *>(adj.pending), traj_layer + (count - 1) * kLayerFactors * Lc, g_layer);
+            CUDA_TRY(s, cudaGetLastError());
+        }
         if ((rc = run(1, x, reverse, count)) != FDTD_OK) return rc;
         if (count & 1) x = 1 - x;
     }
@@ -1930,7 +1950,7 @@ size_t pool_bytes(const fdtd_solver *s, const AdjointLists &l, uint64_t steps, u
     list(l.layer_read_start.size(), 4), list(l.layer_interior.size(), 1);
     list(l.special_order.size(), 4), list(l.corrected_order.size(), 4);
     const uint64_t Lc = s->layers;
-    if (Lc) total += pool_round(e * 9 * Lc) + pool_round(e * 6 * n);
+    if (Lc) total += pool_round(e * 9 * Lc) + 2 * pool_round(e * 6 * n) + pool_round(e * 9 * Lc);
     total += 2 * (pool_round(e * n) + pool_round(e * S)) + 2 * pool_round(e * K);
     if (segment == 0 || segment > steps) segment = steps;
     const uint64_t segments = (steps + segment - 1) / segment;
@@ -2513,19 +2533,23 @@ int fdtd_autotune(fdtd_solver *s, uint64_t trial_steps, int *layer_per_sm, int *
     CUDA_TRY(s, cudaEventCreate(&end));
     const bool timing = s->timing;
     s->timing = false;
-    // Times trial_steps steps of the handle's present choice (one untimed dispatch first); ms < 0
+    // Times trial_steps steps of the handle's present choice: one untimed dispatch, then the
+    // faster of two timed ones (a single short pass was too noisy to rank close choices); ms < 0
     // when it could not run.
     auto trial = [&](float &ms) -> int {
         ms = -1.0f;
-        for (int pass = 0; pass < 2; ++pass) {
-            if (pass == 1) CUDA_TRY(s, cudaEventRecord(start, s->stream));
+        for (int pass = 0; pass < 3; ++pass) {
+            if (pass > 0) CUDA_TRY(s, cudaEventRecord(start, s->stream));
             const int r = dispatch(s, static_cast<const float *>(sig), trial_steps, static_cast<double *>(rec), trial_steps);
             if (r != FDTD_OK) return r;
             settle(s, trial_steps);
+            if (pass == 0) continue;
+            CUDA_TRY(s, cudaEventRecord(end, s->stream));
+            CUDA_TRY(s, cudaEventSynchronize(end));
+            float t = 0.0f;
+            CUDA_TRY(s, cudaEventElapsedTime(&t, start, end));
+            if (ms < 0.0f || t < ms) ms = t;
         }
-        CUDA_TRY(s, cudaEventRecord(end, s->stream));
-        CUDA_TRY(s, cudaEventSynchronize(end));
-        CUDA_TRY(s, cudaEventElapsedTime(&ms, start, end));
         return FDTD_OK;
     };
     // The sweep's tile shape and planes a tile (the default chunk, a quarter, half and twice it,

@@ -263,7 +263,7 @@ class B200WaveSolver:
         if status != _abi.FDTD_OK:
             _raise(self._lib, status, self._handle)
 
-    def autotune(self, trial_steps: int = 8) -> dict[str, int]:
+    def autotune(self, trial_steps: int = 12) -> dict[str, int]:
         """Chooses the launch shapes for this grid by timing a few steps of each candidate (from
         rest; the state is reset after): the interior sweep's tile shape and planes a tile, then
         the matched-layer and special-row kernels' blocks per multiprocessor. Returns the choice
