@@ -727,7 +727,9 @@ int launch_steps(fdtd_solver *s, const float *d_signal, uint64_t steps, double *
         if (ev) CUDA_TRY(s, cudaEventRecord(ev[3], layer));
         if (ev) CUDA_TRY(s, cudaEventRecord(ev[4], side));
         if (special_blocks) {
-            if (s->link_slots <= 6)
+            if (g.link_mask)
+                special_kernel<T, 0, COMP><<<special_blocks, kBlock, 0, side>>>(g, f);
+            else if (s->link_slots <= 6)
                 special_kernel<T, 6, COMP><<<special_blocks, kBlock, 0, side>>>(g, f);
             else
                 special_kernel<T, 18, COMP><<<special_blocks, kBlock, 0, side>>>(g, f);
@@ -1028,6 +1030,24 @@ int build(fdtd_solver *s, const fdtd_layout *L) {
         g.link_direction = u8;
         if ((rc = upload(s, weight.data(), weight.size(), &fp))) return rc;
         g.link_weight = fp;
+        // Every row's links axial, in the directions' order, of the axial weight: masks.
+        bool axial_rows = K > 0 && L->weight_count >= 1;
+        std::vector<uint8_t> mask(K, 0);
+        for (uint64_t k = 0; k < K && axial_rows; ++k) {
+            int last = -1;
+            for (uint64_t l = L->link_start[k]; l < L->link_start[k + 1] && axial_rows; ++l) {
+                const int d = L->link_direction[l];
+                axial_rows = d < 6 && d > last && std::memcmp(&L->link_weight[l], &L->weights[0], sizeof(float)) == 0;
+                last = d;
+                mask[k] |= (uint8_t)(1u << (d & 7));
+            }
+        }
+        g.link_mask = nullptr;
+        g.link_axial = L->weights[0];
+        if (axial_rows) {
+            if ((rc = upload(s, mask.data(), K, &u8))) return rc;
+            g.link_mask = u8;
+        }
     }
     if ((rc = upload(s, L->coef_a, K, &fp))) return rc;
     g.coef_a = fp;

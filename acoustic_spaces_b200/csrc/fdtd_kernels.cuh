@@ -474,6 +474,11 @@ struct Tables {
     uint32_t link_slots;
     const uint8_t *link_count, *link_direction;
     const float *link_weight, *coef_a, *coef_b, *coef_inv, *source;
+    // Where every row's links are axial, in the directions' order, each of the axial weight (walls
+    // on cell faces without a speed field), each row's links as a mask of the six directions
+    // instead (special_kernel<T, 0>): one byte a row in place of five a link.
+    const uint8_t *link_mask;
+    float link_axial;
     const float *row_residual;  // COMP: each row's constant-mode residual
     const float *state_weight, *state_now, *state_before, *state_gain;
     int32_t offset[18];
@@ -522,25 +527,39 @@ struct Fields {
 template <typename T, int SLOTS, bool COMP>
 __device__ __forceinline__ void special_row(const Tables &g, const Fields<T> &f, const uint32_t k, const uint32_t i) {
     const uint32_t K = g.specials;
-    const uint32_t links = g.link_count[k];
     const T *__restrict__ b = f.b;
-    T value[SLOTS];
-    float weight[SLOTS];
-#pragma unroll
-    for (int l = 0; l < SLOTS; ++l) {
-        value[l] = (T)0;
-        weight[l] = 0.0f;
-        if ((uint32_t)l < links) {
-            const uint32_t at = l * K + k;
-            weight[l] = g.link_weight[at];
-            value[l] = b[(uint32_t)((int64_t)i + g.offset[g.link_direction[at]])];
-        }
-    }
-    const T here = b[i];
     T sum = 0;
+    T here;
+    if constexpr (SLOTS == 0) {
+        // The links as a mask of the axial directions, in their order, each of the axial weight.
+        const uint32_t mask = g.link_mask[k];
+        T value[6];
 #pragma unroll
-    for (int l = 0; l < SLOTS; ++l)
-        if ((uint32_t)l < links) sum += COMP ? (T)weight[l] * (value[l] - here) : (T)weight[l] * value[l];
+        for (int d = 0; d < 6; ++d) value[d] = (mask >> d) & 1u ? b[(uint32_t)((int64_t)i + g.offset[d])] : (T)0;
+        here = b[i];
+        const T w = (T)g.link_axial;
+#pragma unroll
+        for (int d = 0; d < 6; ++d)
+            if ((mask >> d) & 1u) sum += COMP ? w * (value[d] - here) : w * value[d];
+    } else {
+        const uint32_t links = g.link_count[k];
+        T value[SLOTS];
+        float weight[SLOTS];
+#pragma unroll
+        for (int l = 0; l < SLOTS; ++l) {
+            value[l] = (T)0;
+            weight[l] = 0.0f;
+            if ((uint32_t)l < links) {
+                const uint32_t at = l * K + k;
+                weight[l] = g.link_weight[at];
+                value[l] = b[(uint32_t)((int64_t)i + g.offset[g.link_direction[at]])];
+            }
+        }
+        here = b[i];
+#pragma unroll
+        for (int l = 0; l < SLOTS; ++l)
+            if ((uint32_t)l < links) sum += COMP ? (T)weight[l] * (value[l] - here) : (T)weight[l] * value[l];
+    }
     const uint32_t s0 = g.state_start[k], s1 = g.state_start[k + 1];
     T flow = 0;
     for (uint32_t j = s0; j < s1; ++j) {
