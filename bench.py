@@ -105,6 +105,17 @@ def decay_times(p: np.ndarray, rate: float) -> tuple[float, float]:
     return out[0], out[1]
 
 
+def apply_launch(solver, launch) -> None:
+    """Gives `solver` the launch choice `launch` (an autotuned solver's `launch` of the same grid)."""
+    if not launch:
+        return
+    if "tile_shape" in launch:
+        solver.set_tiles(launch["tile_shape"], launch["tile_planes"])
+    solver.set_launch(launch["layer_blocks_per_sm"], launch["special_blocks_per_sm"])
+    if "concurrent" in launch:
+        solver.set_streams(bool(launch["concurrent"]))
+
+
 def ir_errors(p32: np.ndarray, p64: np.ndarray, rate: float) -> dict:
     """FP32 against FP64 impulse responses (probes, steps): the relative L2 error of each receiver,
     and of its energy-decay curve (Schroeder's backward integral) the largest difference in dB
@@ -867,6 +878,7 @@ def main() -> None:
     parser.add_argument("--gradient-segment", type=int, default=50)
     parser.add_argument("--no-fp64-rate", action="store_true", help="skip timing the FP64 stepper alike")
     parser.add_argument("--launch", default="", help="layer,special blocks per SM (skips the autotuner)")
+    parser.add_argument("--tiles", default="", help="with --launch: the sweep's tile shape,planes a tile")
     parser.add_argument("--slab-count", type=int, default=0,
                         help="with --slabs on one GPU: this many slabs stepped together in one process")  # fmt: skip
     parser.add_argument("--slabs", action="store_true",
@@ -939,6 +951,10 @@ def main() -> None:
     if args.launch:
         solver = B200WaveSolver(workload.built.layout, precision=args.precision, device=local, autotune=False)
         solver.set_launch(*(int(v) for v in args.launch.split(",")))
+        if args.tiles:
+            solver.set_tiles(*(int(v) for v in args.tiles.split(",")))
+        solver.launch = {**solver.tiles(), "layer_blocks_per_sm": int(args.launch.split(",")[0]),
+                         "special_blocks_per_sm": int(args.launch.split(",")[1])}  # fmt: skip
     else:
         solver = B200WaveSolver(workload.built.layout, precision=args.precision, device=local)
     handle_s = time.perf_counter() - t_setup
@@ -1075,7 +1091,7 @@ def main() -> None:
         try:
             g_steps = min(args.gradient_steps, len(signal))
             grad_solver = B200WaveSolver(workload.built.layout, device=local, autotune=False)
-            grad_solver.launch = solver.launch
+            apply_launch(grad_solver, solver.launch)
             head = np.ascontiguousarray(signal[:g_steps])
             y = grad_solver.run(head)
             dloss = 2.0 * (y - 0.9 * y)
