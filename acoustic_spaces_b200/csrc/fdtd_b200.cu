@@ -123,13 +123,13 @@ struct fdtd_solver {
     void *u[2] = {nullptr, nullptr};
     void *w[2] = {nullptr, nullptr};
     void *increment = nullptr;              // FDTD_FP32_COMPENSATED: p_n - p_(n-1) per cell (pitched)
-    void *layer_parts = nullptr;            // the layer's cells' parts p_x, p_y, p_z, kPartStride a cell
     std::vector<uint32_t> layer_cells;      // pitched, in the layout's order (for fdtd_read_state)
     const uint8_t *types_device = nullptr;  // the pitched cell types
     const float *scale_device = nullptr;    // with a speed field: each pitched cell's scale
-    // Per axis, the velocity on each cell's + face (pitched, only the layer's faces used), in two
-    // buffers: faces[1] holds the latest values between runs, as u[1] does.
-    void *faces[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
+    // The matched layer's state (kLayerSlots values a pitched cell: its parts and the velocities on
+    // its + faces; only the layer's cells and their - faces used), in two buffers: layer_state[1]
+    // holds the latest values between runs, as u[1] does.
+    void *layer_state[2] = {nullptr, nullptr};
     uint32_t link_slots = 0;  // the most links of a special row (6 or 18 kernels)
     // Moving air (fdtd_flow.cuh): whether the grid's air moves, which form carries it, the carry's
     // cell lists, fields and stage buffers, and its launches' blocks.
@@ -567,11 +567,8 @@ Fields<T> fields_for(const fdtd_solver *s, bool flip) {
     f.wb = static_cast<const T *>(s->w[cur]);
     f.wa = static_cast<T *>(s->w[prev]);
     f.d = static_cast<T *>(s->increment);
-    f.layer_parts = static_cast<T *>(s->layer_parts);
-    for (int axis = 0; axis < 3; ++axis) {
-        f.face_old[axis] = static_cast<const T *>(s->faces[cur][axis]);
-        f.face_new[axis] = static_cast<T *>(s->faces[prev][axis]);
-    }
+    f.cell_old = static_cast<const T *>(s->layer_state[cur]);
+    f.cell_new = static_cast<T *>(s->layer_state[prev]);
     return f;
 }
 
@@ -791,7 +788,7 @@ void settle(fdtd_solver *s, uint64_t steps) {
         s->flipped = !s->flipped;
         std::swap(s->u[0], s->u[1]);
         std::swap(s->w[0], s->w[1]);
-        for (int axis = 0; axis < 3; ++axis) std::swap(s->faces[0][axis], s->faces[1][axis]);
+        std::swap(s->layer_state[0], s->layer_state[1]);
         std::swap(s->map_b[0], s->map_b[1]);
         std::swap(s->map_a[0], s->map_a[1]);
     }
@@ -945,12 +942,10 @@ int build(fdtd_solver *s, const fdtd_layout *L) {
         if ((rc = zeros(s, e * s->n_device, &s->u[k]))) return rc;
         if ((rc = zeros(s, e * L->state_count, &s->w[k]))) return rc;
     }
-    if ((rc = zeros(s, e * kPartStride * L->layer_count, &s->layer_parts))) return rc;
     if (s->precision == FDTD_FP32_COMPENSATED && (rc = zeros(s, e * s->n_device, &s->increment))) return rc;
     if (L->layer_count)
         for (int k = 0; k < 2; ++k)
-            for (int axis = 0; axis < 3; ++axis)
-                if ((rc = zeros(s, e * s->n_device, &s->faces[k][axis]))) return rc;
+            if ((rc = zeros(s, e * kLayerSlots * s->n_device, &s->layer_state[k]))) return rc;
     void *flag;
     if ((rc = zeros(s, sizeof(unsigned int), &flag))) return rc;
     s->d_error = static_cast<unsigned int *>(flag);
@@ -1581,12 +1576,11 @@ struct Kept {
 };
 
 // A checkpoint of the state between runs: the current and the previous level, the current and
-// the previous branch velocities, and with a matched layer its pressure parts and the current
-// faces (faces[1]).
+// the previous branch velocities, and with a matched layer its current state (layer_state[1]).
 uint64_t checkpoint_bytes(const fdtd_solver *s) {
     const uint64_t e = s->precision == FDTD_FP64 ? 8 : 4;
     uint64_t bytes = 2 * e * s->n_device + 2 * e * s->states;
-    if (s->layers) bytes += kPartStride * e * s->layers + 3 * e * s->n_device;
+    if (s->layers) bytes += kLayerSlots * e * s->n_device;
     return bytes;
 }
 
@@ -1600,12 +1594,7 @@ int save_checkpoint(fdtd_solver *s, char *c) {
         CUDA_TRY(s, cudaMemcpyAsync(c + states, s->w[0], states, cudaMemcpyDeviceToDevice, s->stream));
     }
     c += 2 * states;
-    if (s->layers) {
-        CUDA_TRY(s, cudaMemcpyAsync(c, s->layer_parts, kPartStride * e * s->layers, cudaMemcpyDeviceToDevice, s->stream));
-        c += kPartStride * e * s->layers;
-        for (int axis = 0; axis < 3; ++axis, c += level)
-            CUDA_TRY(s, cudaMemcpyAsync(c, s->faces[1][axis], level, cudaMemcpyDeviceToDevice, s->stream));
-    }
+    if (s->layers) CUDA_TRY(s, cudaMemcpyAsync(c, s->layer_state[1], kLayerSlots * level, cudaMemcpyDeviceToDevice, s->stream));
     return FDTD_OK;
 }
 
@@ -1619,12 +1608,7 @@ int restore_checkpoint(fdtd_solver *s, const char *c) {
         CUDA_TRY(s, cudaMemcpyAsync(s->w[0], c + states, states, cudaMemcpyDeviceToDevice, s->stream));
     }
     c += 2 * states;
-    if (s->layers) {
-        CUDA_TRY(s, cudaMemcpyAsync(s->layer_parts, c, kPartStride * e * s->layers, cudaMemcpyDeviceToDevice, s->stream));
-        c += kPartStride * e * s->layers;
-        for (int axis = 0; axis < 3; ++axis, c += level)
-            CUDA_TRY(s, cudaMemcpyAsync(s->faces[1][axis], c, level, cudaMemcpyDeviceToDevice, s->stream));
-    }
+    if (s->layers) CUDA_TRY(s, cudaMemcpyAsync(s->layer_state[1], c, kLayerSlots * level, cudaMemcpyDeviceToDevice, s->stream));
     return FDTD_OK;
 }
 
@@ -2724,12 +2708,8 @@ int fdtd_reset(fdtd_solver *s) {
         if (s->states) CUDA_TRY(s, cudaMemsetAsync(s->w[k], 0, e * s->states, s->stream));
     }
     if (s->increment) CUDA_TRY(s, cudaMemsetAsync(s->increment, 0, e * s->n_device, s->stream));
-    if (s->layers) {
-        CUDA_TRY(s, cudaMemsetAsync(s->layer_parts, 0, e * kPartStride * s->layers, s->stream));
-        for (int k = 0; k < 2; ++k)
-            for (int axis = 0; axis < 3; ++axis)
-                CUDA_TRY(s, cudaMemsetAsync(s->faces[k][axis], 0, e * s->n_device, s->stream));
-    }
+    if (s->layers)
+        for (int k = 0; k < 2; ++k) CUDA_TRY(s, cudaMemsetAsync(s->layer_state[k], 0, e * kLayerSlots * s->n_device, s->stream));
     CUDA_TRY(s, cudaStreamSynchronize(s->stream));
     s->steps_done = 0;
     return FDTD_OK;
@@ -2792,19 +2772,17 @@ int fdtd_read_state(const fdtd_solver *cs, void *current, void *previous, void *
         // The reference's nine values per cell (fdtd.hpp:2245): the parts, then per axis the
         // velocity of the - face (the + face of the cell below) and of the + face.
         const std::vector<uint32_t> &cells = s->layer_cells;
-        std::vector<char> parts(e * kPartStride * s->layers);
-        CUDA_TRY(s, cudaMemcpy(parts.data(), s->layer_parts, parts.size(), cudaMemcpyDeviceToHost));
+        std::vector<char> state(e * kLayerSlots * s->n_device);
+        CUDA_TRY(s, cudaMemcpy(state.data(), s->layer_state[1], state.size(), cudaMemcpyDeviceToHost));
         char *dst = static_cast<char *>(layer_state);
-        for (uint64_t c = 0; c < s->layers; ++c)
-            for (int k = 0; k < 3; ++k) std::memcpy(dst + e * (9 * c + k), parts.data() + e * (kPartStride * c + k), e);
-        std::vector<char> face(e * s->n_device);
         const uint64_t strides[3] = {1, s->pitch, s->pitch * s->ny};
-        for (int axis = 0; axis < 3; ++axis) {
-            CUDA_TRY(s, cudaMemcpy(face.data(), s->faces[1][axis], face.size(), cudaMemcpyDeviceToHost));
-            for (uint64_t c = 0; c < s->layers; ++c) {
-                const uint64_t i = cells[c];
-                std::memcpy(dst + e * (9 * c + 3 + 2 * axis), face.data() + e * (i - strides[axis]), e);
-                std::memcpy(dst + e * (9 * c + 4 + 2 * axis), face.data() + e * i, e);
+        for (uint64_t c = 0; c < s->layers; ++c) {
+            const uint64_t i = cells[c];
+            for (int k = 0; k < 3; ++k) std::memcpy(dst + e * (9 * c + k), state.data() + e * (kLayerSlots * i + k), e);
+            for (int axis = 0; axis < 3; ++axis) {
+                const uint64_t below = kLayerSlots * (i - strides[axis]) + 3 + axis, own = kLayerSlots * i + 3 + axis;
+                std::memcpy(dst + e * (9 * c + 3 + 2 * axis), state.data() + e * below, e);
+                std::memcpy(dst + e * (9 * c + 4 + 2 * axis), state.data() + e * own, e);
             }
         }
     }

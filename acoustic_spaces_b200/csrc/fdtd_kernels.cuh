@@ -33,9 +33,10 @@ namespace fdtd {
 
 constexpr int kSolid = 0, kInterior = 1, kSpecial = 2, kLayer = 3;
 constexpr int kBlock = 128;  // threads per block of every kernel
-// A matched-layer cell's three pressure parts sit together, padded to four (one 16-byte load and
-// store a cell in FP32, two in FP64): one stream of memory for the parts, not three.
-constexpr int kPartStride = 4;
+// A matched-layer cell's state — its three pressure parts and the velocities on its three + faces —
+// sits together, six values a cell in a pitched array (two such arrays, the state a step before and
+// the new one): one stream of memory for the state in place of nine.
+constexpr int kLayerSlots = 6;
 
 // ---- the bulk sweep's tiles ------------------------------------------------------------------
 constexpr int kHX = 4;                          // x halo of the pressure tile: 16 bytes of floats
@@ -505,9 +506,11 @@ struct Fields {
     const T *b;        // the current pressure
     T *wa;             // branch velocities a step before, overwritten with the next
     const T *wb;       // current branch velocities
-    T *layer_parts;    // per layer cell c, its pressure parts p_x, p_y, p_z at kPartStride c + axis
-    const T *face_old[3];  // per axis, the velocity on each cell's + face (pitched), a step before
-    T *face_new[3];        // the same, this step
+    // The matched layer's state, kLayerSlots values a (pitched) cell: at kLayerSlots i + axis the
+    // layer cell's pressure part along that axis, at kLayerSlots i + 3 + axis the velocity on its
+    // + face along it (also kept at a cell outside the layer whose + face is a layer cell's - face).
+    const T *cell_old;  // a step before
+    T *cell_new;        // this step
     const float *signal;  // the step's drive at signal[0]
     double *out;       // probe p's record at out[p * out_stride]
     uint64_t out_stride;
@@ -628,22 +631,22 @@ __device__ __forceinline__ void layer_cell(const Tables &g, const Fields<T> &f, 
     const uint32_t at[3] = {r - y * g.pitch, y, z};
     const uint32_t strides[3] = {1u, g.pitch, g.plane};
     const T *__restrict__ b = f.b;
-    T *__restrict__ parts = f.layer_parts;
+    using V2 = typename Pair<T>::type;
     T part[3], lo[3], hi[3], old_below[3], old_above[3];
     float4 c0[3], c1[3];
     {
-        using V2 = typename Pair<T>::type;
-        const V2 *own = reinterpret_cast<const V2 *>(parts + (uint64_t)kPartStride * c);
-        const V2 p01 = own[0], p2 = own[1];
-        part[0] = p01.x, part[1] = p01.y, part[2] = p2.x;
+        // the cell's own state in three vector loads: parts x, y; part z, face x; faces y, z
+        const V2 *own = reinterpret_cast<const V2 *>(f.cell_old + (uint64_t)kLayerSlots * i);
+        const V2 s0 = own[0], s1 = own[1], s2 = own[2];
+        part[0] = s0.x, part[1] = s0.y, part[2] = s1.x;
+        old_above[0] = s1.y, old_above[1] = s2.x, old_above[2] = s2.y;
     }
 #pragma unroll
     for (int axis = 0; axis < 3; ++axis) {
         const uint32_t stride = strides[axis];
         lo[axis] = b[i - stride];
         hi[axis] = b[i + stride];
-        old_below[axis] = __ldg(f.face_old[axis] + (i - stride));
-        old_above[axis] = __ldg(f.face_old[axis] + i);
+        old_below[axis] = f.cell_old[(uint64_t)kLayerSlots * (i - stride) + 3 + axis];
         c0[axis] = __ldg(g.layer_coef[axis] + at[axis]);
         c1[axis] = __ldg(g.layer_coef[axis] + at[axis] + 1);
     }
@@ -681,19 +684,16 @@ __device__ __forceinline__ void layer_cell(const Tables &g, const Fields<T> &f, 
         }
         total += part[axis];
     }
-#pragma unroll
-    for (int axis = 0; axis < 3; ++axis) {
-        f.face_new[axis][i] = above[axis];
-        // The cell below owns the face when it is in the layer.
-        if (!(shared_below & (1u << axis))) f.face_new[axis][i - strides[axis]] = below[axis];
-    }
     {
-        using V2 = typename Pair<T>::type;
-        V2 *own = reinterpret_cast<V2 *>(parts + (uint64_t)kPartStride * c);
-        V2 p01, p2;
-        p01.x = part[0], p01.y = part[1], p2.x = part[2], p2.y = (T)0;
-        own[0] = p01, own[1] = p2;
+        V2 *own = reinterpret_cast<V2 *>(f.cell_new + (uint64_t)kLayerSlots * i);
+        V2 s0, s1, s2;
+        s0.x = part[0], s0.y = part[1], s1.x = part[2], s1.y = above[0], s2.x = above[1], s2.y = above[2];
+        own[0] = s0, own[1] = s1, own[2] = s2;
     }
+    // The cell below owns the face when it is in the layer; else this cell keeps it there.
+#pragma unroll
+    for (int axis = 0; axis < 3; ++axis)
+        if (!(shared_below & (1u << axis))) f.cell_new[(uint64_t)kLayerSlots * (i - strides[axis]) + 3 + axis] = below[axis];
     if (COMP) {
         f.a[i] = here + total;
         f.d[i] = total;  // (read by no update; it keeps the state's level before readable)
