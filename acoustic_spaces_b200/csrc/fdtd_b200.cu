@@ -46,6 +46,7 @@ constexpr int kSteps[18][3] = {
     {-1, 0, 1},  {1, 0, 1},  {0, -1, -1}, {0, 1, -1}, {0, -1, 1},  {0, 1, 1}};
 
 constexpr uint64_t kPitchCells = 16;  // rows padded to a multiple of 16 cells
+constexpr uint64_t kFineX = 32, kFineY = 16;  // the blocks tile_list counts interior cells in
 constexpr uint64_t kGraphSteps = 64;  // steps of fdtd_run's captured chunk (even: the roles return)
 // Grids of at least this many (pitched) cells step by direct launches in fdtd_run: their steps are
 // long enough (a quarter of a millisecond and more) that launching costs nothing, and replaying a
@@ -110,6 +111,10 @@ struct fdtd_solver {
     int bulk_shape = 0;
     uint64_t bulk_chunk = 32;
     std::vector<uint8_t> host_types;
+    // The interior cells of each kFineX x kFineY block of each plane (tile_list's counts), and
+    // the blocks along x and y.
+    std::vector<uint32_t> fine_count;
+    uint64_t fine_x = 0, fine_y = 0;
     void *tiles_device = nullptr;
     const int4 *plain_tiles = nullptr;
     uint32_t plain_count = 0;
@@ -472,15 +477,36 @@ int tile_list(fdtd_solver *s, int shape, uint64_t chunk, bool flags, std::vector
     const uint64_t nz = s->nz, nx = s->nx, ny = s->ny, pitch = s->pitch;
     const uint64_t tiles_x = (bk.x1 - bk.xa + TX - 1) / TX, tiles_y = (bk.y1 - bk.y0 + TY - 1) / TY;
     const uint64_t columns = tiles_x * tiles_y;
+    // The interior cells of each block of kFineX x kFineY cells of each plane, counted once for the
+    // handle (its cell types never change): every shape's tile is a whole number of such blocks.
+    if (s->fine_count.empty()) {
+        s->fine_x = (bk.x1 - bk.xa + kFineX - 1) / kFineX, s->fine_y = (bk.y1 - bk.y0 + kFineY - 1) / kFineY;
+        s->fine_count.assign(s->fine_x * s->fine_y * nz, 0);
+        for (uint64_t z = bk.z0; z < bk.z1; ++z)
+            for (uint64_t y = bk.y0; y < bk.y1; ++y) {
+                const uint8_t *row = &s->host_types[pitch * (y + ny * z)];
+                uint32_t *fine = &s->fine_count[((y - bk.y0) / kFineY * s->fine_x) * nz + z];
+                for (uint64_t x0 = bk.xa; x0 < bk.x1; x0 += kFineX) {
+                    uint32_t n = 0;
+                    for (uint64_t x = x0, x1 = std::min<uint64_t>(x0 + kFineX, bk.x1); x < x1; ++x) n += row[x] == kInterior;
+                    fine[(x0 - bk.xa) / kFineX * nz] += n;
+                }
+            }
+    }
+    static_assert(kFineX == 32 && kFineY == 16, "the shapes' tiles are whole blocks of 32 x 16 cells");
+    const uint64_t per_x = TX / kFineX, per_y = TY / kFineY;
     // Per column and plane: interior cells it holds.
     std::vector<uint32_t> count(columns * nz, 0);
-    for (uint64_t z = bk.z0; z < bk.z1; ++z)
-        for (uint64_t y = bk.y0; y < bk.y1; ++y) {
-            const uint8_t *row = &s->host_types[pitch * (y + ny * z)];
-            const uint64_t base = ((y - bk.y0) / TY * tiles_x) * nz + z;
-            for (uint64_t x = bk.xa; x < bk.x1; ++x)
-                if (row[x] == kInterior) ++count[base + (x - bk.xa) / TX * nz];
-        }
+    for (uint64_t c = 0; c < columns; ++c) {
+        const uint64_t tx = c % tiles_x, ty = c / tiles_x;
+        for (uint64_t b = 0; b < per_y; ++b)
+            for (uint64_t a = 0; a < per_x; ++a) {
+                const uint64_t fx = tx * per_x + a, fy = ty * per_y + b;
+                if (fx >= s->fine_x || fy >= s->fine_y) continue;
+                const uint32_t *fine = &s->fine_count[(fy * s->fine_x + fx) * nz];
+                for (uint64_t z = bk.z0; z < bk.z1; ++z) count[c * nz + z] += fine[z];
+            }
+    }
     list.clear();
     for (uint64_t c = 0; c < columns; ++c) {
         const uint64_t xt = bk.xa + (c % tiles_x) * TX, yt = bk.y0 + (c / tiles_x) * TY;
