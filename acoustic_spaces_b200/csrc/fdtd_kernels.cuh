@@ -323,7 +323,7 @@ __global__ void __launch_bounds__(SH::THREADS) bulk_kernel(const __grid_constant
 #pragma unroll
                 for (int r = 0; r < SH::ROWS; ++r) {
                     const int yl = r0 + r;
-                    if constexpr (SH::COLS == 2 && !WIDE && !COMP) {
+                    if constexpr (SH::COLS == 2 && !WIDE) {
                         // Two cells side by side: the pair's pressures, previous pressures, scales
                         // and neighbours above, below, z-1 and z+1 each as one vector load (even
                         // offsets: the tile's x start, the halo and the pitch are even), and the
@@ -340,6 +340,37 @@ __global__ void __launch_bounds__(SH::THREADS) bulk_kernel(const __grid_constant
                         const V2 zm = *reinterpret_cast<const V2 *>(bm + q);
                         const V2 zp = *reinterpret_cast<const V2 *>(bp + q);
                         const V2 pv = *reinterpret_cast<const V2 *>(pa + c);
+                        T *out = a + (row0 + (uint32_t)r * p.pitch);
+                        if constexpr (COMP) {
+                            // pv holds the pair's increments; the neighbours as differences, in the
+                            // sum's order; the new pressures and increments as one vector store each.
+                            const T sum0 = (left - h.x) + (h.y - h.x) + (up.x - h.x) + (dn.x - h.x) + (zm.x - h.x) +
+                                           (zp.x - h.x);
+                            const T sum1 = (h.x - h.y) + (right - h.y) + (up.y - h.y) + (dn.y - h.y) + (zm.y - h.y) +
+                                           (zp.y - h.y);
+                            T d0, d1;
+                            if (SCALED) {
+                                const float2 sv = *reinterpret_cast<const float2 *>(ps + c);
+                                const T s0 = (T)sv.x, s1 = (T)sv.y;
+                                d0 = pv.x + (s0 * axial) * sum0 + (s0 * residual) * h.x;
+                                d1 = pv.y + (s1 * axial) * sum1 + (s1 * residual) * h.y;
+                            } else {
+                                d0 = pv.x + axial * sum0 + residual * h.x;
+                                d1 = pv.y + axial * sum1 + residual * h.y;
+                            }
+                            T *dout = dd + (row0 + (uint32_t)r * p.pitch);
+                            if (in0 && in1) {
+                                V2 v, w;
+                                v.x = h.x + d0, v.y = h.y + d1, w.x = d0, w.y = d1;
+                                *reinterpret_cast<V2 *>(out) = v;
+                                *reinterpret_cast<V2 *>(dout) = w;
+                            } else if (in0) {
+                                out[0] = h.x + d0, dout[0] = d0;
+                            } else {
+                                out[1] = h.y + d1, dout[1] = d1;
+                            }
+                            continue;
+                        }
                         const T sum0 = left + h.y + up.x + dn.x + zm.x + zp.x;
                         const T sum1 = h.x + right + up.y + dn.y + zm.y + zp.y;
                         T n0, n1;
@@ -352,7 +383,6 @@ __global__ void __launch_bounds__(SH::THREADS) bulk_kernel(const __grid_constant
                             n0 = centre * h.x + axial * sum0 - pv.x;
                             n1 = centre * h.y + axial * sum1 - pv.y;
                         }
-                        T *out = a + (row0 + (uint32_t)r * p.pitch);
                         if (in0 && in1) {
                             V2 v;
                             v.x = n0, v.y = n1;
