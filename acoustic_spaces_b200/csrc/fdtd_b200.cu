@@ -97,9 +97,10 @@ struct fdtd_solver {
     // Blocks an SM of the matched-layer and special-row kernels (0: one thread a cell), chosen by
     // fdtd_autotune.
     int layer_per_sm = kLayerPerSm, special_per_sm = kSpecialPerSm;
-    // Whether a step's kernels run beside one another on the three streams (1) or one after
-    // another on the handle's stream (0): where the special rows are many, running them beside
-    // the sweep can cost the sweep more than it saves (fdtd_autotune times both).
+    // How a step's kernels share the streams (fdtd_set_streams): 1, each kind on its own; 2, the
+    // layer and then the special rows beside the sweep; 3, the special rows after the sweep, the
+    // layer beside them; 0, all in turn (fdtd_autotune times them: where the special rows are many,
+    // running them beside the sweep can cost the sweep more than it saves).
     int concurrent = 1;
     uint32_t bulk_tiles = 0;
     int bulk_per_sm = 0;      // resident bulk blocks per multiprocessor (shape 0)
@@ -679,8 +680,13 @@ int launch_steps(fdtd_solver *s, const float *d_signal, uint64_t steps, double *
     // side stream. The three write disjoint memory; each step starts when all three have ended the
     // step before. While timing, all run one after another on the handle's stream, so that each
     // kernel's events bracket that kernel alone.
-    const bool fork = !s->timing && s->concurrent;
-    cudaStream_t side = fork ? s->side : s->stream, layer = fork ? s->layer_stream : s->stream;
+    // The streams (fdtd_set_streams): 1, the three kinds each on its own; 2, the layer and then the
+    // special rows and probes on the side stream beside the sweep; 3, the special rows and probes
+    // after the sweep on its stream, the layer beside them; 0, all in turn.
+    const int mode = s->timing ? 0 : s->concurrent;
+    const bool fork = mode != 0;
+    cudaStream_t side = mode == 1 || mode == 2 ? s->side : s->stream;
+    cudaStream_t layer = mode == 1 || mode == 3 ? s->layer_stream : (mode == 2 ? s->side : s->stream);
     for (uint64_t k = 0; k < steps; ++k) {
         const bool flip = (k & 1) != 0;
         Fields<T> f = fields_for<T>(s, flip);
@@ -2532,7 +2538,8 @@ int fdtd_set_streams(fdtd_solver *s, int concurrent) {
     if (!s) return set_global(FDTD_EINVAL, "no solver");
     DeviceGuard guard(s->device);
     for (cudaStream_t stream : {s->stream, s->side, s->layer_stream}) CUDA_TRY(s, cudaStreamSynchronize(stream));
-    s->concurrent = concurrent ? 1 : 0;
+    if (concurrent < 0 || concurrent > 3) return fail(s, FDTD_EINVAL, "the streams' arrangement is 0 to 3");
+    s->concurrent = concurrent;
     // The captured chunks and the gradient's graphs hold the old streams' order.
     Kept{s}.drop_graphs();
     for (cudaGraphExec_t &g : s->graph)
@@ -2609,7 +2616,7 @@ int fdtd_autotune(fdtd_solver *s, uint64_t trial_steps, int *layer_per_sm, int *
     auto tune_launch = [&]() -> int {
         float best = -1.0f;
         int r = FDTD_OK;
-        for (int c : {1, 0}) {
+        for (int c : {1, 2, 3, 0}) {
             s->concurrent = c;
             for (int l : layers) {
                 if (r != FDTD_OK) break;

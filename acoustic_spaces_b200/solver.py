@@ -285,10 +285,12 @@ class B200WaveSolver:
                 "tile_planes": int(t.planes), "tiles": int(t.tiles), "tile_blocks_per_sm": t.blocks_per_sm,
                 "tile_threads": t.threads, "tile_cols": t.cols, "concurrent": t.concurrent}  # fmt: skip
 
-    def set_streams(self, concurrent: bool) -> None:
-        """A step's kernels beside one another on three streams (True) or in turn on one (False), as
-        :meth:`autotune` may choose; results are the same to the bit."""
-        status = self._lib.fdtd_set_streams(self._handle, int(bool(concurrent)))
+    def set_streams(self, concurrent: int) -> None:
+        """How a step's kernels share the streams, as :meth:`autotune` may choose (1 or True: each
+        kind on its own; 2: the layer and then the special rows beside the sweep; 3: the special rows
+        after the sweep, the layer beside them; 0 or False: all in turn); results are the same to
+        the bit."""
+        status = self._lib.fdtd_set_streams(self._handle, int(concurrent))
         if status != _abi.FDTD_OK:
             _raise(self._lib, status, self._handle)
         self.launch = {**(getattr(self, "launch", None) or {}), **self.tiles()}

@@ -113,7 +113,7 @@ def apply_launch(solver, launch) -> None:
         solver.set_tiles(launch["tile_shape"], launch["tile_planes"])
     solver.set_launch(launch["layer_blocks_per_sm"], launch["special_blocks_per_sm"])
     if "concurrent" in launch:
-        solver.set_streams(bool(launch["concurrent"]))
+        solver.set_streams(int(launch["concurrent"]))
 
 
 def ir_errors(p32: np.ndarray, p64: np.ndarray, rate: float) -> dict:

@@ -261,7 +261,7 @@ typedef struct fdtd_tiles {
     uint64_t planes;    /* planes of a tile, at most (a tile marches them along z) */
     uint32_t tiles;     /* tiles, one block each */
     int blocks_per_sm;  /* resident blocks of the sweep a multiprocessor */
-    int concurrent;     /* 1: a step's kernels beside one another on three streams; 0: in turn */
+    int concurrent;     /* how a step's kernels share the streams (fdtd_set_streams: 0 to 3) */
     int threads;        /* threads a block of the sweep */
     int cols;           /* adjacent columns a thread (1, or 2: the 7-point stencil a pair at a time) */
 } fdtd_tiles;
@@ -278,10 +278,12 @@ int fdtd_set_tiles(fdtd_solver *solver, int shape, uint64_t planes);
 int fdtd_get_tiles(const fdtd_solver *solver, fdtd_tiles *out);
 
 /*
- * Whether a step's kernels run beside one another — the interior sweep on the handle's stream,
- * the matched layer and the special rows on streams of their own (concurrent 1, the default) — or
- * one after another on the handle's stream (0), as fdtd_autotune may choose (no counterpart in
- * the reference). Results are the same to the bit. Waits for the handle's work.
+ * How a step's kernels share the streams, as fdtd_autotune may choose (no counterpart in the
+ * reference): 1 (the default), the interior sweep on the handle's stream, the matched layer and the
+ * special rows (with the probes) on streams of their own; 2, the layer and then the special rows
+ * on one stream beside the sweep; 3, the special rows after the sweep on the handle's stream, the
+ * layer beside them; 0, all one after another on the handle's stream. Results are the same to
+ * the bit. FDTD_EINVAL outside 0 to 3. Waits for the handle's work.
  */
 int fdtd_set_streams(fdtd_solver *solver, int concurrent);
 

@@ -281,3 +281,24 @@ def test_gpu_steps_a_layout_without_probes_as_the_oracle_does():
     sa, sb = gpu.state(), oracle.state()
     for key in sa:
         assert np.array_equal(sa[key], sb[key]), key
+
+
+@pytest.mark.parametrize("name", ["fitted_open", "open_layer_speed"])
+def test_gpu_every_stream_arrangement_steps_as_the_reference_does(name):
+    # The step's kernels on three streams, on two (the layer then the special rows beside the
+    # sweep; or the special rows after the sweep, the layer beside them) and on one: each gives the
+    # reference's series to the bit, also when the arrangement changes between runs.
+    layout, signal, reference = load_golden(name)
+    for mode in (0, 1, 2, 3):
+        gpu = B200WaveSolver(layout)
+        gpu.set_streams(mode)
+        assert gpu.tiles()["concurrent"] == mode
+        assert np.array_equal(_pieces(gpu, signal, [0, 65, 130, len(signal)]), reference), mode
+    gpu = B200WaveSolver(layout)
+    pieces = []
+    for (a, b), mode in zip([(0, 99), (99, 230), (230, len(signal))], [2, 3, 0]):
+        gpu.set_streams(mode)
+        pieces.append(gpu.run(signal[a:b]))
+    assert np.array_equal(np.concatenate(pieces, axis=1), reference)
+    with pytest.raises(ValueError, match="0 to 3"):
+        gpu.set_streams(4)
