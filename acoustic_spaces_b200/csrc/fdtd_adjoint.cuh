@@ -79,7 +79,8 @@ struct AdjointTables {
     const uint8_t *layer_interior;
     // The layer's terms on a cell's adjoint (layer_terms): bit 2a, the cell below along axis a is a
     // layer cell; bit 2a + 1, the cell above; bit 6, the cell itself. Per special row, per
-    // corrected cell (0 where no layer cell is near) and per layer cell.
+    // corrected cell (0 where no layer cell is near) and per layer cell (whose bit 7 says that rows
+    // link to it or probes read it).
     const uint8_t *special_layer_mask, *corrected_layer_mask, *layer_mask;
     // The special rows and the corrected cells in an order that puts first those whose update
     // gathers none of the layer's terms (special_far of the rows, corrected_far of the cells):
@@ -365,11 +366,15 @@ __device__ __forceinline__ void layer_adjoint_cell(const AdjointTables &t, uint3
     for (int d = 0; d < 6; ++d)
         if (inner & (1u << d)) sum += lam_next[(uint32_t)((int64_t)i + t.offset[d])];
     T value = (T)t.axial * sum;
-    for (uint32_t e = t.layer_from_start[c], end = t.layer_from_start[c + 1]; e < end; ++e)
-        value += (T)t.layer_from_coef[e] * tilde[t.layer_from_row[e]];
-    value += layer_terms<T>(t, hat, i, t.layer_mask[c]);
-    const double probed = probe_terms(t, t.layer_read_start[c], t.layer_read_start[c + 1], dloss, stride, step);
-    if (probed != 0.0) value += (T)probed;
+    const uint32_t mask = t.layer_mask[c];
+    if (mask & 128u)  // rows linking to the cell, or probes reading it
+        for (uint32_t e = t.layer_from_start[c], end = t.layer_from_start[c + 1]; e < end; ++e)
+            value += (T)t.layer_from_coef[e] * tilde[t.layer_from_row[e]];
+    value += layer_terms<T>(t, hat, i, mask & 127u);
+    if (mask & 128u) {
+        const double probed = probe_terms(t, t.layer_read_start[c], t.layer_read_start[c + 1], dloss, stride, step);
+        if (probed != 0.0) value += (T)probed;
+    }
     lam_out[i] = value;
     layer_hat_cell<T>(t, c, i, value, next.carried, next.hat, next.traj, next.g, next.pending);
 }

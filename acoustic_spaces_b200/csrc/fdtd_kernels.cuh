@@ -129,6 +129,11 @@ struct Stage {
     static constexpr uint32_t smem = SH::STAGES * bytes + 8 * SH::STAGES;  // + the stages' mbarriers
 };
 
+// (The adjoint's sweep steps the forward's list of shape 0 with shape 7's pairs: the same tile.)
+static_assert(Shape7::TX == Shape0::TX && Shape7::TY == Shape0::TY && Shape7::STAGES == Shape0::STAGES &&
+                  Shape7::THREADS == Shape0::THREADS,
+              "shapes 0 and 7 share their tiles and stages");
+
 // A tile list entry's w holds z_end, with this bit set when every cell of the tile, in every one
 // of its planes, is interior: its planes' stages then carry no cell types.
 constexpr int kFullTile = 1 << 30;
