@@ -222,15 +222,19 @@ __device__ __forceinline__ void special_adjoint_row(const AdjointTables &t, uint
 // traj[f * layers + c]: q, hi' - lo', hi, b_(i+st) - b_i, lo, b_i - b_(i-st) for axis 0, then 1, 2.
 constexpr int kLayerFactors = 18;
 
-// The carried values (9 per cell: Q^' x3, L^' x3, H^' x3, at carried[v * layers + c]) are
-// updated in place; hat[(2a) * cells + i] = pf[x] L^ and hat[(2a + 1) * cells + i] = pf[x+1] H^ are
-// the terms' factors its neighbours gather. A cell's hats of step n depend only on its own adjoint
+// The carried values (9 per cell, together: Q^' x3, L^' x3, H^' x3 at carried[kCarried c + v]) are
+// updated in place; the hats, together per pitched cell too, hat[kHats i + 2a] = pf[x] L^ and
+// hat[kHats i + 2a + 1] = pf[x+1] H^, are the terms' factors its neighbours gather (a cell's state in
+// one stream of memory, not fifteen). A cell's hats of step n depend only on its own adjoint
 // of level n + 1 and its carried values, so the thread that forms that adjoint (the layer cell's
 // reverse step n + 1, layer_adjoint_cell) forms the hats of step n right after, into the other of
 // two hat buffers: the layer takes one launch a reverse step, not two. The tables' gradient sums
 // g[(6a + f) * layers + c] the products of Q^, H^, L^ with the forward's factors of step n (`traj`,
 // layer_cell's records); where step n's factors are not recorded yet (step n ends the segment
 // before, recomputed later), Q^, L^, H^ wait in `pending` (9 per cell) for layer_pending_kernel.
+constexpr int kCarried = 10;  // a layer cell's carried values, padded to an even count (vector loads)
+constexpr int kHats = 6;      // a pitched cell's hats
+
 template <typename T>
 __device__ __forceinline__ void layer_hat_cell(const AdjointTables &t, uint32_t c, uint32_t i, T lam, T *carried, T *hat,
                                                const T *traj, double *g, T *pending) {
@@ -238,18 +242,27 @@ __device__ __forceinline__ void layer_hat_cell(const AdjointTables &t, uint32_t 
     const uint32_t z = t.by_plane(i), r = i - z * t.plane, y = t.by_pitch(r);
     const uint32_t at[3] = {r - y * t.pitch, y, z};
     const T s = t.layer_scale ? (T)t.layer_scale[c] : (T)1;
+    using V2 = typename Pair<T>::type;
+    V2 *own = reinterpret_cast<V2 *>(carried + (uint64_t)kCarried * c);
+    T cv[kCarried];
+#pragma unroll
+    for (int v = 0; v < kCarried / 2; ++v) {
+        const V2 p = own[v];
+        cv[2 * v] = p.x, cv[2 * v + 1] = p.y;
+    }
+    T hv[kHats];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         const float4 c0 = __ldg(t.layer_coef[a] + at[a]), c1 = __ldg(t.layer_coef[a] + at[a] + 1);
         const T ps = t.layer_scale ? (T)c0.y * s : (T)c0.y;
-        const T q_hat = lam + carried[(uint64_t)a * L + c];
-        const T lo_hat = ps * q_hat + carried[(uint64_t)(3 + a) * L + c];
-        const T hi_hat = -ps * q_hat + carried[(uint64_t)(6 + a) * L + c];
-        carried[(uint64_t)a * L + c] = (T)c0.x * q_hat;
-        carried[(uint64_t)(3 + a) * L + c] = (T)c0.z * lo_hat;
-        carried[(uint64_t)(6 + a) * L + c] = (T)c1.z * hi_hat;
-        hat[(uint64_t)(2 * a) * t.cells + i] = (T)c0.w * lo_hat;
-        hat[(uint64_t)(2 * a + 1) * t.cells + i] = (T)c1.w * hi_hat;
+        const T q_hat = lam + cv[a];
+        const T lo_hat = ps * q_hat + cv[3 + a];
+        const T hi_hat = -ps * q_hat + cv[6 + a];
+        cv[a] = (T)c0.x * q_hat;
+        cv[3 + a] = (T)c0.z * lo_hat;
+        cv[6 + a] = (T)c1.z * hi_hat;
+        hv[2 * a] = (T)c0.w * lo_hat;
+        hv[2 * a + 1] = (T)c1.w * hi_hat;
         if (g && traj) {
             const T *f = traj + (uint64_t)(6 * a) * L + c;
             double *gg = g + (uint64_t)(6 * a) * L + c;
@@ -264,6 +277,20 @@ __device__ __forceinline__ void layer_hat_cell(const AdjointTables &t, uint32_t 
             pending[(uint64_t)(3 * a + 1) * L + c] = lo_hat;
             pending[(uint64_t)(3 * a + 2) * L + c] = hi_hat;
         }
+    }
+    cv[kCarried - 1] = (T)0;
+#pragma unroll
+    for (int v = 0; v < kCarried / 2; ++v) {
+        V2 p;
+        p.x = cv[2 * v], p.y = cv[2 * v + 1];
+        own[v] = p;
+    }
+    V2 *hats = reinterpret_cast<V2 *>(hat + (uint64_t)kHats * i);
+#pragma unroll
+    for (int v = 0; v < kHats / 2; ++v) {
+        V2 p;
+        p.x = hv[2 * v], p.y = hv[2 * v + 1];
+        hats[v] = p;
     }
 }
 
@@ -330,12 +357,12 @@ __device__ __forceinline__ T layer_terms(const AdjointTables &t, const T *hat, u
     const uint32_t strides[3] = {1u, t.pitch, t.plane};
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        if (mask & (1u << (2 * a))) sum -= hat[(uint64_t)(2 * a + 1) * t.cells + (j - strides[a])];
-        if (mask & (1u << (2 * a + 1))) sum += hat[(uint64_t)(2 * a) * t.cells + (j + strides[a])];
+        if (mask & (1u << (2 * a))) sum -= hat[(uint64_t)kHats * (j - strides[a]) + 2 * a + 1];
+        if (mask & (1u << (2 * a + 1))) sum += hat[(uint64_t)kHats * (j + strides[a]) + 2 * a];
     }
     if (mask & 64u) {
 #pragma unroll
-        for (int a = 0; a < 3; ++a) sum += hat[(uint64_t)(2 * a + 1) * t.cells + j] - hat[(uint64_t)(2 * a) * t.cells + j];
+        for (int a = 0; a < 3; ++a) sum += hat[(uint64_t)kHats * j + 2 * a + 1] - hat[(uint64_t)kHats * j + 2 * a];
     }
     return sum;
 }

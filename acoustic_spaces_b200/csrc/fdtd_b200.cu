@@ -70,7 +70,7 @@ struct AdjointState {
     void *tilde[2] = {nullptr, nullptr};  // L~ of the level at hand, and of the next (alternating)
     CUtensorMap lam_b[2], lam_a[2];
     void *carried = nullptr;  // the matched layer's carried values (9 per cell)
-    void *hat[2] = {nullptr, nullptr};  // the matched layer's terms' factors (6 pitched levels), a step's and the next's
+    void *hat[2] = {nullptr, nullptr};  // the matched layer's terms' factors (kHats a pitched cell), a step's and the next's
     void *pending = nullptr;  // the layer's Q^, L^, H^ of a step whose factors come with the next segment
     // The layer cells sorted by their coordinate along each axis in turn (x, then y, then z; each
     // a permutation of the cells) and each coordinate's first entry: the tables' sums by coordinate.
@@ -1516,9 +1516,9 @@ int place_adjoint(fdtd_solver *s, const AdjointLists &l, Pool &pool, AdjointStat
     if ((rc = place(s, pool, l.corrected_order, &t.corrected_order))) return rc;
     t.special_far = l.special_far, t.corrected_far = l.corrected_far;
     if (s->layers) {
-        if ((rc = pool.take(e * 9 * s->layers, &a.carried, true))) return rc;
+        if ((rc = pool.take(e * kCarried * s->layers, &a.carried, true))) return rc;
         for (int k = 0; k < 2; ++k)
-            if ((rc = pool.take(e * 6 * s->n_device, &a.hat[k], true))) return rc;
+            if ((rc = pool.take(e * kHats * s->n_device, &a.hat[k], true))) return rc;
         if ((rc = pool.take(e * 9 * s->layers, &a.pending, true))) return rc;
         if ((rc = place(s, pool, l.by_coord, &a.by_coord))) return rc;
         if ((rc = place(s, pool, l.coord_start, &a.coord_start))) return rc;
@@ -1733,8 +1733,8 @@ int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float
     }
     // (The layer's hats of the first reverse step are those of rest: zero.)
     if (Lc) {
-        CUDA_TRY(s, cudaMemsetAsync(adj.carried, 0, e * 9 * Lc, s->stream));
-        for (int k = 0; k < 2; ++k) CUDA_TRY(s, cudaMemsetAsync(adj.hat[k], 0, e * 6 * s->n_device, s->stream));
+        CUDA_TRY(s, cudaMemsetAsync(adj.carried, 0, e * kCarried * Lc, s->stream));
+        for (int k = 0; k < 2; ++k) CUDA_TRY(s, cudaMemsetAsync(adj.hat[k], 0, e * kHats * s->n_device, s->stream));
     }
     const AdjointTables &t = adj.t;
     const uint32_t row_blocks = (uint32_t)((std::max<uint64_t>(std::max<uint64_t>(K, S), 1) + kBlock - 1) / kBlock);
@@ -1992,7 +1992,7 @@ size_t pool_bytes(const fdtd_solver *s, const AdjointLists &l, uint64_t steps, u
     list(l.layer_read_start.size(), 4), list(l.layer_interior.size(), 1);
     list(l.special_order.size(), 4), list(l.corrected_order.size(), 4);
     const uint64_t Lc = s->layers;
-    if (Lc) total += pool_round(e * 9 * Lc) + 2 * pool_round(e * 6 * n) + pool_round(e * 9 * Lc);
+    if (Lc) total += pool_round(e * kCarried * Lc) + 2 * pool_round(e * kHats * n) + pool_round(e * 9 * Lc);
     total += 2 * (pool_round(e * n) + pool_round(e * S)) + 2 * pool_round(e * K);
     if (segment == 0 || segment > steps) segment = steps;
     const uint64_t segments = (steps + segment - 1) / segment;
