@@ -313,6 +313,7 @@ SIGNATURES = {
     ),
     "fdtd_layer_gradient": (ctypes.c_int, [ctypes.c_void_p, _f64p]),
     "fdtd_set_gradient_tables": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "fdtd_set_adjoint_launch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
     "fdtd_set_tape_budget": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
     "fdtd_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_int),
                                      ctypes.POINTER(ctypes.c_int)]),

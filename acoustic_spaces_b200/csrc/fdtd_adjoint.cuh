@@ -414,7 +414,8 @@ __device__ __forceinline__ void layer_adjoint_cell(const AdjointTables &t, uint3
 struct RowsPart {
     uint32_t special_begin, special_end, special_blocks;
     uint32_t corrected_begin, corrected_end, corrected_blocks;
-    bool layer;
+    uint32_t layer_blocks;  // 0: no layer cells in this launch
+    __host__ __device__ uint32_t blocks() const { return special_blocks + corrected_blocks + layer_blocks; }
 };
 
 template <typename T>
@@ -425,7 +426,8 @@ __global__ void __launch_bounds__(kBlock) rows_adjoint_kernel(const AdjointTable
                                                               double *g_cb, double *g_now, double *g_before,
                                                               double *g_gain, T *tilde_out, const double *dloss,
                                                               uint64_t stride, uint64_t step, const LayerNext<T> next) {
-    const uint32_t b = blockIdx.x;
+    // (The launch may hold fewer blocks than the part's work: each takes blocks' worth in turn.)
+    for (uint32_t b = blockIdx.x; b < part.blocks(); b += gridDim.x) {
     if (b < part.special_blocks) {
         const uint32_t e = part.special_begin + b * kBlock + threadIdx.x;
         if (e < part.special_end)
@@ -435,9 +437,10 @@ __global__ void __launch_bounds__(kBlock) rows_adjoint_kernel(const AdjointTable
         const uint32_t e = part.corrected_begin + (b - part.special_blocks) * kBlock + threadIdx.x;
         if (e < part.corrected_end)
             correct_cell<T>(t, t.corrected_order[e], lam_next, tilde, hat, lam_out, dloss, stride, step);
-    } else if (part.layer) {
+    } else {
         layer_adjoint_cell<T>(t, (b - part.special_blocks - part.corrected_blocks) * kBlock + threadIdx.x, lam_next,
                               tilde, hat, lam_out, dloss, stride, step, next);
+    }
     }
 }
 

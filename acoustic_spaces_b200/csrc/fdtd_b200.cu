@@ -97,6 +97,9 @@ struct fdtd_solver {
     // Blocks an SM of the matched-layer and special-row kernels (0: one thread a cell), chosen by
     // fdtd_autotune.
     int layer_per_sm = kLayerPerSm, special_per_sm = kSpecialPerSm;
+    // Blocks an SM of the reverse step's launches of the rows far from the layer and of those near
+    // it with the layer's cells (0: a block for every 128 items; fdtd_set_adjoint_launch).
+    int adjoint_far_per_sm = 0, adjoint_near_per_sm = 0;
     // How a step's kernels share the streams (fdtd_set_streams): 1, each kind on its own; 2, the
     // layer and then the special rows beside the sweep; 3, the special rows after the sweep, the
     // layer beside them; 0, all in turn (fdtd_autotune times them: where the special rows are many,
@@ -1741,9 +1744,16 @@ int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float
     const uint32_t layer_blocks = (uint32_t)((Lc + kBlock - 1) / kBlock);
     auto blocks_of = [](uint32_t count) { return (count + kBlock - 1) / kBlock; };
     // (Without a layer every row and cell is far from it.)
-    const RowsPart far{0, t.special_far, blocks_of(t.special_far), 0, t.corrected_far, blocks_of(t.corrected_far), false};
+    const RowsPart far{0, t.special_far, blocks_of(t.special_far), 0, t.corrected_far, blocks_of(t.corrected_far), 0};
     const RowsPart near{t.special_far, (uint32_t)K, blocks_of((uint32_t)K - t.special_far),
-                        t.corrected_far, t.corrected, blocks_of(t.corrected - t.corrected_far), true};
+                        t.corrected_far, t.corrected, blocks_of(t.corrected - t.corrected_far), layer_blocks};
+    // Each launch's blocks, at most the handle's count an SM (fdtd_set_adjoint_launch; 0: a block
+    // for every 128 items).
+    auto capped = [&](uint32_t blocks, int per_sm) {
+        return per_sm > 0 ? std::min<uint32_t>(blocks, (uint32_t)(s->sms * per_sm)) : blocks;
+    };
+    const uint32_t far_grid = capped(far.blocks(), s->adjoint_far_per_sm);
+    const uint32_t near_grid = capped(near.blocks(), s->adjoint_near_per_sm);
     const uint32_t smem = s->scaled ? Stage<T, true>::smem : Stage<T, false>::smem;
     int x = 0;  // lam[x], om[x]: level n+1; lam[1-x], om[1-x]: level n+2, then level n
     // A segment's recomputation (the dispatch of its steps, recording the special rows), and its
@@ -1782,13 +1792,12 @@ int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float
             // The rows and corrected cells far from the layer on the side stream; on the layer's
             // stream (the highest priority) the rows and cells that gather the layer's hats and
             // the layer's own cells.
-            if (far.special_blocks + far.corrected_blocks)
-                rows_adjoint_kernel<T><<<far.special_blocks + far.corrected_blocks, kBlock, 0, s->side>>>(
+            if (far.blocks())
+                rows_adjoint_kernel<T><<<far_grid, kBlock, 0, s->side>>>(
                     t, far, lam_next, om_next, tilde, hat, lam_out, om_out, traj_u, traj_w, (uint32_t)m, g[1], g[0],
                     g[2], g[3], g[4], tilde_out, seg_dloss, segment, m, next);
             if (layer_blocks) {
-                rows_adjoint_kernel<T><<<near.special_blocks + near.corrected_blocks + layer_blocks, kBlock, 0,
-                                         s->layer_stream>>>(t, near, lam_next, om_next, tilde, hat, lam_out, om_out,
+                rows_adjoint_kernel<T><<<near_grid, kBlock, 0, s->layer_stream>>>(t, near, lam_next, om_next, tilde, hat, lam_out, om_out,
                                                             traj_u, traj_w, (uint32_t)m, g[1], g[0], g[2], g[3], g[4],
                                                             tilde_out, seg_dloss, segment, m, next);
                 CUDA_TRY(s, cudaEventRecord(s->joined[2], s->layer_stream));
@@ -2537,6 +2546,17 @@ int fdtd_get_tiles(const fdtd_solver *s, fdtd_tiles *out) {
     out->concurrent = s->concurrent;
     out->threads = kShapeInfo[s->bulk_shape].threads;
     out->cols = kShapeInfo[s->bulk_shape].cols;
+    return FDTD_OK;
+}
+
+int fdtd_set_adjoint_launch(fdtd_solver *s, int far_per_sm, int near_per_sm) {
+    if (!s) return set_global(FDTD_EINVAL, "no solver");
+    if (far_per_sm < 0 || near_per_sm < 0 || far_per_sm > 32 || near_per_sm > 32)
+        return fail(s, FDTD_EINVAL, "blocks an SM are 0 to 32");
+    DeviceGuard guard(s->device);
+    CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+    s->adjoint_far_per_sm = far_per_sm, s->adjoint_near_per_sm = near_per_sm;
+    Kept{s}.drop_graphs();  // the gradient's graphs hold the old launches
     return FDTD_OK;
 }
 

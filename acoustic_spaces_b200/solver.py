@@ -285,6 +285,13 @@ class B200WaveSolver:
                 "tile_planes": int(t.planes), "tiles": int(t.tiles), "tile_blocks_per_sm": t.blocks_per_sm,
                 "tile_threads": t.threads, "tile_cols": t.cols, "concurrent": t.concurrent}  # fmt: skip
 
+    def set_adjoint_launch(self, far_blocks_per_sm: int, near_blocks_per_sm: int) -> None:
+        """Blocks an SM of the gradient's reverse-step launches (0: one a 128 items); results are
+        the same to the bit."""
+        status = self._lib.fdtd_set_adjoint_launch(self._handle, int(far_blocks_per_sm), int(near_blocks_per_sm))
+        if status != _abi.FDTD_OK:
+            _raise(self._lib, status, self._handle)
+
     def set_streams(self, concurrent: int) -> None:
         """How a step's kernels share the streams, as :meth:`autotune` may choose (1 or True: each
         kind on its own; 2: the layer and then the special rows beside the sweep; 3: the special rows

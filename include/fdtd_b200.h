@@ -288,6 +288,14 @@ int fdtd_get_tiles(const fdtd_solver *solver, fdtd_tiles *out);
 int fdtd_set_streams(fdtd_solver *solver, int concurrent);
 
 /*
+ * The gradient's reverse step: at most `far_per_sm` blocks an SM for its launch of the special rows
+ * and corrected cells far from the matched layer, `near_per_sm` for its launch of the rest and the
+ * layer's cells (0: a block for every 128 of them; no counterpart in the reference). Fewer blocks
+ * let the launches run beside one another and the interior sweep. Results are the same to the bit.
+ */
+int fdtd_set_adjoint_launch(fdtd_solver *solver, int far_per_sm, int near_per_sm);
+
+/*
  * The device address and size of plane z of the current (which 0) or previous (1) pressure level
  * between runs (no counterpart in the reference): pitch * ny elements, contiguous, pitch the row
  * length rounded up to 16 cells. A grid split into slabs of planes across ranks exchanges its
