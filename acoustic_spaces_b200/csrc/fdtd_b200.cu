@@ -98,8 +98,10 @@ struct fdtd_solver {
     // fdtd_autotune.
     int layer_per_sm = kLayerPerSm, special_per_sm = kSpecialPerSm;
     // Blocks an SM of the reverse step's launches of the rows far from the layer and of those near
-    // it with the layer's cells (0: a block for every 128 items; fdtd_set_adjoint_launch).
-    int adjoint_far_per_sm = 0, adjoint_near_per_sm = 0;
+    // it with the layer's cells (0: a block for every 128 items; fdtd_set_adjoint_launch). Measured
+    // on the 4 cm room's gradient: 0 and 8 took 99 ms for 200 reverse steps, 0 and 0 102.5 ms, and
+    // any cap on the far rows more (106-257 ms).
+    int adjoint_far_per_sm = 0, adjoint_near_per_sm = 8;
     // How a step's kernels share the streams (fdtd_set_streams): 1, each kind on its own; 2, the
     // layer and then the special rows beside the sweep; 3, the special rows after the sweep, the
     // layer beside them; 0, all in turn (fdtd_autotune times them: where the special rows are many,

@@ -169,3 +169,23 @@ def test_the_layer_damping_gradient_on_the_gpu_matches_central_differences():
     measured = (loss(damping + h) - loss(damping - h)) / (2.0 * h)
     assert abs(measured) > 0.0
     assert abs(predicted - measured) <= 2e-3 * abs(measured), (predicted, measured)
+
+
+def test_the_reverse_steps_launch_caps_leave_the_gradient_unchanged():
+    # Bounded grids for the reverse step's rows launches (each block taking blocks' worth of rows
+    # in turn) give the same gradient to the bit, tables included.
+    layout, signal, _ = load_golden("fitted_open")
+    signal = signal[:100]
+    target, _ = _problem(layout, signal)
+    solver = B200WaveSolver(layout, precision="fp32")
+    y = solver.run(signal)
+    solver.reset()
+    dloss = 2.0 * (y - target)
+    plain = solver.gradient(signal, dloss, segment=30)
+    for far, near in [(1, 1), (2, 8), (4, 16)]:
+        solver.set_adjoint_launch(far, near)
+        capped = solver.gradient(signal, dloss, segment=30)
+        for key in plain:
+            np.testing.assert_array_equal(capped[key], plain[key], err_msg=f"{key} {far} {near}")
+    with pytest.raises(ValueError, match="0 to 32"):
+        solver.set_adjoint_launch(-1, 4)
