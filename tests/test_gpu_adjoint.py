@@ -154,7 +154,7 @@ def test_the_autograd_function_gives_the_material_gradient():
     loss.backward()
     ours = np.concatenate([conductance.grad.numpy(), corner.grad.numpy()])
     expected_loss, expected = f.loss_and_gradient(params, "fp64")
-    assert abs(float(loss) - expected_loss) <= 1e-12 * expected_loss
+    assert abs(float(loss.detach()) - expected_loss) <= 1e-12 * expected_loss
     np.testing.assert_allclose(ours, expected, rtol=1e-9, atol=1e-12 * np.abs(expected).max())
 
 
