@@ -326,6 +326,8 @@ SIGNATURES = {
     "fdtd_set_tiles": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_uint64]),
     "fdtd_get_tiles": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(FdtdTiles)]),
     "fdtd_set_streams": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "fdtd_set_layer_tangent": (ctypes.c_int, [ctypes.c_void_p, _f64p, ctypes.c_uint64]),
+    "fdtd_layer_tangent_gradient": (ctypes.c_int, [ctypes.c_void_p, _f64p]),
     "fdtd_level_plane": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int,
                                         ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_uint64)]),
     "fdtd_test_wait": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32]),

@@ -87,6 +87,10 @@ struct AdjointTables {
     // those step back beside the layer's kernels, the others after the layer's hats.
     const uint32_t *special_order, *corrected_order;
     uint32_t special_far, corrected_far;
+    // A gradient along a tangent of the layer's tables (fdtd_set_layer_tangent): each layer cell's
+    // axes of tangent factors and its first factor in a step's (as the forward's Tables holds them).
+    const uint8_t *tangent_axes;
+    const uint32_t *tangent_start;
 };
 
 // The trajectory of a run: level l of the special rows' pressure at traj_u[l * specials + k] and
@@ -235,9 +239,33 @@ constexpr int kLayerFactors = 18;
 constexpr int kCarried = 10;  // a layer cell's carried values, padded to an even count (vector loads)
 constexpr int kHats = 6;      // a pitched cell's hats
 
+// Along a tangent of the tables (d/dθ of each entry, θ a parameter such as the layer's damping) the
+// gradient's step is the tables' products summed with the tangent:
+//   dL/dθ += Q^ (q k'[x] - s (hi' - lo') p'[x]) + H^ (hi kf'[x+1] - (b_(i+st) - b_i) pf'[x+1])
+//          + L^ (lo kf'[x] - (b_i - b_(i-st)) pf'[x])
+// per axis along which the tangent touches the cell: the forward records the three bracketed
+// factors (layer_cell's traj_tangent), and each cell keeps its own sum over the steps in double
+// (`acc`), summed over the cells in a fixed order at the end (layer_tangent_sum_kernel).
+template <typename T>
+__device__ __forceinline__ double tangent_products(const AdjointTables &t, uint32_t c, const T *factors, const T (&q)[3],
+                                                   const T (&lo)[3], const T (&hi)[3]) {
+    const uint32_t axes = t.tangent_axes[c];
+    uint32_t slot = t.tangent_start[c];
+    double sum = 0.0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        if (!(axes & (1u << a))) continue;
+        const T *ff = factors + slot;
+        slot += 3;
+        sum += (double)q[a] * (double)ff[0] + (double)hi[a] * (double)ff[1] + (double)lo[a] * (double)ff[2];
+    }
+    return sum;
+}
+
 template <typename T>
 __device__ __forceinline__ void layer_hat_cell(const AdjointTables &t, uint32_t c, uint32_t i, T lam, T *carried, T *hat,
-                                               const T *traj, double *g, T *pending) {
+                                               const T *traj, double *g, T *pending, const T *tangent = nullptr,
+                                               double *acc = nullptr) {
     const uint32_t L = t.layers;
     const uint32_t z = t.by_plane(i), r = i - z * t.plane, y = t.by_pitch(r);
     const uint32_t at[3] = {r - y * t.pitch, y, z};
@@ -251,6 +279,7 @@ __device__ __forceinline__ void layer_hat_cell(const AdjointTables &t, uint32_t 
         cv[2 * v] = p.x, cv[2 * v + 1] = p.y;
     }
     T hv[kHats];
+    T qs[3], los[3], his[3];  // (the tangent's products)
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         const float4 c0 = __ldg(t.layer_coef[a] + at[a]), c1 = __ldg(t.layer_coef[a] + at[a] + 1);
@@ -258,6 +287,7 @@ __device__ __forceinline__ void layer_hat_cell(const AdjointTables &t, uint32_t 
         const T q_hat = lam + cv[a];
         const T lo_hat = ps * q_hat + cv[3 + a];
         const T hi_hat = -ps * q_hat + cv[6 + a];
+        qs[a] = q_hat, los[a] = lo_hat, his[a] = hi_hat;
         cv[a] = (T)c0.x * q_hat;
         cv[3 + a] = (T)c0.z * lo_hat;
         cv[6 + a] = (T)c1.z * hi_hat;
@@ -278,6 +308,7 @@ __device__ __forceinline__ void layer_hat_cell(const AdjointTables &t, uint32_t 
             pending[(uint64_t)(3 * a + 2) * L + c] = hi_hat;
         }
     }
+    if (tangent && acc) acc[c] += tangent_products<T>(t, c, tangent, qs, los, his);
     cv[kCarried - 1] = (T)0;
 #pragma unroll
     for (int v = 0; v < kCarried / 2; ++v) {
@@ -316,6 +347,42 @@ __global__ void __launch_bounds__(kBlock) layer_pending_kernel(const AdjointTabl
         gg[(uint64_t)4 * L] += (double)lo_hat * (double)f[(uint64_t)4 * L];
         gg[(uint64_t)5 * L] += -(double)lo_hat * (double)f[(uint64_t)5 * L];
     }
+}
+
+// The tangent's products of a step whose Q^, L^, H^ waited in `pending`, once its factors are
+// recorded.
+template <typename T>
+__global__ void __launch_bounds__(kBlock) layer_pending_tangent_kernel(const AdjointTables t, const T *pending,
+                                                                       const T *factors, double *acc) {
+    const uint32_t c = blockIdx.x * kBlock + threadIdx.x;
+    const uint32_t L = t.layers;
+    if (c >= L) return;
+    T q[3], lo[3], hi[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        q[a] = pending[(uint64_t)(3 * a) * L + c];
+        lo[a] = pending[(uint64_t)(3 * a + 1) * L + c];
+        hi[a] = pending[(uint64_t)(3 * a + 2) * L + c];
+    }
+    acc[c] += tangent_products<T>(t, c, factors, q, lo, hi);
+}
+
+// The cells' sums along the tangent, summed in a fixed order: block b sums cells b * span ..
+// (b + 1) * span - 1, each thread a strided share in order, then the shares in a fixed tree, into
+// out[b]; a last launch of one block with `span` = the first's blocks sums those.
+__global__ void __launch_bounds__(kBlock) layer_tangent_sum_kernel(const double *acc, uint64_t count, uint64_t span,
+                                                                   double *out) {
+    __shared__ double part[kBlock];
+    const uint64_t begin = (uint64_t)blockIdx.x * span, end = begin + span < count ? begin + span : count;
+    double sum = 0.0;
+    for (uint64_t e = begin + threadIdx.x; e < end; e += kBlock) sum += acc[e];
+    part[threadIdx.x] = sum;
+    __syncthreads();
+    for (int half = kBlock / 2; half > 0; half /= 2) {
+        if ((int)threadIdx.x < half) part[threadIdx.x] += part[threadIdx.x + half];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[blockIdx.x] = part[0];
 }
 
 // The tables' gradient per coordinate, in a fixed order: block b sums the six products of the
@@ -370,11 +437,17 @@ __device__ __forceinline__ T layer_terms(const AdjointTables &t, const T *hat, u
 // The layer's part of a reverse step: where its hats of the step before go (`next`, the other hat
 // buffer), its carried values, and the tables' sums with the factors of that step (`traj`, or null
 // with `pending` where they are not recorded yet; both null for a gradient without the tables).
+// Along a tangent (`acc` not null): the factors of that step at *tangent_base + tangent_offset
+// (the base in device memory, so that a captured reverse step serves every segment), or with
+// `pending` none yet.
 template <typename T>
 struct LayerNext {
     T *hat, *carried, *pending;
     const T *traj;
     double *g;
+    const T *const *tangent_base = nullptr;
+    uint64_t tangent_offset = 0;
+    double *acc = nullptr;
 };
 
 // A layer cell's adjoint: its interior neighbours' axial x lam (with a speed field their stored
@@ -403,7 +476,8 @@ __device__ __forceinline__ void layer_adjoint_cell(const AdjointTables &t, uint3
         if (probed != 0.0) value += (T)probed;
     }
     lam_out[i] = value;
-    layer_hat_cell<T>(t, c, i, value, next.carried, next.hat, next.traj, next.g, next.pending);
+    const T *tangent = next.acc && !next.pending ? *next.tangent_base + next.tangent_offset : nullptr;
+    layer_hat_cell<T>(t, c, i, value, next.carried, next.hat, next.traj, next.g, next.pending, tangent, next.acc);
 }
 
 // One launch of the special rows' adjoint (the rows special_order[begin .. end), on the first

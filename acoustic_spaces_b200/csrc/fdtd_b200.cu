@@ -174,6 +174,20 @@ struct fdtd_solver {
     // The last gradient's part in the matched layer's tables (fdtd_layer_gradient), empty without.
     std::vector<double> layer_gradient;
     bool gradient_tables = true;  // whether gradients also give the layer tables' (fdtd_set_gradient_tables)
+    // A tangent of the layer's tables (fdtd_set_layer_tangent): gradients then give dL/dθ along it in
+    // place of the tables' gradient. Its factors a step (three per layer cell and axis it touches),
+    // the device tables it uses (freed when replaced), the last gradient's value, and a taped run's
+    // factors of every step beside the rows' trajectory (tape_t, with room for tape_t_steps steps;
+    // stage_t: a captured chunk's, copied onto the tape after it).
+    bool tangent = false;
+    uint64_t tangent_factors = 0;
+    std::vector<void *> tangent_device;
+    bool tangent_valid = false;
+    double tangent_gradient = 0.0;
+    void *record_tangent = nullptr;  // while recording: the factors of a dispatch's first step
+    void *tape_t = nullptr, *stage_t = nullptr;
+    uint64_t tape_t_steps = 0;
+    bool tape_tangent = false;  // the valid tape holds the tangent's factors of every step
     uint64_t branches = 0;
     // fdtd_gradient's device workspace, kept and handed out again in the same order while the
     // sizes asked for stay the same (a fit's iterations then allocate nothing).
@@ -705,6 +719,8 @@ int launch_steps(fdtd_solver *s, const float *d_signal, uint64_t steps, double *
         }
         // The matched layer's factors of step k (the gradient's recomputation).
         if (s->record_layer) f.traj_layer = static_cast<T *>(s->record_layer) + k * kLayerFactors * s->layers;
+        // The factors of step k along the tables' tangent (a gradient's recomputation, or a taped run).
+        if (s->record_tangent) f.traj_tangent = static_cast<T *>(s->record_tangent) + k * s->tangent_factors;
         if (fork) {
             if (k > 0) {
                 CUDA_TRY(s, cudaStreamWaitEvent(s->stream, s->joined[1], 0));
@@ -1653,12 +1669,17 @@ int restore_checkpoint(fdtd_solver *s, const char *c) {
     return FDTD_OK;
 }
 
+// One word of device memory set in stream order (a captured graph reads it when it runs).
+__global__ void set_address_kernel(const void **slot, const void *value) { *slot = value; }
+
 // Whether the handle holds the tape of a run of this drive with these segments: gradient<T> then
 // takes the tape's checkpoints or trajectory and recomputes no forward pass of its own.
-// (A trajectory holds no matched layer's factors: a gradient in the layer's tables recomputes.)
+// (A trajectory holds no matched layer's tables' factors: a gradient in the layer's tables
+// recomputes; one along a tangent of the tables needs the tangent's factors on the tape.)
 bool holds_tape(const fdtd_solver *s, const float *signal, uint64_t steps, uint64_t segment) {
     if (segment == 0 || segment > steps) segment = steps;
-    if (s->tape_traj && s->layers && s->gradient_tables) return false;
+    if (s->tape_traj && s->layers && s->gradient_tables && !s->tangent) return false;
+    if (s->tape_traj && s->layers && s->tangent && !s->tape_tangent) return false;
     return s->tape_valid && s->tape_signal.size() == steps && std::min<uint64_t>(s->tape_segment, steps) == segment &&
            std::memcmp(s->tape_signal.data(), signal, sizeof(float) * steps) == 0;
 }
@@ -1702,7 +1723,8 @@ int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float
     const uint64_t level_bytes = e * s->n_device, state_bytes = e * S;
     // The matched layer: its factors of each step of a segment, and its gradient's sums per cell.
     const uint64_t Lc = s->layers;
-    const bool tables = Lc && s->gradient_tables;
+    const bool tangent = Lc && s->tangent;  // along a tangent of the tables, in place of the tables
+    const bool tables = Lc && s->gradient_tables && !tangent;
     T *traj_layer = nullptr;
     double *g_layer = nullptr, *table_sums = nullptr;
     const uint64_t coords = s->nx + s->ny + s->nz;
@@ -1718,6 +1740,26 @@ int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float
     // or, when the handle holds the tape of a run of this drive with these segments, its states.
     const bool taped = holds_tape(s, signal, steps, segment);
     const bool trajectory = taped && s->tape_traj;  // the tape holds every level: nothing to recompute
+    // Along a tangent: one segment's factors (unless the tape holds every step's), each cell's sum
+    // over the steps, the sums' partial and whole totals, and the device word that holds where the
+    // factors of a segment start (a captured reverse step reads it).
+    const uint64_t Tf = s->tangent_factors;
+    T *traj_tan = nullptr;
+    double *tan_acc = nullptr, *tan_parts = nullptr;
+    const T **tan_base = nullptr;
+    const uint32_t tan_blocks = (uint32_t)std::min<uint64_t>(256, std::max<uint64_t>(1, (Lc + kBlock - 1) / kBlock));
+    if (tangent) {
+        if (!trajectory) {
+            if ((rc = scratch.take(e * Tf * segment, &p))) return rc;
+            traj_tan = static_cast<T *>(p);
+        }
+        if ((rc = scratch.take(sizeof(double) * Lc, &p))) return rc;
+        tan_acc = static_cast<double *>(p);
+        if ((rc = scratch.take(sizeof(double) * (tan_blocks + 1), &p))) return rc;
+        tan_parts = static_cast<double *>(p);
+        if ((rc = scratch.take(sizeof(void *), &p))) return rc;
+        tan_base = static_cast<const T **>(p);
+    }
     std::vector<char *> checkpoints;
     if (taped && !trajectory)
         for (uint64_t k = 0; k + 1 < segments; ++k) checkpoints.push_back(static_cast<char *>(s->tape_checkpoints[k]));
@@ -1741,7 +1783,8 @@ int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float
         CUDA_TRY(s, cudaMemsetAsync(adj.carried, 0, e * kCarried * Lc, s->stream));
         for (int k = 0; k < 2; ++k) CUDA_TRY(s, cudaMemsetAsync(adj.hat[k], 0, e * kHats * s->n_device, s->stream));
     }
-    const AdjointTables &t = adj.t;
+    AdjointTables t = adj.t;
+    t.tangent_axes = s->tables.tangent_axes, t.tangent_start = s->tables.tangent_start;
     const uint32_t row_blocks = (uint32_t)((std::max<uint64_t>(std::max<uint64_t>(K, S), 1) + kBlock - 1) / kBlock);
     const uint32_t layer_blocks = (uint32_t)((Lc + kBlock - 1) / kBlock);
     auto blocks_of = [](uint32_t count) { return (count + kBlock - 1) / kBlock; };
@@ -1763,8 +1806,9 @@ int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float
     auto recompute = [&](uint64_t count) -> int {
         s->record_u = traj_u, s->record_w = traj_w, s->record_offset = 2, s->record_probes = false;
         s->record_layer = tables ? traj_layer : nullptr;
+        s->record_tangent = tangent ? traj_tan : nullptr;
         const int r = dispatch(s, seg_signal, count, d_out, segment);
-        s->record_u = s->record_w = s->record_layer = nullptr, s->record_probes = true;
+        s->record_u = s->record_w = s->record_layer = s->record_tangent = nullptr, s->record_probes = true;
         return r;
     };
     auto reverse = [&](uint64_t count) -> int {
@@ -1789,6 +1833,11 @@ int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float
                               tables ? g_layer : nullptr};
             if (tables) {
                 if (m > 0) next.traj = traj_layer + (m - 1) * kLayerFactors * Lc;
+                else next.pending = static_cast<T *>(adj.pending);
+            }
+            if (tangent) {
+                next.acc = tan_acc, next.tangent_base = tan_base;
+                if (m > 0) next.tangent_offset = (m - 1) * Tf;
                 else next.pending = static_cast<T *>(adj.pending);
             }
             // The rows and corrected cells far from the layer on the side stream; on the layer's
@@ -1864,7 +1913,20 @@ int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float
     };
     for (uint64_t k = segments; k-- > 0;) {
         const uint64_t s0 = k * segment, s1 = std::min(steps, s0 + segment), count = s1 - s0;
+        if (tangent) {
+            // Where the segment's factors start; and the products of its last step, whose Q^, L^,
+            // H^ the segment after left waiting.
+            const T *base = trajectory ? static_cast<const T *>(s->tape_t) + s0 * Tf : traj_tan;
+            set_address_kernel<<<1, 1, 0, s->stream>>>(reinterpret_cast<const void **>(tan_base), base);
+            CUDA_TRY(s, cudaGetLastError());
+        }
         if (trajectory) {
+            if (tangent && k + 1 < segments) {
+                layer_pending_tangent_kernel<T><<<layer_blocks, kBlock, 0, s->stream>>>(
+                    t, static_cast<const T *>(adj.pending), static_cast<const T *>(s->tape_t) + (s0 + count - 1) * Tf,
+                    tan_acc);
+                CUDA_TRY(s, cudaGetLastError());
+            }
             // The segment's levels s0 .. s1+1 from the tape, into the segment's trajectory buffers.
             CUDA_TRY(s, cudaMemcpyAsync(traj_u, static_cast<const T *>(s->tape_u) + s0 * K, e * K * (count + 2),
                                         cudaMemcpyDeviceToDevice, s->stream));
@@ -1904,6 +1966,11 @@ int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float
                 t, static_cast<const T *>(adj.pending), traj_layer + (count - 1) * kLayerFactors * Lc, g_layer);
             CUDA_TRY(s, cudaGetLastError());
         }
+        if (tangent && k + 1 < segments) {
+            layer_pending_tangent_kernel<T><<<layer_blocks, kBlock, 0, s->stream>>>(
+                t, static_cast<const T *>(adj.pending), traj_tan + (count - 1) * Tf, tan_acc);
+            CUDA_TRY(s, cudaGetLastError());
+        }
         if ((rc = run(1, x, reverse, count)) != FDTD_OK) return rc;
         if (count & 1) x = 1 - x;
     }
@@ -1911,6 +1978,19 @@ int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float
     if ((rc = check_device_error(s)) != FDTD_OK) return rc;
     for (int k = 0; k < 5; ++k)
         if (grads[k] && g_len[k]) CUDA_TRY(s, cudaMemcpy(grads[k], g[k], sizeof(double) * g_len[k], cudaMemcpyDeviceToHost));
+    s->tangent_valid = false;
+    if (tangent) {
+        // dL/dθ: the cells' sums in a fixed order, in two launches.
+        const uint64_t span = (Lc + tan_blocks - 1) / tan_blocks;
+        layer_tangent_sum_kernel<<<tan_blocks, kBlock, 0, s->stream>>>(tan_acc, Lc, span, tan_parts);
+        layer_tangent_sum_kernel<<<1, kBlock, 0, s->stream>>>(tan_parts, tan_blocks, tan_blocks, tan_parts + tan_blocks);
+        CUDA_TRY(s, cudaGetLastError());
+        // (on the handle's stream, which does not wait for the legacy default stream's copies)
+        CUDA_TRY(s, cudaMemcpyAsync(&s->tangent_gradient, tan_parts + tan_blocks, sizeof(double), cudaMemcpyDeviceToHost,
+                                    s->stream));
+        CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+        s->tangent_valid = true;
+    }
     if (tables) {
         // The layer tables' gradient: the cells' sums by coordinate on the device, in a fixed
         // order, then each coordinate's six sums into its tables' entries (a product of the cells
@@ -2012,9 +2092,15 @@ size_t pool_bytes(const fdtd_solver *s, const AdjointLists &l, uint64_t steps, u
              pool_round(8 * P * segment);
     total += 2 * pool_round(8 * K) + 3 * pool_round(8 * S);
     if (Lc) total += pool_round(4 * l.by_coord.size()) + pool_round(4 * l.coord_start.size());
-    if (Lc && s->gradient_tables)
+    if (Lc && s->gradient_tables && !s->tangent)
         total += pool_round(e * kLayerFactors * Lc * segment) + pool_round(8 * kLayerFactors * Lc) +
                  pool_round(8 * 6 * (s->nx + s->ny + s->nz));
+    if (Lc && s->tangent) {
+        const bool trajectory = taped && s->tape_traj;
+        const uint64_t blocks = std::min<uint64_t>(256, std::max<uint64_t>(1, (Lc + kBlock - 1) / kBlock));
+        if (!trajectory) total += pool_round(e * s->tangent_factors * segment);
+        total += pool_round(8 * Lc) + pool_round(8 * (blocks + 1)) + pool_round(sizeof(void *));
+    }
     if (!taped) total += (segments - 1) * pool_round(checkpoint_bytes(s));
     return total;
 }
@@ -2182,17 +2268,23 @@ int fdtd_run(fdtd_solver *s, const float *signal, uint64_t steps, double *out) {
     if (taping) {
         s->tape_valid = false;
         s->tape_traj = false;
+        s->tape_tangent = false;
         uint64_t budget = s->tape_budget;
         if (budget == UINT64_MAX) {
             size_t free_bytes = 0, total_bytes = 0;
             CUDA_TRY(s, cudaMemGetInfo(&free_bytes, &total_bytes));
-            budget = free_bytes / 2 + e * (K + S) * s->tape_levels;  // (what the tape holds already counts)
+            budget = free_bytes / 2 + e * (K + S) * s->tape_levels + e * s->tangent_factors * s->tape_t_steps;
+            // (what the tape holds already counts)
         }
         // (A grid with a matched layer whose gradients give its tables keeps checkpoints: the
         // gradient recomputes the layer's factors a segment at a time. Without the tables the
-        // layer steps back on its carried values alone, and the rows' trajectory is all it needs.)
-        keep_traj = K + S > 0 && (!s->layers || !s->gradient_tables) && e * (K + S) * (steps + 2) <= budget;
+        // layer steps back on its carried values alone, and the rows' trajectory is all it needs;
+        // along a tangent of the tables, the trajectory keeps the tangent's factors of every step.)
+        const uint64_t tangent_bytes = s->layers && s->tangent ? e * s->tangent_factors * steps : 0;
+        keep_traj = K + S > 0 && (!s->layers || !s->gradient_tables || s->tangent) &&
+                    e * (K + S) * (steps + 2) + tangent_bytes <= budget;
     }
+    const bool keep_tangent = keep_traj && s->layers && s->tangent;
     if (keep_traj) {
         int r;
         if (s->tape_levels < steps + 2) {
@@ -2213,6 +2305,18 @@ int fdtd_run(fdtd_solver *s, const float *signal, uint64_t steps, double *out) {
             if ((r = zeros(s, e * K * kGraphSteps, &s->stage_u)) != FDTD_OK) return r;
             if ((r = zeros(s, e * S * kGraphSteps, &s->stage_w)) != FDTD_OK) return r;
         }
+        if (keep_tangent && s->tape_t_steps < steps) {
+            if (s->tape_t) {
+                cudaFree(s->tape_t);
+                s->allocations.erase(std::find(s->allocations.begin(), s->allocations.end(), s->tape_t));
+                s->device_bytes -= e * s->tangent_factors * s->tape_t_steps;
+                s->tape_t = nullptr, s->tape_t_steps = 0;
+            }
+            if ((r = zeros(s, e * s->tangent_factors * steps, &s->tape_t)) != FDTD_OK) return r;
+            s->tape_t_steps = steps;
+        }
+        if (keep_tangent && !s->stage_t && (r = zeros(s, e * s->tangent_factors * kGraphSteps, &s->stage_t)) != FDTD_OK)
+            return r;
         // Levels 0 and 1: the state at rest.
         CUDA_TRY(s, cudaMemsetAsync(s->tape_u, 0, e * K * 2, s->stream));
         if (S) CUDA_TRY(s, cudaMemsetAsync(s->tape_w, 0, e * S * 2, s->stream));
@@ -2221,7 +2325,7 @@ int fdtd_run(fdtd_solver *s, const float *signal, uint64_t steps, double *out) {
     // While keeping the trajectory, every step records into the staging (restored on return).
     struct Recording {
         fdtd_solver *s;
-        ~Recording() { s->record_u = s->record_w = nullptr, s->record_offset = 2; }
+        ~Recording() { s->record_u = s->record_w = s->record_tangent = nullptr, s->record_offset = 2; }
     } recording{s};
     if (keep_traj) s->record_u = s->stage_u, s->record_w = s->stage_w, s->record_offset = 0, s->record_probes = true;
     if (taping && !keep_traj) {
@@ -2244,7 +2348,11 @@ int fdtd_run(fdtd_solver *s, const float *signal, uint64_t steps, double *out) {
             if (taping) chunk = std::min(chunk, (at / tape_segment + 1) * tape_segment - at);
             CUDA_TRY(s, cudaMemcpyAsync(s->d_sig, s->stage_signal + done, chunk * sizeof(float), cudaMemcpyHostToDevice,
                                         s->stream));
-            if (chunk == kGraphSteps && s->n_device < kGraphCells) {
+            const bool graphed = chunk == kGraphSteps && s->n_device < kGraphCells;
+            // (The tangent's factors: straight onto the tape, or a captured chunk's into staging.)
+            if (keep_tangent)
+                s->record_tangent = graphed ? s->stage_t : static_cast<char *>(s->tape_t) + e * s->tangent_factors * at;
+            if (graphed) {
                 // A whole chunk: the captured graph of its steps for the levels' present roles
                 // (with the trajectory's recording, a graph of its own).
                 cudaGraphExec_t &graph = keep_traj ? s->tape_graph[s->flipped ? 1 : 0] : s->graph[s->flipped ? 1 : 0];
@@ -2261,6 +2369,9 @@ int fdtd_run(fdtd_solver *s, const float *signal, uint64_t steps, double *out) {
                 if (S)
                     CUDA_TRY(s, cudaMemcpyAsync(static_cast<char *>(s->tape_w) + e * S * (at + 2), s->stage_w,
                                                 e * S * chunk, cudaMemcpyDeviceToDevice, s->stream));
+                if (keep_tangent && graphed)
+                    CUDA_TRY(s, cudaMemcpyAsync(static_cast<char *>(s->tape_t) + e * s->tangent_factors * at, s->stage_t,
+                                                e * s->tangent_factors * chunk, cudaMemcpyDeviceToDevice, s->stream));
             }
             if (taping && !keep_traj && (at + chunk) % tape_segment == 0 && at + chunk < steps) {
                 char *c = static_cast<char *>(s->tape_checkpoints[(at + chunk) / tape_segment - 1]);
@@ -2285,6 +2396,7 @@ int fdtd_run(fdtd_solver *s, const float *signal, uint64_t steps, double *out) {
         s->tape_signal.assign(signal, signal + steps);
         s->tape_valid = true;
         s->tape_traj = keep_traj;
+        s->tape_tangent = keep_tangent;
     }
     for (uint64_t k = 0; k < s->probes * steps; ++k) {
         if (!std::isfinite(out[k])) return fail(s, FDTD_ENONFINITE, "the wave solver's run did not stay finite");
@@ -2792,6 +2904,112 @@ int fdtd_set_gradient_tables(fdtd_solver *s, int enable) {
     // (A tape taken without the tables may hold the rows' trajectory alone: it serves no
     // gradient in the tables, which then runs the forward pass again.)
     s->layer_gradient.clear();
+    return FDTD_OK;
+}
+
+int fdtd_set_layer_tangent(fdtd_solver *s, const double *tangent, uint64_t count) {
+    if (!s) return set_global(FDTD_EINVAL, "no solver");
+    DeviceGuard guard(s->device);
+    for (cudaStream_t stream : {s->stream, s->side, s->layer_stream}) CUDA_TRY(s, cudaStreamSynchronize(stream));
+    if (tangent && !s->layers) return fail(s, FDTD_EINVAL, "the grid has no matched layer");
+    const uint64_t len[3] = {s->nx + 1, s->ny + 1, s->nz + 1};
+    const uint64_t old_factors = s->tangent_factors;
+    if (tangent && count != 4 * (len[0] + len[1] + len[2]))
+        return fail(s, FDTD_EINVAL, "a tangent of the layer's tables has 4 (nx + ny + nz + 3) values, as fdtd_layer_gradient's");
+    for (uint64_t k = 0; tangent && k < count; ++k)
+        if (!std::isfinite(tangent[k])) return fail(s, FDTD_EINVAL, "the tangent of the layer's tables is not finite");
+    // The old tangent's device tables; the captured graphs and the tape that used them.
+    for (void *p : s->tangent_device) {
+        auto it = std::find(s->allocations.begin(), s->allocations.end(), p);
+        if (it != s->allocations.end()) s->allocations.erase(it);
+        cudaFree(p);
+    }
+    s->tangent_device.clear();
+    Tables &g = s->tables;
+    for (int a = 0; a < 3; ++a) g.tangent_centre[a] = g.tangent_face[a] = nullptr;
+    g.tangent_axes = nullptr, g.tangent_start = nullptr;
+    s->tangent = false, s->tangent_factors = 0, s->tangent_valid = false;
+    s->tape_valid = false;
+    Kept{s}.drop_graphs();
+    for (cudaGraphExec_t &graph : s->tape_graph)
+        if (graph) cudaGraphExecDestroy(graph), graph = nullptr;
+    // (A tape and staging sized for another tangent's factors, or for none, are laid out again.)
+    auto drop_tape = [&]() {
+        for (void **p : {&s->tape_t, &s->stage_t}) {
+            if (!*p) continue;
+            auto it = std::find(s->allocations.begin(), s->allocations.end(), *p);
+            if (it != s->allocations.end()) s->allocations.erase(it);
+            cudaFree(*p);
+            *p = nullptr;
+        }
+        s->device_bytes -= s->precision == FDTD_FP64 ? 8 * old_factors * s->tape_t_steps : 4 * old_factors * s->tape_t_steps;
+        s->tape_t_steps = 0;
+    };
+    if (!tangent) {
+        drop_tape();
+        return FDTD_OK;
+    }
+    // Per axis, {keep, push} of the centres and of the faces by coordinate (the entries' order of
+    // fdtd_layer_gradient: the six keep tables, then the six push tables).
+    std::vector<double2> centre[3], face[3];
+    uint64_t at = 0;
+    for (int a = 0; a < 3; ++a) {
+        centre[a].resize(len[a]), face[a].resize(len[a]);
+        for (uint64_t x = 0; x < len[a]; ++x) centre[a][x].x = tangent[at + x], face[a][x].x = tangent[at + len[a] + x];
+        at += 2 * len[a];
+    }
+    for (int a = 0; a < 3; ++a) {
+        for (uint64_t x = 0; x < len[a]; ++x) centre[a][x].y = tangent[at + x], face[a][x].y = tangent[at + len[a] + x];
+        at += 2 * len[a];
+    }
+    auto touches = [](const double2 &v) { return v.x != 0.0 || v.y != 0.0; };
+    // Each layer cell's axes whose entries at its coordinate (centre, face) or the next (face) the
+    // tangent moves, and its first factor in a step's.
+    const uint64_t Lc = s->layers, plane = s->pitch * s->ny;
+    std::vector<uint8_t> axes(Lc);
+    std::vector<uint32_t> start(Lc);
+    uint64_t factors = 0;
+    for (uint64_t c = 0; c < Lc; ++c) {
+        const uint64_t i = s->layer_cells[c], r = i % plane;
+        const uint64_t coord[3] = {r % s->pitch, r / s->pitch, i / plane};
+        uint8_t bits = 0;
+        for (int a = 0; a < 3; ++a)
+            if (touches(centre[a][coord[a]]) || touches(face[a][coord[a]]) || touches(face[a][coord[a] + 1]))
+                bits |= (uint8_t)(1u << a);
+        axes[c] = bits;
+        start[c] = (uint32_t)factors;
+        factors += 3 * (uint64_t)__builtin_popcount(bits);
+        if (factors >= (1ull << 32)) return fail(s, FDTD_EINVAL, "the tangent's factors are too many for 32-bit indices");
+    }
+    int rc;
+    for (int a = 0; a < 3; ++a) {
+        const double2 *p;
+        if ((rc = upload(s, centre[a].data(), len[a], &p))) return rc;
+        g.tangent_centre[a] = p;
+        s->tangent_device.push_back(const_cast<double2 *>(p));
+        if ((rc = upload(s, face[a].data(), len[a], &p))) return rc;
+        g.tangent_face[a] = p;
+        s->tangent_device.push_back(const_cast<double2 *>(p));
+    }
+    const uint8_t *pa;
+    const uint32_t *ps;
+    if ((rc = upload(s, axes.data(), Lc, &pa))) return rc;
+    s->tangent_device.push_back(const_cast<uint8_t *>(pa));
+    if ((rc = upload(s, start.data(), Lc, &ps))) return rc;
+    s->tangent_device.push_back(const_cast<uint32_t *>(ps));
+    g.tangent_axes = pa, g.tangent_start = ps;
+    if (old_factors != factors) drop_tape();
+    s->tangent_factors = factors;
+    s->tangent = true;
+    return FDTD_OK;
+}
+
+int fdtd_layer_tangent_gradient(const fdtd_solver *s, double *out) {
+    if (!s) return set_global(FDTD_EINVAL, "no solver");
+    if (!out) return set_global(FDTD_EINVAL, "no output");
+    if (!s->tangent_valid)
+        return set_global(FDTD_EINVAL, "no gradient along a tangent of the layer's tables since the tangent was set");
+    *out = s->tangent_gradient;
     return FDTD_OK;
 }
 

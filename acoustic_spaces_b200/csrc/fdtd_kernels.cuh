@@ -528,6 +528,13 @@ struct Tables {
     const uint8_t *layer_below;  // bit a: the cell below along axis a is in the layer too
     uint32_t plane;  // pitch * ny
     FastDiv by_plane, by_pitch;  // a pitched index's plane, and its row within the plane
+    // With a tangent of the layer's tables (fdtd_set_layer_tangent): per axis and coordinate the
+    // tangent of the centre's {keep, push} and of the face's {keep, push}; each layer cell's axes
+    // along which the tangent touches it (bit a: at its coordinate or the one after), and the place
+    // of its first factor among a step's (three per such axis, axis by axis).
+    const double2 *tangent_centre[3], *tangent_face[3];
+    const uint8_t *tangent_axes;
+    const uint32_t *tangent_start;
     // Probes (fdtd.hpp:3525-3533).
     uint32_t probes;
     const uint32_t *probe_start, *probe_cells;
@@ -555,6 +562,10 @@ struct Fields {
     // cell's six factors per axis of the tables' gradient, at traj_layer[f * layers + c]
     // (fdtd_adjoint.cuh: q, hi' - lo', hi, b_(i+st) - b_i, lo, b_i - b_(i-st) per axis).
     T *traj_layer;
+    // When not null (a run recording for a gradient along a tangent of the layer's tables): each
+    // layer cell's tangent factors of the step at traj_tangent[tangent_start[c] + 3 j + f], j its
+    // j-th axis of tangent_axes (fdtd_adjoint.cuh: the centre's, the + face's, the - face's).
+    T *traj_tangent;
 };
 
 // Special rows (fdtd.hpp:860-881), one a thread: its links, its branch states' flow, the update,
@@ -688,6 +699,8 @@ __device__ __forceinline__ void layer_cell(const Tables &g, const Fields<T> &f, 
     const T here = b[i];
     const T scale = SCALED ? (T)g.layer_scale[c] : (T)1;
     const uint32_t shared_below = g.layer_below[c];
+    const uint32_t tangent_axes = f.traj_tangent ? g.tangent_axes[c] : 0u;
+    uint32_t tangent_slot = f.traj_tangent ? g.tangent_start[c] : 0u;
     T below[3], above[3];
     T total = 0;
 #pragma unroll
@@ -702,6 +715,17 @@ __device__ __forceinline__ void layer_cell(const Tables &g, const Fields<T> &f, 
             total += (keep - (T)1) * part[axis] - flux;
             part[axis] = keep * part[axis] - flux;
             continue;
+        }
+        if (f.traj_tangent && (tangent_axes & (1u << axis))) {
+            // The step's factors along the tangent: its products with the adjoints of the new part
+            // and faces give the gradient's step (fdtd_adjoint.cuh), in double.
+            const double2 tc = g.tangent_centre[axis][at[axis]];
+            const double2 t0 = g.tangent_face[axis][at[axis]], t1 = g.tangent_face[axis][at[axis] + 1];
+            T *o = f.traj_tangent + tangent_slot;
+            tangent_slot += 3;
+            o[0] = (T)((double)part[axis] * tc.x - (double)scale * (double)(above[axis] - below[axis]) * tc.y);
+            o[1] = (T)((double)old_above[axis] * t1.x - (double)(hi[axis] - here) * t1.y);
+            o[2] = (T)((double)old_below[axis] * t0.x - (double)(here - lo[axis]) * t0.y);
         }
         if (f.traj_layer) {
             T *o = f.traj_layer + (uint64_t)(6 * axis) * L + c;

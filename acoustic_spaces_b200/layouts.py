@@ -310,6 +310,21 @@ def layer_tables_tangent(size: int, layer: int, damping: float, courant: float, 
     return {k: np.array(v, np.float64) for k, v in out.items()}
 
 
+def damping_tangent(layout, layer: int, damping: float, layer_sides=(True,) * 6) -> dict[str, np.ndarray]:
+    """The derivatives in the layer's damping of ``layout``'s twelve tables (by their names, as
+    :meth:`B200WaveSolver.set_layer_tangent` takes them): :func:`layer_tables_tangent` along each
+    axis with the layout's own Courant number (the square root of its axial weight) and the axis'
+    ends that have the layer."""
+    shape = [int(v) for v in np.asarray(layout["shape"]).reshape(-1)]
+    courant = math.sqrt(float(np.asarray(layout["weights"], np.float32)[0]))
+    out = {}
+    for a, name in enumerate("xyz"):
+        t = layer_tables_tangent(shape[a], layer, damping, courant, (layer_sides[2 * a], layer_sides[2 * a + 1]))
+        for kind in ("keep", "push", "keep_face", "push_face"):
+            out[f"{kind}_{name}"] = t[kind]
+    return out
+
+
 def cell_face_layout(room: Room, grid: Grid, source, probes, **options) -> Built:
     """The reference's layout of ``room`` on ``grid`` with walls on cell faces, the 7-point
     stencil, a uniform speed ratio ``speed`` (None: the grid's), the source at ``source`` and

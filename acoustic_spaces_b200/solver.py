@@ -206,9 +206,46 @@ class B200WaveSolver:
         )
         if status != _abi.FDTD_OK:
             _raise(self._lib, status, self._handle)
-        if int(info.layer_cells) and layer_tables:
+        if int(info.layer_cells) and getattr(self, "_tangent", False):
+            value = ctypes.c_double()
+            status = self._lib.fdtd_layer_tangent_gradient(self._handle, ctypes.byref(value))
+            if status != _abi.FDTD_OK:
+                _raise(self._lib, status, self._handle)
+            out["layer_tangent"] = float(value.value)
+        elif int(info.layer_cells) and layer_tables:
             out.update(self.layer_gradient())
         return out
+
+    def set_layer_tangent(self, tangent: Mapping[str, np.ndarray] | None) -> None:
+        """A tangent of the matched layer's twelve tables: d(entry)/dθ for one parameter θ (the
+        layer's damping, say: :func:`layouts.damping_tangent`), by the tables' names (``keep_x``,
+        ``keep_face_x``, ..., ``push_face_z``; a missing table is 0). While it is set, :meth:`gradient`
+        gives ``layer_tangent`` = dL/dθ in place of the tables' gradient, and a taped run keeps the
+        few factors that needs beside the rows' trajectory, so that the gradient recomputes
+        nothing. None clears it. The walls' gradient is the same."""
+        if tangent is None:
+            status = self._lib.fdtd_set_layer_tangent(self._handle, None, 0)
+            if status != _abi.FDTD_OK:
+                _raise(self._lib, status, self._handle)
+            self._tangent = False
+            return
+        nx, ny, nz = self.shape
+        lengths = [nx + 1, nx + 1, ny + 1, ny + 1, nz + 1, nz + 1]
+        unknown = set(tangent) - set(_abi.KEEP + _abi.PUSH)
+        if unknown:
+            raise ValueError(f"no such table of the matched layer: {sorted(unknown)}")
+        parts = []
+        for name, n in zip(_abi.KEEP + _abi.PUSH, lengths + lengths):
+            value = np.asarray(tangent.get(name, np.zeros(n)), np.float64).reshape(-1)
+            if len(value) != n:
+                raise ValueError(f"{name} has {len(value)} values, the grid's table has {n}")
+            parts.append(value)
+        flat = np.ascontiguousarray(np.concatenate(parts))
+        status = self._lib.fdtd_set_layer_tangent(self._handle, flat.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                                  len(flat))  # fmt: skip
+        if status != _abi.FDTD_OK:
+            _raise(self._lib, status, self._handle)
+        self._tangent = True
 
     def layer_gradient(self) -> dict[str, np.ndarray]:
         """The last gradient's part in the matched layer's twelve tables, by the layout's names."""

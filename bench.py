@@ -1105,9 +1105,10 @@ def main() -> None:
             forward_s = time.perf_counter() - t0
             grad_solver.reset()
 
-            def taped_gradient(tables):
+            def taped_gradient(tables, tangent=None):
                 # (a fit's iterations keep the tape and the gradient's workspace: one untimed pass
                 # takes them, as the first iteration would)
+                grad_solver.set_layer_tangent(tangent)
                 grad_solver.set_tape(args.gradient_segment, layer_tables=tables)
                 grad_solver.run(head)
                 grad_solver.gradient(head, dloss, segment=args.gradient_segment, layer_tables=tables)
@@ -1120,6 +1121,13 @@ def main() -> None:
 
             both_s, taped_s, grads = taped_gradient(False)
             tables_s, _, with_tables = taped_gradient(True)
+            # The gradient in the layer's damping: along the tables' tangent in it, on the device.
+            from acoustic_spaces_b200.layouts import LAYER_CELLS, LAYER_DAMPING, damping_tangent
+
+            tangent = damping_tangent(workload.built.layout, LAYER_CELLS, LAYER_DAMPING)
+            damping_s, damping_taped_s, with_damping = taped_gradient(False, tangent)
+            grad_solver.set_layer_tangent(None)
+            tables_along = sum(float(np.sum(with_tables[k] * tangent[k])) for k in tangent)
             adjoint = {
                 "ratio": round(both_s / forward_s, 3),
                 "steps": g_steps,
@@ -1134,6 +1142,17 @@ def main() -> None:
                     "forward_and_adjoint_s": round(tables_s, 4),
                     "finite": bool(all(np.isfinite(v).all() for v in with_tables.values())),
                     "walls_equal": bool(all(np.array_equal(grads[k], with_tables[k]) for k in grads)),
+                },
+                "with_layer_damping": {
+                    "ratio": round(damping_s / forward_s, 3),
+                    "forward_and_adjoint_s": round(damping_s, 4),
+                    "taped_forward_s": round(damping_taped_s, 4),
+                    "dloss_ddamping": with_damping["layer_tangent"],
+                    "tables_gradient_along_the_tangent": tables_along,
+                    "walls_equal": bool(all(np.array_equal(grads[k], with_damping[k]) for k in grads)),
+                    "what": "dL/d(layer damping) on the device along the tables' tangent in the damping "
+                            "(fdtd_set_layer_tangent): the taped run keeps three factors a layer cell and "
+                            "damped axis a step beside the rows' trajectory, and the gradient recomputes nothing",
                 },
                 "what": "taped forward + gradient over the same steps, against a plain forward run; wall clock through "
                         "B200WaveSolver, the tape and workspace kept from an untimed first pass as a fit keeps them; "

@@ -217,6 +217,25 @@ int fdtd_layer_gradient(const fdtd_solver *solver, double *tables);
 int fdtd_set_gradient_tables(fdtd_solver *solver, int enable);
 
 /*
+ * A tangent of the matched layer's tables (no counterpart in the reference): the derivative of each
+ * table entry in one parameter θ — the layer's damping, say (layer_coefficients, fdtd.hpp:2219-2238)
+ * — in fdtd_layer_gradient's order and count (4 (nx + ny + nz + 3) values). While it is set,
+ * gradients give dL/dθ = sum over the entries of dL/d(entry) d(entry)/dθ (fdtd_layer_tangent_gradient)
+ * in place of the twelve tables' gradient: the forward records three factors a step per layer cell
+ * and axis along which the tangent moves an entry at the cell's coordinate (or the next one's
+ * face), not eighteen, each cell sums its products over the steps, and a taped run (fdtd_set_tape)
+ * keeps those factors of every step beside the rows' trajectory where both fit, so that the
+ * gradient recomputes nothing. The walls' gradient is the same. NULL clears it. FDTD_EINVAL on a
+ * grid without a layer, a count other than the tables', or a value that is not finite. Drops the
+ * handle's tape.
+ */
+int fdtd_set_layer_tangent(fdtd_solver *solver, const double *tangent, uint64_t count);
+
+/* The last gradient's dL/dθ along the layer tables' tangent (fdtd_set_layer_tangent); FDTD_EINVAL
+ * when no gradient ran since the tangent was set. */
+int fdtd_layer_tangent_gradient(const fdtd_solver *solver, double *out);
+
+/*
  * The tape of a run for a gradient that follows (no counterpart in the reference). With `segment`
  * > 0, each fdtd_run that starts from rest keeps on the device the state at every multiple of
  * `segment` steps before its end, and a copy of its drive; a following fdtd_gradient of the same

@@ -169,6 +169,10 @@ def test_the_layer_damping_gradient_on_the_gpu_matches_central_differences():
     measured = (loss(damping + h) - loss(damping - h)) / (2.0 * h)
     assert abs(measured) > 0.0
     assert abs(predicted - measured) <= 2e-3 * abs(measured), (predicted, measured)
+    # the same along the damping's tangent on the device (fdtd_set_layer_tangent)
+    solver.set_layer_tangent(L.damping_tangent(lay, layer, damping))
+    along = solver.gradient(signal, 2.0 * (y - target), segment=50)["layer_tangent"]
+    assert abs(along - predicted) <= 1e-9 * abs(predicted), (along, predicted)
 
 
 def test_the_reverse_steps_launch_caps_leave_the_gradient_unchanged():
@@ -189,3 +193,80 @@ def test_the_reverse_steps_launch_caps_leave_the_gradient_unchanged():
             np.testing.assert_array_equal(capped[key], plain[key], err_msg=f"{key} {far} {near}")
     with pytest.raises(ValueError, match="0 to 32"):
         solver.set_adjoint_launch(-1, 4)
+
+
+def _tables_along(grads, tangent):
+    return sum(float(np.sum(grads[name] * tangent[name])) for name in _TABLES)
+
+
+def _random_tangent(solver, seed):
+    # Every entry moved: the factors of every layer cell along every axis.
+    rng = np.random.default_rng(seed)
+    nx, ny, nz = solver.shape
+    lengths = dict(zip(_TABLES, [nx + 1, nx + 1, ny + 1, ny + 1, nz + 1, nz + 1] * 2))
+    return {name: rng.standard_normal(n) for name, n in lengths.items()}
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("name", _LAYER_GRIDS)
+def test_the_gradient_along_a_tangent_is_the_tables_gradient_along_it(name, precision):
+    # dL/dθ along a tangent of the tables (the layer's damping, and a random one moving every entry)
+    # equals the twelve tables' gradient summed with the tangent; the walls' gradient is the same
+    # to the bit, with checkpoints across segments (the products of a segment's last step wait for
+    # its recomputation) and in one segment.
+    layout, signal, _ = load_golden(name)
+    signal = signal[:160]
+    target, _ = _problem(layout, signal)
+    solver = B200WaveSolver(layout, precision=precision)
+    y = solver.run(signal)
+    solver.reset()
+    dloss = 2.0 * (y - target)
+    tangents = [_random_tangent(solver, 7), L.damping_tangent(layout, 4, 0.5)]
+    for segment in (0, 45):
+        solver.set_layer_tangent(None)
+        tables = solver.gradient(signal, dloss, segment=segment)
+        for tangent in tangents:
+            solver.set_layer_tangent(tangent)
+            along = solver.gradient(signal, dloss, segment=segment)
+            assert set(_TABLES).isdisjoint(along)
+            for key in ("coef_b", "coef_inv", "now", "before", "gain"):
+                np.testing.assert_array_equal(along[key], tables[key], err_msg=key)
+            expected = _tables_along(tables, tangent)
+            scale = sum(float(np.sum(np.abs(tables[n] * tangent[n]))) for n in _TABLES)
+            tolerance = 1e-11 if precision == "fp64" else 1e-5
+            assert abs(along["layer_tangent"] - expected) <= tolerance * scale, (segment, along["layer_tangent"], expected)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_a_taped_run_keeps_the_tangents_factors_and_the_gradient_recomputes_nothing(precision):
+    # A taped run from rest with a tangent set keeps the rows' trajectory and the tangent's factors
+    # of every step: the gradient that follows equals the one that recomputes the forward pass, to
+    # the bit, in one segment and across segments.
+    layout, signal, _ = load_golden("fitted_open")
+    signal = signal[:150]
+    target, _ = _problem(layout, signal)
+    solver = B200WaveSolver(layout, precision=precision)
+    tangent = L.damping_tangent(layout, 4, 0.5)
+    solver.set_layer_tangent(tangent)
+    y = solver.run(signal)
+    solver.reset()
+    dloss = 2.0 * (y - target)
+    for segment in (0, 40):
+        plain = solver.gradient(signal, dloss, segment=segment)
+        solver.set_tape(segment if segment else len(signal))
+        solver.run(signal)
+        taped = solver.gradient(signal, dloss, segment=segment)
+        solver.set_tape(0)
+        for key in plain:
+            np.testing.assert_array_equal(taped[key], plain[key], err_msg=f"{key} {segment}")
+    solver.set_layer_tangent(None)
+    assert set(_TABLES) <= set(solver.gradient(signal, dloss, segment=40))
+    with pytest.raises(ValueError, match="keep_x has 3 values"):
+        solver.set_layer_tangent({"keep_x": np.zeros(3)})
+    bad = dict(tangent, push_z=np.full_like(tangent["push_z"], np.nan))
+    with pytest.raises(ValueError, match="not finite"):
+        solver.set_layer_tangent(bad)
+    plain_layout, _, _ = load_golden("resonant7")
+    without = B200WaveSolver(plain_layout)
+    with pytest.raises(ValueError, match="no matched layer"):
+        without.set_layer_tangent({})
