@@ -244,8 +244,9 @@ constexpr int kHats = 6;      // a pitched cell's hats
 //   dL/dθ += Q^ (q k'[x] - s (hi' - lo') p'[x]) + H^ (hi kf'[x+1] - (b_(i+st) - b_i) pf'[x+1])
 //          + L^ (lo kf'[x] - (b_i - b_(i-st)) pf'[x])
 // per axis along which the tangent touches the cell: the forward records the three bracketed
-// factors (layer_cell's traj_tangent), and each cell keeps its own sum over the steps in double
-// (`acc`), summed over the cells in a fixed order at the end (layer_tangent_sum_kernel).
+// factors (layer_cell's traj_tangent); each cell sums a segment's products in the last slot of its
+// carried values, then into its own double sum (`acc`, layer_tangent_flush_kernel), and the cells'
+// sums are summed in a fixed order at the end (layer_tangent_sum_kernel).
 template <typename T>
 __device__ __forceinline__ double tangent_products(const AdjointTables &t, uint32_t c, const T *factors, const T (&q)[3],
                                                    const T (&lo)[3], const T (&hi)[3]) {
@@ -264,8 +265,7 @@ __device__ __forceinline__ double tangent_products(const AdjointTables &t, uint3
 
 template <typename T>
 __device__ __forceinline__ void layer_hat_cell(const AdjointTables &t, uint32_t c, uint32_t i, T lam, T *carried, T *hat,
-                                               const T *traj, double *g, T *pending, const T *tangent = nullptr,
-                                               double *acc = nullptr) {
+                                               const T *traj, double *g, T *pending, const T *tangent = nullptr) {
     const uint32_t L = t.layers;
     const uint32_t z = t.by_plane(i), r = i - z * t.plane, y = t.by_pitch(r);
     const uint32_t at[3] = {r - y * t.pitch, y, z};
@@ -308,8 +308,10 @@ __device__ __forceinline__ void layer_hat_cell(const AdjointTables &t, uint32_t 
             pending[(uint64_t)(3 * a + 2) * L + c] = hi_hat;
         }
     }
-    if (tangent && acc) acc[c] += tangent_products<T>(t, c, tangent, qs, los, his);
-    cv[kCarried - 1] = (T)0;
+    // (Along a tangent the carried values' last slot, read and written anyway, sums the products of
+    // the segment's steps; layer_tangent_flush_kernel adds it to the cell's double sum after each
+    // segment.)
+    if (tangent) cv[kCarried - 1] += (T)tangent_products<T>(t, c, tangent, qs, los, his);
 #pragma unroll
     for (int v = 0; v < kCarried / 2; ++v) {
         V2 p;
@@ -365,6 +367,17 @@ __global__ void __launch_bounds__(kBlock) layer_pending_tangent_kernel(const Adj
         hi[a] = pending[(uint64_t)(3 * a + 2) * L + c];
     }
     acc[c] += tangent_products<T>(t, c, factors, q, lo, hi);
+}
+
+// After a segment's reverse steps along a tangent: each cell's products of the segment (the last
+// slot of its carried values) into its double sum, and the slot back to 0.
+template <typename T>
+__global__ void __launch_bounds__(kBlock) layer_tangent_flush_kernel(uint32_t layers, T *carried, double *acc) {
+    const uint32_t c = blockIdx.x * kBlock + threadIdx.x;
+    if (c >= layers) return;
+    T &slot = carried[(uint64_t)kCarried * c + kCarried - 1];
+    acc[c] += (double)slot;
+    slot = (T)0;
 }
 
 // The cells' sums along the tangent, summed in a fixed order: block b sums cells b * span ..
@@ -437,9 +450,9 @@ __device__ __forceinline__ T layer_terms(const AdjointTables &t, const T *hat, u
 // The layer's part of a reverse step: where its hats of the step before go (`next`, the other hat
 // buffer), its carried values, and the tables' sums with the factors of that step (`traj`, or null
 // with `pending` where they are not recorded yet; both null for a gradient without the tables).
-// Along a tangent (`acc` not null): the factors of that step at *tangent_base + tangent_offset
-// (the base in device memory, so that a captured reverse step serves every segment), or with
-// `pending` none yet.
+// Along a tangent (`tangent_base` not null): the factors of that step at *tangent_base +
+// tangent_offset (the base in device memory, so that a captured reverse step serves every
+// segment), or with `pending` none yet.
 template <typename T>
 struct LayerNext {
     T *hat, *carried, *pending;
@@ -447,7 +460,6 @@ struct LayerNext {
     double *g;
     const T *const *tangent_base = nullptr;
     uint64_t tangent_offset = 0;
-    double *acc = nullptr;
 };
 
 // A layer cell's adjoint: its interior neighbours' axial x lam (with a speed field their stored
@@ -476,8 +488,8 @@ __device__ __forceinline__ void layer_adjoint_cell(const AdjointTables &t, uint3
         if (probed != 0.0) value += (T)probed;
     }
     lam_out[i] = value;
-    const T *tangent = next.acc && !next.pending ? *next.tangent_base + next.tangent_offset : nullptr;
-    layer_hat_cell<T>(t, c, i, value, next.carried, next.hat, next.traj, next.g, next.pending, tangent, next.acc);
+    const T *tangent = next.tangent_base && !next.pending ? *next.tangent_base + next.tangent_offset : nullptr;
+    layer_hat_cell<T>(t, c, i, value, next.carried, next.hat, next.traj, next.g, next.pending, tangent);
 }
 
 // One launch of the special rows' adjoint (the rows special_order[begin .. end), on the first

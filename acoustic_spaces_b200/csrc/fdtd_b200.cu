@@ -1836,7 +1836,7 @@ int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float
                 else next.pending = static_cast<T *>(adj.pending);
             }
             if (tangent) {
-                next.acc = tan_acc, next.tangent_base = tan_base;
+                next.tangent_base = tan_base;
                 if (m > 0) next.tangent_offset = (m - 1) * Tf;
                 else next.pending = static_cast<T *>(adj.pending);
             }
@@ -1911,6 +1911,11 @@ int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float
         CUDA_TRY(s, cudaGraphLaunch(exec, s->stream));
         return FDTD_OK;
     };
+    // Along a tangent: each cell's products of a segment into its double sum.
+    auto flush_tangent = [&]() {
+        layer_tangent_flush_kernel<T><<<layer_blocks, kBlock, 0, s->stream>>>((uint32_t)Lc, static_cast<T *>(adj.carried),
+                                                                              tan_acc);
+    };
     for (uint64_t k = segments; k-- > 0;) {
         const uint64_t s0 = k * segment, s1 = std::min(steps, s0 + segment), count = s1 - s0;
         if (tangent) {
@@ -1937,6 +1942,7 @@ int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float
                 CUDA_TRY(s, cudaMemcpy2DAsync(seg_dloss, sizeof(double) * segment, d_dloss + s0, sizeof(double) * steps,
                                               sizeof(double) * count, P, cudaMemcpyDeviceToDevice, s->stream));
             if ((rc = run(1, x, reverse, count)) != FDTD_OK) return rc;
+            if (tangent) flush_tangent();
             if (count & 1) x = 1 - x;
             continue;
         }
@@ -1972,6 +1978,7 @@ int gradient(fdtd_solver *s, const AdjointState &adj, Pool &scratch, const float
             CUDA_TRY(s, cudaGetLastError());
         }
         if ((rc = run(1, x, reverse, count)) != FDTD_OK) return rc;
+        if (tangent) flush_tangent();
         if (count & 1) x = 1 - x;
     }
     CUDA_TRY(s, cudaStreamSynchronize(s->stream));
