@@ -53,9 +53,29 @@ def _edge(grid: L.Grid) -> np.ndarray:
 
 
 def _accumulate(target: np.ndarray, index: np.ndarray, values) -> None:
-    """target[index] += values for repeated indices (a flat view of target), by bincount."""
+    """target[index] += values for repeated indices (a flat view of target), by bincount: each
+    entry gains the sum of its values in their order. A table of rows (2-D target) sums column by
+    column over its rows, not over the whole table."""
     flat = target.reshape(-1)
-    flat += np.bincount(np.asarray(index, np.int64), np.broadcast_to(values, np.shape(index)), minlength=flat.size)
+    index = np.asarray(index, np.int64).reshape(-1)
+    values = np.broadcast_to(values, index.shape)
+    if target.ndim != 2 or target.shape[1] == 1 or len(index) * 16 > flat.size:
+        flat += np.bincount(index, values, minlength=flat.size)
+        return
+    if not len(index):
+        return
+    cols = target.shape[1]
+    row, col = np.divmod(index, cols)
+    if col.min() == col.max():
+        target[:, col[0]] += np.bincount(row, values, minlength=target.shape[0])
+        return
+    # (grouped by column, each group in the values' order)
+    order = np.argsort(col, kind="stable")
+    row, col, values = row[order], col[order], np.asarray(values)[order]
+    starts = np.flatnonzero(np.concatenate([[True], col[1:] != col[:-1]]))
+    ends = np.concatenate([starts[1:], [len(col)]])
+    for a, b in zip(starts, ends):
+        target[:, col[a]] += np.bincount(row[a:b], values[a:b], minlength=target.shape[0])
 
 
 def opposite(k: int) -> int:
@@ -206,17 +226,17 @@ def set_up_fitted(
     rc = np.maximum(r_of, 0)
     room = (types == 1) | (types == 2)
 
-    # Each candidate's open area towards each direction (area_towards, fdtd.hpp:1087-1100).
-    area = np.zeros((len(cand), 18))
-    for k in range(18):
+    # Each candidate's open area towards each direction (area_towards, fdtd.hpp:1087-1100): a
+    # row's own; along the axes also a plain cell's whole face, and the sliver rule's factors.
+    area = fit.open_area[rc] if R else np.zeros((len(cand), 18))
+    area[~is_row] = 0.0
+    for k in range(6):
         j = cand + offsets[k]
-        a = np.where(is_row, fit.open_area[rc, k] if R else 0.0, 0.0)
-        if k < 6:
-            plain = ~is_row & (types[cand] != 0) & ~edge[j] & (types[j] != 0)
-            a = np.where(plain, face_area(cand, k // 2), a)
-            touched = (a > 0.0) & room[cand] & room[j]
-            a = np.where(touched, a * factor_of(cand, j, k // 2), a)
-        area[:, k] = a
+        a = area[:, k]
+        plain = ~is_row & (types[cand] != 0) & ~edge[j] & (types[j] != 0)
+        a = np.where(plain, face_area(cand, k // 2), a)
+        touched = (a > 0.0) & room[cand] & room[j]
+        area[:, k] = np.where(touched, a * factor_of(cand, j, k // 2), a)
     air_volume = np.where(is_row, fit.air_volume[rc] if R else 0.0, cell_volume(cand))
 
     # The wall term and the branch states (fdtd.hpp:1106-1128), in material order.
@@ -242,12 +262,11 @@ def set_up_fitted(
     # add_special_fitted (fdtd.hpp:1219-1264), s = 1, r = 1 / V.
     r = 1.0 / volume
     lw = np.zeros((len(cand), 18), np.float32)
+    linked = area > 0.0
+    lw[linked] = L.lowered(exact * area[linked] / np.broadcast_to(volume[:, None], area.shape)[linked])
     link_total = np.zeros(len(cand))
     for k in range(18):
-        has = area[:, k] > 0.0
-        w = L.lowered(exact * area[:, k] / volume)
-        lw[:, k] = np.where(has, w, np.float32(0.0))
-        link_total = link_total + np.where(has, lw[:, k].astype(np.float64), 0.0)
+        link_total = link_total + lw[:, k].astype(np.float64)
     centre_d = 2.0 - link_total
     coef_a = centre_d.astype(np.float32)
     over = coef_a.astype(np.float64) > centre_d
@@ -263,11 +282,11 @@ def set_up_fitted(
 
     special = cand[kept]
     K = len(special)
-    volumes = list(volume[kept])
+    volumes = volume[kept]
     has_link = area[kept] > 0.0
-    link_direction = np.tile(np.arange(18, dtype=np.uint8), (K, 1))[has_link]
+    link_direction = np.broadcast_to(np.arange(18, dtype=np.uint8), (K, 18))[has_link]
     link_weight = lw[kept][has_link]
-    link_start = np.concatenate([[0], np.cumsum(has_link.sum(axis=1))]).astype(np.uint64)
+    link_counts = has_link.sum(axis=1)
     # Branch states in row order, each row's in material then branch order.
     if st_cand:
         sc = np.concatenate(st_cand)
@@ -288,11 +307,11 @@ def set_up_fitted(
 
     # The source's cells (fdtd.hpp:1141-1163): a cell not yet special becomes special (a row that
     # stayed plain with its own coefficients, any other cell with the interior's), each fed w / V.
-    special_list = list(special)
-    coef_a_l, coef_b_l, coef_inv_l = list(coef_a[kept]), list(coef_b[kept]), list(coef_inv[kept])
-    link_dir_l, link_w_l = [link_direction], [link_weight]
-    link_counts = list(has_link.sum(axis=1))
-    source = [np.float32(0.0)] * K
+    # (The rows' arrays stay arrays; the few cells the source adds follow them.)
+    coef_a_k, coef_b_k, coef_inv_k = coef_a[kept], coef_b[kept], coef_inv[kept]
+    source_k = np.zeros(K, np.float32)
+    extra_cell, extra_a, extra_b, extra_inv, extra_volume, extra_source = [], [], [], [], [], []
+    extra_dir, extra_w, extra_count = [], [], []
     added: dict[int, int] = {}
     for i, w in source_cells:
         i = int(i)
@@ -304,31 +323,36 @@ def set_up_fitted(
             if at < len(cand) and cand[at] == i and is_row[at]:
                 # a row that stayed plain: its own coefficients (add_special_fitted, no spare)
                 hl = area[at] > 0.0
-                link_dir_l.append(np.arange(18, dtype=np.uint8)[hl])
-                link_w_l.append(lw[at][hl])
-                link_counts.append(int(hl.sum()))
-                coef_a_l.append(coef_a[at]), coef_b_l.append(coef_b[at]), coef_inv_l.append(coef_inv[at])
-                volumes.append(volume[at])
+                extra_dir.append(np.arange(18, dtype=np.uint8)[hl])
+                extra_w.append(lw[at][hl])
+                extra_count.append(int(hl.sum()))
+                extra_a.append(coef_a[at]), extra_b.append(coef_b[at]), extra_inv.append(coef_inv[at])
+                extra_volume.append(volume[at])
             else:
                 # add_special(i, exact, 0): the interior's links and coefficients
-                link_dir_l.append(np.arange(6, dtype=np.uint8))
-                link_w_l.append(np.full(6, weight_plain, np.float32))
-                link_counts.append(6)
+                extra_dir.append(np.arange(6, dtype=np.uint8))
+                extra_w.append(np.full(6, weight_plain, np.float32))
+                extra_count.append(6)
                 tot = 0.0
                 for _ in range(6):
                     tot += exact
-                coef_a_l.append(np.float32(2.0 - tot * (1.0 - L.MARGIN)))
-                coef_b_l.append(np.float32(1.0)), coef_inv_l.append(np.float32(1.0))
-                volumes.append(float(cell_volume(np.array([i]))[0]))
+                extra_a.append(np.float32(2.0 - tot * (1.0 - L.MARGIN)))
+                extra_b.append(np.float32(1.0)), extra_inv.append(np.float32(1.0))
+                extra_volume.append(float(cell_volume(np.array([i]))[0]))
             types[i] = 2
-            k = len(special_list)
-            special_list.append(i)
-            source.append(np.float32(0.0))
+            k = K + len(extra_cell)
+            extra_cell.append(i)
+            extra_source.append(np.float32(0.0))
             added[i] = k
-        source[k] = np.float32(source[k] + np.float32(w / volumes[k]))
-    E = len(special_list) - K
+        if k < K:
+            source_k[k] = np.float32(source_k[k] + np.float32(w / volumes[k]))
+        else:
+            e = k - K
+            extra_source[e] = np.float32(extra_source[e] + np.float32(w / extra_volume[e]))
+    E = len(extra_cell)
     state_start = np.concatenate([state_start, np.full(E, state_start[-1], np.uint64)])
-    link_start = np.concatenate([[0], np.cumsum(link_counts)]).astype(np.uint64)
+    link_start = np.concatenate([[0], np.cumsum(np.concatenate([link_counts, np.array(extra_count, np.int64)]))])
+    link_start = link_start.astype(np.uint64)
 
     layout: dict[str, np.ndarray] = {}
     layout["shape"] = np.array(grid.shape, np.uint64)
@@ -340,14 +364,14 @@ def set_up_fitted(
     layout["scale"] = np.zeros(0, np.float32)
     layout["layer_scale"] = np.zeros(0, np.float32)
     layout["types"] = types
-    layout["special"] = np.array(special_list, np.int64)
+    layout["special"] = np.concatenate([special, np.array(extra_cell, np.int64)]).astype(np.int64)
     layout["link_start"] = link_start
-    layout["link_direction"] = np.concatenate(link_dir_l).astype(np.uint8)
-    layout["link_weight"] = np.concatenate(link_w_l).astype(np.float32)
-    layout["coef_a"] = np.array(coef_a_l, np.float32)
-    layout["coef_b"] = np.array(coef_b_l, np.float32)
-    layout["coef_inv"] = np.array(coef_inv_l, np.float32)
-    layout["source"] = np.array(source, np.float32)
+    layout["link_direction"] = np.concatenate([link_direction, *extra_dir]).astype(np.uint8)
+    layout["link_weight"] = np.concatenate([link_weight, *extra_w]).astype(np.float32)
+    layout["coef_a"] = np.concatenate([coef_a_k, np.array(extra_a, np.float32)]).astype(np.float32)
+    layout["coef_b"] = np.concatenate([coef_b_k, np.array(extra_b, np.float32)]).astype(np.float32)
+    layout["coef_inv"] = np.concatenate([coef_inv_k, np.array(extra_inv, np.float32)]).astype(np.float32)
+    layout["source"] = np.concatenate([source_k, np.array(extra_source, np.float32)]).astype(np.float32)
     layout["state_start"] = state_start
     layout["state_branch"] = sb.astype(np.int32)
     layout["state_weight"] = state_weight

@@ -225,3 +225,23 @@ def test_the_owner_rule_and_sums_on_a_box_are_the_references(open_face):
     np.testing.assert_array_equal(ours.cell, ref.cell)
     for key in ("air_volume", "open_area", "wall_area", "sliver"):
         np.testing.assert_allclose(getattr(ours, key), getattr(ref, key), rtol=0, atol=1e-9, err_msg=key)
+
+
+def test_accumulate_sums_a_tables_columns_as_the_whole_table_does():
+    # target[index] += values with repeated indices: by column over a table's rows (a short index
+    # into a large table) the entries gain exactly what one bincount over the whole table gives.
+    rng = np.random.default_rng(5)
+    rows, cols = 5000, 18
+    base = rng.standard_normal((rows, cols))
+    index = rng.integers(0, rows * cols, 900) // 3 * 3  # repeats, a few columns
+    values = rng.standard_normal(900)
+    by_column = base.copy()
+    fitted._accumulate(by_column, index, values)
+    whole = base.copy().reshape(-1)
+    whole += np.bincount(index, values, minlength=whole.size)
+    np.testing.assert_array_equal(by_column.reshape(-1), whole)
+    scalar = base.copy()
+    fitted._accumulate(scalar, index, 0.5)
+    whole = base.copy().reshape(-1)
+    whole += np.bincount(index, np.full(900, 0.5), minlength=whole.size)
+    np.testing.assert_array_equal(scalar.reshape(-1), whole)
