@@ -242,9 +242,11 @@ int fdtd_layer_tangent_gradient(const fdtd_solver *solver, double *out);
  * drive and steps with the same `segment` starts from those states instead of running the forward
  * pass again, so that a fit's forward run and its gradient together step the grid twice rather
  * than three times. The result is the same to the bit. 0 turns the tape off. The states take
- * (steps / segment - 1) x (2 levels + 2 branch-velocity sets, and with a matched layer its parts
- * and a level of faces per axis) of device memory, kept by the handle; a grid with a matched layer
- * always keeps states, never the trajectory.
+ * (steps / segment - 1) x (2 levels + 2 branch-velocity sets, and with a matched layer its
+ * state) of device memory, kept by the handle. Where the trajectory fits the budget
+ * (fdtd_set_tape_budget) the tape keeps it instead; on a grid with a matched layer only for
+ * gradients without the layer's tables (fdtd_set_gradient_tables) or along a tangent of them
+ * (fdtd_set_layer_tangent, whose factors the tape then keeps too).
  */
 int fdtd_set_tape(fdtd_solver *solver, uint64_t segment);
 
@@ -260,12 +262,14 @@ int fdtd_set_tape_budget(fdtd_solver *solver, uint64_t bytes);
 /*
  * Chooses the launch shapes for this grid (no counterpart in the reference): from rest, steps
  * `trial_steps` steps (0: 8) with each candidate and keeps the fastest by CUDA events — first the
- * interior sweep's tile shape (each of the four shapes of fdtd_tiles that fits a multiprocessor,
+ * interior sweep's tile shape (each of the ten shapes of fdtd_tiles that fits a multiprocessor,
  * each with 1/4, 1/2, 1 and 2 times the default planes a tile, within 8 to 64), then, with the best
- * tiles, the count of blocks per multiprocessor of the matched-layer and special-row kernels, the
- * step's kernels beside one another and in turn (fdtd_set_streams) — and resets the state. The chosen counts are written to *layer_per_sm and *special_per_sm when given
- * (0: one thread a cell); fdtd_get_tiles gives the chosen tiles. Results do not depend on any of
- * these choices. Refused after steps (fdtd_reset first).
+ * tiles, the count of blocks per multiprocessor of the matched-layer and special-row kernels and
+ * the step's kernels beside one another and in turn (fdtd_set_streams), then the tiles again; the
+ * best few whole choices are timed three times more and the fastest kept — and resets the state.
+ * The chosen counts are written to *layer_per_sm and *special_per_sm when given (0: one thread a
+ * cell); fdtd_get_tiles gives the rest. Results do not depend on any of these choices. Refused
+ * after steps (fdtd_reset first).
  */
 int fdtd_autotune(fdtd_solver *solver, uint64_t trial_steps, int *layer_per_sm, int *special_per_sm);
 
