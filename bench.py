@@ -1152,7 +1152,9 @@ def main() -> None:
                     "walls_equal": bool(all(np.array_equal(grads[k], with_damping[k]) for k in grads)),
                     "what": "dL/d(layer damping) on the device along the tables' tangent in the damping "
                             "(fdtd_set_layer_tangent): the taped run keeps three factors a layer cell and "
-                            "damped axis a step beside the rows' trajectory, and the gradient recomputes nothing",
+                            "damped axis a step beside the rows' trajectory, and the gradient recomputes nothing; "
+                            "both values are 0 while the window is too short for sound to reach the layer and "
+                            "come back to a receiver (the gradient's values are checked by the GPU tests)",
                 },
                 "what": "taped forward + gradient over the same steps, against a plain forward run; wall clock through "
                         "B200WaveSolver, the tape and workspace kept from an untimed first pass as a fit keeps them; "
