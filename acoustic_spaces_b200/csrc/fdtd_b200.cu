@@ -701,11 +701,32 @@ int launch_steps(fdtd_solver *s, const float *d_signal, uint64_t steps, double *
     // kernel's events bracket that kernel alone.
     // The streams (fdtd_set_streams): 1, the three kinds each on its own; 2, the layer and then the
     // special rows and probes on the side stream beside the sweep; 3, the special rows and probes
-    // after the sweep on its stream, the layer beside them; 0, all in turn.
+    // after the sweep on its stream, the layer beside them; 0, all in turn; 4 and 5, as 1 and 2
+    // with the special rows launched at the highest priority as well. A kernel's blocks wait until
+    // those of the kernels before it at the same priority have all been dispatched, so beside a
+    // sweep of many waves the special rows would otherwise start only in its last wave.
     const int mode = s->timing ? 0 : s->concurrent;
     const bool fork = mode != 0;
-    cudaStream_t side = mode == 1 || mode == 2 ? s->side : s->stream;
-    cudaStream_t layer = mode == 1 || mode == 3 ? s->layer_stream : (mode == 2 ? s->side : s->stream);
+    const int streams = mode >= 4 ? mode - 3 : mode;
+    const bool special_first = mode >= 4;
+    cudaStream_t side = streams == 1 || streams == 2 ? s->side : s->stream;
+    cudaStream_t layer = streams == 1 || streams == 3 ? s->layer_stream : (streams == 2 ? s->side : s->stream);
+    auto launch_special = [&](auto kernel, const Fields<T> &f) -> cudaError_t {
+        if (!special_first) {
+            kernel<<<special_blocks, kBlock, 0, side>>>(g, f);
+            return cudaGetLastError();
+        }
+        cudaLaunchConfig_t config{};
+        config.gridDim = dim3(special_blocks);
+        config.blockDim = dim3(kBlock);
+        config.stream = side;
+        cudaLaunchAttribute priority{};
+        priority.id = cudaLaunchAttributePriority;
+        priority.val.priority = s->layer_priority;
+        config.attrs = &priority;
+        config.numAttrs = 1;
+        return cudaLaunchKernelEx(&config, kernel, g, f);
+    };
     for (uint64_t k = 0; k < steps; ++k) {
         const bool flip = (k & 1) != 0;
         Fields<T> f = fields_for<T>(s, flip);
@@ -778,11 +799,11 @@ int launch_steps(fdtd_solver *s, const float *d_signal, uint64_t steps, double *
         if (ev) CUDA_TRY(s, cudaEventRecord(ev[4], side));
         if (special_blocks) {
             if (g.link_mask)
-                special_kernel<T, 0, COMP><<<special_blocks, kBlock, 0, side>>>(g, f);
+                CUDA_TRY(s, launch_special(special_kernel<T, 0, COMP>, f));
             else if (s->link_slots <= 6)
-                special_kernel<T, 6, COMP><<<special_blocks, kBlock, 0, side>>>(g, f);
+                CUDA_TRY(s, launch_special(special_kernel<T, 6, COMP>, f));
             else
-                special_kernel<T, 18, COMP><<<special_blocks, kBlock, 0, side>>>(g, f);
+                CUDA_TRY(s, launch_special(special_kernel<T, 18, COMP>, f));
         }
         if (ev) CUDA_TRY(s, cudaEventRecord(ev[5], side));
         if (ev) CUDA_TRY(s, cudaEventRecord(ev[6], side));
@@ -2685,7 +2706,7 @@ int fdtd_set_streams(fdtd_solver *s, int concurrent) {
     if (!s) return set_global(FDTD_EINVAL, "no solver");
     DeviceGuard guard(s->device);
     for (cudaStream_t stream : {s->stream, s->side, s->layer_stream}) CUDA_TRY(s, cudaStreamSynchronize(stream));
-    if (concurrent < 0 || concurrent > 3) return fail(s, FDTD_EINVAL, "the streams' arrangement is 0 to 3");
+    if (concurrent < 0 || concurrent > 5) return fail(s, FDTD_EINVAL, "the streams' arrangement is 0 to 5");
     s->concurrent = concurrent;
     // The captured chunks and the gradient's graphs hold the old streams' order.
     Kept{s}.drop_graphs();
@@ -2773,7 +2794,7 @@ int fdtd_autotune(fdtd_solver *s, uint64_t trial_steps, int *layer_per_sm, int *
     auto tune_launch = [&]() -> int {
         float best = -1.0f;
         int r = FDTD_OK;
-        for (int c : {1, 2, 3, 0}) {
+        for (int c : {1, 4, 2, 5, 3, 0}) {
             s->concurrent = c;
             for (int l : layers) {
                 if (r != FDTD_OK) break;

@@ -332,8 +332,8 @@ class B200WaveSolver:
     def set_streams(self, concurrent: int) -> None:
         """How a step's kernels share the streams, as :meth:`autotune` may choose (1 or True: each
         kind on its own; 2: the layer and then the special rows beside the sweep; 3: the special rows
-        after the sweep, the layer beside them; 0 or False: all in turn); results are the same to
-        the bit."""
+        after the sweep, the layer beside them; 0 or False: all in turn; 4 and 5: as 1 and 2 with the
+        special rows at the highest stream priority); results are the same to the bit."""
         status = self._lib.fdtd_set_streams(self._handle, int(concurrent))
         if status != _abi.FDTD_OK:
             _raise(self._lib, status, self._handle)

@@ -454,6 +454,8 @@ def run_batched(args, world: int, rank: int, local: int) -> None:
                                   part=(rank, world))  # fmt: skip
     desc = batch.description
     solver = B200WaveSolver(batch.stacked.layout, precision=args.precision, device=local)
+    if args.streams >= 0:
+        solver.set_streams(args.streams)
     air = batch.stacked.air_cells
     steps, warmup = args.steps, args.warmup
     sig = torch.from_numpy(np.ascontiguousarray(batch.signal)).to(f"cuda:{local}")
@@ -474,6 +476,13 @@ def run_batched(args, world: int, rank: int, local: int) -> None:
         if world > 1:
             dist.barrier()
     ms = start.elapsed_time(end)
+    # Each kernel's own duration: the step's kernels one after another, CUDA events around each.
+    solver.set_timing(True)
+    solver.run_device(sig.data_ptr(), min(steps, 10), out.data_ptr(), steps + warmup)
+    solver.synchronize()
+    solver.set_timing(False)
+    timed = solver.timing()
+    kernel_us = {k: round(1e3 * v / max(1, timed["steps"]), 2) for k, v in timed.items() if k != "steps" and v}
     total_air = air
     if world > 1:
         t = torch.tensor([ms, float(air)], dtype=torch.float64, device=f"cuda:{local}")
@@ -545,7 +554,9 @@ def run_batched(args, world: int, rank: int, local: int) -> None:
         "config": {"workload": "batched_rooms", **desc, "air_cells_all_ranks": total_air,
                    "parallelism": f"solves sharded over {world} GPUs by cell count" if world > 1 else "single GPU",
                    "precision": "FP32, bit-exact with the reference" if args.precision == "fp32"
-                   else "FP32 compensated: each cell's pressure and its increment"},
+                   else "FP32 compensated: each cell's pressure and its increment",
+                   "launch": solver.launch},
+        "kernel_mean_us_serialised": kernel_us,
         "e2e": {"value": round(total_air * steps / e2e_s / 1e9, 4), "unit": UNIT, "h2d_bytes_per_step": 4,
                 "d2h_bytes_per_step": 8 * solver.probes},  # fmt: skip
         "sequential_solves": {"value": round(sequential, 4), "unit": UNIT, "solves_timed": len(sample),
@@ -878,6 +889,8 @@ def main() -> None:
     parser.add_argument("--gradient-segment", type=int, default=50)
     parser.add_argument("--no-fp64-rate", action="store_true", help="skip timing the FP64 stepper alike")
     parser.add_argument("--launch", default="", help="layer,special blocks per SM (skips the autotuner)")
+    parser.add_argument("--streams", type=int, default=-1,
+                        help="the step's stream arrangement (0 to 5), set after the autotuner's choice")
     parser.add_argument("--tiles", default="", help="with --launch: the sweep's tile shape,planes a tile")
     parser.add_argument("--slab-count", type=int, default=0,
                         help="with --slabs on one GPU: this many slabs stepped together in one process")  # fmt: skip
@@ -957,6 +970,8 @@ def main() -> None:
                          "special_blocks_per_sm": int(args.launch.split(",")[1])}  # fmt: skip
     else:
         solver = B200WaveSolver(workload.built.layout, precision=args.precision, device=local)
+    if args.streams >= 0:
+        solver.set_streams(args.streams)
     handle_s = time.perf_counter() - t_setup
     air = solver.air_cells
     probes = solver.probes

@@ -284,7 +284,7 @@ typedef struct fdtd_tiles {
     uint64_t planes;    /* planes of a tile, at most (a tile marches them along z) */
     uint32_t tiles;     /* tiles, one block each */
     int blocks_per_sm;  /* resident blocks of the sweep a multiprocessor */
-    int concurrent;     /* how a step's kernels share the streams (fdtd_set_streams: 0 to 3) */
+    int concurrent;     /* how a step's kernels share the streams (fdtd_set_streams: 0 to 5) */
     int threads;        /* threads a block of the sweep */
     int cols;           /* adjacent columns a thread (1, or 2: the 7-point stencil a pair at a time) */
 } fdtd_tiles;
@@ -305,8 +305,10 @@ int fdtd_get_tiles(const fdtd_solver *solver, fdtd_tiles *out);
  * reference): 1 (the default), the interior sweep on the handle's stream, the matched layer and the
  * special rows (with the probes) on streams of their own; 2, the layer and then the special rows
  * on one stream beside the sweep; 3, the special rows after the sweep on the handle's stream, the
- * layer beside them; 0, all one after another on the handle's stream. Results are the same to
- * the bit. FDTD_EINVAL outside 0 to 3. Waits for the handle's work.
+ * layer beside them; 0, all one after another on the handle's stream; 4 and 5, as 1 and 2 with
+ * the special rows launched at the device's highest stream priority, so that their blocks run
+ * beside the sweep's from the step's start. Results are the same to the bit. FDTD_EINVAL outside
+ * 0 to 5. Waits for the handle's work.
  */
 int fdtd_set_streams(fdtd_solver *solver, int concurrent);
 

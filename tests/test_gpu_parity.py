@@ -286,19 +286,20 @@ def test_gpu_steps_a_layout_without_probes_as_the_oracle_does():
 @pytest.mark.parametrize("name", ["fitted_open", "open_layer_speed"])
 def test_gpu_every_stream_arrangement_steps_as_the_reference_does(name):
     # The step's kernels on three streams, on two (the layer then the special rows beside the
-    # sweep; or the special rows after the sweep, the layer beside them) and on one: each gives the
-    # reference's series to the bit, also when the arrangement changes between runs.
+    # sweep; or the special rows after the sweep, the layer beside them), on one, and on three or
+    # two with the special rows at the highest priority: each gives the reference's series to the
+    # bit, also when the arrangement changes between runs.
     layout, signal, reference = load_golden(name)
-    for mode in (0, 1, 2, 3):
+    for mode in (0, 1, 2, 3, 4, 5):
         gpu = B200WaveSolver(layout)
         gpu.set_streams(mode)
         assert gpu.tiles()["concurrent"] == mode
         assert np.array_equal(_pieces(gpu, signal, [0, 65, 130, len(signal)]), reference), mode
     gpu = B200WaveSolver(layout)
     pieces = []
-    for (a, b), mode in zip([(0, 99), (99, 230), (230, len(signal))], [2, 3, 0]):
+    for (a, b), mode in zip([(0, 99), (99, 230), (230, len(signal))], [2, 4, 5]):
         gpu.set_streams(mode)
         pieces.append(gpu.run(signal[a:b]))
     assert np.array_equal(np.concatenate(pieces, axis=1), reference)
-    with pytest.raises(ValueError, match="0 to 3"):
-        gpu.set_streams(4)
+    with pytest.raises(ValueError, match="0 to 5"):
+        gpu.set_streams(6)
