@@ -265,7 +265,7 @@ int fdtd_set_tape_budget(fdtd_solver *solver, uint64_t bytes);
  * interior sweep's tile shape (each of the ten shapes of fdtd_tiles that fits a multiprocessor,
  * each with 1/4, 1/2, 1 and 2 times the default planes a tile, within 8 to 64), then, with the best
  * tiles, the count of blocks per multiprocessor of the matched-layer and special-row kernels and
- * the step's kernels beside one another and in turn (fdtd_set_streams), then the tiles again; the
+ * the six arrangements of the step's kernels on the streams (fdtd_set_streams), then the tiles again; the
  * best few whole choices are timed three times more and the fastest kept — and resets the state.
  * The chosen counts are written to *layer_per_sm and *special_per_sm when given (0: one thread a
  * cell); fdtd_get_tiles gives the rest. Results do not depend on any of these choices. Refused
